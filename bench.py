@@ -1,0 +1,470 @@
+#!/usr/bin/env python
+"""Headline benchmark: DGEMM TFLOP/s at FP64 accuracy, 8192^3, Ozaki-INT8 vs native FP64 on B200.
+
+Workload (the reference's dgemm contract, routines/dgemm/dgemm.h:9): row-major C = alpha*A*B + beta*C,
+M = N = K = 8192, alpha = 1.5, beta = 0.5, entries u*2^e with u ~ U[-1,1) and e ~ U{-phi..phi}
+(phi = 0 by default), C0 from the same law; seeded synthetic data generated on the device.
+
+One step = one full DGEMM through the Ozaki INT8 path (exponent + split passes, tcgen05 INT8 slice
+products, fused FP64 recombination). The slice count is the smallest one whose measured
+componentwise error |C - C_exact| / (|alpha||A||B| + |beta||C0|) on sampled rows is no worse than the
+native FP64 path's on the same rows (C_exact from the compensated CPU oracle); that selection runs
+before the timed region. The native FP64 tensor-core kernel and cuBLAS DGEMM are timed alongside.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: replicas only (each rank runs its own 8192^3 problem; no data exchange), weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "DGEMM TFLOP/s at FP64 accuracy, 8192^3: Ozaki-INT8 vs native FP64 on 1 B200"
+UNIT = "TFLOP/s"
+SEED = 1234
+DMMA_PEAK_TFLOPS = 37.0  # measured FP64 mma.sync peak on this pool's B200s (profiles/dmma_peak_b200.md)
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            pass
+    return {}
+
+
+def profile_traffic(name: str):
+    """DRAM bytes per launch recorded in a committed ncu summary (profiles/<name>.txt), or None."""
+    p = ROOT / "profiles" / f"{name}.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if self.proc is None or self.file is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[3]) if v.lower() == "active"})
+        loaded = [r for r in rows if r[2] > 200.0] or rows
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max(r[1] for r in rows),
+                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU legs (oracle = checker; used only for the accuracy selection and the CPU baselines)
+# ------------------------------------------------------------------------------------------------
+def cpu_baseline_blocked(N: int, rows: int, phi: int, threads: int) -> dict:
+    import oracle
+
+    oracle.build()
+    A = oracle.fill(rows, N, 1, phi, SEED)
+    B = oracle.fill(N, N, 2, phi, SEED)
+    C0 = oracle.fill(rows, N, 3, phi, SEED)
+    t0 = time.perf_counter()
+    oracle.dgemm_blocked(A, B, C0, 1.5, 0.5, threads)
+    dt = time.perf_counter() - t0
+    return {"value": 2.0 * rows * N * N / dt / 1e12, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"host blocked FP64 DGEMM (oracle/oracle_blocked.c) on {rows} rows of the {N}^3 problem "
+                      f"({2.0 * rows * N * N:.3g} flop, {dt:.2f} s wall on {threads} threads)"}
+
+
+_REF_STATE = {}
+
+
+def _ref_init(shm_name: str, N: int, phi: int):
+    import ctypes
+    from multiprocessing import shared_memory
+
+    import numpy as np
+    import oracle
+
+    shm = shared_memory.SharedMemory(name=shm_name)
+    _REF_STATE["shm"] = shm
+    _REF_STATE["B"] = np.ndarray((N, N), dtype=np.float64, buffer=shm.buf)
+    R = oracle.ref_lib()
+    if R is not None:
+        _REF_STATE["fn"] = R.ref_dgemm_host
+        _REF_STATE["kind"] = "reference"
+    else:
+        _REF_STATE["fn"] = oracle.lib().oracle_dgemm_naive
+        _REF_STATE["kind"] = "port"
+    _REF_STATE["N"] = N
+    _REF_STATE["phi"] = phi
+
+
+def _ref_rows(row0: int, rows: int):
+    import numpy as np
+    import oracle
+
+    N, phi = _REF_STATE["N"], _REF_STATE["phi"]
+    A = np.empty((rows, N))
+    C = np.empty((rows, N))
+    # rows row0.. of A and C0 of the full problem (same generator indices as the device fill)
+    full_a = oracle.fill(1, (row0 + rows) * N, 1, phi, SEED).reshape(-1, N)[row0:row0 + rows]
+    full_c = oracle.fill(1, (row0 + rows) * N, 3, phi, SEED).reshape(-1, N)[row0:row0 + rows]
+    A[:] = full_a
+    C[:] = full_c
+    B = _REF_STATE["B"]
+    t0 = time.perf_counter()
+    _REF_STATE["fn"](A.ctypes.data, B.ctypes.data, C.ctypes.data, rows, N, N, 1.5, 0.5)
+    return time.perf_counter() - t0, _REF_STATE["kind"]
+
+
+def run_reference(args) -> None:
+    """The reference's own CPU implementation of the path (routines/dgemm/dgemm.cpp:122-133, built
+    from its sources into oracle/_ref; the oracle restatement if that build is absent), on all host
+    cores (one process per core, each running the reference loop on its own rows)."""
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    from multiprocessing import shared_memory
+
+    import numpy as np
+    import oracle
+
+    oracle.build()
+    N = args.size
+    cores = len(os.sched_getaffinity(0))
+    B = oracle.fill(N, N, 2, args.phi, SEED)
+    shm = shared_memory.SharedMemory(create=True, size=B.nbytes)
+    try:
+        np.ndarray(B.shape, dtype=np.float64, buffer=shm.buf)[:] = B
+        del B
+        ctx = mp.get_context("spawn")
+        rows_per_proc = 1
+        with ctx.Pool(cores, initializer=_ref_init, initargs=(shm.name, N, args.phi)) as pool:
+            times = []
+            kind = "reference"
+            for step in range(args.warmup + args.steps):
+                t0 = time.perf_counter()
+                res = pool.starmap(_ref_rows, [(i * rows_per_proc, rows_per_proc) for i in range(cores)])
+                dt = time.perf_counter() - t0
+                kind = res[0][1]
+                if step >= args.warmup:
+                    times.append(dt)
+        flops = 2.0 * cores * rows_per_proc * N * N
+        ms = 1e3 * sum(times) / len(times)
+        value = flops / (ms * 1e-3) / 1e12
+        sample = (f"{cores * rows_per_proc} rows of the {N}^3 problem per step ({flops:.3g} flop), "
+                  f"reference loop dgemm.cpp:122-133, one process per core")
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+                "config": {"workload": f"dgemm {N}^3 alpha=1.5 beta=0.5 phi={args.phi}", "M": N, "N": N, "K": N,
+                           "sample_rows_per_step": cores * rows_per_proc},
+                "impl": "reference",
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+    finally:
+        shm.close()
+        shm.unlink()
+
+
+# ------------------------------------------------------------------------------------------------
+# GPU arm
+# ------------------------------------------------------------------------------------------------
+def pairs(s: int) -> int:
+    return s * (s + 1) // 2
+
+
+def run_ours(args) -> None:
+    import numpy as np
+    import torch
+
+    import libthom_b200 as lt
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    N = M = K = args.size
+    alpha, beta = 1.5, 0.5
+    flop = 2.0 * M * N * K
+
+    A = torch.empty(M, K, dtype=torch.float64, device=dev)
+    B = torch.empty(K, N, dtype=torch.float64, device=dev)
+    C0 = torch.empty(M, N, dtype=torch.float64, device=dev)
+    C = torch.empty(M, N, dtype=torch.float64, device=dev)
+    lt.fill(A, M * K, SEED, 1, args.phi, stream)
+    lt.fill(B, K * N, SEED, 2, args.phi, stream)
+    lt.fill(C0, M * N, SEED, 3, args.phi, stream)
+    torch.cuda.synchronize()
+
+    # ---- accuracy selection (untimed): smallest slice count no worse than native FP64 ----
+    import oracle
+
+    rows = np.linspace(0, M - 1, args.check_rows).astype(np.int64)
+    Ah = A.cpu().numpy()
+    Bh = B.cpu().numpy()
+    C0h = C0.cpu().numpy()
+    t0 = time.perf_counter()
+    Cref, den = oracle.dot2_rows(Ah, Bh, C0h, alpha, beta, rows=rows)
+    oracle_s = time.perf_counter() - t0
+    del Ah, Bh
+
+    def err_of(Cdev):
+        Cs = Cdev[torch.from_numpy(rows).to(dev)].cpu().numpy()
+        return oracle.componentwise_error(Cs, Cref, den)[0]
+
+    C.copy_(C0)
+    lt.dgemm_fp64(A, B, C, M, N, K, alpha, beta, stream)
+    torch.cuda.synchronize()
+    err_fp64 = err_of(C)
+    C.copy_(C0)
+    lt.dgemm_cublas(A, B, C, M, N, K, alpha, beta, stream)
+    torch.cuda.synchronize()
+    err_cublas = err_of(C)
+    ws = torch.empty(lt.ozaki_workspace_size(M, N, K, lt.LT_OZAKI_MAX_SLICES), dtype=torch.uint8, device=dev)
+    errs = {}
+    chosen = None
+    for s in (range(args.slices, args.slices + 1) if args.slices else range(6, lt.LT_OZAKI_MAX_SLICES + 1)):
+        C.copy_(C0)
+        lt.dgemm_ozaki(A, B, C, M, N, K, alpha, beta, s, stream, workspace=ws)
+        torch.cuda.synchronize()
+        errs[s] = err_of(C)
+        if errs[s] <= err_fp64:
+            chosen = s
+            break
+    if chosen is None:
+        chosen = max(errs)
+    s = chosen
+    lt.device_status()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- headline: Ozaki INT8 path, inputs resident in HBM (512 MiB each > 126 MB L2) ----
+    for _ in range(args.warmup):
+        lt.ozaki_split(A, B, M, N, K, s, ws, stream)
+        lt.ozaki_product(C, M, N, K, alpha, beta, s, ws, stream)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    barrier()
+    with ClockSampler(local) as clk:
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for i in range(args.steps):
+            ev[i][0].record(stream)
+            lt.ozaki_split(A, B, M, N, K, s, ws, stream)
+            ev[i][1].record(stream)
+            lt.ozaki_product(C, M, N, K, alpha, beta, s, ws, stream)
+            ev[i][2].record(stream)
+        stop.record(stream)
+        barrier()
+    total_ms = max_over_ranks(start.elapsed_time(stop))
+    split_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
+    prod_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in ev)
+    lt.device_status()
+    ms_step = total_ms / args.steps
+    value = world * flop / (ms_step * 1e-3) / 1e12
+
+    # ---- native FP64 tensor-core path and cuBLAS, same inputs ----
+    def time_loop(fn) -> float:
+        for _ in range(args.warmup):
+            fn()
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            fn()
+        b.record(stream)
+        barrier()
+        return max_over_ranks(a.elapsed_time(b)) / args.steps
+
+    fp64_ms = time_loop(lambda: lt.dgemm_fp64(A, B, C, M, N, K, alpha, beta, stream))
+    cublas_ms = time_loop(lambda: lt.dgemm_cublas(A, B, C, M, N, K, alpha, beta, stream))
+    lt.device_status()
+
+    # ---- end to end through the C ABI with host buffers (pinned), copies inside the timed region ----
+    Ah = torch.empty(M, K, dtype=torch.float64, pin_memory=True)
+    Bh = torch.empty(K, N, dtype=torch.float64, pin_memory=True)
+    C0h = torch.empty(M, N, dtype=torch.float64, pin_memory=True)
+    Ch = torch.empty(M, N, dtype=torch.float64, pin_memory=True)
+    Ah.copy_(A)
+    Bh.copy_(B)
+    C0h.copy_(C0)
+    Ad = torch.empty_like(A)
+    Bd = torch.empty_like(B)
+    Cd = torch.empty_like(C)
+    e2e_steps = max(1, min(args.steps, 3))
+
+    def e2e_step():
+        Ad.copy_(Ah, non_blocking=True)
+        Bd.copy_(Bh, non_blocking=True)
+        Cd.copy_(C0h, non_blocking=True)
+        lt.check(lt.lib().lt_dgemm_ozaki(Ad.data_ptr(), Bd.data_ptr(), Cd.data_ptr(), M, N, K, alpha, beta, s,
+                                         stream.cuda_stream))
+        Ch.copy_(Cd, non_blocking=True)
+
+    e2e_step()
+    barrier()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    b.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(a.elapsed_time(b)) / e2e_steps
+    e2e_value = world * flop / (e2e_ms * 1e-3) / 1e12
+    del Ah, Bh, C0h, Ch, Ad, Bd, Cd
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    peaks = measured_peaks()
+    bf16 = peaks.get("bf16_tflops")
+    int8_peak = 2.0 * bf16 if bf16 else 2.0 * 1590.0
+    int8_ops = pairs(s) * flop
+    achieved = int8_ops / (prod_ms * 1e-3) / 1e12
+    traffic = profile_traffic("ozaki_gemm_8192")
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_blocked(N, args.cpu_rows, args.phi, len(os.sched_getaffinity(0)))
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (int8 slices, int32 accumulate)", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"dgemm {N}^3 alpha={alpha} beta={beta} phi={args.phi}, Ozaki-INT8 s={s}",
+                   "M": M, "N": N, "K": K, "slices": s, "pairs": pairs(s),
+                   "l2": "inputs larger than L2 (512 MiB per matrix), no flush",
+                   "parallelism": f"replicas x{world}"},
+        "accuracy": {"max_componentwise_err": {"ozaki": errs[s], "native_fp64": err_fp64, "cublas": err_cublas},
+                     "ozaki_by_slices": errs, "rows_checked": len(rows),
+                     "oracle": f"compensated Dot2 on {len(rows)} rows ({oracle_s:.1f} s)"},
+        "native_fp64": {"value": world * flop / (fp64_ms * 1e-3) / 1e12, "ms_per_step": fp64_ms,
+                        "frac_of_dmma_peak": flop / (fp64_ms * 1e-3) / 1e12 / DMMA_PEAK_TFLOPS},
+        "cublas_fp64": {"value": world * flop / (cublas_ms * 1e-3) / 1e12, "ms_per_step": cublas_ms},
+        "speedup_vs_native_fp64": fp64_ms / ms_step,
+        "stages_ms": {"split": split_ms, "product": prod_ms},
+        "roofline": {"bound": "tensor", "kernel": "ozaki_gemm_kernel", "achieved": achieved,
+                     "peak": int8_peak, "unit": "TOP/s (INT8)", "frac": achieved / int8_peak,
+                     "peak_source": "2 x bf16_tflops of MEASURED_PEAKS.json (dense INT8 = 2x dense BF16 on B200)"
+                     if bf16 else "2 x 1590 fallback", "traffic": traffic,
+                     "algorithmic": f"{pairs(s)} INT8 slice products x 2MNK = {int8_ops:.4g} ops per launch"},
+        "roofline_fp64": {"bound": "tensor", "kernel": "dgemm_fp64_kernel",
+                          "achieved": flop / (fp64_ms * 1e-3) / 1e12, "peak": DMMA_PEAK_TFLOPS,
+                          "unit": "TFLOP/s (FP64)", "frac": flop / (fp64_ms * 1e-3) / 1e12 / DMMA_PEAK_TFLOPS,
+                          "peak_source": "measured mma.sync f64 throughput (profiles/dmma_peak_b200.md)"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * M * N,
+                "d2h_bytes_per_step": 8 * M * N, "ms_per_step": e2e_ms,
+                "path": "lt_dgemm_ozaki C ABI, pinned host buffers, H2D A,B,C0 + D2H C in the timed region"},
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "gpu_launches": 5 * args.steps,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=8192)
+    ap.add_argument("--phi", type=int, default=0)
+    ap.add_argument("--slices", type=int, default=0, help="fix the slice count (0 = accuracy-matched)")
+    ap.add_argument("--check-rows", type=int, default=16)
+    ap.add_argument("--cpu-rows", type=int, default=1024)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps, reported as run
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,185 @@
+/*
+ * libthom_dgemm.h — C ABI of the sm_100a (B200) DGEMM library for libthom's `dgemm` routine.
+ *
+ * Every matrix is row-major and contiguous, as in the reference: A[i*K+k], B[k*N+j], C[i*N+j],
+ * C = alpha*A*B + beta*C (routines/dgemm/dgemm.h:9, routines/dgemm/dgemm.cpp:36,122-133).
+ * Pointers are device pointers unless a function says otherwise. When beta == 0, C is not read
+ * (BLAS convention; the reference computes 0*C, which differs only if C holds NaN or Inf).
+ *
+ * Two families of entry points:
+ *  - dgemm_<impl>(...) -> float: the reference's implementation contract (dgemm.h:9): synchronous
+ *    on the legacy default stream, returns the elapsed milliseconds measured with CUDA events
+ *    around every pass of the implementation. Failures are printed to stderr, as the reference
+ *    wrappers do (e.g. routines/dgemm/dgemm_final.cu:204-207), and recorded for
+ *    lt_get_last_error().
+ *  - lt_*(...) -> int: asynchronous on the given stream (NULL = legacy default stream),
+ *    returning an LT_* status code.
+ */
+#ifndef LIBTHOM_DGEMM_H
+#define LIBTHOM_DGEMM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------------- */
+#define LT_OK 0
+#define LT_ERR_INVALID_ARGUMENT 1 /* bad size, null pointer, slice count out of range */
+#define LT_ERR_UNALIGNED 2        /* a pointer is not 16-byte aligned where a kernel needs it */
+#define LT_ERR_CUDA 3             /* a CUDA runtime call failed (message: lt_last_error_message) */
+#define LT_ERR_NO_MEMORY 4        /* workspace allocation failed or a caller workspace is too small */
+#define LT_ERR_DEVICE_TIMEOUT 5   /* a bounded device-side wait gave up (pipeline fault) */
+#define LT_ERR_UNSUPPORTED 6      /* not an sm_100 device, or a feature missing on it */
+#define LT_ERR_NOT_FOUND 7        /* unknown implementation / config name, missing file */
+
+/* Last status recorded by any entry point of this library on the calling host thread. */
+int lt_get_last_error(void);
+const char* lt_error_string(int code);
+const char* lt_last_error_message(void);
+/* Reads (and clears) the device error word written by bounded waits inside the kernels; call after
+ * a synchronize. Returns LT_OK or LT_ERR_DEVICE_TIMEOUT. */
+int lt_check_device_status(void);
+int lt_version(void);
+
+/* ---- reference-contract implementations (routines/dgemm/dgemm.h:8-42 registry entries) ------ */
+/* Native FP64 tensor-core DGEMM: TMA-staged, warp-specialised DMMA (no reference counterpart;
+ * replaces the reference's best kernel dgemm_final, routines/dgemm/dgemm_final.cu:175-213). */
+float dgemm_tc100(const double* A, const double* B, double* C, size_t M, size_t N, size_t K,
+                  double alpha, double beta);
+/* Ozaki INT8-slice DGEMM with s = 3..10 slices (tcgen05 kind::i8 products, FP64 recombination). */
+float dgemm_ozaki3(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);
+float dgemm_ozaki4(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);
+float dgemm_ozaki5(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);
+float dgemm_ozaki6(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);
+float dgemm_ozaki7(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);
+float dgemm_ozaki8(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);
+float dgemm_ozaki9(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);
+float dgemm_ozaki10(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);
+/* Ozaki DGEMM whose slice count is picked per call by the learned selector (analytic fallback);
+ * the target tolerance is lt_set_ozaki_tolerance() (default 1e-15). */
+float dgemm_ozaki_auto(const double* A, const double* B, double* C, size_t M, size_t N, size_t K,
+                       double alpha, double beta);
+/* The reference's cuBLAS baseline, same call (routines/dgemm/dgemm_cublas_tc.cu:4-33):
+ * cublasGemmEx, CUBLAS_COMPUTE_64F, row-major through the transposition trick. */
+float dgemm_cublas_tc(const double* A, const double* B, double* C, size_t M, size_t N, size_t K,
+                      double alpha, double beta);
+
+/* ---- stream-ordered API --------------------------------------------------------------------- */
+int lt_dgemm_fp64(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
+                  double alpha, double beta, void* stream);
+/* Runs one specific FP64 kernel configuration (index into lt_fp64_config_name); -1 = tuned choice. */
+int lt_dgemm_fp64_config(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
+                         double alpha, double beta, int config, void* stream);
+int lt_fp64_num_configs(void);
+const char* lt_fp64_config_name(int config);
+
+#define LT_OZAKI_MAX_SLICES 12
+/* Ozaki DGEMM using the library's cached per-device workspace (grown with cudaMalloc on demand). */
+int lt_dgemm_ozaki(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
+                   double alpha, double beta, int slices, void* stream);
+/* Same, with a caller-provided device workspace of at least lt_ozaki_workspace_size() bytes,
+ * 256-byte aligned. Performs no allocation. */
+size_t lt_ozaki_workspace_size(int64_t M, int64_t N, int64_t K, int slices);
+int lt_dgemm_ozaki_ws(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
+                      double alpha, double beta, int slices, void* workspace, size_t workspace_bytes,
+                      void* stream);
+/* The two stages of lt_dgemm_ozaki_ws, for callers that time or overlap them separately:
+ * lt_ozaki_split writes the exponents and INT8 slices of A and B into the workspace;
+ * lt_ozaki_product runs the tensor-core slice products and the fused FP64 recombination into C.
+ * The same workspace (and M, N, K, slices) must be passed to both. */
+int lt_ozaki_split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int slices,
+                   void* workspace, size_t workspace_bytes, void* stream);
+int lt_ozaki_product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int slices,
+                     const void* workspace, size_t workspace_bytes, void* stream);
+int lt_dgemm_cublas(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
+                    double alpha, double beta, void* stream);
+
+/* ---- grouped / batched DGEMM (the `dgemmb` routine) ----------------------------------------- */
+typedef struct lt_gemm_problem {
+  int64_t M, N, K;
+  const double* A; /* device, row-major M x K */
+  const double* B; /* device, row-major K x N */
+  double* C;       /* device, row-major M x N */
+  double alpha, beta;
+} lt_gemm_problem;
+
+#define LT_FORM_FP64 0
+#define LT_FORM_OZAKI 1
+typedef struct lt_grouped_plan lt_grouped_plan;
+/* Builds the device-side problem table and tile queue for `count` problems (host array). */
+int lt_grouped_plan_create(const lt_gemm_problem* problems, int count, int form, int slices,
+                           lt_grouped_plan** plan);
+/* One persistent grouped launch (FP64) or split + grouped INT8 + recombine launches (Ozaki). */
+int lt_grouped_plan_run(lt_grouped_plan* plan, void* stream);
+/* Captures lt_grouped_plan_run into a CUDA graph once, then replays it on `stream`. */
+int lt_grouped_plan_run_graph(lt_grouped_plan* plan, void* stream);
+int lt_grouped_plan_info(const lt_grouped_plan* plan, int64_t* tiles, double* flops);
+void lt_grouped_plan_destroy(lt_grouped_plan* plan);
+/* Convenience: create, run once, destroy. */
+int lt_dgemm_grouped(const lt_gemm_problem* problems, int count, int form, int slices, void* stream);
+
+/* ---- autotuner ------------------------------------------------------------------------------ */
+typedef struct lt_tune_entry {
+  int config;        /* chosen FP64 config index */
+  float ms;          /* median time of the chosen config */
+  float max_rel_err; /* validation error of the chosen config vs cuBLAS FP64 */
+} lt_tune_entry;
+/* Validates every FP64 candidate on an M x N x K problem (against cuBLAS FP64), times the valid
+ * ones (median of `iters`), records the winner for the shape class and returns it. */
+int lt_tune_fp64(int64_t M, int64_t N, int64_t K, int iters, lt_tune_entry* best);
+int lt_tuner_save(const char* path);
+int lt_tuner_load(const char* path);
+int lt_tuner_lookup(int64_t M, int64_t N, int64_t K);
+
+/* ---- learned slice-count selector ---------------------------------------------------------- */
+#define LT_SEL_FEATURES 34
+#define LT_SEL_HIDDEN 64
+#define LT_SEL_CLASSES 8 /* slice counts 3..10 */
+#define LT_SEL_PARAMS (LT_SEL_FEATURES * LT_SEL_HIDDEN + LT_SEL_HIDDEN + LT_SEL_HIDDEN * LT_SEL_HIDDEN + LT_SEL_HIDDEN + LT_SEL_HIDDEN * LT_SEL_CLASSES + LT_SEL_CLASSES)
+/* Features of one problem (device output, 34 floats): 16-bin histogram of the row exponent spreads
+ * of A, 16-bin histogram of the column exponent spreads of B, log2 K, log10 tol. */
+int lt_ozaki_features(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol,
+                      float* features, void* stream);
+/* MLP 34 -> 64 -> 64 -> 8 (GELU, tanh form), softmax over slice counts 3..10. Parameters are one
+ * flat float array of LT_SEL_PARAMS (W1, b1, W2, b2, W3, b3; W row-major [out][in]). */
+int lt_mlp_forward(const float* params, const float* x, int batch, float* probs, void* stream);
+/* One Adam step on a batch: x [batch][34], labels [batch] in 0..7; grads and moments are
+ * device arrays of LT_SEL_PARAMS floats. Writes the mean cross-entropy loss to *loss (device). */
+int lt_mlp_train_step(float* params, float* m, float* v, float* grads, const float* x, const int* labels,
+                      int batch, float lr, int step, float* loss, void* stream);
+/* Gradient only (for the gradient check against the CPU oracle). */
+int lt_mlp_backward(const float* params, const float* x, const int* labels, int batch, float* grads,
+                    float* loss, void* stream);
+/* Installs selector weights (host array of LT_SEL_PARAMS floats) used by dgemm_ozaki_auto;
+ * NULL removes them, leaving the analytic fallback. */
+int lt_selector_set_params(const float* host_params);
+void lt_set_ozaki_tolerance(double tol);
+/* Analytic (conservative) slice count for a tolerance, K and exponent spread. */
+int lt_ozaki_analytic_slices(double tol, int64_t K, int phi_spread);
+/* Slice count the selector picks for this problem (learned when weights are installed and the
+ * prediction is confident, analytic otherwise). */
+int lt_ozaki_select_slices(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol,
+                           int* slices, void* stream);
+
+/* ---- harness helpers (replace the reference's cuRAND fill, routines/dgemm/dgemm.cpp:100-119) -- */
+/* X[i] = u 2^e, u ~ U[-1,1), e ~ U{-phi..phi}; counter-based, identical to the CPU oracle. */
+int lt_fill(double* X, int64_t n, uint64_t seed, uint64_t stream_id, int phi, void* stream);
+int lt_scale_rows(double* X, int64_t rows, int64_t cols, uint64_t seed, uint64_t stream_id, int smax, void* stream);
+int lt_scale_cols(double* X, int64_t rows, int64_t cols, uint64_t seed, uint64_t stream_id, int smax, void* stream);
+/* Componentwise error of C against Cref with denominator den (all device, n elements):
+ * out_host[0] = max |C-Cref|/den, out_host[1] = count of elements above `tol`. Synchronous. */
+int lt_componentwise_error(const double* C, const double* Cref, const double* den, int64_t n, double tol,
+                           double* out_host, void* stream);
+/* den = |alpha| |A||B| + |beta| |C0| on the device (FP64 kernel on absolute values). */
+int lt_abs_denominator(const double* A, const double* B, const double* C0, double* den, int64_t M, int64_t N,
+                       int64_t K, double alpha, double beta, void* stream);
+/* Writes over the whole L2 (twice its size), as the reference's flushL2 (routines/common.cpp:12-24). */
+int lt_flush_l2(void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LIBTHOM_DGEMM_H */

@@ -1,0 +1,228 @@
+"""libthom_b200 — sm_100a (B200) DGEMM for libthom's `dgemm` routine.
+
+The product is the C-ABI shared library ``liblibthom_dgemm.so`` built from ``csrc/`` (declared in
+``include/libthom_dgemm.h``). This module only loads it with ctypes and gives Python callers the
+same entry points; it never computes anything itself. If the library is missing or no sm_100 GPU
+is present, calls raise — there is no CPU fallback.
+
+Implementation registry (the reference's ``dgemmImpls``, routines/dgemm/dgemm.cpp:36-68):
+``tc100`` (native FP64 tensor cores), ``ozaki3`` .. ``ozaki10`` (INT8 Ozaki slices),
+``ozaki_auto`` (learned slice selector) and ``cublas_tc`` (the reference's cuBLAS baseline).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "liblibthom_dgemm.so"
+
+LT_OK = 0
+LT_ERR_INVALID_ARGUMENT = 1
+LT_ERR_UNALIGNED = 2
+LT_ERR_CUDA = 3
+LT_ERR_NO_MEMORY = 4
+LT_ERR_DEVICE_TIMEOUT = 5
+LT_ERR_UNSUPPORTED = 6
+LT_ERR_NOT_FOUND = 7
+LT_OZAKI_MAX_SLICES = 12
+LT_FORM_FP64 = 0
+LT_FORM_OZAKI = 1
+LT_SEL_FEATURES = 34
+LT_SEL_HIDDEN = 64
+LT_SEL_CLASSES = 8
+LT_SEL_PARAMS = (LT_SEL_FEATURES * LT_SEL_HIDDEN + LT_SEL_HIDDEN + LT_SEL_HIDDEN * LT_SEL_HIDDEN +
+                 LT_SEL_HIDDEN + LT_SEL_HIDDEN * LT_SEL_CLASSES + LT_SEL_CLASSES)
+
+IMPLS = ["tc100"] + [f"ozaki{s}" for s in range(3, 11)] + ["ozaki_auto", "cublas_tc"]
+
+_c = ctypes
+_vp, _i64, _i32, _f64, _f32, _sz = _c.c_void_p, _c.c_int64, _c.c_int, _c.c_double, _c.c_float, _c.c_size_t
+_u64 = _c.c_uint64
+
+
+class LtError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"libthom_dgemm error {code}: {message}")
+        self.code = code
+
+
+class GemmProblem(ctypes.Structure):
+    """lt_gemm_problem (include/libthom_dgemm.h)."""
+    _fields_ = [("M", _i64), ("N", _i64), ("K", _i64), ("A", _vp), ("B", _vp), ("C", _vp),
+                ("alpha", _f64), ("beta", _f64)]
+
+
+class TuneEntry(ctypes.Structure):
+    _fields_ = [("config", _i32), ("ms", _f32), ("max_rel_err", _f32)]
+
+
+# name -> (restype, argtypes)
+_GEMM = [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64]
+_REF = [_vp, _vp, _vp, _sz, _sz, _sz, _f64, _f64]
+SIGNATURES = {
+    "lt_get_last_error": (_i32, []),
+    "lt_error_string": (_c.c_char_p, [_i32]),
+    "lt_last_error_message": (_c.c_char_p, []),
+    "lt_check_device_status": (_i32, []),
+    "lt_version": (_i32, []),
+    "dgemm_tc100": (_f32, _REF),
+    "dgemm_ozaki3": (_f32, _REF), "dgemm_ozaki4": (_f32, _REF), "dgemm_ozaki5": (_f32, _REF),
+    "dgemm_ozaki6": (_f32, _REF), "dgemm_ozaki7": (_f32, _REF), "dgemm_ozaki8": (_f32, _REF),
+    "dgemm_ozaki9": (_f32, _REF), "dgemm_ozaki10": (_f32, _REF),
+    "dgemm_ozaki_auto": (_f32, _REF),
+    "dgemm_cublas_tc": (_f32, _REF),
+    "lt_dgemm_fp64": (_i32, _GEMM + [_vp]),
+    "lt_dgemm_fp64_config": (_i32, _GEMM + [_i32, _vp]),
+    "lt_fp64_num_configs": (_i32, []),
+    "lt_fp64_config_name": (_c.c_char_p, [_i32]),
+    "lt_dgemm_ozaki": (_i32, _GEMM + [_i32, _vp]),
+    "lt_ozaki_workspace_size": (_sz, [_i64, _i64, _i64, _i32]),
+    "lt_dgemm_ozaki_ws": (_i32, _GEMM + [_i32, _vp, _sz, _vp]),
+    "lt_ozaki_split": (_i32, [_vp, _vp, _i64, _i64, _i64, _i32, _vp, _sz, _vp]),
+    "lt_ozaki_product": (_i32, [_vp, _i64, _i64, _i64, _f64, _f64, _i32, _vp, _sz, _vp]),
+    "lt_dgemm_cublas": (_i32, _GEMM + [_vp]),
+    "lt_grouped_plan_create": (_i32, [_vp, _i32, _i32, _i32, _c.POINTER(_vp)]),
+    "lt_grouped_plan_run": (_i32, [_vp, _vp]),
+    "lt_grouped_plan_run_graph": (_i32, [_vp, _vp]),
+    "lt_grouped_plan_info": (_i32, [_vp, _c.POINTER(_i64), _c.POINTER(_f64)]),
+    "lt_grouped_plan_destroy": (None, [_vp]),
+    "lt_dgemm_grouped": (_i32, [_vp, _i32, _i32, _i32, _vp]),
+    "lt_tune_fp64": (_i32, [_i64, _i64, _i64, _i32, _c.POINTER(TuneEntry)]),
+    "lt_tuner_save": (_i32, [_c.c_char_p]),
+    "lt_tuner_load": (_i32, [_c.c_char_p]),
+    "lt_tuner_lookup": (_i32, [_i64, _i64, _i64]),
+    "lt_ozaki_features": (_i32, [_vp, _vp, _i64, _i64, _i64, _f64, _vp, _vp]),
+    "lt_mlp_forward": (_i32, [_vp, _vp, _i32, _vp, _vp]),
+    "lt_mlp_train_step": (_i32, [_vp, _vp, _vp, _vp, _vp, _vp, _i32, _f32, _i32, _vp, _vp]),
+    "lt_mlp_backward": (_i32, [_vp, _vp, _vp, _i32, _vp, _vp, _vp]),
+    "lt_selector_set_params": (_i32, [_vp]),
+    "lt_set_ozaki_tolerance": (None, [_f64]),
+    "lt_ozaki_analytic_slices": (_i32, [_f64, _i64, _i32]),
+    "lt_ozaki_select_slices": (_i32, [_vp, _vp, _i64, _i64, _i64, _f64, _c.POINTER(_i32), _vp]),
+    "lt_fill": (_i32, [_vp, _i64, _u64, _u64, _i32, _vp]),
+    "lt_scale_rows": (_i32, [_vp, _i64, _i64, _u64, _u64, _i32, _vp]),
+    "lt_scale_cols": (_i32, [_vp, _i64, _i64, _u64, _u64, _i32, _vp]),
+    "lt_componentwise_error": (_i32, [_vp, _vp, _vp, _i64, _f64, _c.POINTER(_f64), _vp]),
+    "lt_abs_denominator": (_i32, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _vp]),
+    "lt_flush_l2": (_i32, [_vp]),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded C-ABI library. Raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m libthom_b200.build` "
+                               "(the DGEMM has no CPU fallback)")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name, None)
+            if fn is None:
+                continue
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != LT_OK:
+        msg = lib().lt_last_error_message()
+        raise LtError(rc, (msg or b"").decode(errors="replace"))
+
+
+def _ptr(x) -> int:
+    """Device pointer of a torch tensor, or an int pointer as is."""
+    if isinstance(x, int):
+        return x
+    return x.data_ptr()
+
+
+def _stream(stream) -> int | None:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def dgemm(impl: str, A, B, C, M: int, N: int, K: int, alpha: float = 1.0, beta: float = 0.0) -> float:
+    """Reference-contract call (routines/dgemm/dgemm.h:9): synchronous, returns elapsed ms."""
+    if impl not in IMPLS:
+        raise KeyError(f"unknown implementation {impl!r}; available: {' '.join(IMPLS)}")
+    fn = getattr(lib(), "dgemm_" + impl)
+    ms = fn(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta)
+    check(lib().lt_get_last_error())
+    return ms
+
+
+def dgemm_fp64(A, B, C, M, N, K, alpha=1.0, beta=0.0, stream=None, config: int = -1) -> None:
+    if config < 0:
+        check(lib().lt_dgemm_fp64(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, _stream(stream)))
+    else:
+        check(lib().lt_dgemm_fp64_config(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, config,
+                                         _stream(stream)))
+
+
+def dgemm_ozaki(A, B, C, M, N, K, alpha=1.0, beta=0.0, slices=8, stream=None, workspace=None) -> None:
+    if workspace is None:
+        check(lib().lt_dgemm_ozaki(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, slices, _stream(stream)))
+    else:
+        check(lib().lt_dgemm_ozaki_ws(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, slices,
+                                      _ptr(workspace), workspace.numel() * workspace.element_size(),
+                                      _stream(stream)))
+
+
+def ozaki_split(A, B, M, N, K, slices, workspace, stream=None) -> None:
+    check(lib().lt_ozaki_split(_ptr(A), _ptr(B), M, N, K, slices, _ptr(workspace),
+                               workspace.numel() * workspace.element_size(), _stream(stream)))
+
+
+def ozaki_product(C, M, N, K, alpha, beta, slices, workspace, stream=None) -> None:
+    check(lib().lt_ozaki_product(_ptr(C), M, N, K, alpha, beta, slices, _ptr(workspace),
+                                 workspace.numel() * workspace.element_size(), _stream(stream)))
+
+
+def dgemm_cublas(A, B, C, M, N, K, alpha=1.0, beta=0.0, stream=None) -> None:
+    check(lib().lt_dgemm_cublas(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, _stream(stream)))
+
+
+def ozaki_workspace_size(M, N, K, slices) -> int:
+    return int(lib().lt_ozaki_workspace_size(M, N, K, slices))
+
+
+def fill(X, n: int, seed: int, stream_id: int, phi: int = 0, stream=None) -> None:
+    check(lib().lt_fill(_ptr(X), n, seed, stream_id, phi, _stream(stream)))
+
+
+def scale_rows(X, rows, cols, seed, stream_id, smax, stream=None) -> None:
+    check(lib().lt_scale_rows(_ptr(X), rows, cols, seed, stream_id, smax, _stream(stream)))
+
+
+def scale_cols(X, rows, cols, seed, stream_id, smax, stream=None) -> None:
+    check(lib().lt_scale_cols(_ptr(X), rows, cols, seed, stream_id, smax, _stream(stream)))
+
+
+def device_status() -> None:
+    check(lib().lt_check_device_status())
+
+
+def fp64_configs() -> list[str]:
+    L = lib()
+    return [L.lt_fp64_config_name(i).decode() for i in range(L.lt_fp64_num_configs())]
+
+
+def componentwise_error(C, Cref, den, n: int, tol: float = 0.0, stream=None) -> tuple[float, int]:
+    out = (ctypes.c_double * 2)()
+    check(lib().lt_componentwise_error(_ptr(C), _ptr(Cref), _ptr(den), n, tol, out, _stream(stream)))
+    return float(out[0]), int(out[1])
+
+
+def abs_denominator(A, B, C0, den, M, N, K, alpha, beta, stream=None) -> None:
+    check(lib().lt_abs_denominator(_ptr(A), _ptr(B), None if C0 is None else _ptr(C0), _ptr(den), M, N, K,
+                                   alpha, beta, _stream(stream)))

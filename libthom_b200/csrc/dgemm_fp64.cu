@@ -1,0 +1,111 @@
+// dgemm_fp64.cu — host launchers and configuration registry of the native FP64 DGEMM.
+#include <mutex>
+
+#include "dgemm_fp64.cuh"
+#include "lt_runtime.cuh"
+#include "lt_internal.h"
+
+namespace lt {
+namespace fp64 {
+
+namespace {
+
+template <class Cfg>
+int launch(const Params& p0, cudaStream_t stream, DeviceContext* ctx) {
+  Params p = p0;
+  p.status = ctx->status;
+  CUtensorMap tmA, tmB;
+  memset(&tmA, 0, sizeof tmA);
+  memset(&tmB, 0, sizeof tmB);
+  if (Cfg::kTMA) {
+    if (!tma_compatible(p.A, p.B, p.N, p.K))
+      return set_error(LT_ERR_UNALIGNED, "TMA configuration needs 16-byte aligned A/B and even N and K");
+    LT_TRY(make_tmap_2d(&tmA, p.A, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, static_cast<uint64_t>(p.M),
+                        static_cast<uint64_t>(p.K), static_cast<uint64_t>(p.K) * 8, Cfg::BM, 16));
+    LT_TRY(make_tmap_2d(&tmB, p.B, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, static_cast<uint64_t>(p.K),
+                        static_cast<uint64_t>(p.N), static_cast<uint64_t>(p.N) * 8, 16, 16));
+  }
+  static std::once_flag once[64];
+  static int occupancy[64];
+  static cudaError_t attr_err[64];
+  std::call_once(once[ctx->device], [&] {
+    attr_err[ctx->device] = cudaFuncSetAttribute(dgemm_fp64_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 Cfg::SMEM_BYTES);
+    int occ = 0;
+    if (attr_err[ctx->device] == cudaSuccess)
+      attr_err[ctx->device] = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, dgemm_fp64_kernel<Cfg>,
+                                                                            Cfg::THREADS, Cfg::SMEM_BYTES);
+    occupancy[ctx->device] = occ > 0 ? occ : 1;
+  });
+  LT_CUDA_TRY(attr_err[ctx->device]);
+  const int64_t tiles = ((p.M + Cfg::BM - 1) / Cfg::BM) * ((p.N + Cfg::BN - 1) / Cfg::BN);
+  int64_t grid = static_cast<int64_t>(ctx->sm_count) * occupancy[ctx->device];
+  if (grid > tiles) grid = tiles;
+  dgemm_fp64_kernel<Cfg><<<static_cast<unsigned>(grid), Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(tmA, tmB, p);
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
+using LaunchFn = int (*)(const Params&, cudaStream_t, DeviceContext*);
+
+struct Entry {
+  const char* name;
+  LaunchFn fn;
+  int bm, bn;
+  bool tma;
+};
+
+// Candidate list of the autotuner (compile-time instances, as hgemm's tuner in the reference:
+// routines/hgemm/hgemm_better_reuse.cu:378-454).
+const Entry kConfigs[] = {
+    {"tma_128x64_s6", launch<Config<128, 64, 6, true>>, 128, 64, true},
+    {"tma_64x128_s6", launch<Config<64, 128, 6, true>>, 64, 128, true},
+    {"tma_64x64_s8", launch<Config<64, 64, 8, true>>, 64, 64, true},
+    {"tma_64x32_s8", launch<Config<64, 32, 8, true>>, 64, 32, true},
+    {"tma_32x64_s8", launch<Config<32, 64, 8, true>>, 32, 64, true},
+    {"cpa_128x64_s6", launch<Config<128, 64, 6, false>>, 128, 64, false},
+    {"cpa_64x64_s6", launch<Config<64, 64, 6, false>>, 64, 64, false},
+    {"cpa_64x32_s6", launch<Config<64, 32, 6, false>>, 64, 32, false},
+    {"cpa_32x32_s6", launch<Config<32, 32, 6, false>>, 32, 32, false},
+};
+constexpr int kNumConfigs = static_cast<int>(sizeof(kConfigs) / sizeof(kConfigs[0]));
+
+}  // namespace
+
+bool tma_compatible(const double* A, const double* B, int64_t N, int64_t K) {
+  return ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) == 0 && (N % 2 == 0) &&
+         (K % 2 == 0);
+}
+
+int num_configs() { return kNumConfigs; }
+const char* config_name(int i) { return (i >= 0 && i < kNumConfigs) ? kConfigs[i].name : nullptr; }
+bool config_is_tma(int i) { return i >= 0 && i < kNumConfigs && kConfigs[i].tma; }
+
+// Default choice without a tuning table: the largest tile that still gives every SM a tile.
+int heuristic_config(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int sm_count) {
+  const bool tma = tma_compatible(A, B, N, K);
+  struct Pick { int bm, bn; };
+  const Pick order[] = {{128, 64}, {64, 64}, {64, 32}, {32, 32}};
+  int chosen_bm = 32, chosen_bn = 32;
+  for (const Pick& pk : order) {
+    int64_t tiles = ((M + pk.bm - 1) / pk.bm) * ((N + pk.bn - 1) / pk.bn);
+    if (tiles >= sm_count) { chosen_bm = pk.bm; chosen_bn = pk.bn; break; }
+  }
+  for (int i = 0; i < kNumConfigs; ++i)
+    if (kConfigs[i].tma == tma && kConfigs[i].bm == chosen_bm && kConfigs[i].bn == chosen_bn) return i;
+  for (int i = 0; i < kNumConfigs; ++i)
+    if (kConfigs[i].tma == tma && kConfigs[i].bm * kConfigs[i].bn <= chosen_bm * chosen_bn) return i;
+  return kNumConfigs - 1;
+}
+
+int run_config(int cfg, const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
+               double beta, cudaStream_t stream) {
+  if (cfg < 0 || cfg >= kNumConfigs) return set_error(LT_ERR_INVALID_ARGUMENT, "FP64 config %d out of range", cfg);
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  Params p{A, B, C, M, N, K, alpha, beta, nullptr};
+  return kConfigs[cfg].fn(p, stream, ctx);
+}
+
+}  // namespace fp64
+}  // namespace lt

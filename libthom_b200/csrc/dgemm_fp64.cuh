@@ -1,0 +1,261 @@
+// dgemm_fp64.cuh — native FP64 tensor-core DGEMM for sm_100a.
+//
+// Replaces the reference's register-fed sm_80 kernels (routines/dgemm/dgemm_final.cu:65-173:
+// 64x128x16 tiles, 2-stage cp.async, mma.sync m8n8k4) with a warp-specialised, persistent design:
+//   * one producer warp stages A (BM x 16) and B (16 x BN) k-blocks into a STAGES-deep ring of
+//     128-byte-swizzled shared-memory tiles, either with TMA (cp.async.bulk.tensor, when the
+//     row strides are 16-byte multiples) or with zero-filling cp.async for arbitrary shapes;
+//   * full/empty mbarrier pairs hand each stage to the consumer warps and back;
+//   * consumer warps each own a 32 x 32 sub-tile and issue mma.sync m16n8k16 FP64 (2048 FMAs per
+//     instruction) from fragments read with 128-bit shared loads;
+//   * the alpha/beta epilogue writes 16-byte vectors straight from the accumulators.
+// Tensor cores compute in FP64 throughout (tcgen05 has no FP64 kind on sm_100a; FP64 MMA is the
+// warp-level instruction).
+//
+// Shared-memory layout of one stage (all offsets multiples of 1024 bytes):
+//   A: BM rows x 128 bytes (16 doubles of K); 16-byte chunk c of row r sits at chunk c ^ (r & 7).
+//   B: BN/16 boxes, each 16 k-rows x 128 bytes (16 doubles of N); chunk c of k-row k sits at
+//      chunk c ^ (k & 7).
+// This is exactly what TMA's SWIZZLE_128B writes for boxes {16, BM} and {16, 16}.
+//
+// K-permutation: within a 16-wide k-block, thread t of a quad feeds the MMA's logical k = t+4i
+// with physical k = 4t+i (i = 0..3), for A and B alike. The sum over k is unchanged and every A
+// fragment becomes two contiguous 32-byte row segments (128-bit loads).
+#pragma once
+#include <cuda.h>
+
+#include "lt_common.cuh"
+
+namespace lt {
+namespace fp64 {
+
+struct Params {
+  const double* A;
+  const double* B;
+  double* C;
+  int64_t M, N, K;
+  double alpha, beta;
+  DeviceStatus* status;
+};
+
+template <int BM_, int BN_, int STAGES_, bool TMA_>
+struct Config {
+  static constexpr int BM = BM_, BN = BN_, STAGES = STAGES_;
+  static constexpr bool kTMA = TMA_;
+  static constexpr int BK = 16;  // doubles of K per stage: one 128-byte swizzle row
+  static constexpr int WM = 32, WN = 32;
+  static constexpr int WARPS_M = BM / WM, WARPS_N = BN / WN;
+  static constexpr int CONSUMERS = WARPS_M * WARPS_N;
+  static constexpr int THREADS = (CONSUMERS + 1) * 32;
+  static constexpr int A_BYTES = BM * 128;
+  static constexpr int B_BYTES = BN * 128;
+  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*alignment slack*/ + 256 /*barriers*/;
+  static_assert(BM % WM == 0 && BN % WN == 0, "tile must be a multiple of the warp tile");
+  static_assert(BN % 16 == 0 && BM % 8 == 0, "tile shape");
+};
+
+// Byte offset of the 16-byte chunk holding A(row, 2c..2c+1) in an A stage.
+__device__ __forceinline__ uint32_t a_off(int row, int chunk) {
+  return static_cast<uint32_t>(row * 128 + ((chunk ^ (row & 7)) << 4));
+}
+// Byte offset of B(k, n) (one double) in a B stage.
+__device__ __forceinline__ uint32_t b_off(int k, int n) {
+  int box = n >> 4, col = n & 15;
+  return static_cast<uint32_t>(box * 2048 + k * 128 + ((((col >> 1) ^ (k & 7)) << 4)) + ((col & 1) << 3));
+}
+
+__device__ __forceinline__ void mma_m16n8k16(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
+__device__ __forceinline__ void lds128(double& x, double& y, uint32_t addr) {
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(x), "=d"(y) : "r"(addr));
+}
+__device__ __forceinline__ double lds64(uint32_t addr) {
+  double x;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(x) : "r"(addr));
+  return x;
+}
+
+// Tile order: groups of 8 tile-rows are walked column by column so that consecutive CTAs share
+// B panels and A panels in L2.
+__device__ __forceinline__ void tile_coords(int64_t t, int64_t tiles_m, int64_t tiles_n, int64_t& tm, int64_t& tn) {
+  const int64_t G = 8;
+  int64_t group = t / (G * tiles_n);
+  int64_t first_m = group * G;
+  int64_t gsize = (tiles_m - first_m) < G ? (tiles_m - first_m) : G;
+  int64_t in_group = t - group * G * tiles_n;
+  tm = first_m + in_group % gsize;
+  tn = in_group / gsize;
+}
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS, 1)
+    dgemm_fp64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES);
+  uint64_t* empty = full + Cfg::STAGES;
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(empty + Cfg::STAGES);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t tiles_m = (p.M + Cfg::BM - 1) / Cfg::BM, tiles_n = (p.N + Cfg::BN - 1) / Cfg::BN;
+  const int64_t tiles = tiles_m * tiles_n;
+  const int kblocks = static_cast<int>((p.K + Cfg::BK - 1) / Cfg::BK);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < Cfg::STAGES; ++s) {
+      mbar_init(&full[s], Cfg::kTMA ? 1 : 32);
+      mbar_init(&empty[s], Cfg::CONSUMERS);
+    }
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (warp == Cfg::CONSUMERS) {
+    // ------------------------------- producer warp -------------------------------
+    if (Cfg::kTMA) {
+      if (lane == 0) {
+        tma_prefetch_desc(&tmA);
+        tma_prefetch_desc(&tmB);
+      }
+    }
+    int stage = 0;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+      int64_t tm, tn;
+      tile_coords(t, tiles_m, tiles_n, tm, tn);
+      const int64_t m0 = tm * Cfg::BM, n0 = tn * Cfg::BN;
+      for (int kb = 0; kb < kblocks; ++kb) {
+        if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.status, 1)) { ok = false; break; }
+        uint8_t* sa = smem + stage * Cfg::STAGE_BYTES;
+        uint8_t* sb = sa + Cfg::A_BYTES;
+        const int k0 = kb * Cfg::BK;
+        if (Cfg::kTMA) {
+          if (lane == 0) {
+            mbar_arrive_expect_tx(&full[stage], Cfg::STAGE_BYTES);
+            tma_load_2d(sa, &tmA, &full[stage], k0, static_cast<int>(m0));
+#pragma unroll
+            for (int j = 0; j < Cfg::BN / 16; ++j)
+              tma_load_2d(sb + j * 2048, &tmB, &full[stage], static_cast<int>(n0) + 16 * j, k0);
+          }
+        } else {
+          // A: BM rows x 16 doubles, one double per cp.async (rows and K may be ragged/odd).
+          for (int e = lane; e < Cfg::BM * 16; e += 32) {
+            int r = e >> 4, c = e & 15;
+            int64_t gr = m0 + r, gk = k0 + c;
+            bool v = (gr < p.M) && (gk < p.K);
+            const double* src = v ? p.A + gr * p.K + gk : p.A;
+            cp_async_8(sa + a_off(r, c >> 1) + ((c & 1) << 3), src, v);
+          }
+          for (int e = lane; e < 16 * Cfg::BN; e += 32) {
+            int k = e / Cfg::BN, n = e % Cfg::BN;
+            int64_t gk = k0 + k, gn = n0 + n;
+            bool v = (gk < p.K) && (gn < p.N);
+            const double* src = v ? p.B + gk * p.N + gn : p.B;
+            cp_async_8(sb + b_off(k, n), src, v);
+          }
+          cp_async_mbar_arrive_noinc(&full[stage]);
+        }
+        if (++stage == Cfg::STAGES) { stage = 0; phase ^= 1; }
+      }
+    }
+    if (!Cfg::kTMA) asm volatile("cp.async.wait_all;" ::: "memory");
+  } else {
+    // ------------------------------- consumer warps -------------------------------
+    const int wm = warp / Cfg::WARPS_N, wn = warp % Cfg::WARPS_N;
+    const int g = lane >> 2, tq = lane & 3;
+    const uint32_t smem_base = smem_u32(smem);
+    int stage = 0;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+      int64_t tm, tn;
+      tile_coords(t, tiles_m, tiles_n, tm, tn);
+      double acc[2][4][4];
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
+
+      for (int kb = 0; kb < kblocks; ++kb) {
+        if (!mbar_wait(&full[stage], phase, abort_flag, p.status, 2)) { ok = false; break; }
+        const uint32_t sa = smem_base + stage * Cfg::STAGE_BYTES;
+        const uint32_t sb = sa + Cfg::A_BYTES;
+        double af[2][8], bf[4][4];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int r0 = wm * Cfg::WM + i * 16 + g;
+          // physical k 4tq..4tq+3 = chunks 2tq, 2tq+1 of rows r0 and r0+8
+          double x0, x1, x2, x3, y0, y1, y2, y3;
+          lds128(x0, x1, sa + a_off(r0, 2 * tq));
+          lds128(x2, x3, sa + a_off(r0, 2 * tq + 1));
+          lds128(y0, y1, sa + a_off(r0 + 8, 2 * tq));
+          lds128(y2, y3, sa + a_off(r0 + 8, 2 * tq + 1));
+          af[i][0] = x0; af[i][1] = y0; af[i][2] = x1; af[i][3] = y1;
+          af[i][4] = x2; af[i][5] = y2; af[i][6] = x3; af[i][7] = y3;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int n = wn * Cfg::WN + j * 8 + g;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) bf[j][i] = lds64(sb + b_off(4 * tq + i, n));
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[stage]);
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) mma_m16n8k16(acc[i][j], af[i], bf[j]);
+        if (++stage == Cfg::STAGES) { stage = 0; phase ^= 1; }
+      }
+      if (!ok) break;
+
+      // ---- epilogue: C = alpha*acc + beta*C0, 16-byte vectors where the row stride allows ----
+      const int64_t m0 = tm * Cfg::BM + wm * Cfg::WM, n0 = tn * Cfg::BN + wn * Cfg::WN;
+      const bool vec = ((p.N & 1) == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0);
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int64_t row = m0 + i * 16 + g + 8 * h;
+          if (row >= p.M) continue;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int64_t col = n0 + j * 8 + 2 * tq;
+            double v0 = acc[i][j][2 * h], v1 = acc[i][j][2 * h + 1];
+            double* cp = p.C + row * p.N + col;
+            if (vec && col + 1 < p.N) {
+              double2 o;
+              if (p.beta != 0.0) {
+                double2 c0 = *reinterpret_cast<const double2*>(cp);
+                o.x = fma(p.alpha, v0, p.beta * c0.x);
+                o.y = fma(p.alpha, v1, p.beta * c0.y);
+              } else {
+                o.x = p.alpha * v0;
+                o.y = p.alpha * v1;
+              }
+              *reinterpret_cast<double2*>(cp) = o;
+            } else {
+              if (col < p.N) cp[0] = (p.beta != 0.0) ? fma(p.alpha, v0, p.beta * cp[0]) : p.alpha * v0;
+              if (col + 1 < p.N) cp[1] = (p.beta != 0.0) ? fma(p.alpha, v1, p.beta * cp[1]) : p.alpha * v1;
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+}  // namespace fp64
+}  // namespace lt

@@ -1,0 +1,189 @@
+"""ctypes bindings of the CPU oracle (oracle.c / oracle_blocked.c) and of oracle/_ref.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU legs
+as the checker. The product library never uses it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libref_dgemm.so"
+
+_c = ctypes
+_vp, _i64, _i32, _f64, _u64 = _c.c_void_p, _c.c_int64, _c.c_int, _c.c_double, _c.c_uint64
+
+
+def build(quiet: bool = True) -> None:
+    """Compiles liboracle.so, and oracle/_ref when the reference sources are present."""
+    out = subprocess.run(["make", "-C", str(HERE), "all"], stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout)
+    if not quiet:
+        print(out.stdout)
+
+
+_lib = None
+_ref = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = ctypes.CDLL(str(LIB))
+        L.oracle_mix64.restype = _u64
+        L.oracle_mix64.argtypes = [_u64]
+        L.oracle_bits.restype = _u64
+        L.oracle_bits.argtypes = [_u64, _u64, _u64]
+        L.oracle_uniform.restype = _f64
+        L.oracle_uniform.argtypes = [_u64, _u64, _u64]
+        L.oracle_fill.argtypes = [_vp, _i64, _u64, _u64, _i32]
+        L.oracle_scale_rows.argtypes = [_vp, _i64, _i64, _u64, _u64, _i32]
+        L.oracle_scale_cols.argtypes = [_vp, _i64, _i64, _u64, _u64, _i32]
+        L.oracle_dgemm_naive.argtypes = [_vp, _vp, _vp, _i32, _i32, _i32, _f64, _f64]
+        L.oracle_dgemm_blocked.argtypes = [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _i32]
+        L.oracle_dgemm_dot2_rows.argtypes = [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _vp, _i64, _i32]
+        L.oracle_componentwise_error.argtypes = [_vp, _vp, _vp, _i64, _vp]
+        L.oracle_ozaki_row_exponents.argtypes = [_vp, _i64, _i64, _vp]
+        L.oracle_ozaki_col_exponents.argtypes = [_vp, _i64, _i64, _vp]
+        L.oracle_ozaki_split_rows.argtypes = [_vp, _i64, _i64, _vp, _i32, _vp, _i64]
+        L.oracle_ozaki_split_cols.argtypes = [_vp, _i64, _i64, _vp, _i32, _vp, _i64]
+        L.oracle_ozaki_dgemm.argtypes = [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _i32, _i32]
+        L.oracle_ozaki_analytic_slices.restype = _i32
+        L.oracle_ozaki_analytic_slices.argtypes = [_f64, _i64, _i32]
+        _lib = L
+    return _lib
+
+
+def ref_lib() -> ctypes.CDLL | None:
+    """The reference's own host check loop (routines/dgemm/dgemm.cpp:122-133), if built here."""
+    global _ref
+    if _ref is None and REF_LIB.exists():
+        R = ctypes.CDLL(str(REF_LIB))
+        R.ref_dgemm_host.argtypes = [_vp, _vp, _vp, _i32, _i32, _i32, _f64, _f64]
+        _ref = R
+    return _ref
+
+
+def _p(a: np.ndarray) -> int:
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+def nthreads() -> int:
+    return max(1, len(os.sched_getaffinity(0)))
+
+
+# ---- generator ---------------------------------------------------------------------------------
+def fill(rows: int, cols: int, stream: int, phi: int = 0, seed: int = 1234) -> np.ndarray:
+    x = np.empty((rows, cols), dtype=np.float64)
+    lib().oracle_fill(_p(x), rows * cols, seed, stream, phi)
+    return x
+
+
+def scale_rows(x: np.ndarray, seed: int, stream: int, smax: int) -> None:
+    lib().oracle_scale_rows(_p(x), x.shape[0], x.shape[1], seed, stream, smax)
+
+
+def scale_cols(x: np.ndarray, seed: int, stream: int, smax: int) -> None:
+    lib().oracle_scale_cols(_p(x), x.shape[0], x.shape[1], seed, stream, smax)
+
+
+def make_problem(M: int, N: int, K: int, phi: int = 0, seed: int = 1234, smax: int = 0):
+    """A (stream 1), B (stream 2), C0 (stream 3); rows of A / columns of B scaled by 2^s with
+    s ~ U{-smax..smax} (streams 4, 5) when smax > 0."""
+    A = fill(M, K, 1, phi, seed)
+    B = fill(K, N, 2, phi, seed)
+    C0 = fill(M, N, 3, phi, seed)
+    if smax > 0:
+        scale_rows(A, seed, 4, smax)
+        scale_cols(B, seed, 5, smax)
+    return A, B, C0
+
+
+# ---- GEMM oracles ------------------------------------------------------------------------------
+def dgemm_naive(A, B, C0, alpha, beta) -> np.ndarray:
+    M, K = A.shape
+    N = B.shape[1]
+    C = np.ascontiguousarray(C0).copy()
+    lib().oracle_dgemm_naive(_p(A), _p(B), _p(C), M, N, K, alpha, beta)
+    return C
+
+
+def dgemm_ref(A, B, C0, alpha, beta) -> np.ndarray | None:
+    R = ref_lib()
+    if R is None:
+        return None
+    M, K = A.shape
+    N = B.shape[1]
+    C = np.ascontiguousarray(C0).copy()
+    R.ref_dgemm_host(_p(A), _p(B), _p(C), M, N, K, alpha, beta)
+    return C
+
+
+def dgemm_blocked(A, B, C0, alpha, beta, threads: int | None = None) -> np.ndarray:
+    M, K = A.shape
+    N = B.shape[1]
+    C = np.ascontiguousarray(C0).copy()
+    lib().oracle_dgemm_blocked(_p(A), _p(B), _p(C), M, N, K, alpha, beta, threads or nthreads())
+    return C
+
+
+def dot2_rows(A, B, C0, alpha, beta, rows=None, threads: int | None = None):
+    """Near-exact C and the componentwise denominator on the listed rows."""
+    M, K = A.shape
+    N = B.shape[1]
+    rows = np.arange(M, dtype=np.int64) if rows is None else np.ascontiguousarray(rows, dtype=np.int64)
+    Cref = np.empty((len(rows), N))
+    den = np.empty((len(rows), N))
+    c0 = np.ascontiguousarray(C0) if C0 is not None else np.zeros((M, N))
+    lib().oracle_dgemm_dot2_rows(_p(A), _p(B), _p(c0), _p(Cref), _p(den), M, N, K, alpha, beta, _p(rows),
+                                 len(rows), threads or nthreads())
+    return Cref, den
+
+
+def componentwise_error(C, Cref, den):
+    """(max, median, mean, non-finite mismatches) of |C - Cref| / den."""
+    out = np.zeros(4)
+    C = np.ascontiguousarray(C, dtype=np.float64)
+    lib().oracle_componentwise_error(_p(C), _p(np.ascontiguousarray(Cref)), _p(np.ascontiguousarray(den)), C.size,
+                                     _p(out))
+    return tuple(out)
+
+
+# ---- Ozaki restatement -------------------------------------------------------------------------
+def ozaki_dgemm(A, B, C0, alpha, beta, s, threads: int | None = None) -> np.ndarray:
+    M, K = A.shape
+    N = B.shape[1]
+    C = np.ascontiguousarray(C0).copy()
+    lib().oracle_ozaki_dgemm(_p(A), _p(B), _p(C), M, N, K, alpha, beta, s, threads or nthreads())
+    return C
+
+
+def ozaki_split(A, B, s):
+    """(sigma, tau, A slices [s][M][Kp], B slices [s][N][Kp])."""
+    M, K = A.shape
+    N = B.shape[1]
+    Kp = (max(K, 1) + 31) // 32 * 32
+    sigma = np.empty(M, dtype=np.int32)
+    tau = np.empty(N, dtype=np.int32)
+    sa = np.empty((s, M, Kp), dtype=np.int8)
+    sb = np.empty((s, N, Kp), dtype=np.int8)
+    L = lib()
+    L.oracle_ozaki_row_exponents(_p(A), M, K, _p(sigma))
+    L.oracle_ozaki_col_exponents(_p(B), K, N, _p(tau))
+    L.oracle_ozaki_split_rows(_p(A), M, K, _p(sigma), s, _p(sa), Kp)
+    L.oracle_ozaki_split_cols(_p(B), K, N, _p(tau), s, _p(sb), Kp)
+    return sigma, tau, sa, sb
+
+
+def analytic_slices(tol: float, K: int, phi_spread: int) -> int:
+    return int(lib().oracle_ozaki_analytic_slices(tol, K, phi_spread))

@@ -1,0 +1,388 @@
+/*
+ * oracle.c — CPU oracle for the libthom DGEMM hot path (TEST INFRASTRUCTURE ONLY; see oracle.h).
+ *
+ * Compiled with -ffp-contract=off so that every a*b+c below rounds twice, exactly as written;
+ * the blocked (fast) DGEMM lives in oracle_blocked.c where contraction is allowed.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------------------------------ */
+/* Seeded counter-based generator. splitmix64 finaliser (Steele, Lea, Flood 2014), keyed by     */
+/* (seed, stream) and indexed by element position so any element is reproducible anywhere.    */
+/* The CUDA generator in libthom_b200/csrc/gen.cu computes the same bits.                      */
+/* ------------------------------------------------------------------------------------------ */
+uint64_t oracle_mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+static uint64_t stream_key(uint64_t seed, uint64_t stream) {
+  return oracle_mix64(seed ^ oracle_mix64(stream));
+}
+
+uint64_t oracle_bits(uint64_t seed, uint64_t stream, uint64_t idx) {
+  return oracle_mix64(stream_key(seed, stream) + idx * 0xD1B54A32D192ED03ULL);
+}
+
+static double bits_to_uniform(uint64_t h) {
+  /* 53 random bits -> k * 2^-52 - 1, exactly representable, in [-1, 1). */
+  return (double)(h >> 11) * 0x1p-52 - 1.0;
+}
+
+double oracle_uniform(uint64_t seed, uint64_t stream, uint64_t idx) {
+  return bits_to_uniform(oracle_bits(seed, stream, idx));
+}
+
+static int bits_to_exponent(uint64_t h, int phi) {
+  if (phi <= 0) return 0;
+  uint64_t e = oracle_mix64(h ^ 0x5851F42D4C957F2DULL) % (uint64_t)(2 * phi + 1);
+  return (int)e - phi;
+}
+
+void oracle_fill(double* X, int64_t n, uint64_t seed, uint64_t stream, int phi) {
+  uint64_t key = stream_key(seed, stream);
+  for (int64_t i = 0; i < n; ++i) {
+    uint64_t h = oracle_mix64(key + (uint64_t)i * 0xD1B54A32D192ED03ULL);
+    X[i] = ldexp(bits_to_uniform(h), bits_to_exponent(h, phi));
+  }
+}
+
+static int scale_exponent(uint64_t key, int64_t i, int smax) {
+  if (smax <= 0) return 0;
+  uint64_t h = oracle_mix64(key + (uint64_t)i * 0xD1B54A32D192ED03ULL);
+  return (int)(h % (uint64_t)(2 * smax + 1)) - smax;
+}
+
+void oracle_scale_rows(double* X, int64_t rows, int64_t cols, uint64_t seed, uint64_t stream, int smax) {
+  uint64_t key = stream_key(seed, stream);
+  for (int64_t r = 0; r < rows; ++r) {
+    int e = scale_exponent(key, r, smax);
+    for (int64_t c = 0; c < cols; ++c) X[r * cols + c] = ldexp(X[r * cols + c], e);
+  }
+}
+
+void oracle_scale_cols(double* X, int64_t rows, int64_t cols, uint64_t seed, uint64_t stream, int smax) {
+  uint64_t key = stream_key(seed, stream);
+  for (int64_t c = 0; c < cols; ++c) {
+    int e = scale_exponent(key, c, smax);
+    for (int64_t r = 0; r < rows; ++r) X[r * cols + c] = ldexp(X[r * cols + c], e);
+  }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Reference host check, restated: routines/dgemm/dgemm.cpp:122-133. Same loop order, same   */
+/* operations (double sum, += a*b, then alpha*sum + beta*C), no contraction.                   */
+/* ------------------------------------------------------------------------------------------ */
+void oracle_dgemm_naive(const double* A, const double* B, double* C, int M, int N, int K,
+                        double alpha, double beta) {
+  for (int row = 0; row < M; row++) {
+    for (int col = 0; col < N; col++) {
+      double sum = 0;
+      for (int k = 0; k < K; k++) sum += A[(int64_t)row * K + k] * B[(int64_t)k * N + col];
+      C[(int64_t)row * N + col] = alpha * sum + beta * C[(int64_t)row * N + col];
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Double-double helpers (error-free transformations: Knuth TwoSum, FMA-based TwoProduct).    */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct { double hi, lo; } dd_t;
+
+static inline dd_t two_sum(double a, double b) {
+  double s = a + b;
+  double bb = s - a;
+  double e = (a - (s - bb)) + (b - bb);
+  dd_t r = {s, e};
+  return r;
+}
+static inline dd_t two_prod(double a, double b) {
+  double p = a * b;
+  double e = fma(a, b, -p);
+  dd_t r = {p, e};
+  return r;
+}
+static inline dd_t dd_add(dd_t x, dd_t y) {
+  dd_t s = two_sum(x.hi, y.hi);
+  double lo = s.lo + x.lo + y.lo;
+  return two_sum(s.hi, lo);
+}
+static inline dd_t dd_mul_d(dd_t x, double a) {
+  dd_t p = two_prod(x.hi, a);
+  double lo = p.lo + x.lo * a;
+  return two_sum(p.hi, lo);
+}
+
+typedef struct {
+  const double *A, *B, *C0;
+  double *Cref, *den;
+  int64_t M, N, K;
+  double alpha, beta;
+  const int64_t* rows;
+  int64_t nrows;
+  int tid, nthreads;
+} dot2_job_t;
+
+static void* dot2_worker(void* arg) {
+  dot2_job_t* j = (dot2_job_t*)arg;
+  const int64_t N = j->N, K = j->K;
+  dd_t* acc = (dd_t*)malloc(sizeof(dd_t) * (size_t)N);
+  double* aab = (double*)malloc(sizeof(double) * (size_t)N);
+  for (int64_t ri = j->tid; ri < j->nrows; ri += j->nthreads) {
+    int64_t r = j->rows[ri];
+    for (int64_t c = 0; c < N; ++c) { acc[c].hi = 0; acc[c].lo = 0; aab[c] = 0; }
+    /* i-k-j order: row r of A times B, each product error-free, sums in double-double. */
+    for (int64_t k = 0; k < K; ++k) {
+      double a = j->A[r * K + k];
+      const double* brow = j->B + k * N;
+      double aa = fabs(a);
+      for (int64_t c = 0; c < N; ++c) {
+        dd_t p = two_prod(a, brow[c]);
+        acc[c] = dd_add(acc[c], p);
+        aab[c] += aa * fabs(brow[c]);
+      }
+    }
+    for (int64_t c = 0; c < N; ++c) {
+      dd_t v = dd_mul_d(acc[c], j->alpha);
+      double den = fabs(j->alpha) * aab[c];
+      if (j->beta != 0.0) {
+        double c0 = j->C0[r * N + c];
+        v = dd_add(v, two_prod(j->beta, c0));
+        den += fabs(j->beta) * fabs(c0);
+      }
+      j->Cref[ri * N + c] = v.hi + v.lo;
+      j->den[ri * N + c] = den;
+    }
+  }
+  free(acc);
+  free(aab);
+  return NULL;
+}
+
+void oracle_dgemm_dot2_rows(const double* A, const double* B, const double* C0, double* Cref, double* den,
+                            int64_t M, int64_t N, int64_t K, double alpha, double beta,
+                            const int64_t* rows, int64_t nrows, int nthreads) {
+  (void)M;
+  if (nthreads < 1) nthreads = 1;
+  if (nthreads > 256) nthreads = 256;
+  pthread_t th[256];
+  dot2_job_t jobs[256];
+  for (int t = 0; t < nthreads; ++t) {
+    dot2_job_t j = {A, B, C0, Cref, den, M, N, K, alpha, beta, rows, nrows, t, nthreads};
+    jobs[t] = j;
+    pthread_create(&th[t], NULL, dot2_worker, &jobs[t]);
+  }
+  for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+}
+
+static int cmp_double(const void* a, const void* b) {
+  double x = *(const double*)a, y = *(const double*)b;
+  return (x > y) - (x < y);
+}
+
+void oracle_componentwise_error(const double* C, const double* Cref, const double* den, int64_t n,
+                                double* out) {
+  double* e = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+  double mx = 0, sum = 0, bad = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    double d = fabs(C[i] - Cref[i]);
+    double v;
+    if (!isfinite(C[i]) || !isfinite(Cref[i])) {
+      v = (C[i] == Cref[i] || (isnan(C[i]) && isnan(Cref[i]))) ? 0.0 : INFINITY;
+      if (v != 0.0) bad += 1;
+    } else if (den[i] > 0) {
+      v = d / den[i];
+    } else {
+      v = (d == 0.0) ? 0.0 : INFINITY;
+    }
+    e[i] = v;
+    if (v > mx) mx = v;
+    sum += v;
+  }
+  qsort(e, (size_t)n, sizeof(double), cmp_double);
+  out[0] = mx;
+  out[1] = n > 0 ? e[n / 2] : 0.0;
+  out[2] = n > 0 ? sum / (double)n : 0.0;
+  out[3] = bad;
+  free(e);
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Ozaki INT8-slice DGEMM restatement. Same arithmetic, same order as the CUDA kernels:       */
+/*  1. sigma_i = frexp exponent of max_k |A[i,k]| (0 for an all-zero row), tau_j likewise for  */
+/*     the columns of B, so |A[i,k] 2^-sigma_i| < 1.                                             */
+/*  2. x = A[i,k] 2^-sigma_i; for p = 1..s: y = 128 x, q_p = trunc(y), x = y - q_p (all exact). */
+/*  3. D = sum over pairs (p,q) with p+q = d and over a K group of q_p(A) q_q(B) in INT32.      */
+/*  4. acc = sum D 2^(-7d) in the band / group / diagonal order described at ozaki_worker.        */
+/*  5. C = fma(alpha, acc 2^sigma_i 2^tau_j, beta*C0)   (alpha * t when beta == 0).              */
+/* ------------------------------------------------------------------------------------------ */
+static double pow2i(int e) {
+  /* exact 2^e for e in [-1022, 1023] */
+  uint64_t bits = (uint64_t)(e + 1023) << 52;
+  double r;
+  memcpy(&r, &bits, sizeof r);
+  return r;
+}
+
+static double scale_pow2(double x, int e) {
+  while (e > 1023) { x *= pow2i(1023); e -= 1023; }
+  while (e < -1022) { x *= pow2i(-1022); e += 1022; }
+  return x * pow2i(e);
+}
+
+static int32_t exponent_of_max(double amax) {
+  if (!(amax > 0.0)) return 0;          /* zero row (or NaN: handled by NaN propagation in C) */
+  if (isinf(amax)) return 0;
+  int e;
+  frexp(amax, &e);                       /* amax = m 2^e, m in [0.5, 1) -> amax < 2^e */
+  return (int32_t)e;
+}
+
+void oracle_ozaki_row_exponents(const double* A, int64_t M, int64_t K, int32_t* sigma) {
+  for (int64_t i = 0; i < M; ++i) {
+    double m = 0;
+    for (int64_t k = 0; k < K; ++k) { double v = fabs(A[i * K + k]); if (v > m) m = v; }
+    sigma[i] = exponent_of_max(m);
+  }
+}
+
+void oracle_ozaki_col_exponents(const double* B, int64_t K, int64_t N, int32_t* tau) {
+  for (int64_t j = 0; j < N; ++j) {
+    double m = 0;
+    for (int64_t k = 0; k < K; ++k) { double v = fabs(B[k * N + j]); if (v > m) m = v; }
+    tau[j] = exponent_of_max(m);
+  }
+}
+
+static void split_value(double a, int32_t e, int s, int8_t* out, int64_t stride) {
+  if (!isfinite(a)) { for (int p = 0; p < s; ++p) out[p * stride] = 0; return; }
+  double x = scale_pow2(a, -e);
+  for (int p = 0; p < s; ++p) {
+    double y = x * 128.0;
+    double q = trunc(y);
+    x = y - q;
+    out[p * stride] = (int8_t)q;
+  }
+}
+
+void oracle_ozaki_split_rows(const double* A, int64_t M, int64_t K, const int32_t* sigma, int s,
+                             int8_t* slices, int64_t Kp) {
+  memset(slices, 0, (size_t)(s * M * Kp));
+  for (int64_t i = 0; i < M; ++i)
+    for (int64_t k = 0; k < K; ++k)
+      split_value(A[i * K + k], sigma[i], s, slices + i * Kp + k, M * Kp);
+}
+
+void oracle_ozaki_split_cols(const double* B, int64_t K, int64_t N, const int32_t* tau, int s,
+                             int8_t* slices, int64_t Kp) {
+  memset(slices, 0, (size_t)(s * N * Kp));
+  for (int64_t k = 0; k < K; ++k)
+    for (int64_t j = 0; j < N; ++j)
+      split_value(B[k * N + j], tau[j], s, slices + j * Kp + k, N * Kp);
+}
+
+typedef struct {
+  const int8_t *sa, *sb;
+  const int32_t *sigma, *tau;
+  const double *A, *B;
+  double* C;
+  int64_t M, N, K, Kp;
+  double alpha, beta;
+  int s, tid, nthreads;
+} ozaki_job_t;
+
+/* Band schedule shared with the CUDA kernel: diagonals d = s+1 .. 2 are taken in bands of
+ * ORACLE_OZAKI_BAND consecutive diagonals (highest first); each band runs over K in 32-byte chunks,
+ * split into groups whose INT32 sums cannot overflow: a group holds
+ * floor(ORACLE_OZAKI_KPAIR_LIMIT / (32 * max pairs of a diagonal in the band)) chunks.
+ * FP64 accumulation order: band, then group, then diagonal (highest first). */
+static void* ozaki_worker(void* arg) {
+  ozaki_job_t* j = (ozaki_job_t*)arg;
+  const int s = j->s;
+  const int64_t M = j->M, N = j->N, K = j->K, Kp = j->Kp;
+  const int64_t nkc = Kp / ORACLE_OZAKI_KCHUNK;
+  for (int64_t i = j->tid; i < M; i += j->nthreads) {
+    int row_bad = 0;
+    for (int64_t k = 0; k < K; ++k) if (!isfinite(j->A[i * K + k])) { row_bad = 1; break; }
+    for (int64_t c = 0; c < N; ++c) {
+      int col_bad = row_bad;
+      if (!col_bad) for (int64_t k = 0; k < K; ++k) if (!isfinite(j->B[k * N + c])) { col_bad = 1; break; }
+      double acc = 0.0;
+      for (int dhi = s + 1; dhi >= 2; dhi -= ORACLE_OZAKI_BAND) {
+        int dlo = dhi - ORACLE_OZAKI_BAND + 1 < 2 ? 2 : dhi - ORACLE_OZAKI_BAND + 1;
+        int maxp = 0;
+        for (int d = dhi; d >= dlo; --d) {
+          int plo = d - s > 1 ? d - s : 1, phi = d - 1 < s ? d - 1 : s;
+          if (phi - plo + 1 > maxp) maxp = phi - plo + 1;
+        }
+        int64_t gchunks = ORACLE_OZAKI_KPAIR_LIMIT / (ORACLE_OZAKI_KCHUNK * maxp);
+        for (int64_t c0 = 0; c0 < nkc; c0 += gchunks) {
+          int64_t c1 = c0 + gchunks < nkc ? c0 + gchunks : nkc;
+          int64_t k0 = c0 * ORACLE_OZAKI_KCHUNK, k1 = c1 * ORACLE_OZAKI_KCHUNK;
+          for (int d = dhi; d >= dlo; --d) {
+            int plo = d - s > 1 ? d - s : 1, phi = d - 1 < s ? d - 1 : s;
+            int32_t D = 0;
+            for (int p = plo; p <= phi; ++p) {
+              int q = d - p;
+              const int8_t* ar = j->sa + ((int64_t)(p - 1) * M + i) * Kp;
+              const int8_t* bc = j->sb + ((int64_t)(q - 1) * N + c) * Kp;
+              for (int64_t k = k0; k < k1; ++k) D += (int32_t)ar[k] * (int32_t)bc[k];
+            }
+            acc = acc + (double)D * pow2i(-7 * d);
+          }
+        }
+      }
+      double t = scale_pow2(scale_pow2(acc, j->sigma[i]), j->tau[c]);
+      double out;
+      if (j->beta != 0.0) out = fma(j->alpha, t, j->beta * j->C[i * N + c]);
+      else out = j->alpha * t;
+      if (col_bad) out = NAN;
+      j->C[i * N + c] = out;
+    }
+  }
+  return NULL;
+}
+
+void oracle_ozaki_dgemm(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
+                        double alpha, double beta, int s, int nthreads) {
+  int64_t Kp = (K + ORACLE_OZAKI_KCHUNK - 1) / ORACLE_OZAKI_KCHUNK * ORACLE_OZAKI_KCHUNK;
+  int32_t* sigma = (int32_t*)malloc(sizeof(int32_t) * (size_t)(M > 0 ? M : 1));
+  int32_t* tau = (int32_t*)malloc(sizeof(int32_t) * (size_t)(N > 0 ? N : 1));
+  int8_t* sa = (int8_t*)malloc((size_t)(s * M * Kp + 1));
+  int8_t* sb = (int8_t*)malloc((size_t)(s * N * Kp + 1));
+  oracle_ozaki_row_exponents(A, M, K, sigma);
+  oracle_ozaki_col_exponents(B, K, N, tau);
+  oracle_ozaki_split_rows(A, M, K, sigma, s, sa, Kp);
+  oracle_ozaki_split_cols(B, K, N, tau, s, sb, Kp);
+  if (nthreads < 1) nthreads = 1;
+  if (nthreads > 256) nthreads = 256;
+  pthread_t th[256];
+  ozaki_job_t jobs[256];
+  for (int t = 0; t < nthreads; ++t) {
+    ozaki_job_t j = {sa, sb, sigma, tau, A, B, C, M, N, K, Kp, alpha, beta, s, t, nthreads};
+    jobs[t] = j;
+    pthread_create(&th[t], NULL, ozaki_worker, &jobs[t]);
+  }
+  for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+  free(sigma); free(tau); free(sa); free(sb);
+}
+
+/* Conservative slice count. Truncating every entry of row i after s slices leaves an error
+ * below 2^(sigma_i - 7s); the dropped pairs p+q > s+1 add at most s more such terms. Relative to
+ * the componentwise denominator sum_k |a_ik||b_kj|, the worst case loses the full exponent spread
+ * of a row and of a column (phi_spread bits each), so s must satisfy
+ *   (s + 2) K 2^(2 phi_spread - 7 s) <= tol. */
+int oracle_ozaki_analytic_slices(double tol, int64_t K, int phi_spread) {
+  for (int s = 1; s <= 16; ++s) {
+    double bound = (double)(s + 2) * (double)K * ldexp(1.0, 2 * phi_spread - 7 * s);
+    if (bound <= tol) return s;
+  }
+  return 16;
+}

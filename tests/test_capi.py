@@ -1,0 +1,70 @@
+"""CPU checks of the C ABI boundary: the library loads, exports every function declared in
+include/*.h, and rejects bad arguments before touching a GPU."""
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions() -> list[str]:
+    names = []
+    for h in sorted((ROOT / "include").glob("*.h")):
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        text = re.sub(r"#[^\n]*", "", text)
+        for m in re.finditer(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", text):
+            name = m.group(1)
+            if name.startswith(("lt_", "dgemm_")) and name not in names:
+                names.append(name)
+    return names
+
+
+def test_header_declares_reference_contract():
+    names = declared_functions()
+    for impl in ["tc100", "cublas_tc", "ozaki_auto"] + [f"ozaki{s}" for s in range(3, 11)]:
+        assert f"dgemm_{impl}" in names
+
+
+def test_library_exports_every_declared_symbol():
+    import libthom_b200 as lt
+
+    L = lt.lib()
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, f"declared but not exported: {missing}"
+    # and the Python layer knows every signature
+    assert not [n for n in declared_functions() if n not in lt.SIGNATURES]
+
+
+def test_errors_without_gpu():
+    import libthom_b200 as lt
+
+    L = lt.lib()
+    assert L.lt_error_string(lt.LT_ERR_INVALID_ARGUMENT) == b"invalid argument"
+    # argument validation happens before any device work
+    rc = L.lt_dgemm_fp64(None, None, None, -1, 4, 4, 1.0, 0.0, None)
+    assert rc == lt.LT_ERR_INVALID_ARGUMENT and L.lt_get_last_error() == rc
+    rc = L.lt_dgemm_ozaki(None, None, None, 4, 4, 4, 1.0, 0.0, 3, None)
+    assert rc == lt.LT_ERR_INVALID_ARGUMENT
+    rc = L.lt_dgemm_ozaki(ctypes.c_void_p(0x1000), ctypes.c_void_p(0x1000), ctypes.c_void_p(0x1000), 4, 4, 4, 1.0,
+                          0.0, 0, None)
+    assert rc == lt.LT_ERR_INVALID_ARGUMENT  # slice count 0
+    rc = L.lt_dgemm_fp64(ctypes.c_void_p(0x1004), ctypes.c_void_p(0x1000), ctypes.c_void_p(0x1000), 4, 4, 4, 1.0,
+                         0.0, None)
+    assert rc == lt.LT_ERR_UNALIGNED
+    assert b"8-byte" in L.lt_last_error_message()
+    assert L.lt_ozaki_workspace_size(8192, 8192, 8192, 8) >= 8 * 2 * 8192 * 8192
+    assert L.lt_ozaki_workspace_size(8, 8, 8, 0) == 0
+    assert L.lt_ozaki_analytic_slices(1e-15, 8192, 0) >= 8
+
+
+def test_unknown_impl_rejected():
+    import libthom_b200 as lt
+
+    with pytest.raises(KeyError):
+        lt.dgemm("final", 0, 0, 0, 1, 1, 1)

@@ -1,0 +1,108 @@
+"""GPU parity of the Ozaki INT8-slice DGEMM (lt_dgemm_ozaki / dgemm_ozaki<s>).
+
+Oracle: oracle_ozaki_dgemm, a CPU restatement with the same arithmetic in the same order, so the
+GPU result must be bit-identical (integer slice products are exact; every FP64 step is
+specified). Accuracy against the compensated Dot2 oracle is checked separately.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import U, fp64_bound, to_dev
+
+pytestmark = pytest.mark.gpu
+
+
+def run_ozaki(torch, A, B, C0, alpha, beta, s, workspace=None):
+    import libthom_b200 as lt
+
+    M, K = A.shape
+    N = B.shape[1]
+    dA, dB, dC = to_dev(torch, A), to_dev(torch, B), to_dev(torch, C0)
+    lt.dgemm_ozaki(dA, dB, dC, M, N, K, alpha, beta, slices=s, workspace=workspace)
+    torch.cuda.synchronize()
+    lt.device_status()
+    return dC.cpu().numpy().reshape(M, N)
+
+
+def assert_bit_exact(C, R):
+    same = (C == R) | (np.isnan(C) & np.isnan(R))
+    if not same.all():
+        idx = np.argwhere(~same)[:5]
+        raise AssertionError(f"{(~same).sum()} mismatches, first {[(tuple(i), C[tuple(i)], R[tuple(i)]) for i in idx]}")
+
+
+@pytest.mark.parametrize("s", [1, 3, 5, 8, 10, 12])
+def test_bit_exact_vs_restatement(cuda, oracle_mod, s):
+    M, N, K = 200, 150, 300
+    A, B, C0 = oracle_mod.make_problem(M, N, K, phi=8, seed=s)
+    C = run_ozaki(cuda, A, B, C0, 1.5, 0.5, s)
+    assert_bit_exact(C, oracle_mod.ozaki_dgemm(A, B, C0, 1.5, 0.5, s))
+
+
+@pytest.mark.parametrize("M,N,K", [(1, 1, 1), (129, 130, 33), (127, 255, 64), (64, 17, 1000), (300, 8, 96)])
+def test_ragged_shapes_bit_exact(cuda, oracle_mod, M, N, K):
+    A, B, C0 = oracle_mod.make_problem(M, N, K, phi=3, seed=M * 7 + N)
+    C = run_ozaki(cuda, A, B, C0, -1.0, 0.75, 7)
+    assert_bit_exact(C, oracle_mod.ozaki_dgemm(A, B, C0, -1.0, 0.75, 7))
+
+
+def test_long_k_multiple_groups(cuda, oracle_mod):
+    """K = 20000 > 16640 (the INT32-safe group length of an 8-pair diagonal): two groups."""
+    M, N, K = 64, 48, 20000
+    A, B, C0 = oracle_mod.make_problem(M, N, K, seed=77, smax=8)
+    C = run_ozaki(cuda, A, B, C0, 1.0, 0.0, 8)
+    assert_bit_exact(C, oracle_mod.ozaki_dgemm(A, B, C0, 1.0, 0.0, 8))
+
+
+def test_nan_inf_zero(cuda, oracle_mod):
+    M, N, K = 40, 30, 64
+    A, B, C0 = oracle_mod.make_problem(M, N, K, seed=9)
+    A[3, 7] = np.nan
+    B[11, 5] = np.inf
+    A[6, :] = 0.0
+    B[:, 9] = 0.0
+    C = run_ozaki(cuda, A, B, C0, 1.0, 0.5, 6)
+    R = oracle_mod.ozaki_dgemm(A, B, C0, 1.0, 0.5, 6)
+    assert_bit_exact(C, R)
+    assert np.all(np.isnan(C[3, :])) and np.all(np.isnan(C[:, 5]))
+
+
+def test_accuracy_reaches_fp64(cuda, oracle_mod):
+    """Eight slices on unscaled data: componentwise error within the FP64 bound."""
+    M, N, K = 256, 256, 1024
+    A, B, C0 = oracle_mod.make_problem(M, N, K, seed=1234)
+    C = run_ozaki(cuda, A, B, C0, 1.5, 0.5, 8)
+    Cref, den = oracle_mod.dot2_rows(A, B, C0, 1.5, 0.5)
+    err = oracle_mod.componentwise_error(C, Cref, den)
+    assert err[0] <= fp64_bound(K), err
+
+
+def test_caller_workspace(cuda, oracle_mod):
+    import libthom_b200 as lt
+
+    torch = cuda
+    M, N, K, s = 96, 80, 200, 5
+    A, B, C0 = oracle_mod.make_problem(M, N, K, seed=31)
+    need = lt.ozaki_workspace_size(M, N, K, s)
+    ws = torch.empty(need, dtype=torch.uint8, device="cuda")
+    C = run_ozaki(torch, A, B, C0, 1.0, 1.0, s, workspace=ws)
+    assert_bit_exact(C, oracle_mod.ozaki_dgemm(A, B, C0, 1.0, 1.0, s))
+    small = torch.empty(need - 256, dtype=torch.uint8, device="cuda")
+    with pytest.raises(lt.LtError) as ei:
+        run_ozaki(torch, A, B, C0, 1.0, 1.0, s, workspace=small)
+    assert ei.value.code == lt.LT_ERR_NO_MEMORY
+
+
+def test_reference_contract_wrappers(cuda, oracle_mod):
+    import libthom_b200 as lt
+
+    torch = cuda
+    M = N = K = 128
+    A, B, C0 = oracle_mod.make_problem(M, N, K, seed=3)
+    for s in range(3, 11):
+        dA, dB, dC = to_dev(torch, A), to_dev(torch, B), to_dev(torch, C0)
+        ms = lt.dgemm(f"ozaki{s}", dA, dB, dC, M, N, K, 1.0, 1.0)
+        assert ms > 0
+        assert_bit_exact(dC.cpu().numpy(), oracle_mod.ozaki_dgemm(A, B, C0, 1.0, 1.0, s))

@@ -1,0 +1,153 @@
+"""CPU tests of the oracle: pinned against the reference's own host loop and its golden fixtures.
+
+Reference: routines/dgemm/dgemm.cpp:122-133 (getReferenceResults) and the cuRAND-free generator
+that replaces dgemm.cpp:100-119.
+"""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import U, fp64_bound
+
+
+def _cases(golden):
+    for i in range(int(golden["ncases"][0])):
+        M, N, K, phi, smax, seed = (int(x) for x in golden[f"case{i}_params"])
+        alpha, beta = (float(x) for x in golden[f"case{i}_scalars"])
+        yield i, M, N, K, phi, smax, seed, alpha, beta
+
+
+def test_generator_pinned(oracle_mod, golden):
+    gen = [oracle_mod.fill(1, 16, st, phi, 1234)[0] for st in (1, 2, 3) for phi in (0, 8)]
+    assert np.array_equal(np.stack(gen), golden["generator_first16"])
+
+
+def test_generator_ranges(oracle_mod):
+    x = oracle_mod.fill(256, 256, 1, 0)
+    assert x.min() >= -1.0 and x.max() < 1.0
+    assert abs(x.mean()) < 0.01
+    y = oracle_mod.fill(256, 256, 1, 8)
+    e = np.frexp(y[y != 0])[1]
+    assert e.min() >= -8 - 52 and e.max() <= 9
+    # same stream and seed -> same values; different stream -> different values
+    assert np.array_equal(oracle_mod.fill(3, 5, 7, 2), oracle_mod.fill(3, 5, 7, 2))
+    assert not np.array_equal(oracle_mod.fill(3, 5, 7, 2), oracle_mod.fill(3, 5, 8, 2))
+
+
+def test_row_col_scaling(oracle_mod):
+    A = oracle_mod.fill(20, 30, 1, 0)
+    S = A.copy()
+    oracle_mod.scale_rows(S, 1234, 4, 64)
+    ratio = S / A
+    r = np.log2(np.abs(ratio[:, 0]))
+    assert np.all(r == np.round(r)) and np.abs(r).max() <= 64
+    assert np.all(ratio == ratio[:, :1])  # one power of two per row
+
+
+def test_naive_matches_golden_bit_exact(oracle_mod, golden):
+    for i, M, N, K, phi, smax, seed, alpha, beta in _cases(golden):
+        A, B, C0 = oracle_mod.make_problem(M, N, K, phi=phi, seed=seed, smax=smax)
+        d = hashlib.sha256()
+        for a in (A, B, C0):
+            d.update(np.ascontiguousarray(a).tobytes())
+        assert bytes(golden[f"case{i}_digest"]).decode() == d.hexdigest(), f"case {i}: inputs differ"
+        C = oracle_mod.dgemm_naive(A, B, C0, alpha, beta)
+        assert np.array_equal(C, golden[f"case{i}_C"]), f"case {i}"
+
+
+def test_naive_matches_reference_build(oracle_mod):
+    if oracle_mod.ref_lib() is None:
+        pytest.skip("oracle/_ref not built (reference sources absent)")
+    for (M, N, K) in [(37, 41, 53), (1, 1, 1), (70, 3, 129)]:
+        A, B, C0 = oracle_mod.make_problem(M, N, K, phi=4, seed=99)
+        assert np.array_equal(oracle_mod.dgemm_naive(A, B, C0, 0.75, -1.25),
+                              oracle_mod.dgemm_ref(A, B, C0, 0.75, -1.25))
+
+
+@pytest.mark.parametrize("M,N,K", [(64, 64, 64), (17, 23, 31), (100, 130, 257), (5, 300, 7)])
+def test_blocked_within_fp64_bound(oracle_mod, M, N, K):
+    A, B, C0 = oracle_mod.make_problem(M, N, K, phi=8, seed=5)
+    Cb = oracle_mod.dgemm_blocked(A, B, C0, 1.5, 0.5)
+    Cref, den = oracle_mod.dot2_rows(A, B, C0, 1.5, 0.5)
+    err = oracle_mod.componentwise_error(Cb, Cref, den)
+    assert err[0] <= fp64_bound(K), err
+    assert err[3] == 0
+
+
+def test_dot2_is_more_accurate_than_naive(oracle_mod):
+    M, N, K = 40, 40, 2000
+    A, B, C0 = oracle_mod.make_problem(M, N, K, phi=16, seed=3)
+    Cn = oracle_mod.dgemm_naive(A, B, C0, 1.0, 0.0)
+    Cref, den = oracle_mod.dot2_rows(A, B, C0, 1.0, 0.0)
+    err = oracle_mod.componentwise_error(Cn, Cref, den)
+    assert 0 < err[0] <= fp64_bound(K)
+    # Dot2 of a subset equals Dot2 of the full set
+    Cs, dens = oracle_mod.dot2_rows(A, B, C0, 1.0, 0.0, rows=np.array([3, 17, 39]))
+    assert np.array_equal(Cs, Cref[[3, 17, 39]]) and np.array_equal(dens, den[[3, 17, 39]])
+
+
+def test_ozaki_slices_reconstruct(oracle_mod):
+    """Slices are the 7-bit digits of |a| 2^-sigma truncated toward zero (sign on every digit)."""
+    A, B, _ = oracle_mod.make_problem(30, 20, 50, phi=20, seed=11)
+    for s in (1, 4, 8, 12):
+        sigma, tau, sa, sb = oracle_mod.ozaki_split(A, B, s)
+        assert np.abs(sa).max() <= 127 and np.abs(sb).max() <= 127
+        w = 2.0 ** (-7 * np.arange(1, s + 1))
+        recon = np.einsum("p,pmk->mk", w, sa[:, :, :50].astype(np.float64)) * 2.0 ** sigma[:, None]
+        resid = A - recon
+        assert np.all(np.abs(resid) < 2.0 ** (sigma[:, None] - 7 * s))
+        assert np.all(resid * A >= 0)  # truncation toward zero
+        assert np.all(sa[:, :, 50:] == 0)  # K padding
+        reconb = np.einsum("p,pnk->kn", w, sb[:, :, :50].astype(np.float64)) * 2.0 ** tau[None, :]
+        assert np.all(np.abs(B - reconb) < 2.0 ** (tau[None, :] - 7 * s))
+
+
+def test_ozaki_restatement_accuracy(oracle_mod):
+    M, N, K = 60, 50, 300
+    A, B, C0 = oracle_mod.make_problem(M, N, K, phi=0, seed=21)
+    Cref, den = oracle_mod.dot2_rows(A, B, C0, 1.5, 0.5)
+    errs = []
+    for s in range(3, 11):
+        C = oracle_mod.ozaki_dgemm(A, B, C0, 1.5, 0.5, s)
+        errs.append(oracle_mod.componentwise_error(C, Cref, den)[0])
+    assert all(errs[i + 1] <= errs[i] for i in range(len(errs) - 1)), errs
+    # each slice buys about 7 bits
+    assert errs[0] / errs[4] > 2.0 ** 25
+    # eight slices reach FP64 accuracy on unscaled data
+    assert errs[5] <= fp64_bound(K)
+    assert errs[5] <= 64 * U
+
+
+def test_ozaki_nan_inf_and_zero_rows(oracle_mod):
+    M, N, K = 12, 9, 40
+    A, B, C0 = oracle_mod.make_problem(M, N, K, seed=8)
+    A[3, 7] = np.nan
+    B[11, 5] = np.inf
+    A[6, :] = 0.0
+    C = oracle_mod.ozaki_dgemm(A, B, C0, 1.0, 0.5, 6)
+    assert np.all(np.isnan(C[3, :])) and np.all(np.isnan(C[:, 5]))
+    rows = [i for i in range(M) if i != 3]
+    cols = [j for j in range(N) if j != 5]
+    assert np.all(np.isfinite(C[np.ix_(rows, cols)]))
+    assert np.array_equal(C[6, cols], 0.5 * C0[6, cols])
+
+
+def test_ozaki_long_k_groups(oracle_mod):
+    """K beyond the INT32-safe group length splits the band into several groups; the result is
+    still accurate (no INT32 overflow)."""
+    M, N, K = 4, 3, 40000
+    A, B, C0 = oracle_mod.make_problem(M, N, K, seed=13)
+    A[:] = np.where(A >= 0, 1.0 - 2.0 ** -40, -(1.0 - 2.0 ** -40))  # slices at +-127 everywhere
+    B[:] = np.abs(A[0, :])[:, None]
+    C = oracle_mod.ozaki_dgemm(A, B, C0, 1.0, 0.0, 8)
+    Cref, den = oracle_mod.dot2_rows(A, B, C0, 1.0, 0.0)
+    assert oracle_mod.componentwise_error(C, Cref, den)[0] < 1e-13
+
+
+def test_analytic_slices_monotone(oracle_mod):
+    a = [oracle_mod.analytic_slices(t, 8192, 0) for t in (1e-6, 1e-10, 1e-12, 1e-14, 1e-15)]
+    assert a == sorted(a) and a[-1] >= 8
+    assert oracle_mod.analytic_slices(1e-12, 8192, 32) > oracle_mod.analytic_slices(1e-12, 8192, 0)
