@@ -157,12 +157,17 @@ int lt_mlp_backward(const float* params, const float* x, const int* labels, int 
  * NULL removes them, leaving the analytic fallback. */
 int lt_selector_set_params(const float* host_params);
 void lt_set_ozaki_tolerance(double tol);
-/* Analytic (conservative) slice count for a tolerance, K and exponent spread. */
-int lt_ozaki_analytic_slices(double tol, int64_t K, int phi_spread);
+/* Analytic (conservative) slice count for a tolerance, where gap_bits is the largest exponent gap
+ * (e(max) - e(min nonzero)) within a row of A plus the largest within a column of B. Returns 0 on
+ * bad arguments. */
+int lt_ozaki_analytic_slices(double tol, int gap_bits);
 /* Slice count the selector picks for this problem (learned when weights are installed and the
- * prediction is confident, analytic otherwise). */
+ * prediction is confident, analytic otherwise). Synchronous. */
 int lt_ozaki_select_slices(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol,
                            int* slices, void* stream);
+/* Same, also reporting whether the learned choice was used and the measured gap_bits. */
+int lt_ozaki_select_info(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol,
+                         int* slices, int* learned, int* gap_bits, void* stream);
 
 /* ---- harness helpers (replace the reference's cuRAND fill, routines/dgemm/dgemm.cpp:100-119) -- */
 /* X[i] = u 2^e, u ~ U[-1,1), e ~ U{-phi..phi}; counter-based, identical to the CPU oracle. */

@@ -1,0 +1,554 @@
+// selector.cu — learned slice-count selector for the Ozaki DGEMM (no reference counterpart).
+//
+// Features (34 floats per problem): a 16-bin histogram of exponent gaps in sampled rows of A, the same
+// for sampled columns of B, log2 K / 16 and -log10(tol) / 16. The gap of a nonzero entry is how many
+// binades it sits below the largest entry of its row (column): g = e(max) - e(x), bins of width 4
+// (g >= 60 in the last bin); zeros count in bin 0. The gap is what the per-row power-of-two scaling
+// costs in precision, so the histograms carry what decides the slice count.
+//
+// Network: 34 -> 64 -> 64 -> 8, GELU (tanh form: 0.5 x (1 + tanh(sqrt(2/pi)(x + 0.044715 x^3)))),
+// softmax over slice counts 3..10, cross-entropy loss, Adam. Forward, backward and the optimizer
+// step are hand-written kernels: one block per sample for forward/backward (per-sample gradients
+// written to a buffer), then a fixed-order reduction over the batch, so gradients are deterministic.
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "lt_internal.h"
+#include "lt_runtime.cuh"
+
+namespace lt {
+namespace sel {
+
+constexpr int F = LT_SEL_FEATURES, H = LT_SEL_HIDDEN, C = LT_SEL_CLASSES, P = LT_SEL_PARAMS;
+constexpr int OW1 = 0, OB1 = OW1 + H * F, OW2 = OB1 + H, OB2 = OW2 + H * H, OW3 = OB2 + H, OB3 = OW3 + C * H;
+static_assert(OB3 + C == P, "parameter layout");
+constexpr int kSampleRows = 128;
+constexpr int kColGroups = 4;  // sampled groups of 32 consecutive columns of B
+
+__device__ __forceinline__ int exp_of(double v) {
+  int e;
+  frexp(v, &e);
+  return e;
+}
+
+__device__ __forceinline__ int gap_bin(int g) { return g >= 60 ? 15 : (g < 0 ? 0 : g >> 2); }
+
+// One block per sampled row of A: max exponent, then the gap histogram (block-local, then global).
+__global__ void row_hist_kernel(const double* __restrict__ A, int64_t M, int64_t K, int rows,
+                                unsigned int* __restrict__ hist) {
+  __shared__ int s_max;
+  __shared__ unsigned int s_hist[16];
+  const int64_t row = (rows > 1) ? (static_cast<int64_t>(blockIdx.x) * (M - 1)) / (rows - 1) : 0;
+  if (threadIdx.x == 0) s_max = -100000;
+  if (threadIdx.x < 16) s_hist[threadIdx.x] = 0;
+  __syncthreads();
+  const double* a = A + row * K;
+  int m = -100000;
+  for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
+    double v = fabs(a[k]);
+    if (v != 0.0 && isfinite(v)) m = max(m, exp_of(v));
+  }
+  atomicMax(&s_max, m);
+  __syncthreads();
+  const int em = s_max;
+  for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
+    double v = fabs(a[k]);
+    int b = (v != 0.0 && isfinite(v)) ? gap_bin(em - exp_of(v)) : 0;
+    atomicAdd(&s_hist[b], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < 16) atomicAdd(&hist[threadIdx.x], s_hist[threadIdx.x]);
+}
+
+// One block (8 warps) per sampled group of 32 consecutive columns of B; lane = column.
+__global__ void col_hist_kernel(const double* __restrict__ B, int64_t K, int64_t N, int groups,
+                                unsigned int* __restrict__ hist) {
+  __shared__ int s_max[32];
+  __shared__ unsigned int s_hist[16];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int64_t span = N > 32 ? N - 32 : 0;
+  const int64_t c0 = (groups > 1) ? (static_cast<int64_t>(blockIdx.x) * span) / (groups - 1) : 0;
+  const int64_t col = c0 + lane;
+  if (threadIdx.x < 32) s_max[threadIdx.x] = -100000;
+  if (threadIdx.x < 16) s_hist[threadIdx.x] = 0;
+  __syncthreads();
+  int m = -100000;
+  if (col < N)
+    for (int64_t k = warp; k < K; k += nwarps) {
+      double v = fabs(B[k * N + col]);
+      if (v != 0.0 && isfinite(v)) m = max(m, exp_of(v));
+    }
+  atomicMax(&s_max[lane], m);
+  __syncthreads();
+  const int em = s_max[lane];
+  if (col < N)
+    for (int64_t k = warp; k < K; k += nwarps) {
+      double v = fabs(B[k * N + col]);
+      int b = (v != 0.0 && isfinite(v)) ? gap_bin(em - exp_of(v)) : 0;
+      atomicAdd(&s_hist[b], 1u);
+    }
+  __syncthreads();
+  if (threadIdx.x < 16) atomicAdd(&hist[threadIdx.x], s_hist[threadIdx.x]);
+}
+
+__global__ void features_finish_kernel(const unsigned int* __restrict__ hist, int64_t K, double tol,
+                                       float* __restrict__ feat) {
+  const int t = threadIdx.x;
+  if (t < 32) {
+    const unsigned int* h = hist + (t < 16 ? 0 : 16);
+    unsigned long long tot = 0;
+    for (int i = 0; i < 16; ++i) tot += h[i];
+    feat[t] = tot ? static_cast<float>(static_cast<double>(hist[t]) / static_cast<double>(tot)) : 0.f;
+  } else if (t == 32) {
+    feat[32] = static_cast<float>(log2(static_cast<double>(K > 0 ? K : 1)) / 16.0);
+  } else if (t == 33) {
+    feat[33] = static_cast<float>(-log10(tol) / 16.0);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// MLP
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ float gelu(float x) {
+  const float k = 0.7978845608028654f;  // sqrt(2/pi)
+  float t = tanhf(k * (x + 0.044715f * x * x * x));
+  return 0.5f * x * (1.f + t);
+}
+__device__ __forceinline__ float gelu_grad(float x) {
+  const float k = 0.7978845608028654f;
+  float u = k * (x + 0.044715f * x * x * x);
+  float t = tanhf(u);
+  return 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * k * (1.f + 3.f * 0.044715f * x * x);
+}
+
+struct Acts {
+  float x[F], h1[H], a1[H], h2[H], a2[H], logit[C], prob[C];
+};
+
+// Block of H threads computes one sample's forward pass into shared memory.
+__device__ void forward_block(const float* __restrict__ p, const float* __restrict__ x, Acts& s) {
+  const int t = threadIdx.x;
+  for (int i = t; i < F; i += blockDim.x) s.x[i] = x[i];
+  __syncthreads();
+  if (t < H) {
+    float acc = p[OB1 + t];
+    for (int i = 0; i < F; ++i) acc += p[OW1 + t * F + i] * s.x[i];
+    s.h1[t] = acc;
+    s.a1[t] = gelu(acc);
+  }
+  __syncthreads();
+  if (t < H) {
+    float acc = p[OB2 + t];
+    for (int i = 0; i < H; ++i) acc += p[OW2 + t * H + i] * s.a1[i];
+    s.h2[t] = acc;
+    s.a2[t] = gelu(acc);
+  }
+  __syncthreads();
+  if (t < C) {
+    float acc = p[OB3 + t];
+    for (int i = 0; i < H; ++i) acc += p[OW3 + t * H + i] * s.a2[i];
+    s.logit[t] = acc;
+  }
+  __syncthreads();
+  if (t == 0) {
+    float mx = s.logit[0];
+    for (int c = 1; c < C; ++c) mx = fmaxf(mx, s.logit[c]);
+    float sum = 0.f;
+    for (int c = 0; c < C; ++c) {
+      s.prob[c] = expf(s.logit[c] - mx);
+      sum += s.prob[c];
+    }
+    for (int c = 0; c < C; ++c) s.prob[c] /= sum;
+  }
+  __syncthreads();
+}
+
+__global__ void mlp_forward_kernel(const float* __restrict__ p, const float* __restrict__ x, int batch,
+                                   float* __restrict__ probs) {
+  __shared__ Acts s;
+  const int b = blockIdx.x;
+  if (b >= batch) return;
+  forward_block(p, x + static_cast<int64_t>(b) * F, s);
+  if (threadIdx.x < C) probs[static_cast<int64_t>(b) * C + threadIdx.x] = s.prob[threadIdx.x];
+}
+
+// Per-sample gradient of the cross-entropy loss into g[b][P]; per-sample loss into loss_b[b].
+__global__ void mlp_backward_kernel(const float* __restrict__ p, const float* __restrict__ x,
+                                    const int* __restrict__ labels, int batch, float* __restrict__ g,
+                                    float* __restrict__ loss_b) {
+  __shared__ Acts s;
+  __shared__ float d3[C], d2[H], d1[H];
+  const int b = blockIdx.x, t = threadIdx.x;
+  if (b >= batch) return;
+  forward_block(p, x + static_cast<int64_t>(b) * F, s);
+  const int y = labels[b];
+  float* gb = g + static_cast<int64_t>(b) * P;
+  if (t < C) d3[t] = s.prob[t] - (t == y ? 1.f : 0.f);
+  if (t == 0) loss_b[b] = -logf(fmaxf(s.prob[y], 1e-30f));
+  __syncthreads();
+  // layer 3
+  for (int i = t; i < C * H; i += blockDim.x) gb[OW3 + i] = d3[i / H] * s.a2[i % H];
+  if (t < C) gb[OB3 + t] = d3[t];
+  if (t < H) {
+    float acc = 0.f;
+    for (int c = 0; c < C; ++c) acc += p[OW3 + c * H + t] * d3[c];
+    d2[t] = acc * gelu_grad(s.h2[t]);
+  }
+  __syncthreads();
+  // layer 2
+  for (int i = t; i < H * H; i += blockDim.x) gb[OW2 + i] = d2[i / H] * s.a1[i % H];
+  if (t < H) gb[OB2 + t] = d2[t];
+  if (t < H) {
+    float acc = 0.f;
+    for (int j = 0; j < H; ++j) acc += p[OW2 + j * H + t] * d2[j];
+    d1[t] = acc * gelu_grad(s.h1[t]);
+  }
+  __syncthreads();
+  // layer 1
+  for (int i = t; i < H * F; i += blockDim.x) gb[OW1 + i] = d1[i / F] * s.x[i % F];
+  if (t < H) gb[OB1 + t] = d1[t];
+}
+
+// grads[i] = mean over the batch of g[b][i] (fixed summation order); loss = mean of loss_b.
+__global__ void reduce_grads_kernel(const float* __restrict__ g, const float* __restrict__ loss_b, int batch,
+                                    float* __restrict__ grads, float* __restrict__ loss) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const float inv = 1.f / static_cast<float>(batch);
+  if (i < P) {
+    float acc = 0.f;
+    for (int b = 0; b < batch; ++b) acc += g[static_cast<int64_t>(b) * P + i];
+    grads[i] = acc * inv;
+  }
+  if (i == 0 && loss != nullptr) {
+    float acc = 0.f;
+    for (int b = 0; b < batch; ++b) acc += loss_b[b];
+    *loss = acc * inv;
+  }
+}
+
+__global__ void adam_kernel(float* __restrict__ p, float* __restrict__ m, float* __restrict__ v,
+                            const float* __restrict__ g, float lr, float b1, float b2, float eps, float c1, float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// Scratch for training (per device): per-sample gradients and losses.
+struct Scratch {
+  float* g = nullptr;
+  float* loss_b = nullptr;
+  int cap = 0;
+};
+std::mutex g_mutex;
+Scratch g_scratch[64];
+std::vector<float> g_host_params;  // installed selector weights (empty = none)
+float* g_dev_params[64] = {};
+bool g_dev_params_valid[64] = {};
+double g_tol = 1e-15;
+
+int ensure_scratch(int batch, Scratch** out) {
+  int dev = 0;
+  LT_CUDA_TRY(cudaGetDevice(&dev));
+  Scratch& s = g_scratch[dev];
+  if (s.cap < batch) {
+    if (s.g) cudaFree(s.g);
+    if (s.loss_b) cudaFree(s.loss_b);
+    s.g = nullptr;
+    s.loss_b = nullptr;
+    s.cap = 0;
+    LT_CUDA_TRY(cudaMalloc(&s.g, sizeof(float) * static_cast<size_t>(batch) * P));
+    LT_CUDA_TRY(cudaMalloc(&s.loss_b, sizeof(float) * batch));
+    s.cap = batch;
+  }
+  *out = &s;
+  return LT_OK;
+}
+
+int backward(const float* params, const float* x, const int* labels, int batch, float* grads, float* loss,
+             cudaStream_t stream) {
+  Scratch* s = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    LT_TRY(ensure_scratch(batch, &s));
+  }
+  mlp_backward_kernel<<<batch, H, 0, stream>>>(params, x, labels, batch, s->g, s->loss_b);
+  LT_CUDA_TRY(cudaGetLastError());
+  reduce_grads_kernel<<<(P + 255) / 256, 256, 0, stream>>>(s->g, s->loss_b, batch, grads, loss);
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
+// Conservative slice count. With gap_bits = (largest exponent gap within a row of A) + (largest
+// within a column of B), every entry a keeps at least 7s - g_a - 1 bits after truncation, so the two
+// truncated tails and the dropped pairs p + q > s + 1 (at most s + 1 of them matter) bound the
+// componentwise error by (s + 3) 2^(gap_bits + 2 - 7s) relative to |A||B|; the FP64 recombination
+// and the alpha/beta epilogue add at most 4u (the diagonal terms shrink by 2^-7 each).
+double analytic_bound(int s, int gap_bits) {
+  return (s + 3) * ldexp(1.0, gap_bits + 2 - 7 * s) + 4.0 * ldexp(1.0, -53);
+}
+
+int analytic(double tol, int gap_bits) {
+  for (int s = 1; s <= LT_OZAKI_MAX_SLICES; ++s)
+    if (analytic_bound(s, gap_bits) <= tol) return s;
+  return LT_OZAKI_MAX_SLICES;
+}
+
+// Largest exponent gap of any row of A: e(max |a|) - e(min nonzero |a|), one warp per row.
+__global__ void row_gap_kernel(const double* __restrict__ A, int64_t M, int64_t K, int* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  int best = 0;
+  for (int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; row < M; row += warps) {
+    int emax = -100000, emin = 100000;
+    for (int64_t k = lane; k < K; k += 32) {
+      double v = fabs(A[row * K + k]);
+      if (v != 0.0 && isfinite(v)) {
+        int e = exp_of(v);
+        emax = max(emax, e);
+        emin = min(emin, e);
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      emax = max(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+      emin = min(emin, __shfl_xor_sync(0xffffffffu, emin, o));
+    }
+    if (emax >= emin) best = max(best, emax - emin);
+  }
+  if (lane == 0) atomicMax(out, best);
+}
+
+// Largest exponent gap of any column of B, one thread per column.
+__global__ void col_gap_kernel(const double* __restrict__ B, int64_t K, int64_t N, int* __restrict__ out) {
+  int best = 0;
+  for (int64_t col = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; col < N;
+       col += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int emax = -100000, emin = 100000;
+    for (int64_t k = 0; k < K; ++k) {
+      double v = fabs(B[k * N + col]);
+      if (v != 0.0 && isfinite(v)) {
+        int e = exp_of(v);
+        emax = max(emax, e);
+        emin = min(emin, e);
+      }
+    }
+    if (emax >= emin) best = max(best, emax - emin);
+  }
+  for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, best);
+}
+
+// Learned choice: the smallest slice count whose cumulative predicted probability reaches 0.9,
+// used only when the network is confident (largest class probability >= 0.5) and never above the
+// analytic count; otherwise the analytic count.
+int decide(const float* probs, int s_analytic, bool* learned) {
+  float mx = 0.f;
+  for (int c = 0; c < C; ++c) mx = fmaxf(mx, probs[c]);
+  *learned = false;
+  if (!(mx >= 0.5f)) return s_analytic;
+  float cdf = 0.f;
+  for (int c = 0; c < C; ++c) {
+    cdf += probs[c];
+    if (cdf >= 0.9f) {
+      int s = 3 + c;
+      if (s > s_analytic) return s_analytic;
+      *learned = true;
+      return s;
+    }
+  }
+  return s_analytic;
+}
+
+int device_params(const float** out) {
+  int dev = 0;
+  LT_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (g_host_params.empty()) {
+    *out = nullptr;
+    return LT_OK;
+  }
+  if (!g_dev_params_valid[dev]) {
+    if (g_dev_params[dev] == nullptr) LT_CUDA_TRY(cudaMalloc(&g_dev_params[dev], sizeof(float) * P));
+    LT_CUDA_TRY(cudaMemcpy(g_dev_params[dev], g_host_params.data(), sizeof(float) * P, cudaMemcpyHostToDevice));
+    g_dev_params_valid[dev] = true;
+  }
+  *out = g_dev_params[dev];
+  return LT_OK;
+}
+
+// Slice count for one problem (synchronous: the count decides the workspace layout and launches).
+int select(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, int* slices,
+           bool* learned, int* gap_bits, cudaStream_t stream) {
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  const float* params = nullptr;
+  LT_TRY(device_params(&params));
+  struct Scr {
+    float feat[F];
+    float probs[C];
+    int gaps[2];
+  };
+  Scr* d = nullptr;
+  LT_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(Scr), stream));
+  cudaError_t e = cudaMemsetAsync(d, 0, sizeof(Scr), stream);
+  if (e == cudaSuccess) {
+    row_gap_kernel<<<ctx->sm_count * 4, 256, 0, stream>>>(A, M, K, &d->gaps[0]);
+    col_gap_kernel<<<static_cast<unsigned>((N + 255) / 256), 256, 0, stream>>>(B, K, N, &d->gaps[1]);
+    e = cudaGetLastError();
+  }
+  int rc = LT_OK;
+  if (e == cudaSuccess && params != nullptr) {
+    rc = lt_ozaki_features(A, B, M, N, K, tol, d->feat, stream);
+    if (rc == LT_OK) rc = lt_mlp_forward(params, d->feat, 1, d->probs, stream);
+  }
+  Scr h;
+  if (e == cudaSuccess && rc == LT_OK) e = cudaMemcpyAsync(&h, d, sizeof(Scr), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  cudaFreeAsync(d, stream);
+  if (rc != LT_OK) return rc;
+  if (e != cudaSuccess) return set_error(LT_ERR_CUDA, "slice selection: %s", cudaGetErrorString(e));
+  *gap_bits = h.gaps[0] + h.gaps[1];
+  const int sa = analytic(tol, *gap_bits);
+  *slices = params != nullptr ? decide(h.probs, sa, learned) : sa;
+  if (params == nullptr) *learned = false;
+  return LT_OK;
+}
+
+}  // namespace sel
+}  // namespace lt
+
+extern "C" {
+
+int lt_ozaki_features(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, float* features,
+                      void* stream) {
+  if (M <= 0 || N <= 0 || K <= 0 || A == nullptr || B == nullptr || features == nullptr || !(tol > 0.0))
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_ozaki_features: bad arguments");
+  if (lt::context() == nullptr) return lt::last_error();
+  cudaStream_t s = lt::as_stream(stream);
+  unsigned int* hist = nullptr;
+  LT_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&hist), 32 * sizeof(unsigned int), s));
+  LT_CUDA_TRY(cudaMemsetAsync(hist, 0, 32 * sizeof(unsigned int), s));
+  const int rows = static_cast<int>(M < lt::sel::kSampleRows ? M : lt::sel::kSampleRows);
+  const int groups = static_cast<int>((N + 31) / 32 < lt::sel::kColGroups ? (N + 31) / 32 : lt::sel::kColGroups);
+  lt::sel::row_hist_kernel<<<rows, 256, 0, s>>>(A, M, K, rows, hist);
+  lt::sel::col_hist_kernel<<<groups, 256, 0, s>>>(B, K, N, groups, hist + 16);
+  lt::sel::features_finish_kernel<<<1, 64, 0, s>>>(hist, K, tol, features);
+  cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(hist, s);
+  if (e != cudaSuccess) return lt::set_error(LT_ERR_CUDA, "features: %s", cudaGetErrorString(e));
+  return lt::ok();
+}
+
+int lt_mlp_forward(const float* params, const float* x, int batch, float* probs, void* stream) {
+  if (params == nullptr || x == nullptr || probs == nullptr || batch <= 0)
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_mlp_forward: bad arguments");
+  if (lt::context() == nullptr) return lt::last_error();
+  lt::sel::mlp_forward_kernel<<<batch, LT_SEL_HIDDEN, 0, lt::as_stream(stream)>>>(params, x, batch, probs);
+  LT_CUDA_TRY(cudaGetLastError());
+  return lt::ok();
+}
+
+int lt_mlp_backward(const float* params, const float* x, const int* labels, int batch, float* grads, float* loss,
+                    void* stream) {
+  if (params == nullptr || x == nullptr || labels == nullptr || grads == nullptr || batch <= 0)
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_mlp_backward: bad arguments");
+  if (lt::context() == nullptr) return lt::last_error();
+  LT_TRY(lt::sel::backward(params, x, labels, batch, grads, loss, lt::as_stream(stream)));
+  return lt::ok();
+}
+
+int lt_mlp_train_step(float* params, float* m, float* v, float* grads, const float* x, const int* labels, int batch,
+                      float lr, int step, float* loss, void* stream) {
+  if (params == nullptr || m == nullptr || v == nullptr || grads == nullptr || x == nullptr || labels == nullptr ||
+      batch <= 0 || step < 1 || !(lr > 0.f))
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_mlp_train_step: bad arguments");
+  if (lt::context() == nullptr) return lt::last_error();
+  cudaStream_t s = lt::as_stream(stream);
+  LT_TRY(lt::sel::backward(params, x, labels, batch, grads, loss, s));
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - powf(b1, static_cast<float>(step)), c2 = 1.f - powf(b2, static_cast<float>(step));
+  lt::sel::adam_kernel<<<(LT_SEL_PARAMS + 255) / 256, 256, 0, s>>>(params, m, v, grads, lr, b1, b2, 1e-8f, c1, c2);
+  LT_CUDA_TRY(cudaGetLastError());
+  return lt::ok();
+}
+
+int lt_selector_set_params(const float* host_params) {
+  std::lock_guard<std::mutex> lock(lt::sel::g_mutex);
+  if (host_params == nullptr) {
+    lt::sel::g_host_params.clear();
+  } else {
+    lt::sel::g_host_params.assign(host_params, host_params + LT_SEL_PARAMS);
+  }
+  for (int d = 0; d < 64; ++d) lt::sel::g_dev_params_valid[d] = false;
+  return lt::ok();
+}
+
+void lt_set_ozaki_tolerance(double tol) {
+  if (tol > 0.0) lt::sel::g_tol = tol;
+}
+
+int lt_ozaki_analytic_slices(double tol, int gap_bits) {
+  if (!(tol > 0.0) || gap_bits < 0) {
+    lt::set_error(LT_ERR_INVALID_ARGUMENT, "bad tolerance or gap");
+    return 0;
+  }
+  return lt::sel::analytic(tol, gap_bits);
+}
+
+int lt_ozaki_select_slices(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, int* slices,
+                           void* stream) {
+  if (M <= 0 || N <= 0 || K <= 0 || A == nullptr || B == nullptr || slices == nullptr || !(tol > 0.0))
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_ozaki_select_slices: bad arguments");
+  bool learned = false;
+  int gap = 0;
+  LT_TRY(lt::sel::select(A, B, M, N, K, tol, slices, &learned, &gap, lt::as_stream(stream)));
+  return lt::ok();
+}
+
+int lt_ozaki_select_info(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, int* slices,
+                         int* learned, int* gap_bits, void* stream) {
+  if (M <= 0 || N <= 0 || K <= 0 || A == nullptr || B == nullptr || slices == nullptr || !(tol > 0.0))
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_ozaki_select_info: bad arguments");
+  bool l = false;
+  int g = 0;
+  LT_TRY(lt::sel::select(A, B, M, N, K, tol, slices, &l, &g, lt::as_stream(stream)));
+  if (learned) *learned = l ? 1 : 0;
+  if (gap_bits) *gap_bits = g;
+  return lt::ok();
+}
+
+float dgemm_ozaki_auto(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha,
+                       double beta) {
+  cudaEvent_t start, stop;
+  cudaEventCreate(&start);
+  cudaEventCreate(&stop);
+  cudaEventRecord(start, 0);
+  int rc = LT_OK;
+  int s = 0;
+  if (M > 0 && N > 0 && K > 0)
+    rc = lt_ozaki_select_slices(A, B, static_cast<int64_t>(M), static_cast<int64_t>(N), static_cast<int64_t>(K),
+                                lt::sel::g_tol, &s, nullptr);
+  if (rc == LT_OK)
+    rc = lt_dgemm_ozaki(A, B, C, static_cast<int64_t>(M), static_cast<int64_t>(N), static_cast<int64_t>(K), alpha,
+                        beta, s > 0 ? s : 1, nullptr);
+  cudaEventRecord(stop, 0);
+  cudaEventSynchronize(stop);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, start, stop);
+  cudaEventDestroy(start);
+  cudaEventDestroy(stop);
+  if (rc == LT_OK) rc = lt_check_device_status();
+  if (rc != LT_OK) {
+    fprintf(stderr, "Kernel launch error (ozaki_auto): %s: %s\n", lt_error_string(rc), lt::last_message());
+    lt::set_error(rc, "%s", lt::last_message());
+  }
+  return ms;
+}
+
+}  // extern "C"

@@ -58,7 +58,13 @@ def lib() -> ctypes.CDLL:
         L.oracle_ozaki_split_cols.argtypes = [_vp, _i64, _i64, _vp, _i32, _vp, _i64]
         L.oracle_ozaki_dgemm.argtypes = [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _i32, _i32]
         L.oracle_ozaki_analytic_slices.restype = _i32
-        L.oracle_ozaki_analytic_slices.argtypes = [_f64, _i64, _i32]
+        L.oracle_ozaki_analytic_slices.argtypes = [_f64, _i32]
+        L.oracle_max_gap.restype = _i32
+        L.oracle_max_gap.argtypes = [_vp, _i64, _i64, _i32]
+        L.oracle_features.argtypes = [_vp, _vp, _i64, _i64, _i64, _f64, _vp]
+        L.oracle_mlp_forward.argtypes = [_vp, _vp, _i32, _vp]
+        L.oracle_mlp_backward.restype = _f64
+        L.oracle_mlp_backward.argtypes = [_vp, _vp, _vp, _i32, _vp]
         _lib = L
     return _lib
 
@@ -185,5 +191,40 @@ def ozaki_split(A, B, s):
     return sigma, tau, sa, sb
 
 
-def analytic_slices(tol: float, K: int, phi_spread: int) -> int:
-    return int(lib().oracle_ozaki_analytic_slices(tol, K, phi_spread))
+def analytic_slices(tol: float, gap_bits: int) -> int:
+    return int(lib().oracle_ozaki_analytic_slices(tol, gap_bits))
+
+
+def gap_bits(A, B) -> int:
+    """Largest exponent gap within a row of A plus the largest within a column of B."""
+    L = lib()
+    return int(L.oracle_max_gap(_p(A), A.shape[0], A.shape[1], 1)) + int(L.oracle_max_gap(_p(B), B.shape[0], B.shape[1], 0))
+
+
+# ---- selector restatements ---------------------------------------------------------------------
+SEL_F, SEL_H, SEL_C = 34, 64, 8
+SEL_P = SEL_F * SEL_H + SEL_H + SEL_H * SEL_H + SEL_H + SEL_H * SEL_C + SEL_C
+
+
+def features(A, B, tol: float) -> np.ndarray:
+    M, K = A.shape
+    N = B.shape[1]
+    f = np.empty(SEL_F, dtype=np.float32)
+    lib().oracle_features(_p(A), _p(B), M, N, K, tol, _p(f))
+    return f
+
+
+def mlp_forward(params: np.ndarray, x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty((x.shape[0], SEL_C), dtype=np.float32)
+    lib().oracle_mlp_forward(_p(np.ascontiguousarray(params, dtype=np.float32)), _p(x), x.shape[0], _p(out))
+    return out
+
+
+def mlp_backward(params: np.ndarray, x: np.ndarray, labels: np.ndarray):
+    """(mean loss, mean gradient) in double precision."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.ascontiguousarray(labels, dtype=np.int32)
+    g = np.empty(SEL_P, dtype=np.float64)
+    loss = lib().oracle_mlp_backward(_p(np.ascontiguousarray(params, dtype=np.float32)), _p(x), _p(y), x.shape[0], _p(g))
+    return float(loss), g

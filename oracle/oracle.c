@@ -374,15 +374,175 @@ void oracle_ozaki_dgemm(const double* A, const double* B, double* C, int64_t M, 
   free(sigma); free(tau); free(sa); free(sb);
 }
 
-/* Conservative slice count. Truncating every entry of row i after s slices leaves an error
- * below 2^(sigma_i - 7s); the dropped pairs p+q > s+1 add at most s more such terms. Relative to
- * the componentwise denominator sum_k |a_ik||b_kj|, the worst case loses the full exponent spread
- * of a row and of a column (phi_spread bits each), so s must satisfy
- *   (s + 2) K 2^(2 phi_spread - 7 s) <= tol. */
-int oracle_ozaki_analytic_slices(double tol, int64_t K, int phi_spread) {
-  for (int s = 1; s <= 16; ++s) {
-    double bound = (double)(s + 2) * (double)K * ldexp(1.0, 2 * phi_spread - 7 * s);
+/* Conservative slice count (same rule as the library's selector fallback). gap_bits = largest
+ * exponent gap e(max) - e(min nonzero) within a row of A plus the largest within a column of B. An
+ * entry with gap g keeps at least 7s - g - 1 bits after truncation, so the two truncated tails and
+ * the dropped pairs p + q > s + 1 bound the componentwise error by (s + 3) 2^(gap_bits + 2 - 7s);
+ * the FP64 recombination and epilogue add at most 4u. The smallest s in [1, 12] meeting tol. */
+int oracle_ozaki_analytic_slices(double tol, int gap_bits) {
+  for (int s = 1; s <= 12; ++s) {
+    double bound = (double)(s + 3) * ldexp(1.0, gap_bits + 2 - 7 * s) + 4.0 * ldexp(1.0, -53);
     if (bound <= tol) return s;
   }
-  return 16;
+  return 12;
+}
+
+/* Largest exponent gap of any row (by_rows) or column of a rows x cols row-major matrix. */
+int oracle_max_gap(const double* X, int64_t rows, int64_t cols, int by_rows) {
+  int best = 0;
+  int64_t outer = by_rows ? rows : cols, inner = by_rows ? cols : rows;
+  for (int64_t o = 0; o < outer; ++o) {
+    int emax = -100000, emin = 100000;
+    for (int64_t i = 0; i < inner; ++i) {
+      double v = fabs(by_rows ? X[o * cols + i] : X[i * cols + o]);
+      if (v != 0.0 && isfinite(v)) {
+        int e;
+        frexp(v, &e);
+        if (e > emax) emax = e;
+        if (e < emin) emin = e;
+      }
+    }
+    if (emax >= emin && emax - emin > best) best = emax - emin;
+  }
+  return best;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Selector restatements: features and the 34-64-64-8 GELU MLP (forward, backward), in double. */
+/* ------------------------------------------------------------------------------------------ */
+static int gap_bin(int g) { return g >= 60 ? 15 : (g < 0 ? 0 : g >> 2); }
+
+void oracle_features(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, float* feat) {
+  double hist[32];
+  memset(hist, 0, sizeof hist);
+  int rows = (int)(M < 128 ? M : 128);
+  for (int r = 0; r < rows; ++r) {
+    int64_t row = rows > 1 ? ((int64_t)r * (M - 1)) / (rows - 1) : 0;
+    int em = -100000;
+    for (int64_t k = 0; k < K; ++k) {
+      double v = fabs(A[row * K + k]);
+      if (v != 0.0 && isfinite(v)) { int e; frexp(v, &e); if (e > em) em = e; }
+    }
+    for (int64_t k = 0; k < K; ++k) {
+      double v = fabs(A[row * K + k]);
+      int b = 0;
+      if (v != 0.0 && isfinite(v)) { int e; frexp(v, &e); b = gap_bin(em - e); }
+      hist[b] += 1;
+    }
+  }
+  int groups = (int)((N + 31) / 32 < 4 ? (N + 31) / 32 : 4);
+  int64_t span = N > 32 ? N - 32 : 0;
+  for (int gI = 0; gI < groups; ++gI) {
+    int64_t c0 = groups > 1 ? ((int64_t)gI * span) / (groups - 1) : 0;
+    for (int l = 0; l < 32; ++l) {
+      int64_t col = c0 + l;
+      if (col >= N) continue;
+      int em = -100000;
+      for (int64_t k = 0; k < K; ++k) {
+        double v = fabs(B[k * N + col]);
+        if (v != 0.0 && isfinite(v)) { int e; frexp(v, &e); if (e > em) em = e; }
+      }
+      for (int64_t k = 0; k < K; ++k) {
+        double v = fabs(B[k * N + col]);
+        int b = 0;
+        if (v != 0.0 && isfinite(v)) { int e; frexp(v, &e); b = gap_bin(em - e); }
+        hist[16 + b] += 1;
+      }
+    }
+  }
+  for (int h = 0; h < 2; ++h) {
+    double tot = 0;
+    for (int i = 0; i < 16; ++i) tot += hist[16 * h + i];
+    for (int i = 0; i < 16; ++i) feat[16 * h + i] = tot > 0 ? (float)(hist[16 * h + i] / tot) : 0.f;
+  }
+  feat[32] = (float)(log2((double)(K > 0 ? K : 1)) / 16.0);
+  feat[33] = (float)(-log10(tol) / 16.0);
+}
+
+#define SEL_F 34
+#define SEL_H 64
+#define SEL_C 8
+#define OW1 0
+#define OB1 (OW1 + SEL_H * SEL_F)
+#define OW2 (OB1 + SEL_H)
+#define OB2 (OW2 + SEL_H * SEL_H)
+#define OW3 (OB2 + SEL_H)
+#define OB3 (OW3 + SEL_C * SEL_H)
+#define SEL_P (OB3 + SEL_C)
+
+static double gelu_d(double x) {
+  const double k = 0.7978845608028654;
+  return 0.5 * x * (1.0 + tanh(k * (x + 0.044715 * x * x * x)));
+}
+static double gelu_grad_d(double x) {
+  const double k = 0.7978845608028654;
+  double t = tanh(k * (x + 0.044715 * x * x * x));
+  return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * k * (1.0 + 3.0 * 0.044715 * x * x);
+}
+
+static void mlp_fwd1(const float* p, const float* x, double* h1, double* a1, double* h2, double* a2, double* prob) {
+  for (int j = 0; j < SEL_H; ++j) {
+    double acc = p[OB1 + j];
+    for (int i = 0; i < SEL_F; ++i) acc += (double)p[OW1 + j * SEL_F + i] * x[i];
+    h1[j] = acc; a1[j] = gelu_d(acc);
+  }
+  for (int j = 0; j < SEL_H; ++j) {
+    double acc = p[OB2 + j];
+    for (int i = 0; i < SEL_H; ++i) acc += (double)p[OW2 + j * SEL_H + i] * a1[i];
+    h2[j] = acc; a2[j] = gelu_d(acc);
+  }
+  double lg[SEL_C], mx = -1e300, sum = 0;
+  for (int c = 0; c < SEL_C; ++c) {
+    double acc = p[OB3 + c];
+    for (int i = 0; i < SEL_H; ++i) acc += (double)p[OW3 + c * SEL_H + i] * a2[i];
+    lg[c] = acc; if (acc > mx) mx = acc;
+  }
+  for (int c = 0; c < SEL_C; ++c) { prob[c] = exp(lg[c] - mx); sum += prob[c]; }
+  for (int c = 0; c < SEL_C; ++c) prob[c] /= sum;
+}
+
+void oracle_mlp_forward(const float* params, const float* x, int batch, float* probs) {
+  double h1[SEL_H], a1[SEL_H], h2[SEL_H], a2[SEL_H], pr[SEL_C];
+  for (int b = 0; b < batch; ++b) {
+    mlp_fwd1(params, x + (int64_t)b * SEL_F, h1, a1, h2, a2, pr);
+    for (int c = 0; c < SEL_C; ++c) probs[(int64_t)b * SEL_C + c] = (float)pr[c];
+  }
+}
+
+/* Mean cross-entropy gradient over the batch (double accumulation); returns the mean loss. */
+double oracle_mlp_backward(const float* p, const float* x, const int* labels, int batch, double* grads) {
+  double h1[SEL_H], a1[SEL_H], h2[SEL_H], a2[SEL_H], pr[SEL_C], d3[SEL_C], d2[SEL_H], d1[SEL_H];
+  double loss = 0;
+  memset(grads, 0, sizeof(double) * SEL_P);
+  for (int b = 0; b < batch; ++b) {
+    const float* xb = x + (int64_t)b * SEL_F;
+    mlp_fwd1(p, xb, h1, a1, h2, a2, pr);
+    int y = labels[b];
+    loss += -log(pr[y] > 1e-30 ? pr[y] : 1e-30);
+    for (int c = 0; c < SEL_C; ++c) d3[c] = pr[c] - (c == y ? 1.0 : 0.0);
+    for (int c = 0; c < SEL_C; ++c) {
+      for (int i = 0; i < SEL_H; ++i) grads[OW3 + c * SEL_H + i] += d3[c] * a2[i];
+      grads[OB3 + c] += d3[c];
+    }
+    for (int i = 0; i < SEL_H; ++i) {
+      double acc = 0;
+      for (int c = 0; c < SEL_C; ++c) acc += (double)p[OW3 + c * SEL_H + i] * d3[c];
+      d2[i] = acc * gelu_grad_d(h2[i]);
+    }
+    for (int j = 0; j < SEL_H; ++j) {
+      for (int i = 0; i < SEL_H; ++i) grads[OW2 + j * SEL_H + i] += d2[j] * a1[i];
+      grads[OB2 + j] += d2[j];
+    }
+    for (int i = 0; i < SEL_H; ++i) {
+      double acc = 0;
+      for (int j = 0; j < SEL_H; ++j) acc += (double)p[OW2 + j * SEL_H + i] * d2[j];
+      d1[i] = acc * gelu_grad_d(h1[i]);
+    }
+    for (int j = 0; j < SEL_H; ++j) {
+      for (int i = 0; i < SEL_F; ++i) grads[OW1 + j * SEL_F + i] += d1[j] * xb[i];
+      grads[OB1 + j] += d1[j];
+    }
+  }
+  for (int i = 0; i < SEL_P; ++i) grads[i] /= batch;
+  return loss / batch;
 }

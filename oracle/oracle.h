@@ -73,8 +73,15 @@ void oracle_ozaki_split_cols(const double* B, int64_t K, int64_t N, const int32_
 /* Full Ozaki DGEMM, triangular pair set p+q <= s+1, same accumulation order as the CUDA path. */
 void oracle_ozaki_dgemm(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
                         double alpha, double beta, int s, int nthreads);
-/* Analytic slice count for a target componentwise tolerance (the conservative selector). */
-int oracle_ozaki_analytic_slices(double tol, int64_t K, int phi_spread);
+/* Analytic slice count for a target componentwise tolerance (the selector's conservative fallback);
+ * gap_bits = largest exponent gap within a row of A plus the largest within a column of B. */
+int oracle_ozaki_analytic_slices(double tol, int gap_bits);
+int oracle_max_gap(const double* X, int64_t rows, int64_t cols, int by_rows);
+
+/* ---- learned slice selector restatements ---- */
+void oracle_features(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, float* feat);
+void oracle_mlp_forward(const float* params, const float* x, int batch, float* probs);
+double oracle_mlp_backward(const float* params, const float* x, const int* labels, int batch, double* grads);
 
 #ifdef __cplusplus
 }

@@ -60,7 +60,17 @@ def test_errors_without_gpu():
     assert b"8-byte" in L.lt_last_error_message()
     assert L.lt_ozaki_workspace_size(8192, 8192, 8192, 8) >= 8 * 2 * 8192 * 8192
     assert L.lt_ozaki_workspace_size(8, 8, 8, 0) == 0
-    assert L.lt_ozaki_analytic_slices(1e-15, 8192, 0) >= 8
+    assert L.lt_ozaki_analytic_slices(1e-15, 0) >= 8
+    assert L.lt_ozaki_analytic_slices(-1.0, 0) == 0
+
+
+def test_analytic_rule_matches_oracle(oracle_mod):
+    import libthom_b200 as lt
+
+    L = lt.lib()
+    for tol in (1e-6, 1e-10, 1e-12, 1e-14, 1e-15):
+        for gap in (0, 5, 20, 40, 64, 100):
+            assert L.lt_ozaki_analytic_slices(tol, gap) == oracle_mod.analytic_slices(tol, gap)
 
 
 def test_unknown_impl_rejected():

@@ -148,6 +148,48 @@ def test_ozaki_long_k_groups(oracle_mod):
 
 
 def test_analytic_slices_monotone(oracle_mod):
-    a = [oracle_mod.analytic_slices(t, 8192, 0) for t in (1e-6, 1e-10, 1e-12, 1e-14, 1e-15)]
+    a = [oracle_mod.analytic_slices(t, 0) for t in (1e-6, 1e-10, 1e-12, 1e-14, 1e-15)]
     assert a == sorted(a) and a[-1] >= 8
-    assert oracle_mod.analytic_slices(1e-12, 8192, 32) > oracle_mod.analytic_slices(1e-12, 8192, 0)
+    assert oracle_mod.analytic_slices(1e-12, 64) > oracle_mod.analytic_slices(1e-12, 0)
+
+
+@pytest.mark.parametrize("phi,smax", [(0, 0), (8, 0), (32, 0), (0, 64)])
+def test_analytic_count_is_conservative(oracle_mod, phi, smax):
+    """The analytic count meets its tolerance on every sampled problem (it is the fallback)."""
+    M, N, K = 40, 30, 256
+    A, B, C0 = oracle_mod.make_problem(M, N, K, phi=phi, seed=phi + smax, smax=smax)
+    Cref, den = oracle_mod.dot2_rows(A, B, C0, 1.0, 0.0)
+    g = oracle_mod.gap_bits(A, B)
+    for tol in (1e-12, 1e-14):
+        s = oracle_mod.analytic_slices(tol, g)
+        if s == 12 and (s + 3) * 2.0 ** (g + 2 - 7 * s) > tol:
+            continue  # beyond the largest slice count: no claim
+        C = oracle_mod.ozaki_dgemm(A, B, C0, 1.0, 0.0, s)
+        assert oracle_mod.componentwise_error(C, Cref, den)[0] <= tol, (phi, smax, tol, s, g)
+
+
+def test_mlp_backward_matches_finite_differences(oracle_mod):
+    rng = np.random.default_rng(0)
+    P = oracle_mod.SEL_P
+    params = (rng.standard_normal(P) * 0.2).astype(np.float32)
+    x = rng.random((6, oracle_mod.SEL_F)).astype(np.float32)
+    y = rng.integers(0, 8, 6).astype(np.int32)
+    loss, g = oracle_mod.mlp_backward(params, x, y)
+    for i in rng.choice(P, 25, replace=False):
+        h = 1e-2
+        pp = params.astype(np.float64)
+        for sign, store in ((1, "p"), (-1, "m")):
+            q = pp.copy()
+            q[i] += sign * h
+            val = oracle_mod.mlp_backward(q.astype(np.float32), x, y)[0]
+            if store == "p":
+                lp = val
+            else:
+                lm = val
+        # the float32 parameter perturbation is exact for h = 1e-2 only up to float rounding
+        hp = float(np.float32(pp[i] + h)) - pp[i]
+        hm = pp[i] - float(np.float32(pp[i] - h))
+        fd = (lp - lm) / (hp + hm)
+        assert abs(fd - g[i]) <= 2e-3 * max(1.0, abs(g[i])), (i, fd, g[i])
+    probs = oracle_mod.mlp_forward(params, x)
+    assert np.allclose(probs.sum(axis=1), 1.0, atol=1e-6)
