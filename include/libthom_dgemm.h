@@ -117,6 +117,11 @@ int lt_grouped_plan_run(lt_grouped_plan* plan, void* stream);
 /* Captures lt_grouped_plan_run into a CUDA graph once, then replays it on `stream`. */
 int lt_grouped_plan_run_graph(lt_grouped_plan* plan, void* stream);
 int lt_grouped_plan_info(const lt_grouped_plan* plan, int64_t* tiles, double* flops);
+/* Autotunes the plan's FP64 tile shape on its own problems (validated against cuBLAS FP64, median
+ * of `iters` timed runs, scratch outputs); no-op for the Ozaki form. Synchronous. */
+int lt_grouped_plan_tune(lt_grouped_plan* plan, int iters, float* best_ms);
+/* Name of the kernel configuration the plan runs. */
+int lt_grouped_plan_config(const lt_grouped_plan* plan, char* name, int name_len);
 void lt_grouped_plan_destroy(lt_grouped_plan* plan);
 /* Convenience: create, run once, destroy. */
 int lt_dgemm_grouped(const lt_gemm_problem* problems, int count, int form, int slices, void* stream);

@@ -88,6 +88,8 @@ SIGNATURES = {
     "lt_grouped_plan_run_graph": (_i32, [_vp, _vp]),
     "lt_grouped_plan_info": (_i32, [_vp, _c.POINTER(_i64), _c.POINTER(_f64)]),
     "lt_grouped_plan_destroy": (None, [_vp]),
+    "lt_grouped_plan_tune": (_i32, [_vp, _i32, _c.POINTER(_f32)]),
+    "lt_grouped_plan_config": (_i32, [_vp, _c.c_char_p, _i32]),
     "lt_dgemm_grouped": (_i32, [_vp, _i32, _i32, _i32, _vp]),
     "lt_tune_fp64": (_i32, [_i64, _i64, _i64, _i32, _c.POINTER(TuneEntry)]),
     "lt_tuner_save": (_i32, [_c.c_char_p]),

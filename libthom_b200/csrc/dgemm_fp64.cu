@@ -1,5 +1,7 @@
 // dgemm_fp64.cu — host launchers and configuration registry of the native FP64 DGEMM.
+#include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "dgemm_fp64.cuh"
 #include "lt_runtime.cuh"
@@ -97,6 +99,116 @@ int heuristic_config(const double* A, const double* B, int64_t M, int64_t N, int
     if (kConfigs[i].tma == tma && kConfigs[i].bm * kConfigs[i].bn <= chosen_bm * chosen_bn) return i;
   return kNumConfigs - 1;
 }
+
+// ---- grouped launches (cp.async staging: problems have arbitrary shapes and alignment) ----
+namespace {
+
+template <class Cfg>
+int launch_grouped(const GroupProblem* problems, const GroupTile* tiles, int64_t ntiles, cudaStream_t stream,
+                   DeviceContext* ctx) {
+  static std::once_flag once[64];
+  static int occupancy[64];
+  static cudaError_t attr_err[64];
+  std::call_once(once[ctx->device], [&] {
+    attr_err[ctx->device] = cudaFuncSetAttribute(dgemm_fp64_grouped_kernel<Cfg>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM_BYTES);
+    int occ = 0;
+    if (attr_err[ctx->device] == cudaSuccess)
+      attr_err[ctx->device] = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, dgemm_fp64_grouped_kernel<Cfg>,
+                                                                            Cfg::THREADS, Cfg::SMEM_BYTES);
+    occupancy[ctx->device] = occ > 0 ? occ : 1;
+  });
+  LT_CUDA_TRY(attr_err[ctx->device]);
+  int64_t grid = static_cast<int64_t>(ctx->sm_count) * occupancy[ctx->device];
+  if (grid > ntiles) grid = ntiles;
+  if (grid < 1) return LT_OK;
+  GroupedSource src{problems, tiles, ntiles};
+  dgemm_fp64_grouped_kernel<Cfg><<<static_cast<unsigned>(grid), Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(src,
+                                                                                                         ctx->status);
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
+using GroupedFn = int (*)(const GroupProblem*, const GroupTile*, int64_t, cudaStream_t, DeviceContext*);
+struct GroupedEntry {
+  const char* name;
+  GroupedFn fn;
+  int bm, bn;
+};
+const GroupedEntry kGrouped[] = {
+    {"grouped_cpa_128x64_s6", launch_grouped<Config<128, 64, 6, false>>, 128, 64},
+    {"grouped_cpa_64x64_s6", launch_grouped<Config<64, 64, 6, false>>, 64, 64},
+    {"grouped_cpa_64x32_s6", launch_grouped<Config<64, 32, 6, false>>, 64, 32},
+    {"grouped_cpa_32x32_s6", launch_grouped<Config<32, 32, 6, false>>, 32, 32},
+};
+constexpr int kNumGrouped = static_cast<int>(sizeof(kGrouped) / sizeof(kGrouped[0]));
+
+}  // namespace
+
+struct GroupedFp64 {
+  int cfg = 0;
+  void* dev = nullptr;
+  GroupProblem* d_problems = nullptr;
+  GroupTile* d_tiles = nullptr;
+  int64_t ntiles = 0;
+};
+
+int grouped_num_configs() { return kNumGrouped; }
+const char* grouped_config_name(int cfg) { return (cfg >= 0 && cfg < kNumGrouped) ? kGrouped[cfg].name : nullptr; }
+
+int grouped_create(const lt_gemm_problem* problems, int count, int cfg, GroupedFp64** out) {
+  if (cfg < 0 || cfg >= kNumGrouped) return set_error(LT_ERR_INVALID_ARGUMENT, "grouped config %d", cfg);
+  const int bm = kGrouped[cfg].bm, bn = kGrouped[cfg].bn;
+  std::vector<GroupProblem> probs(count);
+  std::vector<int> order(count);
+  for (int i = 0; i < count; ++i) {
+    const lt_gemm_problem& p = problems[i];
+    probs[i] = GroupProblem{p.A, p.B, p.C, p.M, p.N, p.K, p.alpha, p.beta};
+    order[i] = i;
+  }
+  // Longest-K problems first: with a static round-robin over the CTAs this balances the work.
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return problems[a].K > problems[b].K; });
+  std::vector<GroupTile> tiles;
+  for (int i : order) {
+    const int64_t tm = (problems[i].M + bm - 1) / bm, tn = (problems[i].N + bn - 1) / bn;
+    for (int64_t a = 0; a < tm; ++a)
+      for (int64_t b = 0; b < tn; ++b) tiles.push_back(GroupTile{i, static_cast<int>(a * bm), static_cast<int>(b * bn), 0});
+  }
+  auto* G = new GroupedFp64();
+  G->cfg = cfg;
+  G->ntiles = static_cast<int64_t>(tiles.size());
+  const size_t pb = (sizeof(GroupProblem) * count + 255) / 256 * 256;
+  const size_t tb = sizeof(GroupTile) * (tiles.size() + 1);
+  cudaError_t e = cudaMalloc(&G->dev, pb + tb);
+  if (e == cudaSuccess) {
+    G->d_problems = static_cast<GroupProblem*>(G->dev);
+    G->d_tiles = reinterpret_cast<GroupTile*>(static_cast<uint8_t*>(G->dev) + pb);
+    e = cudaMemcpy(G->d_problems, probs.data(), sizeof(GroupProblem) * count, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !tiles.empty())
+      e = cudaMemcpy(G->d_tiles, tiles.data(), sizeof(GroupTile) * tiles.size(), cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    cudaFree(G->dev);
+    delete G;
+    return set_error(LT_ERR_NO_MEMORY, "grouped FP64 tables: %s", cudaGetErrorString(e));
+  }
+  *out = G;
+  return LT_OK;
+}
+
+int grouped_run(const GroupedFp64* G, cudaStream_t stream) {
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  return kGrouped[G->cfg].fn(G->d_problems, G->d_tiles, G->ntiles, stream, ctx);
+}
+
+void grouped_destroy(GroupedFp64* G) {
+  if (G == nullptr) return;
+  cudaFree(G->dev);
+  delete G;
+}
+
+int64_t grouped_tiles(const GroupedFp64* G) { return G->ntiles; }
 
 int run_config(int cfg, const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
                double beta, cudaStream_t stream) {

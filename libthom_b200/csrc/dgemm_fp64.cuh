@@ -95,9 +95,58 @@ __device__ __forceinline__ void tile_coords(int64_t t, int64_t tiles_m, int64_t 
   tn = in_group / gsize;
 }
 
+// One output tile of one problem.
+struct Job {
+  const double* A;
+  const double* B;
+  double* C;
+  int64_t M, N, K;
+  double alpha, beta;
+  int64_t m0, n0;
+};
+
+// Tiles of a single problem, walked in grouped raster order.
 template <class Cfg>
-__global__ void __launch_bounds__(Cfg::THREADS, 1)
-    dgemm_fp64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p) {
+struct SingleSource {
+  Params p;
+  int64_t tiles_m, tiles_n;
+  __device__ int64_t count() const { return tiles_m * tiles_n; }
+  __device__ Job get(int64_t t) const {
+    int64_t tm, tn;
+    tile_coords(t, tiles_m, tiles_n, tm, tn);
+    return Job{p.A, p.B, p.C, p.M, p.N, p.K, p.alpha, p.beta, tm * Cfg::BM, tn * Cfg::BN};
+  }
+};
+
+// Grouped launch: a device table of problems and a tile list (sorted by decreasing K on the host
+// so that the static round-robin over CTAs hands out the expensive tiles first).
+struct GroupProblem {
+  const double* A;
+  const double* B;
+  double* C;
+  int64_t M, N, K;
+  double alpha, beta;
+};
+struct GroupTile {
+  int problem;
+  int m0, n0;
+  int pad;
+};
+struct GroupedSource {
+  const GroupProblem* problems;
+  const GroupTile* tiles;
+  int64_t ntiles;
+  __device__ int64_t count() const { return ntiles; }
+  __device__ Job get(int64_t t) const {
+    const GroupTile gt = tiles[t];
+    const GroupProblem& pr = problems[gt.problem];
+    return Job{pr.A, pr.B, pr.C, pr.M, pr.N, pr.K, pr.alpha, pr.beta, gt.m0, gt.n0};
+  }
+};
+
+template <class Cfg, class Source>
+__device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensorMap* tmB, const Source& src,
+                                          DeviceStatus* status) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES);
@@ -105,9 +154,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(empty + Cfg::STAGES);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t tiles_m = (p.M + Cfg::BM - 1) / Cfg::BM, tiles_n = (p.N + Cfg::BN - 1) / Cfg::BN;
-  const int64_t tiles = tiles_m * tiles_n;
-  const int kblocks = static_cast<int>((p.K + Cfg::BK - 1) / Cfg::BK);
+  const int64_t tiles = src.count();
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < Cfg::STAGES; ++s) {
@@ -123,45 +170,45 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
     // ------------------------------- producer warp -------------------------------
     if (Cfg::kTMA) {
       if (lane == 0) {
-        tma_prefetch_desc(&tmA);
-        tma_prefetch_desc(&tmB);
+        tma_prefetch_desc(tmA);
+        tma_prefetch_desc(tmB);
       }
     }
     int stage = 0;
     uint32_t phase = 0;
     bool ok = true;
     for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-      int64_t tm, tn;
-      tile_coords(t, tiles_m, tiles_n, tm, tn);
-      const int64_t m0 = tm * Cfg::BM, n0 = tn * Cfg::BN;
+      const Job J = src.get(t);
+      const int64_t m0 = J.m0, n0 = J.n0;
+      const int kblocks = static_cast<int>((J.K + Cfg::BK - 1) / Cfg::BK);
       for (int kb = 0; kb < kblocks; ++kb) {
-        if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.status, 1)) { ok = false; break; }
+        if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, status, 1)) { ok = false; break; }
         uint8_t* sa = smem + stage * Cfg::STAGE_BYTES;
         uint8_t* sb = sa + Cfg::A_BYTES;
         const int k0 = kb * Cfg::BK;
         if (Cfg::kTMA) {
           if (lane == 0) {
             mbar_arrive_expect_tx(&full[stage], Cfg::STAGE_BYTES);
-            tma_load_2d(sa, &tmA, &full[stage], k0, static_cast<int>(m0));
+            tma_load_2d(sa, tmA, &full[stage], k0, static_cast<int>(m0));
 #pragma unroll
             for (int j = 0; j < Cfg::BN / 16; ++j)
-              tma_load_2d(sb + j * 2048, &tmB, &full[stage], static_cast<int>(n0) + 16 * j, k0);
+              tma_load_2d(sb + j * 2048, tmB, &full[stage], static_cast<int>(n0) + 16 * j, k0);
           }
         } else {
           // A: BM rows x 16 doubles, one double per cp.async (rows and K may be ragged/odd).
           for (int e = lane; e < Cfg::BM * 16; e += 32) {
             int r = e >> 4, c = e & 15;
             int64_t gr = m0 + r, gk = k0 + c;
-            bool v = (gr < p.M) && (gk < p.K);
-            const double* src = v ? p.A + gr * p.K + gk : p.A;
-            cp_async_8(sa + a_off(r, c >> 1) + ((c & 1) << 3), src, v);
+            bool v = (gr < J.M) && (gk < J.K);
+            const double* gp = v ? J.A + gr * J.K + gk : J.A;
+            cp_async_8(sa + a_off(r, c >> 1) + ((c & 1) << 3), gp, v);
           }
           for (int e = lane; e < 16 * Cfg::BN; e += 32) {
             int k = e / Cfg::BN, n = e % Cfg::BN;
             int64_t gk = k0 + k, gn = n0 + n;
-            bool v = (gk < p.K) && (gn < p.N);
-            const double* src = v ? p.B + gk * p.N + gn : p.B;
-            cp_async_8(sb + b_off(k, n), src, v);
+            bool v = (gk < J.K) && (gn < J.N);
+            const double* gp = v ? J.B + gk * J.N + gn : J.B;
+            cp_async_8(sb + b_off(k, n), gp, v);
           }
           cp_async_mbar_arrive_noinc(&full[stage]);
         }
@@ -178,8 +225,8 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
     uint32_t phase = 0;
     bool ok = true;
     for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-      int64_t tm, tn;
-      tile_coords(t, tiles_m, tiles_n, tm, tn);
+      const Job J = src.get(t);
+      const int kblocks = static_cast<int>((J.K + Cfg::BK - 1) / Cfg::BK);
       double acc[2][4][4];
 #pragma unroll
       for (int i = 0; i < 2; ++i)
@@ -189,7 +236,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
           for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
 
       for (int kb = 0; kb < kblocks; ++kb) {
-        if (!mbar_wait(&full[stage], phase, abort_flag, p.status, 2)) { ok = false; break; }
+        if (!mbar_wait(&full[stage], phase, abort_flag, status, 2)) { ok = false; break; }
         const uint32_t sa = smem_base + stage * Cfg::STAGE_BYTES;
         const uint32_t sb = sa + Cfg::A_BYTES;
         double af[2][8], bf[4][4];
@@ -222,39 +269,53 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
       if (!ok) break;
 
       // ---- epilogue: C = alpha*acc + beta*C0, 16-byte vectors where the row stride allows ----
-      const int64_t m0 = tm * Cfg::BM + wm * Cfg::WM, n0 = tn * Cfg::BN + wn * Cfg::WN;
-      const bool vec = ((p.N & 1) == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0);
+      const int64_t m0 = J.m0 + wm * Cfg::WM, n0 = J.n0 + wn * Cfg::WN;
+      const bool vec = ((J.N & 1) == 0) && ((reinterpret_cast<uintptr_t>(J.C) & 15) == 0);
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int64_t row = m0 + i * 16 + g + 8 * h;
-          if (row >= p.M) continue;
+          if (row >= J.M) continue;
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             const int64_t col = n0 + j * 8 + 2 * tq;
             double v0 = acc[i][j][2 * h], v1 = acc[i][j][2 * h + 1];
-            double* cp = p.C + row * p.N + col;
-            if (vec && col + 1 < p.N) {
+            double* cp = J.C + row * J.N + col;
+            if (vec && col + 1 < J.N) {
               double2 o;
-              if (p.beta != 0.0) {
+              if (J.beta != 0.0) {
                 double2 c0 = *reinterpret_cast<const double2*>(cp);
-                o.x = fma(p.alpha, v0, p.beta * c0.x);
-                o.y = fma(p.alpha, v1, p.beta * c0.y);
+                o.x = fma(J.alpha, v0, J.beta * c0.x);
+                o.y = fma(J.alpha, v1, J.beta * c0.y);
               } else {
-                o.x = p.alpha * v0;
-                o.y = p.alpha * v1;
+                o.x = J.alpha * v0;
+                o.y = J.alpha * v1;
               }
               *reinterpret_cast<double2*>(cp) = o;
             } else {
-              if (col < p.N) cp[0] = (p.beta != 0.0) ? fma(p.alpha, v0, p.beta * cp[0]) : p.alpha * v0;
-              if (col + 1 < p.N) cp[1] = (p.beta != 0.0) ? fma(p.alpha, v1, p.beta * cp[1]) : p.alpha * v1;
+              if (col < J.N) cp[0] = (J.beta != 0.0) ? fma(J.alpha, v0, J.beta * cp[0]) : J.alpha * v0;
+              if (col + 1 < J.N) cp[1] = (J.beta != 0.0) ? fma(J.alpha, v1, J.beta * cp[1]) : J.alpha * v1;
             }
           }
         }
       }
     }
   }
+}
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS, 1)
+    dgemm_fp64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p) {
+  SingleSource<Cfg> src{p, (p.M + Cfg::BM - 1) / Cfg::BM, (p.N + Cfg::BN - 1) / Cfg::BN};
+  gemm_body<Cfg>(&tmA, &tmB, src, p.status);
+}
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS, 1)
+    dgemm_fp64_grouped_kernel(GroupedSource src, DeviceStatus* status) {
+  static_assert(!Cfg::kTMA, "grouped launches stage tiles with cp.async");
+  gemm_body<Cfg>(nullptr, nullptr, src, status);
 }
 
 }  // namespace fp64

@@ -1,0 +1,269 @@
+// grouped.cu — grouped/batched DGEMM plans: many independent, unevenly sized problems in one
+// persistent launch (FP64 form) or in one launch per stage (Ozaki form: grouped exponent and split
+// passes, then one persistent INT8 product launch over the tiles of every problem). A plan can be
+// replayed as a CUDA graph, and its FP64 tile shape can be chosen by the autotuner.
+//
+// No reference counterpart: the reference runs one problem per call (routines/dgemm/dgemm.cpp:178);
+// each problem here keeps that call's contract (row-major C = alpha A B + beta C, dgemm.h:9).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lt_internal.h"
+#include "lt_runtime.cuh"
+
+struct lt_grouped_plan {
+  int device = -1;
+  int form = LT_FORM_FP64;
+  int slices = 0;
+  int count = 0;
+  int fp64_cfg = 1;
+  std::vector<lt_gemm_problem> problems;
+  double flops = 0.0;
+  lt::fp64::GroupedFp64* fp = nullptr;
+  lt::ozaki::Grouped* oz = nullptr;
+  cudaStream_t capture_stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace lt {
+namespace {
+
+int check_problems(const lt_gemm_problem* problems, int count) {
+  if (problems == nullptr || count <= 0) return set_error(LT_ERR_INVALID_ARGUMENT, "empty problem list");
+  for (int i = 0; i < count; ++i) {
+    const lt_gemm_problem& p = problems[i];
+    if (p.M < 0 || p.N < 0 || p.K < 0 || p.M > 0x7fffffff || p.N > 0x7fffffff || p.K > 0x7fffffff)
+      return set_error(LT_ERR_INVALID_ARGUMENT, "problem %d: bad dimensions", i);
+    if ((p.M > 0 && p.K > 0 && p.A == nullptr) || (p.K > 0 && p.N > 0 && p.B == nullptr) ||
+        (p.M > 0 && p.N > 0 && p.C == nullptr))
+      return set_error(LT_ERR_INVALID_ARGUMENT, "problem %d: null matrix pointer", i);
+    if (((reinterpret_cast<uintptr_t>(p.A) | reinterpret_cast<uintptr_t>(p.B) | reinterpret_cast<uintptr_t>(p.C)) &
+         7) != 0)
+      return set_error(LT_ERR_UNALIGNED, "problem %d: pointers must be 8-byte aligned", i);
+  }
+  return LT_OK;
+}
+
+void drop_graph(lt_grouped_plan* plan) {
+  if (plan->exec) cudaGraphExecDestroy(plan->exec);
+  if (plan->graph) cudaGraphDestroy(plan->graph);
+  plan->exec = nullptr;
+  plan->graph = nullptr;
+}
+
+int build_fp64(lt_grouped_plan* plan, int cfg) {
+  fp64::GroupedFp64* g = nullptr;
+  LT_TRY(fp64::grouped_create(plan->problems.data(), plan->count, cfg, &g));
+  fp64::grouped_destroy(plan->fp);
+  plan->fp = g;
+  plan->fp64_cfg = cfg;
+  drop_graph(plan);
+  return LT_OK;
+}
+
+__global__ void max_rel_err_kernel(const double* C, const double* R, int64_t n, unsigned long long* out) {
+  double mx = 0.0;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double r = R[i], e = fabs(C[i] - r) / fmax(fabs(r), 1e-300);
+    if (!(e <= 1e300)) e = 1e300;
+    mx = fmax(mx, e);
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(mx)));
+}
+
+}  // namespace
+}  // namespace lt
+
+extern "C" {
+
+int lt_grouped_plan_create(const lt_gemm_problem* problems, int count, int form, int slices, lt_grouped_plan** plan) {
+  if (plan == nullptr) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "null plan pointer");
+  *plan = nullptr;
+  LT_TRY(lt::check_problems(problems, count));
+  if (form != LT_FORM_FP64 && form != LT_FORM_OZAKI) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "unknown form %d", form);
+  if (form == LT_FORM_OZAKI && (slices < 1 || slices > LT_OZAKI_MAX_SLICES))
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "slice count %d outside [1, %d]", slices, LT_OZAKI_MAX_SLICES);
+  lt::DeviceContext* ctx = lt::context();
+  if (ctx == nullptr) return lt::last_error();
+  auto* p = new lt_grouped_plan();
+  p->device = ctx->device;
+  p->form = form;
+  p->slices = slices;
+  p->count = count;
+  p->problems.assign(problems, problems + count);
+  for (const auto& q : p->problems)
+    p->flops += 2.0 * static_cast<double>(q.M) * static_cast<double>(q.N) * static_cast<double>(q.K);
+  int rc;
+  if (form == LT_FORM_FP64) {
+    // Without a tuning run: 64x64 tiles suit problems of a few hundred rows and columns.
+    rc = lt::build_fp64(p, 1);
+  } else {
+    rc = lt::ozaki::grouped_create(problems, count, slices, &p->oz);
+  }
+  if (rc != LT_OK) {
+    delete p;
+    return rc;
+  }
+  *plan = p;
+  return lt::ok();
+}
+
+int lt_grouped_plan_run(lt_grouped_plan* plan, void* stream) {
+  if (plan == nullptr) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "null plan");
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (dev != plan->device) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "plan belongs to device %d", plan->device);
+  if (plan->form == LT_FORM_FP64) {
+    LT_TRY(lt::fp64::grouped_run(plan->fp, lt::as_stream(stream)));
+  } else {
+    LT_TRY(lt::ozaki::grouped_run(plan->oz, lt::as_stream(stream)));
+  }
+  return lt::ok();
+}
+
+int lt_grouped_plan_run_graph(lt_grouped_plan* plan, void* stream) {
+  if (plan == nullptr) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "null plan");
+  if (plan->exec == nullptr) {
+    if (plan->capture_stream == nullptr)
+      LT_CUDA_TRY(cudaStreamCreateWithFlags(&plan->capture_stream, cudaStreamNonBlocking));
+    // The first launches set kernel attributes; do them outside the capture.
+    LT_TRY(lt_grouped_plan_run(plan, plan->capture_stream));
+    LT_CUDA_TRY(cudaStreamSynchronize(plan->capture_stream));
+    LT_CUDA_TRY(cudaStreamBeginCapture(plan->capture_stream, cudaStreamCaptureModeThreadLocal));
+    int rc = lt_grouped_plan_run(plan, plan->capture_stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(plan->capture_stream, &g);
+    if (rc != LT_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return lt::set_error(LT_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    plan->graph = g;
+    LT_CUDA_TRY(cudaGraphInstantiate(&plan->exec, plan->graph, 0));
+  }
+  LT_CUDA_TRY(cudaGraphLaunch(plan->exec, lt::as_stream(stream)));
+  return lt::ok();
+}
+
+int lt_grouped_plan_info(const lt_grouped_plan* plan, int64_t* tiles, double* flops) {
+  if (plan == nullptr) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "null plan");
+  if (tiles) *tiles = plan->form == LT_FORM_FP64 ? lt::fp64::grouped_tiles(plan->fp) : lt::ozaki::grouped_tiles(plan->oz);
+  if (flops) *flops = plan->flops;
+  return lt::ok();
+}
+
+void lt_grouped_plan_destroy(lt_grouped_plan* plan) {
+  if (plan == nullptr) return;
+  lt::drop_graph(plan);
+  if (plan->capture_stream) cudaStreamDestroy(plan->capture_stream);
+  lt::fp64::grouped_destroy(plan->fp);
+  lt::ozaki::grouped_destroy(plan->oz);
+  delete plan;
+}
+
+int lt_dgemm_grouped(const lt_gemm_problem* problems, int count, int form, int slices, void* stream) {
+  lt_grouped_plan* plan = nullptr;
+  LT_TRY(lt_grouped_plan_create(problems, count, form, slices, &plan));
+  int rc = lt_grouped_plan_run(plan, stream);
+  // The plan's tables must outlive the launch.
+  if (rc == LT_OK && cudaStreamSynchronize(lt::as_stream(stream)) != cudaSuccess)
+    rc = lt::set_error(LT_ERR_CUDA, "grouped run failed");
+  lt_grouped_plan_destroy(plan);
+  return rc == LT_OK ? lt::ok() : rc;
+}
+
+int lt_grouped_plan_config(const lt_grouped_plan* plan, char* name, int name_len) {
+  if (plan == nullptr || name == nullptr || name_len <= 0) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "bad arguments");
+  const char* n = plan->form == LT_FORM_FP64 ? lt::fp64::grouped_config_name(plan->fp64_cfg) : "ozaki_128x128";
+  snprintf(name, static_cast<size_t>(name_len), "%s", n);
+  return lt::ok();
+}
+
+// Autotuning of the FP64 tile shape for this problem set: every candidate runs on scratch outputs
+// (beta = 0), is validated against cuBLAS FP64 problem by problem, and the valid candidate with the
+// smallest median time over `iters` runs is kept. Synchronous; the plan's own C buffers are untouched.
+int lt_grouped_plan_tune(lt_grouped_plan* plan, int iters, float* best_ms) {
+  if (plan == nullptr || iters < 1) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "bad arguments");
+  if (plan->form != LT_FORM_FP64) return lt::ok();  // the Ozaki form has a single tile shape
+  lt::DeviceContext* ctx = lt::context();
+  if (ctx == nullptr) return lt::last_error();
+  size_t total = 0;
+  for (const auto& p : plan->problems) total += static_cast<size_t>(p.M * p.N);
+  double* scratch = nullptr;
+  unsigned long long* err = nullptr;
+  LT_CUDA_TRY(cudaMalloc(&scratch, sizeof(double) * (2 * total + 2)));
+  cudaError_t e = cudaMalloc(&err, sizeof(unsigned long long));
+  if (e != cudaSuccess) {
+    cudaFree(scratch);
+    return lt::set_error(LT_ERR_NO_MEMORY, "tuning scratch: %s", cudaGetErrorString(e));
+  }
+  std::vector<lt_gemm_problem> probs = plan->problems;
+  size_t off = 0;
+  for (auto& p : probs) {
+    p.C = scratch + off;
+    p.beta = 0.0;
+    off += static_cast<size_t>(p.M * p.N);
+  }
+  double* ref = scratch + total;
+  int rc = LT_OK;
+  off = 0;
+  for (const auto& p : probs) {
+    if (p.M > 0 && p.N > 0) rc = lt_dgemm_cublas(p.A, p.B, ref + off, p.M, p.N, p.K, p.alpha, 0.0, nullptr);
+    if (rc != LT_OK) break;
+    off += static_cast<size_t>(p.M * p.N);
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int best = -1;
+  float best_t = 0.f;
+  for (int cfg = 0; cfg < lt::fp64::grouped_num_configs() && rc == LT_OK; ++cfg) {
+    lt::fp64::GroupedFp64* g = nullptr;
+    if (lt::fp64::grouped_create(probs.data(), plan->count, cfg, &g) != LT_OK) continue;
+    bool valid = lt::fp64::grouped_run(g, nullptr) == LT_OK;
+    if (valid) {
+      cudaMemset(err, 0, sizeof(unsigned long long));
+      lt::max_rel_err_kernel<<<ctx->sm_count * 4, 256>>>(scratch, ref, static_cast<int64_t>(total), err);
+      unsigned long long bits = 0;
+      valid = cudaMemcpy(&bits, err, sizeof bits, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              lt_check_device_status() == LT_OK;
+      double v;
+      memcpy(&v, &bits, sizeof v);
+      valid = valid && v < 1e-8;
+    }
+    if (valid) {
+      std::vector<float> ts;
+      for (int it = 0; it < iters; ++it) {
+        cudaEventRecord(e0);
+        lt::fp64::grouped_run(g, nullptr);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ts.push_back(ms);
+      }
+      std::sort(ts.begin(), ts.end());
+      if (best < 0 || ts[ts.size() / 2] < best_t) {
+        best = cfg;
+        best_t = ts[ts.size() / 2];
+      }
+    }
+    lt::fp64::grouped_destroy(g);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(scratch);
+  cudaFree(err);
+  if (rc != LT_OK) return rc;
+  if (best < 0) return lt::set_error(LT_ERR_NOT_FOUND, "no grouped candidate validated");
+  LT_TRY(lt::build_fp64(plan, best));
+  if (best_ms) *best_ms = best_t;
+  return lt::ok();
+}
+
+}  // extern "C"

@@ -4,6 +4,8 @@
 
 #include <cstdint>
 
+#include "../../include/libthom_dgemm.h"
+
 namespace lt {
 
 int last_error();
@@ -32,6 +34,21 @@ int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double bet
             size_t workspace_bytes, cudaStream_t stream);
 int run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta,
         int slices, void* workspace, size_t workspace_bytes, cudaStream_t stream);
+struct Grouped;
+int grouped_create(const lt_gemm_problem* problems, int count, int slices, Grouped** out);
+int grouped_run(const Grouped* G, cudaStream_t stream);
+void grouped_destroy(Grouped* G);
+int64_t grouped_tiles(const Grouped* G);
 }  // namespace ozaki
+
+namespace fp64 {
+struct GroupedFp64;
+int grouped_num_configs();
+const char* grouped_config_name(int cfg);
+int grouped_create(const lt_gemm_problem* problems, int count, int cfg, GroupedFp64** out);
+int grouped_run(const GroupedFp64* G, cudaStream_t stream);
+void grouped_destroy(GroupedFp64* G);
+int64_t grouped_tiles(const GroupedFp64* G);
+}  // namespace fp64
 
 }  // namespace lt

@@ -5,11 +5,10 @@
 // with INT8 slices as in Ootomo, Ozaki and Yokota (2024); the code is written from the mathematics.
 //
 //   1. amax pass (HBM-bound): per row of A and per column of B, the largest |x| as IEEE bits
-//      (NaN/Inf order above every finite value, so one atomicMax finds both). sigma_i / tau_j are
-//      the frexp exponents of those maxima, so |A[i,k] 2^-sigma_i| < 1.
+//      (NaN/Inf order above every finite value, so one max finds both). sigma_i / tau_j are the
+//      frexp exponents of those maxima, so |A[i,k] 2^-sigma_i| < 1.
 //   2. split pass (HBM-bound): x = a 2^-sigma; for p = 1..s: y = 128 x, q_p = trunc(y), x = y - q_p.
-//      Every step is exact in FP64; q_p in [-127, 127] is stored as int8. A slices are laid out
-//      [s][M][Kp] and B slices [s][N][Kp] (B transposed to K-major), Kp = K rounded up to 32.
+//      Every step is exact in FP64; q_p in [-127, 127] is stored as int8.
 //   3. product pass (tensor cores): for the triangular pair set p + q <= s + 1, INT8 x INT8 -> INT32
 //      MMAs. Diagonals d = p + q share a power of two, so all pairs of a diagonal accumulate into one
 //      INT32 TMEM accumulator. Four diagonals ("a band") are live at once (4 x 128 TMEM columns),
@@ -22,9 +21,18 @@
 //      C = fma(alpha, acc 2^sigma_i 2^tau_j, beta C0).
 // The CPU oracle (oracle/oracle.c, oracle_ozaki_dgemm) performs the same arithmetic in the same
 // order, so results are bit-identical.
+//
+// Slice layout in HBM ("tiles"): every 128-row x 32-byte block of one slice — exactly one MMA
+// operand — is stored as a contiguous 4 KB tile, already in the 32-byte-swizzled K-major order the
+// tensor core reads from shared memory (16-byte half h of row r at r*32 + 16*(h ^ ((r >> 2) & 1))).
+// The producer moves each tile with one 1-D bulk copy (cp.async.bulk), so L2 serves whole lines.
+// Tile (p, rb, c) of an operand with RB row blocks and NC chunks sits at ((p*RB + rb)*NC + c)*4 KB;
+// rows beyond M (N) in the last block are zero.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "lt_internal.h"
 #include "lt_runtime.cuh"
@@ -38,29 +46,33 @@ constexpr int kChunk = 32;                       // K elements per MMA (= bytes 
 constexpr int kTileBytes = kTileM * kChunk;      // one 128 x 32 INT8 tile
 constexpr int kBand = 4;                         // live diagonal accumulators (4 x 128 TMEM cols)
 constexpr int kKPairLimit = 133144;              // floor((2^31 - 1) / 127^2)
-constexpr int kThreads = 320;                    // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
+constexpr int kThreads = 320;                    // warp 0 loads, warp 1 MMA, warps 2..9 epilogue
 constexpr int kEpilogueWarps = 8;
 constexpr int kMaxSmem = 232448;                 // sm_100 opt-in dynamic shared memory per block
+constexpr int kSmemOverhead = 1024 + 256;        // alignment slack + barriers
 constexpr int kSentinel = 0x7fffffff;            // exponent of a row/column holding NaN or Inf
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+inline int64_t ceil_div(int64_t x, int64_t m) { return (x + m - 1) / m; }
 
 // ---------------------------------------------------------------------------------------------
-// Workspace: [amaxA: M u64][amaxB: N u64][A slices: s*M*Kp][B slices: s*N*Kp], 256-byte aligned.
+// Workspace: [amaxA: M u64][amaxB: N u64][A tiles: s*RBa*NC*4K][B tiles: s*RBb*NC*4K], 256-aligned.
 // ---------------------------------------------------------------------------------------------
 struct Layout {
-  int64_t Kp;
+  int64_t NC, RBa, RBb;
   size_t off_amax_a, off_amax_b, off_sa, off_sb, total;
 };
 
 Layout layout_for(int64_t M, int64_t N, int64_t K, int s) {
   Layout L;
-  L.Kp = round_up(K > 0 ? K : 1, kChunk);
+  L.NC = ceil_div(K > 0 ? K : 1, kChunk);
+  L.RBa = ceil_div(M, kTileM);
+  L.RBb = ceil_div(N, kTileN);
   size_t o = 0;
   L.off_amax_a = o; o += round_up(8 * M, 256);
   L.off_amax_b = o; o += round_up(8 * N, 256);
-  L.off_sa = o;     o += round_up(static_cast<int64_t>(s) * M * L.Kp, 256);
-  L.off_sb = o;     o += round_up(static_cast<int64_t>(s) * N * L.Kp, 256);
+  L.off_sa = o;     o += static_cast<size_t>(s) * L.RBa * L.NC * kTileBytes;
+  L.off_sb = o;     o += static_cast<size_t>(s) * L.RBb * L.NC * kTileBytes;
   L.total = o;
   return L;
 }
@@ -68,7 +80,7 @@ Layout layout_for(int64_t M, int64_t N, int64_t K, int s) {
 size_t workspace_size(int64_t M, int64_t N, int64_t K, int slices) { return layout_for(M, N, K, slices).total; }
 
 // ---------------------------------------------------------------------------------------------
-// Exponent helpers
+// Exponents
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ int exponent_of_maxbits(unsigned long long bits) {
   if (bits == 0ull) return 0;
@@ -118,6 +130,9 @@ __global__ void amax_cols_kernel(const double* __restrict__ B, int64_t K, int64_
   if (m != 0) atomicMax(&amax[col], m);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Split
+// ---------------------------------------------------------------------------------------------
 // Splits one value into S slices q_1..q_S, OR-ing byte j of each into packed[p][j / 4].
 template <int S>
 __device__ __forceinline__ void split_value(double a, int e, int j, uint32_t (&packed)[S][8]) {
@@ -132,77 +147,143 @@ __device__ __forceinline__ void split_value(double a, int e, int j, uint32_t (&p
   }
 }
 
-// A rows -> slices [s][M][Kp]. Each thread: one row, 32 consecutive k (32 bytes per slice).
+// Writes row r (32 bytes per slice) of tile (rb, c) of every slice, in the swizzled tile order.
 template <int S>
-__global__ void split_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K, int64_t Kp,
-                                  const unsigned long long* __restrict__ amax, int8_t* __restrict__ out) {
-  const int64_t chunks = Kp / kChunk;
-  const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (idx >= M * chunks) return;
-  const int64_t row = idx / chunks, c = idx % chunks;
-  const int e = exponent_of_maxbits(amax[row]);
-  const int64_t k0 = c * kChunk;
-  const double* a = A + row * K;
-  uint32_t packed[S][8];
-#pragma unroll
-  for (int p = 0; p < S; ++p)
-#pragma unroll
-    for (int w = 0; w < 8; ++w) packed[p][w] = 0u;
-#pragma unroll
-  for (int j = 0; j < kChunk; ++j) {
-    const int64_t k = k0 + j;
-    const double v = (k < K) ? __ldg(a + k) : 0.0;
-    split_value<S>(v, e, j, packed);
-  }
+__device__ __forceinline__ void store_tile_row(int8_t* out, int64_t RB, int64_t NC, int64_t rb, int64_t c, int r,
+                                               const uint32_t (&packed)[S][8]) {
+  const int flip = (r >> 2) & 1;
 #pragma unroll
   for (int p = 0; p < S; ++p) {
-    uint4* dst = reinterpret_cast<uint4*>(out + (static_cast<int64_t>(p) * M + row) * Kp + k0);
-    dst[0] = make_uint4(packed[p][0], packed[p][1], packed[p][2], packed[p][3]);
-    dst[1] = make_uint4(packed[p][4], packed[p][5], packed[p][6], packed[p][7]);
+    int8_t* tile = out + ((static_cast<int64_t>(p) * RB + rb) * NC + c) * kTileBytes + r * 32;
+    uint4 lo = make_uint4(packed[p][0], packed[p][1], packed[p][2], packed[p][3]);
+    uint4 hi = make_uint4(packed[p][4], packed[p][5], packed[p][6], packed[p][7]);
+    reinterpret_cast<uint4*>(tile)[flip] = lo;
+    reinterpret_cast<uint4*>(tile)[flip ^ 1] = hi;
   }
 }
 
-// B columns -> slices [s][N][Kp] (K-major). Each thread: one column, 32 consecutive k; the loads
-// of a warp are 32 consecutive doubles of one row of B.
+// Tile (rb, c) of A: thread r handles row rb*128 + r, K elements 32c .. 32c + 31.
 template <int S>
-__global__ void split_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N, int64_t Kp,
-                                  const unsigned long long* __restrict__ amax, int8_t* __restrict__ out) {
-  const int64_t col = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (col >= N) return;
-  const int e = exponent_of_maxbits(amax[col]);
-  for (int64_t kc = blockIdx.y; kc < Kp / kChunk; kc += gridDim.y) {
-  const int64_t k0 = kc * kChunk;
+__device__ __forceinline__ void split_rows_tile(const double* __restrict__ A, int64_t M, int64_t K, int64_t NC,
+                                                int64_t RB, const unsigned long long* __restrict__ amax,
+                                                int8_t* __restrict__ out, int64_t rb, int64_t c, int r) {
+  const int64_t row = rb * kTileM + r;
   uint32_t packed[S][8];
 #pragma unroll
   for (int p = 0; p < S; ++p)
 #pragma unroll
     for (int w = 0; w < 8; ++w) packed[p][w] = 0u;
+  if (row < M) {
+    const int e = exponent_of_maxbits(amax[row]);
+    const double* a = A + row * K;
+    const int64_t k0 = c * kChunk;
 #pragma unroll
-  for (int j = 0; j < kChunk; ++j) {
-    const int64_t k = k0 + j;
-    const double v = (k < K) ? __ldg(B + k * N + col) : 0.0;
-    split_value<S>(v, e, j, packed);
+    for (int j = 0; j < kChunk; ++j) {
+      const int64_t k = k0 + j;
+      const double v = (k < K) ? __ldg(a + k) : 0.0;
+      split_value<S>(v, e, j, packed);
+    }
   }
+  store_tile_row<S>(out, RB, NC, rb, c, r, packed);
+}
+
+// Tile (rb, c) of B (transposed to K-major): thread r handles column rb*128 + r.
+template <int S>
+__device__ __forceinline__ void split_cols_tile(const double* __restrict__ B, int64_t K, int64_t N, int64_t NC,
+                                                int64_t RB, const unsigned long long* __restrict__ amax,
+                                                int8_t* __restrict__ out, int64_t rb, int64_t c, int r) {
+  const int64_t col = rb * kTileN + r;
+  uint32_t packed[S][8];
 #pragma unroll
-  for (int p = 0; p < S; ++p) {
-    uint4* dst = reinterpret_cast<uint4*>(out + (static_cast<int64_t>(p) * N + col) * Kp + k0);
-    dst[0] = make_uint4(packed[p][0], packed[p][1], packed[p][2], packed[p][3]);
-    dst[1] = make_uint4(packed[p][4], packed[p][5], packed[p][6], packed[p][7]);
+  for (int p = 0; p < S; ++p)
+#pragma unroll
+    for (int w = 0; w < 8; ++w) packed[p][w] = 0u;
+  if (col < N) {
+    const int e = exponent_of_maxbits(amax[col]);
+    const int64_t k0 = c * kChunk;
+#pragma unroll
+    for (int j = 0; j < kChunk; ++j) {
+      const int64_t k = k0 + j;
+      const double v = (k < K) ? __ldg(B + k * N + col) : 0.0;
+      split_value<S>(v, e, j, packed);
+    }
   }
-  }
+  store_tile_row<S>(out, RB, NC, rb, c, r, packed);
+}
+
+// One block (128 threads) per tile; tiles walked with a grid stride.
+template <int S>
+__global__ void __launch_bounds__(128) split_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K, int64_t NC,
+                                                         int64_t RB, const unsigned long long* __restrict__ amax,
+                                                         int8_t* __restrict__ out) {
+  for (int64_t t = blockIdx.x; t < RB * NC; t += gridDim.x)
+    split_rows_tile<S>(A, M, K, NC, RB, amax, out, t / NC, t % NC, threadIdx.x);
+}
+
+template <int S>
+__global__ void __launch_bounds__(128) split_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N, int64_t NC,
+                                                         int64_t RB, const unsigned long long* __restrict__ amax,
+                                                         int8_t* __restrict__ out) {
+  for (int64_t t = blockIdx.x; t < RB * NC; t += gridDim.x)
+    split_cols_tile<S>(B, K, N, NC, RB, amax, out, t / NC, t % NC, threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------------------------
 // Product + recombination kernel
 // ---------------------------------------------------------------------------------------------
+// Launch-wide parameters (the slice count is shared by every tile of a launch).
 struct GemmParams {
-  int64_t M, N, nkc;  // nkc = Kp / 32
   int s, stages, stage_tiles;
-  double alpha, beta;
+  DeviceStatus* status;
+};
+
+// One problem: its slice tiles, exponents, C and scalars.
+struct OzProblem {
+  const int8_t* sa;
+  const int8_t* sb;
   double* C;
   const unsigned long long* amax_a;
   const unsigned long long* amax_b;
-  DeviceStatus* status;
+  int64_t M, N, nkc, rba, rbb;
+  double alpha, beta;
+};
+
+// One output tile of one problem.
+struct OzJob {
+  const OzProblem* pr;
+  int m0, n0;
+};
+
+struct OzSingleSource {
+  const OzProblem* pr;
+  int64_t tiles_m, tiles_n;
+  __device__ int64_t count() const { return tiles_m * tiles_n; }
+  __device__ OzJob get(int64_t t) const {
+    const int64_t G = 8;
+    int64_t group = t / (G * tiles_n), first_m = group * G;
+    int64_t gsize = (tiles_m - first_m) < G ? (tiles_m - first_m) : G;
+    int64_t in_group = t - group * G * tiles_n;
+    const int64_t tm = first_m + in_group % gsize, tn = in_group / gsize;
+    return OzJob{pr, static_cast<int>(tm * kTileM), static_cast<int>(tn * kTileN)};
+  }
+};
+
+struct OzTile {
+  int problem;
+  int m0, n0;
+  int pad;
+};
+
+// Grouped launch: a device table of problems and a tile list sorted by decreasing K on the host.
+struct OzGroupedSource {
+  const OzProblem* problems;
+  const OzTile* tiles;
+  int64_t ntiles;
+  __device__ int64_t count() const { return ntiles; }
+  __device__ OzJob get(int64_t t) const {
+    const OzTile ot = tiles[t];
+    return OzJob{problems + ot.problem, ot.m0, ot.n0};
+  }
 };
 
 // Band b of s slices: diagonals dhi = s + 1 - 4b down to dlo; A/B slices 1..nsl are involved.
@@ -242,8 +323,15 @@ __device__ __forceinline__ uint64_t desc_k_sw32(uint32_t addr) {
   return d;
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
-    ozaki_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmParams p) {
+// Contiguous global -> shared bulk copy, completion counted in bytes on `bar`.
+__device__ __forceinline__ void bulk_load(void* smem_dst, const void* gsrc, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_u32(smem_dst)), "l"(reinterpret_cast<uint64_t>(gsrc)), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+template <class Source>
+__device__ __forceinline__ void ozaki_body(const Source& src, const GemmParams& p) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int stage_bytes = p.stage_tiles * kTileBytes;
@@ -256,8 +344,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t tiles_m = (p.M + kTileM - 1) / kTileM, tiles_n = (p.N + kTileN - 1) / kTileN;
-  const int64_t tiles = tiles_m * tiles_n;
+  const int64_t tiles = src.count();
   const int nb = num_bands(p.s);
 
   if (threadIdx.x == 0) {
@@ -281,28 +368,22 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem_base = *tmem_slot;
 
   if (warp == 0) {
-    // ----------------------------------- TMA producer -----------------------------------
+    // ---------------------------------- bulk-copy producer ----------------------------------
     if (lane == 0) {
-      tma_prefetch_desc(&tmA);
-      tma_prefetch_desc(&tmB);
       int stage = 0;
       uint32_t phase = 0;
       bool ok = true;
       for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-        int64_t tm, tn;
-        {
-          const int64_t G = 8;
-          int64_t group = t / (G * tiles_n), first_m = group * G;
-          int64_t gsize = (tiles_m - first_m) < G ? (tiles_m - first_m) : G;
-          int64_t in_group = t - group * G * tiles_n;
-          tm = first_m + in_group % gsize;
-          tn = in_group / gsize;
-        }
-        const int m0 = static_cast<int>(tm * kTileM), n0 = static_cast<int>(tn * kTileN);
+        const OzJob J = src.get(t);
+        const OzProblem& pr = *J.pr;
+        const int64_t nkc = pr.nkc;
+        const int8_t* a_blk = pr.sa + static_cast<int64_t>(J.m0 / kTileM) * nkc * kTileBytes;
+        const int8_t* b_blk = pr.sb + static_cast<int64_t>(J.n0 / kTileN) * nkc * kTileBytes;
+        const int64_t a_slice = pr.rba * nkc * kTileBytes, b_slice = pr.rbb * nkc * kTileBytes;
         for (int b = 0; b < nb && ok; ++b) {
           const Band bd = make_band(b, p.s, p.stage_tiles);
-          for (int64_t c0 = 0; c0 < p.nkc && ok; c0 += bd.gchunks) {
-            const int64_t c1 = (c0 + bd.gchunks < p.nkc) ? c0 + bd.gchunks : p.nkc;
+          for (int64_t c0 = 0; c0 < nkc && ok; c0 += bd.gchunks) {
+            const int64_t c1 = (c0 + bd.gchunks < nkc) ? c0 + bd.gchunks : nkc;
             for (int64_t cs = c0; cs < c1; cs += bd.cps) {
               const int64_t ce = (cs + bd.cps < c1) ? cs + bd.cps : c1;
               if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.status, 11)) { ok = false; break; }
@@ -310,10 +391,11 @@ __global__ void __launch_bounds__(kThreads, 1)
               mbar_arrive_expect_tx(&full[stage], static_cast<uint32_t>((ce - cs) * 2 * bd.nsl * kTileBytes));
               for (int64_t c = cs; c < ce; ++c) {
                 uint8_t* base = st + (c - cs) * 2 * bd.nsl * kTileBytes;
-                const int x = static_cast<int>(c * kChunk);
-                for (int q = 0; q < bd.nsl; ++q) tma_load_3d(base + q * kTileBytes, &tmA, &full[stage], x, m0, q);
                 for (int q = 0; q < bd.nsl; ++q)
-                  tma_load_3d(base + (bd.nsl + q) * kTileBytes, &tmB, &full[stage], x, n0, q);
+                  bulk_load(base + q * kTileBytes, a_blk + q * a_slice + c * kTileBytes, kTileBytes, &full[stage]);
+                for (int q = 0; q < bd.nsl; ++q)
+                  bulk_load(base + (bd.nsl + q) * kTileBytes, b_blk + q * b_slice + c * kTileBytes, kTileBytes,
+                            &full[stage]);
               }
               if (++stage == p.stages) { stage = 0; phase ^= 1; }
             }
@@ -331,10 +413,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint32_t group = 0;
     bool ok = true;
     for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+      const int64_t nkc = src.get(t).pr->nkc;
       for (int b = 0; b < nb && ok; ++b) {
         const Band bd = make_band(b, p.s, p.stage_tiles);
-        for (int64_t c0 = 0; c0 < p.nkc && ok; c0 += bd.gchunks) {
-          const int64_t c1 = (c0 + bd.gchunks < p.nkc) ? c0 + bd.gchunks : p.nkc;
+        for (int64_t c0 = 0; c0 < nkc && ok; c0 += bd.gchunks) {
+          const int64_t c1 = (c0 + bd.gchunks < nkc) ? c0 + bd.gchunks : nkc;
           if (!mbar_wait(acc_empty, (group & 1) ^ 1, abort_flag, p.status, 12)) { ok = false; break; }
           tc_fence_after();
           for (int64_t cs = c0; cs < c1; cs += bd.cps) {
@@ -387,21 +470,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint32_t group = 0;
     bool ok = true;
     for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-      int64_t tm, tn;
-      {
-        const int64_t G = 8;
-        int64_t grp = t / (G * tiles_n), first_m = grp * G;
-        int64_t gsize = (tiles_m - first_m) < G ? (tiles_m - first_m) : G;
-        int64_t in_group = t - grp * G * tiles_n;
-        tm = first_m + in_group % gsize;
-        tn = in_group / gsize;
-      }
+      const OzJob J = src.get(t);
+      const OzProblem& pr = *J.pr;
       double acc[64];
 #pragma unroll
       for (int i = 0; i < 64; ++i) acc[i] = 0.0;
       for (int b = 0; b < nb && ok; ++b) {
         const Band bd = make_band(b, p.s, p.stage_tiles);
-        for (int64_t c0 = 0; c0 < p.nkc; c0 += bd.gchunks) {
+        for (int64_t c0 = 0; c0 < pr.nkc; c0 += bd.gchunks) {
           if (!mbar_wait(acc_full, group & 1, abort_flag, p.status, 14)) { ok = false; break; }
           tc_fence_after();
           for (int j = 0; j < kBand; ++j) {
@@ -417,7 +493,8 @@ __global__ void __launch_bounds__(kThreads, 1)
               tmem_ld_wait();
 #pragma unroll
               for (int i = 0; i < 32; ++i)
-                acc[cc * 32 + i] = __dadd_rn(acc[cc * 32 + i], __dmul_rn(static_cast<double>(static_cast<int32_t>(v[i])), sc));
+                acc[cc * 32 + i] =
+                    __dadd_rn(acc[cc * 32 + i], __dmul_rn(static_cast<double>(static_cast<int32_t>(v[i])), sc));
             }
           }
           tc_fence_before();
@@ -428,22 +505,22 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       if (!ok) break;
       // ---- C = fma(alpha, acc 2^sigma 2^tau, beta C0) ----
-      const int64_t row = tm * kTileM + row_in_tile;
-      if (row < p.M) {
-        const int sig = exponent_of_maxbits(p.amax_a[row]);
-        const int64_t col0 = tn * kTileN + half * 64;
-        double* crow = p.C + row * p.N;
+      const int64_t row = J.m0 + row_in_tile;
+      if (row < pr.M) {
+        const int sig = exponent_of_maxbits(pr.amax_a[row]);
+        const int64_t col0 = J.n0 + half * 64;
+        double* crow = pr.C + row * pr.N;
 #pragma unroll
         for (int i = 0; i < 64; ++i) {
           const int64_t col = col0 + i;
-          if (col < p.N) {
-            const int tau = exponent_of_maxbits(p.amax_b[col]);
+          if (col < pr.N) {
+            const int tau = exponent_of_maxbits(pr.amax_b[col]);
             double out;
             if (sig == kSentinel || tau == kSentinel) {
               out = __longlong_as_double(0x7ff8000000000000ll);
             } else {
               const double tv = scale_pow2(scale_pow2(acc[i], sig), tau);
-              out = (p.beta != 0.0) ? fma(p.alpha, tv, __dmul_rn(p.beta, crow[col])) : __dmul_rn(p.alpha, tv);
+              out = (pr.beta != 0.0) ? fma(pr.alpha, tv, __dmul_rn(pr.beta, crow[col])) : __dmul_rn(pr.alpha, tv);
             }
             crow[col] = out;
           }
@@ -460,30 +537,39 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+__global__ void __maxnreg__(200) ozaki_gemm_kernel(OzProblem pr, GemmParams p) {
+  OzSingleSource src{&pr, (pr.M + kTileM - 1) / kTileM, (pr.N + kTileN - 1) / kTileN};
+  ozaki_body(src, p);
+}
+
+__global__ void __maxnreg__(200) ozaki_gemm_grouped_kernel(OzGroupedSource src, GemmParams p) {
+  ozaki_body(src, p);
+}
+
 // ---------------------------------------------------------------------------------------------
-// Host driver
+// Host driver (single problem)
 // ---------------------------------------------------------------------------------------------
 template <int S>
-int launch_split_s(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int64_t Kp,
+int launch_split_s(const double* A, const double* B, int64_t M, int64_t N, int64_t K, const Layout& L,
                    const unsigned long long* amax_a, const unsigned long long* amax_b, int8_t* sa, int8_t* sb,
-                   cudaStream_t stream) {
-  const int64_t chunks = Kp / kChunk;
-  const int64_t n = M * chunks;
-  if (n > 0) split_rows_kernel<S><<<static_cast<unsigned>((n + 127) / 128), 128, 0, stream>>>(A, M, K, Kp, amax_a, sa);
+                   int sms, cudaStream_t stream) {
+  const int64_t cap = static_cast<int64_t>(sms) * 64;
+  const int64_t ta = L.RBa * L.NC, tb = L.RBb * L.NC;
+  if (ta > 0) split_rows_kernel<S><<<static_cast<unsigned>(ta < cap ? ta : cap), 128, 0, stream>>>(A, M, K, L.NC, L.RBa,
+                                                                                                   amax_a, sa);
   LT_CUDA_TRY(cudaGetLastError());
-  if (N > 0)
-    split_cols_kernel<S><<<dim3(static_cast<unsigned>((N + 127) / 128), static_cast<unsigned>(chunks < 65535 ? chunks : 65535)), 128, 0, stream>>>(
-        B, K, N, Kp, amax_b, sb);
+  if (tb > 0) split_cols_kernel<S><<<static_cast<unsigned>(tb < cap ? tb : cap), 128, 0, stream>>>(B, K, N, L.NC, L.RBb,
+                                                                                                   amax_b, sb);
   LT_CUDA_TRY(cudaGetLastError());
   return LT_OK;
 }
 
-int launch_split(int s, const double* A, const double* B, int64_t M, int64_t N, int64_t K, int64_t Kp,
-                 const unsigned long long* amax_a, const unsigned long long* amax_b, int8_t* sa, int8_t* sb,
+int launch_split(int s, const double* A, const double* B, int64_t M, int64_t N, int64_t K, const Layout& L,
+                 const unsigned long long* amax_a, const unsigned long long* amax_b, int8_t* sa, int8_t* sb, int sms,
                  cudaStream_t stream) {
   switch (s) {
 #define LT_SPLIT_CASE(S) \
-  case S: return launch_split_s<S>(A, B, M, N, K, Kp, amax_a, amax_b, sa, sb, stream);
+  case S: return launch_split_s<S>(A, B, M, N, K, L, amax_a, amax_b, sa, sb, sms, stream);
     LT_SPLIT_CASE(1) LT_SPLIT_CASE(2) LT_SPLIT_CASE(3) LT_SPLIT_CASE(4) LT_SPLIT_CASE(5) LT_SPLIT_CASE(6)
     LT_SPLIT_CASE(7) LT_SPLIT_CASE(8) LT_SPLIT_CASE(9) LT_SPLIT_CASE(10) LT_SPLIT_CASE(11) LT_SPLIT_CASE(12)
 #undef LT_SPLIT_CASE
@@ -525,7 +611,30 @@ int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int
         B, K, N, kseg_b, amax_b);
     LT_CUDA_TRY(cudaGetLastError());
   }
-  LT_TRY(launch_split(s, A, B, M, N, K, L.Kp, amax_a, amax_b, sa, sb, stream));
+  return launch_split(s, A, B, M, N, K, L, amax_a, amax_b, sa, sb, sms, stream);
+}
+
+int gemm_params(int s, DeviceContext* ctx, GemmParams* gp) {
+  gp->s = s;
+  gp->stage_tiles = 2 * s;
+  const int stage_bytes = gp->stage_tiles * kTileBytes;
+  gp->stages = (kMaxSmem - kSmemOverhead) / stage_bytes;
+  if (gp->stages > 8) gp->stages = 8;
+  if (gp->stages < 2) return set_error(LT_ERR_UNSUPPORTED, "slice count %d needs more shared memory", s);
+  gp->status = ctx->status;
+  return LT_OK;
+}
+
+int set_gemm_smem(DeviceContext* ctx) {
+  static std::once_flag once[64];
+  static cudaError_t attr_err[64];
+  std::call_once(once[ctx->device], [&] {
+    attr_err[ctx->device] = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+    if (attr_err[ctx->device] == cudaSuccess)
+      attr_err[ctx->device] =
+          cudaFuncSetAttribute(ozaki_gemm_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+  });
+  LT_CUDA_TRY(attr_err[ctx->device]);
   return LT_OK;
 }
 
@@ -537,51 +646,26 @@ int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double bet
   const Layout L = layout_for(M, N, K, s);
   if (workspace_bytes < L.total) return set_error(LT_ERR_NO_MEMORY, "Ozaki workspace too small");
   const uint8_t* ws = static_cast<const uint8_t*>(workspace);
-  const auto* amax_a = reinterpret_cast<const unsigned long long*>(ws + L.off_amax_a);
-  const auto* amax_b = reinterpret_cast<const unsigned long long*>(ws + L.off_amax_b);
-  const auto* sa = reinterpret_cast<const int8_t*>(ws + L.off_sa);
-  const auto* sb = reinterpret_cast<const int8_t*>(ws + L.off_sb);
-  const int sms = ctx->sm_count;
-  const int64_t chunks = L.Kp / kChunk;
-
-  // Slices as 3-D tensors [s][rows][Kp] of bytes; one TMA box = 32 K x 128 rows of one slice.
-  CUtensorMap tmA, tmB;
-  LT_TRY(make_tmap_3d(&tmA, sa, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, static_cast<uint64_t>(s), static_cast<uint64_t>(M),
-                      static_cast<uint64_t>(L.Kp), static_cast<uint64_t>(L.Kp), static_cast<uint64_t>(M * L.Kp),
-                      kTileM, kChunk, CU_TENSOR_MAP_SWIZZLE_32B));
-  LT_TRY(make_tmap_3d(&tmB, sb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, static_cast<uint64_t>(s), static_cast<uint64_t>(N),
-                      static_cast<uint64_t>(L.Kp), static_cast<uint64_t>(L.Kp), static_cast<uint64_t>(N * L.Kp),
-                      kTileN, kChunk, CU_TENSOR_MAP_SWIZZLE_32B));
-
+  OzProblem pr;
+  pr.sa = reinterpret_cast<const int8_t*>(ws + L.off_sa);
+  pr.sb = reinterpret_cast<const int8_t*>(ws + L.off_sb);
+  pr.C = C;
+  pr.amax_a = reinterpret_cast<const unsigned long long*>(ws + L.off_amax_a);
+  pr.amax_b = reinterpret_cast<const unsigned long long*>(ws + L.off_amax_b);
+  pr.M = M;
+  pr.N = N;
+  pr.nkc = L.NC;
+  pr.rba = L.RBa;
+  pr.rbb = L.RBb;
+  pr.alpha = alpha;
+  pr.beta = beta;
   GemmParams gp;
-  gp.M = M;
-  gp.N = N;
-  gp.nkc = chunks;
-  gp.s = s;
-  gp.stage_tiles = 2 * s;
-  const int stage_bytes = gp.stage_tiles * kTileBytes;
-  const int overhead = 1024 + 256;
-  gp.stages = (kMaxSmem - overhead) / stage_bytes;
-  if (gp.stages > 6) gp.stages = 6;
-  if (gp.stages < 2) return set_error(LT_ERR_UNSUPPORTED, "slice count %d needs more shared memory", s);
-  gp.alpha = alpha;
-  gp.beta = beta;
-  gp.C = C;
-  gp.amax_a = amax_a;
-  gp.amax_b = amax_b;
-  gp.status = ctx->status;
-  const int smem = gp.stages * stage_bytes + overhead;
-
-  static std::once_flag once[64];
-  static cudaError_t attr_err[64];
-  std::call_once(once[ctx->device], [&] {
-    attr_err[ctx->device] =
-        cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-  });
-  LT_CUDA_TRY(attr_err[ctx->device]);
-  const int64_t tiles = ((M + kTileM - 1) / kTileM) * ((N + kTileN - 1) / kTileN);
-  const int64_t grid = tiles < sms ? tiles : sms;
-  ozaki_gemm_kernel<<<static_cast<unsigned>(grid), kThreads, smem, stream>>>(tmA, tmB, gp);
+  LT_TRY(gemm_params(s, ctx, &gp));
+  LT_TRY(set_gemm_smem(ctx));
+  const int smem = gp.stages * gp.stage_tiles * kTileBytes + kSmemOverhead;
+  const int64_t tiles = L.RBa * L.RBb;
+  const int64_t grid = tiles < ctx->sm_count ? tiles : ctx->sm_count;
+  ozaki_gemm_kernel<<<static_cast<unsigned>(grid), kThreads, smem, stream>>>(pr, gp);
   LT_CUDA_TRY(cudaGetLastError());
   return LT_OK;
 }
@@ -591,6 +675,232 @@ int run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64
   LT_TRY(split(A, B, M, N, K, s, workspace, workspace_bytes, stream));
   return product(C, M, N, K, alpha, beta, s, workspace, workspace_bytes, stream);
 }
+
+// ---------------------------------------------------------------------------------------------
+// Grouped form: many independent problems, one launch per stage.
+// Workspace: [amax of every problem (one contiguous region, zeroed by one memset)]
+//            [per problem: A tiles | B tiles].
+// Block tables map blockIdx.x to (problem, local block) through prefix sums searched on device.
+// ---------------------------------------------------------------------------------------------
+struct GSplit {
+  const double* A;
+  const double* B;
+  int64_t M, N, K, NC, RBa, RBb;
+  unsigned long long* amax_a;
+  unsigned long long* amax_b;
+  int8_t* sa;
+  int8_t* sb;
+};
+
+__device__ __forceinline__ int find_problem(const int* off, int count, int b) {
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= b) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// 8 rows (one warp each) per block.
+__global__ void g_amax_rows_kernel(const GSplit* __restrict__ P, const int* __restrict__ off, int count) {
+  const int pi = find_problem(off, count, blockIdx.x);
+  const GSplit g = P[pi];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t row = static_cast<int64_t>(blockIdx.x - off[pi]) * 8 + warp;
+  if (row >= g.M) return;
+  unsigned long long m = 0;
+  for (int64_t k = lane; k < g.K; k += 32) {
+    unsigned long long b = abs_bits(__ldg(g.A + row * g.K + k));
+    m = b > m ? b : m;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long x = __shfl_xor_sync(0xffffffffu, m, o);
+    m = x > m ? x : m;
+  }
+  if (lane == 0) g.amax_a[row] = m;
+}
+
+// 256 columns (one per thread) per block.
+__global__ void g_amax_cols_kernel(const GSplit* __restrict__ P, const int* __restrict__ off, int count) {
+  const int pi = find_problem(off, count, blockIdx.x);
+  const GSplit g = P[pi];
+  const int64_t col = static_cast<int64_t>(blockIdx.x - off[pi]) * 256 + threadIdx.x;
+  if (col >= g.N) return;
+  unsigned long long m = 0;
+  for (int64_t k = 0; k < g.K; ++k) {
+    unsigned long long b = abs_bits(__ldg(g.B + k * g.N + col));
+    m = b > m ? b : m;
+  }
+  g.amax_b[col] = m;
+}
+
+// One block (128 threads) per slice tile.
+template <int S>
+__global__ void __launch_bounds__(128) g_split_rows_kernel(const GSplit* __restrict__ P, const int* __restrict__ off,
+                                                           int count) {
+  const int pi = find_problem(off, count, blockIdx.x);
+  const GSplit& g = P[pi];
+  const int64_t t = blockIdx.x - off[pi];
+  split_rows_tile<S>(g.A, g.M, g.K, g.NC, g.RBa, g.amax_a, g.sa, t / g.NC, t % g.NC, threadIdx.x);
+}
+
+template <int S>
+__global__ void __launch_bounds__(128) g_split_cols_kernel(const GSplit* __restrict__ P, const int* __restrict__ off,
+                                                           int count) {
+  const int pi = find_problem(off, count, blockIdx.x);
+  const GSplit& g = P[pi];
+  const int64_t t = blockIdx.x - off[pi];
+  split_cols_tile<S>(g.B, g.K, g.N, g.NC, g.RBb, g.amax_b, g.sb, t / g.NC, t % g.NC, threadIdx.x);
+}
+
+struct Grouped {
+  int count = 0, s = 0;
+  void* dev = nullptr;   // tables (one allocation)
+  void* ws = nullptr;    // amax + slice tiles
+  size_t amax_bytes = 0;
+  GSplit* d_split = nullptr;
+  int* d_off = nullptr;  // 4 x (count + 1): amax rows, amax cols, split rows, split cols
+  int blocks[4] = {0, 0, 0, 0};
+  OzProblem* d_problems = nullptr;
+  OzTile* d_tiles = nullptr;
+  int64_t ntiles = 0;
+};
+
+template <int S>
+int g_split_launch(const Grouped& G, cudaStream_t stream) {
+  const int n = G.count;
+  if (G.blocks[2] > 0) g_split_rows_kernel<S><<<G.blocks[2], 128, 0, stream>>>(G.d_split, G.d_off + 2 * (n + 1), n);
+  if (G.blocks[3] > 0) g_split_cols_kernel<S><<<G.blocks[3], 128, 0, stream>>>(G.d_split, G.d_off + 3 * (n + 1), n);
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
+int grouped_create(const lt_gemm_problem* problems, int count, int s, Grouped** out) {
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  std::vector<Layout> lay(count);
+  std::vector<size_t> off_aa(count), off_ab(count), off_sa(count), off_sb(count);
+  size_t o = 0;
+  for (int i = 0; i < count; ++i) {
+    lay[i] = layout_for(problems[i].M, problems[i].N, problems[i].K, s);
+    off_aa[i] = o; o += round_up(8 * problems[i].M, 256);
+    off_ab[i] = o; o += round_up(8 * problems[i].N, 256);
+  }
+  const size_t amax_bytes = o;
+  for (int i = 0; i < count; ++i) {
+    off_sa[i] = o; o += static_cast<size_t>(s) * lay[i].RBa * lay[i].NC * kTileBytes;
+    off_sb[i] = o; o += static_cast<size_t>(s) * lay[i].RBb * lay[i].NC * kTileBytes;
+  }
+  // block counts must fit the int prefix tables
+  int64_t tot[4] = {0, 0, 0, 0};
+  for (int i = 0; i < count; ++i) {
+    const lt_gemm_problem& p = problems[i];
+    tot[0] += p.K > 0 ? (p.M + 7) / 8 : 0;
+    tot[1] += p.K > 0 ? (p.N + 255) / 256 : 0;
+    tot[2] += lay[i].RBa * lay[i].NC;
+    tot[3] += lay[i].RBb * lay[i].NC;
+  }
+  for (int k = 0; k < 4; ++k)
+    if (tot[k] > 0x7fffffff) return set_error(LT_ERR_INVALID_ARGUMENT, "grouped problem set too large");
+  auto* G = new Grouped();
+  G->count = count;
+  G->s = s;
+  G->amax_bytes = amax_bytes;
+  cudaError_t e = cudaMalloc(&G->ws, o > 0 ? o : 256);
+  if (e != cudaSuccess) {
+    delete G;
+    return set_error(LT_ERR_NO_MEMORY, "grouped Ozaki workspace (%zu bytes): %s", o, cudaGetErrorString(e));
+  }
+  uint8_t* ws = static_cast<uint8_t*>(G->ws);
+  std::vector<GSplit> split(count);
+  std::vector<int> offs(4 * (count + 1), 0);
+  std::vector<OzProblem> probs(count);
+  for (int i = 0; i < count; ++i) {
+    const lt_gemm_problem& p = problems[i];
+    const Layout& L = lay[i];
+    GSplit& g = split[i];
+    g = GSplit{p.A, p.B, p.M, p.N, p.K, L.NC, L.RBa, L.RBb,
+               reinterpret_cast<unsigned long long*>(ws + off_aa[i]), reinterpret_cast<unsigned long long*>(ws + off_ab[i]),
+               reinterpret_cast<int8_t*>(ws + off_sa[i]), reinterpret_cast<int8_t*>(ws + off_sb[i])};
+    const int64_t nb[4] = {p.K > 0 ? (p.M + 7) / 8 : 0, p.K > 0 ? (p.N + 255) / 256 : 0, L.RBa * L.NC, L.RBb * L.NC};
+    for (int k = 0; k < 4; ++k) offs[k * (count + 1) + i + 1] = offs[k * (count + 1) + i] + static_cast<int>(nb[k]);
+    probs[i] = OzProblem{g.sa, g.sb, p.C, g.amax_a, g.amax_b, p.M, p.N, L.NC, L.RBa, L.RBb, p.alpha, p.beta};
+    G->ntiles += L.RBa * L.RBb;
+  }
+  for (int k = 0; k < 4; ++k) G->blocks[k] = offs[k * (count + 1) + count];
+  // tiles of the longest-K problems first (a tile's cost is proportional to its problem's NC)
+  std::vector<int> order(count);
+  for (int i = 0; i < count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return lay[a].NC > lay[b].NC; });
+  std::vector<OzTile> tiles;
+  tiles.reserve(static_cast<size_t>(G->ntiles));
+  for (int i : order)
+    for (int64_t a = 0; a < lay[i].RBa; ++a)
+      for (int64_t b = 0; b < lay[i].RBb; ++b)
+        tiles.push_back(OzTile{i, static_cast<int>(a * kTileM), static_cast<int>(b * kTileN), 0});
+  const size_t split_bytes = round_up(sizeof(GSplit) * count, 256);
+  const size_t offs_bytes = round_up(sizeof(int) * offs.size(), 256);
+  const size_t prob_bytes = round_up(sizeof(OzProblem) * count, 256);
+  const size_t tile_bytes = round_up(sizeof(OzTile) * (tiles.size() + 1), 256);
+  e = cudaMalloc(&G->dev, split_bytes + offs_bytes + prob_bytes + tile_bytes);
+  if (e == cudaSuccess) {
+    uint8_t* d = static_cast<uint8_t*>(G->dev);
+    G->d_split = reinterpret_cast<GSplit*>(d);
+    G->d_off = reinterpret_cast<int*>(d + split_bytes);
+    G->d_problems = reinterpret_cast<OzProblem*>(d + split_bytes + offs_bytes);
+    G->d_tiles = reinterpret_cast<OzTile*>(d + split_bytes + offs_bytes + prob_bytes);
+    e = cudaMemcpy(G->d_split, split.data(), sizeof(GSplit) * count, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(G->d_off, offs.data(), sizeof(int) * offs.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(G->d_problems, probs.data(), sizeof(OzProblem) * count, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !tiles.empty())
+      e = cudaMemcpy(G->d_tiles, tiles.data(), sizeof(OzTile) * tiles.size(), cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    cudaFree(G->dev);
+    cudaFree(G->ws);
+    delete G;
+    return set_error(LT_ERR_NO_MEMORY, "grouped tables: %s", cudaGetErrorString(e));
+  }
+  *out = G;
+  return LT_OK;
+}
+
+int grouped_run(const Grouped* G, cudaStream_t stream) {
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  const int n = G->count;
+  LT_CUDA_TRY(cudaMemsetAsync(G->ws, 0, G->amax_bytes, stream));
+  if (G->blocks[0] > 0) g_amax_rows_kernel<<<G->blocks[0], 256, 0, stream>>>(G->d_split, G->d_off, n);
+  if (G->blocks[1] > 0) g_amax_cols_kernel<<<G->blocks[1], 256, 0, stream>>>(G->d_split, G->d_off + (n + 1), n);
+  LT_CUDA_TRY(cudaGetLastError());
+  switch (G->s) {
+#define LT_GSPLIT_CASE(S) \
+  case S: LT_TRY(g_split_launch<S>(*G, stream)); break;
+    LT_GSPLIT_CASE(1) LT_GSPLIT_CASE(2) LT_GSPLIT_CASE(3) LT_GSPLIT_CASE(4) LT_GSPLIT_CASE(5) LT_GSPLIT_CASE(6)
+    LT_GSPLIT_CASE(7) LT_GSPLIT_CASE(8) LT_GSPLIT_CASE(9) LT_GSPLIT_CASE(10) LT_GSPLIT_CASE(11) LT_GSPLIT_CASE(12)
+#undef LT_GSPLIT_CASE
+    default: return set_error(LT_ERR_INVALID_ARGUMENT, "slice count %d unsupported", G->s);
+  }
+  if (G->ntiles == 0) return LT_OK;
+  GemmParams gp;
+  LT_TRY(gemm_params(G->s, ctx, &gp));
+  LT_TRY(set_gemm_smem(ctx));
+  const int smem = gp.stages * gp.stage_tiles * kTileBytes + kSmemOverhead;
+  OzGroupedSource src{G->d_problems, G->d_tiles, G->ntiles};
+  const int64_t grid = G->ntiles < ctx->sm_count ? G->ntiles : ctx->sm_count;
+  ozaki_gemm_grouped_kernel<<<static_cast<unsigned>(grid), kThreads, smem, stream>>>(src, gp);
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
+void grouped_destroy(Grouped* G) {
+  if (G == nullptr) return;
+  cudaFree(G->dev);
+  cudaFree(G->ws);
+  delete G;
+}
+
+int64_t grouped_tiles(const Grouped* G) { return G->ntiles; }
 
 }  // namespace ozaki
 }  // namespace lt

@@ -1,0 +1,121 @@
+"""GPU parity of the grouped/batched DGEMM plans (one persistent launch for many uneven problems).
+
+Each problem keeps the reference's contract (routines/dgemm/dgemm.h:9). FP64 form: componentwise
+error within (K + 4) u against the compensated oracle. Ozaki form: bit-identical to the CPU
+restatement problem by problem. CUDA-graph replay must reproduce the direct launch bit for bit.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import fp64_bound, to_dev
+
+pytestmark = pytest.mark.gpu
+
+
+def make_set(oracle_mod, count, lo, hi, seed):
+    rng = np.random.default_rng(seed)
+    dims = np.rint(np.exp(rng.uniform(np.log(lo), np.log(hi), size=(count, 3)))).astype(int)
+    probs = []
+    for i, (M, N, K) in enumerate(dims):
+        A, B, C0 = oracle_mod.make_problem(int(M), int(N), int(K), phi=2, seed=seed * 1000 + i)
+        probs.append((A, B, C0, 1.5 if i % 2 else 1.0, 0.5 if i % 3 else 0.0))
+    return probs
+
+
+def upload(torch, probs):
+    import libthom_b200 as lt
+
+    dev = []
+    table = (lt.GemmProblem * len(probs))()
+    for i, (A, B, C0, alpha, beta) in enumerate(probs):
+        dA, dB, dC = to_dev(torch, A), to_dev(torch, B), to_dev(torch, C0)
+        dev.append((dA, dB, dC))
+        table[i] = lt.GemmProblem(A.shape[0], B.shape[1], A.shape[1], dA.data_ptr(), dB.data_ptr(), dC.data_ptr(),
+                                  alpha, beta)
+    return dev, table
+
+
+def plan_run(torch, table, n, form, slices, graph=False, tune=False):
+    import libthom_b200 as lt
+
+    L = lt.lib()
+    plan = ctypes.c_void_p()
+    lt.check(L.lt_grouped_plan_create(table, n, form, slices, ctypes.byref(plan)))
+    try:
+        if tune:
+            ms = ctypes.c_float()
+            lt.check(L.lt_grouped_plan_tune(plan, 3, ctypes.byref(ms)))
+        if graph:
+            lt.check(L.lt_grouped_plan_run_graph(plan, None))
+        else:
+            lt.check(L.lt_grouped_plan_run(plan, None))
+        torch.cuda.synchronize()
+        lt.device_status()
+        tiles = ctypes.c_int64()
+        flops = ctypes.c_double()
+        lt.check(L.lt_grouped_plan_info(plan, ctypes.byref(tiles), ctypes.byref(flops)))
+        return tiles.value, flops.value
+    finally:
+        L.lt_grouped_plan_destroy(plan)
+
+
+@pytest.mark.parametrize("graph,tune", [(False, False), (True, False), (False, True)])
+def test_grouped_fp64(cuda, oracle_mod, graph, tune):
+    import libthom_b200 as lt
+
+    probs = make_set(oracle_mod, 24, 8, 300, seed=5)
+    dev, table = upload(cuda, probs)
+    _, flops = plan_run(cuda, table, len(probs), lt.LT_FORM_FP64, 0, graph=graph, tune=tune)
+    assert flops == pytest.approx(sum(2.0 * A.shape[0] * A.shape[1] * B.shape[1] for A, B, *_ in probs))
+    for (A, B, C0, alpha, beta), (_, _, dC) in zip(probs, dev):
+        Cref, den = oracle_mod.dot2_rows(A, B, C0, alpha, beta)
+        err = oracle_mod.componentwise_error(dC.cpu().numpy(), Cref, den)
+        assert err[0] <= fp64_bound(A.shape[1]), (A.shape, B.shape, err)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_grouped_ozaki_bit_exact(cuda, oracle_mod, graph):
+    import libthom_b200 as lt
+
+    probs = make_set(oracle_mod, 16, 16, 300, seed=9)
+    dev, table = upload(cuda, probs)
+    plan_run(cuda, table, len(probs), lt.LT_FORM_OZAKI, 7, graph=graph)
+    for (A, B, C0, alpha, beta), (_, _, dC) in zip(probs, dev):
+        R = oracle_mod.ozaki_dgemm(A, B, C0, alpha, beta, 7)
+        assert np.array_equal(dC.cpu().numpy(), R), (A.shape, B.shape)
+
+
+def test_graph_replay_matches_direct(cuda, oracle_mod):
+    import libthom_b200 as lt
+
+    torch = cuda
+    L = lt.lib()
+    probs = make_set(oracle_mod, 12, 32, 200, seed=3)
+    for form, s in ((lt.LT_FORM_FP64, 0), (lt.LT_FORM_OZAKI, 8)):
+        dev, table = upload(torch, [(A, B, C0, 1.0, 0.0) for A, B, C0, *_ in probs])
+        plan = ctypes.c_void_p()
+        lt.check(L.lt_grouped_plan_create(table, len(probs), form, s, ctypes.byref(plan)))
+        lt.check(L.lt_grouped_plan_run(plan, None))
+        torch.cuda.synchronize()
+        first = [d[2].clone() for d in dev]
+        for _ in range(3):
+            lt.check(L.lt_grouped_plan_run_graph(plan, None))
+        torch.cuda.synchronize()
+        L.lt_grouped_plan_destroy(plan)
+        for a, (_, _, c) in zip(first, dev):
+            assert torch.equal(a, c)
+
+
+def test_grouped_rejects_bad_problems(cuda):
+    import libthom_b200 as lt
+
+    L = lt.lib()
+    table = (lt.GemmProblem * 1)()
+    table[0] = lt.GemmProblem(4, 4, 4, None, None, None, 1.0, 0.0)
+    plan = ctypes.c_void_p()
+    assert L.lt_grouped_plan_create(table, 1, lt.LT_FORM_FP64, 0, ctypes.byref(plan)) == lt.LT_ERR_INVALID_ARGUMENT
+    assert L.lt_grouped_plan_create(table, 0, lt.LT_FORM_FP64, 0, ctypes.byref(plan)) == lt.LT_ERR_INVALID_ARGUMENT
