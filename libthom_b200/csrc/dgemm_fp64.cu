@@ -105,7 +105,7 @@ namespace {
 
 template <class Cfg>
 int launch_grouped(const GroupProblem* problems, const GroupTile* tiles, int64_t ntiles, cudaStream_t stream,
-                   DeviceContext* ctx) {
+                   DeviceContext* ctx, bool setup_only) {
   static std::once_flag once[64];
   static int occupancy[64];
   static cudaError_t attr_err[64];
@@ -121,7 +121,7 @@ int launch_grouped(const GroupProblem* problems, const GroupTile* tiles, int64_t
   LT_CUDA_TRY(attr_err[ctx->device]);
   int64_t grid = static_cast<int64_t>(ctx->sm_count) * occupancy[ctx->device];
   if (grid > ntiles) grid = ntiles;
-  if (grid < 1) return LT_OK;
+  if (grid < 1 || setup_only) return LT_OK;
   GroupedSource src{problems, tiles, ntiles};
   dgemm_fp64_grouped_kernel<Cfg><<<static_cast<unsigned>(grid), Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(src,
                                                                                                          ctx->status);
@@ -129,7 +129,7 @@ int launch_grouped(const GroupProblem* problems, const GroupTile* tiles, int64_t
   return LT_OK;
 }
 
-using GroupedFn = int (*)(const GroupProblem*, const GroupTile*, int64_t, cudaStream_t, DeviceContext*);
+using GroupedFn = int (*)(const GroupProblem*, const GroupTile*, int64_t, cudaStream_t, DeviceContext*, bool);
 struct GroupedEntry {
   const char* name;
   GroupedFn fn;
@@ -199,7 +199,14 @@ int grouped_create(const lt_gemm_problem* problems, int count, int cfg, GroupedF
 int grouped_run(const GroupedFp64* G, cudaStream_t stream) {
   DeviceContext* ctx = context();
   if (ctx == nullptr) return last_error();
-  return kGrouped[G->cfg].fn(G->d_problems, G->d_tiles, G->ntiles, stream, ctx);
+  return kGrouped[G->cfg].fn(G->d_problems, G->d_tiles, G->ntiles, stream, ctx, false);
+}
+
+// Kernel attribute set-up only (before a stream capture, which must not contain it).
+int grouped_prepare(const GroupedFp64* G) {
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  return kGrouped[G->cfg].fn(G->d_problems, G->d_tiles, G->ntiles, nullptr, ctx, true);
 }
 
 void grouped_destroy(GroupedFp64* G) {

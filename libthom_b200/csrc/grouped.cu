@@ -131,9 +131,12 @@ int lt_grouped_plan_run_graph(lt_grouped_plan* plan, void* stream) {
   if (plan->exec == nullptr) {
     if (plan->capture_stream == nullptr)
       LT_CUDA_TRY(cudaStreamCreateWithFlags(&plan->capture_stream, cudaStreamNonBlocking));
-    // The first launches set kernel attributes; do them outside the capture.
-    LT_TRY(lt_grouped_plan_run(plan, plan->capture_stream));
-    LT_CUDA_TRY(cudaStreamSynchronize(plan->capture_stream));
+    // Kernel attributes are set outside the capture (no launch: C must be written once per replay).
+    if (plan->form == LT_FORM_FP64) {
+      LT_TRY(lt::fp64::grouped_prepare(plan->fp));
+    } else {
+      LT_TRY(lt::ozaki::grouped_prepare());
+    }
     LT_CUDA_TRY(cudaStreamBeginCapture(plan->capture_stream, cudaStreamCaptureModeThreadLocal));
     int rc = lt_grouped_plan_run(plan, plan->capture_stream);
     cudaGraph_t g = nullptr;

@@ -37,6 +37,7 @@ int run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64
 struct Grouped;
 int grouped_create(const lt_gemm_problem* problems, int count, int slices, Grouped** out);
 int grouped_run(const Grouped* G, cudaStream_t stream);
+int grouped_prepare();
 void grouped_destroy(Grouped* G);
 int64_t grouped_tiles(const Grouped* G);
 }  // namespace ozaki
@@ -47,6 +48,7 @@ int grouped_num_configs();
 const char* grouped_config_name(int cfg);
 int grouped_create(const lt_gemm_problem* problems, int count, int cfg, GroupedFp64** out);
 int grouped_run(const GroupedFp64* G, cudaStream_t stream);
+int grouped_prepare(const GroupedFp64* G);
 void grouped_destroy(GroupedFp64* G);
 int64_t grouped_tiles(const GroupedFp64* G);
 }  // namespace fp64

@@ -893,6 +893,12 @@ int grouped_run(const Grouped* G, cudaStream_t stream) {
   return LT_OK;
 }
 
+int grouped_prepare() {
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  return set_gemm_smem(ctx);
+}
+
 void grouped_destroy(Grouped* G) {
   if (G == nullptr) return;
   cudaFree(G->dev);

@@ -10,9 +10,14 @@
 // softmax over slice counts 3..10, cross-entropy loss, Adam. Forward, backward and the optimizer
 // step are hand-written kernels: one block per sample for forward/backward (per-sample gradients
 // written to a buffer), then a fixed-order reduction over the batch, so gradients are deterministic.
+#include <dlfcn.h>
+
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "lt_internal.h"
@@ -365,9 +370,45 @@ int decide(const float* probs, int s_analytic, bool* learned) {
   return s_analytic;
 }
 
+// Trained weights shipped beside the library (selector_weights.bin, LT_SEL_PARAMS floats), or the
+// file named by LIBTHOM_SELECTOR_WEIGHTS; loaded once unless the caller installed weights (or
+// explicitly none) with lt_selector_set_params.
+bool g_params_explicit = false;
+std::once_flag g_default_once;
+
+void load_default_params() {
+  std::call_once(g_default_once, [] {
+    std::string path;
+    if (const char* env = getenv("LIBTHOM_SELECTOR_WEIGHTS")) {
+      path = env;
+    } else {
+      Dl_info info;
+      if (dladdr(reinterpret_cast<void*>(&load_default_params), &info) != 0 && info.dli_fname != nullptr) {
+        path = info.dli_fname;
+        size_t slash = path.find_last_of('/');
+        path = (slash == std::string::npos ? std::string(".") : path.substr(0, slash)) + "/selector_weights.bin";
+      }
+    }
+    if (path.empty()) return;
+    FILE* f = fopen(path.c_str(), "rb");
+    if (f == nullptr) return;
+    std::vector<float> w(P);
+    size_t n = fread(w.data(), sizeof(float), P, f);
+    char extra;
+    bool exact = n == static_cast<size_t>(P) && fread(&extra, 1, 1, f) == 0;
+    fclose(f);
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (exact && !g_params_explicit) {
+      g_host_params = w;
+      for (int d = 0; d < 64; ++d) g_dev_params_valid[d] = false;
+    }
+  });
+}
+
 int device_params(const float** out) {
   int dev = 0;
   LT_CUDA_TRY(cudaGetDevice(&dev));
+  load_default_params();
   std::lock_guard<std::mutex> lock(g_mutex);
   if (g_host_params.empty()) {
     *out = nullptr;
@@ -480,6 +521,7 @@ int lt_mlp_train_step(float* params, float* m, float* v, float* grads, const flo
 
 int lt_selector_set_params(const float* host_params) {
   std::lock_guard<std::mutex> lock(lt::sel::g_mutex);
+  lt::sel::g_params_explicit = true;
   if (host_params == nullptr) {
     lt::sel::g_host_params.clear();
   } else {

@@ -14,7 +14,7 @@ using RoutineHandler = void (*)(RunMode, int, char**);
 // (grouped/batched DGEMM, one persistent launch for many uneven problems).
 static const std::unordered_map<std::string, RoutineHandler> routinesMap = {
     {"dgemm", dgemm_handler},
-
+    {"dgemmb", dgemmb_handler},
 };
 
 int main(int argc, char* argv[]) {

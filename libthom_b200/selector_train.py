@@ -1,0 +1,297 @@
+"""Trains and evaluates the learned Ozaki slice-count selector on the GPU.
+
+Data: seeded matrices with shapes from the library's three DGEMM families, capped at 2048 per
+dimension — square (M = N = K), tall-skinny (large M, small N) and long-K — with exponent spread
+phi ~ U{0..64} and, for the last two families, rows of A / columns of B scaled by 2^s with
+s ~ U{-smax..smax}. Each matrix is run through the Ozaki kernels at s = 3..10; its componentwise
+error max |C_s - C_64| / (|alpha||A||B|) against the native FP64 result C_64 labels it, for each
+tolerance in {1e-12, 1e-14, 1e-15}, with the smallest s meeting the tolerance (class s - 3; 7 when
+none does). Features come from lt_ozaki_features; training runs lt_mlp_train_step (hand-written
+forward, backward and Adam kernels). The held-out set reports the tolerance-miss rate of the
+learned choice (with and without the analytic fallback), the mean slices saved against the
+analytic count and end-to-end throughput against fixed-slice Ozaki and native FP64.
+
+    python -m libthom_b200.selector_train [--train 20000] [--test 2000] [--out PATH]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import time
+from pathlib import Path
+
+import numpy as np
+
+import libthom_b200 as lt
+
+TOLS = (1e-12, 1e-14, 1e-15)
+SLICES = list(range(3, 11))
+WEIGHTS = Path(__file__).resolve().parent / "selector_weights.bin"
+
+
+def draw_shape(rng):
+    fam = int(rng.integers(0, 3))
+    lu = lambda lo, hi: int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+    if fam == 0:
+        n = lu(64, 2048)
+        M = N = K = n
+        smax = 0
+    elif fam == 1:
+        M, N, K = lu(256, 2048), lu(16, 128), lu(256, 2048)
+        smax = int(rng.integers(0, 65))
+    else:
+        M = N = lu(64, 512)
+        K = lu(1024, 2048)
+        smax = int(rng.integers(0, 65))
+    return fam, M, N, K, int(rng.integers(0, 65)), smax, int(rng.integers(1, 2**62))
+
+
+class Generator:
+    """Device buffers reused across problems (sized for the largest shape)."""
+
+    def __init__(self, torch, cap=2048):
+        self.torch = torch
+        n2 = cap * cap
+        f = dict(dtype=torch.float64, device="cuda")
+        self.A = torch.empty(n2, **f)
+        self.B = torch.empty(n2, **f)
+        self.C64 = torch.empty(n2, **f)
+        self.C = torch.empty(n2, **f)
+        self.den = torch.empty(n2, **f)
+        self.feat = torch.empty(lt.LT_SEL_FEATURES, dtype=torch.float32, device="cuda")
+
+    def problem(self, M, N, K, phi, smax, seed):
+        L = lt.lib()
+        lt.check(L.lt_fill(self.A.data_ptr(), M * K, seed, 1, phi, None))
+        lt.check(L.lt_fill(self.B.data_ptr(), K * N, seed, 2, phi, None))
+        if smax > 0:
+            lt.check(L.lt_scale_rows(self.A.data_ptr(), M, K, seed, 4, smax, None))
+            lt.check(L.lt_scale_cols(self.B.data_ptr(), K, N, seed, 5, smax, None))
+
+    def errors(self, M, N, K):
+        """Componentwise error of the Ozaki result for every s in SLICES against the FP64 result."""
+        L = lt.lib()
+        A, B = self.A.data_ptr(), self.B.data_ptr()
+        lt.check(L.lt_dgemm_fp64(A, B, self.C64.data_ptr(), M, N, K, 1.0, 0.0, None))
+        lt.check(L.lt_abs_denominator(A, B, None, self.den.data_ptr(), M, N, K, 1.0, 0.0, None))
+        out = []
+        for s in SLICES:
+            lt.check(L.lt_dgemm_ozaki(A, B, self.C.data_ptr(), M, N, K, 1.0, 0.0, s, None))
+            e, _ = lt.componentwise_error(self.C, self.C64, self.den, M * N)
+            out.append(e)
+        return out
+
+    def features(self, M, N, K):
+        lt.check(lt.lib().lt_ozaki_features(self.A.data_ptr(), self.B.data_ptr(), M, N, K, 1.0,
+                                            self.feat.data_ptr(), None))
+        return self.feat.cpu().numpy().copy()
+
+    def analytic(self, M, N, K, tol):
+        s = ctypes.c_int()
+        learned = ctypes.c_int()
+        gap = ctypes.c_int()
+        lt.check(lt.lib().lt_ozaki_select_info(self.A.data_ptr(), self.B.data_ptr(), M, N, K, tol, ctypes.byref(s),
+                                               ctypes.byref(learned), ctypes.byref(gap), None))
+        return s.value, gap.value
+
+
+def label_of(errs, tol):
+    for s, e in zip(SLICES, errs):
+        if e <= tol:
+            return s - 3
+    return len(SLICES) - 1
+
+
+def build_dataset(torch, gen, n, seed, log_every=0):
+    rng = np.random.default_rng(seed)
+    rows = []
+    t0 = time.time()
+    for i in range(n):
+        fam, M, N, K, phi, smax, pseed = draw_shape(rng)
+        gen.problem(M, N, K, phi, smax, pseed)
+        errs = gen.errors(M, N, K)
+        f = gen.features(M, N, K)
+        rows.append(dict(fam=fam, M=M, N=N, K=K, phi=phi, smax=smax, seed=pseed, errs=errs, feat=f))
+        if log_every and (i + 1) % log_every == 0:
+            print(f"  {i + 1}/{n} problems ({time.time() - t0:.0f} s)", flush=True)
+    return rows
+
+
+def expand(rows):
+    X, Y = [], []
+    for r in rows:
+        for tol in TOLS:
+            f = r["feat"].copy()
+            f[33] = np.float32(-math.log10(tol) / 16.0)
+            X.append(f)
+            Y.append(label_of(r["errs"], tol))
+    return np.stack(X).astype(np.float32), np.array(Y, dtype=np.int32)
+
+
+def init_params(seed):
+    rng = np.random.default_rng(seed)
+    F, H, C = lt.LT_SEL_FEATURES, lt.LT_SEL_HIDDEN, lt.LT_SEL_CLASSES
+    parts = [rng.standard_normal(H * F) * math.sqrt(2.0 / F), np.zeros(H),
+             rng.standard_normal(H * H) * math.sqrt(2.0 / H), np.zeros(H),
+             rng.standard_normal(C * H) * math.sqrt(1.0 / H), np.zeros(C)]
+    return np.concatenate(parts).astype(np.float32)
+
+
+def train(torch, X, Y, epochs=40, batch=256, lr=2e-3, seed=0):
+    L = lt.lib()
+    dev = dict(device="cuda")
+    params = torch.from_numpy(init_params(seed)).to(**dev)
+    m = torch.zeros_like(params)
+    v = torch.zeros_like(params)
+    g = torch.zeros_like(params)
+    loss = torch.zeros(1, dtype=torch.float32, **dev)
+    Xd = torch.from_numpy(X).to(**dev)
+    Yd = torch.from_numpy(Y).to(**dev)
+    rng = np.random.default_rng(seed)
+    step = 0
+    hist = []
+    for ep in range(epochs):
+        perm = torch.from_numpy(rng.permutation(len(Y))).to(**dev)
+        tot = 0.0
+        nb = 0
+        for b0 in range(0, len(Y) - batch + 1, batch):
+            idx = perm[b0:b0 + batch]
+            xb = Xd[idx].contiguous()
+            yb = Yd[idx].contiguous()
+            step += 1
+            lt.check(L.lt_mlp_train_step(params.data_ptr(), m.data_ptr(), v.data_ptr(), g.data_ptr(), xb.data_ptr(),
+                                         yb.data_ptr(), batch, lr, step, loss.data_ptr(), None))
+            tot += float(loss.item()) if (nb % 20 == 0) else 0.0
+            nb += 1
+        hist.append(tot / max(1, (nb + 19) // 20))
+    return params.cpu().numpy(), hist
+
+
+def predict(torch, params, X):
+    L = lt.lib()
+    p = torch.from_numpy(params).cuda()
+    x = torch.from_numpy(X).cuda()
+    out = torch.empty(len(X), lt.LT_SEL_CLASSES, dtype=torch.float32, device="cuda")
+    lt.check(L.lt_mlp_forward(p.data_ptr(), x.data_ptr(), len(X), out.data_ptr(), None))
+    return out.cpu().numpy()
+
+
+def decide(probs, s_analytic):
+    """The library's rule (selector.cu, decide): CDF >= 0.9 if the top class has >= 0.5, clamped to
+    the analytic count; analytic otherwise. Returns (slices, learned?)."""
+    if probs.max() < 0.5:
+        return s_analytic, False
+    cdf = np.cumsum(probs)
+    c = int(np.argmax(cdf >= 0.9))
+    s = 3 + c
+    if s > s_analytic:
+        return s_analytic, False
+    return s, True
+
+
+def evaluate(torch, gen, params, rows):
+    X, Y = expand(rows)
+    P = predict(torch, params, X)
+    out = dict(samples=len(Y))
+    miss_learned = miss_final = 0
+    saved = []
+    used_learned = 0
+    per_tol = {}
+    k = 0
+    chosen = []
+    for r in rows:
+        gen.problem(r["M"], r["N"], r["K"], r["phi"], r["smax"], r["seed"])
+        for tol in TOLS:
+            s_a, _ = gen.analytic(r["M"], r["N"], r["K"], tol)
+            s_raw = 3 + int(np.argmax(np.cumsum(P[k]) >= 0.9))
+            s_final, learned = decide(P[k], s_a)
+            err = lambda s: r["errs"][s - 3] if 3 <= s <= 10 else (0.0 if s > 10 else float("inf"))
+            miss_learned += err(s_raw) > tol
+            miss_final += err(s_final) > tol
+            used_learned += learned
+            saved.append(s_a - s_final)
+            d = per_tol.setdefault(tol, dict(n=0, miss=0, saved=0.0, analytic=0.0, chosen=0.0))
+            d["n"] += 1
+            d["miss"] += err(s_final) > tol
+            d["saved"] += s_a - s_final
+            d["analytic"] += s_a
+            d["chosen"] += s_final
+            chosen.append((r, tol, s_final, s_a))
+            k += 1
+    n = len(Y)
+    out.update(miss_rate_learned_only=miss_learned / n, miss_rate_with_fallback=miss_final / n,
+               learned_used_fraction=used_learned / n, mean_slices_saved_vs_analytic=float(np.mean(saved)),
+               accuracy_top1=float(np.mean(np.argmax(P, axis=1) == Y)),
+               per_tolerance={str(t): {kk: (vv / d["n"] if kk != "n" else vv) for kk, vv in d.items()}
+                              for t, d in per_tol.items()})
+    return out, chosen
+
+
+def throughput(torch, gen, chosen, limit=150):
+    """End-to-end time over held-out problems: learned choice (through dgemm_ozaki_auto's path:
+    selection + Ozaki), the analytic count, fixed s = 10, and native FP64."""
+    L = lt.lib()
+    A, B, C = gen.A.data_ptr(), gen.B.data_ptr(), gen.C.data_ptr()
+    tot = dict(learned=0.0, analytic=0.0, fixed10=0.0, fp64=0.0)
+    flops = 0.0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for r, tol, s_final, s_a in chosen[:limit]:
+        M, N, K = r["M"], r["N"], r["K"]
+        gen.problem(M, N, K, r["phi"], r["smax"], r["seed"])
+        flops += 2.0 * M * N * K
+        runs = {
+            "learned": lambda: (L.lt_ozaki_select_slices(A, B, M, N, K, tol, ctypes.byref(ctypes.c_int()), None),
+                                L.lt_dgemm_ozaki(A, B, C, M, N, K, 1.0, 0.0, s_final, None)),
+            "analytic": lambda: L.lt_dgemm_ozaki(A, B, C, M, N, K, 1.0, 0.0, s_a, None),
+            "fixed10": lambda: L.lt_dgemm_ozaki(A, B, C, M, N, K, 1.0, 0.0, 10, None),
+            "fp64": lambda: L.lt_dgemm_fp64(A, B, C, M, N, K, 1.0, 0.0, None),
+        }
+        for name, fn in runs.items():
+            fn()
+            torch.cuda.synchronize()
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            tot[name] += e0.elapsed_time(e1)
+    return {k: flops / (v * 1e-3) / 1e12 for k, v in tot.items()}, {k: v for k, v in tot.items()}
+
+
+def main():
+    import torch
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", type=int, default=20000)
+    ap.add_argument("--test", type=int, default=2000)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--out", default=str(WEIGHTS))
+    ap.add_argument("--report", default="")
+    args = ap.parse_args()
+    torch.cuda.set_device(0)
+    gen = Generator(torch)
+    t0 = time.time()
+    train_rows = build_dataset(torch, gen, args.train, seed=1234, log_every=2000)
+    test_rows = build_dataset(torch, gen, args.test, seed=98765)
+    t_data = time.time() - t0
+    X, Y = expand(train_rows)
+    t1 = time.time()
+    params, hist = train(torch, X, Y, epochs=args.epochs)
+    t_train = time.time() - t1
+    params.astype(np.float32).tofile(args.out)
+    lt.check(lt.lib().lt_selector_set_params(params.ctypes.data))
+    ev, chosen = evaluate(torch, gen, params, test_rows)
+    tput, ms = throughput(torch, gen, chosen)
+    report = dict(train_matrices=args.train, test_matrices=args.test, train_samples=len(Y),
+                  label_histogram=np.bincount(Y, minlength=8).tolist(), data_seconds=t_data, train_seconds=t_train,
+                  loss_by_epoch=hist, evaluation=ev, throughput_tflops=tput, throughput_ms=ms, weights=args.out)
+    text = json.dumps(report, indent=1)
+    print(text)
+    if args.report:
+        Path(args.report).write_text(text)
+
+
+if __name__ == "__main__":
+    main()

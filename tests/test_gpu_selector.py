@@ -1,0 +1,174 @@
+"""GPU checks of the learned slice-count selector: features and MLP kernels against the CPU oracle
+(gradient check included), training progress, the analytic fallback, and what the trained network
+gains over the analytic count on held-out problems.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import to_dev
+
+pytestmark = pytest.mark.gpu
+WEIGHTS = Path(__file__).resolve().parents[1] / "libthom_b200" / "selector_weights.bin"
+
+
+def gpu_features(torch, A, B, tol):
+    import libthom_b200 as lt
+
+    dA, dB = to_dev(torch, A), to_dev(torch, B)
+    f = torch.empty(lt.LT_SEL_FEATURES, dtype=torch.float32, device="cuda")
+    lt.check(lt.lib().lt_ozaki_features(dA.data_ptr(), dB.data_ptr(), A.shape[0], B.shape[1], A.shape[1], tol,
+                                        f.data_ptr(), None))
+    return f.cpu().numpy()
+
+
+@pytest.mark.parametrize("M,N,K,phi,smax", [(300, 200, 150, 0, 0), (90, 17, 500, 30, 40), (1, 1, 1, 0, 0)])
+def test_features_match_oracle(cuda, oracle_mod, M, N, K, phi, smax):
+    A, B, _ = oracle_mod.make_problem(M, N, K, phi=phi, seed=M + N, smax=smax)
+    A[0, 0] = 0.0
+    f = gpu_features(cuda, A, B, 1e-14)
+    r = oracle_mod.features(A, B, 1e-14)
+    assert np.array_equal(f, r), np.abs(f - r).max()
+
+
+def rand_params(seed, scale=0.3):
+    import libthom_b200 as lt
+
+    return (np.random.default_rng(seed).standard_normal(lt.LT_SEL_PARAMS) * scale).astype(np.float32)
+
+
+def test_mlp_forward_matches_oracle(cuda, oracle_mod):
+    import libthom_b200 as lt
+
+    torch = cuda
+    p = rand_params(1)
+    x = np.random.default_rng(2).random((64, lt.LT_SEL_FEATURES)).astype(np.float32)
+    out = torch.empty(64, lt.LT_SEL_CLASSES, dtype=torch.float32, device="cuda")
+    lt.check(lt.lib().lt_mlp_forward(to_dev(torch, p).data_ptr(), to_dev(torch, x).data_ptr(), 64, out.data_ptr(), None))
+    assert np.allclose(out.cpu().numpy(), oracle_mod.mlp_forward(p, x), atol=2e-6)
+
+
+def test_mlp_gradient_check(cuda, oracle_mod):
+    """Backward kernel (per-sample gradients, fixed-order batch mean) vs the double-precision CPU
+    oracle, which is itself checked against finite differences in test_oracle.py."""
+    import libthom_b200 as lt
+
+    torch = cuda
+    p = rand_params(3)
+    rng = np.random.default_rng(4)
+    x = rng.random((96, lt.LT_SEL_FEATURES)).astype(np.float32)
+    y = rng.integers(0, lt.LT_SEL_CLASSES, 96).astype(np.int32)
+    g = torch.empty(lt.LT_SEL_PARAMS, dtype=torch.float32, device="cuda")
+    loss = torch.empty(1, dtype=torch.float32, device="cuda")
+    lt.check(lt.lib().lt_mlp_backward(to_dev(torch, p).data_ptr(), to_dev(torch, x).data_ptr(),
+                                      to_dev(torch, y).data_ptr(), 96, g.data_ptr(), loss.data_ptr(), None))
+    ref_loss, ref_g = oracle_mod.mlp_backward(p, x, y)
+    gg = g.cpu().numpy().astype(np.float64)
+    assert abs(float(loss.item()) - ref_loss) <= 1e-5 * max(1.0, abs(ref_loss))
+    assert np.all(np.abs(gg - ref_g) <= 2e-6 + 1e-4 * np.abs(ref_g)), np.abs(gg - ref_g).max()
+
+
+def test_training_reduces_loss(cuda):
+    import libthom_b200 as lt
+
+    torch = cuda
+    L = lt.lib()
+    rng = np.random.default_rng(5)
+    x = rng.random((256, lt.LT_SEL_FEATURES)).astype(np.float32)
+    y = (x[:, 0] * 7.99).astype(np.int32)  # a learnable labelling
+    p = to_dev(torch, rand_params(6, 0.1))
+    m, v, g = (torch.zeros_like(p) for _ in range(3))
+    loss = torch.empty(1, dtype=torch.float32, device="cuda")
+    xd, yd = to_dev(torch, x), to_dev(torch, y)
+    losses = []
+    for step in range(1, 301):
+        lt.check(L.lt_mlp_train_step(p.data_ptr(), m.data_ptr(), v.data_ptr(), g.data_ptr(), xd.data_ptr(),
+                                     yd.data_ptr(), 256, 3e-3, step, loss.data_ptr(), None))
+        losses.append(float(loss.item()))
+    assert losses[-1] < 0.5 * losses[0], (losses[0], losses[-1])
+
+
+def select(torch, A, B, tol):
+    import libthom_b200 as lt
+
+    dA, dB = to_dev(torch, A), to_dev(torch, B)
+    s, learned, gap = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    lt.check(lt.lib().lt_ozaki_select_info(dA.data_ptr(), dB.data_ptr(), A.shape[0], B.shape[1], A.shape[1], tol,
+                                           ctypes.byref(s), ctypes.byref(learned), ctypes.byref(gap), None))
+    return s.value, bool(learned.value), gap.value
+
+
+def test_analytic_fallback_without_weights(cuda, oracle_mod):
+    import libthom_b200 as lt
+
+    L = lt.lib()
+    lt.check(L.lt_selector_set_params(None))
+    try:
+        for phi, smax in ((0, 0), (16, 0), (0, 40)):
+            A, B, _ = oracle_mod.make_problem(120, 80, 200, phi=phi, seed=phi + smax, smax=smax)
+            s, learned, gap = select(cuda, A, B, 1e-14)
+            assert not learned
+            assert gap == oracle_mod.gap_bits(A, B)
+            assert s == oracle_mod.analytic_slices(1e-14, gap)
+    finally:
+        if WEIGHTS.exists():
+            w = np.fromfile(WEIGHTS, dtype=np.float32)
+            lt.check(L.lt_selector_set_params(w.ctypes.data))
+
+
+def test_trained_selector_gains_over_analytic(cuda, oracle_mod):
+    """Held-out problems (seeds never used in training): with the trained weights, the chosen slice
+    count is never above the analytic one, is smaller on average, and still meets the tolerance
+    (checked against the compensated oracle) on all but a small fraction."""
+    import libthom_b200 as lt
+
+    if not WEIGHTS.exists():
+        pytest.fail("libthom_b200/selector_weights.bin missing: run python -m libthom_b200.selector_train")
+    L = lt.lib()
+    w = np.fromfile(WEIGHTS, dtype=np.float32)
+    lt.check(L.lt_selector_set_params(w.ctypes.data))
+    torch = cuda
+    rng = np.random.default_rng(424242)
+    saved, misses, n = [], 0, 0
+    for i in range(24):
+        M, N, K = (int(rng.integers(64, 257)) for _ in range(3))
+        phi = int(rng.integers(0, 65))
+        smax = int(rng.integers(0, 65)) if i % 2 else 0
+        A, B, C0 = oracle_mod.make_problem(M, N, K, phi=phi, seed=10**9 + i, smax=smax)
+        Cref, den = oracle_mod.dot2_rows(A, B, None, 1.0, 0.0)
+        tol = (1e-12, 1e-14, 1e-15)[i % 3]
+        s, learned, gap = select(torch, A, B, tol)
+        sa = oracle_mod.analytic_slices(tol, gap)
+        assert s <= sa
+        saved.append(sa - s)
+        dA, dB = to_dev(torch, A), to_dev(torch, B)
+        dC = torch.zeros(M, N, dtype=torch.float64, device="cuda")
+        lt.dgemm_ozaki(dA, dB, dC, M, N, K, 1.0, 0.0, slices=s)
+        err = oracle_mod.componentwise_error(dC.cpu().numpy(), Cref, den)[0]
+        misses += err > tol
+        n += 1
+    assert np.mean(saved) >= 1.0, saved
+    assert misses <= 0.15 * n, (misses, n)
+
+
+def test_ozaki_auto_meets_tolerance(cuda, oracle_mod):
+    import libthom_b200 as lt
+
+    torch = cuda
+    L = lt.lib()
+    M, N, K = 256, 192, 512
+    A, B, C0 = oracle_mod.make_problem(M, N, K, phi=4, seed=77)
+    Cref, den = oracle_mod.dot2_rows(A, B, C0, 1.5, 0.5)
+    L.lt_set_ozaki_tolerance(1e-12)
+    try:
+        dA, dB, dC = to_dev(torch, A), to_dev(torch, B), to_dev(torch, C0)
+        ms = lt.dgemm("ozaki_auto", dA, dB, dC, M, N, K, 1.5, 0.5)
+        assert ms > 0
+        assert oracle_mod.componentwise_error(dC.cpu().numpy(), Cref, den)[0] <= 1e-12
+    finally:
+        L.lt_set_ozaki_tolerance(1e-15)
