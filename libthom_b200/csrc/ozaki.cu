@@ -537,12 +537,14 @@ __device__ __forceinline__ void ozaki_body(const Source& src, const GemmParams& 
   }
 }
 
-__global__ void __maxnreg__(200) ozaki_gemm_kernel(OzProblem pr, GemmParams p) {
+// 10 warps per CTA put 3 warps on two of the four SM sub-partitions, whose register files hold
+// 16K registers each: 168 registers per thread is the most a launch can use.
+__global__ void __launch_bounds__(kThreads, 1) ozaki_gemm_kernel(OzProblem pr, GemmParams p) {
   OzSingleSource src{&pr, (pr.M + kTileM - 1) / kTileM, (pr.N + kTileN - 1) / kTileN};
   ozaki_body(src, p);
 }
 
-__global__ void __maxnreg__(200) ozaki_gemm_grouped_kernel(OzGroupedSource src, GemmParams p) {
+__global__ void __launch_bounds__(kThreads, 1) ozaki_gemm_grouped_kernel(OzGroupedSource src, GemmParams p) {
   ozaki_body(src, p);
 }
 
