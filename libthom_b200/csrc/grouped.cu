@@ -135,7 +135,7 @@ int lt_grouped_plan_run_graph(lt_grouped_plan* plan, void* stream) {
     if (plan->form == LT_FORM_FP64) {
       LT_TRY(lt::fp64::grouped_prepare(plan->fp));
     } else {
-      LT_TRY(lt::ozaki::grouped_prepare());
+      LT_TRY(lt::ozaki::grouped_prepare(plan->oz));
     }
     LT_CUDA_TRY(cudaStreamBeginCapture(plan->capture_stream, cudaStreamCaptureModeThreadLocal));
     int rc = lt_grouped_plan_run(plan, plan->capture_stream);

@@ -37,7 +37,7 @@ int run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64
 struct Grouped;
 int grouped_create(const lt_gemm_problem* problems, int count, int slices, Grouped** out);
 int grouped_run(const Grouped* G, cudaStream_t stream);
-int grouped_prepare();
+int grouped_prepare(const Grouped* G);
 void grouped_destroy(Grouped* G);
 int64_t grouped_tiles(const Grouped* G);
 }  // namespace ozaki

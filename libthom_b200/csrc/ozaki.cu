@@ -231,12 +231,6 @@ __global__ void __launch_bounds__(128) split_cols_kernel(const double* __restric
 // ---------------------------------------------------------------------------------------------
 // Product + recombination kernel
 // ---------------------------------------------------------------------------------------------
-// Launch-wide parameters (the slice count is shared by every tile of a launch).
-struct GemmParams {
-  int s, stages, stage_tiles;
-  DeviceStatus* status;
-};
-
 // One problem: its slice tiles, exponents, C and scalars.
 struct OzProblem {
   const int8_t* sa;
@@ -288,31 +282,42 @@ struct OzGroupedSource {
 
 // Band b of s slices: diagonals dhi = s + 1 - 4b down to dlo; A/B slices 1..nsl are involved.
 struct Band {
-  int dhi, dlo, nsl, maxp, gchunks, cps;
+  int dhi, dlo, nsl, maxp;
 };
 
-__device__ __forceinline__ int pair_lo(int d, int s) { return d - s > 1 ? d - s : 1; }
-__device__ __forceinline__ int pair_hi(int d, int s) { return d - 1 < s ? d - 1 : s; }
-
-__device__ __forceinline__ Band make_band(int b, int s, int stage_tiles) {
-  Band B;
+__host__ __device__ constexpr int pair_lo(int d, int s) { return d - s > 1 ? d - s : 1; }
+__host__ __device__ constexpr int pair_hi(int d, int s) { return d - 1 < s ? d - 1 : s; }
+__host__ __device__ constexpr int num_bands(int s) { return (s + kBand - 1) / kBand; }
+__host__ __device__ constexpr Band band_of(int s, int b) {
+  Band B{0, 0, 0, 0};
   B.dhi = s + 1 - kBand * b;
   B.dlo = B.dhi - kBand + 1 < 2 ? 2 : B.dhi - kBand + 1;
   B.nsl = B.dhi - 1 < s ? B.dhi - 1 : s;
-  B.maxp = 0;
   for (int d = B.dhi; d >= B.dlo; --d) {
-    int np = pair_hi(d, s) - pair_lo(d, s) + 1;
-    B.maxp = np > B.maxp ? np : B.maxp;
+    const int np = pair_hi(d, s) - pair_lo(d, s) + 1;
+    if (np > B.maxp) B.maxp = np;
   }
-  B.gchunks = kKPairLimit / (kChunk * B.maxp);
-  B.cps = stage_tiles / (2 * B.nsl);
   return B;
 }
 
-__device__ __forceinline__ int num_bands(int s) { return (s + kBand - 1) / kBand; }
+// Pipeline geometry for S slices: a stage holds the 2*nsl tiles of one 32-wide K chunk of the
+// widest band (nsl = S), narrower bands pack several chunks into a stage.
+template <int S>
+struct Geo {
+  static constexpr int kStageTiles = 2 * S;
+  static constexpr int kStageBytes = kStageTiles * kTileBytes;
+  static constexpr int kStagesFit = (kMaxSmem - kSmemOverhead) / kStageBytes;
+  static constexpr int kStages = kStagesFit > 8 ? 8 : kStagesFit;
+  static constexpr int kSmem = kStages * kStageBytes + kSmemOverhead;
+  static_assert(kStages >= 2, "slice count too large for the shared-memory ring");
+  __host__ __device__ static constexpr int gchunks(int b) { return kKPairLimit / (kChunk * band_of(S, b).maxp); }
+  __host__ __device__ static constexpr int cps(int b) { return kStageTiles / (2 * band_of(S, b).nsl); }
+};
 
 // Shared-memory matrix descriptor, K-major, 32-byte swizzle: rows of 32 bytes, 8-row groups
-// 256 bytes apart (SBO), layout type SWIZZLE_32B (6), descriptor version 1.
+// 256 bytes apart (SBO), layout type SWIZZLE_32B (6), descriptor version 1. The start address
+// (bits 0..13, in 16-byte units) of consecutive 4 KB tiles differs by 256, so tile t of a stage
+// is desc(stage) + 256 t.
 __device__ __forceinline__ uint64_t desc_k_sw32(uint32_t addr) {
   uint64_t d = 0;
   d |= static_cast<uint64_t>((addr >> 4) & 0x3FFFu);
@@ -330,14 +335,41 @@ __device__ __forceinline__ void bulk_load(void* smem_dst, const void* gsrc, uint
                : "memory");
 }
 
-template <class Source>
-__device__ __forceinline__ void ozaki_body(const Source& src, const GemmParams& p) {
+// All MMAs of band B for one K chunk, unrolled at compile time: diagonal J of the band (d = dhi - J)
+// accumulates pairs (PP, d - PP) into TMEM columns J*128 .. +127. A tiles sit at slots 0..nsl-1 of
+// the chunk, B tiles at nsl..2nsl-1. The first pair of each diagonal overwrites when `first`.
+template <int S, int B, int J, int PP>
+__device__ __forceinline__ void issue_pairs(uint64_t a0, uint32_t tmem, uint32_t accumulate_first) {
+  constexpr Band bd = band_of(S, B);
+  constexpr int d = bd.dhi - J;
+  if constexpr (J < kBand && d >= bd.dlo) {
+    if constexpr (PP <= pair_hi(d, S)) {
+      constexpr uint32_t idesc = idesc_i8_s32(kTileM, kTileN);
+      constexpr uint64_t a_off = static_cast<uint64_t>((PP - 1) * (kTileBytes >> 4));
+      constexpr uint64_t b_off = static_cast<uint64_t>((bd.nsl + d - PP - 1) * (kTileBytes >> 4));
+      mma_i8(tmem + static_cast<uint32_t>(J * kTileN), a0 + a_off, a0 + b_off, idesc,
+             PP == pair_lo(d, S) ? accumulate_first : 1u);
+      issue_pairs<S, B, J, PP + 1>(a0, tmem, accumulate_first);
+    } else {
+      issue_pairs<S, B, J + 1, pair_lo(d - 1, S)>(a0, tmem, accumulate_first);
+    }
+  }
+}
+
+template <int S, int B>
+__device__ __forceinline__ void issue_chunk(uint64_t a0, uint32_t tmem, uint32_t accumulate_first) {
+  if constexpr (B < num_bands(S)) issue_pairs<S, B, 0, pair_lo(band_of(S, B).dhi, S)>(a0, tmem, accumulate_first);
+}
+
+template <int S, class Source>
+__device__ __forceinline__ void ozaki_body(const Source& src, DeviceStatus* status) {
+  using G = Geo<S>;
+  constexpr int NB = num_bands(S);
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const int stage_bytes = p.stage_tiles * kTileBytes;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + p.stages * stage_bytes);
-  uint64_t* empty = full + p.stages;
-  uint64_t* acc_full = empty + p.stages;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + G::kStages * G::kStageBytes);
+  uint64_t* empty = full + G::kStages;
+  uint64_t* acc_full = empty + G::kStages;
   uint64_t* acc_empty = acc_full + 1;
   uint64_t* drain = acc_empty + 1;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
@@ -345,10 +377,9 @@ __device__ __forceinline__ void ozaki_body(const Source& src, const GemmParams& 
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t tiles = src.count();
-  const int nb = num_bands(p.s);
 
   if (threadIdx.x == 0) {
-    for (int i = 0; i < p.stages; ++i) {
+    for (int i = 0; i < G::kStages; ++i) {
       mbar_init(&full[i], 1);
       mbar_init(&empty[i], 1);
     }
@@ -380,24 +411,26 @@ __device__ __forceinline__ void ozaki_body(const Source& src, const GemmParams& 
         const int8_t* a_blk = pr.sa + static_cast<int64_t>(J.m0 / kTileM) * nkc * kTileBytes;
         const int8_t* b_blk = pr.sb + static_cast<int64_t>(J.n0 / kTileN) * nkc * kTileBytes;
         const int64_t a_slice = pr.rba * nkc * kTileBytes, b_slice = pr.rbb * nkc * kTileBytes;
-        for (int b = 0; b < nb && ok; ++b) {
-          const Band bd = make_band(b, p.s, p.stage_tiles);
-          for (int64_t c0 = 0; c0 < nkc && ok; c0 += bd.gchunks) {
-            const int64_t c1 = (c0 + bd.gchunks < nkc) ? c0 + bd.gchunks : nkc;
-            for (int64_t cs = c0; cs < c1; cs += bd.cps) {
-              const int64_t ce = (cs + bd.cps < c1) ? cs + bd.cps : c1;
-              if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.status, 11)) { ok = false; break; }
-              uint8_t* st = smem + stage * stage_bytes;
+        for (int b = 0; b < NB && ok; ++b) {
+          const Band bd = band_of(S, b);
+          const int gch = G::gchunks(b), cps = G::cps(b);
+          for (int64_t c0 = 0; c0 < nkc && ok; c0 += gch) {
+            const int64_t c1 = (c0 + gch < nkc) ? c0 + gch : nkc;
+            for (int64_t cs = c0; cs < c1; cs += cps) {
+              const int64_t ce = (cs + cps < c1) ? cs + cps : c1;
+              if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, status, 11)) { ok = false; break; }
+              uint8_t* st = smem + stage * G::kStageBytes;
               mbar_arrive_expect_tx(&full[stage], static_cast<uint32_t>((ce - cs) * 2 * bd.nsl * kTileBytes));
               for (int64_t c = cs; c < ce; ++c) {
                 uint8_t* base = st + (c - cs) * 2 * bd.nsl * kTileBytes;
-                for (int q = 0; q < bd.nsl; ++q)
-                  bulk_load(base + q * kTileBytes, a_blk + q * a_slice + c * kTileBytes, kTileBytes, &full[stage]);
-                for (int q = 0; q < bd.nsl; ++q)
-                  bulk_load(base + (bd.nsl + q) * kTileBytes, b_blk + q * b_slice + c * kTileBytes, kTileBytes,
-                            &full[stage]);
+                const int8_t* ga = a_blk + c * kTileBytes;
+                const int8_t* gb = b_blk + c * kTileBytes;
+                for (int q = 0; q < bd.nsl; ++q) {
+                  bulk_load(base + q * kTileBytes, ga + q * a_slice, kTileBytes, &full[stage]);
+                  bulk_load(base + (bd.nsl + q) * kTileBytes, gb + q * b_slice, kTileBytes, &full[stage]);
+                }
               }
-              if (++stage == p.stages) { stage = 0; phase ^= 1; }
+              if (++stage == G::kStages) { stage = 0; phase ^= 1; }
             }
           }
         }
@@ -406,45 +439,39 @@ __device__ __forceinline__ void ozaki_body(const Source& src, const GemmParams& 
     __syncwarp();
   } else if (warp == 1) {
     // ------------------------------------ MMA issuer ------------------------------------
-    constexpr uint32_t idesc = idesc_i8_s32(kTileM, kTileN);
-    const uint32_t smem_base = smem_u32(smem);
+    const uint64_t desc0 = desc_k_sw32(smem_u32(smem));
     int stage = 0;
     uint32_t phase = 0;
     uint32_t group = 0;
     bool ok = true;
     for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
       const int64_t nkc = src.get(t).pr->nkc;
-      for (int b = 0; b < nb && ok; ++b) {
-        const Band bd = make_band(b, p.s, p.stage_tiles);
-        for (int64_t c0 = 0; c0 < nkc && ok; c0 += bd.gchunks) {
-          const int64_t c1 = (c0 + bd.gchunks < nkc) ? c0 + bd.gchunks : nkc;
-          if (!mbar_wait(acc_empty, (group & 1) ^ 1, abort_flag, p.status, 12)) { ok = false; break; }
+      for (int b = 0; b < NB && ok; ++b) {
+        const Band bd = band_of(S, b);
+        const int gch = G::gchunks(b), cps = G::cps(b);
+        const uint64_t chunk_step = static_cast<uint64_t>(2 * bd.nsl * (kTileBytes >> 4));
+        for (int64_t c0 = 0; c0 < nkc && ok; c0 += gch) {
+          const int64_t c1 = (c0 + gch < nkc) ? c0 + gch : nkc;
+          if (!mbar_wait(acc_empty, (group & 1) ^ 1, abort_flag, status, 12)) { ok = false; break; }
           tc_fence_after();
-          for (int64_t cs = c0; cs < c1; cs += bd.cps) {
-            const int64_t ce = (cs + bd.cps < c1) ? cs + bd.cps : c1;
-            if (!mbar_wait(&full[stage], phase, abort_flag, p.status, 13)) { ok = false; break; }
+          for (int64_t cs = c0; cs < c1; cs += cps) {
+            const int64_t ce = (cs + cps < c1) ? cs + cps : c1;
+            if (!mbar_wait(&full[stage], phase, abort_flag, status, 13)) { ok = false; break; }
             tc_fence_after();
             if (lane == 0) {
-              const uint32_t st = smem_base + stage * stage_bytes;
-              for (int64_t c = cs; c < ce; ++c) {
-                const uint32_t base = st + static_cast<uint32_t>((c - cs) * 2 * bd.nsl * kTileBytes);
-                for (int j = 0; j < kBand; ++j) {
-                  const int d = bd.dhi - j;
-                  if (d < bd.dlo) break;
-                  const int plo = pair_lo(d, p.s), phi = pair_hi(d, p.s);
-                  for (int pp = plo; pp <= phi; ++pp) {
-                    const int qq = d - pp;
-                    const uint64_t adesc = desc_k_sw32(base + (pp - 1) * kTileBytes);
-                    const uint64_t bdesc = desc_k_sw32(base + (bd.nsl + qq - 1) * kTileBytes);
-                    const uint32_t accum = (c == c0 && pp == plo) ? 0u : 1u;
-                    mma_i8(tmem_base + static_cast<uint32_t>(j * kTileN), adesc, bdesc, idesc, accum);
-                  }
+              uint64_t a0 = desc0 + static_cast<uint64_t>(stage) * (G::kStageBytes >> 4);
+              for (int64_t c = cs; c < ce; ++c, a0 += chunk_step) {
+                const uint32_t acc_first = (c == c0) ? 0u : 1u;
+                switch (b) {
+                  case 0: issue_chunk<S, 0>(a0, tmem_base, acc_first); break;
+                  case 1: issue_chunk<S, 1>(a0, tmem_base, acc_first); break;
+                  default: issue_chunk<S, 2>(a0, tmem_base, acc_first); break;
                 }
               }
               mma_commit(&empty[stage]);
             }
             __syncwarp();
-            if (++stage == p.stages) { stage = 0; phase ^= 1; }
+            if (++stage == G::kStages) { stage = 0; phase ^= 1; }
           }
           if (!ok) break;
           if (lane == 0) mma_commit(acc_full);
@@ -471,14 +498,15 @@ __device__ __forceinline__ void ozaki_body(const Source& src, const GemmParams& 
     bool ok = true;
     for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
       const OzJob J = src.get(t);
-      const OzProblem& pr = *J.pr;
+      const int64_t nkc = J.pr->nkc;
       double acc[64];
 #pragma unroll
       for (int i = 0; i < 64; ++i) acc[i] = 0.0;
-      for (int b = 0; b < nb && ok; ++b) {
-        const Band bd = make_band(b, p.s, p.stage_tiles);
-        for (int64_t c0 = 0; c0 < pr.nkc; c0 += bd.gchunks) {
-          if (!mbar_wait(acc_full, group & 1, abort_flag, p.status, 14)) { ok = false; break; }
+      for (int b = 0; b < NB && ok; ++b) {
+        const Band bd = band_of(S, b);
+        const int gch = G::gchunks(b);
+        for (int64_t c0 = 0; c0 < nkc; c0 += gch) {
+          if (!mbar_wait(acc_full, group & 1, abort_flag, status, 14)) { ok = false; break; }
           tc_fence_after();
           for (int j = 0; j < kBand; ++j) {
             const int d = bd.dhi - j;
@@ -505,22 +533,26 @@ __device__ __forceinline__ void ozaki_body(const Source& src, const GemmParams& 
       }
       if (!ok) break;
       // ---- C = fma(alpha, acc 2^sigma 2^tau, beta C0) ----
+      const OzProblem& pr = *J.pr;
       const int64_t row = J.m0 + row_in_tile;
       if (row < pr.M) {
         const int sig = exponent_of_maxbits(pr.amax_a[row]);
         const int64_t col0 = J.n0 + half * 64;
         double* crow = pr.C + row * pr.N;
+        const int64_t N = pr.N;
+        const double alpha = pr.alpha, beta = pr.beta;
+        const unsigned long long* amax_b = pr.amax_b;
 #pragma unroll
         for (int i = 0; i < 64; ++i) {
           const int64_t col = col0 + i;
-          if (col < pr.N) {
-            const int tau = exponent_of_maxbits(pr.amax_b[col]);
+          if (col < N) {
+            const int tau = exponent_of_maxbits(amax_b[col]);
             double out;
             if (sig == kSentinel || tau == kSentinel) {
               out = __longlong_as_double(0x7ff8000000000000ll);
             } else {
               const double tv = scale_pow2(scale_pow2(acc[i], sig), tau);
-              out = (pr.beta != 0.0) ? fma(pr.alpha, tv, __dmul_rn(pr.beta, crow[col])) : __dmul_rn(pr.alpha, tv);
+              out = (beta != 0.0) ? fma(alpha, tv, __dmul_rn(beta, crow[col])) : __dmul_rn(alpha, tv);
             }
             crow[col] = out;
           }
@@ -539,13 +571,52 @@ __device__ __forceinline__ void ozaki_body(const Source& src, const GemmParams& 
 
 // 10 warps per CTA put 3 warps on two of the four SM sub-partitions, whose register files hold
 // 16K registers each: 168 registers per thread is the most a launch can use.
-__global__ void __launch_bounds__(kThreads, 1) ozaki_gemm_kernel(OzProblem pr, GemmParams p) {
+template <int S>
+__global__ void __launch_bounds__(kThreads, 1) ozaki_gemm_kernel(OzProblem pr, DeviceStatus* status) {
   OzSingleSource src{&pr, (pr.M + kTileM - 1) / kTileM, (pr.N + kTileN - 1) / kTileN};
-  ozaki_body(src, p);
+  ozaki_body<S>(src, status);
 }
 
-__global__ void __launch_bounds__(kThreads, 1) ozaki_gemm_grouped_kernel(OzGroupedSource src, GemmParams p) {
-  ozaki_body(src, p);
+template <int S>
+__global__ void __launch_bounds__(kThreads, 1) ozaki_gemm_grouped_kernel(OzGroupedSource src, DeviceStatus* status) {
+  ozaki_body<S>(src, status);
+}
+
+// Launches the product kernel for S slices over `src` (single problem or grouped tile list).
+template <int S, bool kGrouped, class Src>
+int launch_gemm_s(const Src& src, int64_t ntiles, DeviceContext* ctx, cudaStream_t stream) {
+  using G = Geo<S>;
+  static std::once_flag once[64];
+  static cudaError_t attr_err[64];
+  std::call_once(once[ctx->device], [&] {
+    if (kGrouped)
+      attr_err[ctx->device] =
+          cudaFuncSetAttribute(ozaki_gemm_grouped_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::kSmem);
+    else
+      attr_err[ctx->device] =
+          cudaFuncSetAttribute(ozaki_gemm_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::kSmem);
+  });
+  LT_CUDA_TRY(attr_err[ctx->device]);
+  if (ntiles <= 0) return LT_OK;
+  const int64_t grid = ntiles < ctx->sm_count ? ntiles : ctx->sm_count;
+  if constexpr (kGrouped)
+    ozaki_gemm_grouped_kernel<S><<<static_cast<unsigned>(grid), kThreads, G::kSmem, stream>>>(src, ctx->status);
+  else
+    ozaki_gemm_kernel<S><<<static_cast<unsigned>(grid), kThreads, G::kSmem, stream>>>(src, ctx->status);
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
+template <bool kGrouped, class Src>
+int launch_gemm(int s, const Src& src, int64_t ntiles, DeviceContext* ctx, cudaStream_t stream) {
+  switch (s) {
+#define LT_GEMM_CASE(S) \
+  case S: return launch_gemm_s<S, kGrouped>(src, ntiles, ctx, stream);
+    LT_GEMM_CASE(1) LT_GEMM_CASE(2) LT_GEMM_CASE(3) LT_GEMM_CASE(4) LT_GEMM_CASE(5) LT_GEMM_CASE(6)
+    LT_GEMM_CASE(7) LT_GEMM_CASE(8) LT_GEMM_CASE(9) LT_GEMM_CASE(10) LT_GEMM_CASE(11) LT_GEMM_CASE(12)
+#undef LT_GEMM_CASE
+    default: return set_error(LT_ERR_INVALID_ARGUMENT, "slice count %d unsupported", s);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -616,30 +687,6 @@ int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int
   return launch_split(s, A, B, M, N, K, L, amax_a, amax_b, sa, sb, sms, stream);
 }
 
-int gemm_params(int s, DeviceContext* ctx, GemmParams* gp) {
-  gp->s = s;
-  gp->stage_tiles = 2 * s;
-  const int stage_bytes = gp->stage_tiles * kTileBytes;
-  gp->stages = (kMaxSmem - kSmemOverhead) / stage_bytes;
-  if (gp->stages > 8) gp->stages = 8;
-  if (gp->stages < 2) return set_error(LT_ERR_UNSUPPORTED, "slice count %d needs more shared memory", s);
-  gp->status = ctx->status;
-  return LT_OK;
-}
-
-int set_gemm_smem(DeviceContext* ctx) {
-  static std::once_flag once[64];
-  static cudaError_t attr_err[64];
-  std::call_once(once[ctx->device], [&] {
-    attr_err[ctx->device] = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-    if (attr_err[ctx->device] == cudaSuccess)
-      attr_err[ctx->device] =
-          cudaFuncSetAttribute(ozaki_gemm_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-  });
-  LT_CUDA_TRY(attr_err[ctx->device]);
-  return LT_OK;
-}
-
 // Stage 3+4: slice products on the tensor cores and the fused FP64 recombination into C.
 int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int s, const void* workspace,
             size_t workspace_bytes, cudaStream_t stream) {
@@ -661,15 +708,7 @@ int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double bet
   pr.rbb = L.RBb;
   pr.alpha = alpha;
   pr.beta = beta;
-  GemmParams gp;
-  LT_TRY(gemm_params(s, ctx, &gp));
-  LT_TRY(set_gemm_smem(ctx));
-  const int smem = gp.stages * gp.stage_tiles * kTileBytes + kSmemOverhead;
-  const int64_t tiles = L.RBa * L.RBb;
-  const int64_t grid = tiles < ctx->sm_count ? tiles : ctx->sm_count;
-  ozaki_gemm_kernel<<<static_cast<unsigned>(grid), kThreads, smem, stream>>>(pr, gp);
-  LT_CUDA_TRY(cudaGetLastError());
-  return LT_OK;
+  return launch_gemm<false>(s, pr, L.RBa * L.RBb, ctx, stream);
 }
 
 int run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int s,
@@ -884,21 +923,16 @@ int grouped_run(const Grouped* G, cudaStream_t stream) {
     default: return set_error(LT_ERR_INVALID_ARGUMENT, "slice count %d unsupported", G->s);
   }
   if (G->ntiles == 0) return LT_OK;
-  GemmParams gp;
-  LT_TRY(gemm_params(G->s, ctx, &gp));
-  LT_TRY(set_gemm_smem(ctx));
-  const int smem = gp.stages * gp.stage_tiles * kTileBytes + kSmemOverhead;
   OzGroupedSource src{G->d_problems, G->d_tiles, G->ntiles};
-  const int64_t grid = G->ntiles < ctx->sm_count ? G->ntiles : ctx->sm_count;
-  ozaki_gemm_grouped_kernel<<<static_cast<unsigned>(grid), kThreads, smem, stream>>>(src, gp);
-  LT_CUDA_TRY(cudaGetLastError());
-  return LT_OK;
+  return launch_gemm<true>(G->s, src, G->ntiles, ctx, stream);
 }
 
-int grouped_prepare() {
+// Kernel attribute set-up only (ntiles = 0: nothing is launched), before a stream capture.
+int grouped_prepare(const Grouped* G) {
   DeviceContext* ctx = context();
   if (ctx == nullptr) return last_error();
-  return set_gemm_smem(ctx);
+  OzGroupedSource src{G->d_problems, G->d_tiles, 0};
+  return launch_gemm<true>(G->s, src, 0, ctx, nullptr);
 }
 
 void grouped_destroy(Grouped* G) {

@@ -49,7 +49,8 @@ def test_mlp_forward_matches_oracle(cuda, oracle_mod):
     p = rand_params(1)
     x = np.random.default_rng(2).random((64, lt.LT_SEL_FEATURES)).astype(np.float32)
     out = torch.empty(64, lt.LT_SEL_CLASSES, dtype=torch.float32, device="cuda")
-    lt.check(lt.lib().lt_mlp_forward(to_dev(torch, p).data_ptr(), to_dev(torch, x).data_ptr(), 64, out.data_ptr(), None))
+    dp, dx = to_dev(torch, p), to_dev(torch, x)  # keep the buffers alive across the launch
+    lt.check(lt.lib().lt_mlp_forward(dp.data_ptr(), dx.data_ptr(), 64, out.data_ptr(), None))
     assert np.allclose(out.cpu().numpy(), oracle_mod.mlp_forward(p, x), atol=2e-6)
 
 
@@ -65,8 +66,9 @@ def test_mlp_gradient_check(cuda, oracle_mod):
     y = rng.integers(0, lt.LT_SEL_CLASSES, 96).astype(np.int32)
     g = torch.empty(lt.LT_SEL_PARAMS, dtype=torch.float32, device="cuda")
     loss = torch.empty(1, dtype=torch.float32, device="cuda")
-    lt.check(lt.lib().lt_mlp_backward(to_dev(torch, p).data_ptr(), to_dev(torch, x).data_ptr(),
-                                      to_dev(torch, y).data_ptr(), 96, g.data_ptr(), loss.data_ptr(), None))
+    dp, dx, dy = to_dev(torch, p), to_dev(torch, x), to_dev(torch, y)
+    lt.check(lt.lib().lt_mlp_backward(dp.data_ptr(), dx.data_ptr(), dy.data_ptr(), 96, g.data_ptr(),
+                                      loss.data_ptr(), None))
     ref_loss, ref_g = oracle_mod.mlp_backward(p, x, y)
     gg = g.cpu().numpy().astype(np.float64)
     assert abs(float(loss.item()) - ref_loss) <= 1e-5 * max(1.0, abs(ref_loss))
