@@ -134,16 +134,49 @@ __global__ void amax_cols_kernel(const double* __restrict__ B, int64_t K, int64_
 // Split
 // ---------------------------------------------------------------------------------------------
 // Splits one value into S slices q_1..q_S, OR-ing byte j of each into packed[p][j / 4].
+//
+// The recurrence y = 128 x, q = trunc(y), x = y - q on x = a 2^-e is exact, so q_1..q_S are the
+// base-128 digits of |x| (each carrying the sign of a). They are read here straight from the IEEE
+// fields: |a| = m 2^t (m the significand with its hidden bit), X = floor(|x| 2^(7S)) =
+// floor(m 2^(t - e + 7S)) < 2^(7S), and q_p = bits [7(S-p), 7(S-p)+7) of X. (When x underflows in
+// the FP64 recurrence, X's leading 7S bits are zero as well.)
 template <int S>
 __device__ __forceinline__ void split_value(double a, int e, int j, uint32_t (&packed)[S][8]) {
-  if (e == kSentinel || !isfinite(a)) return;  // all-zero slices
-  double x = scale_pow2(a, -e);
+  if (e == kSentinel) return;  // NaN/Inf somewhere in the row/column: zero slices, NaN output
+  const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(a));
+  const unsigned long long mag = bits & 0x7fffffffffffffffull;
+  const int E = static_cast<int>(mag >> 52);
+  if (mag == 0ull || E == 0x7ff) return;  // zero, or a non-finite entry: zero slices
+  unsigned long long m = mag & 0x000fffffffffffffull;
+  int t;
+  if (E == 0) {
+    t = -1074;
+  } else {
+    m |= 0x0010000000000000ull;
+    t = E - 1075;
+  }
+  const int sh = t - e + 7 * S;
+  const uint32_t neg = static_cast<uint32_t>(bits >> 63);  // 1 for negative a
+  if constexpr (7 * S <= 63) {
+    unsigned long long X;
+    if (sh >= 0) X = m << sh;
+    else X = (-sh >= 64) ? 0ull : (m >> (-sh));
 #pragma unroll
-  for (int p = 0; p < S; ++p) {
-    double y = __dmul_rn(x, 128.0);
-    double q = trunc(y);
-    x = __dsub_rn(y, q);
-    packed[p][j >> 2] |= (static_cast<uint32_t>(static_cast<int>(q)) & 0xffu) << (8 * (j & 3));
+    for (int p = 0; p < S; ++p) {
+      const uint32_t dgt = static_cast<uint32_t>(X >> (7 * (S - 1 - p))) & 127u;
+      const uint32_t q = (dgt ^ (0u - neg)) + neg;  // two's-complement negation when negative
+      packed[p][j >> 2] |= (q & 0xffu) << (8 * (j & 3));
+    }
+  } else {
+    unsigned __int128 X;
+    if (sh >= 0) X = static_cast<unsigned __int128>(m) << sh;
+    else X = (-sh >= 128) ? static_cast<unsigned __int128>(0) : (static_cast<unsigned __int128>(m) >> (-sh));
+#pragma unroll
+    for (int p = 0; p < S; ++p) {
+      const uint32_t dgt = static_cast<uint32_t>(X >> (7 * (S - 1 - p))) & 127u;
+      const uint32_t q = (dgt ^ (0u - neg)) + neg;
+      packed[p][j >> 2] |= (q & 0xffu) << (8 * (j & 3));
+    }
   }
 }
 
