@@ -36,6 +36,35 @@ SEED = 1234
 DMMA_PEAK_TFLOPS = 37.0  # measured FP64 mma.sync peak on this pool's B200s (profiles/dmma_peak_b200.md)
 
 
+WORKLOADS = ("square", "tall", "longk")
+
+
+def workload(args):
+    """(M, N, K, alpha, beta, row/column scale exponent bound, description) of the selected workload."""
+    if args.workload == "tall":
+        return 65536, 64, 4096, 1.0, 0.0, 64, "dgemm 65536x64x4096, rows/cols scaled 2^U{-64..64}"
+    if args.workload == "longk":
+        return 2048, 2048, 65536, 1.0, 0.0, 64, "dgemm 2048x2048x65536, rows/cols scaled 2^U{-64..64}"
+    n = args.size
+    return n, n, n, 1.5, 0.5, 0, f"dgemm {n}^3 alpha=1.5 beta=0.5 phi={args.phi}"
+
+
+def reduce_max(x: float, dist=None, device="cpu") -> float:
+    """The largest of every rank's x (timings are reported as the slowest rank's)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(flop_per_rank: float, world: int, ms_per_step: float) -> float:
+    """Whole-job TFLOP/s of `world` replicas, each doing flop_per_rank per step, timed by the slowest."""
+    return world * flop_per_rank / (ms_per_step * 1e-3) / 1e12
+
+
 def env_rank():
     return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0)))
 
@@ -120,19 +149,25 @@ class ClockSampler:
 # ------------------------------------------------------------------------------------------------
 # CPU legs (oracle = checker; used only for the accuracy selection and the CPU baselines)
 # ------------------------------------------------------------------------------------------------
-def cpu_baseline_blocked(N: int, rows: int, phi: int, threads: int) -> dict:
+def cpu_baseline_blocked(M: int, N: int, K: int, rows: int, phi: int, smax: int, threads: int) -> dict:
+    """Host blocked FP64 DGEMM on the first `rows` rows of the workload (A rows x K times K x N)."""
     import oracle
 
     oracle.build()
-    A = oracle.fill(rows, N, 1, phi, SEED)
-    B = oracle.fill(N, N, 2, phi, SEED)
+    rows = min(rows, M)
+    A = oracle.fill(rows, K, 1, phi, SEED)
+    B = oracle.fill(K, N, 2, phi, SEED)
     C0 = oracle.fill(rows, N, 3, phi, SEED)
+    if smax > 0:
+        oracle.scale_rows(A, SEED, 4, smax)
+        oracle.scale_cols(B, SEED, 5, smax)
     t0 = time.perf_counter()
     oracle.dgemm_blocked(A, B, C0, 1.5, 0.5, threads)
     dt = time.perf_counter() - t0
-    return {"value": 2.0 * rows * N * N / dt / 1e12, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"host blocked FP64 DGEMM (oracle/oracle_blocked.c) on {rows} rows of the {N}^3 problem "
-                      f"({2.0 * rows * N * N:.3g} flop, {dt:.2f} s wall on {threads} threads)"}
+    flop = 2.0 * rows * N * K
+    return {"value": flop / dt / 1e12, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"host blocked FP64 DGEMM (oracle/oracle_blocked.c) on {rows} of {M} rows of the "
+                      f"{M}x{N}x{K} problem ({flop:.3g} flop, {dt:.2f} s wall on {threads} threads)"}
 
 
 _REF_STATE = {}
@@ -253,8 +288,7 @@ def run_ours(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
-    N = M = K = args.size
-    alpha, beta = 1.5, 0.5
+    M, N, K, alpha, beta, smax, wname = workload(args)
     flop = 2.0 * M * N * K
 
     A = torch.empty(M, K, dtype=torch.float64, device=dev)
@@ -264,6 +298,9 @@ def run_ours(args) -> None:
     lt.fill(A, M * K, SEED, 1, args.phi, stream)
     lt.fill(B, K * N, SEED, 2, args.phi, stream)
     lt.fill(C0, M * N, SEED, 3, args.phi, stream)
+    if smax > 0:
+        lt.scale_rows(A, M, K, SEED, 4, smax, stream)
+        lt.scale_cols(B, K, N, SEED, 5, smax, stream)
     torch.cuda.synchronize()
 
     # ---- accuracy selection (untimed): smallest slice count no worse than native FP64 ----
@@ -312,11 +349,7 @@ def run_ours(args) -> None:
         torch.cuda.synchronize()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, dev)
 
     # ---- headline: Ozaki INT8 path, inputs resident in HBM (512 MiB each > 126 MB L2) ----
     for _ in range(args.warmup):
@@ -408,14 +441,15 @@ def run_ours(args) -> None:
     traffic = profile_traffic("ozaki_gemm_8192")
     cpu = None
     if world == 1 and not args.no_cpu:
-        cpu = cpu_baseline_blocked(N, args.cpu_rows, args.phi, len(os.sched_getaffinity(0)))
+        cpu = cpu_baseline_blocked(M, N, K, args.cpu_rows, args.phi, smax, len(os.sched_getaffinity(0)))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 (int8 slices, int32 accumulate)", "data": "synthetic (seeded generator)",
-        "config": {"workload": f"dgemm {N}^3 alpha={alpha} beta={beta} phi={args.phi}, Ozaki-INT8 s={s}",
-                   "M": M, "N": N, "K": K, "slices": s, "pairs": pairs(s),
-                   "l2": "inputs larger than L2 (512 MiB per matrix), no flush",
+        "config": {"workload": f"{wname}, Ozaki-INT8 s={s}",
+                   "M": M, "N": N, "K": K, "alpha": alpha, "beta": beta, "phi": args.phi, "scale_s": smax,
+                   "slices": s, "pairs": pairs(s),
+                   "l2": f"inputs larger than L2 (A {8 * M * K / 2**20:.0f} MiB), no flush",
                    "parallelism": f"replicas x{world}"},
         "accuracy": {"max_componentwise_err": {"ozaki": errs[s], "native_fp64": err_fp64, "cublas": err_cublas},
                      "ozaki_by_slices": errs, "rows_checked": len(rows),
@@ -434,7 +468,7 @@ def run_ours(args) -> None:
                           "achieved": flop / (fp64_ms * 1e-3) / 1e12, "peak": DMMA_PEAK_TFLOPS,
                           "unit": "TFLOP/s (FP64)", "frac": flop / (fp64_ms * 1e-3) / 1e12 / DMMA_PEAK_TFLOPS,
                           "peak_source": "measured mma.sync f64 throughput (profiles/dmma_peak_b200.md)"},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * M * N,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * (M * K + K * N + M * N),
                 "d2h_bytes_per_step": 8 * M * N, "ms_per_step": e2e_ms,
                 "path": "lt_dgemm_ozaki C ABI, pinned host buffers, H2D A,B,C0 + D2H C in the timed region"},
         "cpu_baseline": cpu,
@@ -453,6 +487,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--size", type=int, default=8192)
+    ap.add_argument("--workload", choices=list(WORKLOADS), default="square",
+                    help="square: size^3, alpha=1.5, beta=0.5 (the headline); tall: 65536x64x4096 and longk: "
+                         "2048x2048x65536, alpha=1, beta=0, rows of A / columns of B scaled by 2^s, s ~ U{-64..64}")
     ap.add_argument("--phi", type=int, default=0)
     ap.add_argument("--slices", type=int, default=0, help="fix the slice count (0 = accuracy-matched)")
     ap.add_argument("--check-rows", type=int, default=16)

@@ -65,6 +65,8 @@ const Entry kConfigs[] = {
     {"tma_64x64_s8", launch<Config<64, 64, 8, true>>, 64, 64, true},
     {"tma_64x32_s8", launch<Config<64, 32, 8, true>>, 64, 32, true},
     {"tma_32x64_s8", launch<Config<32, 64, 8, true>>, 32, 64, true},
+    {"tma_128x64_s4", launch<Config<128, 64, 4, true>>, 128, 64, true},
+    {"tma_64x64_s4", launch<Config<64, 64, 4, true>>, 64, 64, true},
     {"cpa_128x64_s6", launch<Config<128, 64, 6, false>>, 128, 64, false},
     {"cpa_64x64_s6", launch<Config<64, 64, 6, false>>, 64, 64, false},
     {"cpa_64x32_s6", launch<Config<64, 32, 6, false>>, 64, 32, false},
@@ -140,6 +142,11 @@ const GroupedEntry kGrouped[] = {
     {"grouped_cpa_64x64_s6", launch_grouped<Config<64, 64, 6, false>>, 64, 64},
     {"grouped_cpa_64x32_s6", launch_grouped<Config<64, 32, 6, false>>, 64, 32},
     {"grouped_cpa_32x32_s6", launch_grouped<Config<32, 32, 6, false>>, 32, 32},
+    // shallower rings leave room for more CTAs per SM (more warps to hide load latency)
+    {"grouped_cpa_64x64_s3", launch_grouped<Config<64, 64, 3, false>>, 64, 64},
+    {"grouped_cpa_64x32_s3", launch_grouped<Config<64, 32, 3, false>>, 64, 32},
+    {"grouped_cpa_32x64_s3", launch_grouped<Config<32, 64, 3, false>>, 32, 64},
+    {"grouped_cpa_32x32_s3", launch_grouped<Config<32, 32, 3, false>>, 32, 32},
 };
 constexpr int kNumGrouped = static_cast<int>(sizeof(kGrouped) / sizeof(kGrouped[0]));
 
