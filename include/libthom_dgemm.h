@@ -97,6 +97,19 @@ int lt_ozaki_product(double* C, int64_t M, int64_t N, int64_t K, double alpha, d
 int lt_dgemm_cublas(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
                     double alpha, double beta, void* stream);
 
+/* Allocation-free Ozaki DGEMM. No counterpart in the reference. For callers that cannot allocate
+ * device memory (a framework whose own pool owns the GPU, a service that must not allocate on its
+ * request path, a process under a hard memory cap): its scratch is a fixed device array of
+ * LT_OZAKI_NOALLOC_BYTES that the library holds on every GPU it is loaded on until the process exits,
+ * so no call allocates or frees anything. Problems whose scratch would exceed that size
+ * (lt_ozaki_workspace_size) are rejected with LT_ERR_INVALID_ARGUMENT. The first call on a device
+ * looks up the array's device address (once per device). All calls on a device share the array:
+ * calls whose work overlaps on the GPU (other streams, other host threads) race on it. Results are
+ * bit-identical to lt_dgemm_ozaki. Stream-ordered like lt_dgemm_ozaki. */
+#define LT_OZAKI_NOALLOC_BYTES (32ll << 20)
+int lt_dgemm_ozaki_noalloc(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
+                           double alpha, double beta, int slices, void* stream);
+
 /* ---- grouped / batched DGEMM (the `dgemmb` routine) ----------------------------------------- */
 typedef struct lt_gemm_problem {
   int64_t M, N, K;

@@ -977,5 +977,114 @@ void grouped_destroy(Grouped* G) {
 
 int64_t grouped_tiles(const Grouped* G) { return G->ntiles; }
 
+// ---------------------------------------------------------------------------------------------
+// Allocation-free Ozaki DGEMM (lt_dgemm_ozaki_noalloc).
+//
+// For callers that cannot allocate device memory themselves or let a library do it — frameworks
+// whose own pool owns every byte of the GPU, services that must not allocate on their request path,
+// processes under a hard memory cap — this entry point keeps its scratch (row/column exponents and
+// INT8 slice tiles) in a fixed array declared at file scope below. Every GPU that loads the library
+// holds LT_OZAKI_NOALLOC_BYTES of device memory for it until the process exits. The array is shared
+// by every call on a device and keeps the last call's contents; each call clears the exponent
+// region it needs and overwrites the slice tiles it reads, so nothing leaks between calls, but two
+// calls whose work overlaps on the GPU (different streams, or host threads) race on the array.
+// ---------------------------------------------------------------------------------------------
+static __device__ __align__(256) uint8_t g_noalloc_scratch[LT_OZAKI_NOALLOC_BYTES];
+static __device__ DeviceStatus g_noalloc_status;
+
+namespace {
+
+struct NoAllocDevice {
+  std::once_flag once;
+  cudaError_t err = cudaSuccess;
+  void* scratch = nullptr;     // device address of g_noalloc_scratch on this device
+  DeviceStatus* status = nullptr;
+  int sm_count = 0;
+};
+NoAllocDevice g_noalloc[64];
+
+// Per-device set-up on the first call made with that device current. In host code the symbols'
+// names are host-side stand-ins, so their device addresses come from cudaGetSymbolAddress.
+int noalloc_setup(int dev, NoAllocDevice** out) {
+  NoAllocDevice& d = g_noalloc[dev];
+  std::call_once(d.once, [&] {
+    d.err = cudaGetSymbolAddress(&d.scratch, g_noalloc_scratch);
+    if (d.err == cudaSuccess) d.err = cudaGetSymbolAddress(reinterpret_cast<void**>(&d.status), g_noalloc_status);
+    if (d.err == cudaSuccess) d.err = cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev);
+  });
+  if (d.err != cudaSuccess)
+    return set_error(LT_ERR_CUDA, "static scratch set-up failed: %s", cudaGetErrorString(d.err));
+  *out = &d;
+  return LT_OK;
+}
+
+}  // namespace
+
+int noalloc_run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
+                double beta, int s, cudaStream_t stream) {
+  int dev = -1;
+  LT_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return set_error(LT_ERR_INVALID_ARGUMENT, "device %d out of range", dev);
+  int major = 0;
+  LT_CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+  if (major != 10) return set_error(LT_ERR_UNSUPPORTED, "device %d is not an sm_100 device", dev);
+  const Layout L = layout_for(M, N, K, s);
+  if (L.total > static_cast<size_t>(LT_OZAKI_NOALLOC_BYTES))
+    return set_error(LT_ERR_INVALID_ARGUMENT,
+                     "%lld x %lld x %lld with %d slices needs %zu bytes of scratch; the static scratch holds %lld",
+                     static_cast<long long>(M), static_cast<long long>(N), static_cast<long long>(K), s, L.total,
+                     static_cast<long long>(LT_OZAKI_NOALLOC_BYTES));
+  NoAllocDevice* nd = nullptr;
+  LT_TRY(noalloc_setup(dev, &nd));
+  DeviceContext ctx;  // a stack description of the device: nothing is allocated
+  ctx.device = dev;
+  ctx.sm_count = nd->sm_count;
+  ctx.status = nd->status;
+  uint8_t* ws = static_cast<uint8_t*>(nd->scratch);
+  auto* amax_a = reinterpret_cast<unsigned long long*>(ws + L.off_amax_a);
+  auto* amax_b = reinterpret_cast<unsigned long long*>(ws + L.off_amax_b);
+  auto* sa = reinterpret_cast<int8_t*>(ws + L.off_sa);
+  auto* sb = reinterpret_cast<int8_t*>(ws + L.off_sb);
+  // exponents start from zero (atomicMax); the slice tiles are fully rewritten by the split
+  LT_CUDA_TRY(cudaMemsetAsync(ws, 0, L.off_sa, stream));
+  const int sms = ctx.sm_count;
+  if (K > 0) {
+    int64_t row_blocks = (M + 7) / 8;
+    int64_t ksplit = (4 * sms + row_blocks - 1) / row_blocks;
+    ksplit = ksplit < 1 ? 1 : ksplit;
+    int64_t kseg = round_up((K + ksplit - 1) / ksplit, 256);
+    ksplit = (K + kseg - 1) / kseg;
+    amax_rows_kernel<<<dim3(static_cast<unsigned>(row_blocks), static_cast<unsigned>(ksplit)), 256, 0, stream>>>(
+        A, M, K, kseg, amax_a);
+    LT_CUDA_TRY(cudaGetLastError());
+    int64_t col_blocks = (N + 255) / 256;
+    int64_t ksplit_b = (8 * sms + col_blocks - 1) / col_blocks;
+    ksplit_b = ksplit_b < 1 ? 1 : ksplit_b;
+    int64_t kseg_b = (K + ksplit_b - 1) / ksplit_b;
+    ksplit_b = (K + kseg_b - 1) / kseg_b;
+    amax_cols_kernel<<<dim3(static_cast<unsigned>(col_blocks), static_cast<unsigned>(ksplit_b)), 256, 0, stream>>>(
+        B, K, N, kseg_b, amax_b);
+    LT_CUDA_TRY(cudaGetLastError());
+  }
+  LT_TRY(launch_split(s, A, B, M, N, K, L, amax_a, amax_b, sa, sb, sms, stream));
+  OzProblem pr{sa, sb, C, amax_a, amax_b, M, N, L.NC, L.RBa, L.RBb, alpha, beta};
+  return launch_gemm<false>(s, pr, L.RBa * L.RBb, &ctx, stream);
+}
+
 }  // namespace ozaki
 }  // namespace lt
+
+extern "C" int lt_dgemm_ozaki_noalloc(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
+                                      double alpha, double beta, int slices, void* stream) {
+  if (M < 0 || N < 0 || K < 0 || M > 0x7fffffff || N > 0x7fffffff || K > 0x7fffffff)
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "bad dimensions");
+  if ((M > 0 && K > 0 && A == nullptr) || (K > 0 && N > 0 && B == nullptr) || (M > 0 && N > 0 && C == nullptr))
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "null matrix pointer");
+  if (((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(C)) & 7) != 0)
+    return lt::set_error(LT_ERR_UNALIGNED, "matrix pointers must be 8-byte aligned");
+  if (slices < 1 || slices > LT_OZAKI_MAX_SLICES)
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "slice count %d outside [1, %d]", slices, LT_OZAKI_MAX_SLICES);
+  if (M == 0 || N == 0) return lt::ok();
+  LT_TRY(lt::ozaki::noalloc_run(A, B, C, M, N, K, alpha, beta, slices, reinterpret_cast<cudaStream_t>(stream)));
+  return lt::ok();
+}
