@@ -179,11 +179,16 @@ void lt_set_ozaki_tolerance(double tol);
  * (e(max) - e(min nonzero)) within a row of A plus the largest within a column of B. Returns 0 on
  * bad arguments. */
 int lt_ozaki_analytic_slices(double tol, int gap_bits);
-/* Slice count the selector picks for this problem (learned when weights are installed and the
- * prediction is confident, analytic otherwise). Synchronous. */
+/* gap_bits of a problem (the analytic count's input), measured on the device. Synchronous. */
+int lt_ozaki_gap_bits(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int* gap_bits,
+                      void* stream);
+/* Slice count the selector picks for this problem: the learned choice when weights are installed,
+ * the network is confident and predicts fewer than 10 slices; the analytic count otherwise.
+ * Synchronous. */
 int lt_ozaki_select_slices(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol,
                            int* slices, void* stream);
-/* Same, also reporting whether the learned choice was used and the measured gap_bits. */
+/* Same, also reporting whether the learned choice was used and the measured gap_bits (-1 when the
+ * learned choice was used and no gap was measured). */
 int lt_ozaki_select_info(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol,
                          int* slices, int* learned, int* gap_bits, void* stream);
 

@@ -103,6 +103,7 @@ SIGNATURES = {
     "lt_selector_set_params": (_i32, [_vp]),
     "lt_set_ozaki_tolerance": (None, [_f64]),
     "lt_ozaki_analytic_slices": (_i32, [_f64, _i32]),
+    "lt_ozaki_gap_bits": (_i32, [_vp, _vp, _i64, _i64, _i64, _c.POINTER(_i32), _vp]),
     "lt_ozaki_select_slices": (_i32, [_vp, _vp, _i64, _i64, _i64, _f64, _c.POINTER(_i32), _vp]),
     "lt_ozaki_select_info": (_i32, [_vp, _vp, _i64, _i64, _i64, _f64, _c.POINTER(_i32), _c.POINTER(_i32),
                                     _c.POINTER(_i32), _vp]),

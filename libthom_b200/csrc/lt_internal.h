@@ -21,6 +21,14 @@ int run_config(int cfg, const double* A, const double* B, double* C, int64_t M, 
                double beta, cudaStream_t stream);
 }  // namespace fp64
 
+// Selector statistics (selector_stats.cu). features_into needs kStatsScratchBytes of scratch,
+// gap_into 8 (M + N) bytes and a zeroed pair of ints at `out` (row gap, column gap).
+constexpr size_t kStatsScratchBytes = 4096;
+int features_into(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, float* feat,
+                  void* scratch, cudaStream_t stream);
+int gap_into(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int* out, void* scratch,
+             cudaStream_t stream);
+
 namespace tuner {
 // Tuned FP64 config for this shape class, or -1.
 int lookup(int64_t M, int64_t N, int64_t K, bool tma);

@@ -1,10 +1,11 @@
 // selector.cu — learned slice-count selector for the Ozaki DGEMM (no reference counterpart).
 //
-// Features (34 floats per problem): a 16-bin histogram of exponent gaps in sampled rows of A, the same
-// for sampled columns of B, log2 K / 16 and -log10(tol) / 16. The gap of a nonzero entry is how many
-// binades it sits below the largest entry of its row (column): g = e(max) - e(x), bins of width 4
-// (g >= 60 in the last bin); zeros count in bin 0. The gap is what the per-row power-of-two scaling
-// costs in precision, so the histograms carry what decides the slice count.
+// Features (34 floats per problem, computed in selector_stats.cu): a 16-bin histogram of exponent
+// gaps in sampled rows of A, the same for sampled columns of B, log2 K / 16 and -log10(tol) / 16. The
+// gap of a nonzero entry is how many binades it sits below the largest entry of its row (column):
+// g = e(max) - e(x), bins of width 4 (g >= 60 in the last bin); zeros count in bin 0. The gap is what
+// the per-row power-of-two scaling costs in precision, so the histograms carry what decides the
+// slice count.
 //
 // Network: 34 -> 64 -> 64 -> 8, GELU (tanh form: 0.5 x (1 + tanh(sqrt(2/pi)(x + 0.044715 x^3)))),
 // softmax over slice counts 3..10, cross-entropy loss, Adam. Forward, backward and the optimizer
@@ -29,90 +30,6 @@ namespace sel {
 constexpr int F = LT_SEL_FEATURES, H = LT_SEL_HIDDEN, C = LT_SEL_CLASSES, P = LT_SEL_PARAMS;
 constexpr int OW1 = 0, OB1 = OW1 + H * F, OW2 = OB1 + H, OB2 = OW2 + H * H, OW3 = OB2 + H, OB3 = OW3 + C * H;
 static_assert(OB3 + C == P, "parameter layout");
-constexpr int kSampleRows = 128;
-constexpr int kColGroups = 4;  // sampled groups of 32 consecutive columns of B
-
-__device__ __forceinline__ int exp_of(double v) {
-  int e;
-  frexp(v, &e);
-  return e;
-}
-
-__device__ __forceinline__ int gap_bin(int g) { return g >= 60 ? 15 : (g < 0 ? 0 : g >> 2); }
-
-// One block per sampled row of A: max exponent, then the gap histogram (block-local, then global).
-__global__ void row_hist_kernel(const double* __restrict__ A, int64_t M, int64_t K, int rows,
-                                unsigned int* __restrict__ hist) {
-  __shared__ int s_max;
-  __shared__ unsigned int s_hist[16];
-  const int64_t row = (rows > 1) ? (static_cast<int64_t>(blockIdx.x) * (M - 1)) / (rows - 1) : 0;
-  if (threadIdx.x == 0) s_max = -100000;
-  if (threadIdx.x < 16) s_hist[threadIdx.x] = 0;
-  __syncthreads();
-  const double* a = A + row * K;
-  int m = -100000;
-  for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
-    double v = fabs(a[k]);
-    if (v != 0.0 && isfinite(v)) m = max(m, exp_of(v));
-  }
-  atomicMax(&s_max, m);
-  __syncthreads();
-  const int em = s_max;
-  for (int64_t k = threadIdx.x; k < K; k += blockDim.x) {
-    double v = fabs(a[k]);
-    int b = (v != 0.0 && isfinite(v)) ? gap_bin(em - exp_of(v)) : 0;
-    atomicAdd(&s_hist[b], 1u);
-  }
-  __syncthreads();
-  if (threadIdx.x < 16) atomicAdd(&hist[threadIdx.x], s_hist[threadIdx.x]);
-}
-
-// One block (8 warps) per sampled group of 32 consecutive columns of B; lane = column.
-__global__ void col_hist_kernel(const double* __restrict__ B, int64_t K, int64_t N, int groups,
-                                unsigned int* __restrict__ hist) {
-  __shared__ int s_max[32];
-  __shared__ unsigned int s_hist[16];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int64_t span = N > 32 ? N - 32 : 0;
-  const int64_t c0 = (groups > 1) ? (static_cast<int64_t>(blockIdx.x) * span) / (groups - 1) : 0;
-  const int64_t col = c0 + lane;
-  if (threadIdx.x < 32) s_max[threadIdx.x] = -100000;
-  if (threadIdx.x < 16) s_hist[threadIdx.x] = 0;
-  __syncthreads();
-  int m = -100000;
-  if (col < N)
-    for (int64_t k = warp; k < K; k += nwarps) {
-      double v = fabs(B[k * N + col]);
-      if (v != 0.0 && isfinite(v)) m = max(m, exp_of(v));
-    }
-  atomicMax(&s_max[lane], m);
-  __syncthreads();
-  const int em = s_max[lane];
-  if (col < N)
-    for (int64_t k = warp; k < K; k += nwarps) {
-      double v = fabs(B[k * N + col]);
-      int b = (v != 0.0 && isfinite(v)) ? gap_bin(em - exp_of(v)) : 0;
-      atomicAdd(&s_hist[b], 1u);
-    }
-  __syncthreads();
-  if (threadIdx.x < 16) atomicAdd(&hist[threadIdx.x], s_hist[threadIdx.x]);
-}
-
-__global__ void features_finish_kernel(const unsigned int* __restrict__ hist, int64_t K, double tol,
-                                       float* __restrict__ feat) {
-  const int t = threadIdx.x;
-  if (t < 32) {
-    const unsigned int* h = hist + (t < 16 ? 0 : 16);
-    unsigned long long tot = 0;
-    for (int i = 0; i < 16; ++i) tot += h[i];
-    feat[t] = tot ? static_cast<float>(static_cast<double>(hist[t]) / static_cast<double>(tot)) : 0.f;
-  } else if (t == 32) {
-    feat[32] = static_cast<float>(log2(static_cast<double>(K > 0 ? K : 1)) / 16.0);
-  } else if (t == 33) {
-    feat[33] = static_cast<float>(-log10(tol) / 16.0);
-  }
-}
-
 // ---------------------------------------------------------------------------------------------
 // MLP
 // ---------------------------------------------------------------------------------------------
@@ -305,71 +222,6 @@ int analytic(double tol, int gap_bits) {
   return LT_OZAKI_MAX_SLICES;
 }
 
-// Largest exponent gap of any row of A: e(max |a|) - e(min nonzero |a|), one warp per row.
-__global__ void row_gap_kernel(const double* __restrict__ A, int64_t M, int64_t K, int* __restrict__ out) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
-  int best = 0;
-  for (int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; row < M; row += warps) {
-    int emax = -100000, emin = 100000;
-    for (int64_t k = lane; k < K; k += 32) {
-      double v = fabs(A[row * K + k]);
-      if (v != 0.0 && isfinite(v)) {
-        int e = exp_of(v);
-        emax = max(emax, e);
-        emin = min(emin, e);
-      }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      emax = max(emax, __shfl_xor_sync(0xffffffffu, emax, o));
-      emin = min(emin, __shfl_xor_sync(0xffffffffu, emin, o));
-    }
-    if (emax >= emin) best = max(best, emax - emin);
-  }
-  if (lane == 0) atomicMax(out, best);
-}
-
-// Largest exponent gap of any column of B, one thread per column.
-__global__ void col_gap_kernel(const double* __restrict__ B, int64_t K, int64_t N, int* __restrict__ out) {
-  int best = 0;
-  for (int64_t col = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; col < N;
-       col += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    int emax = -100000, emin = 100000;
-    for (int64_t k = 0; k < K; ++k) {
-      double v = fabs(B[k * N + col]);
-      if (v != 0.0 && isfinite(v)) {
-        int e = exp_of(v);
-        emax = max(emax, e);
-        emin = min(emin, e);
-      }
-    }
-    if (emax >= emin) best = max(best, emax - emin);
-  }
-  for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, best);
-}
-
-// Learned choice: the smallest slice count whose cumulative predicted probability reaches 0.9,
-// used only when the network is confident (largest class probability >= 0.5) and never above the
-// analytic count; otherwise the analytic count.
-int decide(const float* probs, int s_analytic, bool* learned) {
-  float mx = 0.f;
-  for (int c = 0; c < C; ++c) mx = fmaxf(mx, probs[c]);
-  *learned = false;
-  if (!(mx >= 0.5f)) return s_analytic;
-  float cdf = 0.f;
-  for (int c = 0; c < C; ++c) {
-    cdf += probs[c];
-    if (cdf >= 0.9f) {
-      int s = 3 + c;
-      if (s > s_analytic) return s_analytic;
-      *learned = true;
-      return s;
-    }
-  }
-  return s_analytic;
-}
-
 // Trained weights shipped beside the library (selector_weights.bin, LT_SEL_PARAMS floats), or the
 // file named by LIBTHOM_SELECTOR_WEIGHTS; loaded once unless the caller installed weights (or
 // explicitly none) with lt_selector_set_params.
@@ -423,41 +275,70 @@ int device_params(const float** out) {
   return LT_OK;
 }
 
+// Learned choice from the network's class probabilities (slice counts 3..10, the last class
+// standing for "10 or more"): the smallest count whose cumulative probability reaches 0.9, if the
+// network is confident (top class >= 0.5) and neither the top class nor that count is the last
+// class. Returns false when the analytic fallback must decide.
+bool decide(const float* probs, int* slices) {
+  int top = 0;
+  for (int c = 1; c < C; ++c)
+    if (probs[c] > probs[top]) top = c;
+  if (!(probs[top] >= 0.5f) || top == C - 1) return false;
+  float cdf = 0.f;
+  for (int c = 0; c < C - 1; ++c) {
+    cdf += probs[c];
+    if (cdf >= 0.9f) {
+      *slices = 3 + c;
+      return true;
+    }
+  }
+  return false;
+}
+
 // Slice count for one problem (synchronous: the count decides the workspace layout and launches).
+// The exponent-gap pass that feeds the analytic count runs only when the learned choice is not
+// used; *gap_bits is -1 then.
 int select(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, int* slices,
            bool* learned, int* gap_bits, cudaStream_t stream) {
   DeviceContext* ctx = context();
   if (ctx == nullptr) return last_error();
   const float* params = nullptr;
   LT_TRY(device_params(&params));
-  struct Scr {
-    float feat[F];
-    float probs[C];
-    int gaps[2];
-  };
-  Scr* d = nullptr;
-  LT_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(Scr), stream));
-  cudaError_t e = cudaMemsetAsync(d, 0, sizeof(Scr), stream);
-  if (e == cudaSuccess) {
-    row_gap_kernel<<<ctx->sm_count * 4, 256, 0, stream>>>(A, M, K, &d->gaps[0]);
-    col_gap_kernel<<<static_cast<unsigned>((N + 255) / 256), 256, 0, stream>>>(B, K, N, &d->gaps[1]);
-    e = cudaGetLastError();
-  }
+  *learned = false;
+  *gap_bits = -1;
+  const size_t head = kStatsScratchBytes + 256;
+  uint8_t* d = nullptr;
+  LT_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&d), head + 8 * (M + N), stream));
+  float* feat = reinterpret_cast<float*>(d + kStatsScratchBytes);   // 34 floats
+  float* probs = feat + 48;                                          // 8 floats
+  int* gap = reinterpret_cast<int*>(probs + 8);                      // 2 ints
   int rc = LT_OK;
-  if (e == cudaSuccess && params != nullptr) {
-    rc = lt_ozaki_features(A, B, M, N, K, tol, d->feat, stream);
-    if (rc == LT_OK) rc = lt_mlp_forward(params, d->feat, 1, d->probs, stream);
+  cudaError_t e = cudaSuccess;
+  if (params != nullptr) {
+    rc = features_into(A, B, M, N, K, tol, feat, d, stream);
+    if (rc == LT_OK) {
+      mlp_forward_kernel<<<1, H, 0, stream>>>(params, feat, 1, probs);
+      e = cudaGetLastError();
+    }
+    float hp[C];
+    if (rc == LT_OK && e == cudaSuccess) e = cudaMemcpyAsync(hp, probs, sizeof hp, cudaMemcpyDeviceToHost, stream);
+    if (rc == LT_OK && e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (rc == LT_OK && e == cudaSuccess) *learned = decide(hp, slices);
   }
-  Scr h;
-  if (e == cudaSuccess && rc == LT_OK) e = cudaMemcpyAsync(&h, d, sizeof(Scr), cudaMemcpyDeviceToHost, stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (rc == LT_OK && e == cudaSuccess && !*learned) {
+    e = cudaMemsetAsync(gap, 0, 2 * sizeof(int), stream);
+    if (e == cudaSuccess) rc = gap_into(A, B, M, N, K, gap, d + head, stream);
+    int hg[2] = {0, 0};
+    if (rc == LT_OK && e == cudaSuccess) e = cudaMemcpyAsync(hg, gap, sizeof hg, cudaMemcpyDeviceToHost, stream);
+    if (rc == LT_OK && e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (rc == LT_OK && e == cudaSuccess) {
+      *gap_bits = hg[0] + hg[1];
+      *slices = analytic(tol, *gap_bits);
+    }
+  }
   cudaFreeAsync(d, stream);
   if (rc != LT_OK) return rc;
   if (e != cudaSuccess) return set_error(LT_ERR_CUDA, "slice selection: %s", cudaGetErrorString(e));
-  *gap_bits = h.gaps[0] + h.gaps[1];
-  const int sa = analytic(tol, *gap_bits);
-  *slices = params != nullptr ? decide(h.probs, sa, learned) : sa;
-  if (params == nullptr) *learned = false;
   return LT_OK;
 }
 
@@ -465,26 +346,6 @@ int select(const double* A, const double* B, int64_t M, int64_t N, int64_t K, do
 }  // namespace lt
 
 extern "C" {
-
-int lt_ozaki_features(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, float* features,
-                      void* stream) {
-  if (M <= 0 || N <= 0 || K <= 0 || A == nullptr || B == nullptr || features == nullptr || !(tol > 0.0))
-    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_ozaki_features: bad arguments");
-  if (lt::context() == nullptr) return lt::last_error();
-  cudaStream_t s = lt::as_stream(stream);
-  unsigned int* hist = nullptr;
-  LT_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&hist), 32 * sizeof(unsigned int), s));
-  LT_CUDA_TRY(cudaMemsetAsync(hist, 0, 32 * sizeof(unsigned int), s));
-  const int rows = static_cast<int>(M < lt::sel::kSampleRows ? M : lt::sel::kSampleRows);
-  const int groups = static_cast<int>((N + 31) / 32 < lt::sel::kColGroups ? (N + 31) / 32 : lt::sel::kColGroups);
-  lt::sel::row_hist_kernel<<<rows, 256, 0, s>>>(A, M, K, rows, hist);
-  lt::sel::col_hist_kernel<<<groups, 256, 0, s>>>(B, K, N, groups, hist + 16);
-  lt::sel::features_finish_kernel<<<1, 64, 0, s>>>(hist, K, tol, features);
-  cudaError_t e = cudaGetLastError();
-  cudaFreeAsync(hist, s);
-  if (e != cudaSuccess) return lt::set_error(LT_ERR_CUDA, "features: %s", cudaGetErrorString(e));
-  return lt::ok();
-}
 
 int lt_mlp_forward(const float* params, const float* x, int batch, float* probs, void* stream) {
   if (params == nullptr || x == nullptr || probs == nullptr || batch <= 0)

@@ -3,13 +3,14 @@
 Data: seeded matrices with shapes from the library's three DGEMM families, capped at 2048 per
 dimension — square (M = N = K), tall-skinny (large M, small N) and long-K — with exponent spread
 phi ~ U{0..64} and, for the last two families, rows of A / columns of B scaled by 2^s with
-s ~ U{-smax..smax}. Each matrix is run through the Ozaki kernels at s = 3..10; its componentwise
-error max |C_s - C_64| / (|alpha||A||B|) against the native FP64 result C_64 labels it, for each
-tolerance in {1e-12, 1e-14, 1e-15}, with the smallest s meeting the tolerance (class s - 3; 7 when
-none does). Features come from lt_ozaki_features; training runs lt_mlp_train_step (hand-written
-forward, backward and Adam kernels). The held-out set reports the tolerance-miss rate of the
-learned choice (with and without the analytic fallback), the mean slices saved against the
-analytic count and end-to-end throughput against fixed-slice Ozaki and native FP64.
+s ~ U{-smax..smax}. Each matrix is run through the Ozaki kernels; its componentwise error max |C_s - C_64| / (|alpha||A||B|) against the native FP64 result C_64 is measured for
+s = 3..12; for each tolerance in {1e-12, 1e-14, 1e-15} the label is the smallest s meeting it,
+as class min(s, 10) - 3 (class 7 = "10 or more slices, or none": the library falls back to the
+analytic count there). Features come from lt_ozaki_features; training runs lt_mlp_train_step
+(hand-written forward, backward and Adam kernels). The held-out set reports the tolerance-miss rate
+of the analytic count, of the learned choice alone and of the library's final choice (learned, or
+analytic on fallback), the mean slice counts, and end-to-end throughput (selection included)
+against fixed-slice Ozaki and native FP64.
 
     python -m libthom_b200.selector_train [--train 20000] [--test 2000] [--out PATH]
 """
@@ -27,7 +28,8 @@ import numpy as np
 import libthom_b200 as lt
 
 TOLS = (1e-12, 1e-14, 1e-15)
-SLICES = list(range(3, 11))
+SLICES = list(range(3, 13))   # slice counts whose error is measured
+CLASS_TOP = 10                 # classes 3..10, the last one meaning ">= 10 or unreachable"
 WEIGHTS = Path(__file__).resolve().parent / "selector_weights.bin"
 
 
@@ -89,19 +91,17 @@ class Generator:
         return self.feat.cpu().numpy().copy()
 
     def analytic(self, M, N, K, tol):
-        s = ctypes.c_int()
-        learned = ctypes.c_int()
+        """(analytic slice count, gap_bits) — independent of any installed weights."""
         gap = ctypes.c_int()
-        lt.check(lt.lib().lt_ozaki_select_info(self.A.data_ptr(), self.B.data_ptr(), M, N, K, tol, ctypes.byref(s),
-                                               ctypes.byref(learned), ctypes.byref(gap), None))
-        return s.value, gap.value
+        lt.check(lt.lib().lt_ozaki_gap_bits(self.A.data_ptr(), self.B.data_ptr(), M, N, K, ctypes.byref(gap), None))
+        return int(lt.lib().lt_ozaki_analytic_slices(tol, gap.value)), gap.value
 
 
 def label_of(errs, tol):
     for s, e in zip(SLICES, errs):
         if e <= tol:
-            return s - 3
-    return len(SLICES) - 1
+            return min(s, CLASS_TOP) - 3
+    return CLASS_TOP - 3
 
 
 def build_dataset(torch, gen, n, seed, log_every=0):
@@ -178,76 +178,100 @@ def predict(torch, params, X):
     return out.cpu().numpy()
 
 
+def learned_only(probs):
+    """The network's own answer: smallest s whose cumulative probability reaches 0.9."""
+    return 3 + int(np.argmax(np.cumsum(probs) >= 0.9))
+
+
 def decide(probs, s_analytic):
-    """The library's rule (selector.cu, decide): CDF >= 0.9 if the top class has >= 0.5, clamped to
-    the analytic count; analytic otherwise. Returns (slices, learned?)."""
-    if probs.max() < 0.5:
+    """The library's rule (selector.cu, decide): the learned count if the top class has >= 0.5 and
+    neither it nor the 0.9-quantile is the last class; the analytic count otherwise.
+    Returns (slices, learned?)."""
+    top = int(np.argmax(probs))
+    if probs[top] < 0.5 or top == len(probs) - 1:
         return s_analytic, False
-    cdf = np.cumsum(probs)
-    c = int(np.argmax(cdf >= 0.9))
-    s = 3 + c
-    if s > s_analytic:
+    c = int(np.argmax(np.cumsum(probs) >= 0.9))
+    if c == len(probs) - 1:
         return s_analytic, False
-    return s, True
+    return 3 + c, True
 
 
 def evaluate(torch, gen, params, rows):
     X, Y = expand(rows)
     P = predict(torch, params, X)
-    out = dict(samples=len(Y))
-    miss_learned = miss_final = 0
-    saved = []
+    n = len(Y)
+    miss = dict(analytic=0, learned_only=0, final=0)
+    slices = dict(analytic=[], learned_only=[], final=[])
     used_learned = 0
     per_tol = {}
-    k = 0
     chosen = []
+    k = 0
+
+    def err(r, s):
+        return r["errs"][s - 3] if 3 <= s <= 12 else float("inf")
+
     for r in rows:
         gen.problem(r["M"], r["N"], r["K"], r["phi"], r["smax"], r["seed"])
         for tol in TOLS:
-            s_a, _ = gen.analytic(r["M"], r["N"], r["K"], tol)
-            s_raw = 3 + int(np.argmax(np.cumsum(P[k]) >= 0.9))
-            s_final, learned = decide(P[k], s_a)
-            err = lambda s: r["errs"][s - 3] if 3 <= s <= 10 else (0.0 if s > 10 else float("inf"))
-            miss_learned += err(s_raw) > tol
-            miss_final += err(s_final) > tol
+            s_a, gap = gen.analytic(r["M"], r["N"], r["K"], tol)
+            s_l = learned_only(P[k])
+            s_f, learned = decide(P[k], s_a)
+            for name, sv in (("analytic", s_a), ("learned_only", s_l), ("final", s_f)):
+                miss[name] += err(r, sv) > tol
+                slices[name].append(sv)
             used_learned += learned
-            saved.append(s_a - s_final)
-            d = per_tol.setdefault(tol, dict(n=0, miss=0, saved=0.0, analytic=0.0, chosen=0.0))
+            d = per_tol.setdefault(str(tol), dict(n=0, miss_analytic=0, miss_final=0, analytic=0.0, final=0.0,
+                                                 reachable=0))
             d["n"] += 1
-            d["miss"] += err(s_final) > tol
-            d["saved"] += s_a - s_final
+            d["miss_analytic"] += err(r, s_a) > tol
+            d["miss_final"] += err(r, s_f) > tol
             d["analytic"] += s_a
-            d["chosen"] += s_final
-            chosen.append((r, tol, s_final, s_a))
+            d["final"] += s_f
+            d["reachable"] += min(r["errs"]) <= tol
+            chosen.append((r, tol, s_f, s_a))
             k += 1
-    n = len(Y)
-    out.update(miss_rate_learned_only=miss_learned / n, miss_rate_with_fallback=miss_final / n,
-               learned_used_fraction=used_learned / n, mean_slices_saved_vs_analytic=float(np.mean(saved)),
-               accuracy_top1=float(np.mean(np.argmax(P, axis=1) == Y)),
-               per_tolerance={str(t): {kk: (vv / d["n"] if kk != "n" else vv) for kk, vv in d.items()}
+    out = dict(samples=n, accuracy_top1=float(np.mean(np.argmax(P, axis=1) == Y)),
+               learned_used_fraction=used_learned / n,
+               miss_rate={kk: v / n for kk, v in miss.items()},
+               mean_slices={kk: float(np.mean(v)) for kk, v in slices.items()},
+               mean_slices_saved_vs_analytic=float(np.mean(np.array(slices["analytic"]) - np.array(slices["final"]))),
+               per_tolerance={t: {kk: (vv / d["n"] if kk != "n" else vv) for kk, vv in d.items()}
                               for t, d in per_tol.items()})
     return out, chosen
 
 
 def throughput(torch, gen, chosen, limit=150):
-    """End-to-end time over held-out problems: learned choice (through dgemm_ozaki_auto's path:
-    selection + Ozaki), the analytic count, fixed s = 10, and native FP64."""
+    """End-to-end time over held-out problems, selection included: the library's selector
+    (lt_ozaki_select_slices, then Ozaki), the analytic count (gap pass, then Ozaki), fixed s = 8 and
+    s = 10, and native FP64."""
     L = lt.lib()
     A, B, C = gen.A.data_ptr(), gen.B.data_ptr(), gen.C.data_ptr()
-    tot = dict(learned=0.0, analytic=0.0, fixed10=0.0, fp64=0.0)
+    tot = dict(selector=0.0, analytic=0.0, fixed8=0.0, fixed10=0.0, fp64=0.0)
     flops = 0.0
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    sel = ctypes.c_int()
+    gap = ctypes.c_int()
+
+    def via_selector(M, N, K, tol):
+        lt.check(L.lt_ozaki_select_slices(A, B, M, N, K, tol, ctypes.byref(sel), None))
+        lt.check(L.lt_dgemm_ozaki(A, B, C, M, N, K, 1.0, 0.0, sel.value, None))
+
+    def via_analytic(M, N, K, tol):
+        lt.check(L.lt_ozaki_gap_bits(A, B, M, N, K, ctypes.byref(gap), None))
+        s = int(L.lt_ozaki_analytic_slices(tol, gap.value))
+        lt.check(L.lt_dgemm_ozaki(A, B, C, M, N, K, 1.0, 0.0, s, None))
+
     for r, tol, s_final, s_a in chosen[:limit]:
         M, N, K = r["M"], r["N"], r["K"]
         gen.problem(M, N, K, r["phi"], r["smax"], r["seed"])
         flops += 2.0 * M * N * K
         runs = {
-            "learned": lambda: (L.lt_ozaki_select_slices(A, B, M, N, K, tol, ctypes.byref(ctypes.c_int()), None),
-                                L.lt_dgemm_ozaki(A, B, C, M, N, K, 1.0, 0.0, s_final, None)),
-            "analytic": lambda: L.lt_dgemm_ozaki(A, B, C, M, N, K, 1.0, 0.0, s_a, None),
-            "fixed10": lambda: L.lt_dgemm_ozaki(A, B, C, M, N, K, 1.0, 0.0, 10, None),
-            "fp64": lambda: L.lt_dgemm_fp64(A, B, C, M, N, K, 1.0, 0.0, None),
+            "selector": lambda: via_selector(M, N, K, tol),
+            "analytic": lambda: via_analytic(M, N, K, tol),
+            "fixed8": lambda: lt.check(L.lt_dgemm_ozaki(A, B, C, M, N, K, 1.0, 0.0, 8, None)),
+            "fixed10": lambda: lt.check(L.lt_dgemm_ozaki(A, B, C, M, N, K, 1.0, 0.0, 10, None)),
+            "fp64": lambda: lt.check(L.lt_dgemm_fp64(A, B, C, M, N, K, 1.0, 0.0, None)),
         }
         for name, fn in runs.items():
             fn()
@@ -257,7 +281,7 @@ def throughput(torch, gen, chosen, limit=150):
             e1.record()
             e1.synchronize()
             tot[name] += e0.elapsed_time(e1)
-    return {k: flops / (v * 1e-3) / 1e12 for k, v in tot.items()}, {k: v for k, v in tot.items()}
+    return {k: flops / (v * 1e-3) / 1e12 for k, v in tot.items()}, tot
 
 
 def main():
