@@ -207,6 +207,17 @@ int lt_abs_denominator(const double* A, const double* B, const double* C0, doubl
 /* Writes over the whole L2 (twice its size), as the reference's flushL2 (routines/common.cpp:12-24). */
 int lt_flush_l2(void* stream);
 
+/* ---- measured tensor-pipe peaks (roofline denominators; no counterpart in the reference) ------ */
+#define LT_PEAK_FP64_MMA 0      /* mma.sync m16n8k16 f64, operands in registers: FP64 FLOP/s */
+#define LT_PEAK_INT8_MMA_N128 1 /* tcgen05.mma kind::i8 M128 N128 K32, one CTA per SM: INT8 op/s */
+#define LT_PEAK_INT8_MMA_N256 2 /* tcgen05.mma kind::i8 M128 N256 K32, one CTA per SM */
+#define LT_PEAK_INT8_MMA_PAIR 3 /* tcgen05.mma.cta_group::2 kind::i8 M256 N128 K32, CTA pairs */
+/* Runs a loop of the named tensor instruction with its operands on chip (registers, or one
+ * shared-memory tile per operand) on every SM and returns the measured rate of the current device
+ * in *ops_per_second (2 per multiply-add). The tcgen05 kinds first run a check launch with known
+ * operands and return LT_ERR_UNSUPPORTED if any accumulator checked is wrong. Synchronous. */
+int lt_measure_peak(int kind, double* ops_per_second, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,6 +29,10 @@ LT_ERR_NOT_FOUND = 7
 LT_OZAKI_MAX_SLICES = 12
 LT_FORM_FP64 = 0
 LT_FORM_OZAKI = 1
+LT_PEAK_FP64_MMA = 0
+LT_PEAK_INT8_MMA_N128 = 1
+LT_PEAK_INT8_MMA_N256 = 2
+LT_PEAK_INT8_MMA_PAIR = 3
 LT_SEL_FEATURES = 34
 LT_SEL_HIDDEN = 64
 LT_SEL_CLASSES = 8
@@ -113,6 +117,7 @@ SIGNATURES = {
     "lt_componentwise_error": (_i32, [_vp, _vp, _vp, _i64, _f64, _c.POINTER(_f64), _vp]),
     "lt_abs_denominator": (_i32, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _vp]),
     "lt_flush_l2": (_i32, [_vp]),
+    "lt_measure_peak": (_i32, [_i32, _c.POINTER(_f64), _vp]),
 }
 
 _lib = None
@@ -232,3 +237,11 @@ def componentwise_error(C, Cref, den, n: int, tol: float = 0.0, stream=None) -> 
 def abs_denominator(A, B, C0, den, M, N, K, alpha, beta, stream=None) -> None:
     check(lib().lt_abs_denominator(_ptr(A), _ptr(B), None if C0 is None else _ptr(C0), _ptr(den), M, N, K,
                                    alpha, beta, _stream(stream)))
+
+
+def measure_peak(kind: int, stream=None) -> float:
+    """Measured rate (op/s, 2 per multiply-add) of one tensor instruction form on the current
+    device: LT_PEAK_FP64_MMA, LT_PEAK_INT8_MMA_N128, LT_PEAK_INT8_MMA_N256 or LT_PEAK_INT8_MMA_PAIR."""
+    out = ctypes.c_double()
+    check(lib().lt_measure_peak(kind, ctypes.byref(out), _stream(stream)))
+    return out.value

@@ -347,19 +347,9 @@ struct Geo {
   __host__ __device__ static constexpr int cps(int b) { return kStageTiles / (2 * band_of(S, b).nsl); }
 };
 
-// Shared-memory matrix descriptor, K-major, 32-byte swizzle: rows of 32 bytes, 8-row groups
-// 256 bytes apart (SBO), layout type SWIZZLE_32B (6), descriptor version 1. The start address
-// (bits 0..13, in 16-byte units) of consecutive 4 KB tiles differs by 256, so tile t of a stage
-// is desc(stage) + 256 t.
-__device__ __forceinline__ uint64_t desc_k_sw32(uint32_t addr) {
-  uint64_t d = 0;
-  d |= static_cast<uint64_t>((addr >> 4) & 0x3FFFu);
-  d |= static_cast<uint64_t>(1u) << 16;
-  d |= static_cast<uint64_t>(256u >> 4) << 32;
-  d |= static_cast<uint64_t>(1u) << 46;
-  d |= static_cast<uint64_t>(6u) << 61;
-  return d;
-}
+// Tile descriptors: smem_desc_k_sw32 (lt_common.cuh). The start address (bits 0..13, in 16-byte
+// units) of consecutive 4 KB tiles differs by 256, so tile t of a stage is desc(stage) + 256 t.
+__device__ __forceinline__ uint64_t desc_k_sw32(uint32_t addr) { return smem_desc_k_sw32(addr); }
 
 // Contiguous global -> shared bulk copy, completion counted in bytes on `bar`.
 __device__ __forceinline__ void bulk_load(void* smem_dst, const void* gsrc, uint32_t bytes, uint64_t* bar) {

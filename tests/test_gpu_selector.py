@@ -127,7 +127,9 @@ def test_trained_selector_gains_over_analytic(cuda, oracle_mod):
     """Held-out problems (seeds never used in training): with the trained weights the selector
     picks fewer slices than the analytic count on average and still meets the tolerance (checked
     against the compensated oracle, not the FP64 result the labels came from) on all but a small
-    fraction."""
+    fraction of the problems where the tolerance is reachable at all. A problem is unreachable when
+    even the largest slice count misses the tolerance (wide exponent spread in both operands): no
+    choice of s can meet it, so it does not count as a miss of the selector."""
     import libthom_b200 as lt
 
     if not WEIGHTS.exists():
@@ -138,6 +140,12 @@ def test_trained_selector_gains_over_analytic(cuda, oracle_mod):
     torch = cuda
     rng = np.random.default_rng(424242)
     saved, misses, n = [], 0, 0
+
+    def error_at(dA, dB, M, N, K, s, Cref, den):
+        dC = torch.zeros(M, N, dtype=torch.float64, device="cuda")
+        lt.dgemm_ozaki(dA, dB, dC, M, N, K, 1.0, 0.0, slices=s)
+        return oracle_mod.componentwise_error(dC.cpu().numpy(), Cref, den)[0]
+
     for i in range(24):
         M, N, K = (int(rng.integers(64, 257)) for _ in range(3))
         phi = int(rng.integers(0, 65))
@@ -154,13 +162,12 @@ def test_trained_selector_gains_over_analytic(cuda, oracle_mod):
         if not learned:
             assert s == sa
         saved.append(sa - s)
-        dA, dB = to_dev(torch, A), to_dev(torch, B)
-        dC = torch.zeros(M, N, dtype=torch.float64, device="cuda")
-        lt.dgemm_ozaki(dA, dB, dC, M, N, K, 1.0, 0.0, slices=s)
-        err = oracle_mod.componentwise_error(dC.cpu().numpy(), Cref, den)[0]
-        misses += err > tol
+        if error_at(dA, dB, M, N, K, lt.LT_OZAKI_MAX_SLICES, Cref, den) > tol:
+            continue  # unreachable
+        misses += error_at(dA, dB, M, N, K, s, Cref, den) > tol
         n += 1
     assert np.mean(saved) >= 1.0, saved
+    assert n >= 8, n
     assert misses <= 0.15 * n, (misses, n)
 
 
