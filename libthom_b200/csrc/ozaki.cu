@@ -605,6 +605,323 @@ __global__ void __launch_bounds__(kThreads, 1) ozaki_gemm_grouped_kernel(OzGroup
   ozaki_body<S>(src, status);
 }
 
+// ---------------------------------------------------------------------------------------------
+// CTA-pair product kernel (single problem with more than one 128-row block). A cluster of two CTAs
+// computes a 256 x 128 tile with tcgen05.mma.cta_group::2 (M256 N128 K32): CTA rank r holds row
+// block 2i + r of the A slices and rows 64r .. 64r + 63 of the B tile, so each SM's shared memory
+// feeds 6 KB of operands per 64-cycle MMA instead of the 8 KB of a one-CTA M128 N128 MMA, which
+// is the whole 128 B/clk of the port before the bulk copies are counted. Each CTA's TMEM holds its
+// 128 rows of the band's diagonal accumulators and its eight epilogue warps recombine and write
+// those rows. The arithmetic of every output element (pairs, K order, FP64 order) is that of
+// ozaki_body, so both kernels give bit-identical C.
+//
+// Synchronisation (barriers at the same shared-memory offsets in both CTAs):
+//   full[s]   rank 0: its own expect_tx arrival + one relayed arrival from rank 1 (count 2);
+//             rank 1: its own expect_tx arrival (count 1). Rank 1's warp 1 waits on its full[s]
+//             and forwards one arrival to rank 0's, so rank 0's MMA sees both halves landed.
+//   empty[s]  count 1 in each CTA: rank 0's MMA warp commits to both after the stage's MMAs.
+//   acc_full  count 1 in each CTA: committed to both after a group's last MMA.
+//   acc_empty rank 0 only, count 16: every epilogue warp of both CTAs arrives after reading TMEM.
+// ---------------------------------------------------------------------------------------------
+constexpr int kHalfTileBytes = kTileBytes / 2;                // 64 rows of a B tile
+constexpr int kPairChunkBytes = kTileBytes + kHalfTileBytes;  // one slice, one chunk, one CTA
+
+template <int S>
+struct PairGeo {
+  static constexpr int kStageBytes = S * kPairChunkBytes;
+  static constexpr int kStagesFit = (kMaxSmem - kSmemOverhead) / kStageBytes;
+  static constexpr int kStages = kStagesFit > 8 ? 8 : kStagesFit;
+  static constexpr int kSmem = kStages * kStageBytes + kSmemOverhead;
+  static_assert(kStages >= 2, "slice count too large for the shared-memory ring");
+  __host__ __device__ static constexpr int cps(int b) { return S / band_of(S, b).nsl; }
+};
+
+// Pair tiles in groups of 8 pair-rows (2048 rows of C), column-major inside a group.
+struct OzPairSource {
+  int64_t tiles_m, tiles_n;  // 256-row pair blocks, 128-column blocks
+  __device__ int64_t count() const { return tiles_m * tiles_n; }
+  __device__ void get(int64_t t, int* m0, int* n0) const {
+    const int64_t G = 8;
+    int64_t group = t / (G * tiles_n), first_m = group * G;
+    int64_t gsize = (tiles_m - first_m) < G ? (tiles_m - first_m) : G;
+    int64_t in_group = t - group * G * tiles_n;
+    *m0 = static_cast<int>((first_m + in_group % gsize) * 2 * kTileM);
+    *n0 = static_cast<int>((in_group / gsize) * kTileN);
+  }
+};
+
+// As issue_pairs, for the pair layout of a chunk: A tiles (4 KB) at slots 0..nsl-1, then the B
+// half tiles (2 KB) of slices 1..nsl.
+template <int S, int B, int J, int PP>
+__device__ __forceinline__ void issue_pairs2(uint64_t a0, uint32_t tmem, uint32_t accumulate_first) {
+  constexpr Band bd = band_of(S, B);
+  constexpr int d = bd.dhi - J;
+  if constexpr (J < kBand && d >= bd.dlo) {
+    if constexpr (PP <= pair_hi(d, S)) {
+      constexpr uint32_t idesc = idesc_i8_s32(2 * kTileM, kTileN);
+      constexpr uint64_t a_off = static_cast<uint64_t>((PP - 1) * (kTileBytes >> 4));
+      constexpr uint64_t b_off =
+          static_cast<uint64_t>(bd.nsl * (kTileBytes >> 4) + (d - PP - 1) * (kHalfTileBytes >> 4));
+      mma_i8_pair(tmem + static_cast<uint32_t>(J * kTileN), a0 + a_off, a0 + b_off, idesc,
+                  PP == pair_lo(d, S) ? accumulate_first : 1u);
+      issue_pairs2<S, B, J, PP + 1>(a0, tmem, accumulate_first);
+    } else {
+      issue_pairs2<S, B, J + 1, pair_lo(d - 1, S)>(a0, tmem, accumulate_first);
+    }
+  }
+}
+
+template <int S, int B>
+__device__ __forceinline__ void issue_chunk2(uint64_t a0, uint32_t tmem, uint32_t accumulate_first) {
+  if constexpr (B < num_bands(S)) issue_pairs2<S, B, 0, pair_lo(band_of(S, B).dhi, S)>(a0, tmem, accumulate_first);
+}
+
+template <int S>
+__device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatus* status) {
+  using G = PairGeo<S>;
+  constexpr int NB = num_bands(S);
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + G::kStages * G::kStageBytes);
+  uint64_t* empty = full + G::kStages;
+  uint64_t* acc_full = empty + G::kStages;
+  uint64_t* acc_empty = acc_full + 1;
+  uint64_t* drain = acc_empty + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const OzPairSource src{(pr.rba + 1) / 2, pr.rbb};
+  const int64_t tiles = src.count();
+  const int64_t first = cluster_id_x(), stride = num_clusters_x();
+  const int64_t nkc = pr.nkc;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < G::kStages; ++i) {
+      mbar_init(&full[i], rank == 0 ? 2 : 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, 2 * kEpilogueWarps);
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    tmem_alloc_pair(tmem_slot, 512);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // both CTAs' barriers exist before any arrival crosses the pair
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------- bulk-copy producer (both CTAs) -------------------------
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      bool ok = true;
+      const int64_t a_slice = pr.rba * nkc * kTileBytes, b_slice = pr.rbb * nkc * kTileBytes;
+      for (int64_t t = first; t < tiles && ok; t += stride) {
+        int m0, n0;
+        src.get(t, &m0, &n0);
+        const int64_t rb = m0 / kTileM + rank;  // this CTA's row block; past the end: no A copies
+        const bool has_a = rb < pr.rba;
+        const int8_t* a_blk = pr.sa + (has_a ? rb : 0) * nkc * kTileBytes;
+        const int8_t* b_blk = pr.sb + static_cast<int64_t>(n0 / kTileN) * nkc * kTileBytes + rank * kHalfTileBytes;
+        const uint32_t chunk_bytes = (has_a ? kTileBytes : 0) + kHalfTileBytes;
+        for (int b = 0; b < NB && ok; ++b) {
+          const Band bd = band_of(S, b);
+          const int gch = Geo<S>::gchunks(b), cps = G::cps(b);
+          for (int64_t c0 = 0; c0 < nkc && ok; c0 += gch) {
+            const int64_t c1 = (c0 + gch < nkc) ? c0 + gch : nkc;
+            for (int64_t cs = c0; cs < c1; cs += cps) {
+              const int64_t ce = (cs + cps < c1) ? cs + cps : c1;
+              if (!mbar_wait_cluster(&empty[stage], phase ^ 1, abort_flag, status, 21)) { ok = false; break; }
+              uint8_t* st = smem + stage * G::kStageBytes;
+              mbar_arrive_expect_tx(&full[stage], static_cast<uint32_t>((ce - cs) * bd.nsl) * chunk_bytes);
+              for (int64_t c = cs; c < ce; ++c) {
+                uint8_t* base = st + (c - cs) * bd.nsl * kPairChunkBytes;
+                const int8_t* ga = a_blk + c * kTileBytes;
+                const int8_t* gb = b_blk + c * kTileBytes;
+                for (int q = 0; q < bd.nsl; ++q) {
+                  if (has_a) bulk_load(base + q * kTileBytes, ga + q * a_slice, kTileBytes, &full[stage]);
+                  bulk_load(base + bd.nsl * kTileBytes + q * kHalfTileBytes, gb + q * b_slice, kHalfTileBytes,
+                            &full[stage]);
+                }
+              }
+              if (++stage == G::kStages) { stage = 0; phase ^= 1; }
+            }
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1 && rank != 0) {
+    // ------------------- rank 1: forward each landed stage to rank 0 -------------------
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      bool ok = true;
+      for (int64_t t = first; t < tiles && ok; t += stride) {
+        for (int b = 0; b < NB && ok; ++b) {
+          const int gch = Geo<S>::gchunks(b), cps = G::cps(b);
+          for (int64_t c0 = 0; c0 < nkc && ok; c0 += gch) {
+            const int64_t c1 = (c0 + gch < nkc) ? c0 + gch : nkc;
+            for (int64_t cs = c0; cs < c1; cs += cps) {
+              if (!mbar_wait(&full[stage], phase, abort_flag, status, 22)) { ok = false; break; }
+              mbar_arrive_cluster(cluster_addr(&full[stage], 0));
+              if (++stage == G::kStages) { stage = 0; phase ^= 1; }
+            }
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // --------------------------- rank 0: MMA issuer for the pair ---------------------------
+    const uint64_t desc0 = smem_desc_k_sw32(smem_u32(smem));
+    int stage = 0;
+    uint32_t phase = 0;
+    uint32_t group = 0;
+    bool ok = true;
+    for (int64_t t = first; t < tiles && ok; t += stride) {
+      for (int b = 0; b < NB && ok; ++b) {
+        const Band bd = band_of(S, b);
+        const int gch = Geo<S>::gchunks(b), cps = G::cps(b);
+        const uint64_t chunk_step = static_cast<uint64_t>(bd.nsl * (kPairChunkBytes >> 4));
+        for (int64_t c0 = 0; c0 < nkc && ok; c0 += gch) {
+          const int64_t c1 = (c0 + gch < nkc) ? c0 + gch : nkc;
+          if (!mbar_wait_cluster(acc_empty, (group & 1) ^ 1, abort_flag, status, 23)) { ok = false; break; }
+          tc_fence_after();
+          for (int64_t cs = c0; cs < c1; cs += cps) {
+            const int64_t ce = (cs + cps < c1) ? cs + cps : c1;
+            if (!mbar_wait_cluster(&full[stage], phase, abort_flag, status, 24)) { ok = false; break; }
+            tc_fence_after();
+            if (lane == 0) {
+              uint64_t a0 = desc0 + static_cast<uint64_t>(stage) * (G::kStageBytes >> 4);
+              for (int64_t c = cs; c < ce; ++c, a0 += chunk_step) {
+                const uint32_t acc_first = (c == c0) ? 0u : 1u;
+                switch (b) {
+                  case 0: issue_chunk2<S, 0>(a0, tmem_base, acc_first); break;
+                  case 1: issue_chunk2<S, 1>(a0, tmem_base, acc_first); break;
+                  default: issue_chunk2<S, 2>(a0, tmem_base, acc_first); break;
+                }
+              }
+              mma_commit_pair(cluster_addr(&empty[stage], 0));
+              mma_commit_pair(cluster_addr(&empty[stage], 1));
+            }
+            __syncwarp();
+            if (++stage == G::kStages) { stage = 0; phase ^= 1; }
+          }
+          if (!ok) break;
+          if (lane == 0) {
+            mma_commit_pair(cluster_addr(acc_full, 0));
+            mma_commit_pair(cluster_addr(acc_full, 1));
+          }
+          __syncwarp();
+          ++group;
+        }
+      }
+    }
+    if (!ok && lane == 0) {
+      // Let every MMA already issued finish before TMEM is released.
+      mma_commit_pair(cluster_addr(drain, 0));
+      uint64_t t0 = globaltimer();
+      while (!mbar_try_wait(drain, 0) && globaltimer() - t0 < LT_WAIT_TIMEOUT_NS) {
+      }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------- epilogue (8 warps per CTA) -------------------------------
+    const int ew = warp - 2;
+    const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31 are visible to this warp
+    const int half = ew >> 2;      // columns 64*half .. +63 of the tile
+    const int row_in_tile = quarter * 32 + lane;
+    const uint32_t acc_empty_r0 = cluster_addr(acc_empty, 0);
+    uint32_t group = 0;
+    bool ok = true;
+    for (int64_t t = first; t < tiles && ok; t += stride) {
+      int m0, n0;
+      src.get(t, &m0, &n0);
+      double acc[64];
+#pragma unroll
+      for (int i = 0; i < 64; ++i) acc[i] = 0.0;
+      for (int b = 0; b < NB && ok; ++b) {
+        const Band bd = band_of(S, b);
+        const int gch = Geo<S>::gchunks(b);
+        for (int64_t c0 = 0; c0 < nkc; c0 += gch) {
+          if (!mbar_wait_cluster(acc_full, group & 1, abort_flag, status, 25)) { ok = false; break; }
+          tc_fence_after();
+          for (int j = 0; j < kBand; ++j) {
+            const int d = bd.dhi - j;
+            if (d < bd.dlo) break;
+            const double sc = pow2i(-7 * d);
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+              uint32_t v[32];
+              const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) +
+                                     static_cast<uint32_t>(j * kTileN + half * 64 + cc * 32);
+              tmem_ld_32x32b_x32(taddr, v);
+              tmem_ld_wait();
+#pragma unroll
+              for (int i = 0; i < 32; ++i)
+                acc[cc * 32 + i] =
+                    __dadd_rn(acc[cc * 32 + i], __dmul_rn(static_cast<double>(static_cast<int32_t>(v[i])), sc));
+            }
+          }
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive_cluster(acc_empty_r0);
+          ++group;
+        }
+      }
+      if (!ok) break;
+      // ---- C = fma(alpha, acc 2^sigma 2^tau, beta C0) for this CTA's 128 rows ----
+      const int64_t row = m0 + static_cast<int64_t>(rank) * kTileM + row_in_tile;
+      if (row < pr.M) {
+        const int sig = exponent_of_maxbits(pr.amax_a[row]);
+        const int64_t col0 = n0 + half * 64;
+        double* crow = pr.C + row * pr.N;
+        const int64_t N = pr.N;
+        const double alpha = pr.alpha, beta = pr.beta;
+        const unsigned long long* amax_b = pr.amax_b;
+#pragma unroll
+        for (int i = 0; i < 64; ++i) {
+          const int64_t col = col0 + i;
+          if (col < N) {
+            const int tau = exponent_of_maxbits(amax_b[col]);
+            double out;
+            if (sig == kSentinel || tau == kSentinel) {
+              out = __longlong_as_double(0x7ff8000000000000ll);
+            } else {
+              const double tv = scale_pow2(scale_pow2(acc[i], sig), tau);
+              out = (beta != 0.0) ? fma(alpha, tv, __dmul_rn(beta, crow[col])) : __dmul_rn(alpha, tv);
+            }
+            crow[col] = out;
+          }
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // rank 0's MMAs read rank 1's shared memory and write its TMEM until here
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc_pair(tmem_base, 512);
+  }
+}
+
+template <int S>
+__global__ void __launch_bounds__(kThreads, 1) ozaki_pair_kernel(OzProblem pr, DeviceStatus* status) {
+  ozaki_pair_body<S>(pr, status);
+}
+
 // Launches the product kernel for S slices over `src` (single problem or grouped tile list).
 template <int S, bool kGrouped, class Src>
 int launch_gemm_s(const Src& src, int64_t ntiles, DeviceContext* ctx, cudaStream_t stream) {
@@ -628,6 +945,70 @@ int launch_gemm_s(const Src& src, int64_t ntiles, DeviceContext* ctx, cudaStream
     ozaki_gemm_kernel<S><<<static_cast<unsigned>(grid), kThreads, G::kSmem, stream>>>(src, ctx->status);
   LT_CUDA_TRY(cudaGetLastError());
   return LT_OK;
+}
+
+// Launches the CTA-pair product kernel for S slices. *launched = false (nothing launched) when no
+// pair of CTAs with this kernel's shared memory fits on the device.
+template <int S>
+int launch_pair_s(const OzProblem& pr, DeviceContext* ctx, cudaStream_t stream, bool* launched) {
+  using G = PairGeo<S>;
+  static std::once_flag once[64];
+  static cudaError_t attr_err[64];
+  static int max_clusters[64];
+  auto config = [&](cudaLaunchConfig_t* cfg, cudaLaunchAttribute* attr, unsigned grid) {
+    *cfg = cudaLaunchConfig_t{};
+    cfg->gridDim = dim3(grid);
+    cfg->blockDim = dim3(kThreads);
+    cfg->dynamicSmemBytes = G::kSmem;
+    cfg->stream = stream;
+    attr->id = cudaLaunchAttributeClusterDimension;
+    attr->val.clusterDim.x = 2;
+    attr->val.clusterDim.y = 1;
+    attr->val.clusterDim.z = 1;
+    cfg->attrs = attr;
+    cfg->numAttrs = 1;
+  };
+  std::call_once(once[ctx->device], [&] {
+    attr_err[ctx->device] =
+        cudaFuncSetAttribute(ozaki_pair_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::kSmem);
+    if (attr_err[ctx->device] != cudaSuccess) return;
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute attr;
+    config(&cfg, &attr, static_cast<unsigned>(ctx->sm_count & ~1));
+    attr_err[ctx->device] = cudaOccupancyMaxActiveClusters(&max_clusters[ctx->device], ozaki_pair_kernel<S>, &cfg);
+  });
+  LT_CUDA_TRY(attr_err[ctx->device]);
+  *launched = false;
+  const int64_t tiles = ((pr.rba + 1) / 2) * pr.rbb;
+  const int64_t clusters = std::min<int64_t>(std::min<int64_t>(tiles, max_clusters[ctx->device]), ctx->sm_count / 2);
+  if (clusters <= 0) return LT_OK;
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute attr;
+  config(&cfg, &attr, static_cast<unsigned>(2 * clusters));
+  LT_CUDA_TRY(cudaLaunchKernelEx(&cfg, ozaki_pair_kernel<S>, pr, ctx->status));
+  *launched = true;
+  return LT_OK;
+}
+
+int launch_pair(int s, const OzProblem& pr, DeviceContext* ctx, cudaStream_t stream, bool* launched) {
+  switch (s) {
+#define LT_PAIR_CASE(S) \
+  case S: return launch_pair_s<S>(pr, ctx, stream, launched);
+    LT_PAIR_CASE(1) LT_PAIR_CASE(2) LT_PAIR_CASE(3) LT_PAIR_CASE(4) LT_PAIR_CASE(5) LT_PAIR_CASE(6)
+    LT_PAIR_CASE(7) LT_PAIR_CASE(8) LT_PAIR_CASE(9) LT_PAIR_CASE(10) LT_PAIR_CASE(11) LT_PAIR_CASE(12)
+#undef LT_PAIR_CASE
+    default: return set_error(LT_ERR_INVALID_ARGUMENT, "slice count %d unsupported", s);
+  }
+}
+
+// The CTA-pair kernel serves single problems with two or more 128-row blocks unless the
+// environment sets LIBTHOM_OZAKI_PAIR=0 (one-CTA kernel everywhere, for comparison).
+bool pair_enabled() {
+  static const bool on = [] {
+    const char* v = getenv("LIBTHOM_OZAKI_PAIR");
+    return v == nullptr || v[0] != '0';
+  }();
+  return on;
 }
 
 template <bool kGrouped, class Src>
@@ -731,6 +1112,11 @@ int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double bet
   pr.rbb = L.RBb;
   pr.alpha = alpha;
   pr.beta = beta;
+  if (L.RBa >= 2 && pair_enabled()) {
+    bool launched = false;
+    LT_TRY(launch_pair(s, pr, ctx, stream, &launched));
+    if (launched) return LT_OK;
+  }
   return launch_gemm<false>(s, pr, L.RBa * L.RBb, ctx, stream);
 }
 

@@ -48,6 +48,17 @@ def test_ragged_shapes_bit_exact(cuda, oracle_mod, M, N, K):
     assert_bit_exact(C, oracle_mod.ozaki_dgemm(A, B, C0, -1.0, 0.75, 7))
 
 
+@pytest.mark.parametrize("M,N,K,s", [(256, 128, 64, 8), (300, 200, 96, 7), (129, 64, 40, 5), (1536, 1664, 32, 3),
+                                     (260, 24, 17000, 8)])
+def test_cta_pair_kernel_bit_exact(cuda, oracle_mod, M, N, K, s):
+    """Problems with two or more 128-row blocks run on the CTA-pair kernel (tcgen05 cta_group::2,
+    256 x 128 tiles): an odd row-block count (the last pair's second CTA holds no rows of A), more
+    tiles than CTA pairs (persistent loop), and K long enough for two INT32-safe groups."""
+    A, B, C0 = oracle_mod.make_problem(M, N, K, phi=5, seed=M + 3 * N + s)
+    C = run_ozaki(cuda, A, B, C0, 1.25, -0.5, s)
+    assert_bit_exact(C, oracle_mod.ozaki_dgemm(A, B, C0, 1.25, -0.5, s))
+
+
 def test_long_k_multiple_groups(cuda, oracle_mod):
     """K = 20000 > 16640 (the INT32-safe group length of an 8-pair diagonal): two groups."""
     M, N, K = 64, 48, 20000
