@@ -21,9 +21,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 from pathlib import Path
 
@@ -33,7 +31,6 @@ sys.path.insert(0, str(ROOT))
 METRIC = "DGEMM TFLOP/s at FP64 accuracy, 8192^3: Ozaki-INT8 vs native FP64 on 1 B200"
 UNIT = "TFLOP/s"
 SEED = 1234
-DMMA_PEAK_TFLOPS = 37.0  # measured FP64 mma.sync peak on this pool's B200s (profiles/dmma_peak_b200.md)
 
 
 WORKLOADS = ("square", "tall", "longk")
@@ -94,56 +91,64 @@ def profile_traffic(name: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+    """SM clock, power and clock-event reasons of one GPU, read through NVML every 20 ms by a
+    background thread while the timed region runs (reading only; no setting is changed)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksThrottleReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksThrottleReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksThrottleReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksThrottleReasonSwPowerCap"),
+               ("hw_power_brake_slowdown", "nvmlClocksThrottleReasonHwPowerBrakeSlowdown"))
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, period_s: float = 0.02):
         self.device = device
-        self.proc = None
-        self.file = None
+        self.period = period_s
+        self.rows = []
+        self.error = None
+        self.thread = None
+        self.stop = None
+
+    def _loop(self):
+        import pynvml as nv
+
+        h = nv.nvmlDeviceGetHandleByIndex(self.device)
+        self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        masks = [(name, getattr(nv, attr)) for name, attr in self.REASONS]
+        while True:
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+            bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+            self.rows.append((sm, pw, [name for name, m in masks if bits & m]))
+            if self.stop.wait(self.period):
+                break
 
     def __enter__(self):
+        import threading
+
         try:
-            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=self.file, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+            import pynvml as nv
+
+            nv.nvmlInit()
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._loop, daemon=True)
+            self.thread.start()
+        except Exception as e:  # no NVML on this machine
+            self.error = f"NVML unavailable: {e}"
         return self
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
 
     def summary(self) -> dict:
-        if self.proc is None or self.file is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.file.flush()
-        rows = []
-        for line in Path(self.file.name).read_text().splitlines():
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[5:9]))
-            except ValueError:
-                continue
-        os.unlink(self.file.name)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[3]) if v.lower() == "active"})
-        loaded = [r for r in rows if r[2] > 200.0] or rows
-        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max(r[1] for r in rows),
-                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
+        if self.error or not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.error or "no samples"]}
+        loaded = [r for r in self.rows if r[1] > 200.0] or self.rows
+        reasons = sorted({x for r in self.rows for x in r[2]})
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_mhz_min": min(r[0] for r in loaded),
+                "sm_max_mhz": self.max_mhz, "power_w_max": max(r[1] for r in self.rows),
+                "samples": len(self.rows), "source": "NVML, 20 ms", "reasons": reasons}
 
 
 # ------------------------------------------------------------------------------------------------
@@ -343,6 +348,13 @@ def run_ours(args) -> None:
     s = chosen
     lt.device_status()
 
+    # ---- roofline denominators, measured on this GPU now with the instruction forms the kernels
+    # use (lt_measure_peak: operands on chip, every SM; best of two) ----
+    pair = M > 128 and os.environ.get("LIBTHOM_OZAKI_PAIR", "1") != "0"
+    int8_kind = lt.LT_PEAK_INT8_MMA_PAIR if pair else lt.LT_PEAK_INT8_MMA_N128
+    int8_peak = max(lt.measure_peak(int8_kind, stream) for _ in range(2)) / 1e12
+    fp64_peak = max(lt.measure_peak(lt.LT_PEAK_FP64_MMA, stream) for _ in range(2)) / 1e12
+
     def barrier():
         if dist is not None:
             dist.barrier()
@@ -435,7 +447,6 @@ def run_ours(args) -> None:
 
     peaks = measured_peaks()
     bf16 = peaks.get("bf16_tflops")
-    int8_peak = 2.0 * bf16 if bf16 else 2.0 * 1590.0
     int8_ops = pairs(s) * flop
     achieved = int8_ops / (prod_ms * 1e-3) / 1e12
     traffic = profile_traffic("ozaki_gemm_8192")
@@ -455,19 +466,23 @@ def run_ours(args) -> None:
                      "ozaki_by_slices": errs, "rows_checked": len(rows),
                      "oracle": f"compensated Dot2 on {len(rows)} rows ({oracle_s:.1f} s)"},
         "native_fp64": {"value": world * flop / (fp64_ms * 1e-3) / 1e12, "ms_per_step": fp64_ms,
-                        "frac_of_dmma_peak": flop / (fp64_ms * 1e-3) / 1e12 / DMMA_PEAK_TFLOPS},
+                        "frac_of_dmma_peak": flop / (fp64_ms * 1e-3) / 1e12 / fp64_peak},
         "cublas_fp64": {"value": world * flop / (cublas_ms * 1e-3) / 1e12, "ms_per_step": cublas_ms},
         "speedup_vs_native_fp64": fp64_ms / ms_step,
         "stages_ms": {"split": split_ms, "product": prod_ms},
-        "roofline": {"bound": "tensor", "kernel": "ozaki_gemm_kernel", "achieved": achieved,
-                     "peak": int8_peak, "unit": "TOP/s (INT8)", "frac": achieved / int8_peak,
-                     "peak_source": "2 x bf16_tflops of MEASURED_PEAKS.json (dense INT8 = 2x dense BF16 on B200)"
-                     if bf16 else "2 x 1590 fallback", "traffic": traffic,
+        "roofline": {"bound": "tensor", "kernel": "ozaki_pair_kernel" if pair else "ozaki_gemm_kernel",
+                     "achieved": achieved, "peak": int8_peak, "unit": "TOP/s (INT8)", "frac": achieved / int8_peak,
+                     "peak_source": "measured in this run: lt_measure_peak("
+                                    + ("tcgen05.mma.cta_group::2 kind::i8 M256 N128" if pair else
+                                       "tcgen05.mma kind::i8 M128 N128") + "), operands on chip, all SMs",
+                     "peak_bf16x2": 2.0 * bf16 if bf16 else None,
+                     "frac_of_bf16x2": achieved / (2.0 * bf16) if bf16 else None,
+                     "traffic": traffic,
                      "algorithmic": f"{pairs(s)} INT8 slice products x 2MNK = {int8_ops:.4g} ops per launch"},
         "roofline_fp64": {"bound": "tensor", "kernel": "dgemm_fp64_kernel",
-                          "achieved": flop / (fp64_ms * 1e-3) / 1e12, "peak": DMMA_PEAK_TFLOPS,
-                          "unit": "TFLOP/s (FP64)", "frac": flop / (fp64_ms * 1e-3) / 1e12 / DMMA_PEAK_TFLOPS,
-                          "peak_source": "measured mma.sync f64 throughput (profiles/dmma_peak_b200.md)"},
+                          "achieved": flop / (fp64_ms * 1e-3) / 1e12, "peak": fp64_peak,
+                          "unit": "TFLOP/s (FP64)", "frac": flop / (fp64_ms * 1e-3) / 1e12 / fp64_peak,
+                          "peak_source": "measured in this run: lt_measure_peak(mma.sync m16n8k16 f64)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * (M * K + K * N + M * N),
                 "d2h_bytes_per_step": 8 * M * N, "ms_per_step": e2e_ms,
                 "path": "lt_dgemm_ozaki C ABI, pinned host buffers, H2D A,B,C0 + D2H C in the timed region"},
