@@ -96,6 +96,17 @@ int lt_ozaki_product(double* C, int64_t M, int64_t N, int64_t K, double alpha, d
                      const void* workspace, size_t workspace_bytes, void* stream);
 int lt_dgemm_cublas(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
                     double alpha, double beta, void* stream);
+/* Ozaki DGEMM on HOST memory: A, B and C are host pointers (C holds C0 on entry when beta != 0 and
+ * the result on return). Replaces the reference harness's copy-in / kernel / copy-out sequence
+ * (main.cpp and routines/dgemm/dgemm.cpp:135-170 copy whole matrices before and after the call)
+ * with one pipelined call: B is copied and split first, then row panels of A and C0 are copied
+ * while earlier panels are split and multiplied and finished panels of C are copied back, so the
+ * PCIe transfers overlap the kernels. Overlap needs page-locked host buffers (cudaMallocHost or
+ * cudaHostRegister); pageable buffers work but serialise. Uses the cached device workspace, grown
+ * to hold A, B and C as well. Results are bit-identical to lt_dgemm_ozaki. Synchronous: returns
+ * when C is in host memory; `stream` is ordered before and after the call's work. */
+int lt_dgemm_ozaki_host(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
+                        double alpha, double beta, int slices, void* stream);
 
 /* Allocation-free Ozaki DGEMM. No counterpart in the reference. For callers that cannot allocate
  * device memory (a framework whose own pool owns the GPU, a service that must not allocate on its
@@ -212,6 +223,8 @@ int lt_flush_l2(void* stream);
 #define LT_PEAK_INT8_MMA_N128 1 /* tcgen05.mma kind::i8 M128 N128 K32, one CTA per SM: INT8 op/s */
 #define LT_PEAK_INT8_MMA_N256 2 /* tcgen05.mma kind::i8 M128 N256 K32, one CTA per SM */
 #define LT_PEAK_INT8_MMA_PAIR 3 /* tcgen05.mma.cta_group::2 kind::i8 M256 N128 K32, CTA pairs */
+#define LT_PEAK_SUSTAINED 0x10  /* OR into a kind: rate after 0.5 s of back-to-back launches (power- and
+                                   clock-limited), timed over the next 0.5 s; without it one launch */
 /* Runs a loop of the named tensor instruction with its operands on chip (registers, or one
  * shared-memory tile per operand) on every SM and returns the measured rate of the current device
  * in *ops_per_second (2 per multiply-add). The tcgen05 kinds first run a check launch with known

@@ -33,6 +33,7 @@ LT_PEAK_FP64_MMA = 0
 LT_PEAK_INT8_MMA_N128 = 1
 LT_PEAK_INT8_MMA_N256 = 2
 LT_PEAK_INT8_MMA_PAIR = 3
+LT_PEAK_SUSTAINED = 0x10
 LT_SEL_FEATURES = 34
 LT_SEL_HIDDEN = 64
 LT_SEL_CLASSES = 8
@@ -118,6 +119,7 @@ SIGNATURES = {
     "lt_abs_denominator": (_i32, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _vp]),
     "lt_flush_l2": (_i32, [_vp]),
     "lt_measure_peak": (_i32, [_i32, _c.POINTER(_f64), _vp]),
+    "lt_dgemm_ozaki_host": (_i32, [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _i32, _vp]),
 }
 
 _lib = None
@@ -245,3 +247,9 @@ def measure_peak(kind: int, stream=None) -> float:
     out = ctypes.c_double()
     check(lib().lt_measure_peak(kind, ctypes.byref(out), _stream(stream)))
     return out.value
+
+
+def dgemm_ozaki_host(A, B, C, M, N, K, alpha=1.0, beta=0.0, slices=8, stream=None) -> None:
+    """Ozaki DGEMM on host (CPU) tensors or arrays, pipelined through the GPU (lt_dgemm_ozaki_host).
+    C holds C0 on entry and the result on return."""
+    check(lib().lt_dgemm_ozaki_host(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, slices, _stream(stream)))

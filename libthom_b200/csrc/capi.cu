@@ -129,6 +129,16 @@ int lt_dgemm_ozaki(const double* A, const double* B, double* C, int64_t M, int64
   return lt::ok();
 }
 
+int lt_dgemm_ozaki_host(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
+                        double beta, int slices, void* stream) {
+  LT_TRY(lt::check_gemm_args(A, B, C, M, N, K));
+  if (slices < 1 || slices > LT_OZAKI_MAX_SLICES)
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "slice count %d outside [1, %d]", slices, LT_OZAKI_MAX_SLICES);
+  if (M == 0 || N == 0) return lt::ok();
+  LT_TRY(lt::ozaki::host_run(A, B, C, M, N, K, alpha, beta, slices, lt::as_stream(stream)));
+  return lt::ok();
+}
+
 size_t lt_ozaki_workspace_size(int64_t M, int64_t N, int64_t K, int slices) {
   if (M < 0 || N < 0 || K < 0 || slices < 1 || slices > LT_OZAKI_MAX_SLICES) return 0;
   return lt::ozaki::workspace_size(M, N, K, slices);

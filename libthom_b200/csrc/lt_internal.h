@@ -42,6 +42,8 @@ int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double bet
             size_t workspace_bytes, cudaStream_t stream);
 int run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta,
         int slices, void* workspace, size_t workspace_bytes, cudaStream_t stream);
+int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
+             double beta, int slices, cudaStream_t stream);
 int noalloc_run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
                 double beta, int slices, cudaStream_t stream);
 struct Grouped;

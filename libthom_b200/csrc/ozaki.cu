@@ -463,26 +463,30 @@ __device__ __forceinline__ void ozaki_body(const Source& src, DeviceStatus* stat
     __syncwarp();
   } else if (warp == 1) {
     // ------------------------------------ MMA issuer ------------------------------------
-    const uint64_t desc0 = desc_k_sw32(smem_u32(smem));
-    int stage = 0;
-    uint32_t phase = 0;
-    uint32_t group = 0;
-    bool ok = true;
-    for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-      const int64_t nkc = src.get(t).pr->nkc;
-      for (int b = 0; b < NB && ok; ++b) {
-        const Band bd = band_of(S, b);
-        const int gch = G::gchunks(b), cps = G::cps(b);
-        const uint64_t chunk_step = static_cast<uint64_t>(2 * bd.nsl * (kTileBytes >> 4));
-        for (int64_t c0 = 0; c0 < nkc && ok; c0 += gch) {
-          const int64_t c1 = (c0 + gch < nkc) ? c0 + gch : nkc;
-          if (!mbar_wait(acc_empty, (group & 1) ^ 1, abort_flag, status, 12)) { ok = false; break; }
-          tc_fence_after();
-          for (int64_t cs = c0; cs < c1; cs += cps) {
-            const int64_t ce = (cs + cps < c1) ? cs + cps : c1;
-            if (!mbar_wait(&full[stage], phase, abort_flag, status, 13)) { ok = false; break; }
+    // One thread issues. Right after a stage's MMAs are queued it peeks at the next stage's
+    // barrier while those MMAs still run, so a stage whose copies have landed is issued without
+    // a blocking wait in between.
+    if (lane == 0) {
+      const uint64_t desc0 = desc_k_sw32(smem_u32(smem));
+      int stage = 0;
+      uint32_t phase = 0;
+      uint32_t group = 0;
+      bool ok = true;
+      bool ready = false;  // full[stage] seen complete for `phase` by the last peek
+      for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+        const int64_t nkc = src.get(t).pr->nkc;
+        for (int b = 0; b < NB && ok; ++b) {
+          const Band bd = band_of(S, b);
+          const int gch = G::gchunks(b), cps = G::cps(b);
+          const uint64_t chunk_step = static_cast<uint64_t>(2 * bd.nsl * (kTileBytes >> 4));
+          for (int64_t c0 = 0; c0 < nkc && ok; c0 += gch) {
+            const int64_t c1 = (c0 + gch < nkc) ? c0 + gch : nkc;
+            if (!mbar_wait(acc_empty, (group & 1) ^ 1, abort_flag, status, 12)) { ok = false; break; }
             tc_fence_after();
-            if (lane == 0) {
+            for (int64_t cs = c0; cs < c1; cs += cps) {
+              const int64_t ce = (cs + cps < c1) ? cs + cps : c1;
+              if (!ready && !mbar_wait(&full[stage], phase, abort_flag, status, 13)) { ok = false; break; }
+              tc_fence_after();
               uint64_t a0 = desc0 + static_cast<uint64_t>(stage) * (G::kStageBytes >> 4);
               for (int64_t c = cs; c < ce; ++c, a0 += chunk_step) {
                 const uint32_t acc_first = (c == c0) ? 0u : 1u;
@@ -492,23 +496,25 @@ __device__ __forceinline__ void ozaki_body(const Source& src, DeviceStatus* stat
                   default: issue_chunk<S, 2>(a0, tmem_base, acc_first); break;
                 }
               }
+              const int next = stage + 1 == G::kStages ? 0 : stage + 1;
+              const uint32_t next_phase = stage + 1 == G::kStages ? phase ^ 1 : phase;
+              ready = mbar_try_wait(&full[next], next_phase);
               mma_commit(&empty[stage]);
+              stage = next;
+              phase = next_phase;
             }
-            __syncwarp();
-            if (++stage == G::kStages) { stage = 0; phase ^= 1; }
+            if (!ok) break;
+            mma_commit(acc_full);
+            ++group;
           }
-          if (!ok) break;
-          if (lane == 0) mma_commit(acc_full);
-          __syncwarp();
-          ++group;
         }
       }
-    }
-    if (!ok && lane == 0) {
-      // Let every MMA already issued finish before TMEM is released.
-      mma_commit(drain);
-      uint64_t t0 = globaltimer();
-      while (!mbar_try_wait(drain, 0) && globaltimer() - t0 < LT_WAIT_TIMEOUT_NS) {
+      if (!ok) {
+        // Let every MMA already issued finish before TMEM is released.
+        mma_commit(drain);
+        uint64_t t0 = globaltimer();
+        while (!mbar_try_wait(drain, 0) && globaltimer() - t0 < LT_WAIT_TIMEOUT_NS) {
+        }
       }
     }
     __syncwarp();
@@ -782,25 +788,27 @@ __device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatu
     __syncwarp();
   } else if (warp == 1) {
     // --------------------------- rank 0: MMA issuer for the pair ---------------------------
-    const uint64_t desc0 = smem_desc_k_sw32(smem_u32(smem));
-    int stage = 0;
-    uint32_t phase = 0;
-    uint32_t group = 0;
-    bool ok = true;
-    for (int64_t t = first; t < tiles && ok; t += stride) {
-      for (int b = 0; b < NB && ok; ++b) {
-        const Band bd = band_of(S, b);
-        const int gch = Geo<S>::gchunks(b), cps = G::cps(b);
-        const uint64_t chunk_step = static_cast<uint64_t>(bd.nsl * (kPairChunkBytes >> 4));
-        for (int64_t c0 = 0; c0 < nkc && ok; c0 += gch) {
-          const int64_t c1 = (c0 + gch < nkc) ? c0 + gch : nkc;
-          if (!mbar_wait_cluster(acc_empty, (group & 1) ^ 1, abort_flag, status, 23)) { ok = false; break; }
-          tc_fence_after();
-          for (int64_t cs = c0; cs < c1; cs += cps) {
-            const int64_t ce = (cs + cps < c1) ? cs + cps : c1;
-            if (!mbar_wait_cluster(&full[stage], phase, abort_flag, status, 24)) { ok = false; break; }
+    // One thread issues, peeking at the next stage's barrier as in ozaki_body.
+    if (lane == 0) {
+      const uint64_t desc0 = smem_desc_k_sw32(smem_u32(smem));
+      int stage = 0;
+      uint32_t phase = 0;
+      uint32_t group = 0;
+      bool ok = true;
+      bool ready = false;
+      for (int64_t t = first; t < tiles && ok; t += stride) {
+        for (int b = 0; b < NB && ok; ++b) {
+          const Band bd = band_of(S, b);
+          const int gch = Geo<S>::gchunks(b), cps = G::cps(b);
+          const uint64_t chunk_step = static_cast<uint64_t>(bd.nsl * (kPairChunkBytes >> 4));
+          for (int64_t c0 = 0; c0 < nkc && ok; c0 += gch) {
+            const int64_t c1 = (c0 + gch < nkc) ? c0 + gch : nkc;
+            if (!mbar_wait_cluster(acc_empty, (group & 1) ^ 1, abort_flag, status, 23)) { ok = false; break; }
             tc_fence_after();
-            if (lane == 0) {
+            for (int64_t cs = c0; cs < c1; cs += cps) {
+              const int64_t ce = (cs + cps < c1) ? cs + cps : c1;
+              if (!ready && !mbar_wait_cluster(&full[stage], phase, abort_flag, status, 24)) { ok = false; break; }
+              tc_fence_after();
               uint64_t a0 = desc0 + static_cast<uint64_t>(stage) * (G::kStageBytes >> 4);
               for (int64_t c = cs; c < ce; ++c, a0 += chunk_step) {
                 const uint32_t acc_first = (c == c0) ? 0u : 1u;
@@ -810,27 +818,27 @@ __device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatu
                   default: issue_chunk2<S, 2>(a0, tmem_base, acc_first); break;
                 }
               }
+              const int next = stage + 1 == G::kStages ? 0 : stage + 1;
+              const uint32_t next_phase = stage + 1 == G::kStages ? phase ^ 1 : phase;
+              ready = mbar_try_wait_cluster(&full[next], next_phase);
               mma_commit_pair(cluster_addr(&empty[stage], 0));
               mma_commit_pair(cluster_addr(&empty[stage], 1));
+              stage = next;
+              phase = next_phase;
             }
-            __syncwarp();
-            if (++stage == G::kStages) { stage = 0; phase ^= 1; }
-          }
-          if (!ok) break;
-          if (lane == 0) {
+            if (!ok) break;
             mma_commit_pair(cluster_addr(acc_full, 0));
             mma_commit_pair(cluster_addr(acc_full, 1));
+            ++group;
           }
-          __syncwarp();
-          ++group;
         }
       }
-    }
-    if (!ok && lane == 0) {
-      // Let every MMA already issued finish before TMEM is released.
-      mma_commit_pair(cluster_addr(drain, 0));
-      uint64_t t0 = globaltimer();
-      while (!mbar_try_wait(drain, 0) && globaltimer() - t0 < LT_WAIT_TIMEOUT_NS) {
+      if (!ok) {
+        // Let every MMA already issued finish before TMEM is released.
+        mma_commit_pair(cluster_addr(drain, 0));
+        uint64_t t0 = globaltimer();
+        while (!mbar_try_wait(drain, 0) && globaltimer() - t0 < LT_WAIT_TIMEOUT_NS) {
+        }
       }
     }
     __syncwarp();
@@ -1053,6 +1061,76 @@ int launch_split(int s, const double* A, const double* B, int64_t M, int64_t N, 
   }
 }
 
+template <int S>
+void launch_split_rows_s(const double* A, int64_t M, int64_t K, int64_t NC, const unsigned long long* amax, int8_t* sa,
+                         int sms, cudaStream_t stream) {
+  const int64_t cap = static_cast<int64_t>(sms) * 64;
+  const int64_t rb = ceil_div(M, kTileM), t = rb * NC;
+  if (t > 0) split_rows_kernel<S><<<static_cast<unsigned>(t < cap ? t : cap), 128, 0, stream>>>(A, M, K, NC, rb, amax, sa);
+}
+
+template <int S>
+void launch_split_cols_s(const double* B, int64_t K, int64_t N, int64_t NC, const unsigned long long* amax, int8_t* sb,
+                         int sms, cudaStream_t stream) {
+  const int64_t cap = static_cast<int64_t>(sms) * 64;
+  const int64_t rb = ceil_div(N, kTileN), t = rb * NC;
+  if (t > 0) split_cols_kernel<S><<<static_cast<unsigned>(t < cap ? t : cap), 128, 0, stream>>>(B, K, N, NC, rb, amax, sb);
+}
+
+// Row side of the split: exponents of rows 0..M-1 of A (amax must be zero on entry) and their
+// slices, written as row blocks 0.. of `sa` (chunk-major, NC chunks).
+int rows_stage(int s, const double* A, int64_t M, int64_t K, int64_t NC, unsigned long long* amax, int8_t* sa, int sms,
+               cudaStream_t stream) {
+  if (M <= 0) return LT_OK;
+  if (K > 0) {
+    // 8 rows per block, K split so that the grid covers the GPU.
+    int64_t row_blocks = (M + 7) / 8;
+    int64_t ksplit = (4 * sms + row_blocks - 1) / row_blocks;
+    ksplit = ksplit < 1 ? 1 : ksplit;
+    int64_t kseg = round_up((K + ksplit - 1) / ksplit, 256);
+    ksplit = (K + kseg - 1) / kseg;
+    amax_rows_kernel<<<dim3(static_cast<unsigned>(row_blocks), static_cast<unsigned>(ksplit)), 256, 0, stream>>>(
+        A, M, K, kseg, amax);
+    LT_CUDA_TRY(cudaGetLastError());
+  }
+  switch (s) {
+#define LT_ROWS_CASE(S) \
+  case S: launch_split_rows_s<S>(A, M, K, NC, amax, sa, sms, stream); break;
+    LT_ROWS_CASE(1) LT_ROWS_CASE(2) LT_ROWS_CASE(3) LT_ROWS_CASE(4) LT_ROWS_CASE(5) LT_ROWS_CASE(6)
+    LT_ROWS_CASE(7) LT_ROWS_CASE(8) LT_ROWS_CASE(9) LT_ROWS_CASE(10) LT_ROWS_CASE(11) LT_ROWS_CASE(12)
+#undef LT_ROWS_CASE
+    default: return set_error(LT_ERR_INVALID_ARGUMENT, "slice count %d unsupported", s);
+  }
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
+// Column side: exponents of columns 0..N-1 of B (amax zero on entry) and their slices.
+int cols_stage(int s, const double* B, int64_t K, int64_t N, int64_t NC, unsigned long long* amax, int8_t* sb, int sms,
+               cudaStream_t stream) {
+  if (N <= 0) return LT_OK;
+  if (K > 0) {
+    int64_t col_blocks = (N + 255) / 256;
+    int64_t ksplit_b = (8 * sms + col_blocks - 1) / col_blocks;
+    ksplit_b = ksplit_b < 1 ? 1 : ksplit_b;
+    int64_t kseg_b = (K + ksplit_b - 1) / ksplit_b;
+    ksplit_b = (K + kseg_b - 1) / kseg_b;
+    amax_cols_kernel<<<dim3(static_cast<unsigned>(col_blocks), static_cast<unsigned>(ksplit_b)), 256, 0, stream>>>(
+        B, K, N, kseg_b, amax);
+    LT_CUDA_TRY(cudaGetLastError());
+  }
+  switch (s) {
+#define LT_COLS_CASE(S) \
+  case S: launch_split_cols_s<S>(B, K, N, NC, amax, sb, sms, stream); break;
+    LT_COLS_CASE(1) LT_COLS_CASE(2) LT_COLS_CASE(3) LT_COLS_CASE(4) LT_COLS_CASE(5) LT_COLS_CASE(6)
+    LT_COLS_CASE(7) LT_COLS_CASE(8) LT_COLS_CASE(9) LT_COLS_CASE(10) LT_COLS_CASE(11) LT_COLS_CASE(12)
+#undef LT_COLS_CASE
+    default: return set_error(LT_ERR_INVALID_ARGUMENT, "slice count %d unsupported", s);
+  }
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
 // Stage 1+2: exponents and slices of A and B into the workspace.
 int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int s, void* workspace,
           size_t workspace_bytes, cudaStream_t stream) {
@@ -1065,29 +1143,20 @@ int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int
   auto* amax_b = reinterpret_cast<unsigned long long*>(ws + L.off_amax_b);
   auto* sa = reinterpret_cast<int8_t*>(ws + L.off_sa);
   auto* sb = reinterpret_cast<int8_t*>(ws + L.off_sb);
-
   LT_CUDA_TRY(cudaMemsetAsync(ws, 0, L.off_sa, stream));
-  const int sms = ctx->sm_count;
-  if (K > 0) {
-    // amax of A rows: 8 rows per block, K split so that the grid covers the GPU.
-    int64_t row_blocks = (M + 7) / 8;
-    int64_t ksplit = (4 * sms + row_blocks - 1) / row_blocks;
-    ksplit = ksplit < 1 ? 1 : ksplit;
-    int64_t kseg = round_up((K + ksplit - 1) / ksplit, 256);
-    ksplit = (K + kseg - 1) / kseg;
-    amax_rows_kernel<<<dim3(static_cast<unsigned>(row_blocks), static_cast<unsigned>(ksplit)), 256, 0, stream>>>(
-        A, M, K, kseg, amax_a);
-    LT_CUDA_TRY(cudaGetLastError());
-    int64_t col_blocks = (N + 255) / 256;
-    int64_t ksplit_b = (8 * sms + col_blocks - 1) / col_blocks;
-    ksplit_b = ksplit_b < 1 ? 1 : ksplit_b;
-    int64_t kseg_b = (K + ksplit_b - 1) / ksplit_b;
-    ksplit_b = (K + kseg_b - 1) / kseg_b;
-    amax_cols_kernel<<<dim3(static_cast<unsigned>(col_blocks), static_cast<unsigned>(ksplit_b)), 256, 0, stream>>>(
-        B, K, N, kseg_b, amax_b);
-    LT_CUDA_TRY(cudaGetLastError());
+  LT_TRY(rows_stage(s, A, M, K, L.NC, amax_a, sa, ctx->sm_count, stream));
+  return cols_stage(s, B, K, N, L.NC, amax_b, sb, ctx->sm_count, stream);
+}
+
+// Products and recombination of one problem whose slices are in place: the CTA-pair kernel for two
+// or more row blocks, the one-CTA kernel otherwise.
+int launch_product(int s, const OzProblem& pr, DeviceContext* ctx, cudaStream_t stream) {
+  if (pr.rba >= 2 && pair_enabled()) {
+    bool launched = false;
+    LT_TRY(launch_pair(s, pr, ctx, stream, &launched));
+    if (launched) return LT_OK;
   }
-  return launch_split(s, A, B, M, N, K, L, amax_a, amax_b, sa, sb, sms, stream);
+  return launch_gemm<false>(s, pr, pr.rba * pr.rbb, ctx, stream);
 }
 
 // Stage 3+4: slice products on the tensor cores and the fused FP64 recombination into C.
@@ -1111,18 +1180,105 @@ int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double bet
   pr.rbb = L.RBb;
   pr.alpha = alpha;
   pr.beta = beta;
-  if (L.RBa >= 2 && pair_enabled()) {
-    bool launched = false;
-    LT_TRY(launch_pair(s, pr, ctx, stream, &launched));
-    if (launched) return LT_OK;
-  }
-  return launch_gemm<false>(s, pr, L.RBa * L.RBb, ctx, stream);
+  return launch_product(s, pr, ctx, stream);
 }
 
 int run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int s,
         void* workspace, size_t workspace_bytes, cudaStream_t stream) {
   LT_TRY(split(A, B, M, N, K, s, workspace, workspace_bytes, stream));
   return product(C, M, N, K, alpha, beta, s, workspace, workspace_bytes, stream);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host-resident operands (lt_dgemm_ozaki_host). B is copied and split first; then row panels of
+// A (and of C0 when beta != 0) are copied on one stream while the previous panel is split and
+// multiplied on the caller's stream and finished panels of C return on a third, so the PCIe
+// copies overlap the kernels. A panel is a block of whole 128-row blocks; its slices land in the
+// same place of the workspace as in run(), and every output element goes through the same
+// arithmetic, so C is bit-identical to run() on the same data.
+// ---------------------------------------------------------------------------------------------
+int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
+             double beta, int s, cudaStream_t stream) {
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  const Layout L = layout_for(M, N, K, s);
+  const size_t off_a = round_up(static_cast<int64_t>(L.total), 256);
+  const size_t off_b = off_a + round_up(8 * M * K, 256);
+  const size_t off_c = off_b + round_up(8 * K * N, 256);
+  const size_t total = off_c + 8 * static_cast<size_t>(M) * N;
+  void* base = nullptr;
+  LT_TRY(ensure_workspace(ctx, total, &base));
+  uint8_t* ws = static_cast<uint8_t*>(base);
+  auto* amax_a = reinterpret_cast<unsigned long long*>(ws + L.off_amax_a);
+  auto* amax_b = reinterpret_cast<unsigned long long*>(ws + L.off_amax_b);
+  auto* sa = reinterpret_cast<int8_t*>(ws + L.off_sa);
+  auto* sb = reinterpret_cast<int8_t*>(ws + L.off_sb);
+  auto* Ad = reinterpret_cast<double*>(ws + off_a);
+  auto* Bd = reinterpret_cast<double*>(ws + off_b);
+  auto* Cd = reinterpret_cast<double*>(ws + off_c);
+
+  // About eight panels (at least one 128-row block each).
+  const int64_t panel = std::max<int64_t>(kTileM, round_up(ceil_div(M, 8), kTileM));
+  const int64_t npanels = ceil_div(M, panel);
+  const int64_t chunk_block = static_cast<int64_t>(s) * kTileBytes;
+
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  std::vector<cudaEvent_t> ev(2 * npanels + 2, nullptr);
+  int rc = LT_OK;
+  auto cuda = [&](cudaError_t e, const char* what) {
+    if (e != cudaSuccess && rc == LT_OK) rc = set_error(LT_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return rc == LT_OK;
+  };
+  cuda(cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking), "stream");
+  cuda(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking), "stream");
+  for (auto& e : ev)
+    if (rc == LT_OK) cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+  cudaEvent_t e_start = ev[2 * npanels], e_b = ev[2 * npanels + 1];
+  if (rc == LT_OK) {
+    // Everything starts after the work already queued on the caller's stream.
+    cuda(cudaEventRecord(e_start, stream), "record");
+    cuda(cudaStreamWaitEvent(h2d, e_start, 0), "wait");
+    cuda(cudaStreamWaitEvent(d2h, e_start, 0), "wait");
+    cuda(cudaMemcpyAsync(Bd, B, 8 * static_cast<size_t>(K) * N, cudaMemcpyHostToDevice, h2d), "copy B");
+    cuda(cudaEventRecord(e_b, h2d), "record");
+    cuda(cudaMemsetAsync(ws, 0, L.off_sa, stream), "memset");
+    cuda(cudaStreamWaitEvent(stream, e_b, 0), "wait");
+  }
+  if (rc == LT_OK) rc = cols_stage(s, Bd, K, N, L.NC, amax_b, sb, ctx->sm_count, stream);
+  for (int64_t i = 0; i < npanels && rc == LT_OK; ++i) {
+    const int64_t r0 = i * panel, rows = std::min(panel, M - r0);
+    cudaEvent_t e_in = ev[2 * i], e_out = ev[2 * i + 1];
+    cuda(cudaMemcpyAsync(Ad + r0 * K, A + r0 * K, 8 * static_cast<size_t>(rows) * K, cudaMemcpyHostToDevice, h2d),
+         "copy A");
+    if (beta != 0.0)
+      cuda(cudaMemcpyAsync(Cd + r0 * N, C + r0 * N, 8 * static_cast<size_t>(rows) * N, cudaMemcpyHostToDevice, h2d),
+           "copy C0");
+    cuda(cudaEventRecord(e_in, h2d), "record");
+    cuda(cudaStreamWaitEvent(stream, e_in, 0), "wait");
+    if (rc != LT_OK) break;
+    int8_t* sa_panel = sa + (r0 / kTileM) * L.NC * chunk_block;
+    rc = rows_stage(s, Ad + r0 * K, rows, K, L.NC, amax_a + r0, sa_panel, ctx->sm_count, stream);
+    if (rc != LT_OK) break;
+    OzProblem pr{sa_panel, sb, Cd + r0 * N, amax_a + r0, amax_b, rows, N, L.NC, ceil_div(rows, kTileM), L.RBb,
+                 alpha, beta};
+    rc = launch_product(s, pr, ctx, stream);
+    if (rc != LT_OK) break;
+    cuda(cudaEventRecord(e_out, stream), "record");
+    cuda(cudaStreamWaitEvent(d2h, e_out, 0), "wait");
+    cuda(cudaMemcpyAsync(C + r0 * N, Cd + r0 * N, 8 * static_cast<size_t>(rows) * N, cudaMemcpyDeviceToHost, d2h),
+         "copy C");
+  }
+  // The caller's stream is ordered after the last copy back; the call returns with C in host memory.
+  if (rc == LT_OK) cuda(cudaEventRecord(e_start, d2h), "record");
+  if (rc == LT_OK) cuda(cudaStreamWaitEvent(stream, e_start, 0), "wait");
+  if (d2h != nullptr) cuda(cudaStreamSynchronize(d2h), "sync");
+  if (h2d != nullptr) cuda(cudaStreamSynchronize(h2d), "sync");
+  cuda(cudaStreamSynchronize(stream), "sync");
+  for (auto& e : ev)
+    if (e != nullptr) cudaEventDestroy(e);
+  if (h2d != nullptr) cudaStreamDestroy(h2d);
+  if (d2h != nullptr) cudaStreamDestroy(d2h);
+  return rc;
 }
 
 // ---------------------------------------------------------------------------------------------

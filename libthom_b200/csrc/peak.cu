@@ -212,16 +212,18 @@ int run_i8(int mode, int blocks, int iters, int verify, int* mismatches, DeviceC
   }
 }
 
-// Times `launch` (already warmed up) with CUDA events on `stream`; returns milliseconds.
+// Times `launch` with CUDA events on `stream`: one warm-up launch, then `reps` launches (after
+// `warm` more untimed ones). Returns milliseconds per launch.
 template <class F>
-int time_ms(F&& launch, cudaStream_t stream, float* ms) {
+int time_ms(F&& launch, cudaStream_t stream, float* ms, int warm = 0, int reps = 1) {
   cudaEvent_t e0, e1;
   LT_CUDA_TRY(cudaEventCreate(&e0));
   LT_CUDA_TRY(cudaEventCreate(&e1));
-  int rc = launch();  // warm-up
+  int rc = launch();
+  for (int i = 0; i < warm && rc == LT_OK; ++i) rc = launch();
   cudaError_t e = cudaSuccess;
   if (rc == LT_OK) e = cudaEventRecord(e0, stream);
-  if (rc == LT_OK && e == cudaSuccess) rc = launch();
+  for (int i = 0; i < reps && rc == LT_OK && e == cudaSuccess; ++i) rc = launch();
   if (rc == LT_OK && e == cudaSuccess) e = cudaEventRecord(e1, stream);
   if (rc == LT_OK && e == cudaSuccess) e = cudaEventSynchronize(e1);
   if (rc == LT_OK && e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
@@ -229,7 +231,18 @@ int time_ms(F&& launch, cudaStream_t stream, float* ms) {
   cudaEventDestroy(e1);
   if (rc != LT_OK) return rc;
   LT_CUDA_TRY(e);
+  *ms /= static_cast<float>(reps);
   return LT_OK;
+}
+
+// Burst: one timed launch after one warm-up. Sustained: about 0.5 s of launches back to back,
+// then 0.5 s timed, so power and clock limits have settled.
+template <class F>
+int measure(F&& launch, cudaStream_t stream, bool sustained, float* ms) {
+  int rc = time_ms(launch, stream, ms);
+  if (rc != LT_OK || !sustained) return rc;
+  const int n = static_cast<int>(500.0f / (*ms > 0.01f ? *ms : 0.01f)) + 1;
+  return time_ms(launch, stream, ms, n, n);
 }
 
 }  // namespace peak
@@ -238,6 +251,8 @@ int time_ms(F&& launch, cudaStream_t stream, float* ms) {
 extern "C" int lt_measure_peak(int kind, double* ops_per_second, void* stream_) {
   using namespace lt;
   using namespace lt::peak;
+  const bool sustained = (kind & LT_PEAK_SUSTAINED) != 0;
+  kind &= ~LT_PEAK_SUSTAINED;
   if (ops_per_second == nullptr || kind < LT_PEAK_FP64_MMA || kind > LT_PEAK_INT8_MMA_PAIR)
     return set_error(LT_ERR_INVALID_ARGUMENT, "lt_measure_peak: bad kind %d or null output", kind);
   DeviceContext* ctx = context();
@@ -249,13 +264,13 @@ extern "C" int lt_measure_peak(int kind, double* ops_per_second, void* stream_) 
     const int blocks = 2 * ctx->sm_count, iters = 4096;
     double* out = nullptr;
     LT_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&out), sizeof(double) * blocks * kDmmaThreads, stream));
-    int rc = time_ms(
+    int rc = measure(
         [&]() -> int {
           dmma_loop<<<blocks, kDmmaThreads, 0, stream>>>(out, iters);
           LT_CUDA_TRY(cudaGetLastError());
           return LT_OK;
         },
-        stream, &ms);
+        stream, sustained, &ms);
     cudaFreeAsync(out, stream);
     if (rc != LT_OK) return rc;
     const double flops = 2.0 * 16 * 8 * 16 * 4.0 * iters * (kDmmaThreads / 32) * static_cast<double>(blocks);
@@ -283,7 +298,7 @@ extern "C" int lt_measure_peak(int kind, double* ops_per_second, void* stream_) 
     return set_error(LT_ERR_UNSUPPORTED, "lt_measure_peak: check launch of kind %d produced %d wrong accumulators",
                      kind, hbad);
   const int iters = 32768;
-  rc = time_ms([&]() { return run_i8(mode, blocks, iters, 0, nullptr, ctx, stream); }, stream, &ms);
+  rc = measure([&]() { return run_i8(mode, blocks, iters, 0, nullptr, ctx, stream); }, stream, sustained, &ms);
   if (rc != LT_OK) return rc;
   rc = lt_check_device_status();
   if (rc != LT_OK) return rc;

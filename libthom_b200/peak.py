@@ -1,6 +1,7 @@
 """Prints the measured tensor-pipe rates of the current GPU (lt_measure_peak) as one JSON line:
-FP64 mma.sync and the INT8 tcgen05 shapes (M128 N128, M128 N256, CTA pair M256 N128), with the SM
-clock read before and after.
+FP64 mma.sync and the INT8 tcgen05 shapes (M128 N128, M128 N256, CTA pair M256 N128), each as the
+best of `--repeat` single launches (burst) and after 0.5 s at the power limit (sustained), with the
+SM clock read before and after.
 
     python -m libthom_b200.peak [--repeat 3]
 """
@@ -38,6 +39,7 @@ def main():
         vals = [lt.measure_peak(kind) / 1e12 for _ in range(args.repeat)]
         res[name] = max(vals)
         res[name + "_all"] = vals
+        res[name + "_sustained"] = lt.measure_peak(kind | lt.LT_PEAK_SUSTAINED) / 1e12
     res["sm_mhz_after"] = sm_clock_mhz()
     print(json.dumps(res))
 

@@ -59,6 +59,25 @@ def test_cta_pair_kernel_bit_exact(cuda, oracle_mod, M, N, K, s):
     assert_bit_exact(C, oracle_mod.ozaki_dgemm(A, B, C0, 1.25, -0.5, s))
 
 
+@pytest.mark.parametrize("M,N,K,beta,pinned", [(1000, 300, 200, 0.5, True), (300, 130, 96, 0.0, False),
+                                              (2560, 384, 64, 1.0, True)])
+def test_host_resident_bit_exact(cuda, oracle_mod, M, N, K, beta, pinned):
+    """lt_dgemm_ozaki_host: operands in host memory, streamed through the GPU in row panels (a
+    ragged last panel, pageable and pinned buffers, beta = 0 skipping the C0 copy): the same bits
+    as the oracle, and C0 is only read when beta != 0."""
+    import libthom_b200 as lt
+
+    torch = cuda
+    A, B, C0 = oracle_mod.make_problem(M, N, K, phi=4, seed=M + N + K)
+    Ah, Bh = torch.from_numpy(A.copy()), torch.from_numpy(B.copy())
+    Ch = torch.from_numpy(C0.copy() if beta != 0.0 else np.full((M, N), np.nan))
+    if pinned:
+        Ah, Bh, Ch = Ah.pin_memory(), Bh.pin_memory(), Ch.pin_memory()
+    lt.dgemm_ozaki_host(Ah, Bh, Ch, M, N, K, 1.5, beta, slices=6)
+    lt.device_status()
+    assert_bit_exact(Ch.numpy(), oracle_mod.ozaki_dgemm(A, B, C0, 1.5, beta, 6))
+
+
 def test_long_k_multiple_groups(cuda, oracle_mod):
     """K = 20000 > 16640 (the INT32-safe group length of an 8-pair diagonal): two groups."""
     M, N, K = 64, 48, 20000
