@@ -463,10 +463,12 @@ __device__ __forceinline__ void ozaki_body(const Source& src, DeviceStatus* stat
     __syncwarp();
   } else if (warp == 1) {
     // ------------------------------------ MMA issuer ------------------------------------
-    // One thread issues. Right after a stage's MMAs are queued it peeks at the next stage's
-    // barrier while those MMAs still run, so a stage whose copies have landed is issued without
-    // a blocking wait in between.
-    if (lane == 0) {
+    // The whole warp runs the loop and one elected lane issues: under elect.sync the per-MMA
+    // descriptor arithmetic stays in uniform registers (gated by a plain lane test it does not, and
+    // the issue rate drops by a third, measured). Wait results are made warp-uniform. Right after a
+    // stage's MMAs are queued the warp peeks at the next stage's barrier while they run, so a stage
+    // whose copies have landed is issued without a blocking wait in between.
+    {
       const uint64_t desc0 = desc_k_sw32(smem_u32(smem));
       int stage = 0;
       uint32_t phase = 0;
@@ -481,35 +483,45 @@ __device__ __forceinline__ void ozaki_body(const Source& src, DeviceStatus* stat
           const uint64_t chunk_step = static_cast<uint64_t>(2 * bd.nsl * (kTileBytes >> 4));
           for (int64_t c0 = 0; c0 < nkc && ok; c0 += gch) {
             const int64_t c1 = (c0 + gch < nkc) ? c0 + gch : nkc;
-            if (!mbar_wait(acc_empty, (group & 1) ^ 1, abort_flag, status, 12)) { ok = false; break; }
+            if (!__all_sync(0xffffffffu, mbar_wait(acc_empty, (group & 1) ^ 1, abort_flag, status, 12))) {
+              ok = false;
+              break;
+            }
             tc_fence_after();
             for (int64_t cs = c0; cs < c1; cs += cps) {
               const int64_t ce = (cs + cps < c1) ? cs + cps : c1;
-              if (!ready && !mbar_wait(&full[stage], phase, abort_flag, status, 13)) { ok = false; break; }
-              tc_fence_after();
-              uint64_t a0 = desc0 + static_cast<uint64_t>(stage) * (G::kStageBytes >> 4);
-              for (int64_t c = cs; c < ce; ++c, a0 += chunk_step) {
-                const uint32_t acc_first = (c == c0) ? 0u : 1u;
-                switch (b) {
-                  case 0: issue_chunk<S, 0>(a0, tmem_base, acc_first); break;
-                  case 1: issue_chunk<S, 1>(a0, tmem_base, acc_first); break;
-                  default: issue_chunk<S, 2>(a0, tmem_base, acc_first); break;
-                }
+              if (!ready && !__all_sync(0xffffffffu, mbar_wait(&full[stage], phase, abort_flag, status, 13))) {
+                ok = false;
+                break;
               }
+              tc_fence_after();
+              if (elect_one_sync()) {
+                uint64_t a0 = desc0 + static_cast<uint64_t>(stage) * (G::kStageBytes >> 4);
+                for (int64_t c = cs; c < ce; ++c, a0 += chunk_step) {
+                  const uint32_t acc_first = (c == c0) ? 0u : 1u;
+                  switch (b) {
+                    case 0: issue_chunk<S, 0>(a0, tmem_base, acc_first); break;
+                    case 1: issue_chunk<S, 1>(a0, tmem_base, acc_first); break;
+                    default: issue_chunk<S, 2>(a0, tmem_base, acc_first); break;
+                  }
+                }
+                mma_commit(&empty[stage]);
+              }
+              __syncwarp();
               const int next = stage + 1 == G::kStages ? 0 : stage + 1;
               const uint32_t next_phase = stage + 1 == G::kStages ? phase ^ 1 : phase;
-              ready = mbar_try_wait(&full[next], next_phase);
-              mma_commit(&empty[stage]);
+              ready = __all_sync(0xffffffffu, mbar_try_wait(&full[next], next_phase));
               stage = next;
               phase = next_phase;
             }
             if (!ok) break;
-            mma_commit(acc_full);
+            if (elect_one_sync()) mma_commit(acc_full);
+            __syncwarp();
             ++group;
           }
         }
       }
-      if (!ok) {
+      if (!ok && elect_one_sync()) {
         // Let every MMA already issued finish before TMEM is released.
         mma_commit(drain);
         uint64_t t0 = globaltimer();
@@ -788,8 +800,8 @@ __device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatu
     __syncwarp();
   } else if (warp == 1) {
     // --------------------------- rank 0: MMA issuer for the pair ---------------------------
-    // One thread issues, peeking at the next stage's barrier as in ozaki_body.
-    if (lane == 0) {
+    // Warp-convergent loop, one elected lane issues, as in ozaki_body.
+    {
       const uint64_t desc0 = smem_desc_k_sw32(smem_u32(smem));
       int stage = 0;
       uint32_t phase = 0;
@@ -803,37 +815,50 @@ __device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatu
           const uint64_t chunk_step = static_cast<uint64_t>(bd.nsl * (kPairChunkBytes >> 4));
           for (int64_t c0 = 0; c0 < nkc && ok; c0 += gch) {
             const int64_t c1 = (c0 + gch < nkc) ? c0 + gch : nkc;
-            if (!mbar_wait_cluster(acc_empty, (group & 1) ^ 1, abort_flag, status, 23)) { ok = false; break; }
+            if (!__all_sync(0xffffffffu, mbar_wait_cluster(acc_empty, (group & 1) ^ 1, abort_flag, status, 23))) {
+              ok = false;
+              break;
+            }
             tc_fence_after();
             for (int64_t cs = c0; cs < c1; cs += cps) {
               const int64_t ce = (cs + cps < c1) ? cs + cps : c1;
-              if (!ready && !mbar_wait_cluster(&full[stage], phase, abort_flag, status, 24)) { ok = false; break; }
-              tc_fence_after();
-              uint64_t a0 = desc0 + static_cast<uint64_t>(stage) * (G::kStageBytes >> 4);
-              for (int64_t c = cs; c < ce; ++c, a0 += chunk_step) {
-                const uint32_t acc_first = (c == c0) ? 0u : 1u;
-                switch (b) {
-                  case 0: issue_chunk2<S, 0>(a0, tmem_base, acc_first); break;
-                  case 1: issue_chunk2<S, 1>(a0, tmem_base, acc_first); break;
-                  default: issue_chunk2<S, 2>(a0, tmem_base, acc_first); break;
-                }
+              if (!ready &&
+                  !__all_sync(0xffffffffu, mbar_wait_cluster(&full[stage], phase, abort_flag, status, 24))) {
+                ok = false;
+                break;
               }
+              tc_fence_after();
+              if (elect_one_sync()) {
+                uint64_t a0 = desc0 + static_cast<uint64_t>(stage) * (G::kStageBytes >> 4);
+                for (int64_t c = cs; c < ce; ++c, a0 += chunk_step) {
+                  const uint32_t acc_first = (c == c0) ? 0u : 1u;
+                  switch (b) {
+                    case 0: issue_chunk2<S, 0>(a0, tmem_base, acc_first); break;
+                    case 1: issue_chunk2<S, 1>(a0, tmem_base, acc_first); break;
+                    default: issue_chunk2<S, 2>(a0, tmem_base, acc_first); break;
+                  }
+                }
+                mma_commit_pair(cluster_addr(&empty[stage], 0));
+                mma_commit_pair(cluster_addr(&empty[stage], 1));
+              }
+              __syncwarp();
               const int next = stage + 1 == G::kStages ? 0 : stage + 1;
               const uint32_t next_phase = stage + 1 == G::kStages ? phase ^ 1 : phase;
-              ready = mbar_try_wait_cluster(&full[next], next_phase);
-              mma_commit_pair(cluster_addr(&empty[stage], 0));
-              mma_commit_pair(cluster_addr(&empty[stage], 1));
+              ready = __all_sync(0xffffffffu, mbar_try_wait_cluster(&full[next], next_phase));
               stage = next;
               phase = next_phase;
             }
             if (!ok) break;
-            mma_commit_pair(cluster_addr(acc_full, 0));
-            mma_commit_pair(cluster_addr(acc_full, 1));
+            if (elect_one_sync()) {
+              mma_commit_pair(cluster_addr(acc_full, 0));
+              mma_commit_pair(cluster_addr(acc_full, 1));
+            }
+            __syncwarp();
             ++group;
           }
         }
       }
-      if (!ok) {
+      if (!ok && elect_one_sync()) {
         // Let every MMA already issued finish before TMEM is released.
         mma_commit_pair(cluster_addr(drain, 0));
         uint64_t t0 = globaltimer();
