@@ -12,6 +12,29 @@ namespace fp64 {
 
 namespace {
 
+// K split for tile counts that fill the GPU poorly (wave quantisation): the split count S in 1..4
+// minimising waves(S) x (k-blocks per range + pipeline fill) at the FP64 tensor rate, plus the
+// reduction's traffic, and at least 3 % better than no split; ranges keep >= 32 k-blocks.
+int choose_splits(int64_t tiles, int64_t cap, int64_t M, int64_t N, int64_t K, int bm, int bn) {
+  const int64_t nkb = (K + 15) / 16;
+  if (nkb < 64 || cap <= 0) return 1;
+  const double t_kb = 2.0 * bm * bn * 16 / (128.0 * 1.9e9);  // one k-block of one tile on one SM
+  double best = 0.0;
+  int best_s = 1;
+  for (int S = 1; S <= 4; ++S) {
+    const int64_t per = (nkb + S - 1) / S;
+    if (S > 1 && per < 32) break;
+    const int64_t waves = (tiles * S + cap - 1) / cap;
+    double t = static_cast<double>(waves) * static_cast<double>(per + 6) * t_kb;
+    if (S > 1) t += (S + 2) * 8.0 * static_cast<double>(M) * static_cast<double>(N) / 6.0e12;
+    if (S == 1 || t < best * 0.97) {
+      best = t;
+      best_s = S;
+    }
+  }
+  return best_s;
+}
+
 template <class Cfg>
 int launch(const Params& p0, cudaStream_t stream, DeviceContext* ctx) {
   Params p = p0;
@@ -41,10 +64,24 @@ int launch(const Params& p0, cudaStream_t stream, DeviceContext* ctx) {
   });
   LT_CUDA_TRY(attr_err[ctx->device]);
   const int64_t tiles = ((p.M + Cfg::BM - 1) / Cfg::BM) * ((p.N + Cfg::BN - 1) / Cfg::BN);
-  int64_t grid = static_cast<int64_t>(ctx->sm_count) * occupancy[ctx->device];
-  if (grid > tiles) grid = tiles;
+  const int64_t cap = static_cast<int64_t>(ctx->sm_count) * occupancy[ctx->device];
+  p.splits = choose_splits(tiles, cap, p.M, p.N, p.K, Cfg::BM, Cfg::BN);
+  p.W = nullptr;
+  if (p.splits > 1) {
+    void* w = nullptr;
+    LT_TRY(ensure_splitk_workspace(ctx, static_cast<size_t>(p.splits) * p.M * p.N * sizeof(double), &w));
+    p.W = static_cast<double*>(w);
+  }
+  const int64_t units = tiles * p.splits;
+  const int64_t grid = units < cap ? units : cap;
   dgemm_fp64_kernel<Cfg><<<static_cast<unsigned>(grid), Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(tmA, tmB, p);
   LT_CUDA_TRY(cudaGetLastError());
+  if (p.splits > 1) {
+    const int64_t n = p.M * p.N;
+    const int64_t blocks = std::min<int64_t>((n + 255) / 256, static_cast<int64_t>(ctx->sm_count) * 16);
+    splitk_reduce_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p.W, p.C, n, p.splits, p.alpha, p.beta);
+    LT_CUDA_TRY(cudaGetLastError());
+  }
   return LT_OK;
 }
 
@@ -229,7 +266,7 @@ int run_config(int cfg, const double* A, const double* B, double* C, int64_t M, 
   if (cfg < 0 || cfg >= kNumConfigs) return set_error(LT_ERR_INVALID_ARGUMENT, "FP64 config %d out of range", cfg);
   DeviceContext* ctx = context();
   if (ctx == nullptr) return last_error();
-  Params p{A, B, C, M, N, K, alpha, beta, nullptr};
+  Params p{A, B, C, M, N, K, alpha, beta, nullptr, 1, nullptr};
   return kConfigs[cfg].fn(p, stream, ctx);
 }
 

@@ -36,6 +36,10 @@ struct Params {
   int64_t M, N, K;
   double alpha, beta;
   DeviceStatus* status;
+  // K split: `splits` > 1 cuts the k-blocks of every tile into that many contiguous ranges; the
+  // unit for range s writes its raw sums to W + s*M*N (row stride N) and splitk_reduce forms C.
+  int splits;
+  double* W;
 };
 
 template <int BM_, int BN_, int STAGES_, bool TMA_>
@@ -95,7 +99,8 @@ __device__ __forceinline__ void tile_coords(int64_t t, int64_t tiles_m, int64_t 
   tn = in_group / gsize;
 }
 
-// One output tile of one problem.
+// One output tile of one problem, over k-blocks kb0..kb1-1. W != nullptr: write the raw sums
+// there (K-split partial) instead of alpha*acc + beta*C.
 struct Job {
   const double* A;
   const double* B;
@@ -103,18 +108,29 @@ struct Job {
   int64_t M, N, K;
   double alpha, beta;
   int64_t m0, n0;
+  int kb0, kb1;
+  double* W;
 };
 
 // Tiles of a single problem, walked in grouped raster order.
+// With a K split, unit u covers range u / tiles of tile u % tiles, so each wave spans all tiles of
+// one range before the next range starts.
 template <class Cfg>
 struct SingleSource {
   Params p;
   int64_t tiles_m, tiles_n;
-  __device__ int64_t count() const { return tiles_m * tiles_n; }
-  __device__ Job get(int64_t t) const {
+  __device__ int64_t count() const { return tiles_m * tiles_n * p.splits; }
+  __device__ Job get(int64_t u) const {
+    const int64_t tiles = tiles_m * tiles_n;
+    const int64_t sp = u / tiles, t = u - sp * tiles;
     int64_t tm, tn;
     tile_coords(t, tiles_m, tiles_n, tm, tn);
-    return Job{p.A, p.B, p.C, p.M, p.N, p.K, p.alpha, p.beta, tm * Cfg::BM, tn * Cfg::BN};
+    const int nkb = static_cast<int>((p.K + Cfg::BK - 1) / Cfg::BK);
+    const int per = (nkb + p.splits - 1) / p.splits;
+    const int kb0 = static_cast<int>(sp) * per;
+    const int kb1 = kb0 + per < nkb ? kb0 + per : nkb;
+    double* w = p.splits > 1 ? p.W + sp * p.M * p.N : nullptr;
+    return Job{p.A, p.B, p.C, p.M, p.N, p.K, p.alpha, p.beta, tm * Cfg::BM, tn * Cfg::BN, kb0, kb1, w};
   }
 };
 
@@ -140,7 +156,9 @@ struct GroupedSource {
   __device__ Job get(int64_t t) const {
     const GroupTile gt = tiles[t];
     const GroupProblem& pr = problems[gt.problem];
-    return Job{pr.A, pr.B, pr.C, pr.M, pr.N, pr.K, pr.alpha, pr.beta, gt.m0, gt.n0};
+    return Job{pr.A,  pr.B,  pr.C,  pr.M, pr.N,
+               pr.K,  pr.alpha, pr.beta, gt.m0, gt.n0,
+               0,     static_cast<int>((pr.K + 15) / 16), nullptr};
   }
 };
 
@@ -180,8 +198,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
     for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
       const Job J = src.get(t);
       const int64_t m0 = J.m0, n0 = J.n0;
-      const int kblocks = static_cast<int>((J.K + Cfg::BK - 1) / Cfg::BK);
-      for (int kb = 0; kb < kblocks; ++kb) {
+      for (int kb = J.kb0; kb < J.kb1; ++kb) {
         if (!mbar_wait(&empty[stage], phase ^ 1, abort_flag, status, 1)) { ok = false; break; }
         uint8_t* sa = smem + stage * Cfg::STAGE_BYTES;
         uint8_t* sb = sa + Cfg::A_BYTES;
@@ -226,7 +243,6 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
     bool ok = true;
     for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
       const Job J = src.get(t);
-      const int kblocks = static_cast<int>((J.K + Cfg::BK - 1) / Cfg::BK);
       double acc[2][4][4];
 #pragma unroll
       for (int i = 0; i < 2; ++i)
@@ -235,7 +251,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
 #pragma unroll
           for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
 
-      for (int kb = 0; kb < kblocks; ++kb) {
+      for (int kb = J.kb0; kb < J.kb1; ++kb) {
         if (!mbar_wait(&full[stage], phase, abort_flag, status, 2)) { ok = false; break; }
         const uint32_t sa = smem_base + stage * Cfg::STAGE_BYTES;
         const uint32_t sb = sa + Cfg::A_BYTES;
@@ -268,8 +284,31 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
       }
       if (!ok) break;
 
-      // ---- epilogue: C = alpha*acc + beta*C0, 16-byte vectors where the row stride allows ----
+      // ---- epilogue: C = alpha*acc + beta*C0 (or the raw sums into W), 16-byte vectors where the
+      // row stride allows ----
       const int64_t m0 = J.m0 + wm * Cfg::WM, n0 = J.n0 + wn * Cfg::WN;
+      if (J.W != nullptr) {
+        const bool wvec = (J.N & 1) == 0;  // W is 256-byte aligned
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int64_t row = m0 + i * 16 + g + 8 * h;
+            if (row >= J.M) continue;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const int64_t col = n0 + j * 8 + 2 * tq;
+              double* wp = J.W + row * J.N + col;
+              if (wvec && col + 1 < J.N) {
+                *reinterpret_cast<double2*>(wp) = make_double2(acc[i][j][2 * h], acc[i][j][2 * h + 1]);
+              } else {
+                if (col < J.N) wp[0] = acc[i][j][2 * h];
+                if (col + 1 < J.N) wp[1] = acc[i][j][2 * h + 1];
+              }
+            }
+          }
+        continue;
+      }
       const bool vec = ((J.N & 1) == 0) && ((reinterpret_cast<uintptr_t>(J.C) & 15) == 0);
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
@@ -309,6 +348,17 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
     dgemm_fp64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p) {
   SingleSource<Cfg> src{p, (p.M + Cfg::BM - 1) / Cfg::BM, (p.N + Cfg::BN - 1) / Cfg::BN};
   gemm_body<Cfg>(&tmA, &tmB, src, p.status);
+}
+
+// C = alpha * (W_0 + W_1 + ... + W_{splits-1}) + beta * C, summed in split order.
+__global__ void splitk_reduce_kernel(const double* __restrict__ W, double* __restrict__ C, int64_t n, int splits,
+                                     double alpha, double beta) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double s = W[i];
+    for (int k = 1; k < splits; ++k) s += W[k * n + i];
+    C[i] = (beta != 0.0) ? fma(alpha, s, beta * C[i]) : alpha * s;
+  }
 }
 
 template <class Cfg>

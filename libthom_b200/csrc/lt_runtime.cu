@@ -79,14 +79,16 @@ DeviceContext* context() {
   return &c;
 }
 
-int ensure_workspace(DeviceContext* ctx, size_t bytes, void** ptr) {
-  if (ctx->workspace_bytes < bytes) {
-    if (ctx->workspace != nullptr) {
-      // The old buffer may still be in use by work queued on any stream.
+namespace {
+// Grows a cached device buffer to at least `bytes` (12.5 % headroom); the old buffer may still be in
+// use by work queued on any stream, so growing synchronises the device first.
+int ensure_buffer(void** buf, size_t* have, size_t bytes, void** ptr) {
+  if (*have < bytes) {
+    if (*buf != nullptr) {
       LT_CUDA_TRY(cudaDeviceSynchronize());
-      cudaFree(ctx->workspace);
-      ctx->workspace = nullptr;
-      ctx->workspace_bytes = 0;
+      cudaFree(*buf);
+      *buf = nullptr;
+      *have = 0;
     }
     size_t grow = bytes + bytes / 8;
     void* p = nullptr;
@@ -95,11 +97,20 @@ int ensure_workspace(DeviceContext* ctx, size_t bytes, void** ptr) {
       cudaGetLastError();
       return set_error(LT_ERR_NO_MEMORY, "workspace allocation of %zu bytes failed: %s", grow, cudaGetErrorString(e));
     }
-    ctx->workspace = p;
-    ctx->workspace_bytes = grow;
+    *buf = p;
+    *have = grow;
   }
-  *ptr = ctx->workspace;
+  *ptr = *buf;
   return LT_OK;
+}
+}  // namespace
+
+int ensure_workspace(DeviceContext* ctx, size_t bytes, void** ptr) {
+  return ensure_buffer(&ctx->workspace, &ctx->workspace_bytes, bytes, ptr);
+}
+
+int ensure_splitk_workspace(DeviceContext* ctx, size_t bytes, void** ptr) {
+  return ensure_buffer(&ctx->splitk, &ctx->splitk_bytes, bytes, ptr);
 }
 
 EncodeTiledFn encode_tiled() {

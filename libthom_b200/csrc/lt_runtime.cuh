@@ -24,6 +24,8 @@ struct DeviceContext {
   DeviceStatus* status = nullptr;  // device memory, one per device
   void* workspace = nullptr;       // cached Ozaki workspace (grown on demand)
   size_t workspace_bytes = 0;
+  void* splitk = nullptr;          // cached partial sums of K-split FP64 launches
+  size_t splitk_bytes = 0;
   void* l2_flush = nullptr;
   size_t l2_flush_bytes = 0;
 };
@@ -32,6 +34,8 @@ struct DeviceContext {
 DeviceContext* context();
 // Ensures the cached workspace of the current device holds at least `bytes`.
 int ensure_workspace(DeviceContext* ctx, size_t bytes, void** ptr);
+// Same for the FP64 K-split partial sums (a buffer of its own).
+int ensure_splitk_workspace(DeviceContext* ctx, size_t bytes, void** ptr);
 
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,

@@ -15,6 +15,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libref_dgemm.so"
+REF_FINAL_LIB = HERE / "_ref" / "libref_dgemm_final.so"
 
 _c = ctypes
 _vp, _i64, _i32, _f64, _u64 = _c.c_void_p, _c.c_int64, _c.c_int, _c.c_double, _c.c_uint64
@@ -31,6 +32,7 @@ def build(quiet: bool = True) -> None:
 
 _lib = None
 _ref = None
+_ref_final = None
 
 
 def lib() -> ctypes.CDLL:
@@ -77,6 +79,19 @@ def ref_lib() -> ctypes.CDLL | None:
         R.ref_dgemm_host.argtypes = [_vp, _vp, _vp, _i32, _i32, _i32, _f64, _f64]
         _ref = R
     return _ref
+
+
+def ref_final_lib() -> ctypes.CDLL | None:
+    """The reference's dgemm_final CUDA kernel (routines/dgemm/dgemm_final.cu) built for sm_100a,
+    if built here: ref_dgemm_final(A, B, C, M, N, K, alpha, beta) on device pointers, returning
+    the milliseconds its own CUDA events measured."""
+    global _ref_final
+    if _ref_final is None and REF_FINAL_LIB.exists():
+        R = ctypes.CDLL(str(REF_FINAL_LIB))
+        R.ref_dgemm_final.restype = ctypes.c_float
+        R.ref_dgemm_final.argtypes = [_vp, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, _f64, _f64]
+        _ref_final = R
+    return _ref_final
 
 
 def _p(a: np.ndarray) -> int:

@@ -71,6 +71,19 @@ def test_ragged_shapes(cuda, oracle_mod, M, N, K):
     assert oracle_mod.componentwise_error(C, Cref, den)[0] <= fp64_bound(K)
 
 
+@pytest.mark.parametrize("M,N,K,offset,beta", [(256, 256, 8192, 0, 0.5), (1024, 64, 4096, 0, 0.0),
+                                               (300, 130, 5000, 1, 1.0), (128, 96, 2047, 0, -1.0)])
+def test_k_split_shapes(cuda, oracle_mod, M, N, K, offset, beta):
+    """Few tiles and long K: the launch cuts K into ranges whose partial sums are reduced in a
+    second kernel (TMA and cp.async staging, ragged edges, odd K, beta = 0 not reading C)."""
+    A, B, C0 = oracle_mod.make_problem(M, N, K, phi=3, seed=M + K)
+    if beta == 0.0:
+        C0 = np.full_like(C0, np.nan)
+    C = run_fp64(cuda, A, B, C0, 1.25, beta, offset=offset)
+    Cref, den = oracle_mod.dot2_rows(A, B, None if beta == 0.0 else C0, 1.25, beta)
+    assert oracle_mod.componentwise_error(C, Cref, den)[0] <= fp64_bound(K)
+
+
 def test_unaligned_pointers_take_general_path(cuda, oracle_mod):
     M, N, K = 96, 64, 80
     A, B, C0 = oracle_mod.make_problem(M, N, K, seed=4)

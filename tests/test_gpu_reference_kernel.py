@@ -1,0 +1,70 @@
+"""The reference's own best CUDA DGEMM, dgemm_final (routines/dgemm/dgemm_final.cu), compiled for
+sm_100a in oracle/_ref, run beside this library's kernels on the same device buffers: it must give
+a correct result (within the FP64 componentwise bound of the compensated oracle), and this
+library's native FP64 kernel must beat it on the 8192^3 headline shape. The measured times are
+printed (pytest -s) for the record; the reference kernel is never part of the library."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import fp64_bound, to_dev
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ref_final():
+    import oracle
+
+    R = oracle.ref_final_lib()
+    if R is None:
+        pytest.skip("reference dgemm_final not built (reference sources absent at build time)")
+    return R
+
+
+def test_reference_final_kernel_is_correct(cuda, oracle_mod, ref_final):
+    torch = cuda
+    M, N, K = 256, 256, 512  # tile multiples, as the reference kernel requires
+    A, B, C0 = oracle_mod.make_problem(M, N, K, phi=2, seed=11)
+    dA, dB, dC = to_dev(torch, A), to_dev(torch, B), to_dev(torch, C0)
+    ms = ref_final.ref_dgemm_final(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), M, N, K, 1.5, 0.5)
+    torch.cuda.synchronize()
+    assert ms > 0
+    Cref, den = oracle_mod.dot2_rows(A, B, C0, 1.5, 0.5)
+    err = oracle_mod.componentwise_error(dC.cpu().numpy().reshape(M, N), Cref, den)[0]
+    assert err <= fp64_bound(K), err
+
+
+def test_native_and_ozaki_beat_reference_final_at_8192(cuda, ref_final):
+    import libthom_b200 as lt
+
+    torch = cuda
+    n = 8192
+    A = torch.empty(n, n, dtype=torch.float64, device="cuda")
+    B = torch.empty_like(A)
+    C = torch.empty_like(A)
+    lt.fill(A, n * n, 1234, 1, 0)
+    lt.fill(B, n * n, 1234, 2, 0)
+    lt.fill(C, n * n, 1234, 3, 0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    flop = 2.0 * n ** 3
+    t_ref = timed(lambda: ref_final.ref_dgemm_final(A.data_ptr(), B.data_ptr(), C.data_ptr(), n, n, n, 1.5, 0.5))
+    t_fp64 = timed(lambda: lt.dgemm_fp64(A, B, C, n, n, n, 1.5, 0.5))
+    t_oz = timed(lambda: lt.dgemm_ozaki(A, B, C, n, n, n, 1.5, 0.5, slices=8))
+    lt.device_status()
+    tf = {k: flop / (v * 1e-3) / 1e12 for k, v in (("reference dgemm_final", t_ref), ("tc100", t_fp64),
+                                                   ("ozaki8", t_oz))}
+    print("8192^3 TFLOP/s:", {k: round(v, 2) for k, v in tf.items()})
+    assert t_fp64 < t_ref and t_oz < t_fp64, tf
