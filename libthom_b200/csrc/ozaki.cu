@@ -182,6 +182,78 @@ __device__ __forceinline__ void split_value(double a, int e, int j, uint32_t (&p
   }
 }
 
+// ---- four values at a time, S <= 8 (X < 2^56) ----
+// X = floor(|a| 2^(7S - e)) as in split_value, and the sign bit of a; X = 0 for a zero or
+// non-finite entry.
+template <int S>
+__device__ __forceinline__ unsigned long long digit_string(double a, int e, uint32_t* neg) {
+  static_assert(7 * S <= 56, "four-at-a-time path covers S <= 8");
+  const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(a));
+  const unsigned long long mag = bits & 0x7fffffffffffffffull;
+  const int E = static_cast<int>(mag >> 52);
+  *neg = static_cast<uint32_t>(bits >> 63);
+  if (mag == 0ull || E == 0x7ff) return 0ull;
+  unsigned long long m = mag & 0x000fffffffffffffull;
+  int t;
+  if (E == 0) {
+    t = -1074;
+  } else {
+    m |= 0x0010000000000000ull;
+    t = E - 1075;
+  }
+  const int sh = t - e + 7 * S;
+  if (sh >= 0) return m << sh;
+  return (-sh >= 64) ? 0ull : (m >> (-sh));
+}
+
+// Moves four 7-bit fields (bits 0..27) into the four bytes of a word: byte i = bits 7i..7i+6.
+__device__ __forceinline__ uint32_t spread7x4(uint32_t w) {
+  w = (w & 0x00003FFFu) | ((w & 0x0FFFC000u) << 2);
+  return (w & 0x007F007Fu) | ((w & 0x3F803F80u) << 1);
+}
+
+// 4 x 4 byte transpose: on return w[i] byte j = (input w[j]) byte i.
+__device__ __forceinline__ void transpose4x4(uint32_t (&w)[4]) {
+  const uint32_t t0 = __byte_perm(w[0], w[1], 0x5140), t1 = __byte_perm(w[0], w[1], 0x7362);
+  const uint32_t t2 = __byte_perm(w[2], w[3], 0x5140), t3 = __byte_perm(w[2], w[3], 0x7362);
+  w[0] = __byte_perm(t0, t2, 0x5410);
+  w[1] = __byte_perm(t0, t2, 0x7632);
+  w[2] = __byte_perm(t1, t3, 0x5410);
+  w[3] = __byte_perm(t1, t3, 0x7632);
+}
+
+// Slices of four consecutive values v[0..3] (K positions 4w .. 4w+3 of one row): sets word w of
+// every slice, packed[p][w] byte i = digit p of v[i] as a two's-complement byte. The digits are the
+// same as split_value's: byte i of spread7x4(X) is bits 7i..7i+6 of X, i.e. slice S-1-i (low word)
+// and S-5-i (high word, X >> 28); a negative value's digit bytes are negated (__vsub4).
+template <int S>
+__device__ __forceinline__ void split4(const double (&v)[4], int e, int w, uint32_t (&packed)[S][8]) {
+  uint32_t lo[4], hi[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    uint32_t neg;
+    const unsigned long long X = digit_string<S>(v[i], e, &neg);
+    uint32_t l = spread7x4(static_cast<uint32_t>(X) & 0x0FFFFFFFu);
+    uint32_t h = spread7x4(static_cast<uint32_t>(X >> 28));
+    if (neg) {
+      l = __vsub4(0u, l);
+      h = __vsub4(0u, h);
+    }
+    lo[i] = l;
+    hi[i] = h;
+  }
+  transpose4x4(lo);
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    if (S - 1 - i >= 0) packed[(S - 1 - i) >= 0 ? S - 1 - i : 0][w] = lo[i];
+  if constexpr (S > 4) {
+    transpose4x4(hi);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if (S - 5 - i >= 0) packed[(S - 5 - i) >= 0 ? S - 5 - i : 0][w] = hi[i];
+  }
+}
+
 // Writes row r (32 bytes per slice) of tile (rb, c) of every slice, in the swizzled tile order.
 template <int S>
 __device__ __forceinline__ void store_tile_row(int8_t* out, int64_t RB, int64_t NC, int64_t rb, int64_t c, int r,
@@ -214,11 +286,26 @@ __device__ __forceinline__ void split_rows_tile(const double* __restrict__ A, in
     const int e = exponent_of_maxbits(amax[row]);
     const double* a = A + row * K;
     const int64_t k0 = c * kChunk;
+    if constexpr (7 * S <= 56) {
+      if (e != kSentinel) {
 #pragma unroll
-    for (int j = 0; j < kChunk; ++j) {
-      const int64_t k = k0 + j;
-      const double v = (k < K) ? __ldg(a + k) : 0.0;
-      split_value<S>(v, e, j, packed);
+        for (int w = 0; w < 8; ++w) {
+          double v[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int64_t k = k0 + 4 * w + i;
+            v[i] = (k < K) ? __ldg(a + k) : 0.0;
+          }
+          split4<S>(v, e, w, packed);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < kChunk; ++j) {
+        const int64_t k = k0 + j;
+        const double v = (k < K) ? __ldg(a + k) : 0.0;
+        split_value<S>(v, e, j, packed);
+      }
     }
   }
   store_tile_row<S>(out, RB, NC, rb, c, r, packed);
@@ -238,11 +325,26 @@ __device__ __forceinline__ void split_cols_tile(const double* __restrict__ B, in
   if (col < N) {
     const int e = exponent_of_maxbits(amax[col]);
     const int64_t k0 = c * kChunk;
+    if constexpr (7 * S <= 56) {
+      if (e != kSentinel) {
 #pragma unroll
-    for (int j = 0; j < kChunk; ++j) {
-      const int64_t k = k0 + j;
-      const double v = (k < K) ? __ldg(B + k * N + col) : 0.0;
-      split_value<S>(v, e, j, packed);
+        for (int w = 0; w < 8; ++w) {
+          double v[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int64_t k = k0 + 4 * w + i;
+            v[i] = (k < K) ? __ldg(B + k * N + col) : 0.0;
+          }
+          split4<S>(v, e, w, packed);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < kChunk; ++j) {
+        const int64_t k = k0 + j;
+        const double v = (k < K) ? __ldg(B + k * N + col) : 0.0;
+        split_value<S>(v, e, j, packed);
+      }
     }
   }
   store_tile_row<S>(out, RB, NC, rb, c, r, packed);
