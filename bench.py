@@ -497,6 +497,72 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def run_sweep(args) -> None:
+    """The 8192^3 slice-count table: for phi in {0, 8, 32} (entries u 2^e, e ~ U{-phi..phi}), the
+    native FP64 kernel, cuBLAS and the Ozaki path at s = 3..8 (and up to 12 when 8 is not enough),
+    each with its CUDA-event time and its max componentwise error on sampled rows against the
+    compensated oracle and against the native FP64 result C64. One JSON line per phi."""
+    import numpy as np
+    import torch
+
+    import libthom_b200 as lt
+    import oracle
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    n = args.size
+    flop = 2.0 * n ** 3
+    A = torch.empty(n, n, dtype=torch.float64, device=dev)
+    B = torch.empty_like(A)
+    C0 = torch.empty_like(A)
+    C = torch.empty_like(A)
+    ws = torch.empty(lt.ozaki_workspace_size(n, n, n, lt.LT_OZAKI_MAX_SLICES), dtype=torch.uint8, device=dev)
+    rows = np.linspace(0, n - 1, args.check_rows).astype(np.int64)
+    rows_d = torch.from_numpy(rows).to(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            C.copy_(C0)
+            fn()
+        ts = []
+        for _ in range(args.steps):
+            C.copy_(C0)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    for phi in (0, 8, 32):
+        lt.fill(A, n * n, SEED, 1, phi, stream)
+        lt.fill(B, n * n, SEED, 2, phi, stream)
+        lt.fill(C0, n * n, SEED, 3, phi, stream)
+        torch.cuda.synchronize()
+        Cref, den = oracle.dot2_rows(A.cpu().numpy(), B.cpu().numpy(), C0.cpu().numpy(), 1.5, 0.5, rows=rows)
+        res = {}
+        ms = timed(lambda: lt.dgemm_fp64(A, B, C, n, n, n, 1.5, 0.5, stream))
+        c64 = C[rows_d].cpu().numpy()
+        res["native_fp64"] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms": ms,
+                              "err_vs_oracle": oracle.componentwise_error(c64, Cref, den)[0]}
+        ms = timed(lambda: lt.dgemm_cublas(A, B, C, n, n, n, 1.5, 0.5, stream))
+        res["cublas"] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms": ms,
+                         "err_vs_oracle": oracle.componentwise_error(C[rows_d].cpu().numpy(), Cref, den)[0]}
+        for sl in range(3, lt.LT_OZAKI_MAX_SLICES + 1):
+            ms = timed(lambda: lt.dgemm_ozaki(A, B, C, n, n, n, 1.5, 0.5, sl, stream, workspace=ws))
+            cs = C[rows_d].cpu().numpy()
+            e = oracle.componentwise_error(cs, Cref, den)[0]
+            res[f"ozaki{sl}"] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms": ms, "err_vs_oracle": e,
+                                 "err_vs_c64": oracle.componentwise_error(cs, c64, den)[0]}
+            if sl >= 8 and e <= res["native_fp64"]["err_vs_oracle"]:
+                break
+        lt.device_status()
+        print(json.dumps({"sweep": f"{n}^3 alpha=1.5 beta=0.5 phi={phi}", "rows_checked": len(rows),
+                          "oracle": "compensated Dot2", "results": res}), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -512,9 +578,13 @@ def main() -> None:
     ap.add_argument("--check-rows", type=int, default=16)
     ap.add_argument("--cpu-rows", type=int, default=1024)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--sweep", action="store_true",
+                    help="print the phi x slice-count table (error and TFLOP/s of every form) instead")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps, reported as run
-    if args.impl == "reference":
+    if args.sweep:
+        run_sweep(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

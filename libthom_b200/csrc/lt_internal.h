@@ -21,11 +21,12 @@ int run_config(int cfg, const double* A, const double* B, double* C, int64_t M, 
                double beta, cudaStream_t stream);
 }  // namespace fp64
 
-// Selector statistics (selector_stats.cu). features_into needs kStatsScratchBytes of scratch,
-// gap_into 8 (M + N) bytes and a zeroed pair of ints at `out` (row gap, column gap).
-constexpr size_t kStatsScratchBytes = 4096;
-int features_into(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, float* feat,
-                  void* scratch, cudaStream_t stream);
+// Selector statistics (selector_stats.cu). selector_infer: the features of one problem (copied to
+// feat_dev, 34 floats, when given) and, with the network's device parameters, its class
+// probabilities (into probs_host, when given); synchronous, one call at a time per process.
+// gap_into needs 8 (M + N) bytes of scratch and a zeroed pair of ints at `out` (row gap, column gap).
+int selector_infer(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, const float* params,
+                   float* feat_dev, float* probs_host, cudaStream_t stream);
 int gap_into(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int* out, void* scratch,
              cudaStream_t stream);
 

@@ -23,69 +23,10 @@
 
 #include "lt_internal.h"
 #include "lt_runtime.cuh"
+#include "selector_common.cuh"
 
 namespace lt {
 namespace sel {
-
-constexpr int F = LT_SEL_FEATURES, H = LT_SEL_HIDDEN, C = LT_SEL_CLASSES, P = LT_SEL_PARAMS;
-constexpr int OW1 = 0, OB1 = OW1 + H * F, OW2 = OB1 + H, OB2 = OW2 + H * H, OW3 = OB2 + H, OB3 = OW3 + C * H;
-static_assert(OB3 + C == P, "parameter layout");
-// ---------------------------------------------------------------------------------------------
-// MLP
-// ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ float gelu(float x) {
-  const float k = 0.7978845608028654f;  // sqrt(2/pi)
-  float t = tanhf(k * (x + 0.044715f * x * x * x));
-  return 0.5f * x * (1.f + t);
-}
-__device__ __forceinline__ float gelu_grad(float x) {
-  const float k = 0.7978845608028654f;
-  float u = k * (x + 0.044715f * x * x * x);
-  float t = tanhf(u);
-  return 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * k * (1.f + 3.f * 0.044715f * x * x);
-}
-
-struct Acts {
-  float x[F], h1[H], a1[H], h2[H], a2[H], logit[C], prob[C];
-};
-
-// Block of H threads computes one sample's forward pass into shared memory.
-__device__ void forward_block(const float* __restrict__ p, const float* __restrict__ x, Acts& s) {
-  const int t = threadIdx.x;
-  for (int i = t; i < F; i += blockDim.x) s.x[i] = x[i];
-  __syncthreads();
-  if (t < H) {
-    float acc = p[OB1 + t];
-    for (int i = 0; i < F; ++i) acc += p[OW1 + t * F + i] * s.x[i];
-    s.h1[t] = acc;
-    s.a1[t] = gelu(acc);
-  }
-  __syncthreads();
-  if (t < H) {
-    float acc = p[OB2 + t];
-    for (int i = 0; i < H; ++i) acc += p[OW2 + t * H + i] * s.a1[i];
-    s.h2[t] = acc;
-    s.a2[t] = gelu(acc);
-  }
-  __syncthreads();
-  if (t < C) {
-    float acc = p[OB3 + t];
-    for (int i = 0; i < H; ++i) acc += p[OW3 + t * H + i] * s.a2[i];
-    s.logit[t] = acc;
-  }
-  __syncthreads();
-  if (t == 0) {
-    float mx = s.logit[0];
-    for (int c = 1; c < C; ++c) mx = fmaxf(mx, s.logit[c]);
-    float sum = 0.f;
-    for (int c = 0; c < C; ++c) {
-      s.prob[c] = expf(s.logit[c] - mx);
-      sum += s.prob[c];
-    }
-    for (int c = 0; c < C; ++c) s.prob[c] /= sum;
-  }
-  __syncthreads();
-}
 
 __global__ void mlp_forward_kernel(const float* __restrict__ p, const float* __restrict__ x, int batch,
                                    float* __restrict__ probs) {
@@ -306,25 +247,17 @@ int select(const double* A, const double* B, int64_t M, int64_t N, int64_t K, do
   LT_TRY(device_params(&params));
   *learned = false;
   *gap_bits = -1;
-  const size_t head = kStatsScratchBytes + 256;
+  const size_t head = 256;
   uint8_t* d = nullptr;
-  LT_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&d), head + 8 * (M + N), stream));
-  float* feat = reinterpret_cast<float*>(d + kStatsScratchBytes);   // 34 floats
-  float* probs = feat + 48;                                          // 8 floats
-  int* gap = reinterpret_cast<int*>(probs + 8);                      // 2 ints
   int rc = LT_OK;
   cudaError_t e = cudaSuccess;
   if (params != nullptr) {
-    rc = features_into(A, B, M, N, K, tol, feat, d, stream);
-    if (rc == LT_OK) {
-      mlp_forward_kernel<<<1, H, 0, stream>>>(params, feat, 1, probs);
-      e = cudaGetLastError();
-    }
     float hp[C];
-    if (rc == LT_OK && e == cudaSuccess) e = cudaMemcpyAsync(hp, probs, sizeof hp, cudaMemcpyDeviceToHost, stream);
-    if (rc == LT_OK && e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    if (rc == LT_OK && e == cudaSuccess) *learned = decide(hp, slices);
+    rc = selector_infer(A, B, M, N, K, tol, params, nullptr, hp, stream);
+    if (rc == LT_OK) *learned = decide(hp, slices);
   }
+  if (rc == LT_OK && !*learned) e = cudaMallocAsync(reinterpret_cast<void**>(&d), head + 8 * (M + N), stream);
+  int* gap = reinterpret_cast<int*>(d);  // 2 ints
   if (rc == LT_OK && e == cudaSuccess && !*learned) {
     e = cudaMemsetAsync(gap, 0, 2 * sizeof(int), stream);
     if (e == cudaSuccess) rc = gap_into(A, B, M, N, K, gap, d + head, stream);
@@ -336,7 +269,7 @@ int select(const double* A, const double* B, int64_t M, int64_t N, int64_t K, do
       *slices = analytic(tol, *gap_bits);
     }
   }
-  cudaFreeAsync(d, stream);
+  if (d != nullptr) cudaFreeAsync(d, stream);
   if (rc != LT_OK) return rc;
   if (e != cudaSuccess) return set_error(LT_ERR_CUDA, "slice selection: %s", cudaGetErrorString(e));
   return LT_OK;

@@ -9,48 +9,30 @@
 // atomics and histograms through shared-memory then global atomic counts, so the results do not
 // depend on scheduling (the CPU oracle, oracle_features / oracle_max_gap, gives the same numbers).
 #include <cmath>
+#include <cstring>
+#include <mutex>
 
 #include "lt_internal.h"
 #include "lt_runtime.cuh"
+#include "selector_common.cuh"
 
 namespace lt {
 namespace sel {
 
-constexpr int kSampleRows = 128;  // rows of A sampled for the features (evenly spaced)
-constexpr int kColGroups = 4;     // groups of 32 consecutive columns of B sampled for the features
-constexpr int kNone = -0x7f7f7f80;  // memset(0x80) pattern: "no nonzero entry seen" for a max
-constexpr int kNoneMin = 0x7f7f7f7f;  // memset(0x7f) pattern for a min
-
-__device__ __forceinline__ int exp_of(double v) {
-  int e;
-  frexp(v, &e);
-  return e;
-}
-__device__ __forceinline__ bool counts(double v) { return v != 0.0 && isfinite(v); }
-__device__ __forceinline__ int gap_bin(int g) { return g >= 60 ? 15 : (g < 0 ? 0 : g >> 2); }
-
-__device__ __forceinline__ int64_t sampled_row(int i, int rows, int64_t M) {
-  return rows > 1 ? (static_cast<int64_t>(i) * (M - 1)) / (rows - 1) : 0;
-}
-__device__ __forceinline__ int64_t sampled_col0(int g, int groups, int64_t N) {
-  const int64_t span = N > 32 ? N - 32 : 0;
-  return groups > 1 ? (static_cast<int64_t>(g) * span) / (groups - 1) : 0;
-}
-
 // ---- features: pass 1 (largest exponent), pass 2 (gap histogram) ----
-// Rows: grid (sampled row, K segment), 256 threads stride the segment.
+// Row piece: sampled row i, K segment `seg` of length kseg; 256 threads stride the segment.
 template <bool kHist>
-__global__ void feat_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K, int rows, int64_t kseg,
-                                 int* __restrict__ rmax, unsigned int* __restrict__ hist) {
-  __shared__ unsigned int sh[16];
-  const int64_t row = sampled_row(blockIdx.x, rows, M);
-  const int64_t k0 = static_cast<int64_t>(blockIdx.y) * kseg;
+__device__ __forceinline__ void rows_piece(const double* __restrict__ A, int64_t M, int64_t K, int rows, int64_t kseg,
+                                           int i, int64_t seg, int* __restrict__ rmax, unsigned int* __restrict__ hist,
+                                           unsigned int* sh) {
+  const int64_t row = sampled_row(i, rows, M);
+  const int64_t k0 = seg * kseg;
   const int64_t k1 = k0 + kseg < K ? k0 + kseg : K;
   const double* a = A + row * K;
   if (kHist) {
     if (threadIdx.x < 16) sh[threadIdx.x] = 0;
     __syncthreads();
-    const int em = rmax[blockIdx.x];
+    const int em = __ldcg(&rmax[i]);
     for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
       const double v = fabs(a[k]);
       atomicAdd(&sh[counts(v) ? gap_bin(em - exp_of(v)) : 0], 1u);
@@ -64,25 +46,26 @@ __global__ void feat_rows_kernel(const double* __restrict__ A, int64_t M, int64_
       if (counts(v)) m = max(m, exp_of(v));
     }
     for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0 && m != kNone) atomicMax(&rmax[blockIdx.x], m);
+    if ((threadIdx.x & 31) == 0 && m != kNone) atomicMax(&rmax[i], m);
   }
 }
 
-// Columns: grid (sampled group of 32 columns, K segment), 8 warps; lane = column, warps stride K.
+// Column piece: sampled group g of 32 columns, K segment `seg`; 8 warps, lane = column, warps
+// stride K.
 template <bool kHist>
-__global__ void feat_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N, int groups, int64_t kseg,
-                                 int* __restrict__ cmax, unsigned int* __restrict__ hist) {
-  __shared__ unsigned int sh[16];
+__device__ __forceinline__ void cols_piece(const double* __restrict__ B, int64_t K, int64_t N, int groups, int64_t kseg,
+                                           int g, int64_t seg, int* __restrict__ cmax, unsigned int* __restrict__ hist,
+                                           unsigned int* sh) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int64_t col = sampled_col0(blockIdx.x, groups, N) + lane;
-  const int64_t k0 = static_cast<int64_t>(blockIdx.y) * kseg;
+  const int64_t col = sampled_col0(g, groups, N) + lane;
+  const int64_t k0 = seg * kseg;
   const int64_t k1 = k0 + kseg < K ? k0 + kseg : K;
-  int* cm = cmax + blockIdx.x * 32 + lane;
+  int* cm = cmax + g * 32 + lane;
   if (kHist) {
     if (threadIdx.x < 16) sh[threadIdx.x] = 0;
     __syncthreads();
     if (col < N) {
-      const int em = *cm;
+      const int em = __ldcg(cm);
       for (int64_t k = k0 + warp; k < k1; k += nwarps) {
         const double v = fabs(B[k * N + col]);
         atomicAdd(&sh[counts(v) ? gap_bin(em - exp_of(v)) : 0], 1u);
@@ -100,19 +83,97 @@ __global__ void feat_cols_kernel(const double* __restrict__ B, int64_t K, int64_
   }
 }
 
-__global__ void features_finish_kernel(const unsigned int* __restrict__ hist, int64_t K, double tol,
-                                       float* __restrict__ feat) {
-  const int t = threadIdx.x;
+// Rows: grid (sampled row, K segment). Columns: grid (sampled group of 32 columns, K segment).
+template <bool kHist>
+__global__ void feat_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K, int rows, int64_t kseg,
+                                 int* __restrict__ rmax, unsigned int* __restrict__ hist) {
+  __shared__ unsigned int sh[16];
+  rows_piece<kHist>(A, M, K, rows, kseg, blockIdx.x, blockIdx.y, rmax, hist, sh);
+}
+template <bool kHist>
+__global__ void feat_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N, int groups, int64_t kseg,
+                                 int* __restrict__ cmax, unsigned int* __restrict__ hist) {
+  __shared__ unsigned int sh[16];
+  cols_piece<kHist>(B, K, N, groups, kseg, blockIdx.x, blockIdx.y, cmax, hist, sh);
+}
+
+// Feature i < 32 from the two 16-bin histograms (each normalised by its own total), then
+// log2 K / 16 and -log10(tol) / 16.
+__device__ __forceinline__ float feature_value(const unsigned int* hist, int t, int64_t K, double tol) {
   if (t < 32) {
     const unsigned int* h = hist + (t < 16 ? 0 : 16);
     unsigned long long tot = 0;
-    for (int i = 0; i < 16; ++i) tot += h[i];
-    feat[t] = tot ? static_cast<float>(static_cast<double>(hist[t]) / static_cast<double>(tot)) : 0.f;
-  } else if (t == 32) {
-    feat[32] = static_cast<float>(log2(static_cast<double>(K > 0 ? K : 1)) / 16.0);
-  } else if (t == 33) {
-    feat[33] = static_cast<float>(-log10(tol) / 16.0);
+    for (int i = 0; i < 16; ++i) tot += __ldcg(&h[i]);
+    return tot ? static_cast<float>(static_cast<double>(__ldcg(&hist[t])) / static_cast<double>(tot)) : 0.f;
   }
+  if (t == 32) return static_cast<float>(log2(static_cast<double>(K > 0 ? K : 1)) / 16.0);
+  return static_cast<float>(-log10(tol) / 16.0);
+}
+
+// ---- the selector's one-call statistics: two launches over a combined grid (row pieces, then
+// column pieces) on a persistent per-device scratch. The second launch's last block (an atomic
+// count, no block waits for another) turns the histograms into features, runs the network when
+// given its parameters, and resets the scratch for the next call. ----
+struct FeatGrid {
+  int rows, groups, rseg, cseg;
+  int64_t kr, kc;
+};
+
+struct SelScratch {
+  unsigned int hist[32];
+  int rmax[kSampleRows];
+  int cmax[32 * kColGroups];
+  unsigned int done;
+  unsigned int pad[3];
+  float out[64];  // features [0, 34), probabilities [48, 56)
+};
+
+__global__ void feat_max_fused_kernel(const double* __restrict__ A, const double* __restrict__ B, int64_t M, int64_t N,
+                                      int64_t K, FeatGrid g, SelScratch* __restrict__ sc) {
+  __shared__ unsigned int sh[16];
+  const int nr = g.rows * g.rseg;
+  const int b = blockIdx.x;
+  if (b < nr)
+    rows_piece<false>(A, M, K, g.rows, g.kr, b / g.rseg, b % g.rseg, sc->rmax, nullptr, sh);
+  else
+    cols_piece<false>(B, K, N, g.groups, g.kc, (b - nr) / g.cseg, (b - nr) % g.cseg, sc->cmax, nullptr, sh);
+}
+
+__global__ void feat_hist_fused_kernel(const double* __restrict__ A, const double* __restrict__ B, int64_t M,
+                                       int64_t N, int64_t K, FeatGrid g, double tol,
+                                       const float* __restrict__ params, SelScratch* __restrict__ sc) {
+  __shared__ unsigned int sh[16];
+  __shared__ float fx[F];
+  __shared__ Acts acts;
+  __shared__ int last;
+  const int nr = g.rows * g.rseg;
+  const int b = blockIdx.x;
+  if (b < nr)
+    rows_piece<true>(A, M, K, g.rows, g.kr, b / g.rseg, b % g.rseg, sc->rmax, sc->hist, sh);
+  else
+    cols_piece<true>(B, K, N, g.groups, g.kc, (b - nr) / g.cseg, (b - nr) % g.cseg, sc->cmax, sc->hist + 16, sh);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&sc->done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int t = threadIdx.x; t < F; t += blockDim.x) {
+    fx[t] = feature_value(sc->hist, t, K, tol);
+    sc->out[t] = fx[t];
+  }
+  __syncthreads();
+  if (params != nullptr) {
+    forward_block(params, fx, acts);
+    if (threadIdx.x < C) sc->out[48 + threadIdx.x] = acts.prob[threadIdx.x];
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < 32; t += blockDim.x) sc->hist[t] = 0u;
+  for (int t = threadIdx.x; t < kSampleRows; t += blockDim.x) sc->rmax[t] = kNone;
+  for (int t = threadIdx.x; t < 32 * kColGroups; t += blockDim.x) sc->cmax[t] = kNone;
+  if (threadIdx.x == 0) sc->done = 0u;
 }
 
 // ---- largest exponent gap of any row of A / column of B ----
@@ -186,27 +247,55 @@ int64_t k_segment(int64_t K, int64_t outer, int64_t target, int64_t align) {
 
 }  // namespace sel
 
-// Features into `feat` (device, 34 floats). `scratch` must hold kStatsScratchBytes.
-int features_into(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, float* feat,
-                  void* scratch, cudaStream_t stream) {
+namespace {
+std::mutex g_sel_mutex;
+sel::SelScratch* g_sel_scratch[64] = {};
+float* g_sel_host[64] = {};
+}  // namespace
+
+int selector_infer(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, const float* params,
+                   float* feat_dev, float* probs_host, cudaStream_t stream) {
   DeviceContext* ctx = context();
   if (ctx == nullptr) return last_error();
-  auto* hist = static_cast<unsigned int*>(scratch);                 // 32
-  int* rmax = reinterpret_cast<int*>(hist + 32);                   // kSampleRows
-  int* cmax = rmax + sel::kSampleRows;                              // 32 * kColGroups
-  LT_CUDA_TRY(cudaMemsetAsync(hist, 0, 32 * sizeof(unsigned int), stream));
-  LT_CUDA_TRY(cudaMemsetAsync(rmax, 0x80, (sel::kSampleRows + 32 * sel::kColGroups) * sizeof(int), stream));
-  const int rows = static_cast<int>(M < sel::kSampleRows ? M : sel::kSampleRows);
-  const int groups = static_cast<int>((N + 31) / 32 < sel::kColGroups ? (N + 31) / 32 : sel::kColGroups);
+  // One selection at a time per process: the scratch is per device, and every call synchronises
+  // before it returns, so no two calls' kernels overlap on the GPU.
+  std::lock_guard<std::mutex> lock(g_sel_mutex);
+  const int dev = ctx->device;
+  if (g_sel_scratch[dev] == nullptr) {
+    sel::SelScratch* sc = nullptr;
+    LT_CUDA_TRY(cudaMalloc(&sc, sizeof(sel::SelScratch)));
+    cudaError_t e = cudaMemset(sc, 0, sizeof(sel::SelScratch));
+    if (e == cudaSuccess) e = cudaMemset(sc->rmax, 0x80, sizeof(sc->rmax) + sizeof(sc->cmax));  // kNone
+    float* h = nullptr;
+    if (e == cudaSuccess) e = cudaMallocHost(&h, 64 * sizeof(float));
+    if (e != cudaSuccess) {
+      cudaFree(sc);
+      return set_error(LT_ERR_CUDA, "selector scratch: %s", cudaGetErrorString(e));
+    }
+    g_sel_scratch[dev] = sc;
+    g_sel_host[dev] = h;
+  }
+  sel::SelScratch* sc = g_sel_scratch[dev];
+  sel::FeatGrid g;
+  g.rows = static_cast<int>(M < sel::kSampleRows ? M : sel::kSampleRows);
+  g.groups = static_cast<int>((N + 31) / 32 < sel::kColGroups ? (N + 31) / 32 : sel::kColGroups);
   const int64_t target = 4LL * ctx->sm_count;
-  const int64_t kr = sel::k_segment(K, rows, target, 256), kc = sel::k_segment(K, groups, target, 64);
-  const dim3 gr(rows, static_cast<unsigned>((K + kr - 1) / kr)), gc(groups, static_cast<unsigned>((K + kc - 1) / kc));
-  sel::feat_rows_kernel<false><<<gr, 256, 0, stream>>>(A, M, K, rows, kr, rmax, hist);
-  sel::feat_cols_kernel<false><<<gc, 256, 0, stream>>>(B, K, N, groups, kc, cmax, hist + 16);
-  sel::feat_rows_kernel<true><<<gr, 256, 0, stream>>>(A, M, K, rows, kr, rmax, hist);
-  sel::feat_cols_kernel<true><<<gc, 256, 0, stream>>>(B, K, N, groups, kc, cmax, hist + 16);
-  sel::features_finish_kernel<<<1, 64, 0, stream>>>(hist, K, tol, feat);
+  g.kr = sel::k_segment(K, g.rows, target, 256);
+  g.kc = sel::k_segment(K, g.groups, target, 64);
+  g.rseg = static_cast<int>((K + g.kr - 1) / g.kr);
+  g.cseg = static_cast<int>((K + g.kc - 1) / g.kc);
+  const unsigned blocks = static_cast<unsigned>(g.rows * g.rseg + g.groups * g.cseg);
+  sel::feat_max_fused_kernel<<<blocks, 256, 0, stream>>>(A, B, M, N, K, g, sc);
   LT_CUDA_TRY(cudaGetLastError());
+  sel::feat_hist_fused_kernel<<<blocks, 256, 0, stream>>>(A, B, M, N, K, g, tol, params, sc);
+  LT_CUDA_TRY(cudaGetLastError());
+  if (feat_dev != nullptr)
+    LT_CUDA_TRY(cudaMemcpyAsync(feat_dev, sc->out, sel::F * sizeof(float), cudaMemcpyDeviceToDevice, stream));
+  float* h = g_sel_host[dev];
+  if (probs_host != nullptr)
+    LT_CUDA_TRY(cudaMemcpyAsync(h, sc->out + 48, sel::C * sizeof(float), cudaMemcpyDeviceToHost, stream));
+  LT_CUDA_TRY(cudaStreamSynchronize(stream));
+  if (probs_host != nullptr) memcpy(probs_host, h, sel::C * sizeof(float));
   return LT_OK;
 }
 
@@ -246,13 +335,7 @@ int lt_ozaki_features(const double* A, const double* B, int64_t M, int64_t N, in
                       void* stream) {
   if (M <= 0 || N <= 0 || K <= 0 || A == nullptr || B == nullptr || features == nullptr || !(tol > 0.0))
     return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_ozaki_features: bad arguments");
-  if (lt::context() == nullptr) return lt::last_error();
-  cudaStream_t s = lt::as_stream(stream);
-  void* scratch = nullptr;
-  LT_CUDA_TRY(cudaMallocAsync(&scratch, lt::kStatsScratchBytes, s));
-  int rc = lt::features_into(A, B, M, N, K, tol, features, scratch, s);
-  cudaFreeAsync(scratch, s);
-  if (rc != LT_OK) return rc;
+  LT_TRY(lt::selector_infer(A, B, M, N, K, tol, nullptr, features, nullptr, lt::as_stream(stream)));
   return lt::ok();
 }
 

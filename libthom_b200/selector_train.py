@@ -293,22 +293,32 @@ def main():
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--out", default=str(WEIGHTS))
     ap.add_argument("--report", default="")
+    ap.add_argument("--eval-only", action="store_true",
+                    help="evaluate the weights in --out on the held-out set without training")
     args = ap.parse_args()
     torch.cuda.set_device(0)
     gen = Generator(torch)
     t0 = time.time()
-    train_rows = build_dataset(torch, gen, args.train, seed=1234, log_every=2000)
-    test_rows = build_dataset(torch, gen, args.test, seed=98765)
-    t_data = time.time() - t0
-    X, Y = expand(train_rows)
-    t1 = time.time()
-    params, hist = train(torch, X, Y, epochs=args.epochs)
-    t_train = time.time() - t1
-    params.astype(np.float32).tofile(args.out)
+    if args.eval_only:
+        train_rows = []
+        test_rows = build_dataset(torch, gen, args.test, seed=98765)
+        t_data = time.time() - t0
+        params = np.fromfile(args.out, dtype=np.float32)
+        assert params.size == lt.LT_SEL_PARAMS, params.size
+        X, Y, hist, t_train = np.zeros((0, lt.LT_SEL_FEATURES)), np.zeros(0, dtype=np.int64), [], 0.0
+    else:
+        train_rows = build_dataset(torch, gen, args.train, seed=1234, log_every=2000)
+        test_rows = build_dataset(torch, gen, args.test, seed=98765)
+        t_data = time.time() - t0
+        X, Y = expand(train_rows)
+        t1 = time.time()
+        params, hist = train(torch, X, Y, epochs=args.epochs)
+        t_train = time.time() - t1
+        params.astype(np.float32).tofile(args.out)
     lt.check(lt.lib().lt_selector_set_params(params.ctypes.data))
     ev, chosen = evaluate(torch, gen, params, test_rows)
     tput, ms = throughput(torch, gen, chosen)
-    report = dict(train_matrices=args.train, test_matrices=args.test, train_samples=len(Y),
+    report = dict(train_matrices=0 if args.eval_only else args.train, test_matrices=args.test, train_samples=len(Y),
                   label_histogram=np.bincount(Y, minlength=8).tolist(), data_seconds=t_data, train_seconds=t_train,
                   loss_by_epoch=hist, evaluation=ev, throughput_tflops=tput, throughput_ms=ms, weights=args.out)
     text = json.dumps(report, indent=1)
