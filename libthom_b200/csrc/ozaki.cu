@@ -34,6 +34,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "lt_internal.h"
@@ -200,17 +201,20 @@ __device__ __forceinline__ void split_value(double a, int e, int j, uint32_t (&p
   }
 }
 
-// ---- four values at a time, S <= 8 (X < 2^56) ----
-// X = floor(|a| 2^(7S - e)) as in split_value, and the sign bit of a; X = 0 for a zero or
-// non-finite entry.
+// ---- four values at a time ----
+// X = floor(|a| 2^(7S - e)) as in split_value (64 bits for S <= 9, 128 above), and the sign bit of
+// a; X = 0 for a zero or non-finite entry.
 template <int S>
-__device__ __forceinline__ unsigned long long digit_string(double a, int e, uint32_t* neg) {
-  static_assert(7 * S <= 56, "four-at-a-time path covers S <= 8");
+using DigitString = typename std::conditional<(7 * S <= 63), unsigned long long, unsigned __int128>::type;
+
+template <int S>
+__device__ __forceinline__ DigitString<S> digit_string(double a, int e, uint32_t* neg) {
+  using X = DigitString<S>;
   const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(a));
   const unsigned long long mag = bits & 0x7fffffffffffffffull;
   const int E = static_cast<int>(mag >> 52);
   *neg = static_cast<uint32_t>(bits >> 63);
-  if (mag == 0ull || E == 0x7ff) return 0ull;
+  if (mag == 0ull || E == 0x7ff) return X(0);
   unsigned long long m = mag & 0x000fffffffffffffull;
   int t;
   if (E == 0) {
@@ -220,8 +224,9 @@ __device__ __forceinline__ unsigned long long digit_string(double a, int e, uint
     t = E - 1075;
   }
   const int sh = t - e + 7 * S;
-  if (sh >= 0) return m << sh;
-  return (-sh >= 64) ? 0ull : (m >> (-sh));
+  constexpr int kBits = 8 * static_cast<int>(sizeof(X));
+  if (sh >= 0) return X(m) << sh;
+  return (-sh >= kBits) ? X(0) : (X(m) >> (-sh));
 }
 
 // Moves four 7-bit fields (bits 0..27) into the four bytes of a word: byte i = bits 7i..7i+6.
@@ -242,33 +247,31 @@ __device__ __forceinline__ void transpose4x4(uint32_t (&w)[4]) {
 
 // Slices of four consecutive values v[0..3] (K positions 4w .. 4w+3 of one row): sets word w of
 // every slice, packed[p][w] byte i = digit p of v[i] as a two's-complement byte. The digits are the
-// same as split_value's: byte i of spread7x4(X) is bits 7i..7i+6 of X, i.e. slice S-1-i (low word)
-// and S-5-i (high word, X >> 28); a negative value's digit bytes are negated (__vsub4).
+// same as split_value's: byte i of spread7x4(bits 28j .. 28j+27 of X) is digit 4j + i counted from
+// the least significant, i.e. slice S-1-(4j+i); a negative value's digit bytes are negated (__vsub4).
 template <int S>
 __device__ __forceinline__ void split4(const double (&v)[4], int e, int w, uint32_t (&packed)[S][8]) {
-  uint32_t lo[4], hi[4];
+  constexpr int NW = (S + 3) / 4;  // words of four digits
+  uint32_t dw[NW][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     uint32_t neg;
-    const unsigned long long X = digit_string<S>(v[i], e, &neg);
-    uint32_t l = spread7x4(static_cast<uint32_t>(X) & 0x0FFFFFFFu);
-    uint32_t h = spread7x4(static_cast<uint32_t>(X >> 28));
-    if (neg) {
-      l = __vsub4(0u, l);
-      h = __vsub4(0u, h);
+    const DigitString<S> X = digit_string<S>(v[i], e, &neg);
+#pragma unroll
+    for (int j = 0; j < NW; ++j) {
+      uint32_t d = spread7x4(static_cast<uint32_t>(X >> (28 * j)) & 0x0FFFFFFFu);
+      dw[j][i] = neg ? __vsub4(0u, d) : d;
     }
-    lo[i] = l;
-    hi[i] = h;
   }
-  transpose4x4(lo);
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-    if (S - 1 - i >= 0) packed[(S - 1 - i) >= 0 ? S - 1 - i : 0][w] = lo[i];
-  if constexpr (S > 4) {
-    transpose4x4(hi);
+  for (int j = 0; j < NW; ++j) {
+    transpose4x4(dw[j]);
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
-      if (S - 5 - i >= 0) packed[(S - 5 - i) >= 0 ? S - 5 - i : 0][w] = hi[i];
+    for (int i = 0; i < 4; ++i) {
+      constexpr int kS = S;
+      const int p = kS - 1 - (4 * j + i);
+      if (p >= 0) packed[p >= 0 ? p : 0][w] = dw[j][i];
+    }
   }
 }
 
@@ -304,7 +307,7 @@ __device__ __forceinline__ void split_rows_tile(const double* __restrict__ A, in
     const int e = exponent_of_maxbits(amax[row]);
     const double* a = A + row * K;
     const int64_t k0 = c * kChunk;
-    if constexpr (7 * S <= 56) {
+    if constexpr (S <= LT_OZAKI_MAX_SLICES) {
       if (e != kSentinel) {
         // 16-byte loads when the row is 16-byte aligned and the chunk is whole: each lane's two
         // doubles share one L1 sector, half the tag lookups of scalar loads across 32 rows.
@@ -355,7 +358,7 @@ __device__ __forceinline__ void split_cols_tile(const double* __restrict__ B, in
   if (col < N) {
     const int e = exponent_of_maxbits(amax[col]);
     const int64_t k0 = c * kChunk;
-    if constexpr (7 * S <= 56) {
+    if constexpr (S <= LT_OZAKI_MAX_SLICES) {
       if (e != kSentinel) {
         const double* bp = B + k0 * N + col;
         const bool whole = k0 + kChunk <= K;  // no bounds test per load
@@ -771,7 +774,8 @@ __global__ void __launch_bounds__(kThreads, 1) ozaki_gemm_grouped_kernel(OzGroup
 // Synchronisation (barriers at the same shared-memory offsets in both CTAs):
 //   full[s]   rank 0: its own expect_tx arrival + one relayed arrival from rank 1 (count 2);
 //             rank 1: its own expect_tx arrival (count 1). Rank 1's warp 1 waits on its full[s]
-//             and forwards one arrival to rank 0's, so rank 0's MMA sees both halves landed.
+//             and forwards one arrival (relaxed) to rank 0's, so rank 0's MMA sees both halves
+//             landed.
 //   empty[s]  count 1 in each CTA: rank 0's MMA warp commits to both after the stage's MMAs.
 //   acc_full  count 1 in each CTA: committed to both after a group's last MMA.
 //   acc_empty rank 0 only, count 16: every epilogue warp of both CTAs arrives after reading TMEM.
@@ -924,7 +928,9 @@ __device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatu
             const int64_t c1 = (c0 + gch < nkc) ? c0 + gch : nkc;
             for (int64_t cs = c0; cs < c1; cs += cps) {
               if (!mbar_wait(&full[stage], phase, abort_flag, status, 22)) { ok = false; break; }
-              mbar_arrive_cluster(cluster_addr(&full[stage], 0));
+              // The copies into this CTA's stage have landed (complete_tx observed above); the
+              // forwarded arrival carries no data of this thread, so relaxed ordering suffices.
+              mbar_arrive_cluster_relaxed(cluster_addr(&full[stage], 0));
               if (++stage == G::kStages) { stage = 0; phase ^= 1; }
             }
           }
