@@ -141,11 +141,19 @@ int lt_grouped_plan_run(lt_grouped_plan* plan, void* stream);
 /* Captures lt_grouped_plan_run into a CUDA graph once, then replays it on `stream`. */
 int lt_grouped_plan_run_graph(lt_grouped_plan* plan, void* stream);
 int lt_grouped_plan_info(const lt_grouped_plan* plan, int64_t* tiles, double* flops);
-/* Autotunes the plan's FP64 tile shape on its own problems (validated against cuBLAS FP64, median
- * of `iters` timed runs, scratch outputs); no-op for the Ozaki form. Synchronous. */
+/* Autotunes the plan's FP64 tile configuration on its own problems (validated against cuBLAS FP64,
+ * median of `iters` timed runs, scratch outputs): every single tile shape, and two size classes
+ * (problems with min(M, N) at or above a threshold on a large tile, the rest on a small one, as
+ * two persistent launches); no-op for the Ozaki form. Synchronous. */
 int lt_grouped_plan_tune(lt_grouped_plan* plan, int iters, float* best_ms);
 /* Name of the kernel configuration the plan runs. */
 int lt_grouped_plan_config(const lt_grouped_plan* plan, char* name, int name_len);
+/* FP64 grouped tile configurations (index -> name), and setting a plan's explicitly, e.g. to
+ * re-apply a tuned choice: `cfg` for problems with min(M, N) >= split_mn and `cfg_small` for the
+ * others, or `cfg_small` = -1 for one configuration for all. No-op for the Ozaki form. */
+int lt_grouped_num_configs(void);
+const char* lt_grouped_config_name(int cfg);
+int lt_grouped_plan_set_fp64(lt_grouped_plan* plan, int cfg, int cfg_small, int64_t split_mn);
 void lt_grouped_plan_destroy(lt_grouped_plan* plan);
 /* Convenience: create, run once, destroy. */
 int lt_dgemm_grouped(const lt_gemm_problem* problems, int count, int form, int slices, void* stream);

@@ -119,6 +119,9 @@ SIGNATURES = {
     "lt_abs_denominator": (_i32, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _vp]),
     "lt_flush_l2": (_i32, [_vp]),
     "lt_measure_peak": (_i32, [_i32, _c.POINTER(_f64), _vp]),
+    "lt_grouped_num_configs": (_i32, []),
+    "lt_grouped_config_name": (_c.c_char_p, [_i32]),
+    "lt_grouped_plan_set_fp64": (_i32, [_vp, _i32, _i32, _i64]),
     "lt_dgemm_ozaki_host": (_i32, [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _i32, _vp]),
 }
 

@@ -19,9 +19,14 @@ struct lt_grouped_plan {
   int slices = 0;
   int count = 0;
   int fp64_cfg = 1;
+  // Two size classes (FP64 form): problems with min(M, N) >= split_mn run with fp64_cfg, the
+  // others with fp64_cfg_small, as two persistent launches; split_mn = 0 means one class.
+  int fp64_cfg_small = -1;
+  int64_t split_mn = 0;
   std::vector<lt_gemm_problem> problems;
   double flops = 0.0;
   lt::fp64::GroupedFp64* fp = nullptr;
+  lt::fp64::GroupedFp64* fp_small = nullptr;
   lt::ozaki::Grouped* oz = nullptr;
   cudaStream_t capture_stream = nullptr;
   cudaGraph_t graph = nullptr;
@@ -54,12 +59,49 @@ void drop_graph(lt_grouped_plan* plan) {
   plan->graph = nullptr;
 }
 
-int build_fp64(lt_grouped_plan* plan, int cfg) {
-  fp64::GroupedFp64* g = nullptr;
-  LT_TRY(fp64::grouped_create(plan->problems.data(), plan->count, cfg, &g));
+// Splits `problems` by min(M, N) >= split_mn (everything in `big` when split_mn <= 0).
+void split_classes(const std::vector<lt_gemm_problem>& problems, int64_t split_mn, std::vector<lt_gemm_problem>* big,
+                   std::vector<lt_gemm_problem>* small) {
+  big->clear();
+  small->clear();
+  for (const auto& p : problems) (split_mn <= 0 || std::min(p.M, p.N) >= split_mn ? big : small)->push_back(p);
+}
+
+// Launch tables for a tile configuration (and, with split_mn > 0, a second one for the small
+// class); the empty class gets none.
+int create_fp64(const std::vector<lt_gemm_problem>& problems, int cfg, int cfg_small, int64_t split_mn,
+                fp64::GroupedFp64** big_out, fp64::GroupedFp64** small_out) {
+  *big_out = *small_out = nullptr;
+  std::vector<lt_gemm_problem> big, small;
+  split_classes(problems, cfg_small >= 0 ? split_mn : 0, &big, &small);
+  if (!big.empty()) LT_TRY(fp64::grouped_create(big.data(), static_cast<int>(big.size()), cfg, big_out));
+  if (!small.empty()) {
+    int rc = fp64::grouped_create(small.data(), static_cast<int>(small.size()), cfg_small, small_out);
+    if (rc != LT_OK) {
+      fp64::grouped_destroy(*big_out);
+      *big_out = nullptr;
+      return rc;
+    }
+  }
+  return LT_OK;
+}
+
+int run_fp64(const fp64::GroupedFp64* big, const fp64::GroupedFp64* small, cudaStream_t stream) {
+  if (big != nullptr) LT_TRY(fp64::grouped_run(big, stream));
+  if (small != nullptr) LT_TRY(fp64::grouped_run(small, stream));
+  return LT_OK;
+}
+
+int build_fp64(lt_grouped_plan* plan, int cfg, int cfg_small = -1, int64_t split_mn = 0) {
+  fp64::GroupedFp64 *g = nullptr, *gs = nullptr;
+  LT_TRY(create_fp64(plan->problems, cfg, cfg_small, split_mn, &g, &gs));
   fp64::grouped_destroy(plan->fp);
+  fp64::grouped_destroy(plan->fp_small);
   plan->fp = g;
+  plan->fp_small = gs;
   plan->fp64_cfg = cfg;
+  plan->fp64_cfg_small = gs != nullptr ? cfg_small : -1;
+  plan->split_mn = gs != nullptr ? split_mn : 0;
   drop_graph(plan);
   return LT_OK;
 }
@@ -119,7 +161,7 @@ int lt_grouped_plan_run(lt_grouped_plan* plan, void* stream) {
   cudaGetDevice(&dev);
   if (dev != plan->device) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "plan belongs to device %d", plan->device);
   if (plan->form == LT_FORM_FP64) {
-    LT_TRY(lt::fp64::grouped_run(plan->fp, lt::as_stream(stream)));
+    LT_TRY(lt::run_fp64(plan->fp, plan->fp_small, lt::as_stream(stream)));
   } else {
     LT_TRY(lt::ozaki::grouped_run(plan->oz, lt::as_stream(stream)));
   }
@@ -133,7 +175,8 @@ int lt_grouped_plan_run_graph(lt_grouped_plan* plan, void* stream) {
       LT_CUDA_TRY(cudaStreamCreateWithFlags(&plan->capture_stream, cudaStreamNonBlocking));
     // Kernel attributes are set outside the capture (no launch: C must be written once per replay).
     if (plan->form == LT_FORM_FP64) {
-      LT_TRY(lt::fp64::grouped_prepare(plan->fp));
+      if (plan->fp != nullptr) LT_TRY(lt::fp64::grouped_prepare(plan->fp));
+      if (plan->fp_small != nullptr) LT_TRY(lt::fp64::grouped_prepare(plan->fp_small));
     } else {
       LT_TRY(lt::ozaki::grouped_prepare(plan->oz));
     }
@@ -155,7 +198,13 @@ int lt_grouped_plan_run_graph(lt_grouped_plan* plan, void* stream) {
 
 int lt_grouped_plan_info(const lt_grouped_plan* plan, int64_t* tiles, double* flops) {
   if (plan == nullptr) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "null plan");
-  if (tiles) *tiles = plan->form == LT_FORM_FP64 ? lt::fp64::grouped_tiles(plan->fp) : lt::ozaki::grouped_tiles(plan->oz);
+  if (tiles) {
+    if (plan->form == LT_FORM_FP64)
+      *tiles = (plan->fp ? lt::fp64::grouped_tiles(plan->fp) : 0) +
+               (plan->fp_small ? lt::fp64::grouped_tiles(plan->fp_small) : 0);
+    else
+      *tiles = lt::ozaki::grouped_tiles(plan->oz);
+  }
   if (flops) *flops = plan->flops;
   return lt::ok();
 }
@@ -165,6 +214,7 @@ void lt_grouped_plan_destroy(lt_grouped_plan* plan) {
   lt::drop_graph(plan);
   if (plan->capture_stream) cudaStreamDestroy(plan->capture_stream);
   lt::fp64::grouped_destroy(plan->fp);
+  lt::fp64::grouped_destroy(plan->fp_small);
   lt::ozaki::grouped_destroy(plan->oz);
   delete plan;
 }
@@ -182,8 +232,27 @@ int lt_dgemm_grouped(const lt_gemm_problem* problems, int count, int form, int s
 
 int lt_grouped_plan_config(const lt_grouped_plan* plan, char* name, int name_len) {
   if (plan == nullptr || name == nullptr || name_len <= 0) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "bad arguments");
-  const char* n = plan->form == LT_FORM_FP64 ? lt::fp64::grouped_config_name(plan->fp64_cfg) : "ozaki_128x128";
-  snprintf(name, static_cast<size_t>(name_len), "%s", n);
+  if (plan->form == LT_FORM_FP64 && plan->fp_small != nullptr)
+    snprintf(name, static_cast<size_t>(name_len), "%s for min(M,N) >= %lld, else %s",
+             lt::fp64::grouped_config_name(plan->fp64_cfg), static_cast<long long>(plan->split_mn),
+             lt::fp64::grouped_config_name(plan->fp64_cfg_small));
+  else
+    snprintf(name, static_cast<size_t>(name_len), "%s",
+             plan->form == LT_FORM_FP64 ? lt::fp64::grouped_config_name(plan->fp64_cfg) : "ozaki_128x128");
+  return lt::ok();
+}
+
+int lt_grouped_num_configs(void) { return lt::fp64::grouped_num_configs(); }
+const char* lt_grouped_config_name(int cfg) { return lt::fp64::grouped_config_name(cfg); }
+
+int lt_grouped_plan_set_fp64(lt_grouped_plan* plan, int cfg, int cfg_small, int64_t split_mn) {
+  if (plan == nullptr) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "null plan");
+  if (plan->form != LT_FORM_FP64) return lt::ok();
+  const int n = lt::fp64::grouped_num_configs();
+  if (cfg < 0 || cfg >= n || cfg_small < -1 || cfg_small >= n || (cfg_small >= 0 && split_mn <= 0))
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "grouped configuration %d / %d / %lld", cfg, cfg_small,
+                         static_cast<long long>(split_mn));
+  LT_TRY(lt::build_fp64(plan, cfg, cfg_small, split_mn));
   return lt::ok();
 }
 
@@ -223,12 +292,38 @@ int lt_grouped_plan_tune(lt_grouped_plan* plan, int iters, float* best_ms) {
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  // Candidates: every single tile configuration, then two size classes (threshold on min(M, N))
+  // with a large-tile configuration for the big problems and a small-tile one for the rest.
+  struct Cand {
+    int cfg, cfg_small;
+    int64_t split;
+  };
+  std::vector<Cand> cands;
+  const int ncfg = lt::fp64::grouped_num_configs();
+  for (int c = 0; c < ncfg; ++c) cands.push_back({c, -1, 0});
+  for (int64_t split : {96, 192, 384}) {
+    for (int c = 0; c < ncfg; ++c) {
+      const char* nb = lt::fp64::grouped_config_name(c);
+      if (strstr(nb, "32x32") != nullptr) continue;  // big class: 64-wide tiles or more
+      for (int cs = 0; cs < ncfg; ++cs) {
+        const char* ns = lt::fp64::grouped_config_name(cs);
+        if (strstr(ns, "32") == nullptr) continue;  // small class: a 32-wide dimension
+        cands.push_back({c, cs, split});
+      }
+    }
+  }
   int best = -1;
   float best_t = 0.f;
-  for (int cfg = 0; cfg < lt::fp64::grouped_num_configs() && rc == LT_OK; ++cfg) {
-    lt::fp64::GroupedFp64* g = nullptr;
-    if (lt::fp64::grouped_create(probs.data(), plan->count, cfg, &g) != LT_OK) continue;
-    bool valid = lt::fp64::grouped_run(g, nullptr) == LT_OK;
+  for (size_t ci = 0; ci < cands.size() && rc == LT_OK; ++ci) {
+    const Cand& cd = cands[ci];
+    lt::fp64::GroupedFp64 *g = nullptr, *gs = nullptr;
+    if (lt::create_fp64(probs, cd.cfg, cd.cfg_small, cd.split, &g, &gs) != LT_OK) continue;
+    if (cd.cfg_small >= 0 && (g == nullptr || gs == nullptr)) {  // threshold splits nothing off
+      lt::fp64::grouped_destroy(g);
+      lt::fp64::grouped_destroy(gs);
+      continue;
+    }
+    bool valid = lt::run_fp64(g, gs, nullptr) == LT_OK;
     if (valid) {
       cudaMemset(err, 0, sizeof(unsigned long long));
       lt::max_rel_err_kernel<<<ctx->sm_count * 4, 256>>>(scratch, ref, static_cast<int64_t>(total), err);
@@ -243,7 +338,7 @@ int lt_grouped_plan_tune(lt_grouped_plan* plan, int iters, float* best_ms) {
       std::vector<float> ts;
       for (int it = 0; it < iters; ++it) {
         cudaEventRecord(e0);
-        lt::fp64::grouped_run(g, nullptr);
+        lt::run_fp64(g, gs, nullptr);
         cudaEventRecord(e1);
         cudaEventSynchronize(e1);
         float ms = 0.f;
@@ -252,11 +347,12 @@ int lt_grouped_plan_tune(lt_grouped_plan* plan, int iters, float* best_ms) {
       }
       std::sort(ts.begin(), ts.end());
       if (best < 0 || ts[ts.size() / 2] < best_t) {
-        best = cfg;
+        best = static_cast<int>(ci);
         best_t = ts[ts.size() / 2];
       }
     }
     lt::fp64::grouped_destroy(g);
+    lt::fp64::grouped_destroy(gs);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -264,7 +360,7 @@ int lt_grouped_plan_tune(lt_grouped_plan* plan, int iters, float* best_ms) {
   cudaFree(err);
   if (rc != LT_OK) return rc;
   if (best < 0) return lt::set_error(LT_ERR_NOT_FOUND, "no grouped candidate validated");
-  LT_TRY(lt::build_fp64(plan, best));
+  LT_TRY(lt::build_fp64(plan, cands[best].cfg, cands[best].cfg_small, cands[best].split));
   if (best_ms) *best_ms = best_t;
   return lt::ok();
 }

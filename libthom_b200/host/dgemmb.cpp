@@ -114,7 +114,7 @@ static double runImpl(const std::string& impl, Set& s, int iters, int warmup, bo
     exit(1);
   }
   if (plan != nullptr) {
-    char name[64];
+    char name[128];
     lt_grouped_plan_config(plan, name, sizeof name);
     int64_t tiles = 0;
     lt_grouped_plan_info(plan, &tiles, nullptr);
@@ -189,7 +189,7 @@ static void tuneHandler(int argc, char* argv[]) {
   LT_CHECK(lt_grouped_plan_create(s.probs.data(), count, LT_FORM_FP64, 0, &plan));
   float ms = 0.f;
   LT_CHECK(lt_grouped_plan_tune(plan, 5, &ms));
-  char name[64];
+  char name[128];
   lt_grouped_plan_config(plan, name, sizeof name);
   printf("[best] %d problems in [%lld, %lld]: %s %.4f ms (%.1f GFLOP/s)\n", count, static_cast<long long>(lo),
          static_cast<long long>(hi), name, ms, s.flops / (ms * 1e6));

@@ -78,6 +78,42 @@ def test_grouped_fp64(cuda, oracle_mod, graph, tune):
 
 
 @pytest.mark.parametrize("graph", [False, True])
+def test_grouped_fp64_two_size_classes(cuda, oracle_mod, graph):
+    """A plan whose big problems (min(M, N) >= 64) run on 64x64 tiles and the rest on 32x32 tiles,
+    as two persistent launches (and one captured graph)."""
+    import libthom_b200 as lt
+
+    L = lt.lib()
+    names = [L.lt_grouped_config_name(i).decode() for i in range(L.lt_grouped_num_configs())]
+    big, small = names.index("grouped_cpa_64x64_s3"), names.index("grouped_cpa_32x32_s3")
+    probs = make_set(oracle_mod, 20, 8, 300, seed=9)
+    dev, table = upload(cuda, probs)
+    plan = ctypes.c_void_p()
+    lt.check(L.lt_grouped_plan_create(table, len(probs), lt.LT_FORM_FP64, 0, ctypes.byref(plan)))
+    try:
+        lt.check(L.lt_grouped_plan_set_fp64(plan, big, small, 64))
+        name = ctypes.create_string_buffer(128)
+        lt.check(L.lt_grouped_plan_config(plan, name, 128))
+        assert b">= 64" in name.value, name.value
+        if graph:
+            lt.check(L.lt_grouped_plan_run_graph(plan, None))
+        else:
+            lt.check(L.lt_grouped_plan_run(plan, None))
+        cuda.cuda.synchronize()
+        lt.device_status()
+        with pytest.raises(lt.LtError):
+            lt.check(L.lt_grouped_plan_set_fp64(plan, big, small, 0))
+    finally:
+        L.lt_grouped_plan_destroy(plan)
+    assert any(min(A.shape[0], B.shape[1]) >= 64 for A, B, *_ in probs)
+    assert any(min(A.shape[0], B.shape[1]) < 64 for A, B, *_ in probs)
+    for (A, B, C0, alpha, beta), (_, _, dC) in zip(probs, dev):
+        Cref, den = oracle_mod.dot2_rows(A, B, C0, alpha, beta)
+        err = oracle_mod.componentwise_error(dC.cpu().numpy(), Cref, den)
+        assert err[0] <= fp64_bound(A.shape[1]), (A.shape, B.shape, err)
+
+
+@pytest.mark.parametrize("graph", [False, True])
 def test_grouped_ozaki_bit_exact(cuda, oracle_mod, graph):
     import libthom_b200 as lt
 
