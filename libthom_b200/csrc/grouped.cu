@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "lt_internal.h"
@@ -86,9 +87,46 @@ int create_fp64(const std::vector<lt_gemm_problem>& problems, int cfg, int cfg_s
   return LT_OK;
 }
 
+// Side stream and events for running the two size classes concurrently (created once per process
+// and device; a plan run forks onto it and joins back, which a stream capture records as two
+// parallel graph branches).
+struct Fork {
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+int fork_of(Fork** out) {
+  static Fork forks[64];
+  static std::mutex mu;
+  int dev = 0;
+  LT_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  Fork& f = forks[dev];
+  if (f.side == nullptr) {
+    LT_CUDA_TRY(cudaStreamCreateWithFlags(&f.side, cudaStreamNonBlocking));
+    LT_CUDA_TRY(cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming));
+    LT_CUDA_TRY(cudaEventCreateWithFlags(&f.join, cudaEventDisableTiming));
+  }
+  *out = &f;
+  return LT_OK;
+}
+
+// The big class on `stream`, the small class concurrently on the side stream; `stream` waits for
+// both before anything queued after the call.
 int run_fp64(const fp64::GroupedFp64* big, const fp64::GroupedFp64* small, cudaStream_t stream) {
-  if (big != nullptr) LT_TRY(fp64::grouped_run(big, stream));
-  if (small != nullptr) LT_TRY(fp64::grouped_run(small, stream));
+  if (big == nullptr || small == nullptr) {
+    if (big != nullptr) LT_TRY(fp64::grouped_run(big, stream));
+    if (small != nullptr) LT_TRY(fp64::grouped_run(small, stream));
+    return LT_OK;
+  }
+  Fork* f = nullptr;
+  LT_TRY(fork_of(&f));
+  LT_CUDA_TRY(cudaEventRecord(f->fork, stream));
+  LT_CUDA_TRY(cudaStreamWaitEvent(f->side, f->fork, 0));
+  LT_TRY(fp64::grouped_run(big, stream));
+  LT_TRY(fp64::grouped_run(small, f->side));
+  LT_CUDA_TRY(cudaEventRecord(f->join, f->side));
+  LT_CUDA_TRY(cudaStreamWaitEvent(stream, f->join, 0));
   return LT_OK;
 }
 
