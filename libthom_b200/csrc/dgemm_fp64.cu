@@ -122,21 +122,34 @@ int num_configs() { return kNumConfigs; }
 const char* config_name(int i) { return (i >= 0 && i < kNumConfigs) ? kConfigs[i].name : nullptr; }
 bool config_is_tma(int i) { return i >= 0 && i < kNumConfigs && kConfigs[i].tma; }
 
-// Default choice without a tuning table: the largest tile that still gives every SM a tile.
+// Default choice without a tuning table: the configuration (of the staging the pointers allow)
+// minimising waves x tile area / tile efficiency, one CTA per SM. Efficiencies are the tiles'
+// measured 8192^3 rates relative to 128x64 (TMA: 34.8, 33.2, 27.6, 18.0, 18.0 TF/s for 128x64,
+// 64x128, 64x64, 64x32, 32x64). The K split handles what remains of a poorly filled last wave.
 int heuristic_config(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int sm_count) {
+  (void)K;
   const bool tma = tma_compatible(A, B, N, K);
-  struct Pick { int bm, bn; };
-  const Pick order[] = {{128, 64}, {64, 64}, {64, 32}, {32, 32}};
-  int chosen_bm = 32, chosen_bn = 32;
-  for (const Pick& pk : order) {
-    int64_t tiles = ((M + pk.bm - 1) / pk.bm) * ((N + pk.bn - 1) / pk.bn);
-    if (tiles >= sm_count) { chosen_bm = pk.bm; chosen_bn = pk.bn; break; }
+  auto efficiency = [](int bm, int bn) {
+    if (bm == 128 && bn == 64) return 1.0;
+    if (bm == 64 && bn == 128) return 0.95;
+    if (bm == 64 && bn == 64) return 0.79;
+    if (bm * bn == 2048) return 0.52;
+    return 0.35;
+  };
+  int best = -1;
+  double best_cost = 0.0;
+  for (int i = 0; i < kNumConfigs; ++i) {
+    if (kConfigs[i].tma != tma) continue;
+    const int bm = kConfigs[i].bm, bn = kConfigs[i].bn;
+    const int64_t tiles = ((M + bm - 1) / bm) * ((N + bn - 1) / bn);
+    const int64_t waves = (tiles + sm_count - 1) / sm_count;
+    const double cost = static_cast<double>(waves) * bm * bn / efficiency(bm, bn);
+    if (best < 0 || cost < best_cost * 0.999) {
+      best = i;
+      best_cost = cost;
+    }
   }
-  for (int i = 0; i < kNumConfigs; ++i)
-    if (kConfigs[i].tma == tma && kConfigs[i].bm == chosen_bm && kConfigs[i].bn == chosen_bn) return i;
-  for (int i = 0; i < kNumConfigs; ++i)
-    if (kConfigs[i].tma == tma && kConfigs[i].bm * kConfigs[i].bn <= chosen_bm * chosen_bn) return i;
-  return kNumConfigs - 1;
+  return best >= 0 ? best : kNumConfigs - 1;
 }
 
 // ---- grouped launches (cp.async staging: problems have arbitrary shapes and alignment) ----
