@@ -16,3 +16,13 @@ def test_peak_probe(cuda, kind, lo, hi):
     v = lt.measure_peak(kind)
     assert lo < v < hi, v
     lt.device_status()
+
+
+def test_sustained_rate_not_above_burst(cuda):
+    """LT_PEAK_SUSTAINED times the same loop after 0.5 s at the power limit: never meaningfully
+    faster than one launch, and within the physical range."""
+    import libthom_b200 as lt
+
+    burst = max(lt.measure_peak(lt.LT_PEAK_INT8_MMA_PAIR) for _ in range(2))
+    sustained = lt.measure_peak(lt.LT_PEAK_INT8_MMA_PAIR | lt.LT_PEAK_SUSTAINED)
+    assert 2.0e15 < sustained <= 1.05 * burst, (sustained, burst)
