@@ -96,6 +96,17 @@ int lt_ozaki_product(double* C, int64_t M, int64_t N, int64_t K, double alpha, d
                      const void* workspace, size_t workspace_bytes, void* stream);
 int lt_dgemm_cublas(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
                     double alpha, double beta, void* stream);
+/* BLAS-style DGEMM on row-major matrices: C = alpha op(A) op(B) + beta C with op(X) = X ('N') or
+ * X^T ('T'; 'C' is accepted as 'T'), op(A) M x K, op(B) K x N, C M x N, every matrix row-major with
+ * its own row stride: A is M x K (lda >= K) or, transposed, K x M (lda >= M); B is K x N (ldb >= N)
+ * or N x K (ldb >= K); ldc >= N (columns N .. ldc-1 of C are not touched). `form` LT_FORM_FP64
+ * (native tensor cores; `slices` ignored) or LT_FORM_OZAKI (`slices` slices; results bit-identical
+ * to lt_dgemm_ozaki on the packed op(A), op(B)). Generalises the reference's contract
+ * (routines/dgemm/dgemm.h:9: packed, untransposed, tile-multiple operands only) toward a BLAS
+ * dgemm(transA, transB, lda, ...). Stream-ordered; uses the cached workspaces. */
+int lt_dgemm_ex(int form, char transa, char transb, int64_t M, int64_t N, int64_t K, double alpha,
+                const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
+                int slices, void* stream);
 /* Ozaki DGEMM on HOST memory: A, B and C are host pointers (C holds C0 on entry when beta != 0 and
  * the result on return). Replaces the reference harness's copy-in / kernel / copy-out sequence
  * (main.cpp and routines/dgemm/dgemm.cpp:135-170 copy whole matrices before and after the call)

@@ -123,6 +123,8 @@ SIGNATURES = {
     "lt_grouped_config_name": (_c.c_char_p, [_i32]),
     "lt_grouped_plan_set_fp64": (_i32, [_vp, _i32, _i32, _i64]),
     "lt_dgemm_ozaki_host": (_i32, [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _i32, _vp]),
+    "lt_dgemm_ex": (_i32, [_i32, _c.c_char, _c.c_char, _i64, _i64, _i64, _f64, _vp, _i64, _vp, _i64, _f64, _vp, _i64,
+                           _i32, _vp]),
 }
 
 _lib = None
@@ -256,3 +258,10 @@ def dgemm_ozaki_host(A, B, C, M, N, K, alpha=1.0, beta=0.0, slices=8, stream=Non
     """Ozaki DGEMM on host (CPU) tensors or arrays, pipelined through the GPU (lt_dgemm_ozaki_host).
     C holds C0 on entry and the result on return."""
     check(lib().lt_dgemm_ozaki_host(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, slices, _stream(stream)))
+
+
+def dgemm_ex(transa: str, transb: str, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, form=LT_FORM_FP64, slices=8,
+             stream=None) -> None:
+    """BLAS-style DGEMM on row-major device matrices with row strides and transposes (lt_dgemm_ex)."""
+    check(lib().lt_dgemm_ex(form, transa.encode(), transb.encode(), M, N, K, alpha, _ptr(A), lda, _ptr(B), ldb, beta,
+                            _ptr(C), ldc, slices, _stream(stream)))

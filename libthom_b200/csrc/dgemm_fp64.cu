@@ -43,12 +43,12 @@ int launch(const Params& p0, cudaStream_t stream, DeviceContext* ctx) {
   memset(&tmA, 0, sizeof tmA);
   memset(&tmB, 0, sizeof tmB);
   if (Cfg::kTMA) {
-    if (!tma_compatible(p.A, p.B, p.N, p.K))
-      return set_error(LT_ERR_UNALIGNED, "TMA configuration needs 16-byte aligned A/B and even N and K");
+    if (!tma_compatible(p.A, p.B, p.ldb, p.lda))
+      return set_error(LT_ERR_UNALIGNED, "TMA configuration needs 16-byte aligned A/B and even row strides");
     LT_TRY(make_tmap_2d(&tmA, p.A, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, static_cast<uint64_t>(p.M),
-                        static_cast<uint64_t>(p.K), static_cast<uint64_t>(p.K) * 8, Cfg::BM, 16));
+                        static_cast<uint64_t>(p.K), static_cast<uint64_t>(p.lda) * 8, Cfg::BM, 16));
     LT_TRY(make_tmap_2d(&tmB, p.B, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, static_cast<uint64_t>(p.K),
-                        static_cast<uint64_t>(p.N), static_cast<uint64_t>(p.N) * 8, 16, 16));
+                        static_cast<uint64_t>(p.N), static_cast<uint64_t>(p.ldb) * 8, 16, 16));
   }
   static std::once_flag once[64];
   static int occupancy[64];
@@ -79,7 +79,8 @@ int launch(const Params& p0, cudaStream_t stream, DeviceContext* ctx) {
   if (p.splits > 1) {
     const int64_t n = p.M * p.N;
     const int64_t blocks = std::min<int64_t>((n + 255) / 256, static_cast<int64_t>(ctx->sm_count) * 16);
-    splitk_reduce_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p.W, p.C, n, p.splits, p.alpha, p.beta);
+    splitk_reduce_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p.W, p.C, n, p.N, p.ldc, p.splits, p.alpha,
+                                                                          p.beta);
     LT_CUDA_TRY(cudaGetLastError());
   }
   return LT_OK;
@@ -127,8 +128,10 @@ bool config_is_tma(int i) { return i >= 0 && i < kNumConfigs && kConfigs[i].tma;
 // measured 8192^3 rates relative to 128x64 (TMA: 34.8, 33.2, 27.6, 18.0, 18.0 TF/s for 128x64,
 // 64x128, 64x64, 64x32, 32x64). The K split handles what remains of a poorly filled last wave.
 int heuristic_config(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int sm_count) {
-  (void)K;
-  const bool tma = tma_compatible(A, B, N, K);
+  return heuristic_config_for(M, N, sm_count, tma_compatible(A, B, N, K));
+}
+
+int heuristic_config_for(int64_t M, int64_t N, int sm_count, bool tma) {
   auto efficiency = [](int bm, int bn) {
     if (bm == 128 && bn == 64) return 1.0;
     if (bm == 64 && bn == 128) return 0.95;
@@ -276,10 +279,27 @@ int64_t grouped_tiles(const GroupedFp64* G) { return G->ntiles; }
 
 int run_config(int cfg, const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
                double beta, cudaStream_t stream) {
+  return run_config_ld(cfg, A, K, B, N, C, N, M, N, K, alpha, beta, stream);
+}
+
+int run_config_ld(int cfg, const double* A, int64_t lda, const double* B, int64_t ldb, double* C, int64_t ldc, int64_t M,
+                  int64_t N, int64_t K, double alpha, double beta, cudaStream_t stream) {
   if (cfg < 0 || cfg >= kNumConfigs) return set_error(LT_ERR_INVALID_ARGUMENT, "FP64 config %d out of range", cfg);
   DeviceContext* ctx = context();
   if (ctx == nullptr) return last_error();
-  Params p{A, B, C, M, N, K, alpha, beta, nullptr, 1, nullptr};
+  Params p{};
+  p.A = A;
+  p.B = B;
+  p.C = C;
+  p.M = M;
+  p.N = N;
+  p.K = K;
+  p.alpha = alpha;
+  p.beta = beta;
+  p.splits = 1;
+  p.lda = lda;
+  p.ldb = ldb;
+  p.ldc = ldc;
   return kConfigs[cfg].fn(p, stream, ctx);
 }
 

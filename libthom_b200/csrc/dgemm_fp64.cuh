@@ -36,6 +36,7 @@ struct Params {
   int64_t M, N, K;
   double alpha, beta;
   DeviceStatus* status;
+  int64_t lda, ldb, ldc;  // row strides of A (M x K), B (K x N), C (M x N)
   // K split: `splits` > 1 cuts the k-blocks of every tile into that many contiguous ranges; the
   // unit for range s writes its raw sums to W + s*M*N (row stride N) and splitk_reduce forms C.
   int splits;
@@ -114,6 +115,7 @@ struct Job {
   int64_t m0, n0;
   int kb0, kb1;
   double* W;
+  int64_t lda, ldb, ldc;
 };
 
 // Tiles of a single problem, walked in grouped raster order.
@@ -134,7 +136,8 @@ struct SingleSource {
     const int kb0 = static_cast<int>(sp) * per;
     const int kb1 = kb0 + per < nkb ? kb0 + per : nkb;
     double* w = p.splits > 1 ? p.W + sp * p.M * p.N : nullptr;
-    return Job{p.A, p.B, p.C, p.M, p.N, p.K, p.alpha, p.beta, tm * Cfg::BM, tn * Cfg::BN, kb0, kb1, w};
+    return Job{p.A, p.B, p.C, p.M, p.N, p.K, p.alpha, p.beta, tm * Cfg::BM, tn * Cfg::BN, kb0, kb1, w,
+               p.lda, p.ldb, p.ldc};
   }
 };
 
@@ -162,7 +165,7 @@ struct GroupedSource {
     const GroupProblem& pr = problems[gt.problem];
     return Job{pr.A,  pr.B,  pr.C,  pr.M, pr.N,
                pr.K,  pr.alpha, pr.beta, gt.m0, gt.n0,
-               0,     static_cast<int>((pr.K + 15) / 16), nullptr};
+               0,     static_cast<int>((pr.K + 15) / 16), nullptr, pr.K, pr.N, pr.N};
   }
 };
 
@@ -226,7 +229,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
             const int r = e >> 3, c = e & 7;
             const int64_t gr = m0 + r, gk = k0 + 2 * c;
             uint8_t* dst = sa + a_off(r, c);
-            const double* gp = J.A + gr * J.K + gk;
+            const double* gp = J.A + gr * J.lda + gk;
             if (gr < J.M && gk + 1 < J.K && (reinterpret_cast<uintptr_t>(gp) & 15) == 0) {
               cp_async_16(dst, gp, true);
             } else {
@@ -241,7 +244,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
             const int k = e / (Cfg::BN / 2), n = 2 * (e % (Cfg::BN / 2));
             const int64_t gk = k0 + k, gn = n0 + n;
             uint8_t* dst = sb + b_off(k, n);
-            const double* gp = J.B + gk * J.N + gn;
+            const double* gp = J.B + gk * J.ldb + gn;
             if (gk < J.K && gn + 1 < J.N && (reinterpret_cast<uintptr_t>(gp) & 15) == 0) {
               cp_async_16(dst, gp, true);
             } else {
@@ -332,7 +335,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
           }
         continue;
       }
-      const bool vec = ((J.N & 1) == 0) && ((reinterpret_cast<uintptr_t>(J.C) & 15) == 0);
+      const bool vec = ((J.ldc & 1) == 0) && ((reinterpret_cast<uintptr_t>(J.C) & 15) == 0);
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
 #pragma unroll
@@ -343,7 +346,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
           for (int j = 0; j < 4; ++j) {
             const int64_t col = n0 + j * 8 + 2 * tq;
             double v0 = acc[i][j][2 * h], v1 = acc[i][j][2 * h + 1];
-            double* cp = J.C + row * J.N + col;
+            double* cp = J.C + row * J.ldc + col;
             if (vec && col + 1 < J.N) {
               double2 o;
               if (J.beta != 0.0) {
@@ -373,14 +376,16 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
   gemm_body<Cfg>(&tmA, &tmB, src, p.status);
 }
 
-// C = alpha * (W_0 + W_1 + ... + W_{splits-1}) + beta * C, summed in split order.
-__global__ void splitk_reduce_kernel(const double* __restrict__ W, double* __restrict__ C, int64_t n, int splits,
-                                     double alpha, double beta) {
+// C = alpha * (W_0 + W_1 + ... + W_{splits-1}) + beta * C, summed in split order; W is packed
+// (M x N), C has row stride ldc.
+__global__ void splitk_reduce_kernel(const double* __restrict__ W, double* __restrict__ C, int64_t n, int64_t N,
+                                     int64_t ldc, int splits, double alpha, double beta) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     double s = W[i];
     for (int k = 1; k < splits; ++k) s += W[k * n + i];
-    C[i] = (beta != 0.0) ? fma(alpha, s, beta * C[i]) : alpha * s;
+    double* c = C + (i / N) * ldc + (i % N);
+    *c = (beta != 0.0) ? fma(alpha, s, beta * *c) : alpha * s;
   }
 }
 

@@ -17,8 +17,12 @@ int num_configs();
 const char* config_name(int i);
 bool config_is_tma(int i);
 int heuristic_config(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int sm_count);
+int heuristic_config_for(int64_t M, int64_t N, int sm_count, bool tma);
 int run_config(int cfg, const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
                double beta, cudaStream_t stream);
+// Same with row strides (lda >= K, ldb >= N, ldc >= N).
+int run_config_ld(int cfg, const double* A, int64_t lda, const double* B, int64_t ldb, double* C, int64_t ldc, int64_t M,
+                  int64_t N, int64_t K, double alpha, double beta, cudaStream_t stream);
 }  // namespace fp64
 
 // Selector statistics (selector_stats.cu). selector_infer: the features of one problem (copied to
@@ -43,6 +47,9 @@ int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double bet
             size_t workspace_bytes, cudaStream_t stream);
 int run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta,
         int slices, void* workspace, size_t workspace_bytes, cudaStream_t stream);
+int run_ex(bool trans_a, bool trans_b, const double* A, int64_t lda, const double* B, int64_t ldb, double* C, int64_t ldc,
+           int64_t M, int64_t N, int64_t K, double alpha, double beta, int s, void* workspace, size_t workspace_bytes,
+           cudaStream_t stream);
 int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
              double beta, int slices, cudaStream_t stream);
 int noalloc_run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,

@@ -113,6 +113,10 @@ int ensure_splitk_workspace(DeviceContext* ctx, size_t bytes, void** ptr) {
   return ensure_buffer(&ctx->splitk, &ctx->splitk_bytes, bytes, ptr);
 }
 
+int ensure_transpose_workspace(DeviceContext* ctx, size_t bytes, void** ptr) {
+  return ensure_buffer(&ctx->transposed, &ctx->transposed_bytes, bytes, ptr);
+}
+
 EncodeTiledFn encode_tiled() {
   if (g_encode != nullptr) return g_encode;
   void* fn = nullptr;

@@ -26,6 +26,8 @@ struct DeviceContext {
   size_t workspace_bytes = 0;
   void* splitk = nullptr;          // cached partial sums of K-split FP64 launches
   size_t splitk_bytes = 0;
+  void* transposed = nullptr;      // cached transposed operands of lt_dgemm_ex (FP64 form)
+  size_t transposed_bytes = 0;
   void* l2_flush = nullptr;
   size_t l2_flush_bytes = 0;
 };
@@ -36,6 +38,8 @@ DeviceContext* context();
 int ensure_workspace(DeviceContext* ctx, size_t bytes, void** ptr);
 // Same for the FP64 K-split partial sums (a buffer of its own).
 int ensure_splitk_workspace(DeviceContext* ctx, size_t bytes, void** ptr);
+// Same for the transposed operands of lt_dgemm_ex's FP64 form.
+int ensure_transpose_workspace(DeviceContext* ctx, size_t bytes, void** ptr);
 
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,

@@ -98,14 +98,14 @@ __device__ __forceinline__ unsigned long long abs_bits(double v) {
 }
 
 // Row maxima of A: blockIdx.x covers 8 rows (one warp each), blockIdx.y a K segment.
-__global__ void amax_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K, int64_t kseg,
+__global__ void amax_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K, int64_t lda, int64_t kseg,
                                  unsigned long long* __restrict__ amax) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t row = static_cast<int64_t>(blockIdx.x) * 8 + warp;
   if (row >= M) return;
   const int64_t k0 = static_cast<int64_t>(blockIdx.y) * kseg;
   const int64_t k1 = (k0 + kseg < K) ? k0 + kseg : K;
-  const double* a = A + row * K;
+  const double* a = A + row * lda;
   unsigned long long m = 0;
   for (int64_t k = k0 + lane; k < k1; k += 32) {
     unsigned long long b = abs_bits(__ldg(a + k));
@@ -121,7 +121,7 @@ __global__ void amax_rows_kernel(const double* __restrict__ A, int64_t M, int64_
 // Column maxima of B: blockIdx.x covers 256 columns (one per thread), blockIdx.y a K segment.
 // With 16-byte aligned rows (B aligned, N even) each thread reads two adjacent columns per load and
 // the block covers 512 columns (`pairs` set by the launcher).
-__global__ void amax_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N, int64_t kseg,
+__global__ void amax_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N, int64_t ldb, int64_t kseg,
                                  unsigned long long* __restrict__ amax, int pairs) {
   const int64_t k0 = static_cast<int64_t>(blockIdx.y) * kseg;
   const int64_t k1 = (k0 + kseg < K) ? k0 + kseg : K;
@@ -129,9 +129,9 @@ __global__ void amax_cols_kernel(const double* __restrict__ B, int64_t K, int64_
     const int64_t col = 2 * (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x);
     if (col >= N) return;
     unsigned long long m0 = 0, m1 = 0;
-    const double* bp = B + k0 * N + col;
+    const double* bp = B + k0 * ldb + col;
 #pragma unroll 4
-    for (int64_t k = k0; k < k1; ++k, bp += N) {
+    for (int64_t k = k0; k < k1; ++k, bp += ldb) {
       const double2 v = __ldg(reinterpret_cast<const double2*>(bp));
       const unsigned long long b0 = abs_bits(v.x), b1 = abs_bits(v.y);
       m0 = b0 > m0 ? b0 : m0;
@@ -145,7 +145,7 @@ __global__ void amax_cols_kernel(const double* __restrict__ B, int64_t K, int64_
   if (col >= N) return;
   unsigned long long m = 0;
   for (int64_t k = k0; k < k1; ++k) {
-    unsigned long long b = abs_bits(__ldg(B + k * N + col));
+    unsigned long long b = abs_bits(__ldg(B + k * ldb + col));
     m = b > m ? b : m;
   }
   if (m != 0) atomicMax(&amax[col], m);
@@ -294,7 +294,8 @@ __device__ __forceinline__ void store_tile_row(int8_t* out, int64_t RB, int64_t 
 
 // Tile (rb, c) of A: thread r handles row rb*128 + r, K elements 32c .. 32c + 31.
 template <int S>
-__device__ __forceinline__ void split_rows_tile(const double* __restrict__ A, int64_t M, int64_t K, int64_t NC,
+__device__ __forceinline__ void split_rows_tile(const double* __restrict__ A, int64_t M, int64_t K, int64_t lda,
+                                                int64_t NC,
                                                 int64_t RB, const unsigned long long* __restrict__ amax,
                                                 int8_t* __restrict__ out, int64_t rb, int64_t c, int r) {
   const int64_t row = rb * kTileM + r;
@@ -305,7 +306,7 @@ __device__ __forceinline__ void split_rows_tile(const double* __restrict__ A, in
     for (int w = 0; w < 8; ++w) packed[p][w] = 0u;
   if (row < M) {
     const int e = exponent_of_maxbits(amax[row]);
-    const double* a = A + row * K;
+    const double* a = A + row * lda;
     const int64_t k0 = c * kChunk;
     if constexpr (S <= LT_OZAKI_MAX_SLICES) {
       if (e != kSentinel) {
@@ -346,7 +347,8 @@ __device__ __forceinline__ void split_rows_tile(const double* __restrict__ A, in
 
 // Tile (rb, c) of B (transposed to K-major): thread r handles column rb*128 + r.
 template <int S>
-__device__ __forceinline__ void split_cols_tile(const double* __restrict__ B, int64_t K, int64_t N, int64_t NC,
+__device__ __forceinline__ void split_cols_tile(const double* __restrict__ B, int64_t K, int64_t N, int64_t ldb,
+                                                int64_t NC,
                                                 int64_t RB, const unsigned long long* __restrict__ amax,
                                                 int8_t* __restrict__ out, int64_t rb, int64_t c, int r) {
   const int64_t col = rb * kTileN + r;
@@ -360,7 +362,7 @@ __device__ __forceinline__ void split_cols_tile(const double* __restrict__ B, in
     const int64_t k0 = c * kChunk;
     if constexpr (S <= LT_OZAKI_MAX_SLICES) {
       if (e != kSentinel) {
-        const double* bp = B + k0 * N + col;
+        const double* bp = B + k0 * ldb + col;
         const bool whole = k0 + kChunk <= K;  // no bounds test per load
 #pragma unroll
         for (int w = 0; w < 8; ++w) {
@@ -368,7 +370,7 @@ __device__ __forceinline__ void split_cols_tile(const double* __restrict__ B, in
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             const int kk = 4 * w + i;
-            v[i] = (whole || k0 + kk < K) ? __ldg(bp + kk * N) : 0.0;
+            v[i] = (whole || k0 + kk < K) ? __ldg(bp + kk * ldb) : 0.0;
           }
           split4<S>(v, e, w, packed);
         }
@@ -377,7 +379,7 @@ __device__ __forceinline__ void split_cols_tile(const double* __restrict__ B, in
 #pragma unroll
       for (int j = 0; j < kChunk; ++j) {
         const int64_t k = k0 + j;
-        const double v = (k < K) ? __ldg(B + k * N + col) : 0.0;
+        const double v = (k < K) ? __ldg(B + k * ldb + col) : 0.0;
         split_value<S>(v, e, j, packed);
       }
     }
@@ -387,19 +389,21 @@ __device__ __forceinline__ void split_cols_tile(const double* __restrict__ B, in
 
 // One block (128 threads) per tile; tiles walked with a grid stride.
 template <int S>
-__global__ void __launch_bounds__(128) split_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K, int64_t NC,
-                                                         int64_t RB, const unsigned long long* __restrict__ amax,
+__global__ void __launch_bounds__(128) split_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K, int64_t lda,
+                                                         int64_t NC, int64_t RB,
+                                                         const unsigned long long* __restrict__ amax,
                                                          int8_t* __restrict__ out) {
   for (int64_t t = blockIdx.x; t < RB * NC; t += gridDim.x)
-    split_rows_tile<S>(A, M, K, NC, RB, amax, out, t / NC, t % NC, threadIdx.x);
+    split_rows_tile<S>(A, M, K, lda, NC, RB, amax, out, t / NC, t % NC, threadIdx.x);
 }
 
 template <int S>
-__global__ void __launch_bounds__(128) split_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N, int64_t NC,
-                                                         int64_t RB, const unsigned long long* __restrict__ amax,
+__global__ void __launch_bounds__(128) split_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N, int64_t ldb,
+                                                         int64_t NC, int64_t RB,
+                                                         const unsigned long long* __restrict__ amax,
                                                          int8_t* __restrict__ out) {
   for (int64_t t = blockIdx.x; t < RB * NC; t += gridDim.x)
-    split_cols_tile<S>(B, K, N, NC, RB, amax, out, t / NC, t % NC, threadIdx.x);
+    split_cols_tile<S>(B, K, N, ldb, NC, RB, amax, out, t / NC, t % NC, threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -414,6 +418,7 @@ struct OzProblem {
   const unsigned long long* amax_b;
   int64_t M, N, nkc, rba, rbb;
   double alpha, beta;
+  int64_t ldc;  // row stride of C (>= N)
 };
 
 // One output tile of one problem.
@@ -717,7 +722,7 @@ __device__ __forceinline__ void ozaki_body(const Source& src, DeviceStatus* stat
       if (row < pr.M) {
         const int sig = exponent_of_maxbits(pr.amax_a[row]);
         const int64_t col0 = J.n0 + half * 64;
-        double* crow = pr.C + row * pr.N;
+        double* crow = pr.C + row * pr.ldc;
         const int64_t N = pr.N;
         const double alpha = pr.alpha, beta = pr.beta;
         const unsigned long long* amax_b = pr.amax_b;
@@ -1057,7 +1062,7 @@ __device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatu
       if (row < pr.M) {
         const int sig = exponent_of_maxbits(pr.amax_a[row]);
         const int64_t col0 = n0 + half * 64;
-        double* crow = pr.C + row * pr.N;
+        double* crow = pr.C + row * pr.ldc;
         const int64_t N = pr.N;
         const double alpha = pr.alpha, beta = pr.beta;
         const unsigned long long* amax_b = pr.amax_b;
@@ -1204,10 +1209,10 @@ int launch_split_s(const double* A, const double* B, int64_t M, int64_t N, int64
                    int sms, cudaStream_t stream) {
   const int64_t cap = static_cast<int64_t>(sms) * 64;
   const int64_t ta = L.RBa * L.NC, tb = L.RBb * L.NC;
-  if (ta > 0) split_rows_kernel<S><<<static_cast<unsigned>(ta < cap ? ta : cap), 128, 0, stream>>>(A, M, K, L.NC, L.RBa,
+  if (ta > 0) split_rows_kernel<S><<<static_cast<unsigned>(ta < cap ? ta : cap), 128, 0, stream>>>(A, M, K, K, L.NC, L.RBa,
                                                                                                    amax_a, sa);
   LT_CUDA_TRY(cudaGetLastError());
-  if (tb > 0) split_cols_kernel<S><<<static_cast<unsigned>(tb < cap ? tb : cap), 128, 0, stream>>>(B, K, N, L.NC, L.RBb,
+  if (tb > 0) split_cols_kernel<S><<<static_cast<unsigned>(tb < cap ? tb : cap), 128, 0, stream>>>(B, K, N, N, L.NC, L.RBb,
                                                                                                    amax_b, sb);
   LT_CUDA_TRY(cudaGetLastError());
   return LT_OK;
@@ -1227,25 +1232,27 @@ int launch_split(int s, const double* A, const double* B, int64_t M, int64_t N, 
 }
 
 template <int S>
-void launch_split_rows_s(const double* A, int64_t M, int64_t K, int64_t NC, const unsigned long long* amax, int8_t* sa,
+void launch_split_rows_s(const double* A, int64_t M, int64_t K, int64_t lda, int64_t NC, const unsigned long long* amax,
+                         int8_t* sa,
                          int sms, cudaStream_t stream) {
   const int64_t cap = static_cast<int64_t>(sms) * 64;
   const int64_t rb = ceil_div(M, kTileM), t = rb * NC;
-  if (t > 0) split_rows_kernel<S><<<static_cast<unsigned>(t < cap ? t : cap), 128, 0, stream>>>(A, M, K, NC, rb, amax, sa);
+  if (t > 0) split_rows_kernel<S><<<static_cast<unsigned>(t < cap ? t : cap), 128, 0, stream>>>(A, M, K, lda, NC, rb, amax, sa);
 }
 
 template <int S>
-void launch_split_cols_s(const double* B, int64_t K, int64_t N, int64_t NC, const unsigned long long* amax, int8_t* sb,
+void launch_split_cols_s(const double* B, int64_t K, int64_t N, int64_t ldb, int64_t NC, const unsigned long long* amax,
+                         int8_t* sb,
                          int sms, cudaStream_t stream) {
   const int64_t cap = static_cast<int64_t>(sms) * 64;
   const int64_t rb = ceil_div(N, kTileN), t = rb * NC;
-  if (t > 0) split_cols_kernel<S><<<static_cast<unsigned>(t < cap ? t : cap), 128, 0, stream>>>(B, K, N, NC, rb, amax, sb);
+  if (t > 0) split_cols_kernel<S><<<static_cast<unsigned>(t < cap ? t : cap), 128, 0, stream>>>(B, K, N, ldb, NC, rb, amax, sb);
 }
 
 // Row side of the split: exponents of rows 0..M-1 of A (amax must be zero on entry) and their
 // slices, written as row blocks 0.. of `sa` (chunk-major, NC chunks).
-int rows_stage(int s, const double* A, int64_t M, int64_t K, int64_t NC, unsigned long long* amax, int8_t* sa, int sms,
-               cudaStream_t stream) {
+int rows_stage(int s, const double* A, int64_t M, int64_t K, int64_t lda, int64_t NC, unsigned long long* amax,
+               int8_t* sa, int sms, cudaStream_t stream) {
   if (M <= 0) return LT_OK;
   if (K > 0) {
     // 8 rows per block, K split so that the grid covers the GPU.
@@ -1255,12 +1262,12 @@ int rows_stage(int s, const double* A, int64_t M, int64_t K, int64_t NC, unsigne
     int64_t kseg = round_up((K + ksplit - 1) / ksplit, 256);
     ksplit = (K + kseg - 1) / kseg;
     amax_rows_kernel<<<dim3(static_cast<unsigned>(row_blocks), static_cast<unsigned>(ksplit)), 256, 0, stream>>>(
-        A, M, K, kseg, amax);
+        A, M, K, lda, kseg, amax);
     LT_CUDA_TRY(cudaGetLastError());
   }
   switch (s) {
 #define LT_ROWS_CASE(S) \
-  case S: launch_split_rows_s<S>(A, M, K, NC, amax, sa, sms, stream); break;
+  case S: launch_split_rows_s<S>(A, M, K, lda, NC, amax, sa, sms, stream); break;
     LT_ROWS_CASE(1) LT_ROWS_CASE(2) LT_ROWS_CASE(3) LT_ROWS_CASE(4) LT_ROWS_CASE(5) LT_ROWS_CASE(6)
     LT_ROWS_CASE(7) LT_ROWS_CASE(8) LT_ROWS_CASE(9) LT_ROWS_CASE(10) LT_ROWS_CASE(11) LT_ROWS_CASE(12)
 #undef LT_ROWS_CASE
@@ -1271,11 +1278,11 @@ int rows_stage(int s, const double* A, int64_t M, int64_t K, int64_t NC, unsigne
 }
 
 // Column side: exponents of columns 0..N-1 of B (amax zero on entry) and their slices.
-int cols_stage(int s, const double* B, int64_t K, int64_t N, int64_t NC, unsigned long long* amax, int8_t* sb, int sms,
-               cudaStream_t stream) {
+int cols_stage(int s, const double* B, int64_t K, int64_t N, int64_t ldb, int64_t NC, unsigned long long* amax,
+               int8_t* sb, int sms, cudaStream_t stream) {
   if (N <= 0) return LT_OK;
   if (K > 0) {
-    const int pairs = (N % 2 == 0) && ((reinterpret_cast<uintptr_t>(B) & 15) == 0);
+    const int pairs = (N % 2 == 0) && (ldb % 2 == 0) && ((reinterpret_cast<uintptr_t>(B) & 15) == 0);
     const int64_t per_block = pairs ? 512 : 256;
     int64_t col_blocks = (N + per_block - 1) / per_block;
     int64_t ksplit_b = (8 * sms + col_blocks - 1) / col_blocks;
@@ -1283,12 +1290,12 @@ int cols_stage(int s, const double* B, int64_t K, int64_t N, int64_t NC, unsigne
     int64_t kseg_b = (K + ksplit_b - 1) / ksplit_b;
     ksplit_b = (K + kseg_b - 1) / kseg_b;
     amax_cols_kernel<<<dim3(static_cast<unsigned>(col_blocks), static_cast<unsigned>(ksplit_b)), 256, 0, stream>>>(
-        B, K, N, kseg_b, amax, pairs);
+        B, K, N, ldb, kseg_b, amax, pairs);
     LT_CUDA_TRY(cudaGetLastError());
   }
   switch (s) {
 #define LT_COLS_CASE(S) \
-  case S: launch_split_cols_s<S>(B, K, N, NC, amax, sb, sms, stream); break;
+  case S: launch_split_cols_s<S>(B, K, N, ldb, NC, amax, sb, sms, stream); break;
     LT_COLS_CASE(1) LT_COLS_CASE(2) LT_COLS_CASE(3) LT_COLS_CASE(4) LT_COLS_CASE(5) LT_COLS_CASE(6)
     LT_COLS_CASE(7) LT_COLS_CASE(8) LT_COLS_CASE(9) LT_COLS_CASE(10) LT_COLS_CASE(11) LT_COLS_CASE(12)
 #undef LT_COLS_CASE
@@ -1311,8 +1318,8 @@ int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int
   auto* sa = reinterpret_cast<int8_t*>(ws + L.off_sa);
   auto* sb = reinterpret_cast<int8_t*>(ws + L.off_sb);
   LT_CUDA_TRY(cudaMemsetAsync(ws, 0, L.off_sa, stream));
-  LT_TRY(rows_stage(s, A, M, K, L.NC, amax_a, sa, ctx->sm_count, stream));
-  return cols_stage(s, B, K, N, L.NC, amax_b, sb, ctx->sm_count, stream);
+  LT_TRY(rows_stage(s, A, M, K, K, L.NC, amax_a, sa, ctx->sm_count, stream));
+  return cols_stage(s, B, K, N, N, L.NC, amax_b, sb, ctx->sm_count, stream);
 }
 
 // Products and recombination of one problem whose slices are in place: the CTA-pair kernel for two
@@ -1342,11 +1349,45 @@ int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double bet
   pr.amax_b = reinterpret_cast<const unsigned long long*>(ws + L.off_amax_b);
   pr.M = M;
   pr.N = N;
+  pr.ldc = N;
   pr.nkc = L.NC;
   pr.rba = L.RBa;
   pr.rbb = L.RBb;
   pr.alpha = alpha;
   pr.beta = beta;
+  return launch_product(s, pr, ctx, stream);
+}
+
+// Row strides and transposes (lt_dgemm_ex): op(A) = A (M x K, row stride lda) or A^T (A stored
+// K x M, row stride lda), op(B) = B (K x N, ldb) or B^T (B stored N x K, ldb), C is M x N with row
+// stride ldc. A transposed operand goes through the other side's kernels: the rows of op(A) = A^T
+// are the columns of the stored A, which amax_cols / split_cols read, writing the same tiles the row
+// kernels write (tile row = row of op(A)); op(B) = B^T goes through amax_rows / split_rows. Every
+// digit and every output element is the one run() computes on packed op(A) and op(B), so results are
+// bit-identical to it.
+int run_ex(bool trans_a, bool trans_b, const double* A, int64_t lda, const double* B, int64_t ldb, double* C, int64_t ldc,
+           int64_t M, int64_t N, int64_t K, double alpha, double beta, int s, void* workspace, size_t workspace_bytes,
+           cudaStream_t stream) {
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  const Layout L = layout_for(M, N, K, s);
+  if (workspace_bytes < L.total) return set_error(LT_ERR_NO_MEMORY, "Ozaki workspace too small");
+  uint8_t* ws = static_cast<uint8_t*>(workspace);
+  auto* amax_a = reinterpret_cast<unsigned long long*>(ws + L.off_amax_a);
+  auto* amax_b = reinterpret_cast<unsigned long long*>(ws + L.off_amax_b);
+  auto* sa = reinterpret_cast<int8_t*>(ws + L.off_sa);
+  auto* sb = reinterpret_cast<int8_t*>(ws + L.off_sb);
+  LT_CUDA_TRY(cudaMemsetAsync(ws, 0, L.off_sa, stream));
+  const int sms = ctx->sm_count;
+  if (!trans_a)
+    LT_TRY(rows_stage(s, A, M, K, lda, L.NC, amax_a, sa, sms, stream));
+  else
+    LT_TRY(cols_stage(s, A, K, M, lda, L.NC, amax_a, sa, sms, stream));
+  if (!trans_b)
+    LT_TRY(cols_stage(s, B, K, N, ldb, L.NC, amax_b, sb, sms, stream));
+  else
+    LT_TRY(rows_stage(s, B, N, K, ldb, L.NC, amax_b, sb, sms, stream));
+  OzProblem pr{sa, sb, C, amax_a, amax_b, M, N, L.NC, L.RBa, L.RBb, alpha, beta, ldc};
   return launch_product(s, pr, ctx, stream);
 }
 
@@ -1411,7 +1452,7 @@ int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, 
     cuda(cudaMemsetAsync(ws, 0, L.off_sa, stream), "memset");
     cuda(cudaStreamWaitEvent(stream, e_b, 0), "wait");
   }
-  if (rc == LT_OK) rc = cols_stage(s, Bd, K, N, L.NC, amax_b, sb, ctx->sm_count, stream);
+  if (rc == LT_OK) rc = cols_stage(s, Bd, K, N, N, L.NC, amax_b, sb, ctx->sm_count, stream);
   for (int64_t i = 0; i < npanels && rc == LT_OK; ++i) {
     const int64_t r0 = i * panel, rows = std::min(panel, M - r0);
     cudaEvent_t e_in = ev[2 * i], e_out = ev[2 * i + 1];
@@ -1424,10 +1465,10 @@ int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, 
     cuda(cudaStreamWaitEvent(stream, e_in, 0), "wait");
     if (rc != LT_OK) break;
     int8_t* sa_panel = sa + (r0 / kTileM) * L.NC * chunk_block;
-    rc = rows_stage(s, Ad + r0 * K, rows, K, L.NC, amax_a + r0, sa_panel, ctx->sm_count, stream);
+    rc = rows_stage(s, Ad + r0 * K, rows, K, K, L.NC, amax_a + r0, sa_panel, ctx->sm_count, stream);
     if (rc != LT_OK) break;
     OzProblem pr{sa_panel, sb, Cd + r0 * N, amax_a + r0, amax_b, rows, N, L.NC, ceil_div(rows, kTileM), L.RBb,
-                 alpha, beta};
+                 alpha, beta, N};
     rc = launch_product(s, pr, ctx, stream);
     if (rc != LT_OK) break;
     cuda(cudaEventRecord(e_out, stream), "record");
@@ -1513,7 +1554,7 @@ __global__ void __launch_bounds__(128) g_split_rows_kernel(const GSplit* __restr
   const int pi = find_problem(off, count, blockIdx.x);
   const GSplit& g = P[pi];
   const int64_t t = blockIdx.x - off[pi];
-  split_rows_tile<S>(g.A, g.M, g.K, g.NC, g.RBa, g.amax_a, g.sa, t / g.NC, t % g.NC, threadIdx.x);
+  split_rows_tile<S>(g.A, g.M, g.K, g.K, g.NC, g.RBa, g.amax_a, g.sa, t / g.NC, t % g.NC, threadIdx.x);
 }
 
 template <int S>
@@ -1522,7 +1563,7 @@ __global__ void __launch_bounds__(128) g_split_cols_kernel(const GSplit* __restr
   const int pi = find_problem(off, count, blockIdx.x);
   const GSplit& g = P[pi];
   const int64_t t = blockIdx.x - off[pi];
-  split_cols_tile<S>(g.B, g.K, g.N, g.NC, g.RBb, g.amax_b, g.sb, t / g.NC, t % g.NC, threadIdx.x);
+  split_cols_tile<S>(g.B, g.K, g.N, g.N, g.NC, g.RBb, g.amax_b, g.sb, t / g.NC, t % g.NC, threadIdx.x);
 }
 
 struct Grouped {
@@ -1596,7 +1637,7 @@ int grouped_create(const lt_gemm_problem* problems, int count, int s, Grouped** 
                reinterpret_cast<int8_t*>(ws + off_sa[i]), reinterpret_cast<int8_t*>(ws + off_sb[i])};
     const int64_t nb[4] = {p.K > 0 ? (p.M + 7) / 8 : 0, p.K > 0 ? (p.N + 255) / 256 : 0, L.RBa * L.NC, L.RBb * L.NC};
     for (int k = 0; k < 4; ++k) offs[k * (count + 1) + i + 1] = offs[k * (count + 1) + i] + static_cast<int>(nb[k]);
-    probs[i] = OzProblem{g.sa, g.sb, p.C, g.amax_a, g.amax_b, p.M, p.N, L.NC, L.RBa, L.RBb, p.alpha, p.beta};
+    probs[i] = OzProblem{g.sa, g.sb, p.C, g.amax_a, g.amax_b, p.M, p.N, L.NC, L.RBa, L.RBb, p.alpha, p.beta, p.N};
     G->ntiles += L.RBa * L.RBb;
   }
   for (int k = 0; k < 4; ++k) G->blocks[k] = offs[k * (count + 1) + count];
@@ -1753,7 +1794,7 @@ int noalloc_run(const double* A, const double* B, double* C, int64_t M, int64_t 
     int64_t kseg = round_up((K + ksplit - 1) / ksplit, 256);
     ksplit = (K + kseg - 1) / kseg;
     amax_rows_kernel<<<dim3(static_cast<unsigned>(row_blocks), static_cast<unsigned>(ksplit)), 256, 0, stream>>>(
-        A, M, K, kseg, amax_a);
+        A, M, K, K, kseg, amax_a);
     LT_CUDA_TRY(cudaGetLastError());
     int64_t col_blocks = (N + 255) / 256;
     int64_t ksplit_b = (8 * sms + col_blocks - 1) / col_blocks;
@@ -1761,11 +1802,11 @@ int noalloc_run(const double* A, const double* B, double* C, int64_t M, int64_t 
     int64_t kseg_b = (K + ksplit_b - 1) / ksplit_b;
     ksplit_b = (K + kseg_b - 1) / kseg_b;
     amax_cols_kernel<<<dim3(static_cast<unsigned>(col_blocks), static_cast<unsigned>(ksplit_b)), 256, 0, stream>>>(
-        B, K, N, kseg_b, amax_b, 0);
+        B, K, N, N, kseg_b, amax_b, 0);
     LT_CUDA_TRY(cudaGetLastError());
   }
   LT_TRY(launch_split(s, A, B, M, N, K, L, amax_a, amax_b, sa, sb, sms, stream));
-  OzProblem pr{sa, sb, C, amax_a, amax_b, M, N, L.NC, L.RBa, L.RBb, alpha, beta};
+  OzProblem pr{sa, sb, C, amax_a, amax_b, M, N, L.NC, L.RBa, L.RBb, alpha, beta, N};
   return launch_gemm<false>(s, pr, L.RBa * L.RBb, &ctx, stream);
 }
 

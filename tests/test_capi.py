@@ -78,3 +78,26 @@ def test_unknown_impl_rejected():
 
     with pytest.raises(KeyError):
         lt.dgemm("final", 0, 0, 0, 1, 1, 1)
+
+
+def test_dgemm_ex_rejects_bad_arguments():
+    """Argument checks of lt_dgemm_ex run before any device work (no GPU needed)."""
+    import libthom_b200 as lt
+
+    L = lt.lib()
+    ok_args = dict(M=4, N=4, K=4, lda=4, ldb=4, ldc=4)
+
+    def call(form=lt.LT_FORM_FP64, ta=b"N", tb=b"N", slices=8, **kw):
+        a = dict(ok_args, **kw)
+        return L.lt_dgemm_ex(form, ta, tb, a["M"], a["N"], a["K"], 1.0, 8, a["lda"], 8, a["ldb"], 0.0, 8, a["ldc"],
+                             slices, None)
+
+    assert call(ta=b"X") == lt.LT_ERR_INVALID_ARGUMENT
+    assert call(form=9) == lt.LT_ERR_INVALID_ARGUMENT
+    assert call(form=lt.LT_FORM_OZAKI, slices=0) == lt.LT_ERR_INVALID_ARGUMENT
+    assert call(lda=3) == lt.LT_ERR_INVALID_ARGUMENT
+    assert call(ta=b"T", M=6, lda=5) == lt.LT_ERR_INVALID_ARGUMENT  # transposed A: lda >= M
+    assert call(tb=b"T", K=6, ldb=5, lda=6) == lt.LT_ERR_INVALID_ARGUMENT  # transposed B: ldb >= K
+    assert call(ldc=3) == lt.LT_ERR_INVALID_ARGUMENT
+    assert call(M=-1) == lt.LT_ERR_INVALID_ARGUMENT
+    assert L.lt_dgemm_ex(0, b"N", b"N", 4, 4, 4, 1.0, 12, 4, 8, 4, 0.0, 8, 4, 8, None) == lt.LT_ERR_UNALIGNED
