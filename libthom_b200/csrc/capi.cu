@@ -71,7 +71,7 @@ int dgemm_fp64_dispatch(const double* A, const double* B, double* C, int64_t M, 
   if (M == 0 || N == 0) return ok();
   DeviceContext* ctx = context();
   if (ctx == nullptr) return last_error();
-  const bool tma = fp64::tma_compatible(A, B, N, K);
+  const bool tma = K > 0 && fp64::tma_compatible(A, B, N, K);  // no tensor map over zero columns
   if (config < 0) config = tuner::lookup(M, N, K, tma);
   if (config < 0) config = fp64::heuristic_config(A, B, M, N, K, ctx->sm_count);
   if (fp64::config_is_tma(config) && !tma)

@@ -128,7 +128,7 @@ bool config_is_tma(int i) { return i >= 0 && i < kNumConfigs && kConfigs[i].tma;
 // measured 8192^3 rates relative to 128x64 (TMA: 34.8, 33.2, 27.6, 18.0, 18.0 TF/s for 128x64,
 // 64x128, 64x64, 64x32, 32x64). The K split handles what remains of a poorly filled last wave.
 int heuristic_config(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int sm_count) {
-  return heuristic_config_for(M, N, sm_count, tma_compatible(A, B, N, K));
+  return heuristic_config_for(M, N, sm_count, K > 0 && tma_compatible(A, B, N, K));
 }
 
 int heuristic_config_for(int64_t M, int64_t N, int sm_count, bool tma) {
