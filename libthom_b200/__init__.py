@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import struct
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -66,6 +67,8 @@ class TuneEntry(ctypes.Structure):
 # name -> (restype, argtypes)
 _GEMM = [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64]
 _REF = [_vp, _vp, _vp, _sz, _sz, _sz, _f64, _f64]
+_HGEMM = [_vp, _vp, _vp, _i64, _i64, _i64, _f32, _f32]
+_HREF = [_vp, _vp, _vp, _sz, _sz, _sz, _c.c_uint16, _c.c_uint16]
 SIGNATURES = {
     "lt_get_last_error": (_i32, []),
     "lt_error_string": (_c.c_char_p, [_i32]),
@@ -125,6 +128,15 @@ SIGNATURES = {
     "lt_dgemm_ozaki_host": (_i32, [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _i32, _vp]),
     "lt_dgemm_ex": (_i32, [_i32, _c.c_char, _c.c_char, _i64, _i64, _i64, _f64, _vp, _i64, _vp, _i64, _f64, _vp, _i64,
                            _i32, _vp]),
+    # libthom_hgemm.h
+    "hgemm_tc100": (_f32, _HREF),
+    "hgemm_cublas": (_f32, _HREF),
+    "lt_hgemm": (_i32, _HGEMM + [_vp]),
+    "lt_hgemm_config": (_i32, _HGEMM + [_i32, _vp]),
+    "lt_hgemm_num_configs": (_i32, []),
+    "lt_hgemm_config_name": (_c.c_char_p, [_i32]),
+    "lt_hgemm_default_config": (_i32, [_i64, _i64, _i64]),
+    "lt_hgemm_cublas": (_i32, _HGEMM + [_i32, _vp]),
 }
 
 _lib = None
@@ -258,6 +270,35 @@ def dgemm_ozaki_host(A, B, C, M, N, K, alpha=1.0, beta=0.0, slices=8, stream=Non
     """Ozaki DGEMM on host (CPU) tensors or arrays, pipelined through the GPU (lt_dgemm_ozaki_host).
     C holds C0 on entry and the result on return."""
     check(lib().lt_dgemm_ozaki_host(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, slices, _stream(stream)))
+
+
+def _half_bits(x: float) -> int:
+    """IEEE binary16 bit pattern of x (round to nearest even)."""
+    return int.from_bytes(struct.pack("<e", x), "little")
+
+
+def hgemm(impl: str, A, B, C, M: int, N: int, K: int, alpha: float = 1.0, beta: float = 0.0) -> float:
+    """Reference-contract call hgemm_<impl>(A, B, C, M, N, K, alpha, beta) on FP16 device tensors;
+    returns the milliseconds the implementation measured (routines/hgemm/hgemm.h:6-7)."""
+    fn = getattr(lib(), f"hgemm_{impl}")
+    ms = fn(_ptr(A), _ptr(B), _ptr(C), M, N, K, _half_bits(alpha), _half_bits(beta))
+    err = lib().lt_get_last_error()
+    check(err)
+    return ms
+
+
+def hgemm_tc(A, B, C, M, N, K, alpha=1.0, beta=0.0, stream=None, config: int = -1) -> None:
+    """C = alpha*A*B + beta*C on FP16 device tensors (lt_hgemm_config), FP32 accumulation."""
+    check(lib().lt_hgemm_config(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, config, _stream(stream)))
+
+
+def hgemm_cublas(A, B, C, M, N, K, alpha=1.0, beta=0.0, compute_f32: bool = True, stream=None) -> None:
+    check(lib().lt_hgemm_cublas(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, int(compute_f32), _stream(stream)))
+
+
+def hgemm_configs() -> list[str]:
+    L = lib()
+    return [L.lt_hgemm_config_name(i).decode() for i in range(L.lt_hgemm_num_configs())]
 
 
 def dgemm_ex(transa: str, transb: str, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, form=LT_FORM_FP64, slices=8,

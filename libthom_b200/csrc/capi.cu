@@ -2,11 +2,13 @@
 // (float dgemm_<impl>(...) returning milliseconds, routines/dgemm/dgemm.h:9) and the
 // stream-ordered lt_* API.
 #include <cublas_v2.h>
+#include <cuda_fp16.h>
 
 #include <cmath>
 #include <cstdio>
 #include <mutex>
 
+#include "../../include/libthom_hgemm.h"
 #include "lt_internal.h"
 #include "lt_runtime.cuh"
 
@@ -196,6 +198,47 @@ float dgemm_tc100(const double* A, const double* B, double* C, size_t M, size_t 
   return lt::timed("tc100", [&] {
     return lt_dgemm_fp64(A, B, C, static_cast<int64_t>(M), static_cast<int64_t>(N), static_cast<int64_t>(K), alpha,
                          beta, nullptr);
+  });
+}
+
+int lt_hgemm_cublas(const lt_half* A, const lt_half* B, lt_half* C, int64_t M, int64_t N, int64_t K, float alpha,
+                    float beta, int compute_f32, void* stream) {
+  if (M < 0 || N < 0 || K < 0 || M > 0x7fffffff || N > 0x7fffffff || K > 0x7fffffff)
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "bad dimension");
+  if ((M > 0 && K > 0 && A == nullptr) || (K > 0 && N > 0 && B == nullptr) || (M > 0 && N > 0 && C == nullptr))
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "null matrix pointer");
+  if (M == 0 || N == 0) return lt::ok();
+  cublasHandle_t h;
+  LT_TRY(lt::cublas_handle(&h));
+  cublasSetStream(h, lt::as_stream(stream));
+  // Row-major C = A B as column-major C^T = B^T A^T (routines/hgemm/hgemm_cublas.cu:10-22).
+  const __half ha = __float2half_rn(alpha), hb = __float2half_rn(beta);
+  const int n = static_cast<int>(N), m = static_cast<int>(M), k = static_cast<int>(K);
+  const int ldb = n > 0 ? n : 1, lda = k > 0 ? k : 1;
+  cublasStatus_t st =
+      compute_f32 ? cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &alpha, B, CUDA_R_16F, ldb, A, CUDA_R_16F, lda,
+                                 &beta, C, CUDA_R_16F, ldb, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT)
+                  : cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, k, &ha, B, CUDA_R_16F, ldb, A, CUDA_R_16F, lda,
+                                 &hb, C, CUDA_R_16F, ldb, CUBLAS_COMPUTE_16F, CUBLAS_GEMM_DEFAULT);
+  if (st != CUBLAS_STATUS_SUCCESS) return lt::set_error(LT_ERR_CUDA, "cublasGemmEx failed: %d", static_cast<int>(st));
+  return lt::ok();
+}
+
+static float half_bits_to_float(lt_half x) { return __half2float(__ushort_as_half(x)); }
+
+float hgemm_tc100(const lt_half* A, const lt_half* B, lt_half* C, size_t M, size_t N, size_t K, lt_half alpha,
+                  lt_half beta) {
+  return lt::timed("hgemm tc100", [&] {
+    return lt_hgemm(A, B, C, static_cast<int64_t>(M), static_cast<int64_t>(N), static_cast<int64_t>(K),
+                    half_bits_to_float(alpha), half_bits_to_float(beta), nullptr);
+  });
+}
+
+float hgemm_cublas(const lt_half* A, const lt_half* B, lt_half* C, size_t M, size_t N, size_t K, lt_half alpha,
+                   lt_half beta) {
+  return lt::timed("hgemm cublas", [&] {
+    return lt_hgemm_cublas(A, B, C, static_cast<int64_t>(M), static_cast<int64_t>(N), static_cast<int64_t>(K),
+                           half_bits_to_float(alpha), half_bits_to_float(beta), 0, nullptr);
   });
 }
 

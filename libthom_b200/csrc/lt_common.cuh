@@ -320,6 +320,40 @@ __device__ __forceinline__ uint64_t smem_desc_k_sw32(uint32_t addr) {
   return d;
 }
 
+// Shared-memory matrix descriptor for an MN-major operand with 128-byte swizzle, as a tiled TMA
+// copy with CU_TENSOR_MAP_SWIZZLE_128B writes a box whose inner dimension is M or N: one 128-byte
+// row (64 16-bit elements of M/N) per K index, 8 K rows per 1024-byte swizzle atom. `lbo` (bits
+// [16,30)) is the distance between 64-element blocks of M/N, `sbo` (bits [32,46)) the distance
+// between 8-row K groups; version 1, layout type 2 (SWIZZLE_128B). The base is 1024-byte aligned.
+__device__ __forceinline__ uint64_t smem_desc_mn_sw128(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((addr >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16;
+  d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32;
+  d |= static_cast<uint64_t>(1u) << 46;
+  d |= static_cast<uint64_t>(2u) << 61;
+  return d;
+}
+
+// Instruction descriptor for kind::f16 with 32-bit float accumulators: D = F32 (bits [4,6) = 1),
+// A and B F16 (bits [7,10) and [10,13) = 0), A K-major (bit 15 = 0), B K-major or MN-major
+// (bit 16), N >> 3 in [17,23), M >> 4 in [24,29).
+__host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N, bool b_mn_major) {
+  return (1u << 4) | (b_mn_major ? (1u << 16) : 0u) | (static_cast<uint32_t>(N >> 3) << 17) |
+         (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+// Pair MMA, kind::f16 (both operands F16, accumulators F32).
+__device__ __forceinline__ void mma_f16_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                             uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 // Instruction descriptor for kind::i8: D = S32 (bits [4,6) = 2), A and B signed 8-bit
 // (bits [7,10) and [10,13) = 1), both K-major (bits 15, 16 = 0), N >> 3 in [17,23),
 // M >> 4 in [24,29).

@@ -117,6 +117,10 @@ int ensure_transpose_workspace(DeviceContext* ctx, size_t bytes, void** ptr) {
   return ensure_buffer(&ctx->transposed, &ctx->transposed_bytes, bytes, ptr);
 }
 
+int ensure_pack_workspace(DeviceContext* ctx, size_t bytes, void** ptr) {
+  return ensure_buffer(&ctx->pack, &ctx->pack_bytes, bytes, ptr);
+}
+
 EncodeTiledFn encode_tiled() {
   if (g_encode != nullptr) return g_encode;
   void* fn = nullptr;

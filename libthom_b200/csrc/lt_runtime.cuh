@@ -28,6 +28,8 @@ struct DeviceContext {
   size_t splitk_bytes = 0;
   void* transposed = nullptr;      // cached transposed operands of lt_dgemm_ex (FP64 form)
   size_t transposed_bytes = 0;
+  void* pack = nullptr;            // cached padded copies of HGEMM operands with unaligned pitches
+  size_t pack_bytes = 0;
   void* l2_flush = nullptr;
   size_t l2_flush_bytes = 0;
 };
@@ -40,6 +42,8 @@ int ensure_workspace(DeviceContext* ctx, size_t bytes, void** ptr);
 int ensure_splitk_workspace(DeviceContext* ctx, size_t bytes, void** ptr);
 // Same for the transposed operands of lt_dgemm_ex's FP64 form.
 int ensure_transpose_workspace(DeviceContext* ctx, size_t bytes, void** ptr);
+// Same for the padded operand copies of the HGEMM.
+int ensure_pack_workspace(DeviceContext* ctx, size_t bytes, void** ptr);
 
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,

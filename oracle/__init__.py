@@ -16,6 +16,8 @@ HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libref_dgemm.so"
 REF_FINAL_LIB = HERE / "_ref" / "libref_dgemm_final.so"
+REF_HGEMM_LIB = HERE / "_ref" / "libref_hgemm.so"
+REF_HGEMM_KERNELS_LIB = HERE / "_ref" / "libref_hgemm_kernels.so"
 
 _c = ctypes
 _vp, _i64, _i32, _f64, _u64 = _c.c_void_p, _c.c_int64, _c.c_int, _c.c_double, _c.c_uint64
@@ -33,6 +35,8 @@ def build(quiet: bool = True) -> None:
 _lib = None
 _ref = None
 _ref_final = None
+_ref_hgemm = None
+_ref_hgemm_kernels = None
 
 
 def lib() -> ctypes.CDLL:
@@ -50,6 +54,12 @@ def lib() -> ctypes.CDLL:
         L.oracle_fill.argtypes = [_vp, _i64, _u64, _u64, _i32]
         L.oracle_scale_rows.argtypes = [_vp, _i64, _i64, _u64, _u64, _i32]
         L.oracle_scale_cols.argtypes = [_vp, _i64, _i64, _u64, _u64, _i32]
+        L.oracle_half_to_float.restype = _c.c_float
+        L.oracle_half_to_float.argtypes = [_c.c_uint16]
+        L.oracle_float_to_half.restype = _c.c_uint16
+        L.oracle_float_to_half.argtypes = [_c.c_float]
+        L.oracle_hgemm_ref.argtypes = [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _c.c_float, _c.c_float, _vp, _i64]
+        L.oracle_hgemm_exact_rows.argtypes = [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _vp, _i64]
         L.oracle_dgemm_naive.argtypes = [_vp, _vp, _vp, _i32, _i32, _i32, _f64, _f64]
         L.oracle_dgemm_blocked.argtypes = [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _i32]
         L.oracle_dgemm_dot2_rows.argtypes = [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _vp, _i64, _i32]
@@ -92,6 +102,90 @@ def ref_final_lib() -> ctypes.CDLL | None:
         R.ref_dgemm_final.argtypes = [_vp, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, _f64, _f64]
         _ref_final = R
     return _ref_final
+
+
+def ref_hgemm_lib() -> ctypes.CDLL | None:
+    """The reference's own HGEMM host check (routines/hgemm/hgemm.cu:135-149), if built here:
+    ref_hgemm_host(A, B, C, M, N, K, alpha_bits, beta_bits) overwrites C (FP16 bit patterns)."""
+    global _ref_hgemm
+    if _ref_hgemm is None and REF_HGEMM_LIB.exists():
+        R = ctypes.CDLL(str(REF_HGEMM_LIB))
+        R.ref_hgemm_host.argtypes = [_vp, _vp, _vp, _i32, _i32, _i32, _c.c_uint16, _c.c_uint16]
+        _ref_hgemm = R
+    return _ref_hgemm
+
+
+def ref_hgemm_kernels_lib() -> ctypes.CDLL | None:
+    """The reference's HGEMM CUDA kernels hgemm_final and hgemm_better_reuse built for sm_100a, if
+    built here: ref_hgemm_final / ref_hgemm_better_reuse(A, B, C, M, N, K, alpha_bits, beta_bits)
+    on device pointers, returning the milliseconds of their own CUDA events."""
+    global _ref_hgemm_kernels
+    if _ref_hgemm_kernels is None and REF_HGEMM_KERNELS_LIB.exists():
+        R = ctypes.CDLL(str(REF_HGEMM_KERNELS_LIB))
+        for name in ("ref_hgemm_final", "ref_hgemm_better_reuse"):
+            f = getattr(R, name)
+            f.restype = ctypes.c_float
+            f.argtypes = [_vp, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, _c.c_uint16, _c.c_uint16]
+        _ref_hgemm_kernels = R
+    return _ref_hgemm_kernels
+
+
+def half_bits(x) -> np.ndarray:
+    """FP16 bit patterns (uint16) of an array of numbers (numpy's float16 rounding, ties to even)."""
+    return np.array(x, dtype=np.float16, order="C").view(np.uint16)
+
+
+def make_half_problem(M: int, N: int, K: int, seed: int = 1234, lo: float = 0.0, hi: float = 1.0):
+    """FP16 inputs A (M x K), B (K x N), C0 (M x N) as uint16 bit patterns, uniform in [lo, hi) then
+    rounded to FP16 (the reference's fill is cuRAND uniform (0, 1] rounded to FP16,
+    routines/hgemm/hgemm.cu:107-119)."""
+    rng = np.random.default_rng(seed)
+    A = half_bits(rng.uniform(lo, hi, size=(M, K)))
+    B = half_bits(rng.uniform(lo, hi, size=(K, N)))
+    C0 = half_bits(rng.uniform(lo, hi, size=(M, N)))
+    return A, B, C0
+
+
+def hgemm_ref(A, B, C0, alpha: float, beta: float, rows=None) -> np.ndarray:
+    """The reference's HGEMM host check restated (oracle_hgemm_ref) on uint16 bit patterns; the
+    selected rows (all by default) of C as uint16."""
+    M, K = A.shape
+    N = B.shape[1]
+    A, B, C0 = (np.ascontiguousarray(x, dtype=np.uint16) for x in (A, B, C0))
+    if rows is None:
+        out = np.empty((M, N), dtype=np.uint16)
+        lib().oracle_hgemm_ref(_p(A), _p(B), _p(C0), _p(out), M, N, K, alpha, beta, None, 0)
+    else:
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        out = np.empty((len(rows), N), dtype=np.uint16)
+        lib().oracle_hgemm_ref(_p(A), _p(B), _p(C0), _p(out), M, N, K, alpha, beta, _p(rows), len(rows))
+    return out
+
+
+def hgemm_exact_rows(A, B, C0, alpha: float, beta: float, rows=None):
+    """float64 value and componentwise denominator |alpha| sum |a||b| + |beta||c| of the selected
+    rows of alpha*A*B + beta*C0."""
+    M, K = A.shape
+    N = B.shape[1]
+    A, B, C0 = (np.ascontiguousarray(x, dtype=np.uint16) for x in (A, B, C0))
+    rows = np.arange(M, dtype=np.int64) if rows is None else np.ascontiguousarray(rows, dtype=np.int64)
+    ex = np.empty((len(rows), N))
+    den = np.empty((len(rows), N))
+    lib().oracle_hgemm_exact_rows(_p(A), _p(B), _p(C0), _p(ex), _p(den), M, N, K, alpha, beta, _p(rows), len(rows))
+    return ex, den
+
+
+def hgemm_ref_loop(A, B, C0, alpha_bits: int, beta_bits: int) -> np.ndarray | None:
+    """C from the reference's own compiled host check, or None if oracle/_ref is not built."""
+    R = ref_hgemm_lib()
+    if R is None:
+        return None
+    M, K = A.shape
+    N = B.shape[1]
+    C = np.ascontiguousarray(C0, dtype=np.uint16).copy()
+    A, B = (np.ascontiguousarray(x, dtype=np.uint16) for x in (A, B))
+    R.ref_hgemm_host(_p(A), _p(B), _p(C), M, N, K, alpha_bits, beta_bits)
+    return C
 
 
 def _p(a: np.ndarray) -> int:

@@ -546,3 +546,82 @@ double oracle_mlp_backward(const float* p, const float* x, const int* labels, in
   for (int i = 0; i < SEL_P; ++i) grads[i] /= batch;
   return loss / batch;
 }
+
+/* ------------------------------------------------------------------------------------------------
+ * FP16 HGEMM host check (routines/hgemm/hgemm.cu:135-149): float accumulation in k order,
+ * res = alpha*sum + beta*C in float (no contraction), one rounding to FP16.
+ * ---------------------------------------------------------------------------------------------- */
+float oracle_half_to_float(uint16_t h) {
+  const uint32_t sign = (uint32_t)(h & 0x8000u) << 16;
+  const uint32_t e = (h >> 10) & 0x1fu, m = h & 0x3ffu;
+  float f;
+  if (e == 0) {
+    f = ldexpf((float)m, -24); /* zero or subnormal: m * 2^-24, exact */
+    return sign ? -f : f;
+  }
+  uint32_t bits;
+  if (e == 31) bits = sign | 0x7f800000u | (m << 13); /* Inf, NaN (payload kept) */
+  else bits = sign | ((e + 112u) << 23) | (m << 13);
+  memcpy(&f, &bits, sizeof f);
+  return f;
+}
+
+uint16_t oracle_float_to_half(float f) {
+  uint32_t x;
+  memcpy(&x, &f, sizeof x);
+  const uint16_t sign = (uint16_t)((x >> 16) & 0x8000u);
+  const uint32_t ax = x & 0x7fffffffu;
+  if (ax > 0x7f800000u) return sign | 0x7e00u;  /* NaN */
+  if (ax >= 0x477ff000u) return sign | 0x7c00u; /* >= 65520 (Inf included) rounds to Inf */
+  if (ax >= 0x38800000u) {                      /* normal half: rebias, round mantissa to 10 bits */
+    uint32_t r = ax - (112u << 23);
+    r += 0xfffu + ((r >> 13) & 1u);
+    return sign | (uint16_t)(r >> 13);
+  }
+  /* subnormal half (or zero): round(|f| * 2^24) to an integer in [0, 1024] */
+  const int e = (int)(ax >> 23);
+  const int s = 126 - e; /* |f| * 2^24 = mant24 >> s */
+  if (e == 0 || s > 24) return sign;
+  const uint32_t mant = (ax & 0x7fffffu) | 0x800000u;
+  uint32_t q = mant >> s;
+  const uint32_t rem = mant & ((1u << s) - 1u), halfway = 1u << (s - 1);
+  if (rem > halfway || (rem == halfway && (q & 1u))) ++q;
+  return sign | (uint16_t)q;
+}
+
+void oracle_hgemm_ref(const uint16_t* A, const uint16_t* B, const uint16_t* C0, uint16_t* Cout, int64_t M,
+                      int64_t N, int64_t K, float alpha, float beta, const int64_t* rows, int64_t nrows) {
+  const int64_t nr = rows ? nrows : M;
+  for (int64_t i = 0; i < nr; ++i) {
+    const int64_t row = rows ? rows[i] : i;
+    for (int64_t col = 0; col < N; ++col) {
+      float sum = 0.0f;
+      for (int64_t k = 0; k < K; ++k)
+        sum += oracle_half_to_float(A[row * K + k]) * oracle_half_to_float(B[k * N + col]);
+      const float res = alpha * sum + beta * oracle_half_to_float(C0[row * N + col]);
+      Cout[i * N + col] = oracle_float_to_half(res);
+    }
+  }
+}
+
+void oracle_hgemm_exact_rows(const uint16_t* A, const uint16_t* B, const uint16_t* C0, double* Cexact, double* den,
+                             int64_t M, int64_t N, int64_t K, double alpha, double beta, const int64_t* rows,
+                             int64_t nrows) {
+  const int64_t nr = rows ? nrows : M;
+  for (int64_t i = 0; i < nr; ++i) {
+    const int64_t row = rows ? rows[i] : i;
+    for (int64_t col = 0; col < N; ++col) {
+      /* products of FP16 values are exact in double; the double sum's rounding error (about
+       * K * 2^-53 relative to den) is far below FP32 and FP16 resolution */
+      double s = 0.0, a = 0.0;
+      for (int64_t k = 0; k < K; ++k) {
+        const double p = (double)oracle_half_to_float(A[row * K + k]) * (double)oracle_half_to_float(B[k * N + col]);
+        s += p;
+        a += fabs(p);
+      }
+      const double c = (double)oracle_half_to_float(C0[row * N + col]);
+      Cexact[i * N + col] = alpha * s + beta * c;
+      den[i * N + col] = fabs(alpha) * a + fabs(beta) * fabs(c);
+    }
+  }
+}

@@ -14,13 +14,16 @@
  *     version of the same loop for componentwise error measurement.
  *   - oracle_fill_*: the seeded counter-based input generator that replaces the reference's
  *     cuRAND fill (dgemm.cpp:100-119) so host and device produce identical inputs.
+ *   - oracle_hgemm_ref: the reference's HGEMM host check, routines/hgemm/hgemm.cu:135-149 (FP16
+ *     inputs widened to float, float i-j-k loop, alpha*sum + beta*C in float, one rounding to
+ *     FP16), with its own FP16 <-> float conversions (oracle_half_to_float, oracle_float_to_half).
  *   - oracle_ozaki_*: a CPU restatement of this project's Ozaki INT8-slice DGEMM (no reference
  *     counterpart; the method follows Ozaki, Ogita, Oishi, Rump 2012 and Ootomo, Ozaki,
  *     Yokota 2024), bit-for-bit the same arithmetic as the CUDA path.
  *
- * Parity pin: oracle_dgemm_naive is checked bit-exactly against the reference's own
- * getReferenceResults (compiled from its sources into oracle/_ref by oracle/Makefile) and
- * against the golden fixtures in tests/golden/ that were produced by it.
+ * Parity pin: oracle_dgemm_naive and oracle_hgemm_ref are checked bit-exactly against the
+ * reference's own getReferenceResults loops (compiled from its sources into oracle/_ref by
+ * oracle/Makefile) and against the golden fixtures in tests/golden/ that were produced by them.
  */
 #ifndef LIBTHOM_ORACLE_H
 #define LIBTHOM_ORACLE_H
@@ -30,6 +33,20 @@
 #ifdef __cplusplus
 extern "C" {
 #endif
+
+/* ---- FP16 (IEEE binary16) ---- */
+float oracle_half_to_float(uint16_t h);
+/* Round to nearest, ties to even; overflow to +-Inf; NaN to the canonical quiet NaN 0x7e00. */
+uint16_t oracle_float_to_half(float f);
+/* routines/hgemm/hgemm.cu:135-149 on FP16 bit patterns: rows `rows[0..nrows)` (all M rows when rows
+ * is NULL) of C = alpha*A*B + beta*C0, written to Cout (nrows x N, or M x N). */
+void oracle_hgemm_ref(const uint16_t* A, const uint16_t* B, const uint16_t* C0, uint16_t* Cout, int64_t M,
+                      int64_t N, int64_t K, float alpha, float beta, const int64_t* rows, int64_t nrows);
+/* Same rows in float64 with the componentwise denominator |alpha| sum |a||b| + |beta||c| (for error
+ * bounds of FP32-accumulating kernels). */
+void oracle_hgemm_exact_rows(const uint16_t* A, const uint16_t* B, const uint16_t* C0, double* Cexact, double* den,
+                             int64_t M, int64_t N, int64_t K, double alpha, double beta, const int64_t* rows,
+                             int64_t nrows);
 
 /* ---- seeded generator ---- */
 uint64_t oracle_mix64(uint64_t z);

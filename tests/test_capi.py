@@ -20,7 +20,7 @@ def declared_functions() -> list[str]:
         text = re.sub(r"#[^\n]*", "", text)
         for m in re.finditer(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", text):
             name = m.group(1)
-            if name.startswith(("lt_", "dgemm_")) and name not in names:
+            if name.startswith(("lt_", "dgemm_", "hgemm_")) and name not in names:
                 names.append(name)
     return names
 
@@ -29,6 +29,8 @@ def test_header_declares_reference_contract():
     names = declared_functions()
     for impl in ["tc100", "cublas_tc", "ozaki_auto"] + [f"ozaki{s}" for s in range(3, 11)]:
         assert f"dgemm_{impl}" in names
+    # the hgemm routine's contract (routines/hgemm/hgemm.h:6-7)
+    assert "hgemm_tc100" in names and "hgemm_cublas" in names
 
 
 def test_library_exports_every_declared_symbol():
@@ -101,3 +103,18 @@ def test_dgemm_ex_rejects_bad_arguments():
     assert call(ldc=3) == lt.LT_ERR_INVALID_ARGUMENT
     assert call(M=-1) == lt.LT_ERR_INVALID_ARGUMENT
     assert L.lt_dgemm_ex(0, b"N", b"N", 4, 4, 4, 1.0, 12, 4, 8, 4, 0.0, 8, 4, 8, None) == lt.LT_ERR_UNALIGNED
+
+
+def test_hgemm_rejects_bad_arguments():
+    """Argument checks of lt_hgemm run before any device work (no GPU needed)."""
+    import libthom_b200 as lt
+
+    L = lt.lib()
+    p = ctypes.c_void_p(0x1000)
+    assert L.lt_hgemm(p, p, p, -1, 4, 4, 1.0, 0.0, None) == lt.LT_ERR_INVALID_ARGUMENT
+    assert L.lt_hgemm(None, p, p, 4, 4, 4, 1.0, 0.0, None) == lt.LT_ERR_INVALID_ARGUMENT
+    assert L.lt_hgemm(ctypes.c_void_p(0x1001), p, p, 4, 4, 4, 1.0, 0.0, None) == lt.LT_ERR_UNALIGNED
+    assert L.lt_hgemm_config(p, p, p, 4, 4, 4, 1.0, 0.0, 7, None) == lt.LT_ERR_NOT_FOUND
+    assert L.lt_hgemm_num_configs() == len(lt.hgemm_configs()) >= 2
+    # M == 0 or N == 0: nothing to do, no device touched
+    assert L.lt_hgemm(p, p, p, 0, 4, 4, 1.0, 0.0, None) == lt.LT_OK

@@ -10,7 +10,7 @@ import hashlib
 import numpy as np
 import pytest
 
-from conftest import U, fp64_bound
+from conftest import ROOT, U, fp64_bound
 
 
 def _cases(golden):
@@ -193,3 +193,55 @@ def test_mlp_backward_matches_finite_differences(oracle_mod):
         assert abs(fd - g[i]) <= 2e-3 * max(1.0, abs(g[i])), (i, fd, g[i])
     probs = oracle_mod.mlp_forward(params, x)
     assert np.allclose(probs.sum(axis=1), 1.0, atol=1e-6)
+
+
+# ---- FP16 HGEMM host check (routines/hgemm/hgemm.cu:135-149) -------------------------------------
+def test_half_conversions_exhaustive(oracle_mod):
+    """FP16 -> float over all 65536 patterns and float -> FP16 (ties to even, subnormals, overflow)
+    on every midpoint between neighbouring FP16 values, against numpy's IEEE conversions."""
+    L = oracle_mod.lib()
+    allh = np.arange(65536, dtype=np.uint16)
+    ref = allh.view(np.float16).astype(np.float32)
+    got = np.array([L.oracle_half_to_float(int(h)) for h in allh], dtype=np.float32)
+    fin = np.isfinite(ref)
+    assert np.array_equal(ref[fin].view(np.uint32), got[fin].view(np.uint32))
+    assert np.all(np.isnan(got[np.isnan(ref)]))
+    pos = np.arange(0x7c00, dtype=np.uint16).view(np.float16).astype(np.float64)
+    mids = ((pos[:-1] + pos[1:]) / 2).astype(np.float32)  # exact in float32
+    xs = np.concatenate([mids, -mids, np.float32([65519.0, 65520.0, 1e9, 2.0 ** -26, 2.0 ** -25, 0.0])])
+    with np.errstate(over="ignore"):
+        want = xs.astype(np.float16).view(np.uint16)
+    got = np.array([L.oracle_float_to_half(float(x)) for x in xs], dtype=np.uint16)
+    assert np.array_equal(want, got)
+
+
+def test_hgemm_ref_matches_golden_bit_exact(oracle_mod):
+    """The restated HGEMM check against the fixtures made by the reference's own compiled loop."""
+    g = np.load(ROOT / "tests" / "golden" / "hgemm_ref.npz")
+    for i in range(int(g["ncases"][0])):
+        alpha, beta = (float(x) for x in g[f"case{i}_scalars"])
+        C = oracle_mod.hgemm_ref(g[f"case{i}_A"], g[f"case{i}_B"], g[f"case{i}_C0"], alpha, beta)
+        assert np.array_equal(C, g[f"case{i}_C"]), i
+    # and a subset of rows gives the same rows
+    A, B, C0 = g["case2_A"], g["case2_B"], g["case2_C0"]
+    rows = np.array([0, 5, 23])
+    assert np.array_equal(oracle_mod.hgemm_ref(A, B, C0, 1.0, 0.0, rows=rows), g["case2_C"][rows])
+
+
+def test_hgemm_ref_matches_reference_build(oracle_mod):
+    """Where the reference sources are present: a fresh case through both loops, bit for bit."""
+    A, B, C0 = oracle_mod.make_half_problem(33, 47, 129, seed=99, lo=-3.0, hi=3.0)
+    ref = oracle_mod.hgemm_ref_loop(A, B, C0, int(oracle_mod.half_bits(-0.75)), int(oracle_mod.half_bits(2.0)))
+    if ref is None:
+        pytest.skip("oracle/_ref not built (reference sources absent)")
+    assert np.array_equal(oracle_mod.hgemm_ref(A, B, C0, -0.75, 2.0), ref)
+
+
+def test_hgemm_exact_rows_bounds_the_float_loop(oracle_mod):
+    """The float64 value and denominator used for GPU tolerances: the reference's float loop lies
+    within K u32 den + half an FP16 ulp of it."""
+    A, B, C0 = oracle_mod.make_half_problem(20, 30, 700, seed=3, lo=-1.0, hi=1.0)
+    C = oracle_mod.hgemm_ref(A, B, C0, 1.5, 0.5).view(np.float16).astype(np.float64)
+    ex, den = oracle_mod.hgemm_exact_rows(A, B, C0, 1.5, 0.5)
+    tol = (700 + 4) * 2.0 ** -24 * den + 2.0 ** -11 * np.abs(ex) + 2.0 ** -25
+    assert np.all(np.abs(C - ex) <= tol)
