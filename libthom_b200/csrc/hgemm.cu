@@ -7,27 +7,30 @@
 // MN-major SW128 for B), so there is no transpose pass.
 //
 // Kernel: persistent CTA pairs (clusters of two CTAs on two SMs). A pair computes a 256 x BN tile
-// of C (BN = 256 or 128) over 64-wide K blocks: each CTA stages its 128 rows of A and BN/2 columns
-// of B per block, rank 0's MMA warp issues four pair MMAs per block (M = 256, N = BN, K = 16), and
-// each CTA's TMEM receives its own 128 rows. Accumulators are double-buffered in TMEM (2 x BN
-// columns), so the epilogue of one tile overlaps the main loop of the next.
+// of C (BN = 512, 256 or 128) over 64-wide K blocks: each CTA stages its 128 rows of A and BN/2
+// columns of B per block, rank 0's MMA warp issues the pair MMAs (M = 256, N = min(BN, 256),
+// K = 16: four per block and column block), and each CTA's TMEM receives its own 128 rows. With
+// BN <= 256 the accumulators are double-buffered in TMEM, so the epilogue of one tile overlaps
+// the main loop of the next; BN = 512 fills TMEM with one tile and moves a quarter less operand
+// data per flop, which is what counts when the power cap sets the clock.
 //
-// Roles (192 threads per CTA):
+// Roles (320 threads per CTA):
 //   warp 0      TMA producer (one lane), both CTAs
 //   warp 1      rank 0: MMA issuer for the pair; rank 1: forwards each landed stage to rank 0
-//   warps 2..5  epilogue: TMEM -> registers, alpha*acc + beta*C in FP32, one rounding to FP16
+//   warps 2..9  epilogue: TMEM -> registers, alpha*acc + beta*C in FP32, one rounding to FP16
 // Barriers (per CTA):
 //   full[s]      rank 0: count 2 (own expect_tx arrival + the arrival relayed by rank 1);
 //                rank 1: count 1
 //   empty[s]     count 1: rank 0's MMA warp commits to both CTAs after the stage's MMAs
 //   acc_full[b]  count 1: committed to both CTAs after a tile's last MMA into buffer b
-//   acc_empty[b] rank 0 only, count 8: every epilogue warp of both CTAs arrives after reading b
+//   acc_empty[b] rank 0 only, count 16: every epilogue warp of both CTAs arrives after reading b
 // Every wait is bounded (LT_WAIT_TIMEOUT_NS); a wait that gives up records LT_ERR_DEVICE_TIMEOUT,
 // and the MMA warp lets its issued MMAs finish before TMEM is released.
 #include <cuda.h>
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 
 #include "../../include/libthom_hgemm.h"
@@ -41,24 +44,37 @@ namespace hgemm {
 constexpr int kBM = 128;                    // rows of C per CTA (256 per pair)
 constexpr int kBK = 64;                     // K per stage: one 128-byte swizzle row of FP16
 constexpr int kMmaK = 16;                   // K of one kind::f16 MMA
-constexpr int kThreads = 192;
-constexpr int kEpilogueWarps = 4;
+constexpr int kEpilogueWarps = 8;          // two per TMEM lane quarter, each half of the columns
+constexpr int kThreads = 64 + 32 * kEpilogueWarps;
 constexpr int kMaxSmem = 232448;            // 227 KB opt-in per CTA
 constexpr int kABytes = kBM * kBK * 2;      // 16 KB: 128 rows x 64 K
 constexpr int kBBlockBytes = kBK * 64 * 2;  // 8 KB: 64 K rows x 64 columns of B
 constexpr int kOverhead = 1024 + 256;       // alignment slack + barriers
+constexpr int kStoreRows = 32;              // one epilogue warp's TMEM lane quarter
+constexpr int kStoreCols = 32;              // 64 bytes of FP16: one 64-byte swizzle row
+constexpr int kStoreBytes = kStoreRows * kStoreCols * 2;          // 2 KB staging box
+constexpr int kStoreBoxes = 2;                                     // per epilogue warp, alternating
+constexpr int kEpilogueBytes = kEpilogueWarps * kStoreBoxes * kStoreBytes;  // 32 KB
 
+// BN = 128 or 256: one pair MMA of N = BN per K step, accumulators double-buffered in TMEM.
+// BN = 512: two pair MMAs of N = 256 per K step into two accumulators that fill TMEM (single
+// buffer); a quarter less A/B traffic per flop than BN = 256.
 template <int BN>
 struct Geo {
-  static constexpr int kHalfN = BN / 2;  // columns of B staged by each CTA
-  static constexpr int kBBlocks = kHalfN / 64;
+  static constexpr int kMmaN = BN < 256 ? BN : 256;  // N of one pair MMA
+  static constexpr int kMmas = BN / kMmaN;           // MMAs per K step (column blocks of the tile)
+  static constexpr int kHalfN = BN / 2;              // columns of B staged by each CTA
+  static constexpr int kBBlocks = kHalfN / 64;       // 64-column TMA boxes of B per CTA and stage
+  static constexpr int kBPerMma = kBBlocks / kMmas;  // of which one MMA reads
   static constexpr int kStageBytes = kABytes + kBBlocks * kBBlockBytes;
-  static constexpr int kFit = (kMaxSmem - kOverhead) / kStageBytes;
+  static constexpr int kFit = (kMaxSmem - kOverhead - kEpilogueBytes) / kStageBytes;
   static constexpr int kStages = kFit > 8 ? 8 : kFit;
-  static constexpr int kSmem = kStages * kStageBytes + kOverhead;
-  static constexpr int kTmemCols = 2 * BN;
+  static constexpr int kSmem = kStages * kStageBytes + kEpilogueBytes + kOverhead;
+  static constexpr int kAccBufs = BN <= 256 ? 2 : 1;  // TMEM holds 512 FP32 columns
+  static constexpr int kTmemCols = kAccBufs * BN;
   static_assert(kHalfN % 64 == 0 && kStageBytes % 1024 == 0, "tile geometry");
   static_assert(kStages >= 2, "shared-memory ring too small");
+  static_assert(kTmemCols <= 512 && (kTmemCols & (kTmemCols - 1)) == 0, "TMEM allocation");
 };
 
 struct Problem {
@@ -68,12 +84,14 @@ struct Problem {
   int tiles_m, tiles_n;  // 256-row pair blocks, BN-column blocks
   int kblocks;           // ceil(K / 64)
   int vec;               // rows of C are 16-byte aligned: 16-byte loads and stores
+  int group;             // pair-rows per raster group
+  int tma_store;         // beta == 0 and C 16-byte aligned: staged tiles written by TMA stores
 };
 
-// Pair tiles in groups of 8 pair-rows (2048 rows of C), column-major inside a group, so the CTAs
-// resident at one time share A row panels and B column panels in L2.
+// Pair tiles in groups of p.group pair-rows, column-major inside a group, so the CTAs resident at
+// one time share A row panels and B column panels in L2.
 __device__ __forceinline__ void tile_coords(const Problem& p, int64_t t, int bn, int* m0, int* n0) {
-  const int64_t G = 8;
+  const int64_t G = p.group;
   const int64_t group = t / (G * p.tiles_n), first_m = group * G;
   const int64_t gsize = (p.tiles_m - first_m) < G ? (p.tiles_m - first_m) : G;
   const int64_t in_group = t - group * G * p.tiles_n;
@@ -123,14 +141,49 @@ __device__ __forceinline__ void store_row_chunk(const Problem& p, int64_t row, i
   }
 }
 
+// One 32 x 32 box of the output through shared memory: each lane (one row) converts its 32
+// accumulators to FP16 pairs and writes them into the staging box in the 64-byte swizzled order of
+// the tensor map (16-byte chunk q of row r at r*64 + 16*(q ^ ((r >> 1) & 3)): four wavefronts per
+// 32-lane 16-byte store, the minimum), then one lane issues the TMA store. A warp alternates between
+// two boxes; a box is rewritten only after the store issued from it two chunks earlier has finished
+// reading it, so each store overlaps the next chunk's conversion.
+__device__ __forceinline__ void store_box_tma(const CUtensorMap* tmC, uint8_t* box, int lane, float alpha,
+                                              const uint32_t (&v)[32], int x, int y, const Problem& p) {
+  if (lane == 0) bulk_wait_group_read1();
+  __syncwarp();
+  uint8_t* row = box + lane * 64;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint32_t w[4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      float lo = __uint_as_float(v[q * 8 + 2 * h]), hi = __uint_as_float(v[q * 8 + 2 * h + 1]);
+      if (alpha != 1.f) {
+        lo = __fmul_rn(alpha, lo);
+        hi = __fmul_rn(alpha, hi);
+      }
+      const __half2 h2 = __floats2half2_rn(lo, hi);  // one cvt.rn.f16x2.f32
+      w[h] = *reinterpret_cast<const uint32_t*>(&h2);
+    }
+    *reinterpret_cast<uint4*>(row + 16 * (q ^ ((lane >> 1) & 3))) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+  fence_proxy_async_smem();  // the generic-proxy writes above become visible to the TMA engine
+  __syncwarp();
+  if (lane == 0 && x < p.N && y < p.M) {  // boxes wholly past the matrix edge are not issued
+    tma_store_2d(tmC, box, x, y);
+  }
+  if (lane == 0) bulk_commit_group();  // (an empty group when nothing was issued)
+}
+
 template <int BN>
 __global__ void __launch_bounds__(kThreads, 1)
-    hgemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Problem p,
-                      DeviceStatus* status) {
+    hgemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                      const __grid_constant__ CUtensorMap tmC, Problem p, DeviceStatus* status) {
   using G = Geo<BN>;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + G::kStages * G::kStageBytes);
+  uint8_t* staging = smem + G::kStages * G::kStageBytes;  // kEpilogueWarps boxes of kStoreBytes
+  uint64_t* full = reinterpret_cast<uint64_t*>(staging + kEpilogueBytes);
   uint64_t* empty = full + G::kStages;
   uint64_t* acc_full = empty + G::kStages;  // [2]
   uint64_t* acc_empty = acc_full + 2;       // [2]
@@ -160,6 +213,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 0 && lane == 0) {
     tma_prefetch_desc(&tmA);
     tma_prefetch_desc(&tmB);
+    if (p.tma_store) tma_prefetch_desc(&tmC);
   }
   if (warp == 1) {
     tmem_alloc_pair(tmem_slot, G::kTmemCols);
@@ -181,7 +235,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         int m0, n0;
         tile_coords(p, t, BN, &m0, &n0);
         const int arow = m0 + static_cast<int>(rank) * kBM;
-        const int bcol = n0 + static_cast<int>(rank) * G::kHalfN;
+        // column block h of the tile: this CTA stages columns h*kMmaN + rank*kMmaN/2 .. +kMmaN/2
+        const int bcol = n0 + static_cast<int>(rank) * (G::kMmaN / 2);
         for (int kb = 0; kb < kblocks; ++kb) {
           if (!mbar_wait_cluster(&empty[stage], phase ^ 1, abort_flag, status, 61)) { ok = false; break; }
           uint8_t* st = smem + stage * G::kStageBytes;
@@ -189,7 +244,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           tma_load_2d(st, &tmA, &full[stage], kb * kBK, arow);
 #pragma unroll
           for (int j = 0; j < G::kBBlocks; ++j)
-            tma_load_2d(st + kABytes + j * kBBlockBytes, &tmB, &full[stage], bcol + j * 64, kb * kBK);
+            tma_load_2d(st + kABytes + j * kBBlockBytes, &tmB, &full[stage],
+                        bcol + (j / G::kBPerMma) * G::kMmaN + (j % G::kBPerMma) * 64, kb * kBK);
           if (++stage == G::kStages) { stage = 0; phase ^= 1; }
         }
       }
@@ -215,18 +271,19 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp == 1) {
     // ------------------------------ rank 0: MMA issuer for the pair ------------------------------
     // Warp-convergent loop: waits are made warp-uniform with __all_sync, one elected lane issues.
-    constexpr uint32_t idesc = idesc_f16_f32(2 * kBM, BN, /*b_mn_major=*/true);
+    constexpr uint32_t idesc = idesc_f16_f32(2 * kBM, G::kMmaN, /*b_mn_major=*/true);
     const uint64_t a_desc0 = smem_desc_k_sw128(smem_u32(smem));
     const uint64_t b_desc0 = smem_desc_mn_sw128(smem_u32(smem + kABytes), kBBlockBytes, 1024);
     constexpr uint64_t kStageStep = static_cast<uint64_t>(G::kStageBytes >> 4);
     constexpr uint64_t kAStepK = static_cast<uint64_t>((kMmaK * 2) >> 4);    // 32 bytes along a row
     constexpr uint64_t kBStepK = static_cast<uint64_t>((kMmaK * 128) >> 4);  // 16 rows of 128 bytes
+    constexpr uint64_t kBStepN = static_cast<uint64_t>((G::kBPerMma * kBBlockBytes) >> 4);
     int stage = 0;
     uint32_t phase = 0;
     uint32_t iter = 0;
     bool ok = true;
     for (int64_t t = first; t < tiles && ok; t += stride, ++iter) {
-      const uint32_t buf = iter & 1, use = iter >> 1;
+      const uint32_t buf = iter % G::kAccBufs, use = iter / G::kAccBufs;
       if (!__all_sync(0xffffffffu, mbar_wait_cluster(&acc_empty[buf], (use & 1) ^ 1, abort_flag, status, 63))) {
         ok = false;
         break;
@@ -244,7 +301,10 @@ __global__ void __launch_bounds__(kThreads, 1)
           const uint64_t b0 = b_desc0 + static_cast<uint64_t>(stage) * kStageStep;
 #pragma unroll
           for (int k = 0; k < kBK / kMmaK; ++k)
-            mma_f16_pair(d_tmem, a0 + k * kAStepK, b0 + k * kBStepK, idesc, (kb > 0 || k > 0) ? 1u : 0u);
+#pragma unroll
+            for (int h = 0; h < G::kMmas; ++h)
+              mma_f16_pair(d_tmem + h * G::kMmaN, a0 + k * kAStepK, b0 + h * kBStepN + k * kBStepK, idesc,
+                           (kb > 0 || k > 0) ? 1u : 0u);
           mma_commit_pair(cluster_addr(&empty[stage], 0));
           mma_commit_pair(cluster_addr(&empty[stage], 1));
         }
@@ -267,33 +327,58 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     __syncwarp();
   } else {
-    // --------------------------------- epilogue (4 warps per CTA) ---------------------------------
-    const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31 are visible to this warp
+    // --------------------------------- epilogue (8 warps per CTA) ---------------------------------
+    const int quarter = warp & 3;         // TMEM lanes 32*quarter .. +31 are visible to this warp
+    const int colhalf = (warp - 2) >> 2;  // columns colhalf*BN/2 .. +BN/2 of the tile
     const int row_in_tile = quarter * 32 + lane;
     const uint32_t acc_empty_r0[2] = {cluster_addr(&acc_empty[0], 0), cluster_addr(&acc_empty[1], 0)};
+    constexpr int kChunks = BN / 64;  // 32-column chunks per warp
     uint32_t iter = 0;
     for (int64_t t = first; t < tiles; t += stride, ++iter) {
-      const uint32_t buf = iter & 1, use = iter >> 1;
+      const uint32_t buf = iter % G::kAccBufs, use = iter / G::kAccBufs;
       int m0, n0;
       tile_coords(p, t, BN, &m0, &n0);
       if (!mbar_wait_cluster(&acc_full[buf], use & 1, abort_flag, status, 65)) break;
       tc_fence_after();
       const int64_t row = static_cast<int64_t>(m0) + static_cast<int64_t>(rank) * kBM + row_in_tile;
-      const uint32_t lane_base = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + buf * BN;
+      const int col_base = colhalf * (BN / 2);
+      const uint32_t lane_base =
+          tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + buf * BN + static_cast<uint32_t>(col_base);
+      if (p.tma_store) {
+        // beta == 0: 32-column boxes staged in shared memory and written by TMA stores (clipped at
+        // the matrix edges by the tensor map).
+        uint8_t* boxes = staging + (warp - 2) * kStoreBoxes * kStoreBytes;
+        const int y = m0 + static_cast<int>(rank) * kBM + quarter * 32;
 #pragma unroll 1
-      for (int c = 0; c < BN / 32; ++c) {
-        uint32_t v[32];
-        tmem_ld_32x32b_x32(lane_base + static_cast<uint32_t>(c * 32), v);
-        tmem_ld_wait();
-        if (c == BN / 32 - 1) {
-          // The whole accumulator is in registers: hand the buffer back before the last stores.
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive_cluster(acc_empty_r0[buf]);
+        for (int c = 0; c < kChunks; ++c) {
+          uint32_t v[32];
+          tmem_ld_32x32b_x32(lane_base + static_cast<uint32_t>(c * 32), v);
+          tmem_ld_wait();
+          if (c == kChunks - 1) {
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(acc_empty_r0[buf]);
+          }
+          store_box_tma(&tmC, boxes + (c & 1) * kStoreBytes, lane, p.alpha, v, n0 + col_base + c * 32, y, p);
         }
-        if (row < p.M) store_row_chunk(p, row, static_cast<int64_t>(n0) + c * 32, v);
+      } else {
+#pragma unroll 1
+        for (int c = 0; c < kChunks; ++c) {
+          uint32_t v[32];
+          tmem_ld_32x32b_x32(lane_base + static_cast<uint32_t>(c * 32), v);
+          tmem_ld_wait();
+          if (c == kChunks - 1) {
+            // The whole accumulator is in registers: hand the buffer back before the last stores.
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(acc_empty_r0[buf]);
+          }
+          if (row < p.M) store_row_chunk(p, row, static_cast<int64_t>(n0) + col_base + c * 32, v);
+        }
       }
     }
+    if (p.tma_store && lane == 0) bulk_wait_group0();  // the last stores have been performed
+    __syncwarp();
   }
 
   tc_fence_before();
@@ -325,28 +410,33 @@ __global__ void pack_kernel(const uint16_t* src, int64_t rows, int64_t cols, int
   }
 }
 
-constexpr int kNumConfigs = 2;
-constexpr int kConfigBN[kNumConfigs] = {256, 128};
-const char* const kConfigNames[kNumConfigs] = {"pair_256x256", "pair_256x128"};
+constexpr int kNumConfigs = 3;
+constexpr int kConfigBN[kNumConfigs] = {512, 256, 128};
+const char* const kConfigNames[kNumConfigs] = {"pair_256x512", "pair_256x256", "pair_256x128"};
 
 int num_configs() { return kNumConfigs; }
 const char* config_name(int c) { return (c >= 0 && c < kNumConfigs) ? kConfigNames[c] : nullptr; }
 
-// Wave-count cost model: the 256-wide tile does twice the work per tile with the same operand
-// traffic per flop halved on B; the 128-wide tile wins when it fills the SM pairs markedly better.
+// Wave-count cost model: waves x tile width / relative efficiency of the tile shape (wider tiles
+// move less operand data per flop; 512 loses the epilogue overlap).
 int default_config(int64_t M, int64_t N, int sm_count) {
   const int64_t clusters = std::max(1, sm_count / 2);
-  auto cost = [&](int bn, double eff) {
+  int best = 0;
+  double best_cost = 0.0;
+  const double eff[kNumConfigs] = {1.0, 0.97, 0.85};
+  for (int c = 0; c < kNumConfigs; ++c) {
+    const int bn = kConfigBN[c];
     const int64_t tiles = ((M + 255) / 256) * ((N + bn - 1) / bn);
     const int64_t waves = (tiles + clusters - 1) / clusters;
-    return static_cast<double>(waves) * bn / eff;
-  };
-  return cost(256, 1.0) <= cost(128, 0.9) ? 0 : 1;
+    const double cost = static_cast<double>(waves) * bn / eff[c];
+    if (c == 0 || cost < best_cost) { best = c; best_cost = cost; }
+  }
+  return best;
 }
 
 template <int BN>
-int launch(const CUtensorMap& tmA, const CUtensorMap& tmB, const Problem& p, DeviceContext* ctx,
-           cudaStream_t stream) {
+int launch(const CUtensorMap& tmA, const CUtensorMap& tmB, const CUtensorMap& tmC, const Problem& p,
+           DeviceContext* ctx, cudaStream_t stream) {
   using G = Geo<BN>;
   static std::once_flag once[64];
   static cudaError_t attr_err[64];
@@ -380,8 +470,18 @@ int launch(const CUtensorMap& tmA, const CUtensorMap& tmB, const Problem& p, Dev
   cudaLaunchConfig_t cfg;
   cudaLaunchAttribute attr;
   config(&cfg, &attr, static_cast<unsigned>(2 * clusters));
-  LT_CUDA_TRY(cudaLaunchKernelEx(&cfg, hgemm_pair_kernel<BN>, tmA, tmB, p, ctx->status));
+  LT_CUDA_TRY(cudaLaunchKernelEx(&cfg, hgemm_pair_kernel<BN>, tmA, tmB, tmC, p, ctx->status));
   return LT_OK;
+}
+
+// Pair-rows per raster group: 8 (2048 rows of C), or LIBTHOM_HGEMM_GROUP (1..64).
+int raster_group() {
+  static const int g = [] {
+    const char* e = getenv("LIBTHOM_HGEMM_GROUP");
+    const int v = e != nullptr ? atoi(e) : 0;
+    return (v >= 1 && v <= 64) ? v : 8;
+  }();
+  return g;
 }
 
 int check_args(const uint16_t* A, const uint16_t* B, uint16_t* C, int64_t M, int64_t N, int64_t K) {
@@ -456,8 +556,16 @@ int run(const uint16_t* A, const uint16_t* B, uint16_t* C, int64_t M, int64_t N,
   p.tiles_n = static_cast<int>((N + bn - 1) / bn);
   p.kblocks = static_cast<int>((K + kBK - 1) / kBK);
   p.vec = ((reinterpret_cast<uintptr_t>(C) & 15) == 0 && (N % 8) == 0) ? 1 : 0;
-  if (bn == 256) LT_TRY((launch<256>(tmA, tmB, p, ctx, stream)));
-  else LT_TRY((launch<128>(tmA, tmB, p, ctx, stream)));
+  p.group = raster_group();
+  p.tma_store = (p.vec && beta == 0.f) ? 1 : 0;
+  CUtensorMap tmC = tmA;  // not read unless p.tma_store
+  if (p.tma_store)
+    LT_TRY(make_tmap_2d(&tmC, C, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, static_cast<uint64_t>(M),
+                        static_cast<uint64_t>(N), static_cast<uint64_t>(N) * 2, kStoreRows, kStoreCols,
+                        CU_TENSOR_MAP_SWIZZLE_64B));
+  if (bn == 512) LT_TRY((launch<512>(tmA, tmB, tmC, p, ctx, stream)));
+  else if (bn == 256) LT_TRY((launch<256>(tmA, tmB, tmC, p, ctx, stream)));
+  else LT_TRY((launch<128>(tmA, tmB, tmC, p, ctx, stream)));
   return ok();
 }
 

@@ -109,6 +109,21 @@ __device__ __forceinline__ void tma_load_3d(void* smem_dst, const void* desc, ui
       ::"r"(smem_u32(smem_dst)), "l"(reinterpret_cast<uint64_t>(desc)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
 }
+// Tiled store shared -> global of one box at (x, y) >= 0 (rows and columns past the tensor's extent
+// are not written), tracked in this thread's bulk async-group.
+__device__ __forceinline__ void tma_store_2d(const void* desc, const void* smem_src, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];"
+               ::"l"(reinterpret_cast<uint64_t>(desc)), "r"(x), "r"(y), "r"(smem_u32(smem_src))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit_group() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Waits until at most the most recent of this thread's committed bulk groups still reads its
+// shared-memory source.
+__device__ __forceinline__ void bulk_wait_group_read1() {
+  asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+}
+// Waits until all of this thread's committed bulk groups have completed (writes performed).
+__device__ __forceinline__ void bulk_wait_group0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 // ---------------------------------------------------------------------------------------------
 // cp.async (Ampere-style LDGSTS) with zero fill, completion tracked on an mbarrier.

@@ -135,7 +135,7 @@ EncodeTiledFn encode_tiled() {
 }
 
 int make_tmap_2d(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, int elem_bytes, uint64_t rows,
-                 uint64_t cols, uint64_t pitch_bytes, uint32_t box_rows, uint32_t box_cols) {
+                 uint64_t cols, uint64_t pitch_bytes, uint32_t box_rows, uint32_t box_cols, CUtensorMapSwizzle swizzle) {
   EncodeTiledFn enc = encode_tiled();
   if (enc == nullptr) return LT_ERR_UNSUPPORTED;
   if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (pitch_bytes & 15) != 0)
@@ -146,7 +146,7 @@ int make_tmap_2d(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, 
   cuuint32_t estr[2] = {1, 1};
   (void)elem_bytes;
   CUresult r = enc(map, dtype, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                   swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return set_error(LT_ERR_CUDA, "cuTensorMapEncodeTiled (2d) failed: %d", static_cast<int>(r));
   return LT_OK;
 }

@@ -51,9 +51,10 @@ using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t
 EncodeTiledFn encode_tiled();
 
 // 2-D row-major tensor map: rows x cols elements of `elem_bytes`, row pitch `pitch_bytes`,
-// box {box_cols, box_rows}, 128-byte swizzle, zero fill out of bounds.
+// box {box_cols, box_rows}, 128-byte swizzle unless given, zero fill out of bounds.
 int make_tmap_2d(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, int elem_bytes, uint64_t rows,
-                 uint64_t cols, uint64_t pitch_bytes, uint32_t box_rows, uint32_t box_cols);
+                 uint64_t cols, uint64_t pitch_bytes, uint32_t box_rows, uint32_t box_cols,
+                 CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_128B);
 // 3-D: [planes][rows][cols] with plane pitch and row pitch in bytes, box {box_cols, box_rows, 1}.
 int make_tmap_3d(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, int elem_bytes, uint64_t planes,
                  uint64_t rows, uint64_t cols, uint64_t pitch_bytes, uint64_t plane_pitch_bytes, uint32_t box_rows,

@@ -10,11 +10,12 @@ static const std::unordered_map<std::string, RunMode> runModeMap = {
 
 using RoutineHandler = void (*)(RunMode, int, char**);
 
-// Only the DGEMM routines exist in this build: `dgemm` (the reference's routine) and `dgemmb`
+// The GEMM routines of this build: `dgemm` and `hgemm` (the reference's routines) and `dgemmb`
 // (grouped/batched DGEMM, one persistent launch for many uneven problems).
 static const std::unordered_map<std::string, RoutineHandler> routinesMap = {
     {"dgemm", dgemm_handler},
     {"dgemmb", dgemmb_handler},
+    {"hgemm", hgemm_handler},
 };
 
 int main(int argc, char* argv[]) {

@@ -20,6 +20,7 @@ enum RunMode { TEST, BENCH, TUNE };
 
 void dgemm_handler(RunMode runMode, int argc, char* argv[]);
 void dgemmb_handler(RunMode runMode, int argc, char* argv[]);
+void hgemm_handler(RunMode runMode, int argc, char* argv[]);
 
 
 // Reference behaviour kept: a CUDA error is reported as a warning and the run continues

@@ -82,20 +82,23 @@ def test_every_config(cuda, oracle_mod):
 
     A, B, C0 = oracle_mod.make_half_problem(300, 520, 200, seed=7, lo=-1.0, hi=1.0)
     for cfg, name in enumerate(lt.hgemm_configs()):
-        C = run_tc(cuda, A, B, C0, 1.25, -0.5, config=cfg)
-        assert check_against_exact(oracle_mod, C, A, B, C0, 1.25, -0.5) <= 1.0, name
+        for beta in (-0.5, 0.0):
+            C = run_tc(cuda, A, B, C0, 1.25, beta, config=cfg)
+            assert check_against_exact(oracle_mod, C, A, B, C0, 1.25, beta) <= 1.0, name
 
 
+@pytest.mark.parametrize("beta", [0.0, 2.0])
 @pytest.mark.parametrize("M,N,K,offset", [(1, 1, 1, 0), (3, 5, 7, 0), (100, 64, 64, 0), (129, 65, 33, 0),
-                                          (257, 300, 1000, 0), (520, 264, 72, 0), (256, 256, 64, 1),
-                                          (200, 136, 130, 1)])
-def test_ragged_and_unaligned(cuda, oracle_mod, M, N, K, offset):
-    """Any M, N, K: partial tiles in every dimension (zero-filled TMA boxes, masked stores), row
-    pitches that are not multiples of 8 elements and 2-byte aligned pointers (packed operand copies,
-    scalar epilogue)."""
+                                          (257, 300, 1000, 0), (520, 264, 72, 0), (136, 1032, 40, 0),
+                                          (256, 256, 64, 1), (200, 136, 130, 1)])
+def test_ragged_and_unaligned(cuda, oracle_mod, M, N, K, offset, beta):
+    """Any M, N, K: partial tiles in every dimension (zero-filled TMA boxes, clipped TMA stores or
+    masked stores), row pitches that are not multiples of 8 elements and 2-byte aligned pointers
+    (packed operand copies, scalar epilogue). beta == 0 with an aligned C takes the staged TMA-store
+    epilogue, beta != 0 the direct one."""
     A, B, C0 = oracle_mod.make_half_problem(M, N, K, seed=M + N + K, lo=-1.0, hi=1.0)
-    C = run_tc(cuda, A, B, C0, 0.5, 2.0, offset=offset)
-    assert check_against_exact(oracle_mod, C, A, B, C0, 0.5, 2.0) <= 1.0
+    C = run_tc(cuda, A, B, C0, 0.5, beta, offset=offset)
+    assert check_against_exact(oracle_mod, C, A, B, C0, 0.5, beta) <= 1.0
 
 
 def test_many_tiles_per_pair(cuda, oracle_mod):
@@ -103,10 +106,13 @@ def test_many_tiles_per_pair(cuda, oracle_mod):
     buffers and phases; checked on sampled rows of every 256-row block."""
     M, N, K = 4096, 4096, 192
     A, B, C0 = oracle_mod.make_half_problem(M, N, K, seed=11, lo=-1.0, hi=1.0)
+    import libthom_b200 as lt
+
     rows = np.concatenate([np.arange(b, M, 256) for b in (0, 77, 128, 255)])
-    for cfg in (0, 1):
-        C = run_tc(cuda, A, B, C0, 1.0, 1.0, config=cfg)
-        assert check_against_exact(oracle_mod, C, A, B, C0, 1.0, 1.0, rows=rows) <= 1.0
+    for cfg in range(len(lt.hgemm_configs())):
+        for beta in (0.0, 1.0):
+            C = run_tc(cuda, A, B, C0, 1.0, beta, config=cfg)
+            assert check_against_exact(oracle_mod, C, A, B, C0, 1.0, beta, rows=rows) <= 1.0
 
 
 def test_k_zero_alpha_zero_beta_zero(cuda, oracle_mod):
