@@ -563,6 +563,246 @@ def run_sweep(args) -> None:
                           "oracle": "compensated Dot2", "results": res}), flush=True)
 
 
+# ------------------------------------------------------------------------------------------------
+# hgemm routine (routines/hgemm/hgemm.cu): FP16 GEMM on the tcgen05 kind::f16 kernel
+# ------------------------------------------------------------------------------------------------
+HGEMM_METRIC = "HGEMM TFLOP/s (FP16 inputs, FP32 accumulation, FP16 output), 8192^3 on 1 B200"
+
+
+def _hgemm_inputs_host(n: int, rows: int):
+    """Rows 0..rows-1 of A and all of B of the hgemm workload, uniform [0, 1) rounded to FP16 (the
+    reference runner's inputs, routines/hgemm/hgemm.cu:107-121), from numpy's seeded generator."""
+    import numpy as np
+
+    rng = np.random.default_rng(SEED)
+    B = rng.random((n, n), dtype=np.float32).astype(np.float16).view(np.uint16)
+    A = rng.random((rows, n), dtype=np.float32).astype(np.float16).view(np.uint16)
+    return np.ascontiguousarray(A), np.ascontiguousarray(B)
+
+
+def _hgemm_ref_rows(args_tuple):
+    """One worker's share of the reference's HGEMM host loop (built into oracle/_ref), or of its
+    restatement when that build is absent: rows of C = A B for A rows x B."""
+    A, B, n = args_tuple
+    import numpy as np
+    import oracle
+
+    C = np.zeros((A.shape[0], n), dtype=np.uint16)
+    R = oracle.ref_hgemm_lib()
+    t0 = time.perf_counter()
+    if R is not None:
+        R.ref_hgemm_host(A.ctypes.data, B.ctypes.data, C.ctypes.data, A.shape[0], n, n, 0x3C00, 0x0000)
+        kind = "reference"
+    else:
+        oracle.lib().oracle_hgemm_ref(A.ctypes.data, B.ctypes.data, C.ctypes.data, C.ctypes.data, A.shape[0], n, n,
+                                      1.0, 0.0, None, 0)
+        kind = "port"
+    return time.perf_counter() - t0, kind
+
+
+def hgemm_cpu_rows(n: int, rows: int, workers: int) -> dict:
+    """Times the reference HGEMM host loop on `rows` rows of the n^3 problem with `workers`
+    processes (the loop keeps its operands in process-wide statics, so one process per worker)."""
+    import multiprocessing as mp
+
+    A, B = _hgemm_inputs_host(n, rows)
+    per = max(1, rows // workers)
+    chunks = [(A[i:i + per], B, n) for i in range(0, rows, per)]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(len(chunks)) as pool:
+        res = pool.map(_hgemm_ref_rows, chunks)
+    wall = time.perf_counter() - t0
+    loop = max(r[0] for r in res)
+    flop = 2.0 * rows * n * n
+    return {"value": flop / loop / 1e12, "unit": UNIT, "cores": len(chunks), "kind": res[0][1],
+            "seconds": loop, "wall_seconds": wall, "flop": flop}
+
+
+def run_hgemm(args) -> None:
+    import torch
+
+    import libthom_b200 as lt
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    n = args.size
+    M = N = K = n
+    flop = 2.0 * M * N * K
+    g = torch.Generator(device=dev).manual_seed(SEED + rank)
+    A = torch.rand(M, K, device=dev, generator=g).half()
+    B = torch.rand(K, N, device=dev, generator=g).half()
+    C = torch.zeros(M, N, dtype=torch.float16, device=dev)
+    R = torch.zeros_like(C)
+    cfg = lt.lib().lt_hgemm_default_config(M, N, K)
+
+    # ---- agreement with cuBLAS (FP32 accumulation) under the reference's acceptance test ----
+    lt.hgemm_tc(A, B, C, M, N, K, 1.0, 0.0, stream)
+    lt.hgemm_cublas(A, B, R, M, N, K, 1.0, 0.0, compute_f32=True, stream=stream)
+    torch.cuda.synchronize()
+    c, r = C.float(), R.float()
+    diff = (c - r).abs()
+    rel = diff / r.abs().clamp_min(1e-3)
+    differ = int(((rel > 1e-2) & (diff > 1e-3)).sum().item())
+    max_rel = float(rel.max().item())
+    bitwise = float((C.view(torch.int16) == R.view(torch.int16)).float().mean().item())
+    del c, r, diff, rel
+    lt.device_status()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- headline: inputs resident in HBM (A, B, C: 384 MiB in all, above the 126 MB L2) ----
+    for _ in range(args.warmup):
+        lt.hgemm_tc(A, B, C, M, N, K, 1.0, 0.0, stream)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    with ClockSampler(local) as clk:
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for i in range(args.steps):
+            ev[i][0].record(stream)
+            lt.hgemm_tc(A, B, C, M, N, K, 1.0, 0.0, stream)
+            ev[i][1].record(stream)
+        stop.record(stream)
+        barrier()
+    total_ms = reduce_max(start.elapsed_time(stop), dist, dev)
+    kern_ms = statistics.mean(a.elapsed_time(b) for a, b in ev)
+    lt.device_status()
+    ms_step = total_ms / args.steps
+    value = world * flop / (ms_step * 1e-3) / 1e12
+
+    def time_loop(fn) -> float:
+        for _ in range(args.warmup):
+            fn()
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            fn()
+        b.record(stream)
+        barrier()
+        return reduce_max(a.elapsed_time(b), dist, dev) / args.steps
+
+    cublas32_ms = time_loop(lambda: lt.hgemm_cublas(A, B, R, M, N, K, 1.0, 0.0, True, stream))
+    cublas16_ms = time_loop(lambda: lt.hgemm_cublas(A, B, R, M, N, K, 1.0, 0.0, False, stream))
+
+    # ---- end to end: pinned host A and B copied in, the product, C copied out, every step ----
+    Ah = torch.empty(M, K, dtype=torch.float16, pin_memory=True)
+    Bh = torch.empty(K, N, dtype=torch.float16, pin_memory=True)
+    Ch = torch.empty(M, N, dtype=torch.float16, pin_memory=True)
+    Ah.copy_(A)
+    Bh.copy_(B)
+    e2e_steps = max(1, min(args.steps, 5))
+
+    def e2e_step():
+        A.copy_(Ah, non_blocking=True)
+        B.copy_(Bh, non_blocking=True)
+        lt.hgemm_tc(A, B, C, M, N, K, 1.0, 0.0, stream)
+        Ch.copy_(C, non_blocking=True)
+
+    e2e_step()
+    barrier()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    b.record(stream)
+    barrier()
+    e2e_ms = reduce_max(a.elapsed_time(b), dist, dev) / e2e_steps
+    del Ah, Bh, Ch
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    peaks = measured_peaks()
+    burst, sustained = peaks.get("bf16_tflops"), peaks.get("bf16_tflops_sustained")
+    achieved = flop / (kern_ms * 1e-3) / 1e12
+    peak = burst if burst else 1590.0
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        rows = max(1, args.cpu_rows // 64)
+        cb = hgemm_cpu_rows(n, rows, 1)
+        cpu = {"value": cb["value"], "unit": UNIT, "cores": cb["cores"], "kind": cb["kind"],
+               "sample": f"the reference's HGEMM host loop (routines/hgemm/hgemm.cu:135-149) on {rows} of {M} "
+                         f"rows of the {n}^3 problem ({cb['flop']:.3g} flop, {cb['seconds']:.2f} s, 1 thread)"}
+    line = {
+        "metric": HGEMM_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f16 (f32 accumulate)", "data": "synthetic (uniform [0,1) rounded to FP16)",
+        "config": {"workload": f"hgemm {n}^3 alpha=1 beta=0 (the reference runner's setting), config "
+                               f"{lt.hgemm_configs()[cfg]}", "M": M, "N": N, "K": K,
+                   "l2": "inputs larger than L2 in total (A, B, C 128 MiB each), no flush",
+                   "parallelism": f"replicas x{world}"},
+        "accuracy": {"vs_cublas_f32": {"entries_failing_reference_test": differ, "max_rel_diff": max_rel,
+                                       "bitwise_equal_fraction": bitwise}},
+        "cublas_f32_accumulate": {"value": world * flop / (cublas32_ms * 1e-3) / 1e12, "ms_per_step": cublas32_ms},
+        "cublas_f16_accumulate": {"value": world * flop / (cublas16_ms * 1e-3) / 1e12, "ms_per_step": cublas16_ms,
+                                  "note": "the reference's own baseline call (hgemm_cublas.cu:10-22)"},
+        "roofline": {"bound": "tensor", "kernel": "hgemm_pair_kernel", "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak,
+                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS bf16 GEMM burst; FP16 runs at "
+                                    "the bf16 rate)" if burst else "fallback 1590 TFLOP/s",
+                     "peak_sustained": sustained, "frac_of_sustained": achieved / sustained if sustained else None,
+                     "traffic": profile_traffic("hgemm_pair_8192") if n == 8192 else None,
+                     "algorithmic": f"2MNK = {flop:.4g} flop per launch"},
+        "e2e": {"value": world * flop / (e2e_ms * 1e-3) / 1e12, "unit": UNIT,
+                "h2d_bytes_per_step": 2 * (M * K + K * N), "d2h_bytes_per_step": 2 * M * N, "ms_per_step": e2e_ms,
+                "path": "pinned host A, B copied in, lt_hgemm, C copied out, on one stream"},
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "gpu_launches": args.steps,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_reference_hgemm(args) -> None:
+    """The reference's own CPU implementation of the hgemm check loop (routines/hgemm/hgemm.cu:
+    135-149, built from its sources into oracle/_ref; the restatement if absent), one process per
+    host core, each on its own rows of the 8192^3 problem."""
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return
+    n = args.size
+    cores = len(os.sched_getaffinity(0))
+    times, kind = [], "reference"
+    for step in range(args.warmup + args.steps):
+        cb = hgemm_cpu_rows(n, cores, cores)
+        kind = cb["kind"]
+        if step >= args.warmup:
+            times.append(cb["seconds"])
+    flop = 2.0 * cores * n * n
+    ms = 1e3 * statistics.mean(times)
+    value = flop / (ms * 1e-3) / 1e12
+    sample = f"{cores} rows of the {n}^3 problem per step ({flop:.3g} flop), one process per core"
+    line = {"metric": HGEMM_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f16 (f32 accumulate)", "data": "synthetic (uniform [0,1) rounded to FP16)",
+            "config": {"workload": f"hgemm {n}^3 alpha=1 beta=0", "M": n, "N": n, "K": n,
+                       "sample_rows_per_step": cores},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -578,11 +818,15 @@ def main() -> None:
     ap.add_argument("--check-rows", type=int, default=16)
     ap.add_argument("--cpu-rows", type=int, default=1024)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--routine", choices=["dgemm", "hgemm"], default="dgemm",
+                    help="dgemm: the headline (default); hgemm: the FP16 routine on its tcgen05 kernel")
     ap.add_argument("--sweep", action="store_true",
                     help="print the phi x slice-count table (error and TFLOP/s of every form) instead")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps, reported as run
-    if args.sweep:
+    if args.routine == "hgemm":
+        run_reference_hgemm(args) if args.impl == "reference" else run_hgemm(args)
+    elif args.sweep:
         run_sweep(args)
     elif args.impl == "reference":
         run_reference(args)
