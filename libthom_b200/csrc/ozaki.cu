@@ -418,7 +418,8 @@ struct OzProblem {
   const unsigned long long* amax_b;
   int64_t M, N, nkc, rba, rbb;
   double alpha, beta;
-  int64_t ldc;  // row stride of C (>= N)
+  int64_t ldc;     // row stride of C (>= N)
+  int group = 8;   // pair-rows per raster group of the CTA-pair kernel
 };
 
 // One output tile of one problem.
@@ -798,12 +799,12 @@ struct PairGeo {
   __host__ __device__ static constexpr int cps(int b) { return S / band_of(S, b).nsl; }
 };
 
-// Pair tiles in groups of 8 pair-rows (2048 rows of C), column-major inside a group.
+// Pair tiles in groups of G pair-rows, column-major inside a group.
 struct OzPairSource {
   int64_t tiles_m, tiles_n;  // 256-row pair blocks, 128-column blocks
+  int64_t G;                 // pair-rows per raster group
   __device__ int64_t count() const { return tiles_m * tiles_n; }
   __device__ void get(int64_t t, int* m0, int* n0) const {
-    const int64_t G = 8;
     int64_t group = t / (G * tiles_n), first_m = group * G;
     int64_t gsize = (tiles_m - first_m) < G ? (tiles_m - first_m) : G;
     int64_t in_group = t - group * G * tiles_n;
@@ -854,7 +855,7 @@ __device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatu
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t rank = cluster_ctarank();
-  const OzPairSource src{(pr.rba + 1) / 2, pr.rbb};
+  const OzPairSource src{(pr.rba + 1) / 2, pr.rbb, pr.group};
   const int64_t tiles = src.count();
   const int64_t first = cluster_id_x(), stride = num_clusters_x();
   const int64_t nkc = pr.nkc;
@@ -1124,10 +1125,22 @@ int launch_gemm_s(const Src& src, int64_t ntiles, DeviceContext* ctx, cudaStream
   return LT_OK;
 }
 
+// Pair-rows per raster group of the CTA-pair kernel: 8, or LIBTHOM_OZAKI_GROUP (1..64).
+int pair_group() {
+  static const int g = [] {
+    const char* e = getenv("LIBTHOM_OZAKI_GROUP");
+    const int v = e != nullptr ? atoi(e) : 0;
+    return (v >= 1 && v <= 64) ? v : 8;
+  }();
+  return g;
+}
+
 // Launches the CTA-pair product kernel for S slices. *launched = false (nothing launched) when no
 // pair of CTAs with this kernel's shared memory fits on the device.
 template <int S>
-int launch_pair_s(const OzProblem& pr, DeviceContext* ctx, cudaStream_t stream, bool* launched) {
+int launch_pair_s(const OzProblem& problem, DeviceContext* ctx, cudaStream_t stream, bool* launched) {
+  OzProblem pr = problem;
+  pr.group = pair_group();
   using G = PairGeo<S>;
   static std::once_flag once[64];
   static cudaError_t attr_err[64];
