@@ -7,18 +7,20 @@
 //   1. amax pass (HBM-bound): per row of A and per column of B, the largest |x| as IEEE bits
 //      (NaN/Inf order above every finite value, so one max finds both). sigma_i / tau_j are the
 //      frexp exponents of those maxima, so |A[i,k] 2^-sigma_i| < 1.
-//   2. split pass (HBM-bound): x = a 2^-sigma; for p = 1..s: y = 128 x, q_p = trunc(y), x = y - q_p.
-//      Every step is exact in FP64; q_p in [-127, 127] is stored as int8.
+//   2. split pass (HBM-bound): V = trunc(a 2^(8s-2-sigma)), an integer with |V| < 2^(8s-2), is
+//      written in balanced base-256 digits q_1..q_s (q_1 in [-64, 64], the others in [-128, 127]):
+//      a = 2^(sigma+2) sum_p q_p 256^-p up to the truncation. Each q_p is stored as int8; the digits
+//      are the bytes of V + sum_{i<s-1} 128 * 256^i with the top bit flipped in all but the top one.
 //   3. product pass (tensor cores): for the triangular pair set p + q <= s + 1, INT8 x INT8 -> INT32
 //      MMAs. Diagonals d = p + q share a power of two, so all pairs of a diagonal accumulate into one
 //      INT32 TMEM accumulator. Four diagonals ("a band") are live at once (4 x 128 TMEM columns),
 //      so every 32-wide K chunk of each slice is loaded into shared memory once per band and feeds
 //      all pairs of the band that use it. K is cut into groups short enough that no INT32 sum can
-//      overflow (|q| <= 127).
+//      overflow (|q| <= 128).
 //   4. fused recombination: eight epilogue warps keep the 128 x 128 tile of FP64 partial sums in
 //      registers; after each group they read the band's accumulators from TMEM and add
-//      D * 2^(-7d) in a fixed order; at the end of the tile they write
-//      C = fma(alpha, acc 2^sigma_i 2^tau_j, beta C0).
+//      D * 2^(-8d) in a fixed order; at the end of the tile they write
+//      C = fma(alpha, acc 2^(sigma_i+2) 2^(tau_j+2), beta C0).
 // The CPU oracle (oracle/oracle.c, oracle_ozaki_dgemm) performs the same arithmetic in the same
 // order, so results are bit-identical.
 //
@@ -48,7 +50,7 @@ constexpr int kTileN = 128;
 constexpr int kChunk = 32;                       // K elements per MMA (= bytes of an INT8 row)
 constexpr int kTileBytes = kTileM * kChunk;      // one 128 x 32 INT8 tile
 constexpr int kBand = 4;                         // live diagonal accumulators (4 x 128 TMEM cols)
-constexpr int kKPairLimit = 133144;              // floor((2^31 - 1) / 127^2)
+constexpr int kKPairLimit = 131071;              // floor((2^31 - 1) / 128^2)
 constexpr int kThreads = 320;                    // warp 0 loads, warp 1 MMA, warps 2..9 epilogue
 constexpr int kEpilogueWarps = 8;
 constexpr int kMaxSmem = 232448;                 // sm_100 opt-in dynamic shared memory per block
@@ -154,85 +156,74 @@ __global__ void amax_cols_kernel(const double* __restrict__ B, int64_t K, int64_
 // ---------------------------------------------------------------------------------------------
 // Split
 // ---------------------------------------------------------------------------------------------
+// Balanced base-256 digits. With |a| = m 2^t (m the significand with its hidden bit) and e the row's
+// (column's) exponent (|a| < 2^e), V = +-floor(|a| 2^(8S-2-e)) = +-floor(m 2^(t-e+8S-2)) is an
+// integer with |V| < 2^(8S-2) and the sign of a (truncation toward zero). D = V + C with
+// C = sum_{i < S-1} 128 * 256^i, as a two's-complement integer of 8S bits, gives the digits:
+// digit i (i = 0 least significant) = byte_i(D) - 128 in [-128, 127] for i < S-1, and
+// floor(D / 256^(S-1)) in [-64, 64] for the top one, so that V = sum_i digit_i 256^i and
+// a = 2^(e+2) sum_{p=1..S} q_p 256^-p with q_p = digit S-p. As int8 bytes: the bytes of D with the
+// top bit flipped in bytes 0..S-2, and byte S-1 of D as it is. D fits 64 signed bits for S <= 8
+// (|D| < 2^62 + 2^56) and is computed in 128 bits above.
+template <int S>
+using DigitInt = typename std::conditional<(S <= 8), long long, __int128>::type;
+
+template <int S>
+__host__ __device__ constexpr DigitInt<S> digit_offset() {
+  DigitInt<S> c = 0;
+  for (int i = 0; i < S - 1; ++i) c += static_cast<DigitInt<S>>(128) << (8 * i);
+  return c;
+}
+
+// D of one value; a zero or non-finite entry gives V = 0, i.e. D = C, whose digits are all zero.
+template <int S>
+__device__ __forceinline__ DigitInt<S> digit_string(double a, int e) {
+  using X = DigitInt<S>;
+  using U = typename std::conditional<(S <= 8), unsigned long long, unsigned __int128>::type;
+  const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(a));
+  const unsigned long long mag = bits & 0x7fffffffffffffffull;
+  const int E = static_cast<int>(mag >> 52);
+  if (mag == 0ull || E == 0x7ff) return digit_offset<S>();
+  unsigned long long m = mag & 0x000fffffffffffffull;
+  int t;
+  if (E == 0) {
+    t = -1074;
+  } else {
+    m |= 0x0010000000000000ull;
+    t = E - 1075;
+  }
+  const int sh = t - e + 8 * S - 2;
+  constexpr int kBits = 8 * static_cast<int>(sizeof(U));
+  U mg;
+  if (sh >= 0) mg = U(m) << sh;
+  else mg = (-sh >= kBits) ? U(0) : (U(m) >> (-sh));
+  const X v = (bits >> 63) ? -static_cast<X>(mg) : static_cast<X>(mg);
+  return v + digit_offset<S>();
+}
+
+// Bytes 4j .. 4j+3 of the digit string D as an int8 word (top bit flipped in the bytes of the
+// lower S-1 digits).
+template <int S>
+__device__ __forceinline__ uint32_t digit_word(DigitInt<S> D, int j) {
+  uint32_t mask = 0u;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    if (4 * j + i < S - 1) mask |= 0x80u << (8 * i);
+  return static_cast<uint32_t>(D >> (32 * j)) ^ mask;
+}
+
 // Splits one value into S slices q_1..q_S, OR-ing byte j of each into packed[p][j / 4].
-//
-// The recurrence y = 128 x, q = trunc(y), x = y - q on x = a 2^-e is exact, so q_1..q_S are the
-// base-128 digits of |x| (each carrying the sign of a). They are read here straight from the IEEE
-// fields: |a| = m 2^t (m the significand with its hidden bit), X = floor(|x| 2^(7S)) =
-// floor(m 2^(t - e + 7S)) < 2^(7S), and q_p = bits [7(S-p), 7(S-p)+7) of X. (When x underflows in
-// the FP64 recurrence, X's leading 7S bits are zero as well.)
 template <int S>
 __device__ __forceinline__ void split_value(double a, int e, int j, uint32_t (&packed)[S][8]) {
   if (e == kSentinel) return;  // NaN/Inf somewhere in the row/column: zero slices, NaN output
-  const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(a));
-  const unsigned long long mag = bits & 0x7fffffffffffffffull;
-  const int E = static_cast<int>(mag >> 52);
-  if (mag == 0ull || E == 0x7ff) return;  // zero, or a non-finite entry: zero slices
-  unsigned long long m = mag & 0x000fffffffffffffull;
-  int t;
-  if (E == 0) {
-    t = -1074;
-  } else {
-    m |= 0x0010000000000000ull;
-    t = E - 1075;
-  }
-  const int sh = t - e + 7 * S;
-  const uint32_t neg = static_cast<uint32_t>(bits >> 63);  // 1 for negative a
-  if constexpr (7 * S <= 63) {
-    unsigned long long X;
-    if (sh >= 0) X = m << sh;
-    else X = (-sh >= 64) ? 0ull : (m >> (-sh));
+  const DigitInt<S> D = digit_string<S>(a, e);
 #pragma unroll
-    for (int p = 0; p < S; ++p) {
-      const uint32_t dgt = static_cast<uint32_t>(X >> (7 * (S - 1 - p))) & 127u;
-      const uint32_t q = (dgt ^ (0u - neg)) + neg;  // two's-complement negation when negative
-      packed[p][j >> 2] |= (q & 0xffu) << (8 * (j & 3));
-    }
-  } else {
-    unsigned __int128 X;
-    if (sh >= 0) X = static_cast<unsigned __int128>(m) << sh;
-    else X = (-sh >= 128) ? static_cast<unsigned __int128>(0) : (static_cast<unsigned __int128>(m) >> (-sh));
-#pragma unroll
-    for (int p = 0; p < S; ++p) {
-      const uint32_t dgt = static_cast<uint32_t>(X >> (7 * (S - 1 - p))) & 127u;
-      const uint32_t q = (dgt ^ (0u - neg)) + neg;
-      packed[p][j >> 2] |= (q & 0xffu) << (8 * (j & 3));
-    }
+  for (int p = 0; p < S; ++p) {
+    const int i = S - 1 - p;  // digit index of slice p
+    const uint32_t byte = static_cast<uint32_t>(D >> (8 * i)) & 0xffu;
+    const uint32_t q = (i < S - 1) ? (byte ^ 0x80u) : byte;
+    packed[p][j >> 2] |= q << (8 * (j & 3));
   }
-}
-
-// ---- four values at a time ----
-// X = floor(|a| 2^(7S - e)) as in split_value (64 bits for S <= 9, 128 above), and the sign bit of
-// a; X = 0 for a zero or non-finite entry.
-template <int S>
-using DigitString = typename std::conditional<(7 * S <= 63), unsigned long long, unsigned __int128>::type;
-
-template <int S>
-__device__ __forceinline__ DigitString<S> digit_string(double a, int e, uint32_t* neg) {
-  using X = DigitString<S>;
-  const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(a));
-  const unsigned long long mag = bits & 0x7fffffffffffffffull;
-  const int E = static_cast<int>(mag >> 52);
-  *neg = static_cast<uint32_t>(bits >> 63);
-  if (mag == 0ull || E == 0x7ff) return X(0);
-  unsigned long long m = mag & 0x000fffffffffffffull;
-  int t;
-  if (E == 0) {
-    t = -1074;
-  } else {
-    m |= 0x0010000000000000ull;
-    t = E - 1075;
-  }
-  const int sh = t - e + 7 * S;
-  constexpr int kBits = 8 * static_cast<int>(sizeof(X));
-  if (sh >= 0) return X(m) << sh;
-  return (-sh >= kBits) ? X(0) : (X(m) >> (-sh));
-}
-
-// Moves four 7-bit fields (bits 0..27) into the four bytes of a word: byte i = bits 7i..7i+6.
-__device__ __forceinline__ uint32_t spread7x4(uint32_t w) {
-  w = (w & 0x00003FFFu) | ((w & 0x0FFFC000u) << 2);
-  return (w & 0x007F007Fu) | ((w & 0x3F803F80u) << 1);
 }
 
 // 4 x 4 byte transpose: on return w[i] byte j = (input w[j]) byte i.
@@ -246,22 +237,19 @@ __device__ __forceinline__ void transpose4x4(uint32_t (&w)[4]) {
 }
 
 // Slices of four consecutive values v[0..3] (K positions 4w .. 4w+3 of one row): sets word w of
-// every slice, packed[p][w] byte i = digit p of v[i] as a two's-complement byte. The digits are the
-// same as split_value's: byte i of spread7x4(bits 28j .. 28j+27 of X) is digit 4j + i counted from
-// the least significant, i.e. slice S-1-(4j+i); a negative value's digit bytes are negated (__vsub4).
+// every slice, packed[p][w] byte i = digit p of v[i] as a two's-complement byte. Word j of value
+// i's digit string holds digits 4j .. 4j+3 counted from the least significant, i.e. slices
+// S-1-4j .. S-4-4j; a 4 x 4 byte transpose turns four such words into four slice words. A zero or
+// non-finite entry has D = C, whose digits are all zero.
 template <int S>
 __device__ __forceinline__ void split4(const double (&v)[4], int e, int w, uint32_t (&packed)[S][8]) {
   constexpr int NW = (S + 3) / 4;  // words of four digits
   uint32_t dw[NW][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    uint32_t neg;
-    const DigitString<S> X = digit_string<S>(v[i], e, &neg);
+    const DigitInt<S> D = digit_string<S>(v[i], e);
 #pragma unroll
-    for (int j = 0; j < NW; ++j) {
-      uint32_t d = spread7x4(static_cast<uint32_t>(X >> (28 * j)) & 0x0FFFFFFFu);
-      dw[j][i] = neg ? __vsub4(0u, d) : d;
-    }
+    for (int j = 0; j < NW; ++j) dw[j][i] = digit_word<S>(D, j);
   }
 #pragma unroll
   for (int j = 0; j < NW; ++j) {
@@ -696,7 +684,7 @@ __device__ __forceinline__ void ozaki_body(const Source& src, DeviceStatus* stat
           for (int j = 0; j < kBand; ++j) {
             const int d = bd.dhi - j;
             if (d < bd.dlo) break;
-            const double sc = pow2i(-7 * d);
+            const double sc = pow2i(-8 * d);
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
               uint32_t v[32];
@@ -717,7 +705,7 @@ __device__ __forceinline__ void ozaki_body(const Source& src, DeviceStatus* stat
         }
       }
       if (!ok) break;
-      // ---- C = fma(alpha, acc 2^sigma 2^tau, beta C0) ----
+      // ---- C = fma(alpha, acc 2^(sigma+2) 2^(tau+2), beta C0) ----
       const OzProblem& pr = *J.pr;
       const int64_t row = J.m0 + row_in_tile;
       if (row < pr.M) {
@@ -736,7 +724,7 @@ __device__ __forceinline__ void ozaki_body(const Source& src, DeviceStatus* stat
             if (sig == kSentinel || tau == kSentinel) {
               out = __longlong_as_double(0x7ff8000000000000ll);
             } else {
-              const double tv = scale_pow2(scale_pow2(acc[i], sig), tau);
+              const double tv = scale_pow2(scale_pow2(acc[i], sig + 2), tau + 2);
               out = (beta != 0.0) ? fma(alpha, tv, __dmul_rn(beta, crow[col])) : __dmul_rn(alpha, tv);
             }
             crow[col] = out;
@@ -1037,7 +1025,7 @@ __device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatu
           for (int j = 0; j < kBand; ++j) {
             const int d = bd.dhi - j;
             if (d < bd.dlo) break;
-            const double sc = pow2i(-7 * d);
+            const double sc = pow2i(-8 * d);
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
               uint32_t v[32];
@@ -1058,7 +1046,7 @@ __device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatu
         }
       }
       if (!ok) break;
-      // ---- C = fma(alpha, acc 2^sigma 2^tau, beta C0) for this CTA's 128 rows ----
+      // ---- C = fma(alpha, acc 2^(sigma+2) 2^(tau+2), beta C0) for this CTA's 128 rows ----
       const int64_t row = m0 + static_cast<int64_t>(rank) * kTileM + row_in_tile;
       if (row < pr.M) {
         const int sig = exponent_of_maxbits(pr.amax_a[row]);
@@ -1076,7 +1064,7 @@ __device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatu
             if (sig == kSentinel || tau == kSentinel) {
               out = __longlong_as_double(0x7ff8000000000000ll);
             } else {
-              const double tv = scale_pow2(scale_pow2(acc[i], sig), tau);
+              const double tv = scale_pow2(scale_pow2(acc[i], sig + 2), tau + 2);
               out = (beta != 0.0) ? fma(alpha, tv, __dmul_rn(beta, crow[col])) : __dmul_rn(alpha, tv);
             }
             crow[col] = out;

@@ -149,12 +149,12 @@ int backward(const float* params, const float* x, const int* labels, int batch, 
 }
 
 // Conservative slice count. With gap_bits = (largest exponent gap within a row of A) + (largest
-// within a column of B), every entry a keeps at least 7s - g_a - 1 bits after truncation, so the two
-// truncated tails and the dropped pairs p + q > s + 1 (at most s + 1 of them matter) bound the
-// componentwise error by (s + 3) 2^(gap_bits + 2 - 7s) relative to |A||B|; the FP64 recombination
-// and the alpha/beta epilogue add at most 4u (the diagonal terms shrink by 2^-7 each).
+// within a column of B), every entry a keeps at least 8s - 2 - g_a - 1 bits after truncation, so the
+// two truncated tails and the dropped pairs p + q > s + 1 (at most s + 1 of them matter) bound the
+// componentwise error by (s + 3) 2^(gap_bits + 4 - 8s) relative to |A||B|; the FP64 recombination
+// and the alpha/beta epilogue add at most 4u (the diagonal terms shrink by 2^-8 each).
 double analytic_bound(int s, int gap_bits) {
-  return (s + 3) * ldexp(1.0, gap_bits + 2 - 7 * s) + 4.0 * ldexp(1.0, -53);
+  return (s + 3) * ldexp(1.0, gap_bits + 4 - 8 * s) + 4.0 * ldexp(1.0, -53);
 }
 
 int analytic(double tol, int gap_bits) {

@@ -218,10 +218,11 @@ void oracle_componentwise_error(const double* C, const double* Cref, const doubl
 /* Ozaki INT8-slice DGEMM restatement. Same arithmetic, same order as the CUDA kernels:       */
 /*  1. sigma_i = frexp exponent of max_k |A[i,k]| (0 for an all-zero row), tau_j likewise for  */
 /*     the columns of B, so |A[i,k] 2^-sigma_i| < 1.                                             */
-/*  2. x = A[i,k] 2^-sigma_i; for p = 1..s: y = 128 x, q_p = trunc(y), x = y - q_p (all exact). */
+/*  2. V = trunc(A[i,k] 2^(8s-2-sigma_i)) in balanced base-256 digits q_1..q_s (split_value),   */
+/*     so A[i,k] = 2^(sigma_i+2) sum_p q_p 256^-p up to the truncation.                            */
 /*  3. D = sum over pairs (p,q) with p+q = d and over a K group of q_p(A) q_q(B) in INT32.      */
-/*  4. acc = sum D 2^(-7d) in the band / group / diagonal order described at ozaki_worker.        */
-/*  5. C = fma(alpha, acc 2^sigma_i 2^tau_j, beta*C0)   (alpha * t when beta == 0).              */
+/*  4. acc = sum D 2^(-8d) in the band / group / diagonal order described at ozaki_worker.        */
+/*  5. C = fma(alpha, acc 2^(sigma_i+2) 2^(tau_j+2), beta*C0)   (alpha * t when beta == 0).      */
 /* ------------------------------------------------------------------------------------------ */
 static double pow2i(int e) {
   /* exact 2^e for e in [-1022, 1023] */
@@ -261,14 +262,34 @@ void oracle_ozaki_col_exponents(const double* B, int64_t K, int64_t N, int32_t* 
   }
 }
 
+/* Balanced base-256 digits of V = trunc(a 2^(8s-2-e)) (|V| < 2^(8s-2)), from the IEEE fields:
+ * |a| = m 2^t, |V| = floor(m 2^(t-e+8s-2)). D = V + sum_{i<s-1} 128 * 256^i; digit i (0 = least
+ * significant) = byte_i(D) - 128 for i < s-1 and floor(D / 256^(s-1)) (in [-64, 64]) for the top
+ * one; slice p (0-based, most significant first) holds digit s-1-p. */
 static void split_value(double a, int32_t e, int s, int8_t* out, int64_t stride) {
-  if (!isfinite(a)) { for (int p = 0; p < s; ++p) out[p * stride] = 0; return; }
-  double x = scale_pow2(a, -e);
-  for (int p = 0; p < s; ++p) {
-    double y = x * 128.0;
-    double q = trunc(y);
-    x = y - q;
-    out[p * stride] = (int8_t)q;
+  uint64_t bits;
+  memcpy(&bits, &a, sizeof bits);
+  const uint64_t mag = bits & 0x7fffffffffffffffull;
+  const int E = (int)(mag >> 52);
+  unsigned __int128 X = 0;
+  if (mag != 0 && E != 0x7ff) {
+    uint64_t m = mag & 0x000fffffffffffffull;
+    int t;
+    if (E == 0) {
+      t = -1074;
+    } else {
+      m |= 0x0010000000000000ull;
+      t = E - 1075;
+    }
+    const int sh = t - e + 8 * s - 2;
+    if (sh >= 0) X = (unsigned __int128)m << sh;
+    else X = (-sh >= 128) ? 0 : ((unsigned __int128)m >> (-sh));
+  }
+  __int128 D = (bits >> 63) ? -(__int128)X : (__int128)X;
+  for (int i = 0; i < s - 1; ++i) D += (__int128)128 << (8 * i);
+  for (int i = 0; i < s; ++i) {
+    const uint8_t byte = (uint8_t)(D >> (8 * i));
+    out[(s - 1 - i) * stride] = (int8_t)(i < s - 1 ? (uint8_t)(byte ^ 0x80u) : byte);
   }
 }
 
@@ -335,11 +356,11 @@ static void* ozaki_worker(void* arg) {
               const int8_t* bc = j->sb + ((int64_t)(q - 1) * N + c) * Kp;
               for (int64_t k = k0; k < k1; ++k) D += (int32_t)ar[k] * (int32_t)bc[k];
             }
-            acc = acc + (double)D * pow2i(-7 * d);
+            acc = acc + (double)D * pow2i(-8 * d);
           }
         }
       }
-      double t = scale_pow2(scale_pow2(acc, j->sigma[i]), j->tau[c]);
+      double t = scale_pow2(scale_pow2(acc, j->sigma[i] + 2), j->tau[c] + 2);
       double out;
       if (j->beta != 0.0) out = fma(j->alpha, t, j->beta * j->C[i * N + c]);
       else out = j->alpha * t;
@@ -376,12 +397,12 @@ void oracle_ozaki_dgemm(const double* A, const double* B, double* C, int64_t M, 
 
 /* Conservative slice count (same rule as the library's selector fallback). gap_bits = largest
  * exponent gap e(max) - e(min nonzero) within a row of A plus the largest within a column of B. An
- * entry with gap g keeps at least 7s - g - 1 bits after truncation, so the two truncated tails and
- * the dropped pairs p + q > s + 1 bound the componentwise error by (s + 3) 2^(gap_bits + 2 - 7s);
+ * entry with gap g keeps at least 8s - 2 - g - 1 bits after truncation, so the two truncated tails
+ * and the dropped pairs p + q > s + 1 bound the componentwise error by (s + 3) 2^(gap_bits + 4 - 8s);
  * the FP64 recombination and epilogue add at most 4u. The smallest s in [1, 12] meeting tol. */
 int oracle_ozaki_analytic_slices(double tol, int gap_bits) {
   for (int s = 1; s <= 12; ++s) {
-    double bound = (double)(s + 3) * ldexp(1.0, gap_bits + 2 - 7 * s) + 4.0 * ldexp(1.0, -53);
+    double bound = (double)(s + 3) * ldexp(1.0, gap_bits + 4 - 8 * s) + 4.0 * ldexp(1.0, -53);
     if (bound <= tol) return s;
   }
   return 12;

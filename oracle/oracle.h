@@ -76,7 +76,7 @@ void oracle_componentwise_error(const double* C, const double* Cref, const doubl
 
 /* ---- Ozaki INT8-slice restatement ---- */
 /* Largest INT32-safe number of (k, pair) products in one accumulator: floor((2^31-1)/127^2). */
-#define ORACLE_OZAKI_KPAIR_LIMIT 133144
+#define ORACLE_OZAKI_KPAIR_LIMIT 131071 /* floor((2^31 - 1) / 128^2): digits are in [-128, 127] */
 #define ORACLE_OZAKI_KCHUNK 32 /* K elements (bytes of an INT8 row) per MMA step */
 #define ORACLE_OZAKI_BAND 4    /* diagonals whose INT32 accumulators are live together */
 void oracle_ozaki_row_exponents(const double* A, int64_t M, int64_t K, int32_t* sigma);

@@ -90,19 +90,26 @@ def test_dot2_is_more_accurate_than_naive(oracle_mod):
 
 
 def test_ozaki_slices_reconstruct(oracle_mod):
-    """Slices are the 7-bit digits of |a| 2^-sigma truncated toward zero (sign on every digit)."""
+    """Slices are the balanced base-256 digits of trunc(a 2^(8s-2-sigma)): the top digit in
+    [-64, 64], the others in [-128, 127], a = 2^(sigma+2) sum_p q_p 256^-p up to a truncation
+    toward zero smaller than 2^(sigma-(8s-2))."""
+    from fractions import Fraction
+
     A, B, _ = oracle_mod.make_problem(30, 20, 50, phi=20, seed=11)
     for s in (1, 4, 8, 12):
         sigma, tau, sa, sb = oracle_mod.ozaki_split(A, B, s)
-        assert np.abs(sa).max() <= 127 and np.abs(sb).max() <= 127
-        w = 2.0 ** (-7 * np.arange(1, s + 1))
-        recon = np.einsum("p,pmk->mk", w, sa[:, :, :50].astype(np.float64)) * 2.0 ** sigma[:, None]
-        resid = A - recon
-        assert np.all(np.abs(resid) < 2.0 ** (sigma[:, None] - 7 * s))
-        assert np.all(resid * A >= 0)  # truncation toward zero
+        for sl in (sa, sb):
+            assert np.abs(sl[0].astype(np.int64)).max() <= 64
+            assert sl.min() >= -128 and sl.max() <= 127
         assert np.all(sa[:, :, 50:] == 0)  # K padding
-        reconb = np.einsum("p,pnk->kn", w, sb[:, :, :50].astype(np.float64)) * 2.0 ** tau[None, :]
-        assert np.all(np.abs(B - reconb) < 2.0 ** (tau[None, :] - 7 * s))
+        for (i, k) in [(0, 0), (3, 17), (29, 49), (11, 5)]:
+            V = sum(int(sa[p, i, k]) * 256 ** (s - 1 - p) for p in range(s))  # exact integer
+            x = Fraction(A[i, k]) * Fraction(2) ** (8 * s - 2 - int(sigma[i]))
+            assert abs(V) == int(abs(x)) and (V == 0 or (V > 0) == (x > 0))  # trunc toward zero
+        for (k, j) in [(0, 0), (49, 19), (7, 3)]:
+            V = sum(int(sb[p, j, k]) * 256 ** (s - 1 - p) for p in range(s))
+            x = Fraction(B[k, j]) * Fraction(2) ** (8 * s - 2 - int(tau[j]))
+            assert abs(V) == int(abs(x)) and (V == 0 or (V > 0) == (x > 0))
 
 
 def test_ozaki_restatement_accuracy(oracle_mod):
@@ -114,8 +121,8 @@ def test_ozaki_restatement_accuracy(oracle_mod):
         C = oracle_mod.ozaki_dgemm(A, B, C0, 1.5, 0.5, s)
         errs.append(oracle_mod.componentwise_error(C, Cref, den)[0])
     assert all(errs[i + 1] <= errs[i] for i in range(len(errs) - 1)), errs
-    # each slice buys about 7 bits
-    assert errs[0] / errs[4] > 2.0 ** 25
+    # each slice buys about 8 bits
+    assert errs[0] / errs[4] > 2.0 ** 28
     # eight slices reach FP64 accuracy on unscaled data
     assert errs[5] <= fp64_bound(K)
     assert errs[5] <= 64 * U
@@ -140,7 +147,7 @@ def test_ozaki_long_k_groups(oracle_mod):
     still accurate (no INT32 overflow)."""
     M, N, K = 4, 3, 40000
     A, B, C0 = oracle_mod.make_problem(M, N, K, seed=13)
-    A[:] = np.where(A >= 0, 1.0 - 2.0 ** -40, -(1.0 - 2.0 ** -40))  # slices at +-127 everywhere
+    A[:] = np.where(A >= 0, 1.0 - 2.0 ** -40, -(1.0 - 2.0 ** -40))  # digits near their extremes
     B[:] = np.abs(A[0, :])[:, None]
     C = oracle_mod.ozaki_dgemm(A, B, C0, 1.0, 0.0, 8)
     Cref, den = oracle_mod.dot2_rows(A, B, C0, 1.0, 0.0)
