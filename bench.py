@@ -446,7 +446,7 @@ def run_ours(args) -> None:
     bf16 = peaks.get("bf16_tflops")
     int8_ops = pairs(s) * flop
     achieved = int8_ops / (prod_ms * 1e-3) / 1e12
-    traffic = profile_traffic("ozaki_pair_8192_s8" if pair else "ozaki_gemm_8192_s8") if (M, N, K, s) == (8192, 8192, 8192, 8) else None
+    traffic = profile_traffic(f"{'ozaki_pair' if pair else 'ozaki_gemm'}_8192_s{s}") if (M, N, K) == (8192,) * 3 else None
     cpu = None
     if world == 1 and not args.no_cpu:
         cpu = cpu_baseline_blocked(M, N, K, args.cpu_rows, args.phi, smax, len(os.sched_getaffinity(0)))
