@@ -41,6 +41,38 @@ def test_bit_exact_vs_restatement(cuda, oracle_mod, s):
     assert_bit_exact(C, oracle_mod.ozaki_dgemm(A, B, C0, 1.5, 0.5, s))
 
 
+def _digit_edge_matrix(rng, rows, cols, by_rows):
+    """Entries that drive the balanced base-256 digits to their edges: each row (or column) holds
+    its maximum just below a power of two (top digit +-64) or exactly at one (frexp puts it at
+    0.5 2^e), values whose lower digits are all -128 or all 127 (V = +-(2^(8s-2) - 1)-like bit
+    patterns: 1 - 2^-k), tiny values and subnormals far below the maximum, exact zeros, and both
+    signs."""
+    X = rng.uniform(-1.0, 1.0, size=(rows, cols))
+    lines = X if by_rows else X.T
+    specials = np.array([1.0 - 2.0 ** -53, -(1.0 - 2.0 ** -53), 0.5, -0.5, 1.0 - 2.0 ** -20, -(1.0 - 2.0 ** -30),
+                         2.0 ** -60, -(2.0 ** -60), 5e-324, -5e-324, 2.2250738585072014e-308, 0.0,
+                         0.75 + 2.0 ** -40, -(0.5 + 2.0 ** -52), 2.0 ** -8 - 2.0 ** -61, -(2.0 ** -16)])
+    for i in range(lines.shape[0]):
+        idx = rng.choice(lines.shape[1], size=min(len(specials), lines.shape[1]), replace=False)
+        lines[i, idx] = specials[: len(idx)] * (2.0 ** int(rng.integers(-40, 41)))
+        if i % 3 == 0:
+            lines[i] *= 2.0 ** int(rng.integers(-900, 900))  # whole line far from 1
+    return X
+
+
+@pytest.mark.parametrize("s", [1, 2, 7, 8, 9, 12])
+def test_digit_edges_bit_exact(cuda, oracle_mod, s):
+    """Digit extraction at its boundaries, on both integer widths of the GPU split (64-bit up to
+    s = 8, 128-bit above), for the row (A) and column (B) split kernels alike."""
+    rng = np.random.default_rng(100 + s)
+    M, N, K = 150, 140, 96
+    A = _digit_edge_matrix(rng, M, K, by_rows=True)
+    B = _digit_edge_matrix(rng, K, N, by_rows=False)
+    C0 = rng.uniform(-1.0, 1.0, size=(M, N))
+    C = run_ozaki(cuda, A, B, C0, 1.25, -0.5, s)
+    assert_bit_exact(C, oracle_mod.ozaki_dgemm(A, B, C0, 1.25, -0.5, s))
+
+
 @pytest.mark.parametrize("M,N,K", [(1, 1, 1), (129, 130, 33), (127, 255, 64), (64, 17, 1000), (300, 8, 96)])
 def test_ragged_shapes_bit_exact(cuda, oracle_mod, M, N, K):
     A, B, C0 = oracle_mod.make_problem(M, N, K, phi=3, seed=M * 7 + N)
