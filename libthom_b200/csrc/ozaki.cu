@@ -1406,6 +1406,19 @@ int run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64
 // same place of the workspace as in run(), and every output element goes through the same
 // arithmetic, so C is bit-identical to run() on the same data.
 // ---------------------------------------------------------------------------------------------
+// Row panels of the host-resident pipeline: 16, or LIBTHOM_OZAKI_HOST_PANELS (1..64). The step is
+// bound by the host-to-device copies (A, B and C0 at about 55 GB/s); more panels shorten the tail
+// (the last panel's product and copy back) that follows the last copy in. Measured at 8192^3,
+// s = 7: 4 / 8 / 16 / 32 panels take 35.5 / 33.7 / 33.0 / 33.2 ms against a copy-in floor of 29.0 ms.
+int host_panels() {
+  static const int n = [] {
+    const char* e = getenv("LIBTHOM_OZAKI_HOST_PANELS");
+    const int v = e != nullptr ? atoi(e) : 0;
+    return (v >= 1 && v <= 64) ? v : 16;
+  }();
+  return n;
+}
+
 int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
              double beta, int s, cudaStream_t stream) {
   DeviceContext* ctx = context();
@@ -1426,8 +1439,8 @@ int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, 
   auto* Bd = reinterpret_cast<double*>(ws + off_b);
   auto* Cd = reinterpret_cast<double*>(ws + off_c);
 
-  // About eight panels (at least one 128-row block each).
-  const int64_t panel = std::max<int64_t>(kTileM, round_up(ceil_div(M, 8), kTileM));
+  // About `host_panels()` panels (at least one 128-row block each).
+  const int64_t panel = std::max<int64_t>(kTileM, round_up(ceil_div(M, host_panels()), kTileM));
   const int64_t npanels = ceil_div(M, panel);
   const int64_t chunk_block = static_cast<int64_t>(s) * kTileBytes;
 
