@@ -8,7 +8,8 @@ M = N = K = 8192, alpha = 1.5, beta = 0.5, entries u*2^e with u ~ U[-1,1) and e 
 One step = one full DGEMM through the Ozaki INT8 path (exponent + split passes, tcgen05 INT8 slice
 products, fused FP64 recombination). The slice count is the smallest one whose measured
 componentwise error |C - C_exact| / (|alpha||A||B| + |beta||C0|) on sampled rows is no worse than the
-native FP64 path's on the same rows (C_exact from the compensated CPU oracle); that selection runs
+native FP64 path's on the same rows (C_exact from the library's compensated Dot2 reference of
+those rows, computed on the device); that selection runs
 before the timed region. The native FP64 tensor-core kernel and cuBLAS DGEMM are timed alongside.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -152,7 +153,7 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------------------------
-# CPU legs (oracle = checker; used only for the accuracy selection and the CPU baselines)
+# CPU legs (the oracle appears only here: the CPU baseline and the reference arm)
 # ------------------------------------------------------------------------------------------------
 def cpu_baseline_blocked(M: int, N: int, K: int, rows: int, phi: int, smax: int, threads: int) -> dict:
     """Host blocked FP64 DGEMM on the first `rows` rows of the workload (A rows x K times K x N)."""
@@ -272,6 +273,19 @@ def run_reference(args) -> None:
 # ------------------------------------------------------------------------------------------------
 # GPU arm
 # ------------------------------------------------------------------------------------------------
+def dot2_reference(lt, torch, A, B, C0, M, N, K, alpha, beta, rows_d, stream):
+    """Compensated (double-double) reference and componentwise denominator of the sampled rows,
+    computed on the device by the library (lt_dot2_rows)."""
+    Cref = torch.empty(rows_d.numel(), N, dtype=torch.float64, device=A.device)
+    den = torch.empty_like(Cref)
+    lt.dot2_rows(A, B, C0, M, N, K, alpha, beta, rows_d, Cref, den, stream)
+    return Cref, den
+
+
+def max_error(lt, Crows, Cref, den, stream) -> float:
+    """max |C - Cref| / den over the sampled rows (lt_componentwise_error, on the device)."""
+    return lt.componentwise_error(Crows.contiguous(), Cref, den, Cref.numel(), 0.0, stream)[0]
+
 def pairs(s: int) -> int:
     return s * (s + 1) // 2
 
@@ -308,21 +322,17 @@ def run_ours(args) -> None:
         lt.scale_cols(B, K, N, SEED, 5, smax, stream)
     torch.cuda.synchronize()
 
-    # ---- accuracy selection (untimed): smallest slice count no worse than native FP64 ----
-    import oracle
-
+    # ---- accuracy selection (untimed): smallest slice count no worse than native FP64, measured
+    # against the library's compensated (Dot2) reference of sampled rows on the device ----
     rows = np.linspace(0, M - 1, args.check_rows).astype(np.int64)
-    Ah = A.cpu().numpy()
-    Bh = B.cpu().numpy()
-    C0h = C0.cpu().numpy()
+    rows_d = torch.from_numpy(rows).to(dev)
     t0 = time.perf_counter()
-    Cref, den = oracle.dot2_rows(Ah, Bh, C0h, alpha, beta, rows=rows)
-    oracle_s = time.perf_counter() - t0
-    del Ah, Bh
+    Cref, den = dot2_reference(lt, torch, A, B, C0, M, N, K, alpha, beta, rows_d, stream)
+    torch.cuda.synchronize()
+    ref_s = time.perf_counter() - t0
 
     def err_of(Cdev):
-        Cs = Cdev[torch.from_numpy(rows).to(dev)].cpu().numpy()
-        return oracle.componentwise_error(Cs, Cref, den)[0]
+        return max_error(lt, Cdev[rows_d], Cref, den, stream)
 
     C.copy_(C0)
     lt.dgemm_fp64(A, B, C, M, N, K, alpha, beta, stream)
@@ -461,7 +471,8 @@ def run_ours(args) -> None:
                    "parallelism": f"replicas x{world}"},
         "accuracy": {"max_componentwise_err": {"ozaki": errs[s], "native_fp64": err_fp64, "cublas": err_cublas},
                      "ozaki_by_slices": errs, "rows_checked": len(rows),
-                     "oracle": f"compensated Dot2 on {len(rows)} rows ({oracle_s:.1f} s)"},
+                     "reference": f"compensated Dot2 on {len(rows)} rows, on the device (lt_dot2_rows, "
+                                  f"{ref_s:.2f} s)"},
         "native_fp64": {"value": world * flop / (fp64_ms * 1e-3) / 1e12, "ms_per_step": fp64_ms,
                         "frac_of_dmma_peak": flop / (fp64_ms * 1e-3) / 1e12 / fp64_peak},
         "cublas_fp64": {"value": world * flop / (cublas_ms * 1e-3) / 1e12, "ms_per_step": cublas_ms},
@@ -501,12 +512,12 @@ def run_sweep(args) -> None:
     """The 8192^3 slice-count table: for phi in {0, 8, 32} (entries u 2^e, e ~ U{-phi..phi}), the
     native FP64 kernel, cuBLAS and the Ozaki path at s = 3..8 (and up to 12 when 8 is not enough),
     each with its CUDA-event time and its max componentwise error on sampled rows against the
-    compensated oracle and against the native FP64 result C64. One JSON line per phi."""
+    compensated Dot2 reference (lt_dot2_rows) and against the native FP64 result C64. One JSON line
+    per phi."""
     import numpy as np
     import torch
 
     import libthom_b200 as lt
-    import oracle
 
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
@@ -541,26 +552,26 @@ def run_sweep(args) -> None:
         lt.fill(B, n * n, SEED, 2, phi, stream)
         lt.fill(C0, n * n, SEED, 3, phi, stream)
         torch.cuda.synchronize()
-        Cref, den = oracle.dot2_rows(A.cpu().numpy(), B.cpu().numpy(), C0.cpu().numpy(), 1.5, 0.5, rows=rows)
+        Cref, den = dot2_reference(lt, torch, A, B, C0, n, n, n, 1.5, 0.5, rows_d, stream)
         res = {}
         ms = timed(lambda: lt.dgemm_fp64(A, B, C, n, n, n, 1.5, 0.5, stream))
-        c64 = C[rows_d].cpu().numpy()
+        c64 = C[rows_d]
         res["native_fp64"] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms": ms,
-                              "err_vs_oracle": oracle.componentwise_error(c64, Cref, den)[0]}
+                              "err_vs_dot2": max_error(lt, c64, Cref, den, stream)}
         ms = timed(lambda: lt.dgemm_cublas(A, B, C, n, n, n, 1.5, 0.5, stream))
         res["cublas"] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms": ms,
-                         "err_vs_oracle": oracle.componentwise_error(C[rows_d].cpu().numpy(), Cref, den)[0]}
+                         "err_vs_dot2": max_error(lt, C[rows_d], Cref, den, stream)}
         for sl in range(3, lt.LT_OZAKI_MAX_SLICES + 1):
             ms = timed(lambda: lt.dgemm_ozaki(A, B, C, n, n, n, 1.5, 0.5, sl, stream, workspace=ws))
-            cs = C[rows_d].cpu().numpy()
-            e = oracle.componentwise_error(cs, Cref, den)[0]
-            res[f"ozaki{sl}"] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms": ms, "err_vs_oracle": e,
-                                 "err_vs_c64": oracle.componentwise_error(cs, c64, den)[0]}
-            if sl >= 8 and e <= res["native_fp64"]["err_vs_oracle"]:
+            cs = C[rows_d]
+            e = max_error(lt, cs, Cref, den, stream)
+            res[f"ozaki{sl}"] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms": ms, "err_vs_dot2": e,
+                                 "err_vs_c64": max_error(lt, cs, c64, den, stream)}
+            if sl >= 8 and e <= res["native_fp64"]["err_vs_dot2"]:
                 break
         lt.device_status()
         print(json.dumps({"sweep": f"{n}^3 alpha=1.5 beta=0.5 phi={phi}", "rows_checked": len(rows),
-                          "oracle": "compensated Dot2", "results": res}), flush=True)
+                          "reference": "compensated Dot2 on the device (lt_dot2_rows)", "results": res}), flush=True)
 
 
 # ------------------------------------------------------------------------------------------------

@@ -231,6 +231,14 @@ int lt_scale_cols(double* X, int64_t rows, int64_t cols, uint64_t seed, uint64_t
  * out_host[0] = max |C-Cref|/den, out_host[1] = count of elements above `tol`. Synchronous. */
 int lt_componentwise_error(const double* C, const double* Cref, const double* den, int64_t n, double tol,
                            double* out_host, void* stream);
+/* Compensated reference of sampled rows on the device: for each of the nrows row indices in rows[]
+ * (device array, each in [0, M), nrows <= 65535), Cref[i][c] = alpha*A[r]B[:,c] + beta*C0[r][c] with
+ * error-free products and double-double sums in k order (Ogita-Rump-Oishi Dot2), rounded once,
+ * and den[i][c] = |alpha| sum_k |A[r][k]||B[k][c]| + |beta||C0[r][c]| (nrows x N each, row-major).
+ * The extension of the reference's host check (routines/dgemm/dgemm.cpp:122-159) used to measure
+ * componentwise errors without the host. Asynchronous on `stream`. */
+int lt_dot2_rows(const double* A, const double* B, const double* C0, double alpha, double beta, int64_t M,
+                 int64_t N, int64_t K, const int64_t* rows, int64_t nrows, double* Cref, double* den, void* stream);
 /* den = |alpha| |A||B| + |beta| |C0| on the device (FP64 kernel on absolute values). */
 int lt_abs_denominator(const double* A, const double* B, const double* C0, double* den, int64_t M, int64_t N,
                        int64_t K, double alpha, double beta, void* stream);

@@ -128,6 +128,7 @@ SIGNATURES = {
     "lt_dgemm_ozaki_host": (_i32, [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _i32, _vp]),
     "lt_dgemm_ex": (_i32, [_i32, _c.c_char, _c.c_char, _i64, _i64, _i64, _f64, _vp, _i64, _vp, _i64, _f64, _vp, _i64,
                            _i32, _vp]),
+    "lt_dot2_rows": (_i32, [_vp, _vp, _vp, _f64, _f64, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _vp]),
     # libthom_hgemm.h
     "hgemm_tc100": (_f32, _HREF),
     "hgemm_cublas": (_f32, _HREF),
@@ -251,6 +252,13 @@ def componentwise_error(C, Cref, den, n: int, tol: float = 0.0, stream=None) -> 
     out = (ctypes.c_double * 2)()
     check(lib().lt_componentwise_error(_ptr(C), _ptr(Cref), _ptr(den), n, tol, out, _stream(stream)))
     return float(out[0]), int(out[1])
+
+
+def dot2_rows(A, B, C0, M, N, K, alpha, beta, rows, Cref, den, stream=None) -> None:
+    """Compensated reference of the rows listed in the device int64 tensor `rows` (lt_dot2_rows):
+    Cref and den are (len(rows), N) FP64 device tensors."""
+    check(lib().lt_dot2_rows(_ptr(A), _ptr(B), _ptr(C0) if C0 is not None else None, alpha, beta, M, N, K, _ptr(rows),
+                             int(rows.numel()), _ptr(Cref), _ptr(den), _stream(stream)))
 
 
 def abs_denominator(A, B, C0, den, M, N, K, alpha, beta, stream=None) -> None:

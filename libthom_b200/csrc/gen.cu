@@ -1,5 +1,6 @@
 // gen.cu — device side of the seeded counter-based input generator (replaces the reference's
-// cuRAND uniform fill, routines/dgemm/dgemm.cpp:100-119) and the componentwise-error helpers.
+// cuRAND uniform fill, routines/dgemm/dgemm.cpp:100-119) and the componentwise-error helpers,
+// including a compensated (double-double) reference for sampled rows.
 // The bit recipe is the CPU oracle's (splitmix64 finaliser keyed by seed and stream, indexed by
 // element), so host and device inputs are identical.
 #include <cmath>
@@ -33,6 +34,61 @@ __global__ void fill_kernel(double* X, int64_t n, uint64_t key, int phi) {
     if (phi > 0) e = static_cast<int>(mix64(h ^ 0x5851F42D4C957F2Dull) % static_cast<uint64_t>(2 * phi + 1)) - phi;
     X[i] = scale_pow2(u, e);
   }
+}
+
+// Error-free transformations (Knuth TwoSum, FMA-based TwoProduct) with every operation rounded
+// explicitly, so that nothing is contracted or reassociated: the double-double arithmetic is the
+// same step for step as the CPU oracle's Dot2 (oracle/oracle.c, oracle_dgemm_dot2_rows).
+struct DD {
+  double hi, lo;
+};
+__device__ __forceinline__ DD two_sum(double a, double b) {
+  const double s = __dadd_rn(a, b);
+  const double bb = __dsub_rn(s, a);
+  const double e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+  return DD{s, e};
+}
+__device__ __forceinline__ DD two_prod(double a, double b) {
+  const double p = __dmul_rn(a, b);
+  return DD{p, fma(a, b, -p)};
+}
+__device__ __forceinline__ DD dd_add(DD x, DD y) {
+  const DD s = two_sum(x.hi, y.hi);
+  return two_sum(s.hi, __dadd_rn(__dadd_rn(s.lo, x.lo), y.lo));
+}
+__device__ __forceinline__ DD dd_mul_d(DD x, double a) {
+  const DD p = two_prod(x.hi, a);
+  return two_sum(p.hi, __dadd_rn(p.lo, __dmul_rn(x.lo, a)));
+}
+
+// One thread per (sampled row, column): Cref = alpha*sum_k A[r,k] B[k,c] + beta*C0[r,c] with every
+// product error-free and the sums in double-double, in k order, rounded once to double at the end;
+// den = |alpha| sum_k |A[r,k]||B[k,c]| + |beta||C0[r,c]|.
+__global__ void dot2_rows_kernel(const double* __restrict__ A, const double* __restrict__ B,
+                                 const double* __restrict__ C0, const int64_t* __restrict__ rows, int64_t N, int64_t K,
+                                 double alpha, double beta, double* __restrict__ Cref, double* __restrict__ den) {
+  const int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (c >= N) return;
+  const int64_t ri = blockIdx.y;
+  const int64_t r = rows[ri];
+  const double* arow = A + r * K;
+  DD acc{0.0, 0.0};
+  double aab = 0.0;
+  for (int64_t k = 0; k < K; ++k) {
+    const double a = arow[k];
+    const double b = B[k * N + c];
+    acc = dd_add(acc, two_prod(a, b));
+    aab = __dadd_rn(aab, __dmul_rn(fabs(a), fabs(b)));
+  }
+  DD v = dd_mul_d(acc, alpha);
+  double d = __dmul_rn(fabs(alpha), aab);
+  if (beta != 0.0) {
+    const double c0 = C0[r * N + c];
+    v = dd_add(v, two_prod(beta, c0));
+    d = __dadd_rn(d, __dmul_rn(fabs(beta), fabs(c0)));
+  }
+  Cref[ri * N + c] = __dadd_rn(v.hi, v.lo);
+  den[ri * N + c] = d;
 }
 
 __device__ __forceinline__ int scale_exp(uint64_t key, int64_t i, int smax) {
@@ -150,6 +206,20 @@ int lt_componentwise_error(const double* C, const double* Cref, const double* de
   memcpy(&mx, &h[0], sizeof mx);
   out_host[0] = mx;
   out_host[1] = static_cast<double>(h[1]);
+  return lt::ok();
+}
+
+int lt_dot2_rows(const double* A, const double* B, const double* C0, double alpha, double beta, int64_t M,
+                 int64_t N, int64_t K, const int64_t* rows, int64_t nrows, double* Cref, double* den, void* stream) {
+  if (M < 0 || N < 0 || K < 0 || nrows < 0 || nrows > 65535 ||
+      (nrows > 0 && N > 0 && (rows == nullptr || Cref == nullptr || den == nullptr)) ||
+      (K > 0 && nrows > 0 && N > 0 && (A == nullptr || B == nullptr)) || (beta != 0.0 && C0 == nullptr && nrows > 0))
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_dot2_rows: bad arguments");
+  if (nrows == 0 || N == 0) return lt::ok();
+  if (lt::context() == nullptr) return lt::last_error();
+  const dim3 grid(static_cast<unsigned>((N + 255) / 256), static_cast<unsigned>(nrows));
+  lt::dot2_rows_kernel<<<grid, 256, 0, lt::as_stream(stream)>>>(A, B, C0, rows, N, K, alpha, beta, Cref, den);
+  LT_CUDA_TRY(cudaGetLastError());
   return lt::ok();
 }
 

@@ -118,3 +118,16 @@ def test_hgemm_rejects_bad_arguments():
     assert L.lt_hgemm_num_configs() == len(lt.hgemm_configs()) >= 2
     # M == 0 or N == 0: nothing to do, no device touched
     assert L.lt_hgemm(p, p, p, 0, 4, 4, 1.0, 0.0, None) == lt.LT_OK
+
+
+def test_dot2_rows_rejects_bad_arguments():
+    """lt_dot2_rows validates before any device work (no GPU needed)."""
+    import libthom_b200 as lt
+
+    L = lt.lib()
+    p = ctypes.c_void_p(0x1000)
+    assert L.lt_dot2_rows(p, p, p, 1.0, 0.0, -1, 4, 4, p, 2, p, p, None) == lt.LT_ERR_INVALID_ARGUMENT
+    assert L.lt_dot2_rows(p, p, p, 1.0, 0.0, 4, 4, 4, None, 2, p, p, None) == lt.LT_ERR_INVALID_ARGUMENT
+    assert L.lt_dot2_rows(p, p, None, 1.0, 0.5, 4, 4, 4, p, 2, p, p, None) == lt.LT_ERR_INVALID_ARGUMENT  # C0 needed
+    assert L.lt_dot2_rows(p, p, p, 1.0, 0.0, 4, 4, 4, p, 70000, p, p, None) == lt.LT_ERR_INVALID_ARGUMENT
+    assert L.lt_dot2_rows(p, p, p, 1.0, 0.0, 4, 4, 4, p, 0, p, p, None) == lt.LT_OK  # nothing to do
