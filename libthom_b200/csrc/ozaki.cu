@@ -31,7 +31,10 @@
 // ((rb*NC + c)*S + p)*4 KB, so the tiles of slices 1..n of one K chunk are one contiguous n*4 KB
 // block and the producer moves them with a single 1-D bulk copy (cp.async.bulk). Each bulk copy
 // costs the issuing thread about 100 cycles whatever its size (measured on B200), so copies per
-// stage, not bytes, set the producer's pace. Rows beyond M (N) in the last block are zero.
+// stage, not bytes, set the producer's pace. B slices that the CTA-pair kernel reads are stored
+// half-major inside each chunk block (rows 0..63 of every slice's tile, then rows 64..127), so each
+// CTA of the pair loads its halves of all slices with one copy too. Rows beyond M (N) in the last
+// block are zero.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -49,6 +52,7 @@ constexpr int kTileM = 128;
 constexpr int kTileN = 128;
 constexpr int kChunk = 32;                       // K elements per MMA (= bytes of an INT8 row)
 constexpr int kTileBytes = kTileM * kChunk;      // one 128 x 32 INT8 tile
+constexpr int kHalfTileBytes = kTileBytes / 2;   // 64 rows of a tile (one CTA's share of a B tile)
 constexpr int kBand = 4;                         // live diagonal accumulators (4 x 128 TMEM cols)
 constexpr int kKPairLimit = 131071;              // floor((2^31 - 1) / 128^2)
 constexpr int kThreads = 320;                    // warp 0 loads, warp 1 MMA, warps 2..9 epilogue
@@ -264,15 +268,28 @@ __device__ __forceinline__ void split4(const double (&v)[4], int e, int w, uint3
 }
 
 // Writes row r (32 bytes per slice) of tile (rb, c) of every slice, in the swizzled tile order.
+// The chunk block (rb, c) holds the S tiles of the chunk. Tile-major (half_major = 0): tile p at
+// p * 4 KB, its rows 0..127 contiguous, as the one-CTA kernel reads a 128-row operand. Half-major
+// (B slices of the CTA-pair kernel): rows 64h .. 64h+63 of every tile, slices 0..S-1 in turn, form
+// half h (S * 2 KB), so the pair's CTA of rank h finds the halves of all slices it needs in one
+// contiguous run and loads them with one bulk copy.
 template <int S>
 __device__ __forceinline__ void store_tile_row(int8_t* out, int64_t RB, int64_t NC, int64_t rb, int64_t c, int r,
-                                               const uint32_t (&packed)[S][8]) {
+                                               const uint32_t (&packed)[S][8], int half_major) {
   const int flip = (r >> 2) & 1;
   (void)RB;
-  int8_t* block = out + (rb * NC + c) * S * kTileBytes + r * 32;
+  int8_t* block = out + (rb * NC + c) * S * kTileBytes;
+  int64_t step;
+  if (half_major) {
+    block += (r >> 6) * S * kHalfTileBytes + (r & 63) * 32;
+    step = kHalfTileBytes;
+  } else {
+    block += r * 32;
+    step = kTileBytes;
+  }
 #pragma unroll
   for (int p = 0; p < S; ++p) {
-    int8_t* tile = block + p * kTileBytes;
+    int8_t* tile = block + p * step;
     uint4 lo = make_uint4(packed[p][0], packed[p][1], packed[p][2], packed[p][3]);
     uint4 hi = make_uint4(packed[p][4], packed[p][5], packed[p][6], packed[p][7]);
     reinterpret_cast<uint4*>(tile)[flip] = lo;
@@ -285,7 +302,8 @@ template <int S>
 __device__ __forceinline__ void split_rows_tile(const double* __restrict__ A, int64_t M, int64_t K, int64_t lda,
                                                 int64_t NC,
                                                 int64_t RB, const unsigned long long* __restrict__ amax,
-                                                int8_t* __restrict__ out, int64_t rb, int64_t c, int r) {
+                                                int8_t* __restrict__ out, int64_t rb, int64_t c, int r,
+                                                int half_major = 0) {
   const int64_t row = rb * kTileM + r;
   uint32_t packed[S][8];
 #pragma unroll
@@ -330,7 +348,7 @@ __device__ __forceinline__ void split_rows_tile(const double* __restrict__ A, in
       }
     }
   }
-  store_tile_row<S>(out, RB, NC, rb, c, r, packed);
+  store_tile_row<S>(out, RB, NC, rb, c, r, packed, half_major);
 }
 
 // Tile (rb, c) of B (transposed to K-major): thread r handles column rb*128 + r.
@@ -338,7 +356,8 @@ template <int S>
 __device__ __forceinline__ void split_cols_tile(const double* __restrict__ B, int64_t K, int64_t N, int64_t ldb,
                                                 int64_t NC,
                                                 int64_t RB, const unsigned long long* __restrict__ amax,
-                                                int8_t* __restrict__ out, int64_t rb, int64_t c, int r) {
+                                                int8_t* __restrict__ out, int64_t rb, int64_t c, int r,
+                                                int half_major = 0) {
   const int64_t col = rb * kTileN + r;
   uint32_t packed[S][8];
 #pragma unroll
@@ -372,7 +391,7 @@ __device__ __forceinline__ void split_cols_tile(const double* __restrict__ B, in
       }
     }
   }
-  store_tile_row<S>(out, RB, NC, rb, c, r, packed);
+  store_tile_row<S>(out, RB, NC, rb, c, r, packed, half_major);
 }
 
 // One block (128 threads) per tile; tiles walked with a grid stride.
@@ -380,18 +399,18 @@ template <int S>
 __global__ void __launch_bounds__(128) split_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K, int64_t lda,
                                                          int64_t NC, int64_t RB,
                                                          const unsigned long long* __restrict__ amax,
-                                                         int8_t* __restrict__ out) {
+                                                         int8_t* __restrict__ out, int half_major) {
   for (int64_t t = blockIdx.x; t < RB * NC; t += gridDim.x)
-    split_rows_tile<S>(A, M, K, lda, NC, RB, amax, out, t / NC, t % NC, threadIdx.x);
+    split_rows_tile<S>(A, M, K, lda, NC, RB, amax, out, t / NC, t % NC, threadIdx.x, half_major);
 }
 
 template <int S>
 __global__ void __launch_bounds__(128) split_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N, int64_t ldb,
                                                          int64_t NC, int64_t RB,
                                                          const unsigned long long* __restrict__ amax,
-                                                         int8_t* __restrict__ out) {
+                                                         int8_t* __restrict__ out, int half_major) {
   for (int64_t t = blockIdx.x; t < RB * NC; t += gridDim.x)
-    split_cols_tile<S>(B, K, N, ldb, NC, RB, amax, out, t / NC, t % NC, threadIdx.x);
+    split_cols_tile<S>(B, K, N, ldb, NC, RB, amax, out, t / NC, t % NC, threadIdx.x, half_major);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -408,6 +427,7 @@ struct OzProblem {
   double alpha, beta;
   int64_t ldc;     // row stride of C (>= N)
   int group = 8;   // pair-rows per raster group of the CTA-pair kernel
+  int pair = 0;    // 1: CTA-pair kernel, B slices stored half-major (see store_tile_row)
 };
 
 // One output tile of one problem.
@@ -774,7 +794,6 @@ __global__ void __launch_bounds__(kThreads, 1) ozaki_gemm_grouped_kernel(OzGroup
 //   acc_full  count 1 in each CTA: committed to both after a group's last MMA.
 //   acc_empty rank 0 only, count 16: every epilogue warp of both CTAs arrives after reading TMEM.
 // ---------------------------------------------------------------------------------------------
-constexpr int kHalfTileBytes = kTileBytes / 2;                // 64 rows of a B tile
 constexpr int kPairChunkBytes = kTileBytes + kHalfTileBytes;  // one slice, one chunk, one CTA
 
 template <int S>
@@ -882,7 +901,9 @@ __device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatu
         const int64_t rb = m0 / kTileM + rank;  // this CTA's row block; past the end: no A copies
         const bool has_a = rb < pr.rba;
         const int8_t* a_blk = pr.sa + (has_a ? rb : 0) * nkc * kChunkBlock;
-        const int8_t* b_blk = pr.sb + static_cast<int64_t>(n0 / kTileN) * nkc * kChunkBlock + rank * kHalfTileBytes;
+        // B slices are half-major (store_tile_row): this CTA's 64-row halves of all slices of a chunk
+        // are one contiguous run, S * 2 KB past the chunk block's start for rank 1.
+        const int8_t* b_blk = pr.sb + static_cast<int64_t>(n0 / kTileN) * nkc * kChunkBlock + rank * S * kHalfTileBytes;
         const uint32_t chunk_bytes = (has_a ? kTileBytes : 0) + kHalfTileBytes;
         for (int b = 0; b < NB && ok; ++b) {
           const Band bd = band_of(S, b);
@@ -897,10 +918,8 @@ __device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatu
               for (int64_t c = cs; c < ce; ++c) {
                 uint8_t* base = st + (c - cs) * bd.nsl * kPairChunkBytes;
                 if (has_a) bulk_load(base, a_blk + c * kChunkBlock, bd.nsl * kTileBytes, &full[stage]);
-                const int8_t* gb = b_blk + c * kChunkBlock;
-                for (int q = 0; q < bd.nsl; ++q)  // this CTA's half of each B tile (strided)
-                  bulk_load(base + bd.nsl * kTileBytes + q * kHalfTileBytes, gb + q * kTileBytes, kHalfTileBytes,
-                            &full[stage]);
+                // this CTA's halves of the band's B tiles (slices 1..nsl): one copy
+                bulk_load(base + bd.nsl * kTileBytes, b_blk + c * kChunkBlock, bd.nsl * kHalfTileBytes, &full[stage]);
               }
               if (++stage == G::kStages) { stage = 0; phase ^= 1; }
             }
@@ -1189,6 +1208,10 @@ bool pair_enabled() {
   return on;
 }
 
+// Whether a single problem with `rba` row blocks of A runs on the CTA-pair kernel. The split of its
+// B side and the product both ask, so the B slices are laid out for the kernel that reads them.
+bool pair_path(int64_t rba) { return rba >= 2 && pair_enabled(); }
+
 template <bool kGrouped, class Src>
 int launch_gemm(int s, const Src& src, int64_t ntiles, DeviceContext* ctx, cudaStream_t stream) {
   switch (s) {
@@ -1211,10 +1234,10 @@ int launch_split_s(const double* A, const double* B, int64_t M, int64_t N, int64
   const int64_t cap = static_cast<int64_t>(sms) * 64;
   const int64_t ta = L.RBa * L.NC, tb = L.RBb * L.NC;
   if (ta > 0) split_rows_kernel<S><<<static_cast<unsigned>(ta < cap ? ta : cap), 128, 0, stream>>>(A, M, K, K, L.NC, L.RBa,
-                                                                                                   amax_a, sa);
+                                                                                                   amax_a, sa, 0);
   LT_CUDA_TRY(cudaGetLastError());
   if (tb > 0) split_cols_kernel<S><<<static_cast<unsigned>(tb < cap ? tb : cap), 128, 0, stream>>>(B, K, N, N, L.NC, L.RBb,
-                                                                                                   amax_b, sb);
+                                                                                                   amax_b, sb, 0);
   LT_CUDA_TRY(cudaGetLastError());
   return LT_OK;
 }
@@ -1234,26 +1257,29 @@ int launch_split(int s, const double* A, const double* B, int64_t M, int64_t N, 
 
 template <int S>
 void launch_split_rows_s(const double* A, int64_t M, int64_t K, int64_t lda, int64_t NC, const unsigned long long* amax,
-                         int8_t* sa,
-                         int sms, cudaStream_t stream) {
+                         int8_t* sa, int sms, cudaStream_t stream, int half_major) {
   const int64_t cap = static_cast<int64_t>(sms) * 64;
   const int64_t rb = ceil_div(M, kTileM), t = rb * NC;
-  if (t > 0) split_rows_kernel<S><<<static_cast<unsigned>(t < cap ? t : cap), 128, 0, stream>>>(A, M, K, lda, NC, rb, amax, sa);
+  if (t > 0)
+    split_rows_kernel<S><<<static_cast<unsigned>(t < cap ? t : cap), 128, 0, stream>>>(A, M, K, lda, NC, rb, amax, sa,
+                                                                                       half_major);
 }
 
 template <int S>
 void launch_split_cols_s(const double* B, int64_t K, int64_t N, int64_t ldb, int64_t NC, const unsigned long long* amax,
-                         int8_t* sb,
-                         int sms, cudaStream_t stream) {
+                         int8_t* sb, int sms, cudaStream_t stream, int half_major) {
   const int64_t cap = static_cast<int64_t>(sms) * 64;
   const int64_t rb = ceil_div(N, kTileN), t = rb * NC;
-  if (t > 0) split_cols_kernel<S><<<static_cast<unsigned>(t < cap ? t : cap), 128, 0, stream>>>(B, K, N, ldb, NC, rb, amax, sb);
+  if (t > 0)
+    split_cols_kernel<S><<<static_cast<unsigned>(t < cap ? t : cap), 128, 0, stream>>>(B, K, N, ldb, NC, rb, amax, sb,
+                                                                                       half_major);
 }
 
 // Row side of the split: exponents of rows 0..M-1 of A (amax must be zero on entry) and their
-// slices, written as row blocks 0.. of `sa` (chunk-major, NC chunks).
+// slices, written as row blocks 0.. of `sa` (chunk-major, NC chunks; half_major for B slices that
+// the CTA-pair kernel reads, see store_tile_row).
 int rows_stage(int s, const double* A, int64_t M, int64_t K, int64_t lda, int64_t NC, unsigned long long* amax,
-               int8_t* sa, int sms, cudaStream_t stream) {
+               int8_t* sa, int sms, cudaStream_t stream, int half_major) {
   if (M <= 0) return LT_OK;
   if (K > 0) {
     // 8 rows per block, K split so that the grid covers the GPU.
@@ -1268,7 +1294,7 @@ int rows_stage(int s, const double* A, int64_t M, int64_t K, int64_t lda, int64_
   }
   switch (s) {
 #define LT_ROWS_CASE(S) \
-  case S: launch_split_rows_s<S>(A, M, K, lda, NC, amax, sa, sms, stream); break;
+  case S: launch_split_rows_s<S>(A, M, K, lda, NC, amax, sa, sms, stream, half_major); break;
     LT_ROWS_CASE(1) LT_ROWS_CASE(2) LT_ROWS_CASE(3) LT_ROWS_CASE(4) LT_ROWS_CASE(5) LT_ROWS_CASE(6)
     LT_ROWS_CASE(7) LT_ROWS_CASE(8) LT_ROWS_CASE(9) LT_ROWS_CASE(10) LT_ROWS_CASE(11) LT_ROWS_CASE(12)
 #undef LT_ROWS_CASE
@@ -1280,7 +1306,7 @@ int rows_stage(int s, const double* A, int64_t M, int64_t K, int64_t lda, int64_
 
 // Column side: exponents of columns 0..N-1 of B (amax zero on entry) and their slices.
 int cols_stage(int s, const double* B, int64_t K, int64_t N, int64_t ldb, int64_t NC, unsigned long long* amax,
-               int8_t* sb, int sms, cudaStream_t stream) {
+               int8_t* sb, int sms, cudaStream_t stream, int half_major) {
   if (N <= 0) return LT_OK;
   if (K > 0) {
     const int pairs = (N % 2 == 0) && (ldb % 2 == 0) && ((reinterpret_cast<uintptr_t>(B) & 15) == 0);
@@ -1296,7 +1322,7 @@ int cols_stage(int s, const double* B, int64_t K, int64_t N, int64_t ldb, int64_
   }
   switch (s) {
 #define LT_COLS_CASE(S) \
-  case S: launch_split_cols_s<S>(B, K, N, ldb, NC, amax, sb, sms, stream); break;
+  case S: launch_split_cols_s<S>(B, K, N, ldb, NC, amax, sb, sms, stream, half_major); break;
     LT_COLS_CASE(1) LT_COLS_CASE(2) LT_COLS_CASE(3) LT_COLS_CASE(4) LT_COLS_CASE(5) LT_COLS_CASE(6)
     LT_COLS_CASE(7) LT_COLS_CASE(8) LT_COLS_CASE(9) LT_COLS_CASE(10) LT_COLS_CASE(11) LT_COLS_CASE(12)
 #undef LT_COLS_CASE
@@ -1319,17 +1345,18 @@ int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int
   auto* sa = reinterpret_cast<int8_t*>(ws + L.off_sa);
   auto* sb = reinterpret_cast<int8_t*>(ws + L.off_sb);
   LT_CUDA_TRY(cudaMemsetAsync(ws, 0, L.off_sa, stream));
-  LT_TRY(rows_stage(s, A, M, K, K, L.NC, amax_a, sa, ctx->sm_count, stream));
-  return cols_stage(s, B, K, N, N, L.NC, amax_b, sb, ctx->sm_count, stream);
+  LT_TRY(rows_stage(s, A, M, K, K, L.NC, amax_a, sa, ctx->sm_count, stream, 0));
+  return cols_stage(s, B, K, N, N, L.NC, amax_b, sb, ctx->sm_count, stream, pair_path(L.RBa) ? 1 : 0);
 }
 
-// Products and recombination of one problem whose slices are in place: the CTA-pair kernel for two
-// or more row blocks, the one-CTA kernel otherwise.
+// Products and recombination of one problem whose slices are in place: the CTA-pair kernel when
+// pr.pair is set (B slices split half-major), the one-CTA kernel otherwise.
 int launch_product(int s, const OzProblem& pr, DeviceContext* ctx, cudaStream_t stream) {
-  if (pr.rba >= 2 && pair_enabled()) {
+  if (pr.pair) {
     bool launched = false;
     LT_TRY(launch_pair(s, pr, ctx, stream, &launched));
-    if (launched) return LT_OK;
+    if (!launched) return set_error(LT_ERR_UNSUPPORTED, "no pair of CTAs of the Ozaki product kernel fits");
+    return LT_OK;
   }
   return launch_gemm<false>(s, pr, pr.rba * pr.rbb, ctx, stream);
 }
@@ -1356,6 +1383,7 @@ int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double bet
   pr.rbb = L.RBb;
   pr.alpha = alpha;
   pr.beta = beta;
+  pr.pair = pair_path(L.RBa) ? 1 : 0;
   return launch_product(s, pr, ctx, stream);
 }
 
@@ -1380,15 +1408,17 @@ int run_ex(bool trans_a, bool trans_b, const double* A, int64_t lda, const doubl
   auto* sb = reinterpret_cast<int8_t*>(ws + L.off_sb);
   LT_CUDA_TRY(cudaMemsetAsync(ws, 0, L.off_sa, stream));
   const int sms = ctx->sm_count;
+  const int pair = pair_path(L.RBa) ? 1 : 0;
   if (!trans_a)
-    LT_TRY(rows_stage(s, A, M, K, lda, L.NC, amax_a, sa, sms, stream));
+    LT_TRY(rows_stage(s, A, M, K, lda, L.NC, amax_a, sa, sms, stream, 0));
   else
-    LT_TRY(cols_stage(s, A, K, M, lda, L.NC, amax_a, sa, sms, stream));
+    LT_TRY(cols_stage(s, A, K, M, lda, L.NC, amax_a, sa, sms, stream, 0));
   if (!trans_b)
-    LT_TRY(cols_stage(s, B, K, N, ldb, L.NC, amax_b, sb, sms, stream));
+    LT_TRY(cols_stage(s, B, K, N, ldb, L.NC, amax_b, sb, sms, stream, pair));
   else
-    LT_TRY(rows_stage(s, B, N, K, ldb, L.NC, amax_b, sb, sms, stream));
+    LT_TRY(rows_stage(s, B, N, K, ldb, L.NC, amax_b, sb, sms, stream, pair));
   OzProblem pr{sa, sb, C, amax_a, amax_b, M, N, L.NC, L.RBa, L.RBb, alpha, beta, ldc};
+  pr.pair = pair;
   return launch_product(s, pr, ctx, stream);
 }
 
@@ -1466,7 +1496,10 @@ int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, 
     cuda(cudaMemsetAsync(ws, 0, L.off_sa, stream), "memset");
     cuda(cudaStreamWaitEvent(stream, e_b, 0), "wait");
   }
-  if (rc == LT_OK) rc = cols_stage(s, Bd, K, N, N, L.NC, amax_b, sb, ctx->sm_count, stream);
+  // Every panel's product takes the same kernel (the pair kernel also serves a last panel of one
+  // row block), so the B slices are split once in its layout.
+  const int pair = pair_path(ceil_div(panel, kTileM)) ? 1 : 0;
+  if (rc == LT_OK) rc = cols_stage(s, Bd, K, N, N, L.NC, amax_b, sb, ctx->sm_count, stream, pair);
   for (int64_t i = 0; i < npanels && rc == LT_OK; ++i) {
     const int64_t r0 = i * panel, rows = std::min(panel, M - r0);
     cudaEvent_t e_in = ev[2 * i], e_out = ev[2 * i + 1];
@@ -1479,10 +1512,11 @@ int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, 
     cuda(cudaStreamWaitEvent(stream, e_in, 0), "wait");
     if (rc != LT_OK) break;
     int8_t* sa_panel = sa + (r0 / kTileM) * L.NC * chunk_block;
-    rc = rows_stage(s, Ad + r0 * K, rows, K, K, L.NC, amax_a + r0, sa_panel, ctx->sm_count, stream);
+    rc = rows_stage(s, Ad + r0 * K, rows, K, K, L.NC, amax_a + r0, sa_panel, ctx->sm_count, stream, 0);
     if (rc != LT_OK) break;
     OzProblem pr{sa_panel, sb, Cd + r0 * N, amax_a + r0, amax_b, rows, N, L.NC, ceil_div(rows, kTileM), L.RBb,
                  alpha, beta, N};
+    pr.pair = pair;
     rc = launch_product(s, pr, ctx, stream);
     if (rc != LT_OK) break;
     cuda(cudaEventRecord(e_out, stream), "record");
