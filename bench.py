@@ -92,7 +92,7 @@ def profile_traffic(name: str):
 
 
 class ClockSampler:
-    """SM clock, power and clock-event reasons of one GPU, read through NVML every 20 ms by a
+    """SM clock, power and clock-event reasons of one GPU, read through NVML every 2 ms by a
     background thread while the timed region runs (reading only; no setting is changed)."""
 
     REASONS = (("hw_slowdown", "nvmlClocksThrottleReasonHwSlowdown"),
@@ -101,7 +101,7 @@ class ClockSampler:
                ("sw_power_cap", "nvmlClocksThrottleReasonSwPowerCap"),
                ("hw_power_brake_slowdown", "nvmlClocksThrottleReasonHwPowerBrakeSlowdown"))
 
-    def __init__(self, device: int, period_s: float = 0.02):
+    def __init__(self, device: int, period_s: float = 0.002):
         self.device = device
         self.period = period_s
         self.rows = []
@@ -149,7 +149,7 @@ class ClockSampler:
         reasons = sorted({x for r in self.rows for x in r[2]})
         return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_mhz_min": min(r[0] for r in loaded),
                 "sm_max_mhz": self.max_mhz, "power_w_max": max(r[1] for r in self.rows),
-                "samples": len(self.rows), "source": "NVML, 20 ms", "reasons": reasons}
+                "samples": len(self.rows), "source": "NVML, 2 ms", "reasons": reasons}
 
 
 # ------------------------------------------------------------------------------------------------
