@@ -92,7 +92,7 @@ def test_cta_pair_kernel_bit_exact(cuda, oracle_mod, M, N, K, s):
 
 
 @pytest.mark.parametrize("M,N,K,beta,pinned", [(1000, 300, 200, 0.5, True), (300, 130, 96, 0.0, False),
-                                              (2560, 384, 64, 1.0, True)])
+                                              (2560, 384, 64, 1.0, True), (2100, 200, 72, 0.5, True)])
 def test_host_resident_bit_exact(cuda, oracle_mod, M, N, K, beta, pinned):
     """lt_dgemm_ozaki_host: operands in host memory, streamed through the GPU in row panels (a
     ragged last panel, pageable and pinned buffers, beta = 0 skipping the C0 copy): the same bits
