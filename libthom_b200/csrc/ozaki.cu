@@ -316,27 +316,30 @@ __device__ __forceinline__ void split_rows_tile(const double* __restrict__ A, in
     const int64_t k0 = c * kChunk;
     if constexpr (S <= LT_OZAKI_MAX_SLICES) {
       if (e != kSentinel) {
-        // 16-byte loads when the row is 16-byte aligned and the chunk is whole: each lane's two
-        // doubles share one L1 sector, half the tag lookups of scalar loads across 32 rows.
+        // The whole 32-value chunk is loaded before any digit is extracted, so each thread keeps
+        // 256 bytes in flight (memory-level parallelism for an HBM-bound pass). 16-byte loads when
+        // the row is 16-byte aligned and the chunk is whole: each lane's two doubles share one L1
+        // sector, half the tag lookups of scalar loads across 32 rows.
         const bool vec = ((reinterpret_cast<uintptr_t>(a + k0) & 15) == 0) && (k0 + kChunk <= K);
+        double v[kChunk];
+        if (vec) {
+#pragma unroll
+          for (int j = 0; j < kChunk / 2; ++j) {
+            const double2 x = __ldg(reinterpret_cast<const double2*>(a + k0 + 2 * j));
+            v[2 * j] = x.x;
+            v[2 * j + 1] = x.y;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < kChunk; ++j) {
+            const int64_t k = k0 + j;
+            v[j] = (k < K) ? __ldg(a + k) : 0.0;
+          }
+        }
 #pragma unroll
         for (int w = 0; w < 8; ++w) {
-          double v[4];
-          if (vec) {
-            const double2 x = __ldg(reinterpret_cast<const double2*>(a + k0 + 4 * w));
-            const double2 y = __ldg(reinterpret_cast<const double2*>(a + k0 + 4 * w + 2));
-            v[0] = x.x;
-            v[1] = x.y;
-            v[2] = y.x;
-            v[3] = y.y;
-          } else {
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              const int64_t k = k0 + 4 * w + i;
-              v[i] = (k < K) ? __ldg(a + k) : 0.0;
-            }
-          }
-          split4<S>(v, e, w, packed);
+          const double q[4] = {v[4 * w], v[4 * w + 1], v[4 * w + 2], v[4 * w + 3]};
+          split4<S>(q, e, w, packed);
         }
       }
     } else {
@@ -371,15 +374,14 @@ __device__ __forceinline__ void split_cols_tile(const double* __restrict__ B, in
       if (e != kSentinel) {
         const double* bp = B + k0 * ldb + col;
         const bool whole = k0 + kChunk <= K;  // no bounds test per load
+        // All 32 loads first (memory-level parallelism), then the digits.
+        double v[kChunk];
+#pragma unroll
+        for (int kk = 0; kk < kChunk; ++kk) v[kk] = (whole || k0 + kk < K) ? __ldg(bp + kk * ldb) : 0.0;
 #pragma unroll
         for (int w = 0; w < 8; ++w) {
-          double v[4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const int kk = 4 * w + i;
-            v[i] = (whole || k0 + kk < K) ? __ldg(bp + kk * ldb) : 0.0;
-          }
-          split4<S>(v, e, w, packed);
+          const double q[4] = {v[4 * w], v[4 * w + 1], v[4 * w + 2], v[4 * w + 3]};
+          split4<S>(q, e, w, packed);
         }
       }
     } else {
