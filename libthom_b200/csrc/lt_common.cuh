@@ -92,7 +92,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
 }
 
 // ---------------------------------------------------------------------------------------------
-// TMA (tiled bulk tensor copies, global -> shared, completion on an mbarrier). No multicast.
+// TMA (tiled bulk tensor copies, global -> shared, completion on an mbarrier); each CTA loads only
+// into its own shared memory.
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ void tma_prefetch_desc(const void* desc) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(desc)) : "memory");
