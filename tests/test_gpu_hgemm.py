@@ -74,7 +74,7 @@ def test_golden_cases(cuda, oracle_mod):
         ex, den = oracle_mod.hgemm_exact_rows(A, B, C0, alpha, beta)
         a, r = C.view(np.float16).astype(np.float64), Cref.view(np.float16).astype(np.float64)
         both = np.isfinite(a) & np.isfinite(r)
-        assert np.all(np.abs(a - r)[both] <= 2 * tolerance(K, ex, den)[both]), i
+        assert np.all(np.abs(a[both] - r[both]) <= 2 * tolerance(K, ex, den)[both]), i
 
 
 def test_every_config(cuda, oracle_mod):
@@ -198,3 +198,29 @@ def test_reference_contract_wrapper_times(cuda, oracle_mod):
     C = dC.view(torch.int16).cpu().numpy().view(np.uint16).reshape(256, 256)
     assert check_against_exact(oracle_mod, C, A, B, C0, 1.0, 0.0) <= 1.0
     assert lt.hgemm("cublas", dA, dB, dC, 256, 256, 256, 1.0, 0.0) > 0.0
+
+
+def test_long_k(cuda, oracle_mod):
+    """K = 65536 (1024 K blocks): FP32 accumulation over a long K stays within the bound, checked on
+    rows from both CTAs of every pair tile."""
+    M, N, K = 256, 264, 65536
+    A, B, C0 = oracle_mod.make_half_problem(M, N, K, seed=31, lo=-1.0, hi=1.0)
+    C = run_tc(cuda, A, B, C0, 1.0, 0.0)
+    rows = np.array([0, 31, 64, 127, 128, 170, 255])
+    assert check_against_exact(oracle_mod, C, A, B, C0, 1.0, 0.0, rows=rows) <= 1.0
+
+
+def test_nonfinite_inputs_propagate_like_the_reference(cuda, oracle_mod):
+    """An Inf or NaN in A or B makes exactly the outputs non-finite that the reference's check loop
+    (routines/hgemm/hgemm.cu:135-149, restated) makes non-finite, with the same sign for Inf."""
+    M, N, K = 70, 90, 200
+    A, B, C0 = oracle_mod.make_half_problem(M, N, K, seed=17, lo=-1.0, hi=1.0)
+    A[5, 17] = 0x7C00   # +Inf
+    A[40, 3] = 0xFC00   # -Inf
+    B[9, 61] = 0x7E00   # NaN
+    for beta in (0.0, 0.5):
+        C = run_tc(cuda, A, B, C0, 1.0, beta).view(np.float16)
+        R = oracle_mod.hgemm_ref(A, B, C0, 1.0, beta).view(np.float16)
+        assert np.array_equal(np.isnan(C), np.isnan(R))
+        inf = np.isinf(R)
+        assert np.array_equal(np.isinf(C), inf) and np.array_equal(np.sign(C[inf]), np.sign(R[inf]))
