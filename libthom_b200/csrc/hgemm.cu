@@ -85,7 +85,7 @@ struct Problem {
   int kblocks;           // ceil(K / 64)
   int vec;               // rows of C are 16-byte aligned: 16-byte loads and stores
   int group;             // pair-rows per raster group
-  int tma_store;         // beta == 0 and C 16-byte aligned: staged tiles written by TMA stores
+  int tma_store;         // C 16-byte aligned (p.vec): staged tiles written by TMA stores
 };
 
 // Pair tiles in groups of p.group pair-rows, column-major inside a group, so the CTAs resident at
@@ -141,14 +141,27 @@ __device__ __forceinline__ void store_row_chunk(const Problem& p, int64_t row, i
   }
 }
 
+// 32 FP16 values of C (one row, columns col0..col0+31) as four 16-byte words, zero past the matrix
+// edges. Needs p.vec (row pitch a multiple of 8 elements, so a word is wholly inside or outside).
+// Streaming loads: each value of C is read once, just before the TMA store that overwrites it.
+__device__ __forceinline__ void load_c_chunk(const Problem& p, int64_t row, int64_t col0, uint4 (&c)[4]) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    c[q] = make_uint4(0u, 0u, 0u, 0u);
+    if (row < p.M && col0 + q * 8 < p.N) c[q] = __ldcs(reinterpret_cast<const uint4*>(p.C + row * p.ldc + col0 + q * 8));
+  }
+}
+
 // One 32 x 32 box of the output through shared memory: each lane (one row) converts its 32
-// accumulators to FP16 pairs and writes them into the staging box in the 64-byte swizzled order of
-// the tensor map (16-byte chunk q of row r at r*64 + 16*(q ^ ((r >> 1) & 3)): four wavefronts per
-// 32-lane 16-byte store, the minimum), then one lane issues the TMA store. A warp alternates between
-// two boxes; a box is rewritten only after the store issued from it two chunks earlier has finished
-// reading it, so each store overlaps the next chunk's conversion.
+// accumulators (with beta != 0, alpha*acc + beta*C from the prefetched words `cin`) to FP16 pairs
+// and writes them into the staging box in the 64-byte swizzled order of the tensor map (16-byte
+// chunk q of row r at r*64 + 16*(q ^ ((r >> 1) & 3)): four wavefronts per 32-lane 16-byte store,
+// the minimum), then one lane issues the TMA store. A warp alternates between two boxes; a box is
+// rewritten only after the store issued from it two chunks earlier has finished reading it, so
+// each store overlaps the next chunk's conversion.
 __device__ __forceinline__ void store_box_tma(const CUtensorMap* tmC, uint8_t* box, int lane, float alpha,
-                                              const uint32_t (&v)[32], int x, int y, const Problem& p) {
+                                              const uint32_t (&v)[32], const uint4 (&cin)[4], int x, int y,
+                                              const Problem& p) {
   if (lane == 0) bulk_wait_group_read1();
   __syncwarp();
   uint8_t* row = box + lane * 64;
@@ -158,7 +171,11 @@ __device__ __forceinline__ void store_box_tma(const CUtensorMap* tmC, uint8_t* b
 #pragma unroll
     for (int h = 0; h < 4; ++h) {
       float lo = __uint_as_float(v[q * 8 + 2 * h]), hi = __uint_as_float(v[q * 8 + 2 * h + 1]);
-      if (alpha != 1.f) {
+      if (p.beta != 0.f) {
+        const uint32_t cw = h == 0 ? cin[q].x : h == 1 ? cin[q].y : h == 2 ? cin[q].z : cin[q].w;
+        lo = epilogue_value(lo, alpha, p.beta, cw & 0xffffu);
+        hi = epilogue_value(hi, alpha, p.beta, cw >> 16);
+      } else if (alpha != 1.f) {
         lo = __fmul_rn(alpha, lo);
         hi = __fmul_rn(alpha, hi);
       }
@@ -338,19 +355,29 @@ __global__ void __launch_bounds__(kThreads, 1)
       const uint32_t buf = iter % G::kAccBufs, use = iter / G::kAccBufs;
       int m0, n0;
       tile_coords(p, t, BN, &m0, &n0);
-      if (!mbar_wait_cluster(&acc_full[buf], use & 1, abort_flag, status, 65)) break;
-      tc_fence_after();
       const int64_t row = static_cast<int64_t>(m0) + static_cast<int64_t>(rank) * kBM + row_in_tile;
       const int col_base = colhalf * (BN / 2);
+      uint4 c_cur[4] = {}, c_next[4] = {}, c_ahead[4] = {};  // C of chunks c, c+1, c+2
+      if (p.tma_store && p.beta != 0.f) {
+        load_c_chunk(p, row, static_cast<int64_t>(n0) + col_base, c_cur);
+        if (kChunks > 1) load_c_chunk(p, row, static_cast<int64_t>(n0) + col_base + 32, c_next);
+      }
+      if (!mbar_wait_cluster(&acc_full[buf], use & 1, abort_flag, status, 65)) break;
+      tc_fence_after();
       const uint32_t lane_base =
           tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + buf * BN + static_cast<uint32_t>(col_base);
       if (p.tma_store) {
-        // beta == 0: 32-column boxes staged in shared memory and written by TMA stores (clipped at
-        // the matrix edges by the tensor map).
+        // 32-column boxes staged in shared memory and written by TMA stores (clipped at the matrix
+        // edges by the tensor map). With beta != 0 each lane reads its row's 32 values of C two
+        // chunks ahead of the one it converts, so the load latency (longer than one chunk's
+        // conversion) stays off the path from the TMEM reads (which free the accumulator buffer) to
+        // the stores.
         uint8_t* boxes = staging + (warp - 2) * kStoreBoxes * kStoreBytes;
         const int y = m0 + static_cast<int>(rank) * kBM + quarter * 32;
 #pragma unroll 1
         for (int c = 0; c < kChunks; ++c) {
+          if (c + 2 < kChunks && p.beta != 0.f)
+            load_c_chunk(p, row, static_cast<int64_t>(n0) + col_base + (c + 2) * 32, c_ahead);
           uint32_t v[32];
           tmem_ld_32x32b_x32(lane_base + static_cast<uint32_t>(c * 32), v);
           tmem_ld_wait();
@@ -359,7 +386,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             __syncwarp();
             if (lane == 0) mbar_arrive_cluster(acc_empty_r0[buf]);
           }
-          store_box_tma(&tmC, boxes + (c & 1) * kStoreBytes, lane, p.alpha, v, n0 + col_base + c * 32, y, p);
+          store_box_tma(&tmC, boxes + (c & 1) * kStoreBytes, lane, p.alpha, v, c_cur, n0 + col_base + c * 32, y, p);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            c_cur[q] = c_next[q];
+            c_next[q] = c_ahead[q];
+          }
         }
       } else {
 #pragma unroll 1
@@ -560,7 +592,7 @@ int run(const uint16_t* A, const uint16_t* B, uint16_t* C, int64_t M, int64_t N,
   p.kblocks = static_cast<int>((K + kBK - 1) / kBK);
   p.vec = ((reinterpret_cast<uintptr_t>(C) & 15) == 0 && (N % 8) == 0) ? 1 : 0;
   p.group = raster_group(bn);
-  p.tma_store = (p.vec && beta == 0.f) ? 1 : 0;
+  p.tma_store = p.vec;
   CUtensorMap tmC = tmA;  // not read unless p.tma_store
   if (p.tma_store)
     LT_TRY(make_tmap_2d(&tmC, C, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, static_cast<uint64_t>(M),
