@@ -1,5 +1,6 @@
 // dgemm_fp64.cu — host launchers and configuration registry of the native FP64 DGEMM.
 #include <algorithm>
+#include <cstdint>
 #include <mutex>
 #include <vector>
 
@@ -155,8 +156,39 @@ int heuristic_config_for(int64_t M, int64_t N, int sm_count, bool tma) {
   return best >= 0 ? best : kNumConfigs - 1;
 }
 
-// ---- grouped launches (cp.async staging: problems have arbitrary shapes and alignment) ----
+// ---- grouped launches ----
+// cp.async configurations stage tiles of any shape and alignment. TMA configurations read A and B
+// through per-problem tensor maps; an operand whose base is not 16-byte aligned or whose row pitch
+// (K for A, N for B) is odd cannot be described by one, so each run first copies it into a
+// plan-owned buffer with an even pitch (the plan holds pointers, not values, so the copy is part
+// of every run; the padding column is never read: the map's extent is the operand's own).
+struct PackJob {
+  const double* src;  // rows x cols, row pitch cols
+  double* dst;        // rows x cols, row pitch dpitch
+  int64_t rows, cols, dpitch;
+  int64_t row0;  // first row of this job in the launch's row numbering
+};
+
 namespace {
+
+// One warp per row (found by binary search over row0), consecutive lanes on consecutive doubles.
+__global__ void pack_rows_kernel(const PackJob* __restrict__ jobs, int njobs, int64_t total_rows) {
+  const int64_t wpb = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = blockIdx.x * wpb + (threadIdx.x >> 5); r < total_rows; r += gridDim.x * wpb) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (jobs[mid].row0 <= r) lo = mid;
+      else hi = mid - 1;
+    }
+    const PackJob& j = jobs[lo];
+    const int64_t row = r - j.row0;
+    const double* __restrict__ src = j.src + row * j.cols;
+    double* __restrict__ dst = j.dst + row * j.dpitch;
+    for (int64_t c = lane; c < j.cols; c += 32) dst[c] = src[c];
+  }
+}
 
 template <class Cfg>
 int launch_grouped(const GroupProblem* problems, const GroupTile* tiles, int64_t ntiles, cudaStream_t stream,
@@ -189,17 +221,26 @@ struct GroupedEntry {
   const char* name;
   GroupedFn fn;
   int bm, bn;
+  bool tma;
 };
 const GroupedEntry kGrouped[] = {
-    {"grouped_cpa_128x64_s6", launch_grouped<Config<128, 64, 6, false>>, 128, 64},
-    {"grouped_cpa_64x64_s6", launch_grouped<Config<64, 64, 6, false>>, 64, 64},
-    {"grouped_cpa_64x32_s6", launch_grouped<Config<64, 32, 6, false>>, 64, 32},
-    {"grouped_cpa_32x32_s6", launch_grouped<Config<32, 32, 6, false>>, 32, 32},
+    {"grouped_cpa_128x64_s6", launch_grouped<Config<128, 64, 6, false>>, 128, 64, false},
+    {"grouped_cpa_64x64_s6", launch_grouped<Config<64, 64, 6, false>>, 64, 64, false},
+    {"grouped_cpa_64x32_s6", launch_grouped<Config<64, 32, 6, false>>, 64, 32, false},
+    {"grouped_cpa_32x32_s6", launch_grouped<Config<32, 32, 6, false>>, 32, 32, false},
     // shallower rings leave room for more CTAs per SM (more warps to hide load latency)
-    {"grouped_cpa_64x64_s3", launch_grouped<Config<64, 64, 3, false>>, 64, 64},
-    {"grouped_cpa_64x32_s3", launch_grouped<Config<64, 32, 3, false>>, 64, 32},
-    {"grouped_cpa_32x64_s3", launch_grouped<Config<32, 64, 3, false>>, 32, 64},
-    {"grouped_cpa_32x32_s3", launch_grouped<Config<32, 32, 3, false>>, 32, 32},
+    {"grouped_cpa_64x64_s3", launch_grouped<Config<64, 64, 3, false>>, 64, 64, false},
+    {"grouped_cpa_64x32_s3", launch_grouped<Config<64, 32, 3, false>>, 64, 32, false},
+    {"grouped_cpa_32x64_s3", launch_grouped<Config<32, 64, 3, false>>, 32, 64, false},
+    {"grouped_cpa_32x32_s3", launch_grouped<Config<32, 32, 3, false>>, 32, 32, false},
+    {"grouped_tma_128x64_s6", launch_grouped<Config<128, 64, 6, true>>, 128, 64, true},
+    {"grouped_tma_64x64_s8", launch_grouped<Config<64, 64, 8, true>>, 64, 64, true},
+    {"grouped_tma_64x32_s8", launch_grouped<Config<64, 32, 8, true>>, 64, 32, true},
+    {"grouped_tma_32x64_s8", launch_grouped<Config<32, 64, 8, true>>, 32, 64, true},
+    {"grouped_tma_32x32_s8", launch_grouped<Config<32, 32, 8, true>>, 32, 32, true},
+    {"grouped_tma_64x64_s4", launch_grouped<Config<64, 64, 4, true>>, 64, 64, true},
+    {"grouped_tma_32x64_s4", launch_grouped<Config<32, 64, 4, true>>, 32, 64, true},
+    {"grouped_tma_32x32_s4", launch_grouped<Config<32, 32, 4, true>>, 32, 32, true},
 };
 constexpr int kNumGrouped = static_cast<int>(sizeof(kGrouped) / sizeof(kGrouped[0]));
 
@@ -211,6 +252,11 @@ struct GroupedFp64 {
   GroupProblem* d_problems = nullptr;
   GroupTile* d_tiles = nullptr;
   int64_t ntiles = 0;
+  // TMA configurations: operands copied to an even pitch at the start of each run
+  void* pack_buf = nullptr;
+  PackJob* d_pack = nullptr;
+  int npack = 0;
+  int64_t pack_rows = 0;
 };
 
 int grouped_num_configs() { return kNumGrouped; }
@@ -223,7 +269,7 @@ int grouped_create(const lt_gemm_problem* problems, int count, int cfg, GroupedF
   std::vector<int> order(count);
   for (int i = 0; i < count; ++i) {
     const lt_gemm_problem& p = problems[i];
-    probs[i] = GroupProblem{p.A, p.B, p.C, p.M, p.N, p.K, p.alpha, p.beta};
+    probs[i] = GroupProblem{p.A, p.B, p.C, p.M, p.N, p.K, p.alpha, p.beta, nullptr, nullptr};
     order[i] = i;
   }
   // Longest-K problems first: with a static round-robin over the CTAs this balances the work.
@@ -237,19 +283,88 @@ int grouped_create(const lt_gemm_problem* problems, int count, int cfg, GroupedF
   auto* G = new GroupedFp64();
   G->cfg = cfg;
   G->ntiles = static_cast<int64_t>(tiles.size());
+  const bool tma = kGrouped[cfg].tma;
+  // TMA: where each problem's A and B are read from (the caller's array or a packed copy).
+  struct Operand {
+    const double* src;
+    int64_t rows, cols, pitch;
+    size_t pack_off;  // SIZE_MAX: read in place
+  };
+  std::vector<Operand> ops;
+  std::vector<PackJob> packs;
+  size_t pack_bytes = 0;
+  if (tma) {
+    ops.resize(2 * static_cast<size_t>(count));
+    for (int i = 0; i < count; ++i) {
+      const lt_gemm_problem& p = problems[i];
+      const Operand in[2] = {{p.A, p.M, p.K, p.K, SIZE_MAX}, {p.B, p.K, p.N, p.N, SIZE_MAX}};
+      for (int o = 0; o < 2; ++o) {
+        Operand op = in[o];
+        const bool used = p.M > 0 && p.N > 0 && p.K > 0;
+        if (used && (((reinterpret_cast<uintptr_t>(op.src) & 15) != 0) || (op.cols & 1) != 0)) {
+          op.pitch = (op.cols + 1) & ~int64_t(1);
+          op.pack_off = pack_bytes;
+          pack_bytes += (static_cast<size_t>(op.rows * op.pitch) * sizeof(double) + 255) / 256 * 256;
+          packs.push_back(PackJob{op.src, nullptr, op.rows, op.cols, op.pitch, G->pack_rows});
+          G->pack_rows += op.rows;
+        }
+        ops[2 * i + o] = op;
+      }
+    }
+  }
   const size_t pb = (sizeof(GroupProblem) * count + 255) / 256 * 256;
+  const size_t mb = tma ? (sizeof(CUtensorMap) * 2 * count + 255) / 256 * 256 : 0;
+  const size_t jb = (sizeof(PackJob) * packs.size() + 255) / 256 * 256;
   const size_t tb = sizeof(GroupTile) * (tiles.size() + 1);
-  cudaError_t e = cudaMalloc(&G->dev, pb + tb);
+  int rc = LT_OK;
+  cudaError_t e = cudaMalloc(&G->dev, pb + mb + jb + tb);
+  if (e == cudaSuccess && pack_bytes > 0) e = cudaMalloc(&G->pack_buf, pack_bytes);
   if (e == cudaSuccess) {
-    G->d_problems = static_cast<GroupProblem*>(G->dev);
-    G->d_tiles = reinterpret_cast<GroupTile*>(static_cast<uint8_t*>(G->dev) + pb);
-    e = cudaMemcpy(G->d_problems, probs.data(), sizeof(GroupProblem) * count, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !tiles.empty())
+    uint8_t* base = static_cast<uint8_t*>(G->dev);
+    G->d_problems = reinterpret_cast<GroupProblem*>(base);
+    CUtensorMap* d_maps = reinterpret_cast<CUtensorMap*>(base + pb);
+    G->d_pack = reinterpret_cast<PackJob*>(base + pb + mb);
+    G->d_tiles = reinterpret_cast<GroupTile*>(base + pb + mb + jb);
+    G->npack = static_cast<int>(packs.size());
+    if (tma) {
+      std::vector<CUtensorMap> maps(2 * static_cast<size_t>(count));
+      int j = 0;
+      for (int i = 0; i < count && rc == LT_OK; ++i) {
+        const lt_gemm_problem& p = problems[i];
+        if (p.M <= 0 || p.N <= 0 || p.K <= 0) continue;  // no loads: the maps stay null
+        const double* src[2];
+        for (int o = 0; o < 2; ++o) {
+          const Operand& op = ops[2 * i + o];
+          src[o] = op.src;
+          if (op.pack_off != SIZE_MAX) {
+            src[o] = reinterpret_cast<const double*>(static_cast<uint8_t*>(G->pack_buf) + op.pack_off);
+            packs[j++].dst = const_cast<double*>(src[o]);
+          }
+        }
+        const Operand &a = ops[2 * i], &b = ops[2 * i + 1];
+        rc = make_tmap_2d(&maps[2 * i], src[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, static_cast<uint64_t>(a.rows),
+                          static_cast<uint64_t>(a.cols), static_cast<uint64_t>(a.pitch) * 8, bm, 16);
+        if (rc == LT_OK)
+          rc = make_tmap_2d(&maps[2 * i + 1], src[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8,
+                            static_cast<uint64_t>(b.rows), static_cast<uint64_t>(b.cols),
+                            static_cast<uint64_t>(b.pitch) * 8, 16, 16);
+        probs[i].tmA = d_maps + 2 * i;
+        probs[i].tmB = d_maps + 2 * i + 1;
+      }
+      if (rc == LT_OK) e = cudaMemcpy(d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice);
+      if (rc == LT_OK && e == cudaSuccess && !packs.empty())
+        e = cudaMemcpy(G->d_pack, packs.data(), sizeof(PackJob) * packs.size(), cudaMemcpyHostToDevice);
+    }
+    if (rc == LT_OK && e == cudaSuccess)
+      e = cudaMemcpy(G->d_problems, probs.data(), sizeof(GroupProblem) * count, cudaMemcpyHostToDevice);
+    if (rc == LT_OK && e == cudaSuccess && !tiles.empty())
       e = cudaMemcpy(G->d_tiles, tiles.data(), sizeof(GroupTile) * tiles.size(), cudaMemcpyHostToDevice);
   }
-  if (e != cudaSuccess) {
+  if (rc != LT_OK || e != cudaSuccess) {
+    cudaFree(G->pack_buf);
     cudaFree(G->dev);
     delete G;
+    if (rc != LT_OK) return rc;
     return set_error(LT_ERR_NO_MEMORY, "grouped FP64 tables: %s", cudaGetErrorString(e));
   }
   *out = G;
@@ -259,6 +374,12 @@ int grouped_create(const lt_gemm_problem* problems, int count, int cfg, GroupedF
 int grouped_run(const GroupedFp64* G, cudaStream_t stream) {
   DeviceContext* ctx = context();
   if (ctx == nullptr) return last_error();
+  if (G->npack > 0) {
+    int64_t blocks = (G->pack_rows + 7) / 8;
+    if (blocks > 8 * static_cast<int64_t>(ctx->sm_count)) blocks = 8 * static_cast<int64_t>(ctx->sm_count);
+    pack_rows_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(G->d_pack, G->npack, G->pack_rows);
+    LT_CUDA_TRY(cudaGetLastError());
+  }
   return kGrouped[G->cfg].fn(G->d_problems, G->d_tiles, G->ntiles, stream, ctx, false);
 }
 
@@ -271,6 +392,7 @@ int grouped_prepare(const GroupedFp64* G) {
 
 void grouped_destroy(GroupedFp64* G) {
   if (G == nullptr) return;
+  cudaFree(G->pack_buf);
   cudaFree(G->dev);
   delete G;
 }

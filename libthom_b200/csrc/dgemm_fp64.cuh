@@ -116,6 +116,8 @@ struct Job {
   int kb0, kb1;
   double* W;
   int64_t lda, ldb, ldc;
+  const CUtensorMap* tmA;  // TMA configurations: the tensor maps of this job's A and B
+  const CUtensorMap* tmB;
 };
 
 // Tiles of a single problem, walked in grouped raster order.
@@ -125,6 +127,8 @@ template <class Cfg>
 struct SingleSource {
   Params p;
   int64_t tiles_m, tiles_n;
+  const CUtensorMap* tmA;
+  const CUtensorMap* tmB;
   __device__ int64_t count() const { return tiles_m * tiles_n * p.splits; }
   __device__ Job get(int64_t u) const {
     const int64_t tiles = tiles_m * tiles_n;
@@ -137,18 +141,22 @@ struct SingleSource {
     const int kb1 = kb0 + per < nkb ? kb0 + per : nkb;
     double* w = p.splits > 1 ? p.W + sp * p.M * p.N : nullptr;
     return Job{p.A, p.B, p.C, p.M, p.N, p.K, p.alpha, p.beta, tm * Cfg::BM, tn * Cfg::BN, kb0, kb1, w,
-               p.lda, p.ldb, p.ldc};
+               p.lda, p.ldb, p.ldc, tmA, tmB};
   }
 };
 
 // Grouped launch: a device table of problems and a tile list (sorted by decreasing K on the host
-// so that the static round-robin over CTAs hands out the expensive tiles first).
+// so that the static round-robin over CTAs hands out the expensive tiles first). TMA
+// configurations read A and B through per-problem tensor maps held in device memory (written by
+// the host before any launch, null when K == 0).
 struct GroupProblem {
   const double* A;
   const double* B;
   double* C;
   int64_t M, N, K;
   double alpha, beta;
+  const CUtensorMap* tmA;
+  const CUtensorMap* tmB;
 };
 struct GroupTile {
   int problem;
@@ -165,7 +173,8 @@ struct GroupedSource {
     const GroupProblem& pr = problems[gt.problem];
     return Job{pr.A,  pr.B,  pr.C,  pr.M, pr.N,
                pr.K,  pr.alpha, pr.beta, gt.m0, gt.n0,
-               0,     static_cast<int>((pr.K + 15) / 16), nullptr, pr.K, pr.N, pr.N};
+               0,     static_cast<int>((pr.K + 15) / 16), nullptr, pr.K, pr.N, pr.N,
+               pr.tmA, pr.tmB};
   }
 };
 
@@ -195,7 +204,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
     // ------------------------------- producer warp(s) -------------------------------
     const int pt = (warp - Cfg::CONSUMERS) * 32 + lane;  // producer thread index
     constexpr int kPT = 32 * Cfg::PRODUCERS;
-    if (Cfg::kTMA) {
+    if (Cfg::kTMA && tmA != nullptr) {  // single problem: the maps are kernel parameters
       if (lane == 0) {
         tma_prefetch_desc(tmA);
         tma_prefetch_desc(tmB);
@@ -215,10 +224,10 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
         if (Cfg::kTMA) {
           if (lane == 0) {
             mbar_arrive_expect_tx(&full[stage], Cfg::STAGE_BYTES);
-            tma_load_2d(sa, tmA, &full[stage], k0, static_cast<int>(m0));
+            tma_load_2d(sa, J.tmA, &full[stage], k0, static_cast<int>(m0));
 #pragma unroll
             for (int j = 0; j < Cfg::BN / 16; ++j)
-              tma_load_2d(sb + j * 2048, tmB, &full[stage], static_cast<int>(n0) + 16 * j, k0);
+              tma_load_2d(sb + j * 2048, J.tmB, &full[stage], static_cast<int>(n0) + 16 * j, k0);
           }
         } else {
           // A: BM rows x 16 doubles as 16-byte pairs (one shared-memory chunk each): one 16-byte
@@ -269,6 +278,17 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
     bool ok = true;
     for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
       const Job J = src.get(t);
+      if (J.W == nullptr && J.beta != 0.0) {
+        // The C block this warp's epilogue reads (32 rows of 32 doubles, one row per lane) is
+        // fetched into L2 while the main loop runs, so the epilogue waits for L2, not DRAM.
+        const int64_t row = J.m0 + wm * Cfg::WM + lane, col = J.n0 + wn * Cfg::WN;
+        if (row < J.M && col < J.N) {
+          const double* cp = J.C + row * J.ldc + col;
+          prefetch_l2(cp);
+          if (col + 16 < J.N) prefetch_l2(cp + 16);
+          if (col + 31 < J.N) prefetch_l2(cp + 31);
+        }
+      }
       double acc[2][4][4];
 #pragma unroll
       for (int i = 0; i < 2; ++i)
@@ -336,8 +356,33 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
         continue;
       }
       const bool vec = ((J.ldc & 1) == 0) && ((reinterpret_cast<uintptr_t>(J.C) & 15) == 0);
+      const bool use_c = J.beta != 0.0;
+      // Per 16-row half of the warp's block, every C0 value is loaded before the first store: the
+      // stores go through the same pointer, so a load written after one could not be moved ahead
+      // of it, and each 16-byte pair would wait for its own round trip to memory.
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
+        double c0[2][4][2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int64_t row = m0 + i * 16 + g + 8 * h;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int64_t col = n0 + j * 8 + 2 * tq;
+            c0[h][j][0] = c0[h][j][1] = 0.0;
+            if (use_c && row < J.M) {
+              const double* cp = J.C + row * J.ldc + col;
+              if (vec && col + 1 < J.N) {
+                const double2 c = *reinterpret_cast<const double2*>(cp);
+                c0[h][j][0] = c.x;
+                c0[h][j][1] = c.y;
+              } else {
+                if (col < J.N) c0[h][j][0] = cp[0];
+                if (col + 1 < J.N) c0[h][j][1] = cp[1];
+              }
+            }
+          }
+        }
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int64_t row = m0 + i * 16 + g + 8 * h;
@@ -345,22 +390,15 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             const int64_t col = n0 + j * 8 + 2 * tq;
-            double v0 = acc[i][j][2 * h], v1 = acc[i][j][2 * h + 1];
+            const double v0 = acc[i][j][2 * h], v1 = acc[i][j][2 * h + 1];
+            const double o0 = use_c ? fma(J.alpha, v0, J.beta * c0[h][j][0]) : J.alpha * v0;
+            const double o1 = use_c ? fma(J.alpha, v1, J.beta * c0[h][j][1]) : J.alpha * v1;
             double* cp = J.C + row * J.ldc + col;
             if (vec && col + 1 < J.N) {
-              double2 o;
-              if (J.beta != 0.0) {
-                double2 c0 = *reinterpret_cast<const double2*>(cp);
-                o.x = fma(J.alpha, v0, J.beta * c0.x);
-                o.y = fma(J.alpha, v1, J.beta * c0.y);
-              } else {
-                o.x = J.alpha * v0;
-                o.y = J.alpha * v1;
-              }
-              *reinterpret_cast<double2*>(cp) = o;
+              *reinterpret_cast<double2*>(cp) = make_double2(o0, o1);
             } else {
-              if (col < J.N) cp[0] = (J.beta != 0.0) ? fma(J.alpha, v0, J.beta * cp[0]) : J.alpha * v0;
-              if (col + 1 < J.N) cp[1] = (J.beta != 0.0) ? fma(J.alpha, v1, J.beta * cp[1]) : J.alpha * v1;
+              if (col < J.N) cp[0] = o0;
+              if (col + 1 < J.N) cp[1] = o1;
             }
           }
         }
@@ -372,7 +410,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
 template <class Cfg>
 __global__ void __launch_bounds__(Cfg::THREADS, 1)
     dgemm_fp64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p) {
-  SingleSource<Cfg> src{p, (p.M + Cfg::BM - 1) / Cfg::BM, (p.N + Cfg::BN - 1) / Cfg::BN};
+  SingleSource<Cfg> src{p, (p.M + Cfg::BM - 1) / Cfg::BM, (p.N + Cfg::BN - 1) / Cfg::BN, &tmA, &tmB};
   gemm_body<Cfg>(&tmA, &tmB, src, p.status);
 }
 
@@ -392,7 +430,6 @@ __global__ void splitk_reduce_kernel(const double* __restrict__ W, double* __res
 template <class Cfg>
 __global__ void __launch_bounds__(Cfg::THREADS, 1)
     dgemm_fp64_grouped_kernel(GroupedSource src, DeviceStatus* status) {
-  static_assert(!Cfg::kTMA, "grouped launches stage tiles with cp.async");
   gemm_body<Cfg>(nullptr, nullptr, src, status);
 }
 

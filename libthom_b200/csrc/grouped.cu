@@ -130,6 +130,12 @@ int run_fp64(const fp64::GroupedFp64* big, const fp64::GroupedFp64* small, cudaS
   return LT_OK;
 }
 
+int grouped_config_index(const char* name) {
+  for (int i = 0; i < fp64::grouped_num_configs(); ++i)
+    if (strcmp(fp64::grouped_config_name(i), name) == 0) return i;
+  return 0;
+}
+
 int build_fp64(lt_grouped_plan* plan, int cfg, int cfg_small = -1, int64_t split_mn = 0) {
   fp64::GroupedFp64 *g = nullptr, *gs = nullptr;
   LT_TRY(create_fp64(plan->problems, cfg, cfg_small, split_mn, &g, &gs));
@@ -180,8 +186,11 @@ int lt_grouped_plan_create(const lt_gemm_problem* problems, int count, int form,
     p->flops += 2.0 * static_cast<double>(q.M) * static_cast<double>(q.N) * static_cast<double>(q.K);
   int rc;
   if (form == LT_FORM_FP64) {
-    // Without a tuning run: 64x64 tiles suit problems of a few hundred rows and columns.
-    rc = lt::build_fp64(p, 1);
+    // Without a tuning run: problems with min(M, N) >= 96 on 128x64 TMA tiles, the rest on 32x32
+    // cp.async tiles with a shallow ring (many CTAs per SM), concurrently: the tuner's choice on
+    // 512 problems with dimensions log-uniform in [32, 1024].
+    rc = lt::build_fp64(p, lt::grouped_config_index("grouped_tma_128x64_s6"),
+                        lt::grouped_config_index("grouped_cpa_32x32_s3"), 96);
   } else {
     rc = lt::ozaki::grouped_create(problems, count, slices, &p->oz);
   }

@@ -95,6 +95,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
 // TMA (tiled bulk tensor copies, global -> shared, completion on an mbarrier); each CTA loads only
 // into its own shared memory.
 // ---------------------------------------------------------------------------------------------
+// Brings the 128-byte line holding `p` into L2 (no register result, no wait).
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<uint64_t>(p)));
+}
 __device__ __forceinline__ void tma_prefetch_desc(const void* desc) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(desc)) : "memory");
 }

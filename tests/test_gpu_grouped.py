@@ -113,6 +113,73 @@ def test_grouped_fp64_two_size_classes(cuda, oracle_mod, graph):
         assert err[0] <= fp64_bound(A.shape[1]), (A.shape, B.shape, err)
 
 
+def upload_offset(torch, probs, offset):
+    """`upload` with every matrix starting `offset` doubles into its own allocation (offset 1: the
+    base is 8- but not 16-byte aligned)."""
+    import libthom_b200 as lt
+
+    def place(a):
+        buf = torch.zeros(a.size + offset, dtype=torch.float64, device="cuda")
+        view = buf[offset:]
+        view.copy_(torch.from_numpy(np.ascontiguousarray(a).ravel()))
+        return view.view(a.shape)
+
+    dev = []
+    table = (lt.GemmProblem * len(probs))()
+    for i, (A, B, C0, alpha, beta) in enumerate(probs):
+        dA, dB, dC = place(A), place(B), place(C0)
+        dev.append((dA, dB, dC))
+        ptr = lambda t: t.data_ptr() if t.numel() else None
+        table[i] = lt.GemmProblem(A.shape[0], B.shape[1], A.shape[1], ptr(dA), ptr(dB), ptr(dC), alpha, beta)
+    return dev, table
+
+
+@pytest.mark.parametrize("offset", [0, 1])
+def test_grouped_fp64_every_config(cuda, oracle_mod, offset):
+    """Every grouped tile configuration (cp.async and TMA staging) on odd and even K and N, bases
+    that are not 16-byte aligned (offset 1), M below the tile height and K = 0. The TMA
+    configurations copy the operands that no tensor map can describe (odd pitch or base) into even
+    pitches on every run: after the first graph replay A is doubled in place and the second replay
+    must follow the new values."""
+    import libthom_b200 as lt
+
+    torch = cuda
+    L = lt.lib()
+    shapes = [(5, 7, 9), (64, 64, 64), (130, 66, 33), (97, 128, 200), (33, 31, 0), (200, 3, 150), (1, 1, 1),
+              (128, 64, 17), (70, 90, 48)]
+    probs = []
+    for i, (M, N, K) in enumerate(shapes):
+        A, B, C0 = oracle_mod.make_problem(M, N, K, phi=2, seed=4000 + i)
+        probs.append((A, B, C0, 1.5 if i % 2 else 1.0, 0.5 if i % 3 else 0.0))
+    names = [L.lt_grouped_config_name(i).decode() for i in range(L.lt_grouped_num_configs())]
+    assert any("tma" in n for n in names) and any("cpa" in n for n in names)
+    for cfg, cname in enumerate(names):
+        dev, table = upload_offset(torch, probs, offset)
+        plan = ctypes.c_void_p()
+        lt.check(L.lt_grouped_plan_create(table, len(probs), lt.LT_FORM_FP64, 0, ctypes.byref(plan)))
+        try:
+            lt.check(L.lt_grouped_plan_set_fp64(plan, cfg, -1, 0))
+            lt.check(L.lt_grouped_plan_run_graph(plan, None))
+            torch.cuda.synchronize()
+            lt.device_status()
+            for (A, B, C0, alpha, beta), (_, _, dC) in zip(probs, dev):
+                Cref, den = oracle_mod.dot2_rows(A, B, C0, alpha, beta)
+                err = oracle_mod.componentwise_error(dC.cpu().numpy(), Cref, den)
+                assert err[0] <= fp64_bound(A.shape[1]), (cname, A.shape, B.shape, err)
+            for (A, B, C0, alpha, beta), (dA, _, dC) in zip(probs, dev):
+                dA.mul_(2.0)
+                dC.copy_(torch.from_numpy(C0))
+            lt.check(L.lt_grouped_plan_run_graph(plan, None))
+            torch.cuda.synchronize()
+            lt.device_status()
+            for (A, B, C0, alpha, beta), (_, _, dC) in zip(probs, dev):
+                Cref, den = oracle_mod.dot2_rows(2.0 * A, B, C0, alpha, beta)
+                err = oracle_mod.componentwise_error(dC.cpu().numpy(), Cref, den)
+                assert err[0] <= fp64_bound(A.shape[1]), (cname, "after A changed", A.shape, B.shape, err)
+        finally:
+            L.lt_grouped_plan_destroy(plan)
+
+
 @pytest.mark.parametrize("graph", [False, True])
 def test_grouped_ozaki_bit_exact(cuda, oracle_mod, graph):
     import libthom_b200 as lt
