@@ -62,6 +62,10 @@ float dgemm_ozaki10(const double* A, const double* B, double* C, size_t M, size_
  * the target tolerance is lt_set_ozaki_tolerance() (default 1e-15). */
 float dgemm_ozaki_auto(const double* A, const double* B, double* C, size_t M, size_t N, size_t K,
                        double alpha, double beta);
+/* DGEMM in whichever form this GPU runs faster for the shape: native FP64 or Ozaki with the
+ * learned selector's slice count (lt_dgemm_auto below). No reference counterpart. */
+float dgemm_auto(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha,
+                 double beta);
 /* The reference's cuBLAS baseline, same call (routines/dgemm/dgemm_cublas_tc.cu:4-33):
  * cublasGemmEx, CUBLAS_COMPUTE_64F, row-major through the transposition trick. */
 float dgemm_cublas_tc(const double* A, const double* B, double* C, size_t M, size_t N, size_t K,
@@ -131,6 +135,20 @@ int lt_dgemm_ozaki_host(const double* A, const double* B, double* C, int64_t M, 
 #define LT_OZAKI_NOALLOC_BYTES (32ll << 20)
 int lt_dgemm_ozaki_noalloc(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
                            double alpha, double beta, int slices, void* stream);
+
+/* ---- automatic form ------------------------------------------------------------------------- */
+/* C = alpha*A*B + beta*C at FP64 accuracy in the faster form for this call: the learned selector
+ * picks the slice count s that meets lt_set_ozaki_tolerance() (default 1e-15), then a cost model of
+ * this GPU (lt_dgemm_estimate_ms) compares Ozaki with s slices against native FP64. Shapes where
+ * native FP64 wins even against s = 3 (small, or HBM-bound like a 65536 x 64 x 4096 product) skip
+ * the selector. Results are bit-identical to lt_dgemm_fp64, or to lt_dgemm_ozaki with the chosen s.
+ * `form` (LT_FORM_FP64 / LT_FORM_OZAKI) and `slices` (0 for FP64) report the choice when non-NULL.
+ * Stream-ordered except that running the selector reads its answer on the host. */
+int lt_dgemm_auto(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
+                  double beta, int* form, int* slices, void* stream);
+/* The cost model's predicted milliseconds for one DGEMM on a B200 (host arithmetic only, no GPU
+ * needed); -1 for an unknown form or a slice count outside 1..12. */
+double lt_dgemm_estimate_ms(int form, int64_t M, int64_t N, int64_t K, int slices);
 
 /* ---- grouped / batched DGEMM (the `dgemmb` routine) ----------------------------------------- */
 typedef struct lt_gemm_problem {

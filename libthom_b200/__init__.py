@@ -7,7 +7,8 @@ is present, calls raise — there is no CPU fallback.
 
 Implementation registry (the reference's ``dgemmImpls``, routines/dgemm/dgemm.cpp:36-68):
 ``tc100`` (native FP64 tensor cores), ``ozaki3`` .. ``ozaki10`` (INT8 Ozaki slices),
-``ozaki_auto`` (learned slice selector) and ``cublas_tc`` (the reference's cuBLAS baseline).
+``ozaki_auto`` (learned slice selector), ``auto`` (native FP64 or Ozaki, whichever is faster for the
+shape) and ``cublas_tc`` (the reference's cuBLAS baseline).
 """
 from __future__ import annotations
 
@@ -41,7 +42,7 @@ LT_SEL_CLASSES = 8
 LT_SEL_PARAMS = (LT_SEL_FEATURES * LT_SEL_HIDDEN + LT_SEL_HIDDEN + LT_SEL_HIDDEN * LT_SEL_HIDDEN +
                  LT_SEL_HIDDEN + LT_SEL_HIDDEN * LT_SEL_CLASSES + LT_SEL_CLASSES)
 
-IMPLS = ["tc100"] + [f"ozaki{s}" for s in range(3, 11)] + ["ozaki_auto", "cublas_tc"]
+IMPLS = ["tc100"] + [f"ozaki{s}" for s in range(3, 11)] + ["ozaki_auto", "auto", "cublas_tc"]
 
 _c = ctypes
 _vp, _i64, _i32, _f64, _f32, _sz = _c.c_void_p, _c.c_int64, _c.c_int, _c.c_double, _c.c_float, _c.c_size_t
@@ -80,6 +81,9 @@ SIGNATURES = {
     "dgemm_ozaki6": (_f32, _REF), "dgemm_ozaki7": (_f32, _REF), "dgemm_ozaki8": (_f32, _REF),
     "dgemm_ozaki9": (_f32, _REF), "dgemm_ozaki10": (_f32, _REF),
     "dgemm_ozaki_auto": (_f32, _REF),
+    "dgemm_auto": (_f32, _REF),
+    "lt_dgemm_auto": (_i32, _GEMM + [_c.POINTER(_i32), _c.POINTER(_i32), _vp]),
+    "lt_dgemm_estimate_ms": (_f64, [_i32, _i64, _i64, _i64, _i32]),
     "dgemm_cublas_tc": (_f32, _REF),
     "lt_dgemm_fp64": (_i32, _GEMM + [_vp]),
     "lt_dgemm_fp64_config": (_i32, _GEMM + [_i32, _vp]),
@@ -221,6 +225,19 @@ def ozaki_product(C, M, N, K, alpha, beta, slices, workspace, stream=None) -> No
 
 def dgemm_cublas(A, B, C, M, N, K, alpha=1.0, beta=0.0, stream=None) -> None:
     check(lib().lt_dgemm_cublas(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, _stream(stream)))
+
+
+def dgemm_auto(A, B, C, M, N, K, alpha=1.0, beta=0.0, stream=None) -> tuple[int, int]:
+    """lt_dgemm_auto: FP64-accurate DGEMM in the faster form; returns (form, slices) as chosen."""
+    form, slices = ctypes.c_int(-1), ctypes.c_int(-1)
+    check(lib().lt_dgemm_auto(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, ctypes.byref(form),
+                              ctypes.byref(slices), _stream(stream)))
+    return form.value, slices.value
+
+
+def estimate_ms(form: int, M: int, N: int, K: int, slices: int = 0) -> float:
+    """The auto form's cost model (host arithmetic only)."""
+    return lib().lt_dgemm_estimate_ms(form, M, N, K, slices)
 
 
 def ozaki_workspace_size(M, N, K, slices) -> int:

@@ -13,6 +13,7 @@
 // written to a buffer), then a fixed-order reduction over the batch, so gradients are deterministic.
 #include <dlfcn.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -382,6 +383,105 @@ float dgemm_ozaki_auto(const double* A, const double* B, double* C, size_t M, si
   if (rc == LT_OK) rc = lt_check_device_status();
   if (rc != LT_OK) {
     fprintf(stderr, "Kernel launch error (ozaki_auto): %s: %s\n", lt_error_string(rc), lt::last_message());
+    lt::set_error(rc, "%s", lt::last_message());
+  }
+  return ms;
+}
+
+}  // extern "C"
+
+// ---- automatic form: native FP64 or Ozaki, whichever this GPU runs faster (no reference counterpart)
+namespace lt {
+namespace sel {
+
+// Predicted milliseconds of one DGEMM in `form` on a B200 (148 SMs), from rates measured on it.
+// FP64: 128x64 tiles at 34.4 TF/s over the padded tile work; with fewer than 148 tiles the K split
+// (up to 4 ranges) spreads them over more SMs. Ozaki with s slices: exponent passes at 6.2 TB/s
+// (8 bytes per element of A and B), splits at 5.1 TB/s (8 bytes read + s written), then the
+// s(s+1)/2 INT8 slice products at 3.2 POP/s on 256x128 CTA-pair tiles (128x128 tiles when M <= 128)
+// in whole waves, or the slice bytes at 6.0 TB/s when that is longer. Fixed costs: 5 us (FP64),
+// 30 us (Ozaki: five launches). Predicted (measured) Ozaki s = 7 / FP64: 8192^3 10.3 (10.0-10.6) /
+// 32.0 (32.0) ms; 65536x64x4096 1.86 (1.87) / 1.00 (1.04); 2048x2048x65536 6.7 (6.2) / 16.0 (16.0).
+double estimate_ms(int form, int64_t M, int64_t N, int64_t K, int s) {
+  if (M <= 0 || N <= 0 || K <= 0) return 0.0;
+  auto cdiv = [](int64_t a, int64_t b) { return static_cast<double>((a + b - 1) / b); };
+  constexpr double kSms = 148.0;
+  if (form == LT_FORM_FP64) {
+    const double tiles = cdiv(M, 128) * cdiv(N, 64);
+    const double work = 2.0 * tiles * 128.0 * 64.0 * cdiv(K, 16) * 16.0;
+    const double busy = std::min(1.0, 4.0 * tiles / kSms);
+    return work / (34.4e12 * busy) * 1e3 + 0.005;
+  }
+  const bool pair = M > 128;
+  const double tm = pair ? 256.0 : 128.0, slots = pair ? kSms / 2 : kSms;
+  const double tiles = cdiv(M, static_cast<int64_t>(tm)) * cdiv(N, 128);
+  const double waves = std::ceil(tiles / slots);
+  const double products = s * (s + 1) / 2.0;
+  const double t_tile = products * 2.0 * tm * 128.0 * cdiv(K, 32) * 32.0 / (3.2e15 / slots);
+  const double elems = static_cast<double>(M) * K + static_cast<double>(K) * N;
+  const double t_prod = std::max(waves * t_tile, s * elems / 6.0e12);
+  return (8.0 * elems / 6.2e12 + (8.0 + s) * elems / 5.1e12 + t_prod) * 1e3 + 0.030;
+}
+
+constexpr double kSelectMs = 0.035;  // the learned selector: statistics, network, one host read
+
+int run_auto(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta,
+             int* form_out, int* slices_out, cudaStream_t stream) {
+  int form = LT_FORM_FP64, s = 0;
+  // The selector is skipped when native FP64 wins even against the fewest slices.
+  if (M > 0 && N > 0 && K > 0 &&
+      estimate_ms(LT_FORM_OZAKI, M, N, K, 3) + kSelectMs < estimate_ms(LT_FORM_FP64, M, N, K, 0)) {
+    bool learned = false;
+    int gap = 0;
+    LT_TRY(select(A, B, M, N, K, g_tol, &s, &learned, &gap, stream));
+    if (estimate_ms(LT_FORM_OZAKI, M, N, K, s) < estimate_ms(LT_FORM_FP64, M, N, K, 0)) form = LT_FORM_OZAKI;
+  }
+  if (form == LT_FORM_OZAKI) {
+    LT_TRY(lt_dgemm_ozaki(A, B, C, M, N, K, alpha, beta, s, stream));
+  } else {
+    s = 0;
+    LT_TRY(lt_dgemm_fp64(A, B, C, M, N, K, alpha, beta, stream));
+  }
+  if (form_out) *form_out = form;
+  if (slices_out) *slices_out = s;
+  return LT_OK;
+}
+
+}  // namespace sel
+}  // namespace lt
+
+extern "C" {
+
+double lt_dgemm_estimate_ms(int form, int64_t M, int64_t N, int64_t K, int slices) {
+  if ((form != LT_FORM_FP64 && form != LT_FORM_OZAKI) || (form == LT_FORM_OZAKI && (slices < 1 || slices > 12)))
+    return -1.0;
+  return lt::sel::estimate_ms(form, M, N, K, slices);
+}
+
+int lt_dgemm_auto(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
+                  double beta, int* form, int* slices, void* stream) {
+  if (M < 0 || N < 0 || K < 0) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_dgemm_auto: negative size");
+  LT_TRY(lt::sel::run_auto(A, B, C, M, N, K, alpha, beta, form, slices, lt::as_stream(stream)));
+  return lt::ok();
+}
+
+float dgemm_auto(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha,
+                 double beta) {
+  cudaEvent_t start, stop;
+  cudaEventCreate(&start);
+  cudaEventCreate(&stop);
+  cudaEventRecord(start, 0);
+  int rc = lt_dgemm_auto(A, B, C, static_cast<int64_t>(M), static_cast<int64_t>(N), static_cast<int64_t>(K), alpha,
+                         beta, nullptr, nullptr, nullptr);
+  cudaEventRecord(stop, 0);
+  cudaEventSynchronize(stop);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, start, stop);
+  cudaEventDestroy(start);
+  cudaEventDestroy(stop);
+  if (rc == LT_OK) rc = lt_check_device_status();
+  if (rc != LT_OK) {
+    fprintf(stderr, "Kernel launch error (auto): %s: %s\n", lt_error_string(rc), lt::last_message());
     lt::set_error(rc, "%s", lt::last_message());
   }
   return ms;

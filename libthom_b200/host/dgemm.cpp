@@ -33,7 +33,7 @@ static const std::map<std::string, DgemmImpl> dgemmImpls = {
     {"tc100", dgemm_tc100},         {"ozaki3", dgemm_ozaki3},   {"ozaki4", dgemm_ozaki4},
     {"ozaki5", dgemm_ozaki5},       {"ozaki6", dgemm_ozaki6},   {"ozaki7", dgemm_ozaki7},
     {"ozaki8", dgemm_ozaki8},       {"ozaki9", dgemm_ozaki9},   {"ozaki10", dgemm_ozaki10},
-    {"ozaki_auto", dgemm_ozaki_auto}, {"cublas_tc", dgemm_cublas_tc},
+    {"ozaki_auto", dgemm_ozaki_auto}, {"auto", dgemm_auto},     {"cublas_tc", dgemm_cublas_tc},
 };
 
 struct Buffers {

@@ -131,3 +131,23 @@ def test_dot2_rows_rejects_bad_arguments():
     assert L.lt_dot2_rows(p, p, None, 1.0, 0.5, 4, 4, 4, p, 2, p, p, None) == lt.LT_ERR_INVALID_ARGUMENT  # C0 needed
     assert L.lt_dot2_rows(p, p, p, 1.0, 0.0, 4, 4, 4, p, 70000, p, p, None) == lt.LT_ERR_INVALID_ARGUMENT
     assert L.lt_dot2_rows(p, p, p, 1.0, 0.0, 4, 4, 4, p, 0, p, p, None) == lt.LT_OK  # nothing to do
+
+
+def test_auto_form_cost_model_without_gpu():
+    """lt_dgemm_estimate_ms is host arithmetic: the auto form's choices at the workload shapes."""
+    import libthom_b200 as lt
+
+    F, O = lt.LT_FORM_FP64, lt.LT_FORM_OZAKI
+    # 8192^3 and K = 65536: the slice products win; 65536 x 64 x 4096 (the split of A dominates)
+    # and small shapes: native FP64 wins even against 3 slices
+    assert lt.estimate_ms(O, 8192, 8192, 8192, 7) < lt.estimate_ms(F, 8192, 8192, 8192) / 2.5
+    assert lt.estimate_ms(O, 2048, 2048, 65536, 7) < lt.estimate_ms(F, 2048, 2048, 65536) / 2
+    assert lt.estimate_ms(F, 65536, 64, 4096) < lt.estimate_ms(O, 65536, 64, 4096, 3)
+    assert lt.estimate_ms(F, 512, 512, 512) < lt.estimate_ms(O, 512, 512, 512, 3)
+    # 8192^3 FP64 at the measured 34.4 TF/s
+    assert abs(lt.estimate_ms(F, 8192, 8192, 8192) - 2 * 8192 ** 3 / 34.4e9) < 0.1
+    times = [lt.estimate_ms(O, 4096, 4096, 4096, s) for s in range(1, 13)]
+    assert times == sorted(times)
+    assert lt.estimate_ms(F, 0, 5, 5) == 0.0
+    assert lt.estimate_ms(7, 8, 8, 8) == -1.0 and lt.estimate_ms(O, 8, 8, 8, 0) == -1.0
+    assert lt.estimate_ms(O, 8, 8, 8, 13) == -1.0
