@@ -1,6 +1,7 @@
 // dgemm_fp64.cu — host launchers and configuration registry of the native FP64 DGEMM.
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -13,27 +14,55 @@ namespace fp64 {
 
 namespace {
 
-// K split for tile counts that fill the GPU poorly (wave quantisation): the split count S in 1..4
-// minimising waves(S) x (k-blocks per range + pipeline fill) at the FP64 tensor rate, plus the
-// reduction's traffic, and at least 3 % better than no split; ranges keep >= 32 k-blocks.
-int choose_splits(int64_t tiles, int64_t cap, int64_t M, int64_t N, int64_t K, int bm, int bn) {
+struct Schedule {
+  int splits = 1;        // K ranges per tile (1: none)
+  bool streamk = false;  // stream-K (splits == 1)
+  double t = 0.0;        // modelled seconds
+};
+
+// LIBTHOM_FP64_STREAMK=0 turns the stream-K schedule off (the K split and whole tiles remain).
+bool streamk_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("LIBTHOM_FP64_STREAMK");
+    return e == nullptr || std::atoi(e) != 0;
+  }();
+  return on;
+}
+
+// Schedule of one launch for tile counts that fill the GPU poorly (wave quantisation), modelled
+// at the FP64 tensor rate (t_kb: one k-block of one tile on one SM) with a pipeline fill and
+// epilogue of ~6 k-blocks per tile:
+//  * K split S in 2..4 (ranges of >= 32 k-blocks): waves(S) x (k-blocks per range + 6), plus the
+//    reduction's traffic;
+//  * stream-K: the tiles x k-blocks iterations shared evenly by `cap` CTAs; each CTA pays one fill
+//    and ~3 k-blocks per extra tile its range touches, plus the partial-sum slots (mostly L2
+//    traffic) and the fix-up launch.
+// A schedule replaces no split only when it is at least 3 % faster.
+Schedule choose_schedule(int64_t tiles, int64_t cap, int64_t M, int64_t N, int64_t K, int bm, int bn) {
+  Schedule best;
   const int64_t nkb = (K + 15) / 16;
-  if (nkb < 64 || cap <= 0) return 1;
-  const double t_kb = 2.0 * bm * bn * 16 / (128.0 * 1.9e9);  // one k-block of one tile on one SM
-  double best = 0.0;
-  int best_s = 1;
-  for (int S = 1; S <= 4; ++S) {
+  if (tiles <= 0 || nkb <= 0 || cap <= 0) return best;
+  const double t_kb = 2.0 * bm * bn * 16 / (128.0 * 1.9e9);
+  best.t = static_cast<double>((tiles + cap - 1) / cap) * static_cast<double>(nkb + 6) * t_kb;
+  const double plain = best.t;
+  for (int S = 2; S <= 4 && nkb >= 64; ++S) {
     const int64_t per = (nkb + S - 1) / S;
-    if (S > 1 && per < 32) break;
+    if (per < 32) break;
     const int64_t waves = (tiles * S + cap - 1) / cap;
     double t = static_cast<double>(waves) * static_cast<double>(per + 6) * t_kb;
-    if (S > 1) t += (S + 2) * 8.0 * static_cast<double>(M) * static_cast<double>(N) / 6.0e12;
-    if (S == 1 || t < best * 0.97) {
-      best = t;
-      best_s = S;
-    }
+    t += (S + 2) * 8.0 * static_cast<double>(M) * static_cast<double>(N) / 6.0e12;
+    if (t < std::min(best.t, plain * 0.97)) best = Schedule{S, false, t};
   }
-  return best_s;
+  const int64_t total = tiles * nkb;
+  if (total >= 2) {
+    const int64_t G = std::min(cap, total);
+    const int64_t per = (total + G - 1) / G;
+    const int64_t touched = 1 + (per + nkb - 1) / nkb;
+    double t = static_cast<double>(per + 6 + 3 * (touched - 1)) * t_kb;
+    t += 4.0 * G * bm * bn * 8.0 / 20.0e12 + 3.0e-6;
+    if (t < std::min(best.t, plain * 0.97)) best = Schedule{1, true, t};
+  }
+  return best;
 }
 
 template <class Cfg>
@@ -64,19 +93,31 @@ int launch(const Params& p0, cudaStream_t stream, DeviceContext* ctx) {
     occupancy[ctx->device] = occ > 0 ? occ : 1;
   });
   LT_CUDA_TRY(attr_err[ctx->device]);
-  const int64_t tiles = ((p.M + Cfg::BM - 1) / Cfg::BM) * ((p.N + Cfg::BN - 1) / Cfg::BN);
+  const int64_t tiles_m = (p.M + Cfg::BM - 1) / Cfg::BM, tiles_n = (p.N + Cfg::BN - 1) / Cfg::BN;
+  const int64_t tiles = tiles_m * tiles_n;
   const int64_t cap = static_cast<int64_t>(ctx->sm_count) * occupancy[ctx->device];
-  p.splits = choose_splits(tiles, cap, p.M, p.N, p.K, Cfg::BM, Cfg::BN);
+  const int64_t nkb = (p.K + Cfg::BK - 1) / Cfg::BK;
+  const Schedule sched = choose_schedule(tiles, cap, p.M, p.N, p.K, Cfg::BM, Cfg::BN);
+  p.splits = sched.splits;
+  p.streamk = (sched.streamk && streamk_enabled()) ? 1 : 0;
   p.W = nullptr;
-  if (p.splits > 1) {
+  int64_t grid = tiles * p.splits < cap ? tiles * p.splits : cap;
+  if (p.streamk) grid = std::min(cap, tiles * nkb);
+  if (p.splits > 1 || p.streamk) {
+    const size_t bytes = p.streamk ? static_cast<size_t>(2 * grid) * Cfg::BM * Cfg::BN * sizeof(double)
+                                   : static_cast<size_t>(p.splits) * p.M * p.N * sizeof(double);
     void* w = nullptr;
-    LT_TRY(ensure_splitk_workspace(ctx, static_cast<size_t>(p.splits) * p.M * p.N * sizeof(double), &w));
+    LT_TRY(ensure_splitk_workspace(ctx, bytes, &w));
     p.W = static_cast<double*>(w);
   }
-  const int64_t units = tiles * p.splits;
-  const int64_t grid = units < cap ? units : cap;
   dgemm_fp64_kernel<Cfg><<<static_cast<unsigned>(grid), Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(tmA, tmB, p);
   LT_CUDA_TRY(cudaGetLastError());
+  if (p.streamk) {
+    const int64_t blocks = std::min<int64_t>(tiles, static_cast<int64_t>(ctx->sm_count) * 4);
+    streamk_fixup_kernel<Cfg::BM, Cfg::BN><<<static_cast<unsigned>(blocks), kFixupThreads, 0, stream>>>(
+        p.W, p.C, p.M, p.N, p.ldc, tiles_m, tiles_n, nkb, grid, p.alpha, p.beta);
+    LT_CUDA_TRY(cudaGetLastError());
+  }
   if (p.splits > 1) {
     const int64_t n = p.M * p.N;
     const int64_t blocks = std::min<int64_t>((n + 255) / 256, static_cast<int64_t>(ctx->sm_count) * 16);
@@ -125,14 +166,14 @@ const char* config_name(int i) { return (i >= 0 && i < kNumConfigs) ? kConfigs[i
 bool config_is_tma(int i) { return i >= 0 && i < kNumConfigs && kConfigs[i].tma; }
 
 // Default choice without a tuning table: the configuration (of the staging the pointers allow)
-// minimising waves x tile area / tile efficiency, one CTA per SM. Efficiencies are the tiles'
-// measured 8192^3 rates relative to 128x64 (TMA: 34.8, 33.2, 27.6, 18.0, 18.0 TF/s for 128x64,
-// 64x128, 64x64, 64x32, 32x64). The K split handles what remains of a poorly filled last wave.
+// minimising the modelled time of its best schedule (whole tiles, K split or stream-K, one CTA per
+// SM) / tile efficiency. Efficiencies are the tiles' measured 8192^3 rates relative to 128x64
+// (TMA: 34.8, 33.2, 27.6, 18.0, 18.0 TF/s for 128x64, 64x128, 64x64, 64x32, 32x64).
 int heuristic_config(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int sm_count) {
-  return heuristic_config_for(M, N, sm_count, K > 0 && tma_compatible(A, B, N, K));
+  return heuristic_config_for(M, N, K, sm_count, K > 0 && tma_compatible(A, B, N, K));
 }
 
-int heuristic_config_for(int64_t M, int64_t N, int sm_count, bool tma) {
+int heuristic_config_for(int64_t M, int64_t N, int64_t K, int sm_count, bool tma) {
   auto efficiency = [](int bm, int bn) {
     if (bm == 128 && bn == 64) return 1.0;
     if (bm == 64 && bn == 128) return 0.95;
@@ -146,8 +187,7 @@ int heuristic_config_for(int64_t M, int64_t N, int sm_count, bool tma) {
     if (kConfigs[i].tma != tma) continue;
     const int bm = kConfigs[i].bm, bn = kConfigs[i].bn;
     const int64_t tiles = ((M + bm - 1) / bm) * ((N + bn - 1) / bn);
-    const int64_t waves = (tiles + sm_count - 1) / sm_count;
-    const double cost = static_cast<double>(waves) * bm * bn / efficiency(bm, bn);
+    const double cost = choose_schedule(tiles, sm_count, M, N, K, bm, bn).t / efficiency(bm, bn);
     if (best < 0 || cost < best_cost * 0.999) {
       best = i;
       best_cost = cost;

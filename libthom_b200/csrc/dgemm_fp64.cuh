@@ -41,6 +41,11 @@ struct Params {
   // unit for range s writes its raw sums to W + s*M*N (row stride N) and splitk_reduce forms C.
   int splits;
   double* W;
+  // Stream-K (`streamk` = 1, splits = 1): the tiles x k-blocks sequence is cut into gridDim.x equal
+  // contiguous ranges, one per CTA. A tile that one CTA covers whole goes straight to C; the pieces
+  // of a tile shared by several CTAs go to per-CTA slots (W + (2b + j)*BM*BN for CTA b, j = 0 for
+  // its first tile, 1 for its last) and streamk_fixup sums them in K order.
+  int streamk;
 };
 
 template <int BM_, int BN_, int STAGES_, bool TMA_>
@@ -105,7 +110,8 @@ __device__ __forceinline__ void tile_coords(int64_t t, int64_t tiles_m, int64_t 
 }
 
 // One output tile of one problem, over k-blocks kb0..kb1-1. W != nullptr: write the raw sums
-// there (K-split partial) instead of alpha*acc + beta*C.
+// there (partial sums: element (row, col) at W[(row - wr0)*ldw + col - wc0]) instead of
+// alpha*acc + beta*C.
 struct Job {
   const double* A;
   const double* B;
@@ -118,11 +124,25 @@ struct Job {
   int64_t lda, ldb, ldc;
   const CUtensorMap* tmA;  // TMA configurations: the tensor maps of this job's A and B
   const CUtensorMap* tmB;
+  int64_t ldw, wr0, wc0;
 };
+
+// Stream-K: first iteration (tile x k-block) of CTA b's range, b in 0..G.
+__host__ __device__ __forceinline__ int64_t streamk_first(int64_t b, int64_t total, int64_t G) {
+  return b * total / G;
+}
+// The CTA whose range holds iteration i (ranges are non-empty: total >= G).
+__host__ __device__ __forceinline__ int64_t streamk_owner(int64_t i, int64_t total, int64_t G) {
+  int64_t b = i * G / total;
+  while (b + 1 < G && streamk_first(b + 1, total, G) <= i) ++b;
+  while (b > 0 && streamk_first(b, total, G) > i) --b;
+  return b;
+}
 
 // Tiles of a single problem, walked in grouped raster order.
 // With a K split, unit u covers range u / tiles of tile u % tiles, so each wave spans all tiles of
-// one range before the next range starts.
+// one range before the next range starts. With stream-K, CTA b walks the tiles its iteration range
+// touches, in order (the units are then tile indices).
 template <class Cfg>
 struct SingleSource {
   Params p;
@@ -130,7 +150,30 @@ struct SingleSource {
   const CUtensorMap* tmA;
   const CUtensorMap* tmB;
   __device__ int64_t count() const { return tiles_m * tiles_n * p.splits; }
+  __device__ int64_t nkb() const { return (p.K + Cfg::BK - 1) / Cfg::BK; }
+  __device__ int64_t total() const { return tiles_m * tiles_n * nkb(); }
+  __device__ int64_t begin() const {
+    return p.streamk ? streamk_first(blockIdx.x, total(), gridDim.x) / nkb() : static_cast<int64_t>(blockIdx.x);
+  }
+  __device__ int64_t end() const {
+    return p.streamk ? (streamk_first(blockIdx.x + 1, total(), gridDim.x) - 1) / nkb() + 1 : count();
+  }
+  __device__ int64_t step() const { return p.streamk ? 1 : static_cast<int64_t>(gridDim.x); }
   __device__ Job get(int64_t u) const {
+    if (p.streamk) {
+      const int64_t nk = nkb(), it0 = streamk_first(blockIdx.x, total(), gridDim.x);
+      const int64_t it1 = streamk_first(blockIdx.x + 1, total(), gridDim.x);
+      int64_t tm, tn;
+      tile_coords(u, tiles_m, tiles_n, tm, tn);
+      const int64_t kb0 = it0 > u * nk ? it0 - u * nk : 0;
+      const int64_t kb1 = it1 - u * nk < nk ? it1 - u * nk : nk;
+      double* w = nullptr;
+      if (kb0 > 0 || kb1 < nk)
+        w = p.W + (2 * static_cast<int64_t>(blockIdx.x) + (u == it0 / nk ? 0 : 1)) * (Cfg::BM * Cfg::BN);
+      return Job{p.A, p.B, p.C, p.M, p.N, p.K, p.alpha, p.beta, tm * Cfg::BM, tn * Cfg::BN,
+                 static_cast<int>(kb0), static_cast<int>(kb1), w, p.lda, p.ldb, p.ldc, tmA, tmB,
+                 Cfg::BN, tm * Cfg::BM, tn * Cfg::BN};
+    }
     const int64_t tiles = tiles_m * tiles_n;
     const int64_t sp = u / tiles, t = u - sp * tiles;
     int64_t tm, tn;
@@ -141,7 +184,7 @@ struct SingleSource {
     const int kb1 = kb0 + per < nkb ? kb0 + per : nkb;
     double* w = p.splits > 1 ? p.W + sp * p.M * p.N : nullptr;
     return Job{p.A, p.B, p.C, p.M, p.N, p.K, p.alpha, p.beta, tm * Cfg::BM, tn * Cfg::BN, kb0, kb1, w,
-               p.lda, p.ldb, p.ldc, tmA, tmB};
+               p.lda, p.ldb, p.ldc, tmA, tmB, p.N, 0, 0};
   }
 };
 
@@ -168,13 +211,16 @@ struct GroupedSource {
   const GroupTile* tiles;
   int64_t ntiles;
   __device__ int64_t count() const { return ntiles; }
+  __device__ int64_t begin() const { return blockIdx.x; }
+  __device__ int64_t end() const { return ntiles; }
+  __device__ int64_t step() const { return gridDim.x; }
   __device__ Job get(int64_t t) const {
     const GroupTile gt = tiles[t];
     const GroupProblem& pr = problems[gt.problem];
     return Job{pr.A,  pr.B,  pr.C,  pr.M, pr.N,
                pr.K,  pr.alpha, pr.beta, gt.m0, gt.n0,
                0,     static_cast<int>((pr.K + 15) / 16), nullptr, pr.K, pr.N, pr.N,
-               pr.tmA, pr.tmB};
+               pr.tmA, pr.tmB, 0, 0, 0};
   }
 };
 
@@ -188,7 +234,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
   volatile int* abort_flag = reinterpret_cast<volatile int*>(empty + Cfg::STAGES);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t tiles = src.count();
+  const int64_t t_begin = src.begin(), t_end = src.end(), t_step = src.step();
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < Cfg::STAGES; ++s) {
@@ -213,7 +259,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
     int stage = 0;
     uint32_t phase = 0;
     bool ok = true;
-    for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+    for (int64_t t = t_begin; t < t_end && ok; t += t_step) {
       const Job J = src.get(t);
       const int64_t m0 = J.m0, n0 = J.n0;
       for (int kb = J.kb0; kb < J.kb1; ++kb) {
@@ -276,7 +322,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
     int stage = 0;
     uint32_t phase = 0;
     bool ok = true;
-    for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+    for (int64_t t = t_begin; t < t_end && ok; t += t_step) {
       const Job J = src.get(t);
       if (J.W == nullptr && J.beta != 0.0) {
         // The C block this warp's epilogue reads (32 rows of 32 doubles, one row per lane) is
@@ -334,7 +380,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
       // row stride allows ----
       const int64_t m0 = J.m0 + wm * Cfg::WM, n0 = J.n0 + wn * Cfg::WN;
       if (J.W != nullptr) {
-        const bool wvec = (J.N & 1) == 0;  // W is 256-byte aligned
+        const bool wvec = (J.ldw & 1) == 0;  // W and its slots are 16-byte aligned
 #pragma unroll
         for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -344,7 +390,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
               const int64_t col = n0 + j * 8 + 2 * tq;
-              double* wp = J.W + row * J.N + col;
+              double* wp = J.W + (row - J.wr0) * J.ldw + (col - J.wc0);
               if (wvec && col + 1 < J.N) {
                 *reinterpret_cast<double2*>(wp) = make_double2(acc[i][j][2 * h], acc[i][j][2 * h + 1]);
               } else {
@@ -424,6 +470,44 @@ __global__ void splitk_reduce_kernel(const double* __restrict__ W, double* __res
     for (int k = 1; k < splits; ++k) s += W[k * n + i];
     double* c = C + (i / N) * ldc + (i % N);
     *c = (beta != 0.0) ? fma(alpha, s, beta * *c) : alpha * s;
+  }
+}
+
+// Stream-K fix-up: for every tile that several CTAs shared, C = alpha * (their partial sums added
+// in K order, i.e. in CTA order) + beta * C. Tiles that one CTA covered whole are already in C.
+// 256 threads; each holds BM*BN/256 elements of the tile (consecutive threads on consecutive
+// elements), so each slot's index is worked out once per tile and CTA, not per element.
+constexpr int kFixupThreads = 256;
+template <int BM, int BN>
+__global__ void __launch_bounds__(kFixupThreads)
+    streamk_fixup_kernel(const double* __restrict__ W, double* __restrict__ C, int64_t M, int64_t N, int64_t ldc,
+                         int64_t tiles_m, int64_t tiles_n, int64_t nkb, int64_t G, double alpha, double beta) {
+  constexpr int kPer = BM * BN / kFixupThreads;
+  static_assert(BM * BN % kFixupThreads == 0, "tile size");
+  const int64_t tiles = tiles_m * tiles_n, total = tiles * nkb;
+  for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const int64_t b_lo = streamk_owner(t * nkb, total, G), b_hi = streamk_owner((t + 1) * nkb - 1, total, G);
+    if (b_lo == b_hi) continue;
+    double s[kPer];
+    for (int64_t b = b_lo; b <= b_hi; ++b) {
+      const int64_t slot = 2 * b + (t == streamk_first(b, total, G) / nkb ? 0 : 1);
+      const double* __restrict__ w = W + slot * (BM * BN) + threadIdx.x;
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) {
+        const double v = w[k * kFixupThreads];
+        s[k] = (b == b_lo) ? v : s[k] + v;
+      }
+    }
+    int64_t tm, tn;
+    tile_coords(t, tiles_m, tiles_n, tm, tn);
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int e = threadIdx.x + k * kFixupThreads;
+      const int64_t row = tm * BM + e / BN, col = tn * BN + e % BN;
+      if (row >= M || col >= N) continue;
+      double* c = C + row * ldc + col;
+      *c = (beta != 0.0) ? fma(alpha, s[k], beta * *c) : alpha * s[k];
+    }
   }
 }
 

@@ -105,7 +105,7 @@ extern "C" int lt_dgemm_ex(int form, char transa, char transb, int64_t M, int64_
   }
   const bool tma = K > 0 && fp64::tma_compatible(a, b, lb, la);  // no tensor map over zero columns
   int cfg = tuner::lookup(M, N, K, tma);
-  if (cfg < 0 || (fp64::config_is_tma(cfg) && !tma)) cfg = fp64::heuristic_config_for(M, N, ctx->sm_count, tma);
+  if (cfg < 0 || (fp64::config_is_tma(cfg) && !tma)) cfg = fp64::heuristic_config_for(M, N, K, ctx->sm_count, tma);
   LT_TRY(fp64::run_config_ld(cfg, a, la, b, lb, C, ldc, M, N, K, alpha, beta, stream));
   return ok();
 }

@@ -17,7 +17,7 @@ int num_configs();
 const char* config_name(int i);
 bool config_is_tma(int i);
 int heuristic_config(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int sm_count);
-int heuristic_config_for(int64_t M, int64_t N, int sm_count, bool tma);
+int heuristic_config_for(int64_t M, int64_t N, int64_t K, int sm_count, bool tma);
 int run_config(int cfg, const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
                double beta, cudaStream_t stream);
 // Same with row strides (lda >= K, ldb >= N, ldc >= N).
