@@ -84,6 +84,26 @@ def test_k_split_shapes(cuda, oracle_mod, M, N, K, offset, beta):
     assert oracle_mod.componentwise_error(C, Cref, den)[0] <= fp64_bound(K)
 
 
+@pytest.mark.parametrize("M,N,K,offset,beta", [(64, 64, 8192, 0, 0.5), (130, 70, 3001, 1, -1.0),
+                                               (700, 500, 2048, 0, 0.0)])
+def test_stream_k_every_config(cuda, oracle_mod, M, N, K, offset, beta):
+    """Stream-K: few tiles against 148 SMs, so the k-block iterations are dealt out in equal ranges
+    and tiles shared by several CTAs (at 64x64x8192 one tile by all of them) are summed in K order by
+    the fix-up kernel; every tile configuration the pointers allow, ragged edges and odd K."""
+    import libthom_b200 as lt
+
+    A, B, C0 = oracle_mod.make_problem(M, N, K, phi=3, seed=3 * M + K)
+    if beta == 0.0:
+        C0 = np.full_like(C0, np.nan)
+    Cref, den = oracle_mod.dot2_rows(A, B, None if beta == 0.0 else C0, 0.75, beta)
+    names = lt.fp64_configs()
+    for cfg, name in enumerate(names):
+        if offset and name.startswith("tma"):
+            continue  # TMA needs 16-byte aligned operands and even pitches
+        C = run_fp64(cuda, A, B, C0, 0.75, beta, config=cfg, offset=offset)
+        assert oracle_mod.componentwise_error(C, Cref, den)[0] <= fp64_bound(K), name
+
+
 def test_unaligned_pointers_take_general_path(cuda, oracle_mod):
     M, N, K = 96, 64, 80
     A, B, C0 = oracle_mod.make_problem(M, N, K, seed=4)
