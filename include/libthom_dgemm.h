@@ -72,6 +72,13 @@ float dgemm_cublas_tc(const double* A, const double* B, double* C, size_t M, siz
                       double alpha, double beta);
 
 /* ---- stream-ordered API --------------------------------------------------------------------- */
+/* The calls below run on `stream` (NULL = legacy default stream) and return a status. Scratch
+ * memory (Ozaki slices, FP64 partial sums of the K split and stream-K schedules, packed copies) is
+ * a per-device cache that the library grows on demand and keeps until exit, shared by all calls on
+ * that device: calls whose work can overlap on the GPU (other streams, other host threads) must be
+ * ordered by the caller, or use lt_dgemm_ozaki_ws with a workspace of their own. */
+/* Native FP64 tensor-core DGEMM; the tile shape and schedule (whole tiles, K split or stream-K)
+ * follow a cost model of the shape unless a tuning table holds a choice. */
 int lt_dgemm_fp64(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
                   double alpha, double beta, void* stream);
 /* Runs one specific FP64 kernel configuration (index into lt_fp64_config_name); -1 = tuned choice. */
