@@ -42,6 +42,12 @@ const char* lt_last_error_message(void);
 /* Reads (and clears) the device error word written by bounded waits inside the kernels; call after
  * a synchronize. Returns LT_OK or LT_ERR_DEVICE_TIMEOUT. */
 int lt_check_device_status(void);
+/* Failure-detection self-test (no reference counterpart): launches one small kernel whose wait, the
+ * same bounded mbarrier wait every pipeline uses, is on a barrier that nothing arrives at, with a
+ * limit of `limit_ms` (0.001 .. 1000) instead of the pipelines' 2 s. The wait gives up, records
+ * LT_ERR_DEVICE_TIMEOUT with tag 99 in the device error word (read by lt_check_device_status after
+ * a synchronize) and the kernel returns: the context stays usable. Nothing faults or hangs. */
+int lt_selftest_wait_timeout(double limit_ms, void* stream);
 int lt_version(void);
 
 /* ---- reference-contract implementations (routines/dgemm/dgemm.h:8-42 registry entries) ------ */

@@ -75,6 +75,7 @@ SIGNATURES = {
     "lt_error_string": (_c.c_char_p, [_i32]),
     "lt_last_error_message": (_c.c_char_p, []),
     "lt_check_device_status": (_i32, []),
+    "lt_selftest_wait_timeout": (_i32, [_f64, _vp]),
     "lt_version": (_i32, []),
     "dgemm_tc100": (_f32, _REF),
     "dgemm_ozaki3": (_f32, _REF), "dgemm_ozaki4": (_f32, _REF), "dgemm_ozaki5": (_f32, _REF),

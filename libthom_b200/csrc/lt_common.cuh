@@ -72,23 +72,28 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait on phase `parity` of `bar`. Returns false (after recording the failure in `st`
-// and raising the CTA-wide `abort_flag`) if the phase has not completed within the time limit or
+// and raising the CTA-wide `abort_flag`) if the phase has not completed within `limit_ns` or
 // another warp of the CTA has already aborted.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
-                                          DeviceStatus* st, int where) {
+__device__ __forceinline__ bool mbar_wait_for(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                              DeviceStatus* st, int where, uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   uint64_t t0 = globaltimer();
   for (uint32_t it = 1;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((it & 255u) == 0) {
       if (*abort_flag) return false;
-      if (globaltimer() - t0 > LT_WAIT_TIMEOUT_NS) {
+      if (globaltimer() - t0 > limit_ns) {
         *abort_flag = 1;
         report_error(st, LT_ERR_DEVICE_TIMEOUT, where);
         return false;
       }
     }
   }
+}
+// The pipelines' wait: limit LT_WAIT_TIMEOUT_NS.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                          DeviceStatus* st, int where) {
+  return mbar_wait_for(bar, parity, abort_flag, st, where, LT_WAIT_TIMEOUT_NS);
 }
 
 // ---------------------------------------------------------------------------------------------

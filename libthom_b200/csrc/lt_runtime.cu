@@ -169,6 +169,28 @@ int make_tmap_3d(CUtensorMap* map, const void* base, CUtensorMapDataType dtype, 
   return LT_OK;
 }
 
+// Failure-detection self-test: thread 0 waits, through the pipelines' bounded wait, on an mbarrier
+// that nothing arrives at. After `limit_ns` the wait gives up and records LT_ERR_DEVICE_TIMEOUT
+// (tag 99) in the device status word, as a stalled pipeline stage would; the kernel then returns.
+// The other warp waits on the same barrier and must leave through the raised abort flag, as the
+// other roles of a pipeline do. Nothing faults or traps.
+__global__ void wait_timeout_selftest_kernel(uint64_t limit_ns, DeviceStatus* st) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    abort_flag = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_wait_for(&bar, 0, &abort_flag, st, 99, limit_ns);
+  } else if (threadIdx.x == 32) {
+    // gives up only through the abort flag (or, failing that, after twice the limit, tag 98)
+    mbar_wait_for(&bar, 0, &abort_flag, st, 98, 2 * limit_ns);
+  }
+}
+
 }  // namespace lt
 
 extern "C" {
@@ -201,6 +223,17 @@ int lt_check_device_status(void) {
     return lt::set_error(st.code, "device wait gave up (tag %d, block %d)", st.where, st.block);
   }
   return LT_OK;
+}
+
+int lt_selftest_wait_timeout(double limit_ms, void* stream) {
+  if (!(limit_ms >= 0.001 && limit_ms <= 1000.0))
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "wait limit %g ms outside [0.001, 1000]", limit_ms);
+  lt::DeviceContext* ctx = lt::context();
+  if (ctx == nullptr) return lt::last_error();
+  lt::wait_timeout_selftest_kernel<<<1, 64, 0, lt::as_stream(stream)>>>(static_cast<uint64_t>(limit_ms * 1e6),
+                                                                         ctx->status);
+  LT_CUDA_TRY(cudaGetLastError());
+  return lt::ok();
 }
 
 int lt_version(void) { return 100; }

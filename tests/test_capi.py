@@ -133,6 +133,14 @@ def test_dot2_rows_rejects_bad_arguments():
     assert L.lt_dot2_rows(p, p, p, 1.0, 0.0, 4, 4, 4, p, 0, p, p, None) == lt.LT_OK  # nothing to do
 
 
+def test_selftest_rejects_bad_limits_without_gpu():
+    import libthom_b200 as lt
+
+    L = lt.lib()
+    for bad in (0.0, -1.0, 1e4, float("nan")):
+        assert L.lt_selftest_wait_timeout(bad, None) == lt.LT_ERR_INVALID_ARGUMENT
+
+
 def test_auto_form_cost_model_without_gpu():
     """lt_dgemm_estimate_ms is host arithmetic: the auto form's choices at the workload shapes."""
     import libthom_b200 as lt

@@ -69,6 +69,43 @@ def test_two_rank_replicas_gloo():
     assert res[1][3] == "returned"
 
 
+def _failing_worker(rank: int, world: int, port: int, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    sys.path.insert(0, str(ROOT))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    import bench
+
+    if rank == 1:
+        out.put((rank, "failed"))
+        raise SystemExit(3)  # this rank fails between steps, before the max-over-ranks reduction
+    try:
+        bench.reduce_max(1.0, dist)
+        out.put((rank, "no error"))
+    except Exception as e:  # the survivor learns of it from the collective: an error, not a hang
+        out.put((rank, "error " + type(e).__name__))
+
+
+def test_failed_rank_ends_the_others_collective_with_an_error():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+    assert res[1] == "failed" and procs[1].exitcode == 3
+    assert res[0].startswith("error"), res[0]
+    assert procs[0].exitcode == 0
+
+
 def test_single_rank_is_identity():
     sys.path.insert(0, str(ROOT))
     import bench
