@@ -8,7 +8,11 @@
 //   * full/empty mbarrier pairs hand each stage to the consumer warps and back;
 //   * consumer warps each own a 32 x 32 sub-tile and issue mma.sync m16n8k16 FP64 (2048 FMAs per
 //     instruction) from fragments read with 128-bit shared loads;
-//   * the alpha/beta epilogue writes 16-byte vectors straight from the accumulators.
+//   * the alpha/beta epilogue writes 16-byte vectors straight from the accumulators (C0 fetched
+//     into L2 at the start of each tile and loaded before any store of its half-block);
+//   * tiles come from a Source: one problem's tiles in raster order (whole tiles, a K split, or a
+//     stream-K schedule of equal k-block ranges per CTA), or a grouped launch's tile list with
+//     per-problem tensor maps.
 // Tensor cores compute in FP64 throughout (tcgen05 has no FP64 kind on sm_100a; FP64 MMA is the
 // warp-level instruction).
 //
