@@ -432,6 +432,74 @@ struct OzProblem {
   int pair = 0;    // 1: CTA-pair kernel, B slices stored half-major (see store_tile_row)
 };
 
+// One row's 64 results (columns col0 .. col0+63 of C, row < M):
+// C = fma(alpha, acc 2^(sigma+2) 2^(tau+2), beta C0), NaN where the row's or the column's exponent
+// is the non-finite sentinel. C0 is read 8 values at a time (16-byte loads where the row segment
+// is 16-byte aligned and whole), all before those values' stores: the stores go through the same
+// pointer, so a load written after one could not be moved ahead of it, and every value would wait
+// for its own round trip to memory.
+__device__ __forceinline__ void store_c_row64(const OzProblem& pr, int64_t row, int64_t col0,
+                                              const double (&acc)[64]) {
+  const int sig = exponent_of_maxbits(pr.amax_a[row]);
+  double* crow = pr.C + row * pr.ldc;
+  const int64_t N = pr.N;
+  const double alpha = pr.alpha, beta = pr.beta;
+  const bool vec = col0 + 64 <= N && (reinterpret_cast<uintptr_t>(crow + col0) & 15) == 0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    double c0[8] = {};
+    if (beta != 0.0) {
+      if (vec) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const double2 x = *reinterpret_cast<const double2*>(crow + col0 + q * 8 + 2 * v);
+          c0[2 * v] = x.x;
+          c0[2 * v + 1] = x.y;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int64_t col = col0 + q * 8 + i;
+          if (col < N) c0[i] = crow[col];
+        }
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      double out[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int i = q * 8 + 2 * v + h;
+        const int64_t col = col0 + i;
+        const int tau = col < N ? exponent_of_maxbits(pr.amax_b[col]) : 0;
+        if (sig == kSentinel || tau == kSentinel) {
+          out[h] = __longlong_as_double(0x7ff8000000000000ll);
+        } else {
+          const double tv = scale_pow2(scale_pow2(acc[i], sig + 2), tau + 2);
+          out[h] = (beta != 0.0) ? fma(alpha, tv, __dmul_rn(beta, c0[2 * v + h])) : __dmul_rn(alpha, tv);
+        }
+      }
+      const int64_t col = col0 + q * 8 + 2 * v;
+      if (vec) {
+        *reinterpret_cast<double2*>(crow + col) = make_double2(out[0], out[1]);
+      } else {
+        if (col < N) crow[col] = out[0];
+        if (col + 1 < N) crow[col + 1] = out[1];
+      }
+    }
+  }
+}
+
+// Fetches the 512 bytes of C0 that store_c_row64 will read for (row, col0) into L2, when beta != 0.
+__device__ __forceinline__ void prefetch_c_row64(const OzProblem& pr, int64_t row, int64_t col0) {
+  if (pr.beta == 0.0 || row >= pr.M) return;
+  const double* crow = pr.C + row * pr.ldc;
+#pragma unroll
+  for (int q = 0; q < 64; q += 16)
+    if (col0 + q < pr.N) prefetch_l2(crow + col0 + q);
+  if (col0 + 63 < pr.N) prefetch_l2(crow + col0 + 63);
+}
+
 // One output tile of one problem.
 struct OzJob {
   const OzProblem* pr;
@@ -694,6 +762,7 @@ __device__ __forceinline__ void ozaki_body(const Source& src, DeviceStatus* stat
     for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
       const OzJob J = src.get(t);
       const int64_t nkc = J.pr->nkc;
+      prefetch_c_row64(*J.pr, J.m0 + row_in_tile, J.n0 + half * 64);
       double acc[64];
 #pragma unroll
       for (int i = 0; i < 64; ++i) acc[i] = 0.0;
@@ -728,31 +797,8 @@ __device__ __forceinline__ void ozaki_body(const Source& src, DeviceStatus* stat
       }
       if (!ok) break;
       // ---- C = fma(alpha, acc 2^(sigma+2) 2^(tau+2), beta C0) ----
-      const OzProblem& pr = *J.pr;
       const int64_t row = J.m0 + row_in_tile;
-      if (row < pr.M) {
-        const int sig = exponent_of_maxbits(pr.amax_a[row]);
-        const int64_t col0 = J.n0 + half * 64;
-        double* crow = pr.C + row * pr.ldc;
-        const int64_t N = pr.N;
-        const double alpha = pr.alpha, beta = pr.beta;
-        const unsigned long long* amax_b = pr.amax_b;
-#pragma unroll
-        for (int i = 0; i < 64; ++i) {
-          const int64_t col = col0 + i;
-          if (col < N) {
-            const int tau = exponent_of_maxbits(amax_b[col]);
-            double out;
-            if (sig == kSentinel || tau == kSentinel) {
-              out = __longlong_as_double(0x7ff8000000000000ll);
-            } else {
-              const double tv = scale_pow2(scale_pow2(acc[i], sig + 2), tau + 2);
-              out = (beta != 0.0) ? fma(alpha, tv, __dmul_rn(beta, crow[col])) : __dmul_rn(alpha, tv);
-            }
-            crow[col] = out;
-          }
-        }
-      }
+      if (row < J.pr->M) store_c_row64(*J.pr, row, J.n0 + half * 64, acc);
     }
   }
 
@@ -1034,6 +1080,7 @@ __device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatu
     for (int64_t t = first; t < tiles && ok; t += stride) {
       int m0, n0;
       src.get(t, &m0, &n0);
+      prefetch_c_row64(pr, m0 + static_cast<int64_t>(rank) * kTileM + row_in_tile, n0 + half * 64);
       double acc[64];
 #pragma unroll
       for (int i = 0; i < 64; ++i) acc[i] = 0.0;
@@ -1069,29 +1116,7 @@ __device__ __forceinline__ void ozaki_pair_body(const OzProblem& pr, DeviceStatu
       if (!ok) break;
       // ---- C = fma(alpha, acc 2^(sigma+2) 2^(tau+2), beta C0) for this CTA's 128 rows ----
       const int64_t row = m0 + static_cast<int64_t>(rank) * kTileM + row_in_tile;
-      if (row < pr.M) {
-        const int sig = exponent_of_maxbits(pr.amax_a[row]);
-        const int64_t col0 = n0 + half * 64;
-        double* crow = pr.C + row * pr.ldc;
-        const int64_t N = pr.N;
-        const double alpha = pr.alpha, beta = pr.beta;
-        const unsigned long long* amax_b = pr.amax_b;
-#pragma unroll
-        for (int i = 0; i < 64; ++i) {
-          const int64_t col = col0 + i;
-          if (col < N) {
-            const int tau = exponent_of_maxbits(amax_b[col]);
-            double out;
-            if (sig == kSentinel || tau == kSentinel) {
-              out = __longlong_as_double(0x7ff8000000000000ll);
-            } else {
-              const double tv = scale_pow2(scale_pow2(acc[i], sig + 2), tau + 2);
-              out = (beta != 0.0) ? fma(alpha, tv, __dmul_rn(beta, crow[col])) : __dmul_rn(alpha, tv);
-            }
-            crow[col] = out;
-          }
-        }
-      }
+      if (row < pr.M) store_c_row64(pr, row, n0 + half * 64, acc);
     }
   }
 
