@@ -103,13 +103,14 @@ __device__ __forceinline__ unsigned long long abs_bits(double v) {
   return static_cast<unsigned long long>(__double_as_longlong(v)) & 0x7fffffffffffffffull;
 }
 
-// Row maxima of A: blockIdx.x covers 8 rows (one warp each), blockIdx.y a K segment.
-__global__ void amax_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K, int64_t lda, int64_t kseg,
-                                 unsigned long long* __restrict__ amax) {
+// Row maxima of A: block (bx, by) covers 8 rows (one warp each) and K segment by.
+__device__ __forceinline__ void amax_rows_block(const double* __restrict__ A, int64_t M, int64_t K, int64_t lda,
+                                                int64_t kseg, unsigned long long* __restrict__ amax, int64_t bx,
+                                                int64_t by) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t row = static_cast<int64_t>(blockIdx.x) * 8 + warp;
+  const int64_t row = bx * 8 + warp;
   if (row >= M) return;
-  const int64_t k0 = static_cast<int64_t>(blockIdx.y) * kseg;
+  const int64_t k0 = by * kseg;
   const int64_t k1 = (k0 + kseg < K) ? k0 + kseg : K;
   const double* a = A + row * lda;
   unsigned long long m = 0;
@@ -124,15 +125,21 @@ __global__ void amax_rows_kernel(const double* __restrict__ A, int64_t M, int64_
   if (lane == 0 && m != 0) atomicMax(&amax[row], m);
 }
 
-// Column maxima of B: blockIdx.x covers 256 columns (one per thread), blockIdx.y a K segment.
-// With 16-byte aligned rows (B aligned, N even) each thread reads two adjacent columns per load and
-// the block covers 512 columns (`pairs` set by the launcher).
-__global__ void amax_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N, int64_t ldb, int64_t kseg,
-                                 unsigned long long* __restrict__ amax, int pairs) {
-  const int64_t k0 = static_cast<int64_t>(blockIdx.y) * kseg;
+__global__ void amax_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K, int64_t lda, int64_t kseg,
+                                 unsigned long long* __restrict__ amax) {
+  amax_rows_block(A, M, K, lda, kseg, amax, blockIdx.x, blockIdx.y);
+}
+
+// Column maxima of B: block (bx, by) covers 256 columns (one per thread) and K segment by. With
+// 16-byte aligned rows (B aligned, N even) each thread reads two adjacent columns per load and the
+// block covers 512 columns (`pairs` set by the launcher).
+__device__ __forceinline__ void amax_cols_block(const double* __restrict__ B, int64_t K, int64_t N, int64_t ldb,
+                                                int64_t kseg, unsigned long long* __restrict__ amax, int pairs,
+                                                int64_t bx, int64_t by) {
+  const int64_t k0 = by * kseg;
   const int64_t k1 = (k0 + kseg < K) ? k0 + kseg : K;
   if (pairs) {
-    const int64_t col = 2 * (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x);
+    const int64_t col = 2 * (bx * blockDim.x + threadIdx.x);
     if (col >= N) return;
     unsigned long long m0 = 0, m1 = 0;
     const double* bp = B + k0 * ldb + col;
@@ -147,7 +154,7 @@ __global__ void amax_cols_kernel(const double* __restrict__ B, int64_t K, int64_
     if (m1 != 0) atomicMax(&amax[col + 1], m1);
     return;
   }
-  const int64_t col = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t col = bx * blockDim.x + threadIdx.x;
   if (col >= N) return;
   unsigned long long m = 0;
   for (int64_t k = k0; k < k1; ++k) {
@@ -155,6 +162,26 @@ __global__ void amax_cols_kernel(const double* __restrict__ B, int64_t K, int64_
     m = b > m ? b : m;
   }
   if (m != 0) atomicMax(&amax[col], m);
+}
+
+__global__ void amax_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N, int64_t ldb, int64_t kseg,
+                                 unsigned long long* __restrict__ amax, int pairs) {
+  amax_cols_block(B, K, N, ldb, kseg, amax, pairs, blockIdx.x, blockIdx.y);
+}
+
+// Both sides' maxima in one launch (256 threads): blocks 0 .. ra*ka-1 are A's row blocks (ra of
+// them per K segment, ka segments), the rest B's column blocks (rb per segment).
+__global__ void amax_both_kernel(const double* __restrict__ A, int64_t M, int64_t K, int64_t kseg_a, int64_t ra,
+                                 int64_t ka, unsigned long long* __restrict__ amax_a, const double* __restrict__ B,
+                                 int64_t N, int64_t kseg_b, int64_t rb, int pairs,
+                                 unsigned long long* __restrict__ amax_b) {
+  const int64_t id = blockIdx.x;
+  if (id < ra * ka) {
+    amax_rows_block(A, M, K, K, kseg_a, amax_a, id % ra, id / ra);
+  } else {
+    const int64_t j = id - ra * ka;
+    amax_cols_block(B, K, N, N, kseg_b, amax_b, pairs, j % rb, j / rb);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -413,6 +440,23 @@ __global__ void __launch_bounds__(128) split_cols_kernel(const double* __restric
                                                          int8_t* __restrict__ out, int half_major) {
   for (int64_t t = blockIdx.x; t < RB * NC; t += gridDim.x)
     split_cols_tile<S>(B, K, N, ldb, NC, RB, amax, out, t / NC, t % NC, threadIdx.x, half_major);
+}
+
+// Both sides' slices in one launch: blocks 0 .. ga-1 walk A's row tiles (stride ga), the rest B's
+// column tiles (stride gb); row pitches K and N.
+template <int S>
+__global__ void __launch_bounds__(128)
+    split_both_kernel(const double* __restrict__ A, int64_t M, const double* __restrict__ B, int64_t N, int64_t K,
+                      int64_t NC, int64_t RBa, int64_t RBb, const unsigned long long* __restrict__ amax_a,
+                      const unsigned long long* __restrict__ amax_b, int8_t* __restrict__ sa,
+                      int8_t* __restrict__ sb, int64_t ga, int64_t gb, int half_major_b) {
+  if (blockIdx.x < ga) {
+    for (int64_t t = blockIdx.x; t < RBa * NC; t += ga)
+      split_rows_tile<S>(A, M, K, K, NC, RBa, amax_a, sa, t / NC, t % NC, threadIdx.x, 0);
+  } else {
+    for (int64_t t = blockIdx.x - ga; t < RBb * NC; t += gb)
+      split_cols_tile<S>(B, K, N, N, NC, RBb, amax_b, sb, t / NC, t % NC, threadIdx.x, half_major_b);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1359,6 +1403,51 @@ int cols_stage(int s, const double* B, int64_t K, int64_t N, int64_t ldb, int64_
   return LT_OK;
 }
 
+// Both sides of the split in two launches (exponents, then slices), each launch's blocks divided
+// between A's rows and B's columns: the same blocks and results as rows_stage + cols_stage with
+// row pitches K and N, with two kernel boundaries fewer. M, N, K > 0; amax zero on entry.
+template <int S>
+void launch_split_both_s(const double* A, const double* B, int64_t M, int64_t N, int64_t K, const Layout& L,
+                         const unsigned long long* amax_a, const unsigned long long* amax_b, int8_t* sa, int8_t* sb,
+                         int sms, cudaStream_t stream, int half_major_b) {
+  const int64_t cap = static_cast<int64_t>(sms) * 64;
+  const int64_t ta = L.RBa * L.NC, tb = L.RBb * L.NC;
+  const int64_t ga = ta < cap ? ta : cap, gb = tb < cap ? tb : cap;
+  split_both_kernel<S><<<static_cast<unsigned>(ga + gb), 128, 0, stream>>>(A, M, B, N, K, L.NC, L.RBa, L.RBb, amax_a,
+                                                                           amax_b, sa, sb, ga, gb, half_major_b);
+}
+
+int both_stage(int s, const double* A, const double* B, int64_t M, int64_t N, int64_t K, const Layout& L,
+               unsigned long long* amax_a, unsigned long long* amax_b, int8_t* sa, int8_t* sb, int sms,
+               cudaStream_t stream, int half_major_b) {
+  // exponents: the blocks rows_stage and cols_stage would launch
+  const int64_t ra = (M + 7) / 8;
+  int64_t ka = (4 * sms + ra - 1) / ra;
+  ka = ka < 1 ? 1 : ka;
+  const int64_t kseg_a = round_up((K + ka - 1) / ka, 256);
+  ka = (K + kseg_a - 1) / kseg_a;
+  const int pairs = (N % 2 == 0) && ((reinterpret_cast<uintptr_t>(B) & 15) == 0);
+  const int64_t per_block = pairs ? 512 : 256;
+  const int64_t rb = (N + per_block - 1) / per_block;
+  int64_t kb = (8 * sms + rb - 1) / rb;
+  kb = kb < 1 ? 1 : kb;
+  const int64_t kseg_b = (K + kb - 1) / kb;
+  kb = (K + kseg_b - 1) / kseg_b;
+  amax_both_kernel<<<static_cast<unsigned>(ra * ka + rb * kb), 256, 0, stream>>>(A, M, K, kseg_a, ra, ka, amax_a, B, N,
+                                                                                  kseg_b, rb, pairs, amax_b);
+  LT_CUDA_TRY(cudaGetLastError());
+  switch (s) {
+#define LT_BOTH_CASE(S) \
+  case S: launch_split_both_s<S>(A, B, M, N, K, L, amax_a, amax_b, sa, sb, sms, stream, half_major_b); break;
+    LT_BOTH_CASE(1) LT_BOTH_CASE(2) LT_BOTH_CASE(3) LT_BOTH_CASE(4) LT_BOTH_CASE(5) LT_BOTH_CASE(6)
+    LT_BOTH_CASE(7) LT_BOTH_CASE(8) LT_BOTH_CASE(9) LT_BOTH_CASE(10) LT_BOTH_CASE(11) LT_BOTH_CASE(12)
+#undef LT_BOTH_CASE
+    default: return set_error(LT_ERR_INVALID_ARGUMENT, "slice count %d unsupported", s);
+  }
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
 // Stage 1+2: exponents and slices of A and B into the workspace.
 int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int s, void* workspace,
           size_t workspace_bytes, cudaStream_t stream) {
@@ -1372,6 +1461,8 @@ int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int
   auto* sa = reinterpret_cast<int8_t*>(ws + L.off_sa);
   auto* sb = reinterpret_cast<int8_t*>(ws + L.off_sb);
   LT_CUDA_TRY(cudaMemsetAsync(ws, 0, L.off_sa, stream));
+  if (M > 0 && N > 0 && K > 0)
+    return both_stage(s, A, B, M, N, K, L, amax_a, amax_b, sa, sb, ctx->sm_count, stream, pair_path(L.RBa) ? 1 : 0);
   LT_TRY(rows_stage(s, A, M, K, K, L.NC, amax_a, sa, ctx->sm_count, stream, 0));
   return cols_stage(s, B, K, N, N, L.NC, amax_b, sb, ctx->sm_count, stream, pair_path(L.RBa) ? 1 : 0);
 }
