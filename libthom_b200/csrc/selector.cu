@@ -397,12 +397,12 @@ namespace sel {
 // Predicted milliseconds of one DGEMM in `form` on a B200 (148 SMs), from rates measured on it.
 // FP64: 128x64 tiles at 34.4 TF/s over the padded tile work; with fewer than 148 tiles the K split
 // (up to 4 ranges) spreads them over more SMs; 5 us fixed. Ozaki with s slices: exponent passes at
-// 6.2 TB/s (8 bytes per element of A and B), splits at 5.1 TB/s (8 bytes read + s written), 45 us
-// for the four split-stage launches; then the s(s+1)/2 INT8 slice products on 256x128 CTA-pair
+// 6.2 TB/s (8 bytes per element of A and B), splits at 5.1 TB/s (8 bytes read + s written), 30 us
+// for the split stage's launches; then the s(s+1)/2 INT8 slice products on 256x128 CTA-pair
 // tiles (128x128 tiles when M <= 128) in whole waves, each tile at 3.6 POP/s of the GPU plus 40 us
 // (pipeline fill, two band drains, the FP64 epilogue), or the slice bytes at 6.0 TB/s when that is
 // longer; 10 us for the launch. Predicted (measured) Ozaki s = 7 / FP64: 8192^3 10.4 (10.0-10.6) /
-// 32.0 (32.0) ms; 2048^3 0.33 (0.34) / 0.50 (0.51); 1024^3 0.14 (0.16) / 0.067 (0.076);
+// 32.0 (32.0) ms; 2048^3 0.31 (0.30) / 0.50 (0.51); 1024^3 0.13 (0.12) / 0.067 (0.076);
 // 65536x64x4096 2.0 (1.87) / 1.00 (1.04); 2048x2048x65536 6.2 (6.2) / 16.0 (16.0).
 double estimate_ms(int form, int64_t M, int64_t N, int64_t K, int s) {
   if (M <= 0 || N <= 0 || K <= 0) return 0.0;
@@ -422,7 +422,7 @@ double estimate_ms(int form, int64_t M, int64_t N, int64_t K, int s) {
   const double t_tile = products * 2.0 * tm * 128.0 * cdiv(K, 32) * 32.0 / (3.6e15 / slots) + 40e-6;
   const double elems = static_cast<double>(M) * K + static_cast<double>(K) * N;
   const double t_prod = std::max(waves * t_tile, s * elems / 6.0e12) + 10e-6;
-  return (8.0 * elems / 6.2e12 + (8.0 + s) * elems / 5.1e12 + 45e-6 + t_prod) * 1e3;
+  return (8.0 * elems / 6.2e12 + (8.0 + s) * elems / 5.1e12 + 30e-6 + t_prod) * 1e3;
 }
 
 constexpr double kSelectMs = 0.035;  // the learned selector: statistics, network, one host read
