@@ -501,7 +501,8 @@ def run_ours(args) -> None:
                         "the call, row panels overlapping the copies with the kernels"},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
-        "gpu_launches": 5 * args.steps,
+        # per timed step: amax_both_kernel, split_both_kernel<s>, ozaki_pair_kernel<s>
+        "gpu_launches": 3 * args.steps,
     }
     print(json.dumps(line), flush=True)
     if dist is not None:
