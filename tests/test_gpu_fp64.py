@@ -123,7 +123,7 @@ def test_k_zero_and_beta_zero(cuda, oracle_mod):
 
 
 def test_config1_against_cublas(cuda, oracle_mod):
-    """1024^3, alpha=1, beta=0, U[-1,1); checked against cuBLAS DGEMM (the
+    """Plain 1024^3 DGEMM, alpha=1, beta=0, U[-1,1); checked against cuBLAS DGEMM (the
     reference's GPU oracle, routines/dgemm/dgemm_cublas_tc.cu) and the host oracles."""
     import libthom_b200 as lt
 
