@@ -97,6 +97,25 @@ static double check(const Set& s, double tol) {
   return worst;
 }
 
+// Implementation names of the batched routine: the FP64 grouped plan (default or tuned tiles),
+// the Ozaki grouped plan with a slice count, or one cuBLAS call per problem. Checked before any
+// device memory is touched, like the reference's registry lookup (routines/routines.h:108, 149).
+static bool knownImpl(const std::string& impl) {
+  if (impl == "fp64" || impl == "fp64_tuned" || impl == "cublas_loop") return true;
+  if (impl.rfind("ozaki", 0) != 0 || impl.size() == 5 || impl.size() > 7) return false;
+  for (size_t i = 5; i < impl.size(); ++i)
+    if (impl[i] < '0' || impl[i] > '9') return false;
+  int sl = atoi(impl.c_str() + 5);
+  return sl >= 1 && sl <= LT_OZAKI_MAX_SLICES;
+}
+
+static void requireKnownImpl(const std::string& impl) {
+  if (knownImpl(impl)) return;
+  fprintf(stderr, "Invalid implementation %s. Available: fp64 fp64_tuned ozaki<1..%d> cublas_loop\n", impl.c_str(),
+          LT_OZAKI_MAX_SLICES);
+  exit(1);
+}
+
 // Median ms of `iters` timed runs (after `warmup`) of one implementation on the set.
 static double runImpl(const std::string& impl, Set& s, int iters, int warmup, bool doCheck) {
   lt_grouped_plan* plan = nullptr;
@@ -109,9 +128,8 @@ static double runImpl(const std::string& impl, Set& s, int iters, int warmup, bo
   } else if (impl.rfind("ozaki", 0) == 0) {
     int sl = atoi(impl.c_str() + 5);
     LT_CHECK(lt_grouped_plan_create(s.probs.data(), static_cast<int>(s.probs.size()), LT_FORM_OZAKI, sl, &plan));
-  } else if (impl != "cublas_loop") {
-    fprintf(stderr, "Invalid implementation %s. Available: fp64 fp64_tuned ozaki<3..12> cublas_loop\n", impl.c_str());
-    exit(1);
+  } else {
+    requireKnownImpl(impl);
   }
   if (plan != nullptr) {
     char name[128];
@@ -147,11 +165,12 @@ static double runImpl(const std::string& impl, Set& s, int iters, int warmup, bo
 }
 
 static void testHandler(int argc, char* argv[]) {
-  if (argc < 9) {
+  if (argc < 8) {
     fprintf(stderr, "Usage: ./libthom test dgemmb <impl> <count> <lo> <hi> <nb_iter> [check=1]\n");
     exit(1);
   }
   std::string impl = argv[3];
+  requireKnownImpl(impl);
   int count = atoi(argv[4]);
   int64_t lo = atoll(argv[5]), hi = atoll(argv[6]);
   int iters = atoi(argv[7]);
@@ -172,6 +191,7 @@ static void benchHandler(int argc, char* argv[]) {
     exit(1);
   }
   std::string impl = argv[3];
+  requireKnownImpl(impl);
   Set s = makeSet(512, 32, 1024, 1234);
   double ms = runImpl(impl, s, 10, 5, false);
   double gf = s.flops / (ms * 1e6);
@@ -184,6 +204,10 @@ static void benchHandler(int argc, char* argv[]) {
 static void tuneHandler(int argc, char* argv[]) {
   int count = argc > 3 ? atoi(argv[3]) : 512;
   int64_t lo = argc > 4 ? atoll(argv[4]) : 32, hi = argc > 5 ? atoll(argv[5]) : 1024;
+  if (count < 1 || lo < 1 || hi < lo) {
+    fprintf(stderr, "Usage: ./libthom tune dgemmb [count=512] [lo=32] [hi=1024]\n");
+    exit(1);
+  }
   Set s = makeSet(count, lo, hi, 1234);
   lt_grouped_plan* plan = nullptr;
   LT_CHECK(lt_grouped_plan_create(s.probs.data(), count, LT_FORM_FP64, 0, &plan));
