@@ -815,6 +815,34 @@ def run_reference_hgemm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_peaks(args) -> None:
+    """Prints the measured tensor-pipe rates of the current GPU (lt_measure_peak) as one JSON line:
+    FP64 mma.sync and the INT8 tcgen05 shapes (M128 N128, M128 N256, CTA pair M256 N128), each as
+    the best of three single launches (burst) and after 0.5 s at the power limit (sustained), with
+    the SM clock (NVML, read only) before and after."""
+    import libthom_b200 as lt
+
+    def sm_mhz():
+        try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            return nv.nvmlDeviceGetClockInfo(nv.nvmlDeviceGetHandleByIndex(0), nv.NVML_CLOCK_SM)
+        except Exception:
+            return None
+
+    kinds = {"fp64_mma_tflops": lt.LT_PEAK_FP64_MMA, "int8_m128n128_tops": lt.LT_PEAK_INT8_MMA_N128,
+             "int8_m128n256_tops": lt.LT_PEAK_INT8_MMA_N256, "int8_pair_m256n128_tops": lt.LT_PEAK_INT8_MMA_PAIR}
+    res = {"sm_mhz_before": sm_mhz()}
+    for name, kind in kinds.items():
+        vals = [lt.measure_peak(kind) / 1e12 for _ in range(3)]
+        res[name] = max(vals)
+        res[name + "_all"] = vals
+        res[name + "_sustained"] = lt.measure_peak(kind | lt.LT_PEAK_SUSTAINED) / 1e12
+    res["sm_mhz_after"] = sm_mhz()
+    print(json.dumps(res), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -834,9 +862,13 @@ def main() -> None:
                     help="dgemm: the headline (default); hgemm: the FP16 routine on its tcgen05 kernel")
     ap.add_argument("--sweep", action="store_true",
                     help="print the phi x slice-count table (error and TFLOP/s of every form) instead")
+    ap.add_argument("--peaks", action="store_true",
+                    help="print the measured tensor-pipe rates of this GPU (lt_measure_peak) instead")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps, reported as run
-    if args.routine == "hgemm":
+    if args.peaks:
+        run_peaks(args)
+    elif args.routine == "hgemm":
         run_reference_hgemm(args) if args.impl == "reference" else run_hgemm(args)
     elif args.sweep:
         run_sweep(args)

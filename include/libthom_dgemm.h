@@ -39,8 +39,10 @@ extern "C" {
 int lt_get_last_error(void);
 const char* lt_error_string(int code);
 const char* lt_last_error_message(void);
-/* Reads (and clears) the device error word written by bounded waits inside the kernels; call after
- * a synchronize. Returns LT_OK or LT_ERR_DEVICE_TIMEOUT. */
+/* Reads (and clears) the device error words written by bounded waits inside the kernels — the
+ * library's per-device word and, once lt_dgemm_ozaki_noalloc has run on the device, that entry
+ * point's static word — on the current device; call after a synchronize. Allocates nothing.
+ * Returns LT_OK or LT_ERR_DEVICE_TIMEOUT. */
 int lt_check_device_status(void);
 /* Failure-detection self-test (no reference counterpart): launches one small kernel whose wait, the
  * same bounded mbarrier wait every pipeline uses, is on a barrier that nothing arrives at, with a
@@ -148,6 +150,10 @@ int lt_dgemm_ozaki_host(const double* A, const double* B, double* C, int64_t M, 
 #define LT_OZAKI_NOALLOC_BYTES (32ll << 20)
 int lt_dgemm_ozaki_noalloc(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
                            double alpha, double beta, int slices, void* stream);
+/* Failure-detection self-test of the allocation-free path (no reference counterpart): as
+ * lt_selftest_wait_timeout, but the wait that gives up reports into lt_dgemm_ozaki_noalloc's static
+ * error word (set up here if no call has done it yet), which lt_check_device_status then reads. */
+int lt_selftest_wait_timeout_noalloc(double limit_ms, void* stream);
 
 /* ---- automatic form ------------------------------------------------------------------------- */
 /* C = alpha*A*B + beta*C at FP64 accuracy in the faster form for this call: the learned selector

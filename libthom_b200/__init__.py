@@ -97,6 +97,7 @@ SIGNATURES = {
     "lt_ozaki_product": (_i32, [_vp, _i64, _i64, _i64, _f64, _f64, _i32, _vp, _sz, _vp]),
     "lt_dgemm_cublas": (_i32, _GEMM + [_vp]),
     "lt_dgemm_ozaki_noalloc": (_i32, _GEMM + [_i32, _vp]),
+    "lt_selftest_wait_timeout_noalloc": (_i32, [_f64, _vp]),
     "lt_grouped_plan_create": (_i32, [_vp, _i32, _i32, _i32, _c.POINTER(_vp)]),
     "lt_grouped_plan_run": (_i32, [_vp, _vp]),
     "lt_grouped_plan_run_graph": (_i32, [_vp, _vp]),

@@ -8,6 +8,8 @@
 
 namespace lt {
 
+struct DeviceStatus;  // lt_common.cuh
+
 int last_error();
 const char* last_message();
 
@@ -54,6 +56,11 @@ int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, 
              double beta, int slices, cudaStream_t stream);
 int noalloc_run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
                 double beta, int slices, cudaStream_t stream);
+// The allocation-free path's device error word (a static device variable): its address on device
+// `dev` (performing that path's per-device set-up), and a read-and-clear of it that reports zero
+// when the path was never set up on `dev`.
+int noalloc_status_word(int dev, DeviceStatus** st);
+int noalloc_take_status(int dev, DeviceStatus* out);
 struct Grouped;
 int grouped_create(const lt_gemm_problem* problems, int count, int slices, Grouped** out);
 int grouped_run(const Grouped* G, cudaStream_t stream);

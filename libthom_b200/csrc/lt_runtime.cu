@@ -3,6 +3,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "lt_internal.h"
 #include "lt_runtime.cuh"
 
 namespace lt {
@@ -77,6 +78,12 @@ DeviceContext* context() {
   c.status = st;
   c.device = dev;
   return &c;
+}
+
+DeviceContext* existing_context(int dev) {
+  if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(g_ctx_mutex);
+  return g_ctx[dev].device == dev ? &g_ctx[dev] : nullptr;
 }
 
 namespace {
@@ -214,14 +221,25 @@ const char* lt_error_string(int code) {
 }
 
 int lt_check_device_status(void) {
-  lt::DeviceContext* ctx = lt::context();
-  if (ctx == nullptr) return lt::last_error();
-  lt::DeviceStatus st;
-  LT_CUDA_TRY(cudaMemcpy(&st, ctx->status, sizeof st, cudaMemcpyDeviceToHost));
-  if (st.code != 0) {
-    LT_CUDA_TRY(cudaMemset(ctx->status, 0, sizeof st));
-    return lt::set_error(st.code, "device wait gave up (tag %d, block %d)", st.where, st.block);
+  // Two words can hold a report on the current device: the context's (every allocating entry
+  // point) and the allocation-free path's static one. Neither is created here, so a caller that
+  // only uses lt_dgemm_ozaki_noalloc still allocates nothing.
+  int dev = -1;
+  LT_CUDA_TRY(cudaGetDevice(&dev));
+  lt::DeviceStatus st{0, 0, 0, 0};
+  const char* which = "";
+  if (lt::DeviceContext* ctx = lt::existing_context(dev)) {
+    LT_CUDA_TRY(cudaMemcpy(&st, ctx->status, sizeof st, cudaMemcpyDeviceToHost));
+    if (st.code != 0) LT_CUDA_TRY(cudaMemset(ctx->status, 0, sizeof st));
   }
+  lt::DeviceStatus na{0, 0, 0, 0};
+  LT_TRY(lt::ozaki::noalloc_take_status(dev, &na));
+  if (st.code == 0 && na.code != 0) {
+    st = na;
+    which = " in the allocation-free path";
+  }
+  if (st.code != 0)
+    return lt::set_error(st.code, "device wait gave up%s (tag %d, block %d)", which, st.where, st.block);
   return LT_OK;
 }
 
@@ -232,6 +250,18 @@ int lt_selftest_wait_timeout(double limit_ms, void* stream) {
   if (ctx == nullptr) return lt::last_error();
   lt::wait_timeout_selftest_kernel<<<1, 64, 0, lt::as_stream(stream)>>>(static_cast<uint64_t>(limit_ms * 1e6),
                                                                          ctx->status);
+  LT_CUDA_TRY(cudaGetLastError());
+  return lt::ok();
+}
+
+int lt_selftest_wait_timeout_noalloc(double limit_ms, void* stream) {
+  if (!(limit_ms >= 0.001 && limit_ms <= 1000.0))
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "wait limit %g ms outside [0.001, 1000]", limit_ms);
+  int dev = -1;
+  LT_CUDA_TRY(cudaGetDevice(&dev));
+  lt::DeviceStatus* st = nullptr;
+  LT_TRY(lt::ozaki::noalloc_status_word(dev, &st));
+  lt::wait_timeout_selftest_kernel<<<1, 64, 0, lt::as_stream(stream)>>>(static_cast<uint64_t>(limit_ms * 1e6), st);
   LT_CUDA_TRY(cudaGetLastError());
   return lt::ok();
 }

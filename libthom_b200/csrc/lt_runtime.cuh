@@ -36,6 +36,8 @@ struct DeviceContext {
 
 // Context of the current device, created on first use. Returns nullptr (error recorded) on failure.
 DeviceContext* context();
+// Context of device `dev` if one has been created, else nullptr (nothing is created or recorded).
+DeviceContext* existing_context(int dev);
 // Ensures the cached workspace of the current device holds at least `bytes`.
 int ensure_workspace(DeviceContext* ctx, size_t bytes, void** ptr);
 // Same for the FP64 K-split partial sums (a buffer of its own).

@@ -36,6 +36,7 @@
 // CTA of the pair loads its halves of all slices with one copy too. Rows beyond M (N) in the last
 // block are zero.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -1451,11 +1452,9 @@ int both_stage(int s, const double* A, const double* B, int64_t M, int64_t N, in
   return LT_OK;
 }
 
-// Stage 1+2: exponents and slices of A and B into the workspace.
-int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int s, void* workspace,
-          size_t workspace_bytes, cudaStream_t stream) {
-  DeviceContext* ctx = context();
-  if (ctx == nullptr) return last_error();
+// Stage 1+2 on a given device description (see split).
+int split_on(const DeviceContext* ctx, const double* A, const double* B, int64_t M, int64_t N, int64_t K, int s,
+             void* workspace, size_t workspace_bytes, cudaStream_t stream) {
   const Layout L = layout_for(M, N, K, s);
   if (workspace_bytes < L.total) return set_error(LT_ERR_NO_MEMORY, "Ozaki workspace too small");
   uint8_t* ws = static_cast<uint8_t*>(workspace);
@@ -1470,6 +1469,14 @@ int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int
   return cols_stage(s, B, K, N, N, L.NC, amax_b, sb, ctx->sm_count, stream, pair_path(L.RBa) ? 1 : 0);
 }
 
+// Stage 1+2: exponents and slices of A and B into the workspace.
+int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int s, void* workspace,
+          size_t workspace_bytes, cudaStream_t stream) {
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  return split_on(ctx, A, B, M, N, K, s, workspace, workspace_bytes, stream);
+}
+
 // Products and recombination of one problem whose slices are in place: the CTA-pair kernel when
 // pr.pair is set (B slices split half-major), the one-CTA kernel otherwise.
 int launch_product(int s, const OzProblem& pr, DeviceContext* ctx, cudaStream_t stream) {
@@ -1482,11 +1489,9 @@ int launch_product(int s, const OzProblem& pr, DeviceContext* ctx, cudaStream_t 
   return launch_gemm<false>(s, pr, pr.rba * pr.rbb, ctx, stream);
 }
 
-// Stage 3+4: slice products on the tensor cores and the fused FP64 recombination into C.
-int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int s, const void* workspace,
-            size_t workspace_bytes, cudaStream_t stream) {
-  DeviceContext* ctx = context();
-  if (ctx == nullptr) return last_error();
+// Stage 3+4 on a given device description (see product).
+int product_on(DeviceContext* ctx, double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int s,
+               const void* workspace, size_t workspace_bytes, cudaStream_t stream) {
   const Layout L = layout_for(M, N, K, s);
   if (workspace_bytes < L.total) return set_error(LT_ERR_NO_MEMORY, "Ozaki workspace too small");
   const uint8_t* ws = static_cast<const uint8_t*>(workspace);
@@ -1506,6 +1511,14 @@ int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double bet
   pr.beta = beta;
   pr.pair = pair_path(L.RBa) ? 1 : 0;
   return launch_product(s, pr, ctx, stream);
+}
+
+// Stage 3+4: slice products on the tensor cores and the fused FP64 recombination into C.
+int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int s, const void* workspace,
+            size_t workspace_bytes, cudaStream_t stream) {
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  return product_on(ctx, C, M, N, K, alpha, beta, s, workspace, workspace_bytes, stream);
 }
 
 // Row strides and transposes (lt_dgemm_ex): op(A) = A (M x K, row stride lda) or A^T (A stored
@@ -1908,17 +1921,20 @@ struct NoAllocDevice {
   void* scratch = nullptr;     // device address of g_noalloc_scratch on this device
   DeviceStatus* status = nullptr;
   int sm_count = 0;
+  std::atomic<bool> ready{false};  // set-up done on this device: its status word may hold a report
 };
 NoAllocDevice g_noalloc[64];
 
 // Per-device set-up on the first call made with that device current. In host code the symbols'
 // names are host-side stand-ins, so their device addresses come from cudaGetSymbolAddress.
 int noalloc_setup(int dev, NoAllocDevice** out) {
+  if (dev < 0 || dev >= 64) return set_error(LT_ERR_INVALID_ARGUMENT, "device %d out of range", dev);
   NoAllocDevice& d = g_noalloc[dev];
   std::call_once(d.once, [&] {
     d.err = cudaGetSymbolAddress(&d.scratch, g_noalloc_scratch);
     if (d.err == cudaSuccess) d.err = cudaGetSymbolAddress(reinterpret_cast<void**>(&d.status), g_noalloc_status);
     if (d.err == cudaSuccess) d.err = cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (d.err == cudaSuccess) d.ready.store(true);
   });
   if (d.err != cudaSuccess)
     return set_error(LT_ERR_CUDA, "static scratch set-up failed: %s", cudaGetErrorString(d.err));
@@ -1927,6 +1943,25 @@ int noalloc_setup(int dev, NoAllocDevice** out) {
 }
 
 }  // namespace
+
+// Device address of the allocation-free path's error word on device `dev` (set-up included).
+int noalloc_status_word(int dev, DeviceStatus** st) {
+  NoAllocDevice* nd = nullptr;
+  LT_TRY(noalloc_setup(dev, &nd));
+  *st = nd->status;
+  return LT_OK;
+}
+
+// Reads the allocation-free path's error word on device `dev` into *out and clears it; *out is
+// zero when that path has not been set up on the device (nothing can have reported there).
+int noalloc_take_status(int dev, DeviceStatus* out) {
+  *out = DeviceStatus{0, 0, 0, 0};
+  if (dev < 0 || dev >= 64 || !g_noalloc[dev].ready.load()) return LT_OK;
+  DeviceStatus* st = g_noalloc[dev].status;
+  LT_CUDA_TRY(cudaMemcpy(out, st, sizeof *out, cudaMemcpyDeviceToHost));
+  if (out->code != 0) LT_CUDA_TRY(cudaMemset(st, 0, sizeof *out));
+  return LT_OK;
+}
 
 int noalloc_run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
                 double beta, int s, cudaStream_t stream) {
@@ -1944,39 +1979,16 @@ int noalloc_run(const double* A, const double* B, double* C, int64_t M, int64_t 
                      static_cast<long long>(LT_OZAKI_NOALLOC_BYTES));
   NoAllocDevice* nd = nullptr;
   LT_TRY(noalloc_setup(dev, &nd));
-  DeviceContext ctx;  // a stack description of the device: nothing is allocated
+  // A stack description of the device (nothing is allocated) whose status word is the static one,
+  // read by lt_check_device_status. The split and the product are the stages lt_dgemm_ozaki runs,
+  // with the same launch plan (CTA-pair kernel and half-major B slices where it takes them), so
+  // the results are bit-identical to it.
+  DeviceContext ctx;
   ctx.device = dev;
   ctx.sm_count = nd->sm_count;
   ctx.status = nd->status;
-  uint8_t* ws = static_cast<uint8_t*>(nd->scratch);
-  auto* amax_a = reinterpret_cast<unsigned long long*>(ws + L.off_amax_a);
-  auto* amax_b = reinterpret_cast<unsigned long long*>(ws + L.off_amax_b);
-  auto* sa = reinterpret_cast<int8_t*>(ws + L.off_sa);
-  auto* sb = reinterpret_cast<int8_t*>(ws + L.off_sb);
-  // exponents start from zero (atomicMax); the slice tiles are fully rewritten by the split
-  LT_CUDA_TRY(cudaMemsetAsync(ws, 0, L.off_sa, stream));
-  const int sms = ctx.sm_count;
-  if (K > 0) {
-    int64_t row_blocks = (M + 7) / 8;
-    int64_t ksplit = (4 * sms + row_blocks - 1) / row_blocks;
-    ksplit = ksplit < 1 ? 1 : ksplit;
-    int64_t kseg = round_up((K + ksplit - 1) / ksplit, 256);
-    ksplit = (K + kseg - 1) / kseg;
-    amax_rows_kernel<<<dim3(static_cast<unsigned>(row_blocks), static_cast<unsigned>(ksplit)), 256, 0, stream>>>(
-        A, M, K, K, kseg, amax_a);
-    LT_CUDA_TRY(cudaGetLastError());
-    int64_t col_blocks = (N + 255) / 256;
-    int64_t ksplit_b = (8 * sms + col_blocks - 1) / col_blocks;
-    ksplit_b = ksplit_b < 1 ? 1 : ksplit_b;
-    int64_t kseg_b = (K + ksplit_b - 1) / ksplit_b;
-    ksplit_b = (K + kseg_b - 1) / kseg_b;
-    amax_cols_kernel<<<dim3(static_cast<unsigned>(col_blocks), static_cast<unsigned>(ksplit_b)), 256, 0, stream>>>(
-        B, K, N, N, kseg_b, amax_b, 0);
-    LT_CUDA_TRY(cudaGetLastError());
-  }
-  LT_TRY(launch_split(s, A, B, M, N, K, L, amax_a, amax_b, sa, sb, sms, stream));
-  OzProblem pr{sa, sb, C, amax_a, amax_b, M, N, L.NC, L.RBa, L.RBb, alpha, beta, N};
-  return launch_gemm<false>(s, pr, L.RBa * L.RBb, &ctx, stream);
+  LT_TRY(split_on(&ctx, A, B, M, N, K, s, nd->scratch, L.total, stream));
+  return product_on(&ctx, C, M, N, K, alpha, beta, s, nd->scratch, L.total, stream);
 }
 
 }  // namespace ozaki

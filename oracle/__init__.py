@@ -23,9 +23,17 @@ _c = ctypes
 _vp, _i64, _i32, _f64, _u64 = _c.c_void_p, _c.c_int64, _c.c_int, _c.c_double, _c.c_uint64
 
 
+# Where the reference project's sources are read from to build oracle/_ref: LIBTHOM_REFERENCE_SRC,
+# else the checkout this build was developed against (absent on machines that only run the tests;
+# there the prebuilt oracle/_ref files, or none, are used).
+REFERENCE_SRC = os.environ.get("LIBTHOM_REFERENCE_SRC", "/root/reference")
+
+
 def build(quiet: bool = True) -> None:
     """Compiles liboracle.so, and oracle/_ref when the reference sources are present."""
-    out = subprocess.run(["make", "-C", str(HERE), "all"], stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    ref = REFERENCE_SRC if Path(REFERENCE_SRC, "routines").is_dir() else ""
+    out = subprocess.run(["make", "-C", str(HERE), "all", f"REF={ref}"], stdout=subprocess.PIPE,
+                         stderr=subprocess.STDOUT, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout)
     if not quiet:
