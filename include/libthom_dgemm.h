@@ -155,6 +155,43 @@ int lt_dgemm_ozaki_noalloc(const double* A, const double* B, double* C, int64_t 
  * error word (set up here if no call has done it yet), which lt_check_device_status then reads. */
 int lt_selftest_wait_timeout_noalloc(double limit_ms, void* stream);
 
+/* ---- Ozaki scheme II: the CRT form (no reference counterpart) ------------------------------- */
+/* C = alpha*A*B + beta*C from `moduli` INT8 tensor-core products. Rows of A and columns of B are
+ * scaled by powers of two to integers of pa and pb bits (K 2^(pa+pb) <= Mprod / 4, Mprod the product
+ * of the moduli); each product multiplies the residues of those integers modulo one of the first
+ * `moduli` of the pairwise-coprime moduli 256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217,
+ * 211, 199, 197, 193, 191, 181, 179, 173 exactly, and the Chinese remainder theorem recovers the exact
+ * integer product, which FP64 scales back (Ozaki, Uchino and Imamura's scheme II). The only error is
+ * the truncation of A and B to pa and pb bits: on U[-1,1) entries at K = 8192, 15 moduli (pa = pb = 51)
+ * are as accurate as native FP64; each further modulus adds about 8 bits. Rows of A or columns of B
+ * holding NaN or Inf give NaN in their row / column of C. K up to 8388480. Bit-identical to the CPU
+ * restatement. */
+#define LT_OZAKI_CRT_MIN_MODULI 8
+#define LT_OZAKI_CRT_MAX_MODULI 20
+/* Uses the library's cached per-device workspace (grown with cudaMalloc on demand). */
+int lt_dgemm_ozaki_crt(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
+                       double beta, int moduli, void* stream);
+/* Same with a caller-provided device workspace (256-byte aligned, at least lt_ozaki_crt_workspace_size
+ * bytes); performs no allocation. */
+size_t lt_ozaki_crt_workspace_size(int64_t M, int64_t N, int64_t K, int moduli);
+int lt_dgemm_ozaki_crt_ws(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
+                          double beta, int moduli, void* workspace, size_t workspace_bytes, void* stream);
+/* The two stages, for callers that time or overlap them: exponents and residues of A and B into the
+ * workspace; then the products, the reconstruction and the alpha/beta epilogue into C. */
+int lt_ozaki_crt_split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int moduli, void* workspace,
+                       size_t workspace_bytes, void* stream);
+int lt_ozaki_crt_product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int moduli,
+                         const void* workspace, size_t workspace_bytes, void* stream);
+/* The operand bits pa, pb the CRT form uses for `moduli` moduli and inner dimension K, and the moduli
+ * themselves (moduli_out: `moduli` ints; any pointer may be NULL). Host arithmetic only. */
+int lt_ozaki_crt_info(int moduli, int64_t K, int* pa, int* pb, int* moduli_out);
+/* Reference-contract entry points (routines/dgemm/dgemm.h:9 signature) with 14..18 moduli. */
+float dgemm_ozaki_crt14(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);
+float dgemm_ozaki_crt15(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);
+float dgemm_ozaki_crt16(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);
+float dgemm_ozaki_crt17(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);
+float dgemm_ozaki_crt18(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);
+
 /* ---- automatic form ------------------------------------------------------------------------- */
 /* C = alpha*A*B + beta*C at FP64 accuracy in the faster form for this call: the learned selector
  * picks the slice count s that meets lt_set_ozaki_tolerance() (default 1e-15), then a cost model of

@@ -29,6 +29,8 @@ LT_ERR_DEVICE_TIMEOUT = 5
 LT_ERR_UNSUPPORTED = 6
 LT_ERR_NOT_FOUND = 7
 LT_OZAKI_MAX_SLICES = 12
+LT_OZAKI_CRT_MIN_MODULI = 8
+LT_OZAKI_CRT_MAX_MODULI = 20
 LT_FORM_FP64 = 0
 LT_FORM_OZAKI = 1
 LT_PEAK_FP64_MMA = 0
@@ -42,7 +44,8 @@ LT_SEL_CLASSES = 8
 LT_SEL_PARAMS = (LT_SEL_FEATURES * LT_SEL_HIDDEN + LT_SEL_HIDDEN + LT_SEL_HIDDEN * LT_SEL_HIDDEN +
                  LT_SEL_HIDDEN + LT_SEL_HIDDEN * LT_SEL_CLASSES + LT_SEL_CLASSES)
 
-IMPLS = ["tc100"] + [f"ozaki{s}" for s in range(3, 11)] + ["ozaki_auto", "auto", "cublas_tc"]
+IMPLS = (["tc100"] + [f"ozaki{s}" for s in range(3, 11)] + ["ozaki_auto", "auto", "cublas_tc"]
+         + [f"ozaki_crt{n}" for n in range(14, 19)])
 
 _c = ctypes
 _vp, _i64, _i32, _f64, _f32, _sz = _c.c_void_p, _c.c_int64, _c.c_int, _c.c_double, _c.c_float, _c.c_size_t
@@ -97,6 +100,14 @@ SIGNATURES = {
     "lt_ozaki_product": (_i32, [_vp, _i64, _i64, _i64, _f64, _f64, _i32, _vp, _sz, _vp]),
     "lt_dgemm_cublas": (_i32, _GEMM + [_vp]),
     "lt_dgemm_ozaki_noalloc": (_i32, _GEMM + [_i32, _vp]),
+    "lt_dgemm_ozaki_crt": (_i32, _GEMM + [_i32, _vp]),
+    "lt_ozaki_crt_workspace_size": (_sz, [_i64, _i64, _i64, _i32]),
+    "lt_dgemm_ozaki_crt_ws": (_i32, _GEMM + [_i32, _vp, _sz, _vp]),
+    "lt_ozaki_crt_split": (_i32, [_vp, _vp, _i64, _i64, _i64, _i32, _vp, _sz, _vp]),
+    "lt_ozaki_crt_product": (_i32, [_vp, _i64, _i64, _i64, _f64, _f64, _i32, _vp, _sz, _vp]),
+    "lt_ozaki_crt_info": (_i32, [_i32, _i64, _c.POINTER(_i32), _c.POINTER(_i32), _c.POINTER(_i32)]),
+    "dgemm_ozaki_crt14": (_f32, _REF), "dgemm_ozaki_crt15": (_f32, _REF), "dgemm_ozaki_crt16": (_f32, _REF),
+    "dgemm_ozaki_crt17": (_f32, _REF), "dgemm_ozaki_crt18": (_f32, _REF),
     "lt_selftest_wait_timeout_noalloc": (_i32, [_f64, _vp]),
     "lt_grouped_plan_create": (_i32, [_vp, _i32, _i32, _i32, _c.POINTER(_vp)]),
     "lt_grouped_plan_run": (_i32, [_vp, _vp]),
@@ -213,6 +224,37 @@ def dgemm_ozaki(A, B, C, M, N, K, alpha=1.0, beta=0.0, slices=8, stream=None, wo
         check(lib().lt_dgemm_ozaki_ws(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, slices,
                                       _ptr(workspace), workspace.numel() * workspace.element_size(),
                                       _stream(stream)))
+
+
+def dgemm_ozaki_crt(A, B, C, M, N, K, alpha=1.0, beta=0.0, moduli=15, stream=None, workspace=None) -> None:
+    """CRT form (Ozaki scheme II) with `moduli` INT8 products (lt_dgemm_ozaki_crt / _ws)."""
+    if workspace is None:
+        check(lib().lt_dgemm_ozaki_crt(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, moduli, _stream(stream)))
+    else:
+        check(lib().lt_dgemm_ozaki_crt_ws(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, moduli, _ptr(workspace),
+                                          workspace.numel() * workspace.element_size(), _stream(stream)))
+
+
+def ozaki_crt_split(A, B, M, N, K, moduli, workspace, stream=None) -> None:
+    check(lib().lt_ozaki_crt_split(_ptr(A), _ptr(B), M, N, K, moduli, _ptr(workspace),
+                                   workspace.numel() * workspace.element_size(), _stream(stream)))
+
+
+def ozaki_crt_product(C, M, N, K, alpha, beta, moduli, workspace, stream=None) -> None:
+    check(lib().lt_ozaki_crt_product(_ptr(C), M, N, K, alpha, beta, moduli, _ptr(workspace),
+                                     workspace.numel() * workspace.element_size(), _stream(stream)))
+
+
+def ozaki_crt_workspace_size(M, N, K, moduli) -> int:
+    return int(lib().lt_ozaki_crt_workspace_size(M, N, K, moduli))
+
+
+def ozaki_crt_info(moduli: int, K: int) -> tuple[int, int, list[int]]:
+    """(pa, pb, moduli list) of the CRT form (host arithmetic)."""
+    pa, pb = ctypes.c_int(), ctypes.c_int()
+    mods = (ctypes.c_int * moduli)()
+    check(lib().lt_ozaki_crt_info(moduli, K, ctypes.byref(pa), ctypes.byref(pb), mods))
+    return pa.value, pb.value, list(mods)
 
 
 def ozaki_split(A, B, M, N, K, slices, workspace, stream=None) -> None:

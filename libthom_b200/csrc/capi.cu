@@ -268,4 +268,19 @@ LT_OZAKI_WRAPPER(9)
 LT_OZAKI_WRAPPER(10)
 #undef LT_OZAKI_WRAPPER
 
+#define LT_CRT_WRAPPER(NM)                                                                                  \
+  float dgemm_ozaki_crt##NM(const double* A, const double* B, double* C, size_t M, size_t N, size_t K,        \
+                            double alpha, double beta) {                                                   \
+    return lt::timed("ozaki_crt" #NM, [&] {                                                                 \
+      return lt_dgemm_ozaki_crt(A, B, C, static_cast<int64_t>(M), static_cast<int64_t>(N),                  \
+                                static_cast<int64_t>(K), alpha, beta, NM, nullptr);                         \
+    });                                                                                                     \
+  }
+LT_CRT_WRAPPER(14)
+LT_CRT_WRAPPER(15)
+LT_CRT_WRAPPER(16)
+LT_CRT_WRAPPER(17)
+LT_CRT_WRAPPER(18)
+#undef LT_CRT_WRAPPER
+
 }  // extern "C"

@@ -398,6 +398,21 @@ __device__ __forceinline__ uint32_t elect_one_sync() {
   return pred;
 }
 
+// Exponent of a row's (column's) largest magnitude given as IEEE bits (NaN/Inf order above every
+// finite value, so one max over the bits finds both): e with max < 2^e (frexp), 0 for an all-zero
+// row, kSentinel when the row holds NaN or Inf.
+constexpr int kSentinel = 0x7fffffff;
+__device__ __forceinline__ int exponent_of_maxbits(unsigned long long bits) {
+  if (bits == 0ull) return 0;
+  if (bits >= 0x7ff0000000000000ull) return kSentinel;
+  int e;
+  frexp(__longlong_as_double(static_cast<long long>(bits)), &e);
+  return e;
+}
+__device__ __forceinline__ unsigned long long abs_bits(double v) {
+  return static_cast<unsigned long long>(__double_as_longlong(v)) & 0x7fffffffffffffffull;
+}
+
 // Exact 2^e for e in [-1022, 1023] built from its bit pattern.
 __device__ __forceinline__ double pow2i(int e) {
   return __longlong_as_double(static_cast<long long>(e + 1023) << 52);

@@ -43,6 +43,10 @@ int lookup(int64_t M, int64_t N, int64_t K, bool tma);
 
 namespace ozaki {
 size_t workspace_size(int64_t M, int64_t N, int64_t K, int slices);
+// Row maxima of A (M x K, pitch K) and column maxima of B (K x N, pitch N) as IEEE bits, one launch;
+// M, N, K > 0 and both arrays zero on entry.
+int exponents(const double* A, const double* B, int64_t M, int64_t N, int64_t K, unsigned long long* amax_a,
+              unsigned long long* amax_b, int sms, cudaStream_t stream);
 int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int slices, void* workspace,
           size_t workspace_bytes, cudaStream_t stream);
 int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int slices, const void* workspace,

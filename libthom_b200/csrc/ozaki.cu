@@ -60,7 +60,6 @@ constexpr int kThreads = 320;                    // warp 0 loads, warp 1 MMA, wa
 constexpr int kEpilogueWarps = 8;
 constexpr int kMaxSmem = 232448;                 // sm_100 opt-in dynamic shared memory per block
 constexpr int kSmemOverhead = 1024 + 256;        // alignment slack + barriers
-constexpr int kSentinel = 0x7fffffff;            // exponent of a row/column holding NaN or Inf
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 inline int64_t ceil_div(int64_t x, int64_t m) { return (x + m - 1) / m; }
@@ -92,18 +91,6 @@ size_t workspace_size(int64_t M, int64_t N, int64_t K, int slices) { return layo
 // ---------------------------------------------------------------------------------------------
 // Exponents
 // ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ int exponent_of_maxbits(unsigned long long bits) {
-  if (bits == 0ull) return 0;
-  if (bits >= 0x7ff0000000000000ull) return kSentinel;
-  int e;
-  frexp(__longlong_as_double(static_cast<long long>(bits)), &e);
-  return e;
-}
-
-__device__ __forceinline__ unsigned long long abs_bits(double v) {
-  return static_cast<unsigned long long>(__double_as_longlong(v)) & 0x7fffffffffffffffull;
-}
-
 // Row maxima of A: block (bx, by) covers 8 rows (one warp each) and K segment by.
 __device__ __forceinline__ void amax_rows_block(const double* __restrict__ A, int64_t M, int64_t K, int64_t lda,
                                                 int64_t kseg, unsigned long long* __restrict__ amax, int64_t bx,
@@ -1421,10 +1408,10 @@ void launch_split_both_s(const double* A, const double* B, int64_t M, int64_t N,
                                                                            amax_b, sa, sb, ga, gb, half_major_b);
 }
 
-int both_stage(int s, const double* A, const double* B, int64_t M, int64_t N, int64_t K, const Layout& L,
-               unsigned long long* amax_a, unsigned long long* amax_b, int8_t* sa, int8_t* sb, int sms,
-               cudaStream_t stream, int half_major_b) {
-  // exponents: the blocks rows_stage and cols_stage would launch
+// Row maxima of A and column maxima of B (row pitches K and N) in one launch, the blocks rows_stage
+// and cols_stage would launch; M, N, K > 0, amax zero on entry. Shared with the CRT form.
+int exponents(const double* A, const double* B, int64_t M, int64_t N, int64_t K, unsigned long long* amax_a,
+              unsigned long long* amax_b, int sms, cudaStream_t stream) {
   const int64_t ra = (M + 7) / 8;
   int64_t ka = (4 * sms + ra - 1) / ra;
   ka = ka < 1 ? 1 : ka;
@@ -1440,6 +1427,13 @@ int both_stage(int s, const double* A, const double* B, int64_t M, int64_t N, in
   amax_both_kernel<<<static_cast<unsigned>(ra * ka + rb * kb), 256, 0, stream>>>(A, M, K, kseg_a, ra, ka, amax_a, B, N,
                                                                                   kseg_b, rb, pairs, amax_b);
   LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
+int both_stage(int s, const double* A, const double* B, int64_t M, int64_t N, int64_t K, const Layout& L,
+               unsigned long long* amax_a, unsigned long long* amax_b, int8_t* sa, int8_t* sb, int sms,
+               cudaStream_t stream, int half_major_b) {
+  LT_TRY(exponents(A, B, M, N, K, amax_a, amax_b, sms, stream));
   switch (s) {
 #define LT_BOTH_CASE(S) \
   case S: launch_split_both_s<S>(A, B, M, N, K, L, amax_a, amax_b, sa, sb, sms, stream, half_major_b); break;

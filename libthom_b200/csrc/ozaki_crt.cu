@@ -1,0 +1,993 @@
+// ozaki_crt.cu — DGEMM in the Ozaki scheme II ("CRT form") on INT8 tensor cores for sm_100a.
+//
+// No reference counterpart: a new implementation behind the reference's dgemm contract
+// (routines/dgemm/dgemm.h:9). Method: Ozaki, Uchino and Imamura's scheme II (integer emulation
+// of a floating-point product through modular arithmetic and the Chinese remainder theorem),
+// written here from the mathematics:
+//
+//   1. exponents (HBM-bound, shared with the slice form): sigma_i, tau_j = frexp exponents of the
+//      row maxima of A and the column maxima of B.
+//   2. residues (HBM-bound): V = trunc(A[i,k] 2^(pa - sigma_i)) and W = trunc(B[k,j] 2^(pb - tau_j))
+//      are integers below 2^pa, 2^pb in magnitude, with K 2^(pa+pb) <= Mprod / 4, Mprod the product
+//      of n pairwise-coprime moduli m_l <= 256. Each is written as n symmetric residues (one signed
+//      byte each): plane l of A holds V mod m_l, row-major [M][Kp]; plane l of B holds W mod m_l
+//      transposed, [N][Kp] (K-major, as the tensor core reads both operands).
+//   3. products (tensor cores): for each modulus, one INT8 x INT8 -> INT32 GEMM of the residue
+//      planes (exact), reduced to the symmetric residue c_l of (sum_k V W) mod m_l and stored as the
+//      byte c_l + 128 in residue plane l of C.
+//   4. reconstruction (FP64 ALU, its own kernel): C' = sum_k V W is the integer in (-Mprod/2,
+//      Mprod/2) with C' = c_l (mod m_l). With the CRT basis P_l = (Mprod/m_l) y_l,
+//      y_l = (Mprod/m_l)^-1 mod m_l, split into nl limbs of w bits: L_k = sum_l c_l P_lk (exact in
+//      FP64), Q = rint(L_hi F_hi + L_lo F_lo) (F_k = 2^(w k) / Mprod), D_k = fma(-Q, M_k, L_k) and
+//      C' = Horner of the D_k in base 2^w; then C = fma(alpha, C' 2^(sigma_i - pa) 2^(tau_j - pb),
+//      beta C0). The CPU oracle (oracle/oracle.c, oracle_crt_dgemm) performs the same arithmetic,
+//      so results are bit-identical.
+//
+// Against the slice form (ozaki.cu) the product count is n, not s(s+1)/2: at FP64 accuracy on the
+// 8192^3 workload 15 INT8 products instead of 28.
+//
+// Product kernel: persistent CTA pairs; a pair owns a 256 x 256 tile of C and, for each modulus in
+// turn, runs the whole K loop of that modulus into one of two TMEM accumulators (256 columns each)
+// with tcgen05.mma.cta_group::2.kind::i8 (M256 N256 K32), operands staged by 3-D TMA (plane = the
+// modulus) with 128-byte swizzle. Roles (320 threads per CTA):
+//   warp 0      TMA producer (both CTAs)
+//   warp 1      rank 0: MMA issuer for the pair; rank 1: forwards each landed stage to rank 0
+//   warps 2..9  drain: TMEM -> registers, INT32 -> symmetric residue, bytes to the residue planes,
+//               then the accumulator goes back to the MMA warp
+// The reconstruction runs afterwards as a separate kernel at full occupancy: done inside the product
+// kernel by a few warps it was latency-bound (one warp per sub-partition, long FP64 chains, global
+// round trips) and held the tensor pipe back. Every wait is bounded (LT_WAIT_TIMEOUT_NS).
+#include <cuda.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "lt_internal.h"
+#include "lt_runtime.cuh"
+
+namespace lt {
+namespace crt {
+
+constexpr int kMaxMod = LT_OZAKI_CRT_MAX_MODULI;
+constexpr int kMinMod = LT_OZAKI_CRT_MIN_MODULI;
+// Pairwise-coprime moduli no larger than 256, largest first (256 = 2^8; 255 = 3*5*17; 253 = 11*23;
+// 247 = 13*19; 217 = 7*31; the rest prime): every symmetric residue is one signed byte.
+constexpr int kModuli[kMaxMod] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
+                                  223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
+constexpr int kBM = 128;                          // rows of C per CTA (256 per pair)
+constexpr int kBN = 256;                          // columns of C per pair tile (N of one pair MMA)
+constexpr int kBK = 128;                          // K bytes per stage (one 128-byte swizzle row)
+constexpr int kMmaK = 32;                         // K of one kind::i8 MMA
+constexpr int kABytes = kBM * kBK;                // 16 KB
+constexpr int kBBytes = (kBN / 2) * kBK;          // 16 KB: this CTA's 128 rows of the tile's B
+constexpr int kStageBytes = kABytes + kBBytes;
+constexpr int kMaxSmem = 232448;
+constexpr int kOverhead = 1024 + 512;
+constexpr int kStages = std::min(8, (kMaxSmem - kOverhead) / kStageBytes);
+constexpr int kSmem = kStages * kStageBytes + kOverhead;
+constexpr int kDrainWarps = 8;                    // two per TMEM lane quarter, each half the columns
+constexpr int kThreads = 64 + 32 * kDrainWarps;
+constexpr int kGroupSteps = 1023;                 // K steps per INT32 accumulation: 1023*128*128^2 < 2^31
+static_assert(kStages >= 3, "shared-memory ring too small");
+
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+inline int64_t ceil_div(int64_t x, int64_t m) { return (x + m - 1) / m; }
+
+// ---------------------------------------------------------------------------------------------
+// Constants of a modulus set (host arithmetic, exact)
+// ---------------------------------------------------------------------------------------------
+struct Consts {
+  int n, nl, w, pa, pb;
+  int32_t m[kMaxMod];
+  int32_t h[kMaxMod];             // (m - 1) / 2: symmetric residue = residue of V + h in [0, m), minus h
+  // residues of the scaled inputs: x = dp4a(bytes of V + 2^62, coef) + add, x mod m by umulhi
+  uint32_t coef_lo[kMaxMod], coef_hi[kMaxMod];  // bytes (2^(8d) mod m), d = 0..3 and 4..7
+  uint32_t add[kMaxMod];                        // m - (2^62 mod m) + h
+  uint32_t split_magic[kMaxMod];                // ceil(2^32 / m)
+  // INT32 accumulators -> residues: y = (acc >> 16) c16 + (acc & 0xffff) + bias, q = umulhi(y, magic) >> 7
+  int32_t c16[kMaxMod];           // 2^16 mod m
+  int32_t bias[kMaxMod];          // m ceil(2^23 / m): y + bias in [0, 2^25)
+  uint32_t drain_magic[kMaxMod];  // ceil(2^39 / m)
+  // reconstruction
+  double P[kMaxMod][4];  // limbs of the CRT basis
+  double Mk[4];          // limbs of Mprod
+  double Kc[4];          // -128 sum_l P_lk (residues are stored as c + 128)
+  double f_hi, f_lo;
+};
+
+// Unsigned integers of up to 256 bits (little-endian 32-bit words): what the constants need.
+struct Big {
+  uint32_t d[8] = {};
+  void mul_small(uint32_t v) {
+    uint64_t carry = 0;
+    for (uint32_t& x : d) {
+      const uint64_t t = static_cast<uint64_t>(x) * v + carry;
+      x = static_cast<uint32_t>(t);
+      carry = t >> 32;
+    }
+  }
+  uint32_t divmod_small(uint32_t v) {  // *this /= v, returns the remainder
+    uint64_t rem = 0;
+    for (int i = 7; i >= 0; --i) {
+      const uint64_t cur = (rem << 32) | d[i];
+      d[i] = static_cast<uint32_t>(cur / v);
+      rem = cur % v;
+    }
+    return static_cast<uint32_t>(rem);
+  }
+  int bit_length() const {
+    for (int i = 7; i >= 0; --i)
+      if (d[i] != 0) return 32 * i + 32 - __builtin_clz(d[i]);
+    return 0;
+  }
+  uint64_t bits(int lo, int w) const {  // bits lo .. lo+w-1 (w <= 48)
+    uint64_t r = 0;
+    for (int b = 0; b < w; ++b) {
+      const int i = lo + b;
+      if (i < 256 && ((d[i >> 5] >> (i & 31)) & 1u)) r |= uint64_t(1) << b;
+    }
+    return r;
+  }
+};
+
+inline uint32_t pow2_mod(int e, uint32_t m) {
+  uint64_t r = 1 % m;
+  for (int i = 0; i < e; ++i) r = (r * 2) % m;
+  return static_cast<uint32_t>(r);
+}
+
+inline uint32_t inverse_mod(uint32_t a, uint32_t m) {  // a^-1 mod m, gcd(a, m) = 1
+  int64_t t = 0, nt = 1, r = m, nr = a % m;
+  while (nr != 0) {
+    const int64_t q = r / nr;
+    int64_t x = t - q * nt; t = nt; nt = x;
+    x = r - q * nr; r = nr; nr = x;
+  }
+  return static_cast<uint32_t>(t < 0 ? t + m : t);
+}
+
+// Constants for n moduli and inner dimension K (K >= 1): pa + pb is the largest T with
+// K 2^T <= Mprod / 4, split evenly, each at most 62 (the residues are taken from 64-bit integers).
+Consts make_consts(int n, int64_t K) {
+  Consts c;
+  std::memset(&c, 0, sizeof c);
+  c.n = n;
+  Big Mp;
+  Mp.d[0] = 1;
+  for (int l = 0; l < n; ++l) Mp.mul_small(static_cast<uint32_t>(kModuli[l]));
+  c.w = n <= 16 ? 42 : 41;  // n 2^7 2^w <= 2^53: the limb sums stay exact
+  c.nl = (Mp.bit_length() + c.w - 1) / c.w;
+  for (int l = 0; l < n; ++l) {
+    const uint32_t m = static_cast<uint32_t>(kModuli[l]);
+    c.m[l] = static_cast<int32_t>(m);
+    c.h[l] = static_cast<int32_t>((m - 1) / 2);
+    uint32_t lo = 0, hi = 0;
+    for (int b = 0; b < 4; ++b) {
+      lo |= pow2_mod(8 * b, m) << (8 * b);
+      hi |= pow2_mod(8 * (b + 4), m) << (8 * b);
+    }
+    c.coef_lo[l] = lo;
+    c.coef_hi[l] = hi;
+    c.add[l] = m - pow2_mod(62, m) + (m - 1) / 2;
+    c.split_magic[l] = static_cast<uint32_t>(((uint64_t(1) << 32) + m - 1) / m);
+    c.c16[l] = static_cast<int32_t>(pow2_mod(16, m));
+    c.bias[l] = static_cast<int32_t>(m * (((uint32_t(1) << 23) + m - 1) / m));
+    c.drain_magic[l] = static_cast<uint32_t>(((uint64_t(1) << 39) + m - 1) / m);
+    Big Ml = Mp;
+    Ml.divmod_small(m);
+    Big t = Ml;
+    const uint32_t r = t.divmod_small(m);
+    Big P = Ml;
+    P.mul_small(inverse_mod(r, m));
+    for (int k = 0; k < c.nl; ++k) c.P[l][k] = static_cast<double>(P.bits(c.w * k, c.w));
+  }
+  for (int k = 0; k < c.nl; ++k) {
+    c.Mk[k] = static_cast<double>(Mp.bits(c.w * k, c.w));
+    int64_t s = 0;
+    for (int l = 0; l < n; ++l) s += static_cast<int64_t>(c.P[l][k]);
+    c.Kc[k] = -128.0 * static_cast<double>(s);
+  }
+  double md = c.Mk[c.nl - 1];
+  for (int k = c.nl - 2; k >= 0; --k) md = std::fma(md, std::ldexp(1.0, c.w), c.Mk[k]);
+  c.f_hi = std::ldexp(1.0, c.w * (c.nl - 1)) / md;
+  c.f_lo = std::ldexp(1.0, c.w * (c.nl - 2)) / md;
+  Big q = Mp;
+  q.divmod_small(static_cast<uint32_t>(2 * std::max<int64_t>(K, 1)));
+  const int T = q.bit_length() - 2;
+  c.pa = std::min(62, T / 2);
+  c.pb = std::min(62, T - T / 2);
+  return c;
+}
+
+// Limbs of the reconstruction for NM moduli: ceil(bit length of Mprod / w), w = 42 up to 16 moduli
+// and 41 above (make_consts derives the same count; the launchers check it).
+__host__ __device__ constexpr int limbs_for(int nm) { return nm <= 10 ? 2 : (nm <= 16 ? 3 : 4); }
+
+// The constants of every modulus count in constant memory (filled once per device), read by the
+// kernels with compile-time offsets through the constant cache. pa and pb, which depend on K, are
+// kernel arguments.
+__constant__ Consts c_table[kMaxMod - kMinMod + 1];
+
+int ensure_table(int device) {
+  static std::once_flag once[64];
+  static cudaError_t err[64];
+  std::call_once(once[device], [&] {
+    Consts host[kMaxMod - kMinMod + 1];
+    for (int n = kMinMod; n <= kMaxMod; ++n) host[n - kMinMod] = make_consts(n, 1);
+    err[device] = cudaMemcpyToSymbol(c_table, host, sizeof host);
+  });
+  LT_CUDA_TRY(err[device]);
+  return LT_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Workspace: [amaxA: M u64][amaxB: N u64][A residues n x M x Kp][B residues n x N x Kp]
+//            [C residue planes n x Mp x Np], 256-aligned; Mp, Np = M, N rounded up to the 256 x 256
+//            pair tile (the product writes whole tiles).
+// ---------------------------------------------------------------------------------------------
+struct Layout {
+  int64_t Kp, Mp, Np;
+  size_t off_amax_a, off_amax_b, off_ra, off_rb, off_rc, total;
+};
+
+Layout layout_for(int64_t M, int64_t N, int64_t K, int n) {
+  Layout L;
+  L.Kp = round_up(std::max<int64_t>(K, 1), kBK);
+  L.Mp = round_up(std::max<int64_t>(M, 1), 2 * kBM);
+  L.Np = round_up(std::max<int64_t>(N, 1), kBN);
+  size_t o = 0;
+  L.off_amax_a = o; o += round_up(8 * M, 256);
+  L.off_amax_b = o; o += round_up(8 * N, 256);
+  L.off_ra = o;     o += round_up(static_cast<int64_t>(n) * M * L.Kp, 256);
+  L.off_rb = o;     o += round_up(static_cast<int64_t>(n) * N * L.Kp, 256);
+  L.off_rc = o;     o += static_cast<size_t>(n) * L.Mp * L.Np;
+  L.total = o;
+  return L;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Residues of the scaled operands
+// ---------------------------------------------------------------------------------------------
+// trunc(a 2^(p - e)) from the IEEE fields: |a| = m 2^t, so the result is +-(m 2^(t - e + p)) truncated
+// toward zero, below 2^p <= 2^62 because |a| < 2^e. Zero for a zero, NaN or Inf entry.
+__device__ __forceinline__ long long scaled_int(double a, int e, int p) {
+  const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(a));
+  const unsigned long long mag = bits & 0x7fffffffffffffffull;
+  const int E = static_cast<int>(mag >> 52);
+  if (mag == 0ull || E == 0x7ff) return 0;
+  unsigned long long m = mag & 0x000fffffffffffffull;
+  int t;
+  if (E == 0) {
+    t = -1074;
+  } else {
+    m |= 0x0010000000000000ull;
+    t = E - 1075;
+  }
+  const int sh = t - e + p;
+  const unsigned long long X = sh >= 0 ? (m << sh) : (-sh >= 64 ? 0ull : (m >> (-sh)));
+  return (bits >> 63) ? -static_cast<long long>(X) : static_cast<long long>(X);
+}
+
+// Four values' symmetric residues modulo modulus L as one word of two's-complement bytes, from
+// U = V + 2^62 given as two words per value. Modulus 256 (L = 0): the low byte of V. Otherwise
+// x = sum_d byte_d(U) (2^(8d) mod m) + m - (2^62 mod m) + h is congruent to V + h and below 2^19, so
+// floor(x / m) = umulhi(x, ceil(2^32 / m)) exactly and r = x mod m = (V + h) mod m; the bytes r - h,
+// subtracted four at a time, are the residues in [-h, h].
+template <int L>
+__device__ __forceinline__ uint32_t residue_word(const uint32_t* ulo, const uint32_t* uhi, const Consts& c) {
+  if constexpr (L == 0) {
+    return __byte_perm(__byte_perm(ulo[0], ulo[1], 0x0040), __byte_perm(ulo[2], ulo[3], 0x0040), 0x5410);
+  } else {
+    uint32_t r[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint32_t x = __dp4a(ulo[i], c.coef_lo[L], __dp4a(uhi[i], c.coef_hi[L], c.add[L]));
+      r[i] = x - __umulhi(x, c.split_magic[L]) * static_cast<uint32_t>(c.m[L]);
+    }
+    const uint32_t packed = r[0] | (r[1] << 8) | (r[2] << 16) | (r[3] << 24);
+    return __vsub4(packed, static_cast<uint32_t>(c.h[L]) * 0x01010101u);
+  }
+}
+
+// Residues of 16 consecutive values (one thread's share) as one 16-byte word per modulus.
+template <int NM, int L>
+__device__ __forceinline__ void residues16(const uint32_t (&ulo)[16], const uint32_t (&uhi)[16], const Consts& c,
+                                           uint4 (&out)[NM]) {
+  if constexpr (L < NM) {
+    out[L] = make_uint4(residue_word<L>(ulo, uhi, c), residue_word<L>(ulo + 4, uhi + 4, c),
+                        residue_word<L>(ulo + 8, uhi + 8, c), residue_word<L>(ulo + 12, uhi + 12, c));
+    residues16<NM, L + 1>(ulo, uhi, c, out);
+  }
+}
+
+template <int NM>
+__device__ __forceinline__ void residues_of(const double (&v)[16], int e, int p, const Consts& c, uint4 (&out)[NM]) {
+  uint32_t ulo[16], uhi[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const unsigned long long U =
+        (e == kSentinel) ? (1ull << 62) : static_cast<unsigned long long>(scaled_int(v[i], e, p) + (1ll << 62));
+    ulo[i] = static_cast<uint32_t>(U);
+    uhi[i] = static_cast<uint32_t>(U >> 32);
+  }
+  residues16<NM, 0>(ulo, uhi, c, out);
+}
+
+// Rows of A: a warp covers 512 K positions of one row (16 per lane), a block 8 rows (blockIdx.x:
+// row block, blockIdx.y: K segment). Each modulus plane receives 512 contiguous bytes per warp.
+template <int NM>
+__global__ void __launch_bounds__(256) crt_split_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K,
+                                                             int64_t lda, int64_t Kp,
+                                                             const unsigned long long* __restrict__ amax,
+                                                             int8_t* __restrict__ out, int pa) {
+  const Consts& c = c_table[NM - kMinMod];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t row = static_cast<int64_t>(blockIdx.x) * 8 + warp;
+  const int64_t k0 = static_cast<int64_t>(blockIdx.y) * 512 + lane * 16;
+  if (row >= M || k0 >= Kp) return;
+  const int e = exponent_of_maxbits(amax[row]);
+  const double* a = A + row * lda + k0;
+  double v[16];
+  if (k0 + 16 <= K && (reinterpret_cast<uintptr_t>(a) & 15) == 0) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const double2 x = __ldcs(reinterpret_cast<const double2*>(a) + j);
+      v[2 * j] = x.x;
+      v[2 * j + 1] = x.y;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = (k0 + j < K) ? __ldcs(a + j) : 0.0;
+  }
+  uint4 r[NM];
+  residues_of<NM>(v, e, pa, c, r);
+  int8_t* dst = out + row * Kp + k0;
+#pragma unroll
+  for (int l = 0; l < NM; ++l) *reinterpret_cast<uint4*>(dst + l * M * Kp) = r[l];
+}
+
+// Columns of B, transposed to K-major: a block covers 32 columns (one per lane) and 128 K positions
+// (16 per warp). The loads read 32 consecutive columns of a row of B; the residues pass through
+// shared memory, eight planes at a time, so that each plane's 32 x 128-byte block is written as
+// whole 128-byte rows.
+constexpr int kColPitch = 144;  // bytes per column row in shared memory (128 + 16: no bank conflicts)
+constexpr int kColPlanes = 8;   // planes staged at a time (8 x 4.5 KB)
+template <int NM>
+__global__ void __launch_bounds__(256) crt_split_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N,
+                                                             int64_t ldb, int64_t Kp,
+                                                             const unsigned long long* __restrict__ amax,
+                                                             int8_t* __restrict__ out, int pb) {
+  __shared__ __align__(16) uint8_t stage[kColPlanes][32 * kColPitch];
+  const Consts& c = c_table[NM - kMinMod];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t col0 = static_cast<int64_t>(blockIdx.x) * 32;
+  const int64_t kb = static_cast<int64_t>(blockIdx.y) * kBK;
+  const int64_t col = col0 + lane;
+  const int64_t k0 = kb + warp * 16;
+  const int e = col < N ? exponent_of_maxbits(amax[col]) : 0;
+  double v[16];
+  const double* b = B + k0 * ldb + col;
+  if (col < N && k0 + 16 <= K) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __ldcs(b + j * ldb);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = (col < N && k0 + j < K) ? __ldcs(b + j * ldb) : 0.0;
+  }
+  uint4 r[NM];
+  residues_of<NM>(v, e, pb, c, r);
+  // thread t then writes 16 bytes of column t / 8 (K bytes 16 (t % 8) ..) of each staged plane
+  const int cl = threadIdx.x >> 3, part = threadIdx.x & 7;
+  const bool writes = col0 + cl < N;
+  int8_t* dst = out + (col0 + cl) * Kp + kb + part * 16;
+#pragma unroll
+  for (int l0 = 0; l0 < NM; l0 += kColPlanes) {
+    if (l0 > 0) __syncthreads();  // the previous group's reads are done
+#pragma unroll
+    for (int l = l0; l < l0 + kColPlanes && l < NM; ++l)
+      *reinterpret_cast<uint4*>(&stage[l - l0][lane * kColPitch + warp * 16]) = r[l];
+    __syncthreads();
+    if (writes) {
+#pragma unroll
+      for (int l = l0; l < l0 + kColPlanes && l < NM; ++l)
+        *reinterpret_cast<uint4*>(dst + l * N * Kp) =
+            *reinterpret_cast<const uint4*>(&stage[l - l0][cl * kColPitch + part * 16]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Product kernel: residue planes of C
+// ---------------------------------------------------------------------------------------------
+struct Problem {
+  uint8_t* res;         // residue planes of C: n x Mp x Np bytes
+  int64_t plane, Np;    // plane size and row pitch of the residue planes
+  int tiles_m, tiles_n; // 256-row pair blocks, 256-column blocks
+  int ksteps;           // Kp / 128
+  int kgroups;          // ceil(ksteps / kGroupSteps)
+  int group;            // pair-rows per raster group
+};
+
+__device__ __forceinline__ void tile_coords(const Problem& p, int64_t t, int* m0, int* n0) {
+  const int64_t G = p.group;
+  const int64_t group = t / (G * p.tiles_n), first_m = group * G;
+  const int64_t gsize = (p.tiles_m - first_m) < G ? (p.tiles_m - first_m) : G;
+  const int64_t in_group = t - group * G * p.tiles_n;
+  *m0 = static_cast<int>((first_m + in_group % gsize) * 2 * kBM);
+  *n0 = static_cast<int>((in_group / gsize) * kBN);
+}
+
+// Symmetric residue of an INT32 accumulator modulo c.m[l] (an odd modulus), from
+// y = (acc >> 16)(2^16 mod m) + (acc & 0xffff) + m ceil(2^23 / m), congruent to acc and in [0, 2^25):
+// floor(y / m) = (y ceil(2^39 / m)) >> 39 exactly (the error term is below y m / 2^39 < 1 / m).
+__device__ __forceinline__ int sym_residue_odd(int32_t acc, int m, int c16, int bias, uint32_t magic) {
+  const uint32_t y = static_cast<uint32_t>((acc >> 16) * c16 + (acc & 0xffff) + bias);
+  const int q = static_cast<int>(__umulhi(y, magic) >> 7);
+  const int r = static_cast<int>(y) - q * m;
+  return r > (m >> 1) ? r - m : r;
+}
+
+// 32 accumulators of one row -> their residues modulo c.m[l], stored as bytes c + 128, two 16-byte
+// words. For accumulation group g > 0 the residue of the previous groups (already in `dst`) is added.
+__device__ __forceinline__ void drain_chunk(const uint32_t (&v)[32], int l, bool add_prev, const Consts& c,
+                                            uint4* dst) {
+  uint32_t prev[8] = {};
+  if (add_prev) {
+    const uint4 a = dst[0], b = dst[1];
+    prev[0] = a.x; prev[1] = a.y; prev[2] = a.z; prev[3] = a.w;
+    prev[4] = b.x; prev[5] = b.y; prev[6] = b.z; prev[7] = b.w;
+  }
+  const int m = c.m[l], c16 = c.c16[l], bias = c.bias[l];
+  const uint32_t magic = c.drain_magic[l];
+  uint32_t w[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    uint32_t word = 0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int32_t acc = static_cast<int32_t>(v[4 * q + b]);
+      int r;
+      if (l == 0) {
+        r = static_cast<int8_t>(acc & 0xff);
+        if (add_prev) r = static_cast<int8_t>((r + static_cast<int>((prev[q] >> (8 * b)) & 0xffu) - 128) & 0xff);
+      } else {
+        r = sym_residue_odd(acc, m, c16, bias, magic);
+        if (add_prev) {
+          r += static_cast<int>((prev[q] >> (8 * b)) & 0xffu) - 128;  // |r| <= m - 1
+          r = r > (m >> 1) ? r - m : (r < -(m >> 1) ? r + m : r);
+        }
+      }
+      word |= static_cast<uint32_t>(r + 128) << (8 * b);
+    }
+    w[q] = word;
+  }
+  dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+  dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+template <int NM>
+__global__ void __launch_bounds__(kThreads, 1)
+    crt_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Problem p,
+                    DeviceStatus* status) {
+  const Consts& c = c_table[NM - kMinMod];
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
+  uint64_t* empty = full + kStages;
+  uint64_t* acc_full = empty + kStages;  // [2]
+  uint64_t* acc_empty = acc_full + 2;    // [2]
+  uint64_t* drain = acc_empty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const int64_t tiles = static_cast<int64_t>(p.tiles_m) * p.tiles_n;
+  const int64_t first = cluster_id_x(), stride = num_clusters_x();
+  const int ksteps = p.ksteps, kgroups = p.kgroups;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kStages; ++i) {
+      mbar_init(&full[i], rank == 0 ? 2 : 1);
+      mbar_init(&empty[i], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 2 * kDrainWarps);
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    tma_prefetch_desc(&tmA);
+    tma_prefetch_desc(&tmB);
+  }
+  if (warp == 1) {
+    tmem_alloc_pair(tmem_slot, 2 * kBN);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // both CTAs' barriers exist before any arrival crosses the pair
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------ TMA producer (both CTAs) ------------------------------
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      bool ok = true;
+      for (int64_t t = first; t < tiles && ok; t += stride) {
+        int m0, n0;
+        tile_coords(p, t, &m0, &n0);
+        const int arow = m0 + static_cast<int>(rank) * kBM;
+        const int brow = n0 + static_cast<int>(rank) * (kBN / 2);
+        for (int l = 0; l < NM && ok; ++l) {
+          for (int ks = 0; ks < ksteps; ++ks) {
+            if (!mbar_wait_cluster(&empty[stage], phase ^ 1, abort_flag, status, 81)) { ok = false; break; }
+            uint8_t* st = smem + stage * kStageBytes;
+            mbar_arrive_expect_tx(&full[stage], kStageBytes);
+            tma_load_3d(st, &tmA, &full[stage], ks * kBK, arow, l);
+            tma_load_3d(st + kABytes, &tmB, &full[stage], ks * kBK, brow, l);
+            if (++stage == kStages) { stage = 0; phase ^= 1; }
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1 && rank != 0) {
+    // ------------------------ rank 1: forward each landed stage to rank 0 ------------------------
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      bool ok = true;
+      for (int64_t t = first; t < tiles && ok; t += stride) {
+        for (int l = 0; l < NM && ok; ++l) {
+          for (int ks = 0; ks < ksteps; ++ks) {
+            if (!mbar_wait(&full[stage], phase, abort_flag, status, 82)) { ok = false; break; }
+            mbar_arrive_cluster_relaxed(cluster_addr(&full[stage], 0));
+            if (++stage == kStages) { stage = 0; phase ^= 1; }
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ------------------------------ rank 0: MMA issuer for the pair ------------------------------
+    constexpr uint32_t idesc = idesc_i8_s32(2 * kBM, kBN);
+    const uint64_t a_desc0 = smem_desc_k_sw128(smem_u32(smem));
+    const uint64_t b_desc0 = smem_desc_k_sw128(smem_u32(smem + kABytes));
+    constexpr uint64_t kStageStep = static_cast<uint64_t>(kStageBytes >> 4);
+    constexpr uint64_t kStepK = static_cast<uint64_t>(kMmaK >> 4);  // 32 bytes along the swizzled row
+    int stage = 0;
+    uint32_t phase = 0;
+    uint32_t pass = 0;
+    bool ok = true;
+    for (int64_t t = first; t < tiles && ok; t += stride) {
+      for (int l = 0; l < NM && ok; ++l) {
+        for (int g = 0; g < kgroups && ok; ++g, ++pass) {
+          const uint32_t buf = pass & 1, use = pass >> 1;
+          if (!__all_sync(0xffffffffu, mbar_wait_cluster(&acc_empty[buf], (use & 1) ^ 1, abort_flag, status, 83))) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d_tmem = tmem_base + buf * kBN;
+          const int ks0 = g * kGroupSteps, ks1 = std::min(ksteps, ks0 + kGroupSteps);
+          for (int ks = ks0; ks < ks1; ++ks) {
+            if (!__all_sync(0xffffffffu, mbar_wait_cluster(&full[stage], phase, abort_flag, status, 84))) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            if (elect_one_sync()) {
+              const uint64_t a0 = a_desc0 + static_cast<uint64_t>(stage) * kStageStep;
+              const uint64_t b0 = b_desc0 + static_cast<uint64_t>(stage) * kStageStep;
+#pragma unroll
+              for (int k = 0; k < kBK / kMmaK; ++k)
+                mma_i8_pair(d_tmem, a0 + k * kStepK, b0 + k * kStepK, idesc, (ks > ks0 || k > 0) ? 1u : 0u);
+              mma_commit_pair(cluster_addr(&empty[stage], 0));
+              mma_commit_pair(cluster_addr(&empty[stage], 1));
+            }
+            __syncwarp();
+            if (++stage == kStages) { stage = 0; phase ^= 1; }
+          }
+          if (!ok) break;
+          if (elect_one_sync()) {
+            mma_commit_pair(cluster_addr(&acc_full[buf], 0));
+            mma_commit_pair(cluster_addr(&acc_full[buf], 1));
+          }
+          __syncwarp();
+        }
+      }
+    }
+    if (!ok && elect_one_sync()) {
+      // Let every MMA already issued finish before TMEM is released.
+      mma_commit_pair(cluster_addr(drain, 0));
+      const uint64_t t0 = globaltimer();
+      while (!mbar_try_wait(drain, 0) && globaltimer() - t0 < LT_WAIT_TIMEOUT_NS) {
+      }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------ drain: accumulators -> residue planes of C ------------------------
+    const int quarter = warp & 3;             // TMEM lanes 32*quarter .. +31 (rows of this CTA's block)
+    const int colhalf = (warp - 2) >> 2;      // columns 128*colhalf .. +127 of the tile
+    const uint32_t acc_empty_r0[2] = {cluster_addr(&acc_empty[0], 0), cluster_addr(&acc_empty[1], 0)};
+    uint32_t pass = 0;
+    bool ok = true;
+    for (int64_t t = first; t < tiles && ok; t += stride) {
+      int m0, n0;
+      tile_coords(p, t, &m0, &n0);
+      const int64_t row = static_cast<int64_t>(m0) + static_cast<int64_t>(rank) * kBM + quarter * 32 + lane;
+      uint8_t* row_base = p.res + row * p.Np + n0 + colhalf * (kBN / 2);
+      for (int l = 0; l < NM && ok; ++l) {
+        uint8_t* dst = row_base + static_cast<int64_t>(l) * p.plane;
+        for (int g = 0; g < kgroups; ++g, ++pass) {
+          const uint32_t buf = pass & 1, use = pass >> 1;
+          if (!mbar_wait_cluster(&acc_full[buf], use & 1, abort_flag, status, 86)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t lane_base =
+              tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + buf * kBN + colhalf * (kBN / 2);
+#pragma unroll 1
+          for (int ch = 0; ch < kBN / 64; ++ch) {
+            uint32_t v[32];
+            tmem_ld_32x32b_x32(lane_base + static_cast<uint32_t>(ch * 32), v);
+            tmem_ld_wait();
+            if (ch == kBN / 64 - 1) {
+              // The whole accumulator is in registers: hand the buffer back before the last stores.
+              tc_fence_before();
+              __syncwarp();
+              if (lane == 0) mbar_arrive_cluster(acc_empty_r0[buf]);
+            }
+            drain_chunk(v, l, g > 0, c, reinterpret_cast<uint4*>(dst + ch * 32));
+          }
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();  // rank 0's MMAs read rank 1's shared memory and write its TMEM until here
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc_pair(tmem_base, 2 * kBN);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Reconstruction kernel: residue planes -> C
+// ---------------------------------------------------------------------------------------------
+// C' of one element from its NM residue bytes (c + 128, byte e of each word w[l]) as a double.
+template <int NM, int NL>
+__device__ __forceinline__ double reconstruct(const uint32_t (&w)[NM], int e, const Consts& c) {
+  double L[NL];
+#pragma unroll
+  for (int k = 0; k < NL; ++k) L[k] = c.Kc[k];
+#pragma unroll
+  for (int l = 0; l < NM; ++l) {
+    const uint32_t u = (w[l] >> (8 * e)) & 0xffu;
+    const double ud = __hiloint2double(0x43300000, static_cast<int>(u)) - 4503599627370496.0;  // exact u
+#pragma unroll
+    for (int k = 0; k < NL; ++k) L[k] = __fma_rn(ud, c.P[l][k], L[k]);
+  }
+  const double s = __fma_rn(L[NL - 1], c.f_hi, __dmul_rn(L[NL - 2], c.f_lo));
+  const double Q = rint(s);
+  double t = __fma_rn(-Q, c.Mk[NL - 1], L[NL - 1]);
+  const double base = __longlong_as_double(static_cast<long long>(1023 + c.w) << 52);
+#pragma unroll
+  for (int k = NL - 2; k >= 0; --k) t = __fma_rn(t, base, __fma_rn(-Q, c.Mk[k], L[k]));
+  return t;
+}
+
+// One thread per four consecutive columns of a row: 4-byte loads from each residue plane and
+// 16-byte loads / stores of C, coalesced across the warp (128 columns of a row).
+template <int NM>
+__global__ void __launch_bounds__(256) crt_recon_kernel(const uint8_t* __restrict__ res, int64_t plane, int64_t Np,
+                                                        double* __restrict__ C, int64_t M, int64_t N, int64_t ldc,
+                                                        const unsigned long long* __restrict__ amax_a,
+                                                        const unsigned long long* __restrict__ amax_b, double alpha,
+                                                        double beta, int pa, int pb) {
+  constexpr int NL = limbs_for(NM);
+  const Consts& c = c_table[NM - kMinMod];
+  const int64_t nq = (N + 3) / 4, total = M * nq;
+  for (int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; q < total;
+       q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = q / nq, j0 = (q - i * nq) * 4;
+    uint32_t w[NM];
+    const uint8_t* src = res + i * Np + j0;
+#pragma unroll
+    for (int l = 0; l < NM; ++l) w[l] = __ldcs(reinterpret_cast<const unsigned int*>(src + l * plane));
+    double* crow = C + i * ldc;
+    const bool vec = j0 + 4 <= N && (reinterpret_cast<uintptr_t>(crow + j0) & 15) == 0;
+    double c0[4] = {0.0, 0.0, 0.0, 0.0};
+    if (beta != 0.0) {
+      if (vec) {
+        const double2 x = __ldcs(reinterpret_cast<const double2*>(crow + j0));
+        const double2 y = __ldcs(reinterpret_cast<const double2*>(crow + j0) + 1);
+        c0[0] = x.x; c0[1] = x.y; c0[2] = y.x; c0[3] = y.y;
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (j0 + e < N) c0[e] = crow[j0 + e];
+      }
+    }
+    const int sig = exponent_of_maxbits(amax_a[i]);
+    double out[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int tau = j0 + e < N ? exponent_of_maxbits(amax_b[j0 + e]) : 0;
+      if (sig == kSentinel || tau == kSentinel) {
+        out[e] = __longlong_as_double(0x7ff8000000000000ll);
+      } else {
+        const double tv = scale_pow2(scale_pow2(reconstruct<NM, NL>(w, e, c), sig - pa), tau - pb);
+        out[e] = (beta != 0.0) ? fma(alpha, tv, __dmul_rn(beta, c0[e])) : __dmul_rn(alpha, tv);
+      }
+    }
+    if (vec) {
+      __stcs(reinterpret_cast<double2*>(crow + j0), make_double2(out[0], out[1]));
+      __stcs(reinterpret_cast<double2*>(crow + j0) + 1, make_double2(out[2], out[3]));
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (j0 + e < N) crow[j0 + e] = out[e];
+    }
+  }
+}
+
+// C = beta C0 (alpha * 0 when beta == 0) for K = 0, with the epilogue's roundings.
+__global__ void k0_kernel(double* C, int64_t M, int64_t N, int64_t ldc, double alpha, double beta) {
+  const int64_t n = M * N;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double* c = C + (i / N) * ldc + (i % N);
+    *c = beta != 0.0 ? fma(alpha, 0.0, __dmul_rn(beta, *c)) : __dmul_rn(alpha, 0.0);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host driver
+// ---------------------------------------------------------------------------------------------
+int raster_group() {
+  static const int g = [] {
+    const char* e = getenv("LIBTHOM_CRT_GROUP");
+    const int v = e != nullptr ? atoi(e) : 0;
+    return (v >= 1 && v <= 64) ? v : 8;
+  }();
+  return g;
+}
+
+template <int NM>
+int split_n(const double* A, const double* B, int64_t M, int64_t N, int64_t K, const Layout& L, int pa, int pb,
+            const unsigned long long* amax_a, const unsigned long long* amax_b, int8_t* ra, int8_t* rb,
+            cudaStream_t stream) {
+  const dim3 grid_a(static_cast<unsigned>(ceil_div(M, 8)), static_cast<unsigned>(ceil_div(L.Kp, 512)));
+  crt_split_rows_kernel<NM><<<grid_a, 256, 0, stream>>>(A, M, K, K, L.Kp, amax_a, ra, pa);
+  LT_CUDA_TRY(cudaGetLastError());
+  const dim3 grid_b(static_cast<unsigned>(ceil_div(N, 32)), static_cast<unsigned>(L.Kp / kBK));
+  crt_split_cols_kernel<NM><<<grid_b, 256, 0, stream>>>(B, K, N, N, L.Kp, amax_b, rb, pb);
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
+int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int n, void* workspace,
+          size_t workspace_bytes, cudaStream_t stream) {
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  const Layout L = layout_for(M, N, K, n);
+  if (workspace_bytes < L.total) return set_error(LT_ERR_NO_MEMORY, "CRT workspace too small");
+  uint8_t* ws = static_cast<uint8_t*>(workspace);
+  auto* amax_a = reinterpret_cast<unsigned long long*>(ws + L.off_amax_a);
+  auto* amax_b = reinterpret_cast<unsigned long long*>(ws + L.off_amax_b);
+  LT_CUDA_TRY(cudaMemsetAsync(ws, 0, L.off_ra, stream));
+  if (K == 0) return LT_OK;
+  LT_TRY(ensure_table(ctx->device));
+  LT_TRY(ozaki::exponents(A, B, M, N, K, amax_a, amax_b, ctx->sm_count, stream));
+  const Consts c = make_consts(n, K);
+  auto* ra = reinterpret_cast<int8_t*>(ws + L.off_ra);
+  auto* rb = reinterpret_cast<int8_t*>(ws + L.off_rb);
+  switch (n) {
+#define LT_CRT_SPLIT(NM) \
+  case NM: return split_n<NM>(A, B, M, N, K, L, c.pa, c.pb, amax_a, amax_b, ra, rb, stream);
+    LT_CRT_SPLIT(8) LT_CRT_SPLIT(9) LT_CRT_SPLIT(10) LT_CRT_SPLIT(11) LT_CRT_SPLIT(12) LT_CRT_SPLIT(13)
+    LT_CRT_SPLIT(14) LT_CRT_SPLIT(15) LT_CRT_SPLIT(16) LT_CRT_SPLIT(17) LT_CRT_SPLIT(18) LT_CRT_SPLIT(19)
+    LT_CRT_SPLIT(20)
+#undef LT_CRT_SPLIT
+    default: return set_error(LT_ERR_INVALID_ARGUMENT, "modulus count %d outside [%d, %d]", n, kMinMod, kMaxMod);
+  }
+}
+
+template <int NM>
+int launch_product_n(const CUtensorMap& tmA, const CUtensorMap& tmB, const Problem& p, const Consts& c, double* C,
+                     int64_t M, int64_t N, const unsigned long long* amax_a, const unsigned long long* amax_b,
+                     double alpha, double beta, DeviceContext* ctx, cudaStream_t stream) {
+  if (c.nl != limbs_for(NM)) return set_error(LT_ERR_UNSUPPORTED, "CRT limb count %d, kernel built for %d", c.nl, limbs_for(NM));
+  static std::once_flag once[64];
+  static cudaError_t attr_err[64];
+  static int max_clusters[64];
+  auto config = [&](cudaLaunchConfig_t* cfg, cudaLaunchAttribute* attr, unsigned grid) {
+    *cfg = cudaLaunchConfig_t{};
+    cfg->gridDim = dim3(grid);
+    cfg->blockDim = dim3(kThreads);
+    cfg->dynamicSmemBytes = kSmem;
+    cfg->stream = stream;
+    attr->id = cudaLaunchAttributeClusterDimension;
+    attr->val.clusterDim.x = 2;
+    attr->val.clusterDim.y = 1;
+    attr->val.clusterDim.z = 1;
+    cfg->attrs = attr;
+    cfg->numAttrs = 1;
+  };
+  std::call_once(once[ctx->device], [&] {
+    attr_err[ctx->device] = cudaFuncSetAttribute(crt_pair_kernel<NM>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
+    if (attr_err[ctx->device] != cudaSuccess) return;
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute attr;
+    config(&cfg, &attr, static_cast<unsigned>(ctx->sm_count & ~1));
+    attr_err[ctx->device] = cudaOccupancyMaxActiveClusters(&max_clusters[ctx->device], crt_pair_kernel<NM>, &cfg);
+  });
+  LT_CUDA_TRY(attr_err[ctx->device]);
+  const int64_t tiles = static_cast<int64_t>(p.tiles_m) * p.tiles_n;
+  const int64_t clusters = std::min<int64_t>(std::min<int64_t>(tiles, max_clusters[ctx->device]), ctx->sm_count / 2);
+  if (clusters <= 0) return set_error(LT_ERR_UNSUPPORTED, "no pair of CTAs of the CRT product kernel fits");
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute attr;
+  config(&cfg, &attr, static_cast<unsigned>(2 * clusters));
+  LT_CUDA_TRY(cudaLaunchKernelEx(&cfg, crt_pair_kernel<NM>, tmA, tmB, p, ctx->status));
+  const int64_t work = M * ((N + 3) / 4);
+  const int64_t blocks = std::min<int64_t>(ceil_div(work, 256), 8 * ctx->sm_count);
+  crt_recon_kernel<NM><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p.res, p.plane, p.Np, C, M, N, N, amax_a,
+                                                                           amax_b, alpha, beta, c.pa, c.pb);
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
+int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int n, const void* workspace,
+            size_t workspace_bytes, cudaStream_t stream) {
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  const Layout L = layout_for(M, N, K, n);
+  if (workspace_bytes < L.total) return set_error(LT_ERR_NO_MEMORY, "CRT workspace too small");
+  if (K == 0) {
+    const int64_t total = M * N;
+    const int64_t blocks = std::min<int64_t>(ceil_div(total, 256), 4 * ctx->sm_count);
+    k0_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(C, M, N, N, alpha, beta);
+    LT_CUDA_TRY(cudaGetLastError());
+    return LT_OK;
+  }
+  LT_TRY(ensure_table(ctx->device));
+  const uint8_t* ws = static_cast<const uint8_t*>(workspace);
+  CUtensorMap tmA, tmB;
+  LT_TRY(make_tmap_3d(&tmA, ws + L.off_ra, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, n, M, L.Kp, L.Kp, M * L.Kp, kBM, kBK,
+                      CU_TENSOR_MAP_SWIZZLE_128B));
+  LT_TRY(make_tmap_3d(&tmB, ws + L.off_rb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, n, N, L.Kp, L.Kp, N * L.Kp, kBN / 2, kBK,
+                      CU_TENSOR_MAP_SWIZZLE_128B));
+  Problem p;
+  p.res = const_cast<uint8_t*>(ws + L.off_rc);
+  p.plane = L.Mp * L.Np;
+  p.Np = L.Np;
+  p.tiles_m = static_cast<int>(L.Mp / (2 * kBM));
+  p.tiles_n = static_cast<int>(L.Np / kBN);
+  p.ksteps = static_cast<int>(L.Kp / kBK);
+  p.kgroups = static_cast<int>(ceil_div(p.ksteps, kGroupSteps));
+  p.group = raster_group();
+  const Consts c = make_consts(n, K);
+  const auto* amax_a = reinterpret_cast<const unsigned long long*>(ws + L.off_amax_a);
+  const auto* amax_b = reinterpret_cast<const unsigned long long*>(ws + L.off_amax_b);
+  switch (n) {
+#define LT_CRT_PRODUCT(NM) \
+  case NM: return launch_product_n<NM>(tmA, tmB, p, c, C, M, N, amax_a, amax_b, alpha, beta, ctx, stream);
+    LT_CRT_PRODUCT(8) LT_CRT_PRODUCT(9) LT_CRT_PRODUCT(10) LT_CRT_PRODUCT(11) LT_CRT_PRODUCT(12) LT_CRT_PRODUCT(13)
+    LT_CRT_PRODUCT(14) LT_CRT_PRODUCT(15) LT_CRT_PRODUCT(16) LT_CRT_PRODUCT(17) LT_CRT_PRODUCT(18)
+    LT_CRT_PRODUCT(19) LT_CRT_PRODUCT(20)
+#undef LT_CRT_PRODUCT
+    default: return set_error(LT_ERR_INVALID_ARGUMENT, "modulus count %d outside [%d, %d]", n, kMinMod, kMaxMod);
+  }
+}
+
+size_t workspace_size(int64_t M, int64_t N, int64_t K, int n) { return layout_for(M, N, K, n).total; }
+
+}  // namespace crt
+}  // namespace lt
+
+// ---------------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+int check_args(const double* A, const double* B, const double* C, int64_t M, int64_t N, int64_t K, int n) {
+  if (M < 0 || N < 0 || K < 0 || M > 0x7fffffff || N > 0x7fffffff || K > 0x7fffffff)
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "bad dimensions");
+  if ((M > 0 && K > 0 && A == nullptr) || (K > 0 && N > 0 && B == nullptr) || (M > 0 && N > 0 && C == nullptr))
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "null matrix pointer");
+  if (((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(C)) & 7) != 0)
+    return lt::set_error(LT_ERR_UNALIGNED, "matrix pointers must be 8-byte aligned");
+  if (n < LT_OZAKI_CRT_MIN_MODULI || n > LT_OZAKI_CRT_MAX_MODULI)
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "modulus count %d outside [%d, %d]", n, LT_OZAKI_CRT_MIN_MODULI,
+                         LT_OZAKI_CRT_MAX_MODULI);
+  if (K > 65535ll * lt::crt::kBK)  // the residue split's grid covers K in 128-wide blocks (gridDim.y)
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "K = %lld above the CRT form's limit %lld", static_cast<long long>(K),
+                         65535ll * lt::crt::kBK);
+  return LT_OK;
+}
+
+int check_ws(int64_t M, int64_t N, int64_t K, int n, const void* workspace, size_t workspace_bytes) {
+  const size_t need = lt::crt::workspace_size(M, N, K, n);
+  if (workspace == nullptr || workspace_bytes < need)
+    return lt::set_error(LT_ERR_NO_MEMORY, "workspace of %zu bytes given, %zu needed", workspace_bytes, need);
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
+    return lt::set_error(LT_ERR_UNALIGNED, "workspace must be 256-byte aligned");
+  return LT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t lt_ozaki_crt_workspace_size(int64_t M, int64_t N, int64_t K, int moduli) {
+  if (M < 0 || N < 0 || K < 0 || moduli < LT_OZAKI_CRT_MIN_MODULI || moduli > LT_OZAKI_CRT_MAX_MODULI) return 0;
+  return lt::crt::workspace_size(M, N, K, moduli);
+}
+
+int lt_ozaki_crt_info(int moduli, int64_t K, int* pa, int* pb, int* moduli_out) {
+  if (moduli < LT_OZAKI_CRT_MIN_MODULI || moduli > LT_OZAKI_CRT_MAX_MODULI || K < 0)
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "modulus count %d outside [%d, %d]", moduli,
+                         LT_OZAKI_CRT_MIN_MODULI, LT_OZAKI_CRT_MAX_MODULI);
+  const lt::crt::Consts c = lt::crt::make_consts(moduli, K);
+  if (pa != nullptr) *pa = c.pa;
+  if (pb != nullptr) *pb = c.pb;
+  if (moduli_out != nullptr)
+    for (int l = 0; l < moduli; ++l) moduli_out[l] = c.m[l];
+  return lt::ok();
+}
+
+int lt_ozaki_crt_split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int moduli, void* workspace,
+                       size_t workspace_bytes, void* stream) {
+  LT_TRY(check_args(A, B, reinterpret_cast<const double*>(8), M, N, K, moduli));
+  LT_TRY(check_ws(M, N, K, moduli, workspace, workspace_bytes));
+  if (M == 0 || N == 0) return lt::ok();
+  LT_TRY(lt::crt::split(A, B, M, N, K, moduli, workspace, workspace_bytes, lt::as_stream(stream)));
+  return lt::ok();
+}
+
+int lt_ozaki_crt_product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int moduli,
+                         const void* workspace, size_t workspace_bytes, void* stream) {
+  LT_TRY(check_args(reinterpret_cast<const double*>(8), reinterpret_cast<const double*>(8), C, M, N, K, moduli));
+  LT_TRY(check_ws(M, N, K, moduli, workspace, workspace_bytes));
+  if (M == 0 || N == 0) return lt::ok();
+  LT_TRY(lt::crt::product(C, M, N, K, alpha, beta, moduli, workspace, workspace_bytes, lt::as_stream(stream)));
+  return lt::ok();
+}
+
+int lt_dgemm_ozaki_crt_ws(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
+                          double beta, int moduli, void* workspace, size_t workspace_bytes, void* stream) {
+  LT_TRY(check_args(A, B, C, M, N, K, moduli));
+  LT_TRY(check_ws(M, N, K, moduli, workspace, workspace_bytes));
+  if (M == 0 || N == 0) return lt::ok();
+  const cudaStream_t s = lt::as_stream(stream);
+  LT_TRY(lt::crt::split(A, B, M, N, K, moduli, workspace, workspace_bytes, s));
+  LT_TRY(lt::crt::product(C, M, N, K, alpha, beta, moduli, workspace, workspace_bytes, s));
+  return lt::ok();
+}
+
+int lt_dgemm_ozaki_crt(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
+                       double beta, int moduli, void* stream) {
+  LT_TRY(check_args(A, B, C, M, N, K, moduli));
+  if (M == 0 || N == 0) return lt::ok();
+  lt::DeviceContext* ctx = lt::context();
+  if (ctx == nullptr) return lt::last_error();
+  const size_t bytes = lt::crt::workspace_size(M, N, K, moduli);
+  void* ws = nullptr;
+  LT_TRY(lt::ensure_workspace(ctx, bytes, &ws));
+  const cudaStream_t s = lt::as_stream(stream);
+  LT_TRY(lt::crt::split(A, B, M, N, K, moduli, ws, bytes, s));
+  LT_TRY(lt::crt::product(C, M, N, K, alpha, beta, moduli, ws, bytes, s));
+  return lt::ok();
+}
+
+}  // extern "C"

@@ -34,6 +34,8 @@ static const std::map<std::string, DgemmImpl> dgemmImpls = {
     {"ozaki5", dgemm_ozaki5},       {"ozaki6", dgemm_ozaki6},   {"ozaki7", dgemm_ozaki7},
     {"ozaki8", dgemm_ozaki8},       {"ozaki9", dgemm_ozaki9},   {"ozaki10", dgemm_ozaki10},
     {"ozaki_auto", dgemm_ozaki_auto}, {"auto", dgemm_auto},     {"cublas_tc", dgemm_cublas_tc},
+    {"ozaki_crt14", dgemm_ozaki_crt14}, {"ozaki_crt15", dgemm_ozaki_crt15}, {"ozaki_crt16", dgemm_ozaki_crt16},
+    {"ozaki_crt17", dgemm_ozaki_crt17}, {"ozaki_crt18", dgemm_ozaki_crt18},
 };
 
 struct Buffers {

@@ -77,6 +77,10 @@ def lib() -> ctypes.CDLL:
         L.oracle_ozaki_split_rows.argtypes = [_vp, _i64, _i64, _vp, _i32, _vp, _i64]
         L.oracle_ozaki_split_cols.argtypes = [_vp, _i64, _i64, _vp, _i32, _vp, _i64]
         L.oracle_ozaki_dgemm.argtypes = [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _i32, _i32]
+        L.oracle_crt_split_rows.argtypes = [_vp, _i64, _i64, _vp, _i32, _i32, _vp, _vp, _i64]
+        L.oracle_crt_split_cols.argtypes = [_vp, _i64, _i64, _vp, _i32, _i32, _vp, _vp, _i64]
+        L.oracle_crt_dgemm.argtypes = [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _i32, _i32, _i32, _i32, _i32,
+                                       _vp, _vp, _vp, _f64, _f64, _i32]
         L.oracle_ozaki_analytic_slices.restype = _i32
         L.oracle_ozaki_analytic_slices.argtypes = [_f64, _i32]
         L.oracle_max_gap.restype = _i32
@@ -306,6 +310,74 @@ def ozaki_split(A, B, s):
     L.oracle_ozaki_split_rows(_p(A), M, K, _p(sigma), s, _p(sa), Kp)
     L.oracle_ozaki_split_cols(_p(B), K, N, _p(tau), s, _p(sb), Kp)
     return sigma, tau, sa, sb
+
+
+# ---- Ozaki scheme II (CRT form) restatement -----------------------------------------------------
+# Pairwise-coprime moduli no larger than 256 (so every symmetric residue is one signed byte), largest
+# first; a CRT-form DGEMM with n moduli uses the first n.
+CRT_MODULI = (256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197, 193, 191, 181, 179, 173)
+CRT_MIN, CRT_MAX = 8, 20
+
+
+def crt_constants(n: int, K: int) -> dict:
+    """Constants of the CRT form with n moduli for inner dimension K, by exact integer arithmetic:
+    Mprod, the limb width w and count nl, the limbs P[l][k] of the CRT basis
+    P_l = (Mprod/m_l) * ((Mprod/m_l)^-1 mod m_l), the limbs of Mprod, f_hi / f_lo = 2^(w k) / Mprod_d
+    (Mprod_d = the limbs summed by Horner in double), and the operand bits pa, pb with
+    K 2^(pa+pb) <= Mprod / 4 (each at most 62)."""
+    assert CRT_MIN <= n <= CRT_MAX
+    mods = CRT_MODULI[:n]
+    Mp = 1
+    for m in mods:
+        Mp *= m
+    w = 42 if n <= 16 else 41
+    nl = -(-Mp.bit_length() // w)
+    mask = (1 << w) - 1
+    P = []
+    for m in mods:
+        Ml = Mp // m
+        P.append(Ml * pow(Ml % m, -1, m))
+    Pl = np.array([[float((p >> (w * k)) & mask) for k in range(nl)] for p in P], dtype=np.float64)
+    Mk = np.array([float((Mp >> (w * k)) & mask) for k in range(nl)], dtype=np.float64)
+    md = float(Mk[nl - 1])
+    for k in range(nl - 2, -1, -1):
+        md = md * 2.0 ** w + float(Mk[k])  # exact scaling, one rounding per step (= fma(md, 2^w, M_k))
+    T = (Mp // (2 * max(K, 1))).bit_length() - 2
+    pa, pb = min(62, T // 2), min(62, T - T // 2)
+    return {"n": n, "mods": np.array(mods, dtype=np.int32), "Mprod": Mp, "w": w, "nl": nl, "P": Pl, "Mk": Mk,
+            "f_hi": 2.0 ** (w * (nl - 1)) / md, "f_lo": 2.0 ** (w * (nl - 2)) / md, "pa": pa, "pb": pb}
+
+
+def crt_dgemm(A, B, C0, alpha, beta, n, threads: int | None = None) -> np.ndarray:
+    """The CRT form restated (oracle_crt_dgemm) with n moduli."""
+    M, K = A.shape
+    N = B.shape[1]
+    c = crt_constants(n, K)
+    C = np.ascontiguousarray(C0).copy()
+    P = np.ascontiguousarray(c["P"])
+    lib().oracle_crt_dgemm(_p(np.ascontiguousarray(A)), _p(np.ascontiguousarray(B)), _p(C), M, N, K, alpha, beta, n,
+                           c["nl"], c["w"], c["pa"], c["pb"], _p(c["mods"]), _p(P), _p(c["Mk"]), c["f_hi"], c["f_lo"],
+                           threads or nthreads())
+    return C
+
+
+def crt_split(A, B, n):
+    """(sigma, tau, residues of A [n][M][K], residues of B transposed [n][N][K]) of the CRT form."""
+    M, K = A.shape
+    N = B.shape[1]
+    c = crt_constants(n, K)
+    Kp = max(K, 1)
+    sigma = np.empty(M, dtype=np.int32)
+    tau = np.empty(N, dtype=np.int32)
+    ra = np.empty((n, M, Kp), dtype=np.int8)
+    rb = np.empty((n, N, Kp), dtype=np.int8)
+    L = lib()
+    A, B = np.ascontiguousarray(A), np.ascontiguousarray(B)
+    L.oracle_ozaki_row_exponents(_p(A), M, K, _p(sigma))
+    L.oracle_ozaki_col_exponents(_p(B), K, N, _p(tau))
+    L.oracle_crt_split_rows(_p(A), M, K, _p(sigma), c["pa"], n, _p(c["mods"]), _p(ra), Kp)
+    L.oracle_crt_split_cols(_p(B), K, N, _p(tau), c["pb"], n, _p(c["mods"]), _p(rb), Kp)
+    return sigma, tau, ra, rb
 
 
 def analytic_slices(tol: float, gap_bits: int) -> int:

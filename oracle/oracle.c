@@ -646,3 +646,170 @@ void oracle_hgemm_exact_rows(const uint16_t* A, const uint16_t* B, const uint16_
     }
   }
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* Ozaki scheme II restated (integer residues and the Chinese remainder theorem), the arithmetic  */
+/* of the library's CRT form (no reference counterpart; the reference's DGEMM contract is        */
+/* routines/dgemm/dgemm.h:9, its host check routines/dgemm/dgemm.cpp:122-133):                    */
+/*  1. sigma_i, tau_j: frexp exponents of the row / column maxima (as in the slice form).        */
+/*  2. V = trunc(A[i,k] 2^(pa - sigma_i)), W = trunc(B[k,j] 2^(pb - tau_j)): integers below 2^pa  */
+/*     and 2^pb in magnitude, with K 2^(pa+pb) <= Mprod / 4 (Mprod = product of the moduli).       */
+/*  3. For each modulus m_l: symmetric residues of V and W, their exact integer product over K,  */
+/*     reduced to the symmetric residue c_l of sum_k V W modulo m_l.                              */
+/*  4. C' = the integer in (-Mprod/2, Mprod/2) with C' = c_l mod m_l, through FP64 limb sums:      */
+/*     L_k = sum_l c_l P_lk (exact), Q = rint(L_hi F_hi + L_lo F_lo), D_k = fma(-Q, M_k, L_k),     */
+/*     t = Horner of the D_k in base 2^w. The constants (moduli, limbs P_lk of the CRT basis,     */
+/*     limbs M_k of Mprod, F = 2^(w k) / Mprod) come from the caller (oracle/__init__.py derives  */
+/*     them with exact integer arithmetic).                                                        */
+/*  5. C = fma(alpha, t 2^(sigma_i - pa) 2^(tau_j - pb), beta*C0)  (alpha * that when beta == 0); */
+/*     NaN where the row of A or the column of B holds NaN or Inf.                                */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct {
+  int n, nl, w, pa, pb;
+  const int32_t* mods;   /* n moduli */
+  const double* P;       /* n x nl limbs of the CRT basis P_l = (Mprod/m_l) ((Mprod/m_l)^-1 mod m_l) */
+  const double* Mk;      /* nl limbs of Mprod */
+  double f_hi, f_lo;     /* 2^(w (nl-1)) / Mprod_d and 2^(w (nl-2)) / Mprod_d */
+} crt_consts_t;
+
+/* trunc(a 2^(p - e)) from the IEEE fields; |result| < 2^p (p <= 62); zero for zero / NaN / Inf */
+static int64_t crt_scaled_int(double a, int32_t e, int p) {
+  uint64_t bits;
+  memcpy(&bits, &a, sizeof bits);
+  const uint64_t mag = bits & 0x7fffffffffffffffull;
+  const int E = (int)(mag >> 52);
+  if (mag == 0 || E == 0x7ff) return 0;
+  uint64_t m = mag & 0x000fffffffffffffull;
+  int t;
+  if (E == 0) {
+    t = -1074;
+  } else {
+    m |= 0x0010000000000000ull;
+    t = E - 1075;
+  }
+  const int sh = t - e + p;
+  uint64_t X;
+  if (sh >= 0) X = m << sh;
+  else X = (-sh >= 64) ? 0 : (m >> (-sh));
+  return (bits >> 63) ? -(int64_t)X : (int64_t)X;
+}
+
+/* symmetric residue: [-(m-1)/2, (m-1)/2] for odd m, [-128, 127] for m = 256 */
+static int32_t crt_residue(int64_t v, int32_t m) {
+  int64_t r = v % m;
+  if (r < 0) r += m;
+  if (m == 256) return r >= 128 ? (int32_t)(r - 256) : (int32_t)r;
+  return r > m / 2 ? (int32_t)(r - m) : (int32_t)r;
+}
+
+/* residues of the scaled rows of A: out[l][i][k] (Kp >= K, zero padded) */
+void oracle_crt_split_rows(const double* A, int64_t M, int64_t K, const int32_t* sigma, int p, int n,
+                           const int32_t* mods, int8_t* out, int64_t Kp) {
+  memset(out, 0, (size_t)(n * M * Kp));
+  for (int64_t i = 0; i < M; ++i) {
+    int bad = 0;
+    for (int64_t k = 0; k < K; ++k) if (!isfinite(A[i * K + k])) { bad = 1; break; }
+    if (bad) continue;
+    for (int64_t k = 0; k < K; ++k) {
+      const int64_t v = crt_scaled_int(A[i * K + k], sigma[i], p);
+      for (int l = 0; l < n; ++l) out[((int64_t)l * M + i) * Kp + k] = (int8_t)crt_residue(v, mods[l]);
+    }
+  }
+}
+
+/* residues of the scaled columns of B, transposed: out[l][j][k] */
+void oracle_crt_split_cols(const double* B, int64_t K, int64_t N, const int32_t* tau, int p, int n,
+                           const int32_t* mods, int8_t* out, int64_t Kp) {
+  memset(out, 0, (size_t)(n * N * Kp));
+  for (int64_t j = 0; j < N; ++j) {
+    int bad = 0;
+    for (int64_t k = 0; k < K; ++k) if (!isfinite(B[k * N + j])) { bad = 1; break; }
+    if (bad) continue;
+    for (int64_t k = 0; k < K; ++k) {
+      const int64_t v = crt_scaled_int(B[k * N + j], tau[j], p);
+      for (int l = 0; l < n; ++l) out[((int64_t)l * N + j) * Kp + k] = (int8_t)crt_residue(v, mods[l]);
+    }
+  }
+}
+
+/* C' (as a double) from the residues c[0..n-1] */
+double oracle_crt_reconstruct(const int32_t* c, const crt_consts_t* cc) {
+  double L[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int l = 0; l < cc->n; ++l)
+    for (int k = 0; k < cc->nl; ++k) L[k] = fma((double)c[l], cc->P[l * cc->nl + k], L[k]);
+  const int nl = cc->nl;
+  const double s = fma(L[nl - 1], cc->f_hi, L[nl - 2] * cc->f_lo);
+  const double Q = rint(s);
+  double D[8];
+  for (int k = 0; k < nl; ++k) D[k] = fma(-Q, cc->Mk[k], L[k]);
+  const double base = ldexp(1.0, cc->w);
+  double t = D[nl - 1];
+  for (int k = nl - 2; k >= 0; --k) t = fma(t, base, D[k]);
+  return t;
+}
+
+typedef struct {
+  const int8_t *ra, *rb;
+  const int32_t *sigma, *tau;
+  const double *A, *B;
+  double* C;
+  int64_t M, N, K, Kp;
+  double alpha, beta;
+  const crt_consts_t* cc;
+  int tid, nthreads;
+} crt_job_t;
+
+static void* crt_worker(void* arg) {
+  crt_job_t* j = (crt_job_t*)arg;
+  const crt_consts_t* cc = j->cc;
+  const int64_t M = j->M, N = j->N, K = j->K, Kp = j->Kp;
+  int32_t c[32];
+  for (int64_t i = j->tid; i < M; i += j->nthreads) {
+    int row_bad = 0;
+    for (int64_t k = 0; k < K; ++k) if (!isfinite(j->A[i * K + k])) { row_bad = 1; break; }
+    for (int64_t col = 0; col < N; ++col) {
+      int bad = row_bad;
+      if (!bad) for (int64_t k = 0; k < K; ++k) if (!isfinite(j->B[k * N + col])) { bad = 1; break; }
+      for (int l = 0; l < cc->n; ++l) {
+        const int8_t* a = j->ra + ((int64_t)l * M + i) * Kp;
+        const int8_t* b = j->rb + ((int64_t)l * N + col) * Kp;
+        int64_t acc = 0;
+        for (int64_t k = 0; k < K; ++k) acc += (int64_t)a[k] * (int64_t)b[k];
+        c[l] = crt_residue(acc, cc->mods[l]);
+      }
+      const double t = scale_pow2(scale_pow2(oracle_crt_reconstruct(c, cc), j->sigma[i] - cc->pa), j->tau[col] - cc->pb);
+      double out;
+      if (j->beta != 0.0) out = fma(j->alpha, t, j->beta * j->C[i * N + col]);
+      else out = j->alpha * t;
+      if (bad) out = NAN;
+      j->C[i * N + col] = out;
+    }
+  }
+  return NULL;
+}
+
+void oracle_crt_dgemm(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
+                      double beta, int n, int nl, int w, int pa, int pb, const int32_t* mods, const double* P,
+                      const double* Mk, double f_hi, double f_lo, int nthreads) {
+  crt_consts_t cc = {n, nl, w, pa, pb, mods, P, Mk, f_hi, f_lo};
+  const int64_t Kp = K > 0 ? K : 1;
+  int32_t* sigma = (int32_t*)malloc(sizeof(int32_t) * (size_t)(M > 0 ? M : 1));
+  int32_t* tau = (int32_t*)malloc(sizeof(int32_t) * (size_t)(N > 0 ? N : 1));
+  int8_t* ra = (int8_t*)malloc((size_t)(n * M * Kp + 1));
+  int8_t* rb = (int8_t*)malloc((size_t)(n * N * Kp + 1));
+  oracle_ozaki_row_exponents(A, M, K, sigma);
+  oracle_ozaki_col_exponents(B, K, N, tau);
+  oracle_crt_split_rows(A, M, K, sigma, pa, n, mods, ra, Kp);
+  oracle_crt_split_cols(B, K, N, tau, pb, n, mods, rb, Kp);
+  if (nthreads < 1) nthreads = 1;
+  if (nthreads > 256) nthreads = 256;
+  pthread_t th[256];
+  crt_job_t jobs[256];
+  for (int t = 0; t < nthreads; ++t) {
+    crt_job_t jb = {ra, rb, sigma, tau, A, B, C, M, N, K, Kp, alpha, beta, &cc, t, nthreads};
+    jobs[t] = jb;
+    pthread_create(&th[t], NULL, crt_worker, &jobs[t]);
+  }
+  for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+  free(sigma); free(tau); free(ra); free(rb);
+}

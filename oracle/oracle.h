@@ -95,6 +95,18 @@ void oracle_ozaki_dgemm(const double* A, const double* B, double* C, int64_t M, 
 int oracle_ozaki_analytic_slices(double tol, int gap_bits);
 int oracle_max_gap(const double* X, int64_t rows, int64_t cols, int by_rows);
 
+/* ---- Ozaki scheme II (CRT form) restatement ---- */
+/* residues out[(l*M + i)*Kp + k] of trunc(A[i,k] 2^(p - sigma_i)) modulo mods[l] (symmetric) */
+void oracle_crt_split_rows(const double* A, int64_t M, int64_t K, const int32_t* sigma, int p, int n,
+                           const int32_t* mods, int8_t* out, int64_t Kp);
+/* the same for the columns of B, transposed: out[(l*N + j)*Kp + k] */
+void oracle_crt_split_cols(const double* B, int64_t K, int64_t N, const int32_t* tau, int p, int n,
+                           const int32_t* mods, int8_t* out, int64_t Kp);
+/* Full CRT-form DGEMM with the caller's constants (n moduli, nl limbs of w bits, pa / pb bits). */
+void oracle_crt_dgemm(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
+                      double beta, int n, int nl, int w, int pa, int pb, const int32_t* mods, const double* P,
+                      const double* Mk, double f_hi, double f_lo, int nthreads);
+
 /* ---- learned slice selector restatements ---- */
 void oracle_features(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, float* feat);
 void oracle_mlp_forward(const float* params, const float* x, int batch, float* probs);

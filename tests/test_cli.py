@@ -11,7 +11,8 @@ import pytest
 ROOT = Path(__file__).resolve().parents[1]
 CLI = ROOT / "build" / "libthom"
 
-DGEMM_IMPLS = {"tc100", "cublas_tc", "auto", "ozaki_auto"} | {f"ozaki{s}" for s in range(3, 11)}
+DGEMM_IMPLS = ({"tc100", "cublas_tc", "auto", "ozaki_auto"} | {f"ozaki{s}" for s in range(3, 11)}
+               | {f"ozaki_crt{n}" for n in range(14, 19)})
 HGEMM_IMPLS = {"tc100", "cublas"}
 
 
