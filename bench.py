@@ -5,12 +5,14 @@ Workload (the reference's dgemm contract, routines/dgemm/dgemm.h:9): row-major C
 M = N = K = 8192, alpha = 1.5, beta = 0.5, entries u*2^e with u ~ U[-1,1) and e ~ U{-phi..phi}
 (phi = 0 by default), C0 from the same law; seeded synthetic data generated on the device.
 
-One step = one full DGEMM through the Ozaki INT8 path (exponent + split passes, tcgen05 INT8 slice
-products, fused FP64 recombination). The slice count is the smallest one whose measured
-componentwise error |C - C_exact| / (|alpha||A||B| + |beta||C0|) on sampled rows is no worse than the
-native FP64 path's on the same rows (C_exact from the library's compensated Dot2 reference of
-those rows, computed on the device); that selection runs
-before the timed region. The native FP64 tensor-core kernel and cuBLAS DGEMM are timed alongside.
+One step = one full DGEMM through the Ozaki-II CRT form (exponent and residue passes, tcgen05 INT8
+products of the residues, FP64 reconstruction with the alpha/beta epilogue). The modulus count is the
+smallest whose measured componentwise error |C - C_exact| / (|alpha||A||B| + |beta||C0|) on sampled
+rows is no worse than the native FP64 path's on the same rows (C_exact from the library's compensated
+Dot2 reference of those rows, computed on the device); that selection runs before the timed region.
+The native FP64 tensor-core kernel, cuBLAS DGEMM and the Ozaki slice form are timed alongside, and
+the other BASELINE configurations (exponent spreads 8 and 32, the tall and long-K shapes with scaled
+rows and columns, the 512-problem grouped set) are reported as extra keys of the same line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -21,6 +23,8 @@ from __future__ import annotations
 import argparse
 import json
 import os
+
+import numpy as np
 import statistics
 import sys
 import time
@@ -133,6 +137,9 @@ class ClockSampler:
             self.stop = threading.Event()
             self.thread = threading.Thread(target=self._loop, daemon=True)
             self.thread.start()
+            t0 = time.perf_counter()
+            while not self.rows and time.perf_counter() - t0 < 2.0:  # the first sample precedes the work
+                time.sleep(0.001)
         except Exception as e:  # no NVML on this machine
             self.error = f"NVML unavailable: {e}"
         return self
@@ -290,8 +297,137 @@ def pairs(s: int) -> int:
     return s * (s + 1) // 2
 
 
+def event_loop(torch, stream, fn, steps: int, warmup: int) -> float:
+    """Mean milliseconds per call of fn over `steps` calls after `warmup`, CUDA events on `stream`."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        fn()
+    b.record(stream)
+    b.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def fill_problem(lt, torch, dev, stream, M, N, K, phi, smax):
+    A = torch.empty(M, K, dtype=torch.float64, device=dev)
+    B = torch.empty(K, N, dtype=torch.float64, device=dev)
+    C0 = torch.empty(M, N, dtype=torch.float64, device=dev)
+    lt.fill(A, M * K, SEED, 1, phi, stream)
+    lt.fill(B, K * N, SEED, 2, phi, stream)
+    lt.fill(C0, M * N, SEED, 3, phi, stream)
+    if smax > 0:
+        lt.scale_rows(A, M, K, SEED, 4, smax, stream)
+        lt.scale_cols(B, K, N, SEED, 5, smax, stream)
+    torch.cuda.synchronize()
+    return A, B, C0
+
+
+def matched_moduli(lt, torch, stream, A, B, C0, C, M, N, K, alpha, beta, ws, err_of, target, first=13):
+    """Smallest modulus count (first .. 20) whose CRT-form error on the sampled rows is no worse than
+    `target`; returns (n, {n: error})."""
+    errs = {}
+    for n in range(first, lt.LT_OZAKI_CRT_MAX_MODULI + 1):
+        C.copy_(C0)
+        lt.dgemm_ozaki_crt(A, B, C, M, N, K, alpha, beta, n, stream, workspace=ws)
+        torch.cuda.synchronize()
+        errs[n] = err_of(C)
+        if errs[n] <= target:
+            return n, errs
+    return max(errs), errs
+
+
+def config_point(lt, torch, dev, stream, M, N, K, alpha, beta, phi, smax, steps, nrows=8) -> dict:
+    """One BASELINE configuration: native FP64, cuBLAS and the accuracy-matched CRT form, each with its
+    TFLOP/s and max componentwise error on `nrows` sampled rows against the compensated reference."""
+    A, B, C0 = fill_problem(lt, torch, dev, stream, M, N, K, phi, smax)
+    C = torch.empty_like(C0)
+    rows_d = torch.from_numpy(np.linspace(0, M - 1, nrows).astype(np.int64)).to(dev)
+    Cref, den = dot2_reference(lt, torch, A, B, C0, M, N, K, alpha, beta, rows_d, stream)
+
+    def err_of(Cdev):
+        return max_error(lt, Cdev[rows_d], Cref, den, stream)
+
+    flop = 2.0 * M * N * K
+    out = {"M": M, "N": N, "K": K, "alpha": alpha, "beta": beta, "phi": phi, "scale_s": smax, "rows_checked": nrows}
+    C.copy_(C0)
+    lt.dgemm_fp64(A, B, C, M, N, K, alpha, beta, stream)
+    torch.cuda.synchronize()
+    e64 = err_of(C)
+    ms = event_loop(torch, stream, lambda: lt.dgemm_fp64(A, B, C, M, N, K, alpha, beta, stream), steps, 2)
+    out["native_fp64"] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms": ms, "max_err": e64}
+    C.copy_(C0)
+    lt.dgemm_cublas(A, B, C, M, N, K, alpha, beta, stream)
+    torch.cuda.synchronize()
+    ecb = err_of(C)
+    ms = event_loop(torch, stream, lambda: lt.dgemm_cublas(A, B, C, M, N, K, alpha, beta, stream), steps, 2)
+    out["cublas_fp64"] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms": ms, "max_err": ecb}
+    ws = torch.empty(lt.ozaki_crt_workspace_size(M, N, K, lt.LT_OZAKI_CRT_MAX_MODULI), dtype=torch.uint8, device=dev)
+    n, errs = matched_moduli(lt, torch, stream, A, B, C0, C, M, N, K, alpha, beta, ws, err_of, e64)
+    ms = event_loop(torch, stream, lambda: lt.dgemm_ozaki_crt(A, B, C, M, N, K, alpha, beta, n, stream, workspace=ws),
+                    steps, 2)
+    out["ozaki_crt"] = {"moduli": n, "tflops": flop / (ms * 1e-3) / 1e12, "ms": ms, "max_err": errs[n],
+                        "err_by_moduli": errs, "speedup_vs_native_fp64": out["native_fp64"]["ms"] / ms}
+    lt.device_status()
+    del A, B, C0, C, ws, Cref, den
+    torch.cuda.empty_cache()
+    return out
+
+
+def grouped_point(lt, torch, dev, stream, steps, count=512) -> dict:
+    """The batched configuration: `count` problems with M, N, K log-uniform in [32, 1024] (seeded),
+    U[-1,1) entries, alpha = 1, beta = 0, as one grouped plan replayed from a CUDA graph (FP64 form and
+    the Ozaki slice form s = 7), with aggregate TFLOP/s and the max componentwise error over one
+    sampled row of every problem (compensated reference on the device)."""
+    import ctypes
+
+    rng = np.random.default_rng(SEED)
+    dims = np.rint(np.exp(rng.uniform(np.log(32), np.log(1024), size=(count, 3)))).astype(int)
+    bufs, table = [], (lt.GemmProblem * count)()
+    flop = 0.0
+    for i, (M, N, K) in enumerate(dims):
+        M, N, K = int(M), int(N), int(K)
+        A = torch.empty(M, K, dtype=torch.float64, device=dev)
+        B = torch.empty(K, N, dtype=torch.float64, device=dev)
+        C = torch.zeros(M, N, dtype=torch.float64, device=dev)
+        lt.fill(A, M * K, SEED + i, 1, 0, stream)
+        lt.fill(B, K * N, SEED + i, 2, 0, stream)
+        bufs.append((A, B, C))
+        table[i] = lt.GemmProblem(M, N, K, A.data_ptr(), B.data_ptr(), C.data_ptr(), 1.0, 0.0)
+        flop += 2.0 * M * N * K
+    torch.cuda.synchronize()
+    refs = []
+    for (A, B, C) in bufs:
+        M, K, N = A.shape[0], A.shape[1], B.shape[1]
+        r = torch.tensor([M // 2], dtype=torch.int64, device=dev)
+        refs.append((r,) + dot2_reference(lt, torch, A, B, None, M, N, K, 1.0, 0.0, r, stream))
+    L = lt.lib()
+    out = {"problems": count, "dims": "M, N, K log-uniform in [32, 1024]", "flop": flop}
+    for form, slices, key in ((lt.LT_FORM_FP64, 0, "fp64_plan"), (lt.LT_FORM_OZAKI, 7, "ozaki_slices7_plan")):
+        plan = ctypes.c_void_p()
+        lt.check(L.lt_grouped_plan_create(table, count, form, slices, ctypes.byref(plan)))
+        try:
+            lt.check(L.lt_grouped_plan_run_graph(plan, stream.cuda_stream))
+            torch.cuda.synchronize()
+            err = max(max_error(lt, C[r], Cref, den, stream) for (A, B, C), (r, Cref, den) in zip(bufs, refs))
+            ms = event_loop(torch, stream, lambda: lt.check(L.lt_grouped_plan_run_graph(plan, stream.cuda_stream)),
+                            steps, 2)
+            name = ctypes.create_string_buffer(64)
+            L.lt_grouped_plan_config(plan, name, 64)
+            out[key] = {"tflops": flop / (ms * 1e-3) / 1e12, "ms": ms, "max_err_per_problem_max": err,
+                        "config": name.value.decode()}
+        finally:
+            L.lt_grouped_plan_destroy(plan)
+    lt.device_status()
+    del bufs
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(args) -> None:
-    import numpy as np
     import torch
 
     import libthom_b200 as lt
@@ -309,21 +445,12 @@ def run_ours(args) -> None:
     stream = torch.cuda.current_stream()
     M, N, K, alpha, beta, smax, wname = workload(args)
     flop = 2.0 * M * N * K
+    A, B, C0 = fill_problem(lt, torch, dev, stream, M, N, K, args.phi, smax)
+    C = torch.empty_like(C0)
 
-    A = torch.empty(M, K, dtype=torch.float64, device=dev)
-    B = torch.empty(K, N, dtype=torch.float64, device=dev)
-    C0 = torch.empty(M, N, dtype=torch.float64, device=dev)
-    C = torch.empty(M, N, dtype=torch.float64, device=dev)
-    lt.fill(A, M * K, SEED, 1, args.phi, stream)
-    lt.fill(B, K * N, SEED, 2, args.phi, stream)
-    lt.fill(C0, M * N, SEED, 3, args.phi, stream)
-    if smax > 0:
-        lt.scale_rows(A, M, K, SEED, 4, smax, stream)
-        lt.scale_cols(B, K, N, SEED, 5, smax, stream)
-    torch.cuda.synchronize()
-
-    # ---- accuracy selection (untimed): smallest slice count no worse than native FP64, measured
-    # against the library's compensated (Dot2) reference of sampled rows on the device ----
+    # ---- accuracy selection (untimed): the smallest modulus count of the CRT form (and slice count
+    # of the slice form) no worse than native FP64, against the library's compensated (Dot2)
+    # reference of sampled rows computed on the device ----
     rows = np.linspace(0, M - 1, args.check_rows).astype(np.int64)
     rows_d = torch.from_numpy(rows).to(dev)
     t0 = time.perf_counter()
@@ -342,31 +469,35 @@ def run_ours(args) -> None:
     lt.dgemm_cublas(A, B, C, M, N, K, alpha, beta, stream)
     torch.cuda.synchronize()
     err_cublas = err_of(C)
-    ws = torch.empty(lt.ozaki_workspace_size(M, N, K, lt.LT_OZAKI_MAX_SLICES), dtype=torch.uint8, device=dev)
-    errs = {}
-    chosen = None
-    for s in (range(args.slices, args.slices + 1) if args.slices else range(6, lt.LT_OZAKI_MAX_SLICES + 1)):
+    ws = torch.empty(lt.ozaki_crt_workspace_size(M, N, K, lt.LT_OZAKI_CRT_MAX_MODULI), dtype=torch.uint8, device=dev)
+    if args.moduli:
+        n = args.moduli
         C.copy_(C0)
-        lt.dgemm_ozaki(A, B, C, M, N, K, alpha, beta, s, stream, workspace=ws)
+        lt.dgemm_ozaki_crt(A, B, C, M, N, K, alpha, beta, n, stream, workspace=ws)
         torch.cuda.synchronize()
-        errs[s] = err_of(C)
-        if errs[s] <= err_fp64:
-            chosen = s
+        crt_errs = {n: err_of(C)}
+    else:
+        n, crt_errs = matched_moduli(lt, torch, stream, A, B, C0, C, M, N, K, alpha, beta, ws, err_of, err_fp64)
+    ws_sl = torch.empty(lt.ozaki_workspace_size(M, N, K, lt.LT_OZAKI_MAX_SLICES), dtype=torch.uint8, device=dev)
+    sl_errs, s = {}, None
+    for cand in (range(args.slices, args.slices + 1) if args.slices else range(6, lt.LT_OZAKI_MAX_SLICES + 1)):
+        C.copy_(C0)
+        lt.dgemm_ozaki(A, B, C, M, N, K, alpha, beta, cand, stream, workspace=ws_sl)
+        torch.cuda.synchronize()
+        sl_errs[cand] = err_of(C)
+        s = cand
+        if sl_errs[cand] <= err_fp64:
             break
-    if chosen is None:
-        chosen = max(errs)
-    s = chosen
     lt.device_status()
 
     # ---- roofline denominators, measured on this GPU now with the instruction forms the kernels
-    # use (lt_measure_peak: operands on chip, every SM). The timed steps run back to back for longer
-    # than the GPU takes to reach its power limit, so the sustained rate is the denominator; the
-    # one-launch burst rate is reported beside it. ----
-    pair = M > 128 and os.environ.get("LIBTHOM_OZAKI_PAIR", "1") != "0"
-    int8_kind = lt.LT_PEAK_INT8_MMA_PAIR if pair else lt.LT_PEAK_INT8_MMA_N128
+    # use (lt_measure_peak: operands on chip, every SM); the FP64 probe runs after a warm-up launch
+    # so that its burst figure is taken at the ramped clock ----
+    int8_kind = lt.LT_PEAK_INT8_MMA_PAIR
     int8_burst = max(lt.measure_peak(int8_kind, stream) for _ in range(2)) / 1e12
     int8_peak = lt.measure_peak(int8_kind | lt.LT_PEAK_SUSTAINED, stream) / 1e12
-    fp64_burst = max(lt.measure_peak(lt.LT_PEAK_FP64_MMA, stream) for _ in range(2)) / 1e12
+    lt.measure_peak(lt.LT_PEAK_FP64_MMA, stream)
+    fp64_burst = max(lt.measure_peak(lt.LT_PEAK_FP64_MMA, stream) for _ in range(3)) / 1e12
     fp64_peak = lt.measure_peak(lt.LT_PEAK_FP64_MMA | lt.LT_PEAK_SUSTAINED, stream) / 1e12
 
     def barrier():
@@ -377,32 +508,42 @@ def run_ours(args) -> None:
     def max_over_ranks(x: float) -> float:
         return reduce_max(x, dist, dev)
 
-    # ---- headline: Ozaki INT8 path, inputs resident in HBM (512 MiB each > 126 MB L2) ----
-    for _ in range(args.warmup):
-        lt.ozaki_split(A, B, M, N, K, s, ws, stream)
-        lt.ozaki_product(C, M, N, K, alpha, beta, s, ws, stream)
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
-    barrier()
+    def crt_step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        lt.ozaki_crt_split(A, B, M, N, K, n, ws, stream)
+        if ev is not None:
+            ev[1].record(stream)
+        lt.ozaki_crt_multiply(M, N, K, n, ws, stream)
+        if ev is not None:
+            ev[2].record(stream)
+        lt.ozaki_crt_reconstruct(C, M, N, K, alpha, beta, n, ws, stream)
+        if ev is not None:
+            ev[3].record(stream)
+
+    # ---- headline: the CRT form, inputs resident in HBM (512 MiB each > 126 MB L2); the clocks are
+    # sampled from before the warm-up to the end of the timed steps ----
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     with ClockSampler(local) as clk:
+        for _ in range(args.warmup):
+            crt_step()
+        barrier()
         start = torch.cuda.Event(enable_timing=True)
         stop = torch.cuda.Event(enable_timing=True)
         start.record(stream)
         for i in range(args.steps):
-            ev[i][0].record(stream)
-            lt.ozaki_split(A, B, M, N, K, s, ws, stream)
-            ev[i][1].record(stream)
-            lt.ozaki_product(C, M, N, K, alpha, beta, s, ws, stream)
-            ev[i][2].record(stream)
+            crt_step(ev[i])
         stop.record(stream)
         barrier()
     total_ms = max_over_ranks(start.elapsed_time(stop))
     split_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
-    prod_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in ev)
+    mult_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in ev)
+    recon_ms = statistics.mean(e[2].elapsed_time(e[3]) for e in ev)
     lt.device_status()
     ms_step = total_ms / args.steps
     value = world * flop / (ms_step * 1e-3) / 1e12
 
-    # ---- native FP64 tensor-core path and cuBLAS, same inputs ----
+    # ---- native FP64 tensor-core path, cuBLAS and the slice form, same inputs ----
     def time_loop(fn) -> float:
         for _ in range(args.warmup):
             fn()
@@ -418,10 +559,12 @@ def run_ours(args) -> None:
 
     fp64_ms = time_loop(lambda: lt.dgemm_fp64(A, B, C, M, N, K, alpha, beta, stream))
     cublas_ms = time_loop(lambda: lt.dgemm_cublas(A, B, C, M, N, K, alpha, beta, stream))
+    slices_ms = time_loop(lambda: lt.dgemm_ozaki(A, B, C, M, N, K, alpha, beta, s, stream, workspace=ws_sl))
     lt.device_status()
+    del ws_sl
 
-    # ---- end to end through the C ABI with host buffers (pinned): lt_dgemm_ozaki_host copies A, B
-    # and C0 in and C out inside the call (row panels, copies overlapping the kernels). C is updated
+    # ---- end to end through the C ABI with host buffers (pinned): lt_dgemm_ozaki_crt_host copies A,
+    # B and C0 in and C out inside the call (row panels, copies overlapping the kernels). C is updated
     # in place, so each step reads the previous step's C as its C0: same work every step. ----
     Ah = torch.empty(M, K, dtype=torch.float64, pin_memory=True)
     Bh = torch.empty(K, N, dtype=torch.float64, pin_memory=True)
@@ -432,7 +575,7 @@ def run_ours(args) -> None:
     e2e_steps = max(1, min(args.steps, 5))
 
     def e2e_step():
-        lt.dgemm_ozaki_host(Ah, Bh, Ch, M, N, K, alpha, beta, s, stream)
+        lt.dgemm_ozaki_crt_host(Ah, Bh, Ch, M, N, K, alpha, beta, n, stream)
 
     e2e_step()
     barrier()
@@ -447,6 +590,17 @@ def run_ours(args) -> None:
     e2e_value = world * flop / (e2e_ms * 1e-3) / 1e12
     del Ah, Bh, Ch
 
+    extra = {}
+    if args.configs and world == 1:
+        del A, B, C0, C, ws
+        torch.cuda.empty_cache()
+        st = max(2, min(args.steps, 3))
+        extra["config2_phi8"] = config_point(lt, torch, dev, stream, 8192, 8192, 8192, 1.5, 0.5, 8, 0, st)
+        extra["config2_phi32"] = config_point(lt, torch, dev, stream, 8192, 8192, 8192, 1.5, 0.5, 32, 0, st)
+        extra["config4a_tall"] = config_point(lt, torch, dev, stream, 65536, 64, 4096, 1.0, 0.0, 0, 64, st)
+        extra["config4b_longk"] = config_point(lt, torch, dev, stream, 2048, 2048, 65536, 1.0, 0.0, 0, 64, st)
+        extra["config3_grouped"] = grouped_point(lt, torch, dev, stream, st)
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -454,41 +608,55 @@ def run_ours(args) -> None:
 
     peaks = measured_peaks()
     bf16 = peaks.get("bf16_tflops")
-    int8_ops = pairs(s) * flop
-    achieved = int8_ops / (prod_ms * 1e-3) / 1e12
-    traffic = profile_traffic(f"{'ozaki_pair' if pair else 'ozaki_gemm'}_8192_s{s}") if (M, N, K) == (8192,) * 3 else None
+    hbm = peaks.get("hbm_gbs")
+    int8_ops = n * flop
+    achieved = int8_ops / (mult_ms * 1e-3) / 1e12
+    traffic = profile_traffic(f"crt_pair_{M}x{N}x{K}_n{n}")
+    split_bytes = (16 + n) * (M * K + K * N)
+    recon_bytes = (n + (16 if beta != 0.0 else 8)) * M * N
     cpu = None
     if world == 1 and not args.no_cpu:
         cpu = cpu_baseline_blocked(M, N, K, args.cpu_rows, args.phi, smax, len(os.sched_getaffinity(0)))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 (int8 slices, int32 accumulate)", "data": "synthetic (seeded generator)",
-        "config": {"workload": f"{wname}, Ozaki-INT8 s={s}",
+        "vs_baseline": None, "dtype": "f64 (int8 residues, int32 accumulate, f64 reconstruction)",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": f"{wname}, Ozaki-II CRT form with {n} moduli",
                    "M": M, "N": N, "K": K, "alpha": alpha, "beta": beta, "phi": args.phi, "scale_s": smax,
-                   "slices": s, "pairs": pairs(s),
+                   "moduli": n, "int8_products": n,
                    "l2": f"inputs larger than L2 (A {8 * M * K / 2**20:.0f} MiB), no flush",
                    "parallelism": f"replicas x{world}"},
-        "accuracy": {"max_componentwise_err": {"ozaki": errs[s], "native_fp64": err_fp64, "cublas": err_cublas},
-                     "ozaki_by_slices": errs, "rows_checked": len(rows),
+        "accuracy": {"max_componentwise_err": {"ozaki_crt": crt_errs[n], "native_fp64": err_fp64, "cublas": err_cublas,
+                                               "ozaki_slices": sl_errs[s]},
+                     "ozaki_crt_by_moduli": crt_errs, "ozaki_slices_by_count": sl_errs, "rows_checked": len(rows),
                      "reference": f"compensated Dot2 on {len(rows)} rows, on the device (lt_dot2_rows, "
                                   f"{ref_s:.2f} s)"},
         "native_fp64": {"value": world * flop / (fp64_ms * 1e-3) / 1e12, "ms_per_step": fp64_ms,
                         "frac_of_dmma_peak": flop / (fp64_ms * 1e-3) / 1e12 / fp64_peak},
         "cublas_fp64": {"value": world * flop / (cublas_ms * 1e-3) / 1e12, "ms_per_step": cublas_ms},
+        "ozaki_slices": {"slices": s, "pairs": pairs(s), "value": world * flop / (slices_ms * 1e-3) / 1e12,
+                         "ms_per_step": slices_ms},
         "speedup_vs_native_fp64": fp64_ms / ms_step,
-        "stages_ms": {"split": split_ms, "product": prod_ms},
-        "roofline": {"bound": "tensor", "kernel": "ozaki_pair_kernel" if pair else "ozaki_gemm_kernel",
+        "stages_ms": {"split": split_ms, "multiply": mult_ms, "reconstruct": recon_ms},
+        "roofline": {"bound": "tensor", "kernel": "crt_pair_kernel",
                      "achieved": achieved, "peak": int8_peak, "unit": "TOP/s (INT8)", "frac": achieved / int8_peak,
-                     "peak_source": "measured in this run, sustained: lt_measure_peak("
-                                    + ("tcgen05.mma.cta_group::2 kind::i8 M256 N128" if pair else
-                                       "tcgen05.mma kind::i8 M128 N128") + " | LT_PEAK_SUSTAINED), operands on "
-                                    "chip, all SMs, after 0.5 s at the power limit",
+                     "peak_source": "measured in this run, sustained: lt_measure_peak(tcgen05.mma.cta_group::2 "
+                                    "kind::i8 M256 N128 | LT_PEAK_SUSTAINED), operands on chip, all SMs, after 0.5 s "
+                                    "at the power limit",
                      "peak_burst": int8_burst, "frac_of_burst": achieved / int8_burst,
                      "peak_bf16x2": 2.0 * bf16 if bf16 else None,
                      "frac_of_bf16x2": achieved / (2.0 * bf16) if bf16 else None,
                      "traffic": traffic,
-                     "algorithmic": f"{pairs(s)} INT8 slice products x 2MNK = {int8_ops:.4g} ops per launch"},
+                     "algorithmic": f"{n} INT8 residue products x 2MNK = {int8_ops:.4g} ops per launch"},
+        "roofline_split": {"bound": "hbm", "kernels": "amax_both_kernel, crt_split_rows_kernel, crt_split_cols_kernel",
+                           "achieved": split_bytes / (split_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                           "frac": split_bytes / (split_ms * 1e-3) / 1e9 / hbm if hbm else None,
+                           "algorithmic": f"(16 + {n}) (MK + KN) bytes: A, B read twice, {n} residue bytes written"},
+        "roofline_reconstruct": {"bound": "hbm", "kernel": "crt_recon_kernel",
+                                 "achieved": recon_bytes / (recon_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                                 "frac": recon_bytes / (recon_ms * 1e-3) / 1e9 / hbm if hbm else None,
+                                 "algorithmic": f"({n} residue bytes + C0 read + C written) per element of C"},
         "roofline_fp64": {"bound": "tensor", "kernel": "dgemm_fp64_kernel",
                           "achieved": flop / (fp64_ms * 1e-3) / 1e12, "peak": fp64_peak,
                           "unit": "TFLOP/s (FP64)", "frac": flop / (fp64_ms * 1e-3) / 1e12 / fp64_peak,
@@ -497,13 +665,15 @@ def run_ours(args) -> None:
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": 8 * (M * K + K * N + (M * N if beta != 0.0 else 0)),
                 "d2h_bytes_per_step": 8 * M * N, "ms_per_step": e2e_ms,
-                "path": "lt_dgemm_ozaki_host C ABI on pinned host buffers: H2D of A, B, C0 and D2H of C inside "
+                "path": "lt_dgemm_ozaki_crt_host C ABI on pinned host buffers: H2D of A, B, C0 and D2H of C inside "
                         "the call, row panels overlapping the copies with the kernels"},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
-        # per timed step: amax_both_kernel, split_both_kernel<s>, ozaki_pair_kernel<s>
-        "gpu_launches": 3 * args.steps,
+        # per timed step: amax_both_kernel, crt_split_rows_kernel, crt_split_cols_kernel, crt_pair_kernel,
+        # crt_recon_kernel
+        "gpu_launches": 5 * args.steps,
     }
+    line.update(extra)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -854,7 +1024,11 @@ def main() -> None:
                     help="square: size^3, alpha=1.5, beta=0.5 (the headline); tall: 65536x64x4096 and longk: "
                          "2048x2048x65536, alpha=1, beta=0, rows of A / columns of B scaled by 2^s, s ~ U{-64..64}")
     ap.add_argument("--phi", type=int, default=0)
-    ap.add_argument("--slices", type=int, default=0, help="fix the slice count (0 = accuracy-matched)")
+    ap.add_argument("--slices", type=int, default=0, help="fix the slice form's slice count (0 = accuracy-matched)")
+    ap.add_argument("--moduli", type=int, default=0, help="fix the CRT form's modulus count (0 = accuracy-matched)")
+    ap.add_argument("--no-configs", dest="configs", action="store_false",
+                    help="skip the other BASELINE configurations (phi 8 and 32, 65536x64x4096, 2048x2048x65536, "
+                         "the 512-problem grouped set)")
     ap.add_argument("--check-rows", type=int, default=16)
     ap.add_argument("--cpu-rows", type=int, default=1024)
     ap.add_argument("--no-cpu", action="store_true")

@@ -182,6 +182,18 @@ int lt_ozaki_crt_split(const double* A, const double* B, int64_t M, int64_t N, i
                        size_t workspace_bytes, void* stream);
 int lt_ozaki_crt_product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int moduli,
                          const void* workspace, size_t workspace_bytes, void* stream);
+/* lt_ozaki_crt_product in its two launches: the INT8 products into the workspace's residue planes of
+ * C, then the reconstruction of C from them (with alpha and beta). */
+int lt_ozaki_crt_multiply(int64_t M, int64_t N, int64_t K, int moduli, void* workspace, size_t workspace_bytes,
+                          void* stream);
+int lt_ozaki_crt_reconstruct(double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int moduli,
+                             const void* workspace, size_t workspace_bytes, void* stream);
+/* The CRT form on HOST memory (A, B, C host pointers; C holds C0 on entry when beta != 0 and the
+ * result on return), the CRT counterpart of lt_dgemm_ozaki_host: B is copied and split first, then row
+ * panels of A and C0 are copied while earlier panels are multiplied and finished panels of C copied
+ * back. Overlap needs page-locked host buffers. Bit-identical to lt_dgemm_ozaki_crt. Synchronous. */
+int lt_dgemm_ozaki_crt_host(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
+                            double alpha, double beta, int moduli, void* stream);
 /* The operand bits pa, pb the CRT form uses for `moduli` moduli and inner dimension K, and the moduli
  * themselves (moduli_out: `moduli` ints; any pointer may be NULL). Host arithmetic only. */
 int lt_ozaki_crt_info(int moduli, int64_t K, int* pa, int* pb, int* moduli_out);

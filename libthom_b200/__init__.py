@@ -105,6 +105,9 @@ SIGNATURES = {
     "lt_dgemm_ozaki_crt_ws": (_i32, _GEMM + [_i32, _vp, _sz, _vp]),
     "lt_ozaki_crt_split": (_i32, [_vp, _vp, _i64, _i64, _i64, _i32, _vp, _sz, _vp]),
     "lt_ozaki_crt_product": (_i32, [_vp, _i64, _i64, _i64, _f64, _f64, _i32, _vp, _sz, _vp]),
+    "lt_dgemm_ozaki_crt_host": (_i32, _GEMM + [_i32, _vp]),
+    "lt_ozaki_crt_multiply": (_i32, [_i64, _i64, _i64, _i32, _vp, _sz, _vp]),
+    "lt_ozaki_crt_reconstruct": (_i32, [_vp, _i64, _i64, _i64, _f64, _f64, _i32, _vp, _sz, _vp]),
     "lt_ozaki_crt_info": (_i32, [_i32, _i64, _c.POINTER(_i32), _c.POINTER(_i32), _c.POINTER(_i32)]),
     "dgemm_ozaki_crt14": (_f32, _REF), "dgemm_ozaki_crt15": (_f32, _REF), "dgemm_ozaki_crt16": (_f32, _REF),
     "dgemm_ozaki_crt17": (_f32, _REF), "dgemm_ozaki_crt18": (_f32, _REF),
@@ -243,6 +246,22 @@ def ozaki_crt_split(A, B, M, N, K, moduli, workspace, stream=None) -> None:
 def ozaki_crt_product(C, M, N, K, alpha, beta, moduli, workspace, stream=None) -> None:
     check(lib().lt_ozaki_crt_product(_ptr(C), M, N, K, alpha, beta, moduli, _ptr(workspace),
                                      workspace.numel() * workspace.element_size(), _stream(stream)))
+
+
+def dgemm_ozaki_crt_host(A, B, C, M, N, K, alpha=1.0, beta=0.0, moduli=15, stream=None) -> None:
+    """CRT form on host (CPU) tensors or arrays, pipelined through the GPU (lt_dgemm_ozaki_crt_host).
+    C holds C0 on entry and the result on return."""
+    check(lib().lt_dgemm_ozaki_crt_host(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, moduli, _stream(stream)))
+
+
+def ozaki_crt_multiply(M, N, K, moduli, workspace, stream=None) -> None:
+    check(lib().lt_ozaki_crt_multiply(M, N, K, moduli, _ptr(workspace), workspace.numel() * workspace.element_size(),
+                                      _stream(stream)))
+
+
+def ozaki_crt_reconstruct(C, M, N, K, alpha, beta, moduli, workspace, stream=None) -> None:
+    check(lib().lt_ozaki_crt_reconstruct(_ptr(C), M, N, K, alpha, beta, moduli, _ptr(workspace),
+                                         workspace.numel() * workspace.element_size(), _stream(stream)))
 
 
 def ozaki_crt_workspace_size(M, N, K, moduli) -> int:

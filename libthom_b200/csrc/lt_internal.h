@@ -47,6 +47,11 @@ size_t workspace_size(int64_t M, int64_t N, int64_t K, int slices);
 // M, N, K > 0 and both arrays zero on entry.
 int exponents(const double* A, const double* B, int64_t M, int64_t N, int64_t K, unsigned long long* amax_a,
               unsigned long long* amax_b, int sms, cudaStream_t stream);
+// The same for one side, with a row stride.
+int exponents_rows(const double* A, int64_t M, int64_t K, int64_t lda, unsigned long long* amax, int sms,
+                   cudaStream_t stream);
+int exponents_cols(const double* B, int64_t K, int64_t N, int64_t ldb, unsigned long long* amax, int sms,
+                   cudaStream_t stream);
 int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int slices, void* workspace,
           size_t workspace_bytes, cudaStream_t stream);
 int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int slices, const void* workspace,

@@ -1340,20 +1340,41 @@ void launch_split_cols_s(const double* B, int64_t K, int64_t N, int64_t ldb, int
 // Row side of the split: exponents of rows 0..M-1 of A (amax must be zero on entry) and their
 // slices, written as row blocks 0.. of `sa` (chunk-major, NC chunks; half_major for B slices that
 // the CTA-pair kernel reads, see store_tile_row).
+// Row maxima of A (M x K, row stride lda) as IEEE bits into amax (zero on entry); M, K > 0.
+int exponents_rows(const double* A, int64_t M, int64_t K, int64_t lda, unsigned long long* amax, int sms,
+                   cudaStream_t stream) {
+  // 8 rows per block, K split so that the grid covers the GPU.
+  int64_t row_blocks = (M + 7) / 8;
+  int64_t ksplit = (4 * sms + row_blocks - 1) / row_blocks;
+  ksplit = ksplit < 1 ? 1 : ksplit;
+  int64_t kseg = round_up((K + ksplit - 1) / ksplit, 256);
+  ksplit = (K + kseg - 1) / kseg;
+  amax_rows_kernel<<<dim3(static_cast<unsigned>(row_blocks), static_cast<unsigned>(ksplit)), 256, 0, stream>>>(
+      A, M, K, lda, kseg, amax);
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
+// Column maxima of B (K x N, row stride ldb) as IEEE bits into amax (zero on entry); N, K > 0.
+int exponents_cols(const double* B, int64_t K, int64_t N, int64_t ldb, unsigned long long* amax, int sms,
+                   cudaStream_t stream) {
+  const int pairs = (N % 2 == 0) && (ldb % 2 == 0) && ((reinterpret_cast<uintptr_t>(B) & 15) == 0);
+  const int64_t per_block = pairs ? 512 : 256;
+  int64_t col_blocks = (N + per_block - 1) / per_block;
+  int64_t ksplit_b = (8 * sms + col_blocks - 1) / col_blocks;
+  ksplit_b = ksplit_b < 1 ? 1 : ksplit_b;
+  int64_t kseg_b = (K + ksplit_b - 1) / ksplit_b;
+  ksplit_b = (K + kseg_b - 1) / kseg_b;
+  amax_cols_kernel<<<dim3(static_cast<unsigned>(col_blocks), static_cast<unsigned>(ksplit_b)), 256, 0, stream>>>(
+      B, K, N, ldb, kseg_b, amax, pairs);
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
 int rows_stage(int s, const double* A, int64_t M, int64_t K, int64_t lda, int64_t NC, unsigned long long* amax,
                int8_t* sa, int sms, cudaStream_t stream, int half_major) {
   if (M <= 0) return LT_OK;
-  if (K > 0) {
-    // 8 rows per block, K split so that the grid covers the GPU.
-    int64_t row_blocks = (M + 7) / 8;
-    int64_t ksplit = (4 * sms + row_blocks - 1) / row_blocks;
-    ksplit = ksplit < 1 ? 1 : ksplit;
-    int64_t kseg = round_up((K + ksplit - 1) / ksplit, 256);
-    ksplit = (K + kseg - 1) / kseg;
-    amax_rows_kernel<<<dim3(static_cast<unsigned>(row_blocks), static_cast<unsigned>(ksplit)), 256, 0, stream>>>(
-        A, M, K, lda, kseg, amax);
-    LT_CUDA_TRY(cudaGetLastError());
-  }
+  if (K > 0) LT_TRY(exponents_rows(A, M, K, lda, amax, sms, stream));
   switch (s) {
 #define LT_ROWS_CASE(S) \
   case S: launch_split_rows_s<S>(A, M, K, lda, NC, amax, sa, sms, stream, half_major); break;
@@ -1370,18 +1391,7 @@ int rows_stage(int s, const double* A, int64_t M, int64_t K, int64_t lda, int64_
 int cols_stage(int s, const double* B, int64_t K, int64_t N, int64_t ldb, int64_t NC, unsigned long long* amax,
                int8_t* sb, int sms, cudaStream_t stream, int half_major) {
   if (N <= 0) return LT_OK;
-  if (K > 0) {
-    const int pairs = (N % 2 == 0) && (ldb % 2 == 0) && ((reinterpret_cast<uintptr_t>(B) & 15) == 0);
-    const int64_t per_block = pairs ? 512 : 256;
-    int64_t col_blocks = (N + per_block - 1) / per_block;
-    int64_t ksplit_b = (8 * sms + col_blocks - 1) / col_blocks;
-    ksplit_b = ksplit_b < 1 ? 1 : ksplit_b;
-    int64_t kseg_b = (K + ksplit_b - 1) / ksplit_b;
-    ksplit_b = (K + kseg_b - 1) / kseg_b;
-    amax_cols_kernel<<<dim3(static_cast<unsigned>(col_blocks), static_cast<unsigned>(ksplit_b)), 256, 0, stream>>>(
-        B, K, N, ldb, kseg_b, amax, pairs);
-    LT_CUDA_TRY(cudaGetLastError());
-  }
+  if (K > 0) LT_TRY(exponents_cols(B, K, N, ldb, amax, sms, stream));
   switch (s) {
 #define LT_COLS_CASE(S) \
   case S: launch_split_cols_s<S>(B, K, N, ldb, NC, amax, sb, sms, stream, half_major); break;

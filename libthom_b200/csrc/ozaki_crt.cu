@@ -43,6 +43,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "lt_internal.h"
 #include "lt_runtime.cuh"
@@ -321,7 +322,7 @@ template <int NM>
 __global__ void __launch_bounds__(256) crt_split_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K,
                                                              int64_t lda, int64_t Kp,
                                                              const unsigned long long* __restrict__ amax,
-                                                             int8_t* __restrict__ out, int pa) {
+                                                             int8_t* __restrict__ out, int64_t plane, int pa) {
   const Consts& c = c_table[NM - kMinMod];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t row = static_cast<int64_t>(blockIdx.x) * 8 + warp;
@@ -345,7 +346,7 @@ __global__ void __launch_bounds__(256) crt_split_rows_kernel(const double* __res
   residues_of<NM>(v, e, pa, c, r);
   int8_t* dst = out + row * Kp + k0;
 #pragma unroll
-  for (int l = 0; l < NM; ++l) *reinterpret_cast<uint4*>(dst + l * M * Kp) = r[l];
+  for (int l = 0; l < NM; ++l) *reinterpret_cast<uint4*>(dst + l * plane) = r[l];
 }
 
 // Columns of B, transposed to K-major: a block covers 32 columns (one per lane) and 128 K positions
@@ -358,7 +359,7 @@ template <int NM>
 __global__ void __launch_bounds__(256) crt_split_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N,
                                                              int64_t ldb, int64_t Kp,
                                                              const unsigned long long* __restrict__ amax,
-                                                             int8_t* __restrict__ out, int pb) {
+                                                             int8_t* __restrict__ out, int64_t plane, int pb) {
   __shared__ __align__(16) uint8_t stage[kColPlanes][32 * kColPitch];
   const Consts& c = c_table[NM - kMinMod];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -392,7 +393,7 @@ __global__ void __launch_bounds__(256) crt_split_cols_kernel(const double* __res
     if (writes) {
 #pragma unroll
       for (int l = l0; l < l0 + kColPlanes && l < NM; ++l)
-        *reinterpret_cast<uint4*>(dst + l * N * Kp) =
+        *reinterpret_cast<uint4*>(dst + l * plane) =
             *reinterpret_cast<const uint4*>(&stage[l - l0][cl * kColPitch + part * 16]);
     }
   }
@@ -762,17 +763,47 @@ int raster_group() {
   return g;
 }
 
+// Residue planes of rows 0..M-1 of A (row stride K) into `ra` (plane stride `plane`), and of the
+// columns of B (row stride N) into `rb`, for NM moduli.
 template <int NM>
-int split_n(const double* A, const double* B, int64_t M, int64_t N, int64_t K, const Layout& L, int pa, int pb,
-            const unsigned long long* amax_a, const unsigned long long* amax_b, int8_t* ra, int8_t* rb,
-            cudaStream_t stream) {
-  const dim3 grid_a(static_cast<unsigned>(ceil_div(M, 8)), static_cast<unsigned>(ceil_div(L.Kp, 512)));
-  crt_split_rows_kernel<NM><<<grid_a, 256, 0, stream>>>(A, M, K, K, L.Kp, amax_a, ra, pa);
-  LT_CUDA_TRY(cudaGetLastError());
-  const dim3 grid_b(static_cast<unsigned>(ceil_div(N, 32)), static_cast<unsigned>(L.Kp / kBK));
-  crt_split_cols_kernel<NM><<<grid_b, 256, 0, stream>>>(B, K, N, N, L.Kp, amax_b, rb, pb);
+int split_rows_n(const double* A, int64_t M, int64_t K, int64_t Kp, const unsigned long long* amax, int8_t* ra,
+                 int64_t plane, int pa, cudaStream_t stream) {
+  const dim3 grid(static_cast<unsigned>(ceil_div(M, 8)), static_cast<unsigned>(ceil_div(Kp, 512)));
+  crt_split_rows_kernel<NM><<<grid, 256, 0, stream>>>(A, M, K, K, Kp, amax, ra, plane, pa);
   LT_CUDA_TRY(cudaGetLastError());
   return LT_OK;
+}
+
+template <int NM>
+int split_cols_n(const double* B, int64_t K, int64_t N, int64_t Kp, const unsigned long long* amax, int8_t* rb,
+                 int64_t plane, int pb, cudaStream_t stream) {
+  const dim3 grid(static_cast<unsigned>(ceil_div(N, 32)), static_cast<unsigned>(Kp / kBK));
+  crt_split_cols_kernel<NM><<<grid, 256, 0, stream>>>(B, K, N, N, Kp, amax, rb, plane, pb);
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
+#define LT_CRT_DISPATCH(n, CALL)                                                                             \
+  switch (n) {                                                                                              \
+    case 8: return CALL(8); case 9: return CALL(9); case 10: return CALL(10); case 11: return CALL(11);     \
+    case 12: return CALL(12); case 13: return CALL(13); case 14: return CALL(14); case 15: return CALL(15); \
+    case 16: return CALL(16); case 17: return CALL(17); case 18: return CALL(18); case 19: return CALL(19); \
+    case 20: return CALL(20);                                                                               \
+    default: return set_error(LT_ERR_INVALID_ARGUMENT, "modulus count %d outside [%d, %d]", n, kMinMod, kMaxMod); \
+  }
+
+int split_rows(int n, const double* A, int64_t M, int64_t K, int64_t Kp, const unsigned long long* amax, int8_t* ra,
+               int64_t plane, int pa, cudaStream_t stream) {
+#define LT_CALL(NM) split_rows_n<NM>(A, M, K, Kp, amax, ra, plane, pa, stream)
+  LT_CRT_DISPATCH(n, LT_CALL)
+#undef LT_CALL
+}
+
+int split_cols(int n, const double* B, int64_t K, int64_t N, int64_t Kp, const unsigned long long* amax, int8_t* rb,
+               int64_t plane, int pb, cudaStream_t stream) {
+#define LT_CALL(NM) split_cols_n<NM>(B, K, N, Kp, amax, rb, plane, pb, stream)
+  LT_CRT_DISPATCH(n, LT_CALL)
+#undef LT_CALL
 }
 
 int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int n, void* workspace,
@@ -791,21 +822,34 @@ int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int
   const Consts c = make_consts(n, K);
   auto* ra = reinterpret_cast<int8_t*>(ws + L.off_ra);
   auto* rb = reinterpret_cast<int8_t*>(ws + L.off_rb);
-  switch (n) {
-#define LT_CRT_SPLIT(NM) \
-  case NM: return split_n<NM>(A, B, M, N, K, L, c.pa, c.pb, amax_a, amax_b, ra, rb, stream);
-    LT_CRT_SPLIT(8) LT_CRT_SPLIT(9) LT_CRT_SPLIT(10) LT_CRT_SPLIT(11) LT_CRT_SPLIT(12) LT_CRT_SPLIT(13)
-    LT_CRT_SPLIT(14) LT_CRT_SPLIT(15) LT_CRT_SPLIT(16) LT_CRT_SPLIT(17) LT_CRT_SPLIT(18) LT_CRT_SPLIT(19)
-    LT_CRT_SPLIT(20)
-#undef LT_CRT_SPLIT
-    default: return set_error(LT_ERR_INVALID_ARGUMENT, "modulus count %d outside [%d, %d]", n, kMinMod, kMaxMod);
-  }
+  LT_TRY(split_rows(n, A, M, K, L.Kp, amax_a, ra, M * L.Kp, c.pa, stream));
+  return split_cols(n, B, K, N, L.Kp, amax_b, rb, N * L.Kp, c.pb, stream);
 }
+
+// One product stage over rows 0..M-1 of residue planes `ra` (plane stride a_plane) against all N
+// columns of `rb`, into the C residue planes at `res` (plane stride res_plane, row pitch Np, whole
+// 256 x 256 tiles) and then, reconstructed, into C (row stride ldc).
+struct ProductArgs {
+  const int8_t* ra;
+  int64_t a_plane;
+  const int8_t* rb;
+  int64_t b_plane;
+  int64_t Kp;
+  uint8_t* res;
+  int64_t res_plane, Np;
+  double* C;
+  int64_t M, N, ldc, K;
+  const unsigned long long* amax_a;
+  const unsigned long long* amax_b;
+  double alpha, beta;
+  int n;
+};
 
 template <int NM>
 int launch_product_n(const CUtensorMap& tmA, const CUtensorMap& tmB, const Problem& p, const Consts& c, double* C,
-                     int64_t M, int64_t N, const unsigned long long* amax_a, const unsigned long long* amax_b,
-                     double alpha, double beta, DeviceContext* ctx, cudaStream_t stream) {
+                     int64_t M, int64_t N, int64_t ldc, const unsigned long long* amax_a,
+                     const unsigned long long* amax_b, double alpha, double beta, DeviceContext* ctx,
+                     cudaStream_t stream, bool do_multiply, bool do_reconstruct) {
   if (c.nl != limbs_for(NM)) return set_error(LT_ERR_UNSUPPORTED, "CRT limb count %d, kernel built for %d", c.nl, limbs_for(NM));
   static std::once_flag once[64];
   static cudaError_t attr_err[64];
@@ -838,56 +882,203 @@ int launch_product_n(const CUtensorMap& tmA, const CUtensorMap& tmB, const Probl
   cudaLaunchConfig_t cfg;
   cudaLaunchAttribute attr;
   config(&cfg, &attr, static_cast<unsigned>(2 * clusters));
-  LT_CUDA_TRY(cudaLaunchKernelEx(&cfg, crt_pair_kernel<NM>, tmA, tmB, p, ctx->status));
-  const int64_t work = M * ((N + 3) / 4);
-  const int64_t blocks = std::min<int64_t>(ceil_div(work, 256), 8 * ctx->sm_count);
-  crt_recon_kernel<NM><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p.res, p.plane, p.Np, C, M, N, N, amax_a,
-                                                                           amax_b, alpha, beta, c.pa, c.pb);
-  LT_CUDA_TRY(cudaGetLastError());
+  if (do_multiply) LT_CUDA_TRY(cudaLaunchKernelEx(&cfg, crt_pair_kernel<NM>, tmA, tmB, p, ctx->status));
+  if (do_reconstruct) {
+    const int64_t work = M * ((N + 3) / 4);
+    const int64_t blocks = std::min<int64_t>(ceil_div(work, 256), 8 * ctx->sm_count);
+    crt_recon_kernel<NM><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p.res, p.plane, p.Np, C, M, N, ldc,
+                                                                             amax_a, amax_b, alpha, beta, c.pa, c.pb);
+    LT_CUDA_TRY(cudaGetLastError());
+  }
   return LT_OK;
 }
 
+int run_product(const ProductArgs& a, DeviceContext* ctx, cudaStream_t stream, bool do_multiply, bool do_reconstruct) {
+  LT_TRY(ensure_table(ctx->device));
+  CUtensorMap tmA, tmB;
+  LT_TRY(make_tmap_3d(&tmA, a.ra, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, a.n, a.M, a.Kp, a.Kp, a.a_plane, kBM, kBK,
+                      CU_TENSOR_MAP_SWIZZLE_128B));
+  LT_TRY(make_tmap_3d(&tmB, a.rb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, a.n, a.N, a.Kp, a.Kp, a.b_plane, kBN / 2, kBK,
+                      CU_TENSOR_MAP_SWIZZLE_128B));
+  Problem p;
+  p.res = a.res;
+  p.plane = a.res_plane;
+  p.Np = a.Np;
+  p.tiles_m = static_cast<int>(ceil_div(a.M, 2 * kBM));
+  p.tiles_n = static_cast<int>(ceil_div(a.N, kBN));
+  p.ksteps = static_cast<int>(a.Kp / kBK);
+  p.kgroups = static_cast<int>(ceil_div(p.ksteps, kGroupSteps));
+  p.group = raster_group();
+  const Consts c = make_consts(a.n, a.K);
+#define LT_CALL(NM)                                                                                           \
+  launch_product_n<NM>(tmA, tmB, p, c, a.C, a.M, a.N, a.ldc, a.amax_a, a.amax_b, a.alpha, a.beta, ctx, stream, \
+                       do_multiply, do_reconstruct)
+  LT_CRT_DISPATCH(a.n, LT_CALL)
+#undef LT_CALL
+}
+
+// The products into the residue planes of C (do_multiply) and the reconstruction of C from them
+// (do_reconstruct); both for the whole product stage.
 int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int n, const void* workspace,
-            size_t workspace_bytes, cudaStream_t stream) {
+            size_t workspace_bytes, cudaStream_t stream, bool do_multiply = true, bool do_reconstruct = true) {
   DeviceContext* ctx = context();
   if (ctx == nullptr) return last_error();
   const Layout L = layout_for(M, N, K, n);
   if (workspace_bytes < L.total) return set_error(LT_ERR_NO_MEMORY, "CRT workspace too small");
   if (K == 0) {
+    if (!do_reconstruct) return LT_OK;
     const int64_t total = M * N;
     const int64_t blocks = std::min<int64_t>(ceil_div(total, 256), 4 * ctx->sm_count);
     k0_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(C, M, N, N, alpha, beta);
     LT_CUDA_TRY(cudaGetLastError());
     return LT_OK;
   }
-  LT_TRY(ensure_table(ctx->device));
   const uint8_t* ws = static_cast<const uint8_t*>(workspace);
-  CUtensorMap tmA, tmB;
-  LT_TRY(make_tmap_3d(&tmA, ws + L.off_ra, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, n, M, L.Kp, L.Kp, M * L.Kp, kBM, kBK,
-                      CU_TENSOR_MAP_SWIZZLE_128B));
-  LT_TRY(make_tmap_3d(&tmB, ws + L.off_rb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, n, N, L.Kp, L.Kp, N * L.Kp, kBN / 2, kBK,
-                      CU_TENSOR_MAP_SWIZZLE_128B));
-  Problem p;
-  p.res = const_cast<uint8_t*>(ws + L.off_rc);
-  p.plane = L.Mp * L.Np;
-  p.Np = L.Np;
-  p.tiles_m = static_cast<int>(L.Mp / (2 * kBM));
-  p.tiles_n = static_cast<int>(L.Np / kBN);
-  p.ksteps = static_cast<int>(L.Kp / kBK);
-  p.kgroups = static_cast<int>(ceil_div(p.ksteps, kGroupSteps));
-  p.group = raster_group();
+  ProductArgs a;
+  a.ra = reinterpret_cast<const int8_t*>(ws + L.off_ra);
+  a.a_plane = M * L.Kp;
+  a.rb = reinterpret_cast<const int8_t*>(ws + L.off_rb);
+  a.b_plane = N * L.Kp;
+  a.Kp = L.Kp;
+  a.res = const_cast<uint8_t*>(ws + L.off_rc);
+  a.res_plane = L.Mp * L.Np;
+  a.Np = L.Np;
+  a.C = C;
+  a.M = M;
+  a.N = N;
+  a.ldc = N;
+  a.K = K;
+  a.amax_a = reinterpret_cast<const unsigned long long*>(ws + L.off_amax_a);
+  a.amax_b = reinterpret_cast<const unsigned long long*>(ws + L.off_amax_b);
+  a.alpha = alpha;
+  a.beta = beta;
+  a.n = n;
+  return run_product(a, ctx, stream, do_multiply, do_reconstruct);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host-resident operands (lt_dgemm_ozaki_crt_host): B is copied, its exponents and residues taken;
+// then row panels of A (and of C0 when beta != 0), whole 256-row pair blocks each, are copied on one
+// stream while earlier panels are split, multiplied and reconstructed on the caller's stream, and
+// finished panels of C go back on a third, so the PCIe copies overlap the kernels. Each panel's rows
+// land where run() puts them and go through the same arithmetic: C is bit-identical to
+// lt_dgemm_ozaki_crt.
+// ---------------------------------------------------------------------------------------------
+int host_panels() {
+  static const int n = [] {
+    const char* e = getenv("LIBTHOM_OZAKI_HOST_PANELS");
+    const int v = e != nullptr ? atoi(e) : 0;
+    return (v >= 1 && v <= 64) ? v : 16;
+  }();
+  return n;
+}
+
+int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta,
+             int n, cudaStream_t stream) {
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  const Layout L = layout_for(M, N, K, n);
+  const size_t off_a = round_up(static_cast<int64_t>(L.total), 256);
+  const size_t off_b = off_a + round_up(8 * M * K, 256);
+  const size_t off_c = off_b + round_up(8 * K * N, 256);
+  const size_t total = off_c + 8 * static_cast<size_t>(M) * N;
+  void* base = nullptr;
+  LT_TRY(ensure_workspace(ctx, total, &base));
+  LT_TRY(ensure_table(ctx->device));
+  uint8_t* ws = static_cast<uint8_t*>(base);
+  auto* amax_a = reinterpret_cast<unsigned long long*>(ws + L.off_amax_a);
+  auto* amax_b = reinterpret_cast<unsigned long long*>(ws + L.off_amax_b);
+  auto* ra = reinterpret_cast<int8_t*>(ws + L.off_ra);
+  auto* rb = reinterpret_cast<int8_t*>(ws + L.off_rb);
+  auto* Ad = reinterpret_cast<double*>(ws + off_a);
+  auto* Bd = reinterpret_cast<double*>(ws + off_b);
+  auto* Cd = reinterpret_cast<double*>(ws + off_c);
   const Consts c = make_consts(n, K);
-  const auto* amax_a = reinterpret_cast<const unsigned long long*>(ws + L.off_amax_a);
-  const auto* amax_b = reinterpret_cast<const unsigned long long*>(ws + L.off_amax_b);
-  switch (n) {
-#define LT_CRT_PRODUCT(NM) \
-  case NM: return launch_product_n<NM>(tmA, tmB, p, c, C, M, N, amax_a, amax_b, alpha, beta, ctx, stream);
-    LT_CRT_PRODUCT(8) LT_CRT_PRODUCT(9) LT_CRT_PRODUCT(10) LT_CRT_PRODUCT(11) LT_CRT_PRODUCT(12) LT_CRT_PRODUCT(13)
-    LT_CRT_PRODUCT(14) LT_CRT_PRODUCT(15) LT_CRT_PRODUCT(16) LT_CRT_PRODUCT(17) LT_CRT_PRODUCT(18)
-    LT_CRT_PRODUCT(19) LT_CRT_PRODUCT(20)
-#undef LT_CRT_PRODUCT
-    default: return set_error(LT_ERR_INVALID_ARGUMENT, "modulus count %d outside [%d, %d]", n, kMinMod, kMaxMod);
+
+  const int64_t panel = std::max<int64_t>(2 * kBM, round_up(ceil_div(M, host_panels()), 2 * kBM));
+  const int64_t npanels = ceil_div(M, panel);
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  std::vector<cudaEvent_t> ev(2 * npanels + 2, nullptr);
+  int rc = LT_OK;
+  auto cuda = [&](cudaError_t e, const char* what) {
+    if (e != cudaSuccess && rc == LT_OK) rc = set_error(LT_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return rc == LT_OK;
+  };
+  cuda(cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking), "stream");
+  cuda(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking), "stream");
+  for (auto& e : ev)
+    if (rc == LT_OK) cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+  cudaEvent_t e_start = ev[2 * npanels], e_b = ev[2 * npanels + 1];
+  if (rc == LT_OK) {
+    // Everything starts after the work already queued on the caller's stream.
+    cuda(cudaEventRecord(e_start, stream), "record");
+    cuda(cudaStreamWaitEvent(h2d, e_start, 0), "wait");
+    cuda(cudaStreamWaitEvent(d2h, e_start, 0), "wait");
+    if (K > 0) cuda(cudaMemcpyAsync(Bd, B, 8 * static_cast<size_t>(K) * N, cudaMemcpyHostToDevice, h2d), "copy B");
+    cuda(cudaEventRecord(e_b, h2d), "record");
+    cuda(cudaMemsetAsync(ws, 0, L.off_ra, stream), "memset");
+    cuda(cudaStreamWaitEvent(stream, e_b, 0), "wait");
   }
+  if (rc == LT_OK && K > 0) rc = ozaki::exponents_cols(Bd, K, N, N, amax_b, ctx->sm_count, stream);
+  if (rc == LT_OK && K > 0) rc = split_cols(n, Bd, K, N, L.Kp, amax_b, rb, N * L.Kp, c.pb, stream);
+  for (int64_t i = 0; i < npanels && rc == LT_OK; ++i) {
+    const int64_t r0 = i * panel, rows = std::min(panel, M - r0);
+    cudaEvent_t e_in = ev[2 * i], e_out = ev[2 * i + 1];
+    if (K > 0)
+      cuda(cudaMemcpyAsync(Ad + r0 * K, A + r0 * K, 8 * static_cast<size_t>(rows) * K, cudaMemcpyHostToDevice, h2d),
+           "copy A");
+    if (beta != 0.0)
+      cuda(cudaMemcpyAsync(Cd + r0 * N, C + r0 * N, 8 * static_cast<size_t>(rows) * N, cudaMemcpyHostToDevice, h2d),
+           "copy C0");
+    cuda(cudaEventRecord(e_in, h2d), "record");
+    cuda(cudaStreamWaitEvent(stream, e_in, 0), "wait");
+    if (rc != LT_OK) break;
+    if (K == 0) {
+      const int64_t blocks = std::min<int64_t>(ceil_div(rows * N, 256), 4 * ctx->sm_count);
+      k0_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(Cd + r0 * N, rows, N, N, alpha, beta);
+      cuda(cudaGetLastError(), "k0 kernel");
+    } else {
+      rc = ozaki::exponents_rows(Ad + r0 * K, rows, K, K, amax_a + r0, ctx->sm_count, stream);
+      if (rc == LT_OK) rc = split_rows(n, Ad + r0 * K, rows, K, L.Kp, amax_a + r0, ra + r0 * L.Kp, M * L.Kp, c.pa, stream);
+      if (rc != LT_OK) break;
+      ProductArgs a;
+      a.ra = ra + r0 * L.Kp;
+      a.a_plane = M * L.Kp;
+      a.rb = rb;
+      a.b_plane = N * L.Kp;
+      a.Kp = L.Kp;
+      a.res = ws + L.off_rc + r0 * L.Np;
+      a.res_plane = L.Mp * L.Np;
+      a.Np = L.Np;
+      a.C = Cd + r0 * N;
+      a.M = rows;
+      a.N = N;
+      a.ldc = N;
+      a.K = K;
+      a.amax_a = amax_a + r0;
+      a.amax_b = amax_b;
+      a.alpha = alpha;
+      a.beta = beta;
+      a.n = n;
+      rc = run_product(a, ctx, stream, true, true);
+      if (rc != LT_OK) break;
+    }
+    cuda(cudaEventRecord(e_out, stream), "record");
+    cuda(cudaStreamWaitEvent(d2h, e_out, 0), "wait");
+    cuda(cudaMemcpyAsync(C + r0 * N, Cd + r0 * N, 8 * static_cast<size_t>(rows) * N, cudaMemcpyDeviceToHost, d2h),
+         "copy C");
+  }
+  // The caller's stream is ordered after the last copy back; the call returns with C in host memory.
+  if (rc == LT_OK) cuda(cudaEventRecord(e_start, d2h), "record");
+  if (rc == LT_OK) cuda(cudaStreamWaitEvent(stream, e_start, 0), "wait");
+  if (d2h != nullptr) cuda(cudaStreamSynchronize(d2h), "sync");
+  if (h2d != nullptr) cuda(cudaStreamSynchronize(h2d), "sync");
+  cuda(cudaStreamSynchronize(stream), "sync");
+  for (auto& e : ev)
+    if (e != nullptr) cudaEventDestroy(e);
+  if (h2d != nullptr) cudaStreamDestroy(h2d);
+  if (d2h != nullptr) cudaStreamDestroy(d2h);
+  return rc;
 }
 
 size_t workspace_size(int64_t M, int64_t N, int64_t K, int n) { return layout_for(M, N, K, n).total; }
@@ -961,6 +1152,35 @@ int lt_ozaki_crt_product(double* C, int64_t M, int64_t N, int64_t K, double alph
   LT_TRY(check_ws(M, N, K, moduli, workspace, workspace_bytes));
   if (M == 0 || N == 0) return lt::ok();
   LT_TRY(lt::crt::product(C, M, N, K, alpha, beta, moduli, workspace, workspace_bytes, lt::as_stream(stream)));
+  return lt::ok();
+}
+
+int lt_ozaki_crt_multiply(int64_t M, int64_t N, int64_t K, int moduli, void* workspace, size_t workspace_bytes,
+                          void* stream) {
+  LT_TRY(check_args(reinterpret_cast<const double*>(8), reinterpret_cast<const double*>(8),
+                    reinterpret_cast<const double*>(8), M, N, K, moduli));
+  LT_TRY(check_ws(M, N, K, moduli, workspace, workspace_bytes));
+  if (M == 0 || N == 0) return lt::ok();
+  LT_TRY(lt::crt::product(nullptr, M, N, K, 1.0, 0.0, moduli, workspace, workspace_bytes, lt::as_stream(stream), true,
+                          false));
+  return lt::ok();
+}
+
+int lt_ozaki_crt_reconstruct(double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int moduli,
+                             const void* workspace, size_t workspace_bytes, void* stream) {
+  LT_TRY(check_args(reinterpret_cast<const double*>(8), reinterpret_cast<const double*>(8), C, M, N, K, moduli));
+  LT_TRY(check_ws(M, N, K, moduli, workspace, workspace_bytes));
+  if (M == 0 || N == 0) return lt::ok();
+  LT_TRY(lt::crt::product(C, M, N, K, alpha, beta, moduli, workspace, workspace_bytes, lt::as_stream(stream), false,
+                          true));
+  return lt::ok();
+}
+
+int lt_dgemm_ozaki_crt_host(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
+                            double alpha, double beta, int moduli, void* stream) {
+  LT_TRY(check_args(A, B, C, M, N, K, moduli));
+  if (M == 0 || N == 0) return lt::ok();
+  LT_TRY(lt::crt::host_run(A, B, C, M, N, K, alpha, beta, moduli, lt::as_stream(stream)));
   return lt::ok();
 }
 

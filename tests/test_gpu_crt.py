@@ -97,10 +97,14 @@ def test_crt_entry_points_agree(cuda, oracle_mod):
     lt.ozaki_crt_product(c2, M, N, K, 1.5, 0.5, n, ws)
     c3 = to_dev(torch, C0)
     ms = lt.dgemm("ozaki_crt15", dA, dB, c3, M, N, K, 1.5, 0.5)
+    c4 = to_dev(torch, C0)
+    lt.ozaki_crt_split(dA, dB, M, N, K, n, ws)
+    lt.ozaki_crt_multiply(M, N, K, n, ws)
+    lt.ozaki_crt_reconstruct(c4, M, N, K, 1.5, 0.5, n, ws)
     torch.cuda.synchronize()
     lt.device_status()
     assert ms > 0.0
-    for c in (c1, c2, c3):
+    for c in (c1, c2, c3, c4):
         assert np.array_equal(c.cpu().numpy(), ref)
 
 
@@ -131,3 +135,21 @@ def test_crt_accuracy_at_2048_against_native_fp64(cuda):
     lt.device_status()
     assert ecrt <= e64, (ecrt, e64)
     assert ecrt < 1e-16
+
+
+def test_crt_host_resident_path(cuda, oracle_mod):
+    """lt_dgemm_ozaki_crt_host on pinned host buffers (row panels of A pipelined through the GPU) is
+    bit-identical to the device-resident call, with several panels, ragged edges and K = 0."""
+    import libthom_b200 as lt
+
+    torch = cuda
+    for (M, N, K) in [(1100, 300, 257), (70, 90, 0)]:
+        A, B, C0 = oracle_mod.make_problem(M, N, max(K, 1), phi=3, seed=M)
+        A, B = A[:, :K].copy(), B[:K, :].copy()
+        ref = run_crt(torch, A, B, C0, 1.5, 0.5, 15) if K > 0 else 0.5 * C0
+        Ah = torch.from_numpy(A).pin_memory()
+        Bh = torch.from_numpy(B).pin_memory()
+        Ch = torch.from_numpy(C0.copy()).pin_memory()
+        lt.dgemm_ozaki_crt_host(Ah.data_ptr(), Bh.data_ptr(), Ch.data_ptr(), M, N, K, 1.5, 0.5, 15)
+        lt.device_status()
+        assert np.array_equal(Ch.numpy(), ref)
