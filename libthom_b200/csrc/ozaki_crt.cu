@@ -58,20 +58,32 @@ constexpr int kMinMod = LT_OZAKI_CRT_MIN_MODULI;
 constexpr int kModuli[kMaxMod] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
                                   223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
 constexpr int kBM = 128;                          // rows of C per CTA (256 per pair)
-constexpr int kBN = 256;                          // columns of C per pair tile (N of one pair MMA)
+constexpr int kBN = 256;                          // N of one pair MMA (columns of C)
 constexpr int kBK = 128;                          // K bytes per stage (one 128-byte swizzle row)
 constexpr int kMmaK = 32;                         // K of one kind::i8 MMA
 constexpr int kABytes = kBM * kBK;                // 16 KB
-constexpr int kBBytes = (kBN / 2) * kBK;          // 16 KB: this CTA's 128 rows of the tile's B
-constexpr int kStageBytes = kABytes + kBBytes;
+constexpr int kBHalfBytes = (kBN / 2) * kBK;      // 16 KB: this CTA's 128 rows of one MMA's B
 constexpr int kMaxSmem = 232448;
 constexpr int kOverhead = 1024 + 512;
-constexpr int kStages = std::min(8, (kMaxSmem - kOverhead) / kStageBytes);
-constexpr int kSmem = kStages * kStageBytes + kOverhead;
 constexpr int kDrainWarps = 8;                    // two per TMEM lane quarter, each half the columns
 constexpr int kThreads = 64 + 32 * kDrainWarps;
 constexpr int kGroupSteps = 1023;                 // K steps per INT32 accumulation: 1023*128*128^2 < 2^31
-static_assert(kStages >= 3, "shared-memory ring too small");
+constexpr int kPadN = 512;                        // residue planes of C: columns rounded up to this
+
+// Pair tile of 256 x BN: BN = 256, one pair MMA per K step and two TMEM accumulators (the drain of one
+// modulus overlaps the products of the next); BN = 512, two pair MMAs per K step sharing the A stage
+// (a quarter less operand data per product from L2 into shared memory) into one 512-column
+// accumulator, so each modulus's products wait for the drain of the previous one.
+template <int BN>
+struct Tile {
+  static constexpr int kMmas = BN / kBN;
+  static constexpr int kStageBytes = kABytes + kMmas * kBHalfBytes;
+  static constexpr int kStages = std::min(8, (kMaxSmem - kOverhead) / kStageBytes);
+  static constexpr int kSmem = kStages * kStageBytes + kOverhead;
+  static constexpr int kAccBufs = BN == kBN ? 2 : 1;
+  static_assert(kStages >= 3, "shared-memory ring too small");
+  static_assert(kAccBufs * BN == 512, "TMEM holds 512 INT32 columns");
+};
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 inline int64_t ceil_div(int64_t x, int64_t m) { return (x + m - 1) / m; }
@@ -82,10 +94,10 @@ inline int64_t ceil_div(int64_t x, int64_t m) { return (x + m - 1) / m; }
 struct Consts {
   int n, nl, w, pa, pb;
   int32_t m[kMaxMod];
-  int32_t h[kMaxMod];             // (m - 1) / 2: symmetric residue = residue of V + h in [0, m), minus h
+  int32_t h[kMaxMod];             // (m - 1) / 2: the symmetric residues lie in [-h, h]
   // residues of the scaled inputs: x = dp4a(bytes of V + 2^62, coef) + add, x mod m by umulhi
   uint32_t coef_lo[kMaxMod], coef_hi[kMaxMod];  // bytes (2^(8d) mod m), d = 0..3 and 4..7
-  uint32_t add[kMaxMod];                        // m - (2^62 mod m) + h
+  uint32_t add[kMaxMod];                        // m - (2^62 mod m)
   uint32_t split_magic[kMaxMod];                // ceil(2^32 / m)
   // INT32 accumulators -> residues: y = (acc >> 16) c16 + (acc & 0xffff) + bias, q = umulhi(y, magic) >> 7
   int32_t c16[kMaxMod];           // 2^16 mod m
@@ -171,7 +183,7 @@ Consts make_consts(int n, int64_t K) {
     }
     c.coef_lo[l] = lo;
     c.coef_hi[l] = hi;
-    c.add[l] = m - pow2_mod(62, m) + (m - 1) / 2;
+    c.add[l] = m - pow2_mod(62, m);
     c.split_magic[l] = static_cast<uint32_t>(((uint64_t(1) << 32) + m - 1) / m);
     c.c16[l] = static_cast<int32_t>(pow2_mod(16, m));
     c.bias[l] = static_cast<int32_t>(m * (((uint32_t(1) << 23) + m - 1) / m));
@@ -224,23 +236,26 @@ int ensure_table(int device) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Workspace: [amaxA: M u64][amaxB: N u64][A residues n x M x Kp][B residues n x N x Kp]
+// Workspace: [amaxA: M u64][amaxB: N u64][row exponents: M int][column exponents: N int]
+//            [A residues n x M x Kp][B residues n x N x Kp]
 //            [C residue planes n x Mp x Np], 256-aligned; Mp, Np = M, N rounded up to the 256 x 256
 //            pair tile (the product writes whole tiles).
 // ---------------------------------------------------------------------------------------------
 struct Layout {
   int64_t Kp, Mp, Np;
-  size_t off_amax_a, off_amax_b, off_ra, off_rb, off_rc, total;
+  size_t off_amax_a, off_amax_b, off_ea, off_eb, off_ra, off_rb, off_rc, total;
 };
 
 Layout layout_for(int64_t M, int64_t N, int64_t K, int n) {
   Layout L;
   L.Kp = round_up(std::max<int64_t>(K, 1), kBK);
   L.Mp = round_up(std::max<int64_t>(M, 1), 2 * kBM);
-  L.Np = round_up(std::max<int64_t>(N, 1), kBN);
+  L.Np = round_up(std::max<int64_t>(N, 1), kPadN);
   size_t o = 0;
   L.off_amax_a = o; o += round_up(8 * M, 256);
   L.off_amax_b = o; o += round_up(8 * N, 256);
+  L.off_ea = o;     o += round_up(4 * M, 256);
+  L.off_eb = o;     o += round_up(4 * N, 256);
   L.off_ra = o;     o += round_up(static_cast<int64_t>(n) * M * L.Kp, 256);
   L.off_rb = o;     o += round_up(static_cast<int64_t>(n) * N * L.Kp, 256);
   L.off_rc = o;     o += static_cast<size_t>(n) * L.Mp * L.Np;
@@ -251,31 +266,11 @@ Layout layout_for(int64_t M, int64_t N, int64_t K, int n) {
 // ---------------------------------------------------------------------------------------------
 // Residues of the scaled operands
 // ---------------------------------------------------------------------------------------------
-// trunc(a 2^(p - e)) from the IEEE fields: |a| = m 2^t, so the result is +-(m 2^(t - e + p)) truncated
-// toward zero, below 2^p <= 2^62 because |a| < 2^e. Zero for a zero, NaN or Inf entry.
-__device__ __forceinline__ long long scaled_int(double a, int e, int p) {
-  const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(a));
-  const unsigned long long mag = bits & 0x7fffffffffffffffull;
-  const int E = static_cast<int>(mag >> 52);
-  if (mag == 0ull || E == 0x7ff) return 0;
-  unsigned long long m = mag & 0x000fffffffffffffull;
-  int t;
-  if (E == 0) {
-    t = -1074;
-  } else {
-    m |= 0x0010000000000000ull;
-    t = E - 1075;
-  }
-  const int sh = t - e + p;
-  const unsigned long long X = sh >= 0 ? (m << sh) : (-sh >= 64 ? 0ull : (m >> (-sh)));
-  return (bits >> 63) ? -static_cast<long long>(X) : static_cast<long long>(X);
-}
-
 // Four values' symmetric residues modulo modulus L as one word of two's-complement bytes, from
 // U = V + 2^62 given as two words per value. Modulus 256 (L = 0): the low byte of V. Otherwise
-// x = sum_d byte_d(U) (2^(8d) mod m) + m - (2^62 mod m) + h is congruent to V + h and below 2^19, so
-// floor(x / m) = umulhi(x, ceil(2^32 / m)) exactly and r = x mod m = (V + h) mod m; the bytes r - h,
-// subtracted four at a time, are the residues in [-h, h].
+// raw = sum_d byte_d(U) (2^(8d) mod m) + m - (2^62 mod m) is congruent to V and below 2^19, so
+// q = floor((raw + h) / m) = umulhi(raw + h, ceil(2^32 / m)) exactly and raw - q m, in [-h, h], is the
+// symmetric residue; PRMT packs the low bytes of four of them.
 template <int L>
 __device__ __forceinline__ uint32_t residue_word(const uint32_t* ulo, const uint32_t* uhi, const Consts& c) {
   if constexpr (L == 0) {
@@ -284,11 +279,11 @@ __device__ __forceinline__ uint32_t residue_word(const uint32_t* ulo, const uint
     uint32_t r[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const uint32_t x = __dp4a(ulo[i], c.coef_lo[L], __dp4a(uhi[i], c.coef_hi[L], c.add[L]));
-      r[i] = x - __umulhi(x, c.split_magic[L]) * static_cast<uint32_t>(c.m[L]);
+      const uint32_t raw = __dp4a(ulo[i], c.coef_lo[L], __dp4a(uhi[i], c.coef_hi[L], c.add[L]));
+      const uint32_t q = __umulhi(raw + static_cast<uint32_t>(c.h[L]), c.split_magic[L]);
+      r[i] = raw - q * static_cast<uint32_t>(c.m[L]);
     }
-    const uint32_t packed = r[0] | (r[1] << 8) | (r[2] << 16) | (r[3] << 24);
-    return __vsub4(packed, static_cast<uint32_t>(c.h[L]) * 0x01010101u);
+    return __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
   }
 }
 
@@ -303,15 +298,31 @@ __device__ __forceinline__ void residues16(const uint32_t (&ulo)[16], const uint
   }
 }
 
+// V = trunc(a 2^(p - e)) of 16 finite entries of a row (column) whose largest magnitude is below 2^e:
+// the product by 2^(p - e) is exact whenever it is at least 1 in magnitude (a power-of-two scaling to
+// a normal number) and anything smaller truncates to 0, so one multiplication (two when 2^(p - e) is
+// above the double range) and a truncating conversion give V exactly, below 2^p <= 2^62. A row
+// (column) holding NaN or Inf (e = kSentinel) gets V = 0. Then the residues of each V.
 template <int NM>
 __device__ __forceinline__ void residues_of(const double (&v)[16], int e, int p, const Consts& c, uint4 (&out)[NM]) {
   uint32_t ulo[16], uhi[16];
+  if (e == kSentinel) {
 #pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    const unsigned long long U =
-        (e == kSentinel) ? (1ull << 62) : static_cast<unsigned long long>(scaled_int(v[i], e, p) + (1ll << 62));
-    ulo[i] = static_cast<uint32_t>(U);
-    uhi[i] = static_cast<uint32_t>(U >> 32);
+    for (int i = 0; i < 16; ++i) {
+      ulo[i] = 0u;
+      uhi[i] = 1u << 30;
+    }
+  } else {
+    const int d = p - e, d1 = d < 1023 ? d : 1023;
+    const double s1 = pow2i(d1), s2 = pow2i(d - d1);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      double x = __dmul_rn(v[i], s1);
+      if (d > 1023) x = __dmul_rn(x, s2);
+      const unsigned long long U = static_cast<unsigned long long>(__double2ll_rz(x) + (1ll << 62));
+      ulo[i] = static_cast<uint32_t>(U);
+      uhi[i] = static_cast<uint32_t>(U >> 32);
+    }
   }
   residues16<NM, 0>(ulo, uhi, c, out);
 }
@@ -322,13 +333,15 @@ template <int NM>
 __global__ void __launch_bounds__(256) crt_split_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K,
                                                              int64_t lda, int64_t Kp,
                                                              const unsigned long long* __restrict__ amax,
-                                                             int8_t* __restrict__ out, int64_t plane, int pa) {
+                                                             int8_t* __restrict__ out, int64_t plane, int pa,
+                                                             int* __restrict__ exps) {
   const Consts& c = c_table[NM - kMinMod];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t row = static_cast<int64_t>(blockIdx.x) * 8 + warp;
   const int64_t k0 = static_cast<int64_t>(blockIdx.y) * 512 + lane * 16;
   if (row >= M || k0 >= Kp) return;
   const int e = exponent_of_maxbits(amax[row]);
+  if (blockIdx.y == 0 && lane == 0) exps[row] = e;  // the row's exponent, for the reconstruction
   const double* a = A + row * lda + k0;
   double v[16];
   if (k0 + 16 <= K && (reinterpret_cast<uintptr_t>(a) & 15) == 0) {
@@ -359,7 +372,8 @@ template <int NM>
 __global__ void __launch_bounds__(256) crt_split_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N,
                                                              int64_t ldb, int64_t Kp,
                                                              const unsigned long long* __restrict__ amax,
-                                                             int8_t* __restrict__ out, int64_t plane, int pb) {
+                                                             int8_t* __restrict__ out, int64_t plane, int pb,
+                                                             int* __restrict__ exps) {
   __shared__ __align__(16) uint8_t stage[kColPlanes][32 * kColPitch];
   const Consts& c = c_table[NM - kMinMod];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -368,6 +382,7 @@ __global__ void __launch_bounds__(256) crt_split_cols_kernel(const double* __res
   const int64_t col = col0 + lane;
   const int64_t k0 = kb + warp * 16;
   const int e = col < N ? exponent_of_maxbits(amax[col]) : 0;
+  if (blockIdx.y == 0 && warp == 0 && col < N) exps[col] = e;  // the column's exponent, for the reconstruction
   double v[16];
   const double* b = B + k0 * ldb + col;
   if (col < N && k0 + 16 <= K) {
@@ -409,6 +424,7 @@ struct Problem {
   int ksteps;           // Kp / 128
   int kgroups;          // ceil(ksteps / kGroupSteps)
   int group;            // pair-rows per raster group
+  int bn;               // tile width (256 or 512)
 };
 
 __device__ __forceinline__ void tile_coords(const Problem& p, int64_t t, int* m0, int* n0) {
@@ -417,7 +433,7 @@ __device__ __forceinline__ void tile_coords(const Problem& p, int64_t t, int* m0
   const int64_t gsize = (p.tiles_m - first_m) < G ? (p.tiles_m - first_m) : G;
   const int64_t in_group = t - group * G * p.tiles_n;
   *m0 = static_cast<int>((first_m + in_group % gsize) * 2 * kBM);
-  *n0 = static_cast<int>((in_group / gsize) * kBN);
+  *n0 = static_cast<int>((in_group / gsize) * p.bn);
 }
 
 // Symmetric residue of an INT32 accumulator modulo c.m[l] (an odd modulus), from
@@ -468,10 +484,12 @@ __device__ __forceinline__ void drain_chunk(const uint32_t (&v)[32], int l, bool
   dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
 }
 
-template <int NM>
+template <int NM, int BN>
 __global__ void __launch_bounds__(kThreads, 1)
     crt_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Problem p,
                     DeviceStatus* status) {
+  using T = Tile<BN>;
+  constexpr int kStages = T::kStages, kStageBytes = T::kStageBytes;
   const Consts& c = c_table[NM - kMinMod];
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -507,7 +525,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     tma_prefetch_desc(&tmB);
   }
   if (warp == 1) {
-    tmem_alloc_pair(tmem_slot, 2 * kBN);
+    tmem_alloc_pair(tmem_slot, 512);
     tmem_relinquish_pair();
   }
   tc_fence_before();
@@ -533,7 +551,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             uint8_t* st = smem + stage * kStageBytes;
             mbar_arrive_expect_tx(&full[stage], kStageBytes);
             tma_load_3d(st, &tmA, &full[stage], ks * kBK, arow, l);
-            tma_load_3d(st + kABytes, &tmB, &full[stage], ks * kBK, brow, l);
+#pragma unroll
+            for (int h = 0; h < T::kMmas; ++h)
+              tma_load_3d(st + kABytes + h * kBHalfBytes, &tmB, &full[stage], ks * kBK, brow + h * kBN, l);
             if (++stage == kStages) { stage = 0; phase ^= 1; }
           }
         }
@@ -571,7 +591,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int64_t t = first; t < tiles && ok; t += stride) {
       for (int l = 0; l < NM && ok; ++l) {
         for (int g = 0; g < kgroups && ok; ++g, ++pass) {
-          const uint32_t buf = pass & 1, use = pass >> 1;
+          const uint32_t buf = pass % T::kAccBufs, use = pass / T::kAccBufs;
           if (!__all_sync(0xffffffffu, mbar_wait_cluster(&acc_empty[buf], (use & 1) ^ 1, abort_flag, status, 83))) {
             ok = false;
             break;
@@ -590,7 +610,10 @@ __global__ void __launch_bounds__(kThreads, 1)
               const uint64_t b0 = b_desc0 + static_cast<uint64_t>(stage) * kStageStep;
 #pragma unroll
               for (int k = 0; k < kBK / kMmaK; ++k)
-                mma_i8_pair(d_tmem, a0 + k * kStepK, b0 + k * kStepK, idesc, (ks > ks0 || k > 0) ? 1u : 0u);
+#pragma unroll
+                for (int h = 0; h < T::kMmas; ++h)
+                  mma_i8_pair(d_tmem + h * kBN, a0 + k * kStepK, b0 + h * (kBHalfBytes >> 4) + k * kStepK, idesc,
+                              (ks > ks0 || k > 0) ? 1u : 0u);
               mma_commit_pair(cluster_addr(&empty[stage], 0));
               mma_commit_pair(cluster_addr(&empty[stage], 1));
             }
@@ -617,7 +640,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else {
     // ------------------------ drain: accumulators -> residue planes of C ------------------------
     const int quarter = warp & 3;             // TMEM lanes 32*quarter .. +31 (rows of this CTA's block)
-    const int colhalf = (warp - 2) >> 2;      // columns 128*colhalf .. +127 of the tile
+    const int colhalf = (warp - 2) >> 2;      // columns colhalf*BN/2 .. +BN/2-1 of the tile
     const uint32_t acc_empty_r0[2] = {cluster_addr(&acc_empty[0], 0), cluster_addr(&acc_empty[1], 0)};
     uint32_t pass = 0;
     bool ok = true;
@@ -625,21 +648,21 @@ __global__ void __launch_bounds__(kThreads, 1)
       int m0, n0;
       tile_coords(p, t, &m0, &n0);
       const int64_t row = static_cast<int64_t>(m0) + static_cast<int64_t>(rank) * kBM + quarter * 32 + lane;
-      uint8_t* row_base = p.res + row * p.Np + n0 + colhalf * (kBN / 2);
+      uint8_t* row_base = p.res + row * p.Np + n0 + colhalf * (BN / 2);
       for (int l = 0; l < NM && ok; ++l) {
         uint8_t* dst = row_base + static_cast<int64_t>(l) * p.plane;
         for (int g = 0; g < kgroups; ++g, ++pass) {
-          const uint32_t buf = pass & 1, use = pass >> 1;
+          const uint32_t buf = pass % T::kAccBufs, use = pass / T::kAccBufs;
           if (!mbar_wait_cluster(&acc_full[buf], use & 1, abort_flag, status, 86)) { ok = false; break; }
           tc_fence_after();
           const uint32_t lane_base =
-              tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + buf * kBN + colhalf * (kBN / 2);
+              tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + buf * kBN + colhalf * (BN / 2);
 #pragma unroll 1
-          for (int ch = 0; ch < kBN / 64; ++ch) {
+          for (int ch = 0; ch < BN / 64; ++ch) {
             uint32_t v[32];
             tmem_ld_32x32b_x32(lane_base + static_cast<uint32_t>(ch * 32), v);
             tmem_ld_wait();
-            if (ch == kBN / 64 - 1) {
+            if (ch == BN / 64 - 1) {
               // The whole accumulator is in registers: hand the buffer back before the last stores.
               tc_fence_before();
               __syncwarp();
@@ -657,7 +680,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   cluster_sync();  // rank 0's MMAs read rank 1's shared memory and write its TMEM until here
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc_pair(tmem_base, 2 * kBN);
+    tmem_dealloc_pair(tmem_base, 512);
   }
 }
 
@@ -691,9 +714,8 @@ __device__ __forceinline__ double reconstruct(const uint32_t (&w)[NM], int e, co
 template <int NM>
 __global__ void __launch_bounds__(256) crt_recon_kernel(const uint8_t* __restrict__ res, int64_t plane, int64_t Np,
                                                         double* __restrict__ C, int64_t M, int64_t N, int64_t ldc,
-                                                        const unsigned long long* __restrict__ amax_a,
-                                                        const unsigned long long* __restrict__ amax_b, double alpha,
-                                                        double beta, int pa, int pb) {
+                                                        const int* __restrict__ ea, const int* __restrict__ eb,
+                                                        double alpha, double beta, int pa, int pb) {
   constexpr int NL = limbs_for(NM);
   const Consts& c = c_table[NM - kMinMod];
   const int64_t nq = (N + 3) / 4, total = M * nq;
@@ -718,15 +740,30 @@ __global__ void __launch_bounds__(256) crt_recon_kernel(const uint8_t* __restric
           if (j0 + e < N) c0[e] = crow[j0 + e];
       }
     }
-    const int sig = exponent_of_maxbits(amax_a[i]);
+    const int sig = ea[i];
+    int tau[4];
+    if (j0 + 4 <= N) {
+      const int4 t4 = *reinterpret_cast<const int4*>(eb + j0);
+      tau[0] = t4.x; tau[1] = t4.y; tau[2] = t4.z; tau[3] = t4.w;
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) tau[e] = j0 + e < N ? eb[j0 + e] : 0;
+    }
+    // C' 2^(sigma - pa) 2^(tau - pb): with both factors in the double range this is two exact-factor
+    // multiplications, which is what scale_pow2 does there; scale_pow2 takes the rest
+    const int es = sig - pa;
+    const bool row_fast = sig != kSentinel && es >= -1022 && es <= 1023;
+    const double rs = pow2i(row_fast ? es : 0);
     double out[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
-      const int tau = j0 + e < N ? exponent_of_maxbits(amax_b[j0 + e]) : 0;
-      if (sig == kSentinel || tau == kSentinel) {
+      if (sig == kSentinel || tau[e] == kSentinel) {
         out[e] = __longlong_as_double(0x7ff8000000000000ll);
       } else {
-        const double tv = scale_pow2(scale_pow2(reconstruct<NM, NL>(w, e, c), sig - pa), tau - pb);
+        const double t = reconstruct<NM, NL>(w, e, c);
+        const int et = tau[e] - pb;
+        const double tv = (row_fast && et >= -1022 && et <= 1023) ? __dmul_rn(__dmul_rn(t, rs), pow2i(et))
+                                                                   : scale_pow2(scale_pow2(t, es), et);
         out[e] = (beta != 0.0) ? fma(alpha, tv, __dmul_rn(beta, c0[e])) : __dmul_rn(alpha, tv);
       }
     }
@@ -754,6 +791,18 @@ __global__ void k0_kernel(double* C, int64_t M, int64_t N, int64_t ldc, double a
 // ---------------------------------------------------------------------------------------------
 // Host driver
 // ---------------------------------------------------------------------------------------------
+// Tile width of the product: 512 (less operand traffic per product) unless N fits one 256-wide tile,
+// or LIBTHOM_CRT_TILE = 256 / 512.
+int tile_width(int64_t N) {
+  static const int forced = [] {
+    const char* e = getenv("LIBTHOM_CRT_TILE");
+    const int v = e != nullptr ? atoi(e) : 0;
+    return (v == 256 || v == 512) ? v : 0;
+  }();
+  if (forced != 0) return forced;
+  return N > kBN ? 512 : 256;
+}
+
 int raster_group() {
   static const int g = [] {
     const char* e = getenv("LIBTHOM_CRT_GROUP");
@@ -767,18 +816,18 @@ int raster_group() {
 // columns of B (row stride N) into `rb`, for NM moduli.
 template <int NM>
 int split_rows_n(const double* A, int64_t M, int64_t K, int64_t Kp, const unsigned long long* amax, int8_t* ra,
-                 int64_t plane, int pa, cudaStream_t stream) {
+                 int64_t plane, int pa, int* exps, cudaStream_t stream) {
   const dim3 grid(static_cast<unsigned>(ceil_div(M, 8)), static_cast<unsigned>(ceil_div(Kp, 512)));
-  crt_split_rows_kernel<NM><<<grid, 256, 0, stream>>>(A, M, K, K, Kp, amax, ra, plane, pa);
+  crt_split_rows_kernel<NM><<<grid, 256, 0, stream>>>(A, M, K, K, Kp, amax, ra, plane, pa, exps);
   LT_CUDA_TRY(cudaGetLastError());
   return LT_OK;
 }
 
 template <int NM>
 int split_cols_n(const double* B, int64_t K, int64_t N, int64_t Kp, const unsigned long long* amax, int8_t* rb,
-                 int64_t plane, int pb, cudaStream_t stream) {
+                 int64_t plane, int pb, int* exps, cudaStream_t stream) {
   const dim3 grid(static_cast<unsigned>(ceil_div(N, 32)), static_cast<unsigned>(Kp / kBK));
-  crt_split_cols_kernel<NM><<<grid, 256, 0, stream>>>(B, K, N, N, Kp, amax, rb, plane, pb);
+  crt_split_cols_kernel<NM><<<grid, 256, 0, stream>>>(B, K, N, N, Kp, amax, rb, plane, pb, exps);
   LT_CUDA_TRY(cudaGetLastError());
   return LT_OK;
 }
@@ -793,15 +842,15 @@ int split_cols_n(const double* B, int64_t K, int64_t N, int64_t Kp, const unsign
   }
 
 int split_rows(int n, const double* A, int64_t M, int64_t K, int64_t Kp, const unsigned long long* amax, int8_t* ra,
-               int64_t plane, int pa, cudaStream_t stream) {
-#define LT_CALL(NM) split_rows_n<NM>(A, M, K, Kp, amax, ra, plane, pa, stream)
+               int64_t plane, int pa, int* exps, cudaStream_t stream) {
+#define LT_CALL(NM) split_rows_n<NM>(A, M, K, Kp, amax, ra, plane, pa, exps, stream)
   LT_CRT_DISPATCH(n, LT_CALL)
 #undef LT_CALL
 }
 
 int split_cols(int n, const double* B, int64_t K, int64_t N, int64_t Kp, const unsigned long long* amax, int8_t* rb,
-               int64_t plane, int pb, cudaStream_t stream) {
-#define LT_CALL(NM) split_cols_n<NM>(B, K, N, Kp, amax, rb, plane, pb, stream)
+               int64_t plane, int pb, int* exps, cudaStream_t stream) {
+#define LT_CALL(NM) split_cols_n<NM>(B, K, N, Kp, amax, rb, plane, pb, exps, stream)
   LT_CRT_DISPATCH(n, LT_CALL)
 #undef LT_CALL
 }
@@ -822,8 +871,10 @@ int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int
   const Consts c = make_consts(n, K);
   auto* ra = reinterpret_cast<int8_t*>(ws + L.off_ra);
   auto* rb = reinterpret_cast<int8_t*>(ws + L.off_rb);
-  LT_TRY(split_rows(n, A, M, K, L.Kp, amax_a, ra, M * L.Kp, c.pa, stream));
-  return split_cols(n, B, K, N, L.Kp, amax_b, rb, N * L.Kp, c.pb, stream);
+  auto* ea = reinterpret_cast<int*>(ws + L.off_ea);
+  auto* eb = reinterpret_cast<int*>(ws + L.off_eb);
+  LT_TRY(split_rows(n, A, M, K, L.Kp, amax_a, ra, M * L.Kp, c.pa, ea, stream));
+  return split_cols(n, B, K, N, L.Kp, amax_b, rb, N * L.Kp, c.pb, eb, stream);
 }
 
 // One product stage over rows 0..M-1 of residue planes `ra` (plane stride a_plane) against all N
@@ -839,16 +890,16 @@ struct ProductArgs {
   int64_t res_plane, Np;
   double* C;
   int64_t M, N, ldc, K;
-  const unsigned long long* amax_a;
-  const unsigned long long* amax_b;
+  const int* ea;  // row exponents of A (sigma)
+  const int* eb;  // column exponents of B (tau)
   double alpha, beta;
   int n;
 };
 
-template <int NM>
+template <int NM, int BN>
 int launch_product_n(const CUtensorMap& tmA, const CUtensorMap& tmB, const Problem& p, const Consts& c, double* C,
-                     int64_t M, int64_t N, int64_t ldc, const unsigned long long* amax_a,
-                     const unsigned long long* amax_b, double alpha, double beta, DeviceContext* ctx,
+                     int64_t M, int64_t N, int64_t ldc, const int* ea, const int* eb, double alpha, double beta,
+                     DeviceContext* ctx,
                      cudaStream_t stream, bool do_multiply, bool do_reconstruct) {
   if (c.nl != limbs_for(NM)) return set_error(LT_ERR_UNSUPPORTED, "CRT limb count %d, kernel built for %d", c.nl, limbs_for(NM));
   static std::once_flag once[64];
@@ -858,7 +909,7 @@ int launch_product_n(const CUtensorMap& tmA, const CUtensorMap& tmB, const Probl
     *cfg = cudaLaunchConfig_t{};
     cfg->gridDim = dim3(grid);
     cfg->blockDim = dim3(kThreads);
-    cfg->dynamicSmemBytes = kSmem;
+    cfg->dynamicSmemBytes = Tile<BN>::kSmem;
     cfg->stream = stream;
     attr->id = cudaLaunchAttributeClusterDimension;
     attr->val.clusterDim.x = 2;
@@ -868,12 +919,13 @@ int launch_product_n(const CUtensorMap& tmA, const CUtensorMap& tmB, const Probl
     cfg->numAttrs = 1;
   };
   std::call_once(once[ctx->device], [&] {
-    attr_err[ctx->device] = cudaFuncSetAttribute(crt_pair_kernel<NM>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
+    attr_err[ctx->device] =
+        cudaFuncSetAttribute(crt_pair_kernel<NM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, Tile<BN>::kSmem);
     if (attr_err[ctx->device] != cudaSuccess) return;
     cudaLaunchConfig_t cfg;
     cudaLaunchAttribute attr;
     config(&cfg, &attr, static_cast<unsigned>(ctx->sm_count & ~1));
-    attr_err[ctx->device] = cudaOccupancyMaxActiveClusters(&max_clusters[ctx->device], crt_pair_kernel<NM>, &cfg);
+    attr_err[ctx->device] = cudaOccupancyMaxActiveClusters(&max_clusters[ctx->device], crt_pair_kernel<NM, BN>, &cfg);
   });
   LT_CUDA_TRY(attr_err[ctx->device]);
   const int64_t tiles = static_cast<int64_t>(p.tiles_m) * p.tiles_n;
@@ -882,12 +934,12 @@ int launch_product_n(const CUtensorMap& tmA, const CUtensorMap& tmB, const Probl
   cudaLaunchConfig_t cfg;
   cudaLaunchAttribute attr;
   config(&cfg, &attr, static_cast<unsigned>(2 * clusters));
-  if (do_multiply) LT_CUDA_TRY(cudaLaunchKernelEx(&cfg, crt_pair_kernel<NM>, tmA, tmB, p, ctx->status));
+  if (do_multiply) LT_CUDA_TRY(cudaLaunchKernelEx(&cfg, crt_pair_kernel<NM, BN>, tmA, tmB, p, ctx->status));
   if (do_reconstruct) {
     const int64_t work = M * ((N + 3) / 4);
     const int64_t blocks = std::min<int64_t>(ceil_div(work, 256), 8 * ctx->sm_count);
-    crt_recon_kernel<NM><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p.res, p.plane, p.Np, C, M, N, ldc,
-                                                                             amax_a, amax_b, alpha, beta, c.pa, c.pb);
+    crt_recon_kernel<NM><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p.res, p.plane, p.Np, C, M, N, ldc, ea,
+                                                                             eb, alpha, beta, c.pa, c.pb);
     LT_CUDA_TRY(cudaGetLastError());
   }
   return LT_OK;
@@ -905,14 +957,17 @@ int run_product(const ProductArgs& a, DeviceContext* ctx, cudaStream_t stream, b
   p.plane = a.res_plane;
   p.Np = a.Np;
   p.tiles_m = static_cast<int>(ceil_div(a.M, 2 * kBM));
-  p.tiles_n = static_cast<int>(ceil_div(a.N, kBN));
+  p.bn = tile_width(a.N);
+  p.tiles_n = static_cast<int>(ceil_div(a.N, p.bn));
   p.ksteps = static_cast<int>(a.Kp / kBK);
   p.kgroups = static_cast<int>(ceil_div(p.ksteps, kGroupSteps));
   p.group = raster_group();
   const Consts c = make_consts(a.n, a.K);
-#define LT_CALL(NM)                                                                                           \
-  launch_product_n<NM>(tmA, tmB, p, c, a.C, a.M, a.N, a.ldc, a.amax_a, a.amax_b, a.alpha, a.beta, ctx, stream, \
-                       do_multiply, do_reconstruct)
+#define LT_CALL(NM)                                                                                              \
+  (p.bn == 512 ? launch_product_n<NM, 512>(tmA, tmB, p, c, a.C, a.M, a.N, a.ldc, a.ea, a.eb, a.alpha, a.beta, ctx, \
+                                           stream, do_multiply, do_reconstruct)                                   \
+               : launch_product_n<NM, 256>(tmA, tmB, p, c, a.C, a.M, a.N, a.ldc, a.ea, a.eb, a.alpha, a.beta, ctx, \
+                                           stream, do_multiply, do_reconstruct))
   LT_CRT_DISPATCH(a.n, LT_CALL)
 #undef LT_CALL
 }
@@ -948,8 +1003,8 @@ int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double bet
   a.N = N;
   a.ldc = N;
   a.K = K;
-  a.amax_a = reinterpret_cast<const unsigned long long*>(ws + L.off_amax_a);
-  a.amax_b = reinterpret_cast<const unsigned long long*>(ws + L.off_amax_b);
+  a.ea = reinterpret_cast<const int*>(ws + L.off_ea);
+  a.eb = reinterpret_cast<const int*>(ws + L.off_eb);
   a.alpha = alpha;
   a.beta = beta;
   a.n = n;
@@ -1020,7 +1075,9 @@ int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, 
     cuda(cudaStreamWaitEvent(stream, e_b, 0), "wait");
   }
   if (rc == LT_OK && K > 0) rc = ozaki::exponents_cols(Bd, K, N, N, amax_b, ctx->sm_count, stream);
-  if (rc == LT_OK && K > 0) rc = split_cols(n, Bd, K, N, L.Kp, amax_b, rb, N * L.Kp, c.pb, stream);
+  auto* ea = reinterpret_cast<int*>(ws + L.off_ea);
+  auto* eb = reinterpret_cast<int*>(ws + L.off_eb);
+  if (rc == LT_OK && K > 0) rc = split_cols(n, Bd, K, N, L.Kp, amax_b, rb, N * L.Kp, c.pb, eb, stream);
   for (int64_t i = 0; i < npanels && rc == LT_OK; ++i) {
     const int64_t r0 = i * panel, rows = std::min(panel, M - r0);
     cudaEvent_t e_in = ev[2 * i], e_out = ev[2 * i + 1];
@@ -1039,7 +1096,8 @@ int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, 
       cuda(cudaGetLastError(), "k0 kernel");
     } else {
       rc = ozaki::exponents_rows(Ad + r0 * K, rows, K, K, amax_a + r0, ctx->sm_count, stream);
-      if (rc == LT_OK) rc = split_rows(n, Ad + r0 * K, rows, K, L.Kp, amax_a + r0, ra + r0 * L.Kp, M * L.Kp, c.pa, stream);
+      if (rc == LT_OK)
+        rc = split_rows(n, Ad + r0 * K, rows, K, L.Kp, amax_a + r0, ra + r0 * L.Kp, M * L.Kp, c.pa, ea + r0, stream);
       if (rc != LT_OK) break;
       ProductArgs a;
       a.ra = ra + r0 * L.Kp;
@@ -1055,8 +1113,8 @@ int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, 
       a.N = N;
       a.ldc = N;
       a.K = K;
-      a.amax_a = amax_a + r0;
-      a.amax_b = amax_b;
+      a.ea = ea + r0;
+      a.eb = eb;
       a.alpha = alpha;
       a.beta = beta;
       a.n = n;
