@@ -57,3 +57,11 @@ def fp64_bound(K: int) -> float:
     """Worst-case componentwise error of any FP64 dot-product order (with FMA) for length K,
     plus the alpha/beta epilogue roundings: (K + 4) u relative to |alpha||A||B| + |beta||C0|."""
     return (K + 4) * U
+
+
+def tight_fp64_bound(e_cublas: float) -> float:
+    """Statistical bar for the native FP64 kernels beside the worst case: for these inputs (random signs)
+    the componentwise error of an FP64 product does not grow with K, so the kernel's error may be at
+    most four times cuBLAS DGEMM's own on the same inputs, and at least 16 u where cuBLAS is nearly
+    exact (tiny K)."""
+    return max(4.0 * e_cublas, 16 * U)
