@@ -266,71 +266,63 @@ Layout layout_for(int64_t M, int64_t N, int64_t K, int n) {
 // ---------------------------------------------------------------------------------------------
 // Residues of the scaled operands
 // ---------------------------------------------------------------------------------------------
-// Four values' symmetric residues modulo modulus L as one word of two's-complement bytes, from
-// U = V + 2^62 given as two words per value. Modulus 256 (L = 0): the low byte of V. Otherwise
+// Four values' symmetric residues modulo modulus l as one word of two's-complement bytes, from
+// U = V + 2^62 given as two words per value. Modulus 256 (l = 0): the low byte of V. Otherwise
 // raw = sum_d byte_d(U) (2^(8d) mod m) + m - (2^62 mod m) is congruent to V and below 2^19, so
 // q = floor((raw + h) / m) = umulhi(raw + h, ceil(2^32 / m)) exactly and raw - q m, in [-h, h], is the
-// symmetric residue; PRMT packs the low bytes of four of them.
-template <int L>
-__device__ __forceinline__ uint32_t residue_word(const uint32_t* ulo, const uint32_t* uhi, const Consts& c) {
-  if constexpr (L == 0) {
+// symmetric residue; PRMT packs the low bytes of four of them. Called with a constant l (unrolled
+// loops), so the constants are read with fixed offsets.
+__device__ __forceinline__ uint32_t residue_word(int l, const uint32_t* ulo, const uint32_t* uhi, const Consts& c) {
+  if (l == 0)
     return __byte_perm(__byte_perm(ulo[0], ulo[1], 0x0040), __byte_perm(ulo[2], ulo[3], 0x0040), 0x5410);
-  } else {
-    uint32_t r[4];
+  uint32_t r[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const uint32_t raw = __dp4a(ulo[i], c.coef_lo[L], __dp4a(uhi[i], c.coef_hi[L], c.add[L]));
-      const uint32_t q = __umulhi(raw + static_cast<uint32_t>(c.h[L]), c.split_magic[L]);
-      r[i] = raw - q * static_cast<uint32_t>(c.m[L]);
-    }
-    return __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t raw = __dp4a(ulo[i], c.coef_lo[l], __dp4a(uhi[i], c.coef_hi[l], c.add[l]));
+    const uint32_t q = __umulhi(raw + static_cast<uint32_t>(c.h[l]), c.split_magic[l]);
+    r[i] = raw - q * static_cast<uint32_t>(c.m[l]);
   }
+  return __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
 }
 
-// Residues of 16 consecutive values (one thread's share) as one 16-byte word per modulus.
-template <int NM, int L>
-__device__ __forceinline__ void residues16(const uint32_t (&ulo)[16], const uint32_t (&uhi)[16], const Consts& c,
-                                           uint4 (&out)[NM]) {
-  if constexpr (L < NM) {
-    out[L] = make_uint4(residue_word<L>(ulo, uhi, c), residue_word<L>(ulo + 4, uhi + 4, c),
-                        residue_word<L>(ulo + 8, uhi + 8, c), residue_word<L>(ulo + 12, uhi + 12, c));
-    residues16<NM, L + 1>(ulo, uhi, c, out);
-  }
+// The 16 bytes of plane l for 16 consecutive values (one thread's share).
+__device__ __forceinline__ uint4 residue_plane(int l, const uint32_t (&ulo)[16], const uint32_t (&uhi)[16],
+                                               const Consts& c) {
+  return make_uint4(residue_word(l, ulo, uhi, c), residue_word(l, ulo + 4, uhi + 4, c),
+                    residue_word(l, ulo + 8, uhi + 8, c), residue_word(l, ulo + 12, uhi + 12, c));
 }
 
-// V = trunc(a 2^(p - e)) of 16 finite entries of a row (column) whose largest magnitude is below 2^e:
-// the product by 2^(p - e) is exact whenever it is at least 1 in magnitude (a power-of-two scaling to
-// a normal number) and anything smaller truncates to 0, so one multiplication (two when 2^(p - e) is
-// above the double range) and a truncating conversion give V exactly, below 2^p <= 2^62. A row
-// (column) holding NaN or Inf (e = kSentinel) gets V = 0. Then the residues of each V.
-template <int NM>
-__device__ __forceinline__ void residues_of(const double (&v)[16], int e, int p, const Consts& c, uint4 (&out)[NM]) {
-  uint32_t ulo[16], uhi[16];
+// V = trunc(a 2^(p - e)) of 16 finite entries of a row (column) whose largest magnitude is below 2^e,
+// as U = V + 2^62 in two words each: the product by 2^(p - e) is exact whenever it is at least 1 in
+// magnitude (a power-of-two scaling to a normal number) and anything smaller truncates to 0, so one
+// multiplication (two when 2^(p - e) is above the double range) and a truncating conversion give V
+// exactly, below 2^p <= 2^62. A row (column) holding NaN or Inf (e = kSentinel) gets V = 0.
+__device__ __forceinline__ void scaled_words(const double (&v)[16], int e, int p, uint32_t (&ulo)[16],
+                                             uint32_t (&uhi)[16]) {
   if (e == kSentinel) {
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       ulo[i] = 0u;
       uhi[i] = 1u << 30;
     }
-  } else {
-    const int d = p - e, d1 = d < 1023 ? d : 1023;
-    const double s1 = pow2i(d1), s2 = pow2i(d - d1);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      double x = __dmul_rn(v[i], s1);
-      if (d > 1023) x = __dmul_rn(x, s2);
-      const unsigned long long U = static_cast<unsigned long long>(__double2ll_rz(x) + (1ll << 62));
-      ulo[i] = static_cast<uint32_t>(U);
-      uhi[i] = static_cast<uint32_t>(U >> 32);
-    }
+    return;
   }
-  residues16<NM, 0>(ulo, uhi, c, out);
+  const int d = p - e, d1 = d < 1023 ? d : 1023;
+  const double s1 = pow2i(d1), s2 = pow2i(d - d1);
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    double x = __dmul_rn(v[i], s1);
+    if (d > 1023) x = __dmul_rn(x, s2);
+    const unsigned long long U = static_cast<unsigned long long>(__double2ll_rz(x) + (1ll << 62));
+    ulo[i] = static_cast<uint32_t>(U);
+    uhi[i] = static_cast<uint32_t>(U >> 32);
+  }
 }
 
 // Rows of A: a warp covers 512 K positions of one row (16 per lane), a block 8 rows (blockIdx.x:
 // row block, blockIdx.y: K segment). Each modulus plane receives 512 contiguous bytes per warp.
 template <int NM>
-__global__ void __launch_bounds__(256) crt_split_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K,
+__global__ void __launch_bounds__(256, 3) crt_split_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K,
                                                              int64_t lda, int64_t Kp,
                                                              const unsigned long long* __restrict__ amax,
                                                              int8_t* __restrict__ out, int64_t plane, int pa,
@@ -355,11 +347,11 @@ __global__ void __launch_bounds__(256) crt_split_rows_kernel(const double* __res
 #pragma unroll
     for (int j = 0; j < 16; ++j) v[j] = (k0 + j < K) ? __ldcs(a + j) : 0.0;
   }
-  uint4 r[NM];
-  residues_of<NM>(v, e, pa, c, r);
+  uint32_t ulo[16], uhi[16];
+  scaled_words(v, e, pa, ulo, uhi);
   int8_t* dst = out + row * Kp + k0;
 #pragma unroll
-  for (int l = 0; l < NM; ++l) *reinterpret_cast<uint4*>(dst + l * plane) = r[l];
+  for (int l = 0; l < NM; ++l) *reinterpret_cast<uint4*>(dst + l * plane) = residue_plane(l, ulo, uhi, c);
 }
 
 // Columns of B, transposed to K-major: a block covers 32 columns (one per lane) and 128 K positions
@@ -369,7 +361,7 @@ __global__ void __launch_bounds__(256) crt_split_rows_kernel(const double* __res
 constexpr int kColPitch = 144;  // bytes per column row in shared memory (128 + 16: no bank conflicts)
 constexpr int kColPlanes = 8;   // planes staged at a time (8 x 4.5 KB)
 template <int NM>
-__global__ void __launch_bounds__(256) crt_split_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N,
+__global__ void __launch_bounds__(256, 3) crt_split_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N,
                                                              int64_t ldb, int64_t Kp,
                                                              const unsigned long long* __restrict__ amax,
                                                              int8_t* __restrict__ out, int64_t plane, int pb,
@@ -392,8 +384,8 @@ __global__ void __launch_bounds__(256) crt_split_cols_kernel(const double* __res
 #pragma unroll
     for (int j = 0; j < 16; ++j) v[j] = (col < N && k0 + j < K) ? __ldcs(b + j * ldb) : 0.0;
   }
-  uint4 r[NM];
-  residues_of<NM>(v, e, pb, c, r);
+  uint32_t ulo[16], uhi[16];
+  scaled_words(v, e, pb, ulo, uhi);
   // thread t then writes 16 bytes of column t / 8 (K bytes 16 (t % 8) ..) of each staged plane
   const int cl = threadIdx.x >> 3, part = threadIdx.x & 7;
   const bool writes = col0 + cl < N;
@@ -403,7 +395,7 @@ __global__ void __launch_bounds__(256) crt_split_cols_kernel(const double* __res
     if (l0 > 0) __syncthreads();  // the previous group's reads are done
 #pragma unroll
     for (int l = l0; l < l0 + kColPlanes && l < NM; ++l)
-      *reinterpret_cast<uint4*>(&stage[l - l0][lane * kColPitch + warp * 16]) = r[l];
+      *reinterpret_cast<uint4*>(&stage[l - l0][lane * kColPitch + warp * 16]) = residue_plane(l, ulo, uhi, c);
     __syncthreads();
     if (writes) {
 #pragma unroll
@@ -791,16 +783,22 @@ __global__ void k0_kernel(double* C, int64_t M, int64_t N, int64_t ldc, double a
 // ---------------------------------------------------------------------------------------------
 // Host driver
 // ---------------------------------------------------------------------------------------------
-// Tile width of the product: 512 (less operand traffic per product) unless N fits one 256-wide tile,
-// or LIBTHOM_CRT_TILE = 256 / 512.
-int tile_width(int64_t N) {
+// Tile width of the product (LIBTHOM_CRT_TILE = 256 / 512 forces one): the smaller time of whole
+// waves of pair tiles over `clusters` CTA pairs, a 512-wide tile taking 0.92 of the time of two
+// 256-wide ones (measured at 8192^3: less operand traffic per product) but filling fewer pairs when the
+// problem has few tiles (2048 x 2048: 32 tiles of 512 against 64 of 256 for 74 pairs).
+int tile_width(int64_t M, int64_t N, int clusters) {
   static const int forced = [] {
     const char* e = getenv("LIBTHOM_CRT_TILE");
     const int v = e != nullptr ? atoi(e) : 0;
     return (v == 256 || v == 512) ? v : 0;
   }();
   if (forced != 0) return forced;
-  return N > kBN ? 512 : 256;
+  const int64_t tm = ceil_div(M, 2 * kBM);
+  auto cost = [&](int bn, double eff) {
+    return static_cast<double>(ceil_div(tm * ceil_div(N, bn), std::max(clusters, 1))) * bn * eff;
+  };
+  return cost(512, 0.92) < cost(256, 1.0) ? 512 : 256;
 }
 
 int raster_group() {
@@ -957,7 +955,7 @@ int run_product(const ProductArgs& a, DeviceContext* ctx, cudaStream_t stream, b
   p.plane = a.res_plane;
   p.Np = a.Np;
   p.tiles_m = static_cast<int>(ceil_div(a.M, 2 * kBM));
-  p.bn = tile_width(a.N);
+  p.bn = tile_width(a.M, a.N, ctx->sm_count / 2);
   p.tiles_n = static_cast<int>(ceil_div(a.N, p.bn));
   p.ksteps = static_cast<int>(a.Kp / kBK);
   p.kgroups = static_cast<int>(ceil_div(p.ksteps, kGroupSteps));
