@@ -495,7 +495,11 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t rank = cluster_ctarank();
+  // Work items modulus-major: every pair works on the same residue plane at a time, tile by tile in
+  // raster order, so the operand strips one wave of pairs reads are shared in L2 (tile-major order,
+  // each pair running all moduli of its tile, read 3x the DRAM bytes at 8192^3).
   const int64_t tiles = static_cast<int64_t>(p.tiles_m) * p.tiles_n;
+  const int64_t items = tiles * NM;
   const int64_t first = cluster_id_x(), stride = num_clusters_x();
   const int ksteps = p.ksteps, kgroups = p.kgroups;
 
@@ -532,22 +536,21 @@ __global__ void __launch_bounds__(kThreads, 1)
       int stage = 0;
       uint32_t phase = 0;
       bool ok = true;
-      for (int64_t t = first; t < tiles && ok; t += stride) {
+      for (int64_t w = first; w < items && ok; w += stride) {
+        const int l = static_cast<int>(w / tiles);
         int m0, n0;
-        tile_coords(p, t, &m0, &n0);
+        tile_coords(p, w - l * tiles, &m0, &n0);
         const int arow = m0 + static_cast<int>(rank) * kBM;
         const int brow = n0 + static_cast<int>(rank) * (kBN / 2);
-        for (int l = 0; l < NM && ok; ++l) {
-          for (int ks = 0; ks < ksteps; ++ks) {
-            if (!mbar_wait_cluster(&empty[stage], phase ^ 1, abort_flag, status, 81)) { ok = false; break; }
-            uint8_t* st = smem + stage * kStageBytes;
-            mbar_arrive_expect_tx(&full[stage], kStageBytes);
-            tma_load_3d(st, &tmA, &full[stage], ks * kBK, arow, l);
+        for (int ks = 0; ks < ksteps; ++ks) {
+          if (!mbar_wait_cluster(&empty[stage], phase ^ 1, abort_flag, status, 81)) { ok = false; break; }
+          uint8_t* st = smem + stage * kStageBytes;
+          mbar_arrive_expect_tx(&full[stage], kStageBytes);
+          tma_load_3d(st, &tmA, &full[stage], ks * kBK, arow, l);
 #pragma unroll
-            for (int h = 0; h < T::kMmas; ++h)
-              tma_load_3d(st + kABytes + h * kBHalfBytes, &tmB, &full[stage], ks * kBK, brow + h * kBN, l);
-            if (++stage == kStages) { stage = 0; phase ^= 1; }
-          }
+          for (int h = 0; h < T::kMmas; ++h)
+            tma_load_3d(st + kABytes + h * kBHalfBytes, &tmB, &full[stage], ks * kBK, brow + h * kBN, l);
+          if (++stage == kStages) { stage = 0; phase ^= 1; }
         }
       }
     }
@@ -558,13 +561,11 @@ __global__ void __launch_bounds__(kThreads, 1)
       int stage = 0;
       uint32_t phase = 0;
       bool ok = true;
-      for (int64_t t = first; t < tiles && ok; t += stride) {
-        for (int l = 0; l < NM && ok; ++l) {
-          for (int ks = 0; ks < ksteps; ++ks) {
-            if (!mbar_wait(&full[stage], phase, abort_flag, status, 82)) { ok = false; break; }
-            mbar_arrive_cluster_relaxed(cluster_addr(&full[stage], 0));
-            if (++stage == kStages) { stage = 0; phase ^= 1; }
-          }
+      for (int64_t w = first; w < items && ok; w += stride) {
+        for (int ks = 0; ks < ksteps; ++ks) {
+          if (!mbar_wait(&full[stage], phase, abort_flag, status, 82)) { ok = false; break; }
+          mbar_arrive_cluster_relaxed(cluster_addr(&full[stage], 0));
+          if (++stage == kStages) { stage = 0; phase ^= 1; }
         }
       }
     }
@@ -580,8 +581,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint32_t phase = 0;
     uint32_t pass = 0;
     bool ok = true;
-    for (int64_t t = first; t < tiles && ok; t += stride) {
-      for (int l = 0; l < NM && ok; ++l) {
+    for (int64_t w = first; w < items && ok; w += stride) {
+      {
         for (int g = 0; g < kgroups && ok; ++g, ++pass) {
           const uint32_t buf = pass % T::kAccBufs, use = pass / T::kAccBufs;
           if (!__all_sync(0xffffffffu, mbar_wait_cluster(&acc_empty[buf], (use & 1) ^ 1, abort_flag, status, 83))) {
@@ -636,12 +637,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t acc_empty_r0[2] = {cluster_addr(&acc_empty[0], 0), cluster_addr(&acc_empty[1], 0)};
     uint32_t pass = 0;
     bool ok = true;
-    for (int64_t t = first; t < tiles && ok; t += stride) {
+    for (int64_t w = first; w < items && ok; w += stride) {
+      const int l = static_cast<int>(w / tiles);
       int m0, n0;
-      tile_coords(p, t, &m0, &n0);
+      tile_coords(p, w - l * tiles, &m0, &n0);
       const int64_t row = static_cast<int64_t>(m0) + static_cast<int64_t>(rank) * kBM + quarter * 32 + lane;
       uint8_t* row_base = p.res + row * p.Np + n0 + colhalf * (BN / 2);
-      for (int l = 0; l < NM && ok; ++l) {
+      {
         uint8_t* dst = row_base + static_cast<int64_t>(l) * p.plane;
         for (int g = 0; g < kgroups; ++g, ++pass) {
           const uint32_t buf = pass % T::kAccBufs, use = pass / T::kAccBufs;
@@ -687,7 +689,7 @@ __device__ __forceinline__ double reconstruct(const uint32_t (&w)[NM], int e, co
   for (int k = 0; k < NL; ++k) L[k] = c.Kc[k];
 #pragma unroll
   for (int l = 0; l < NM; ++l) {
-    const uint32_t u = (w[l] >> (8 * e)) & 0xffu;
+    const uint32_t u = __byte_perm(w[l], 0u, 0x4440u | static_cast<uint32_t>(e));  // byte e, zero-extended
     const double ud = __hiloint2double(0x43300000, static_cast<int>(u)) - 4503599627370496.0;  // exact u
 #pragma unroll
     for (int k = 0; k < NL; ++k) L[k] = __fma_rn(ud, c.P[l][k], L[k]);
@@ -701,8 +703,9 @@ __device__ __forceinline__ double reconstruct(const uint32_t (&w)[NM], int e, co
   return t;
 }
 
-// One thread per four consecutive columns of a row: 4-byte loads from each residue plane and
-// 16-byte loads / stores of C, coalesced across the warp (128 columns of a row).
+// One thread per four consecutive columns of a row (blockIdx.x: 1024-column block, blockIdx.y: rows
+// with a grid stride): 4-byte loads from each residue plane and 16-byte loads / stores of C,
+// coalesced across the warp (128 columns of a row).
 template <int NM>
 __global__ void __launch_bounds__(256) crt_recon_kernel(const uint8_t* __restrict__ res, int64_t plane, int64_t Np,
                                                         double* __restrict__ C, int64_t M, int64_t N, int64_t ldc,
@@ -710,10 +713,9 @@ __global__ void __launch_bounds__(256) crt_recon_kernel(const uint8_t* __restric
                                                         double alpha, double beta, int pa, int pb) {
   constexpr int NL = limbs_for(NM);
   const Consts& c = c_table[NM - kMinMod];
-  const int64_t nq = (N + 3) / 4, total = M * nq;
-  for (int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; q < total;
-       q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t i = q / nq, j0 = (q - i * nq) * 4;
+  const int64_t j0 = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 4;
+  if (j0 >= N) return;
+  for (int64_t i = blockIdx.y; i < M; i += gridDim.y) {
     uint32_t w[NM];
     const uint8_t* src = res + i * Np + j0;
 #pragma unroll
@@ -784,10 +786,10 @@ __global__ void k0_kernel(double* C, int64_t M, int64_t N, int64_t ldc, double a
 // Host driver
 // ---------------------------------------------------------------------------------------------
 // Tile width of the product (LIBTHOM_CRT_TILE = 256 / 512 forces one): the smaller time of whole
-// waves of pair tiles over `clusters` CTA pairs, a 512-wide tile taking 0.92 of the time of two
+// waves of (modulus, tile) work items over `clusters` CTA pairs, a 512-wide tile taking 0.92 of the time of two
 // 256-wide ones (measured at 8192^3: less operand traffic per product) but filling fewer pairs when the
 // problem has few tiles (2048 x 2048: 32 tiles of 512 against 64 of 256 for 74 pairs).
-int tile_width(int64_t M, int64_t N, int clusters) {
+int tile_width(int64_t M, int64_t N, int moduli, int clusters) {
   static const int forced = [] {
     const char* e = getenv("LIBTHOM_CRT_TILE");
     const int v = e != nullptr ? atoi(e) : 0;
@@ -796,7 +798,7 @@ int tile_width(int64_t M, int64_t N, int clusters) {
   if (forced != 0) return forced;
   const int64_t tm = ceil_div(M, 2 * kBM);
   auto cost = [&](int bn, double eff) {
-    return static_cast<double>(ceil_div(tm * ceil_div(N, bn), std::max(clusters, 1))) * bn * eff;
+    return static_cast<double>(ceil_div(moduli * tm * ceil_div(N, bn), std::max(clusters, 1))) * bn * eff;
   };
   return cost(512, 0.92) < cost(256, 1.0) ? 512 : 256;
 }
@@ -926,17 +928,21 @@ int launch_product_n(const CUtensorMap& tmA, const CUtensorMap& tmB, const Probl
     attr_err[ctx->device] = cudaOccupancyMaxActiveClusters(&max_clusters[ctx->device], crt_pair_kernel<NM, BN>, &cfg);
   });
   LT_CUDA_TRY(attr_err[ctx->device]);
-  const int64_t tiles = static_cast<int64_t>(p.tiles_m) * p.tiles_n;
-  const int64_t clusters = std::min<int64_t>(std::min<int64_t>(tiles, max_clusters[ctx->device]), ctx->sm_count / 2);
+  const int64_t items = static_cast<int64_t>(p.tiles_m) * p.tiles_n * NM;  // (modulus, tile) work items
+  const int64_t clusters = std::min<int64_t>(std::min<int64_t>(items, max_clusters[ctx->device]), ctx->sm_count / 2);
   if (clusters <= 0) return set_error(LT_ERR_UNSUPPORTED, "no pair of CTAs of the CRT product kernel fits");
   cudaLaunchConfig_t cfg;
   cudaLaunchAttribute attr;
   config(&cfg, &attr, static_cast<unsigned>(2 * clusters));
   if (do_multiply) LT_CUDA_TRY(cudaLaunchKernelEx(&cfg, crt_pair_kernel<NM, BN>, tmA, tmB, p, ctx->status));
   if (do_reconstruct) {
-    const int64_t work = M * ((N + 3) / 4);
-    const int64_t blocks = std::min<int64_t>(ceil_div(work, 256), 8 * ctx->sm_count);
-    crt_recon_kernel<NM><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(p.res, p.plane, p.Np, C, M, N, ldc, ea,
+    // 4 columns per thread; a narrow C takes narrower blocks so few threads idle past column N
+    const int64_t quads = ceil_div(N, 4);
+    const int64_t tx = std::min<int64_t>(256, round_up(quads, 32));
+    const int64_t bx = ceil_div(quads, tx);
+    const int64_t by = std::min<int64_t>(M, std::max<int64_t>(1, 8 * ctx->sm_count * (256 / tx) / bx));
+    crt_recon_kernel<NM><<<dim3(static_cast<unsigned>(bx), static_cast<unsigned>(by)), static_cast<unsigned>(tx), 0,
+                           stream>>>(p.res, p.plane, p.Np, C, M, N, ldc, ea,
                                                                              eb, alpha, beta, c.pa, c.pb);
     LT_CUDA_TRY(cudaGetLastError());
   }
@@ -955,7 +961,7 @@ int run_product(const ProductArgs& a, DeviceContext* ctx, cudaStream_t stream, b
   p.plane = a.res_plane;
   p.Np = a.Np;
   p.tiles_m = static_cast<int>(ceil_div(a.M, 2 * kBM));
-  p.bn = tile_width(a.M, a.N, ctx->sm_count / 2);
+  p.bn = tile_width(a.M, a.N, a.n, ctx->sm_count / 2);
   p.tiles_n = static_cast<int>(ceil_div(a.N, p.bn));
   p.ksteps = static_cast<int>(a.Kp / kBK);
   p.kgroups = static_cast<int>(ceil_div(p.ksteps, kGroupSteps));
