@@ -156,13 +156,14 @@ int lt_dgemm_ozaki_noalloc(const double* A, const double* B, double* C, int64_t 
 int lt_selftest_wait_timeout_noalloc(double limit_ms, void* stream);
 
 /* ---- Ozaki scheme II: the CRT form (no reference counterpart) ------------------------------- */
-/* C = alpha*A*B + beta*C from `moduli` INT8 tensor-core products. Rows of A and columns of B are
- * scaled by powers of two to integers of pa and pb bits (K 2^(pa+pb) <= Mprod / 4, Mprod the product
- * of the moduli); each product multiplies the residues of those integers modulo one of the first
- * `moduli` of the pairwise-coprime moduli 256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217,
- * 211, 199, 197, 193, 191, 181, 179, 173 exactly, and the Chinese remainder theorem recovers the exact
- * integer product, which FP64 scales back (Ozaki, Uchino and Imamura's scheme II). The only error is
- * the truncation of A and B to pa and pb bits: on U[-1,1) entries at K = 8192, 15 moduli (pa = pb = 51)
+/* C = alpha*A*B + beta*C from `moduli` INT8 tensor-core products. Each row of A and column of B is
+ * scaled by a power of two, taken from an integer bound on its 2-norm, and truncated to integers V, W
+ * with |V|_2 |W|_2 < Mprod / 2 (Mprod the product of the moduli), so by the Cauchy-Schwarz inequality
+ * no dot product of V and W reaches Mprod / 2; each product multiplies the residues of those integers
+ * modulo one of the first `moduli` of the pairwise-coprime moduli 256, 255, 253, 251, 247, 241, 239,
+ * 233, 229, 227, 223, 217, 211, 199, 197, 193, 191, 181, 179, 173 exactly, and the Chinese remainder
+ * theorem recovers the exact integer product, which FP64 scales back (Ozaki, Uchino and Imamura's
+ * scheme II). The only error is the truncation of A and B: on U[-1,1) entries at K = 8192, 14 moduli
  * are as accurate as native FP64; each further modulus adds about 8 bits. Rows of A or columns of B
  * holding NaN or Inf give NaN in their row / column of C. K up to 8388480. Bit-identical to the CPU
  * restatement. */
@@ -176,8 +177,8 @@ int lt_dgemm_ozaki_crt(const double* A, const double* B, double* C, int64_t M, i
 size_t lt_ozaki_crt_workspace_size(int64_t M, int64_t N, int64_t K, int moduli);
 int lt_dgemm_ozaki_crt_ws(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
                           double beta, int moduli, void* workspace, size_t workspace_bytes, void* stream);
-/* The two stages, for callers that time or overlap them: exponents and residues of A and B into the
- * workspace; then the products, the reconstruction and the alpha/beta epilogue into C. */
+/* The two stages, for callers that time or overlap them: scaling shifts and residues of A and B into
+ * the workspace; then the products, the reconstruction and the alpha/beta epilogue into C. */
 int lt_ozaki_crt_split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int moduli, void* workspace,
                        size_t workspace_bytes, void* stream);
 int lt_ozaki_crt_product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double beta, int moduli,
@@ -194,9 +195,11 @@ int lt_ozaki_crt_reconstruct(double* C, int64_t M, int64_t N, int64_t K, double 
  * back. Overlap needs page-locked host buffers. Bit-identical to lt_dgemm_ozaki_crt. Synchronous. */
 int lt_dgemm_ozaki_crt_host(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
                             double alpha, double beta, int moduli, void* stream);
-/* The operand bits pa, pb the CRT form uses for `moduli` moduli and inner dimension K, and the moduli
- * themselves (moduli_out: `moduli` ints; any pointer may be NULL). Host arithmetic only. */
-int lt_ozaki_crt_info(int moduli, int64_t K, int* pa, int* pb, int* moduli_out);
+/* The norm bounds of the CRT form with `moduli` moduli (each row of A is scaled to integers of 2-norm
+ * at most 2^ta, each column of B to at most 2^tb; ta + tb is the largest T with 2^T <= Mprod (1 - 2^-20)
+ * / 2, Mprod the product of the moduli) and the moduli themselves (moduli_out: `moduli` ints; any
+ * pointer may be NULL). Host arithmetic only. */
+int lt_ozaki_crt_info(int moduli, int* ta, int* tb, int* moduli_out);
 /* Reference-contract entry points (routines/dgemm/dgemm.h:9 signature) with 14..18 moduli. */
 float dgemm_ozaki_crt14(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);
 float dgemm_ozaki_crt15(const double* A, const double* B, double* C, size_t M, size_t N, size_t K, double alpha, double beta);

@@ -108,7 +108,7 @@ SIGNATURES = {
     "lt_dgemm_ozaki_crt_host": (_i32, _GEMM + [_i32, _vp]),
     "lt_ozaki_crt_multiply": (_i32, [_i64, _i64, _i64, _i32, _vp, _sz, _vp]),
     "lt_ozaki_crt_reconstruct": (_i32, [_vp, _i64, _i64, _i64, _f64, _f64, _i32, _vp, _sz, _vp]),
-    "lt_ozaki_crt_info": (_i32, [_i32, _i64, _c.POINTER(_i32), _c.POINTER(_i32), _c.POINTER(_i32)]),
+    "lt_ozaki_crt_info": (_i32, [_i32, _c.POINTER(_i32), _c.POINTER(_i32), _c.POINTER(_i32)]),
     "dgemm_ozaki_crt14": (_f32, _REF), "dgemm_ozaki_crt15": (_f32, _REF), "dgemm_ozaki_crt16": (_f32, _REF),
     "dgemm_ozaki_crt17": (_f32, _REF), "dgemm_ozaki_crt18": (_f32, _REF),
     "lt_selftest_wait_timeout_noalloc": (_i32, [_f64, _vp]),
@@ -268,12 +268,13 @@ def ozaki_crt_workspace_size(M, N, K, moduli) -> int:
     return int(lib().lt_ozaki_crt_workspace_size(M, N, K, moduli))
 
 
-def ozaki_crt_info(moduli: int, K: int) -> tuple[int, int, list[int]]:
-    """(pa, pb, moduli list) of the CRT form (host arithmetic)."""
-    pa, pb = ctypes.c_int(), ctypes.c_int()
+def ozaki_crt_info(moduli: int) -> tuple[int, int, list[int]]:
+    """(ta, tb, moduli list) of the CRT form (host arithmetic): the rows of A are scaled to 2-norm at
+    most 2^ta, the columns of B to at most 2^tb."""
+    ta, tb = ctypes.c_int(), ctypes.c_int()
     mods = (ctypes.c_int * moduli)()
-    check(lib().lt_ozaki_crt_info(moduli, K, ctypes.byref(pa), ctypes.byref(pb), mods))
-    return pa.value, pb.value, list(mods)
+    check(lib().lt_ozaki_crt_info(moduli, ctypes.byref(ta), ctypes.byref(tb), mods))
+    return ta.value, tb.value, list(mods)
 
 
 def ozaki_split(A, B, M, N, K, slices, workspace, stream=None) -> None:

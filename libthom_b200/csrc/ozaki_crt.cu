@@ -5,13 +5,14 @@
 // of a floating-point product through modular arithmetic and the Chinese remainder theorem),
 // written here from the mathematics:
 //
-//   1. exponents (HBM-bound, shared with the slice form): sigma_i, tau_j = frexp exponents of the
-//      row maxima of A and the column maxima of B.
-//   2. residues (HBM-bound): V = trunc(A[i,k] 2^(pa - sigma_i)) and W = trunc(B[k,j] 2^(pb - tau_j))
-//      are integers below 2^pa, 2^pb in magnitude, with K 2^(pa+pb) <= Mprod / 4, Mprod the product
-//      of n pairwise-coprime moduli m_l <= 256. Each is written as n symmetric residues (one signed
-//      byte each): plane l of A holds V mod m_l, row-major [M][Kp]; plane l of B holds W mod m_l
-//      transposed, [N][Kp] (K-major, as the tensor core reads both operands).
+//   1. scaling (HBM-bound): row i of A is scaled by 2^s_i, column j of B by 2^s_j, the shifts taken
+//      from integer bounds on the rows' and columns' 2-norms so that V = trunc(A[i,k] 2^s_i) and
+//      W = trunc(B[k,j] 2^s_j) satisfy |V_i|_2 <= 2^ta and |W_j|_2 <= 2^tb, where
+//      2^(ta+tb) <= Mprod (1 - 2^-20) / 2 and Mprod is the product of n pairwise-coprime moduli
+//      m_l <= 256: by the Cauchy-Schwarz inequality every |sum_k V W| is below Mprod / 2.
+//   2. residues (HBM-bound): V and W as n symmetric residues each (one signed byte per modulus):
+//      plane l of A holds V mod m_l, row-major [M][Kp]; plane l of B holds W mod m_l transposed,
+//      [N][Kp] (K-major, as the tensor core reads both operands).
 //   3. products (tensor cores): for each modulus, one INT8 x INT8 -> INT32 GEMM of the residue
 //      planes (exact), reduced to the symmetric residue c_l of (sum_k V W) mod m_l and stored as the
 //      byte c_l + 128 in residue plane l of C.
@@ -19,17 +20,19 @@
 //      Mprod/2) with C' = c_l (mod m_l). With the CRT basis P_l = (Mprod/m_l) y_l,
 //      y_l = (Mprod/m_l)^-1 mod m_l, split into nl limbs of w bits: L_k = sum_l c_l P_lk (exact in
 //      FP64), Q = rint(L_hi F_hi + L_lo F_lo) (F_k = 2^(w k) / Mprod), D_k = fma(-Q, M_k, L_k) and
-//      C' = Horner of the D_k in base 2^w; then C = fma(alpha, C' 2^(sigma_i - pa) 2^(tau_j - pb),
-//      beta C0). The CPU oracle (oracle/oracle.c, oracle_crt_dgemm) performs the same arithmetic,
+//      C' = Horner of the D_k in base 2^w; then C = fma(alpha, C' 2^-s_i 2^-s_j, beta C0). The CPU oracle (oracle/oracle.c, oracle_crt_dgemm) performs the same arithmetic,
 //      so results are bit-identical.
 //
 // Against the slice form (ozaki.cu) the product count is n, not s(s+1)/2: at FP64 accuracy on the
-// 8192^3 workload 15 INT8 products instead of 28.
+// 8192^3 workload 14 INT8 products instead of 28. Scaling by the 2-norm rather than by K times the
+// largest entry gains about a bit per operand on uniformly distributed rows and more on rows whose
+// entries spread over many binades: one modulus fewer for the same accuracy.
 //
-// Product kernel: persistent CTA pairs; a pair owns a 256 x 256 tile of C and, for each modulus in
-// turn, runs the whole K loop of that modulus into one of two TMEM accumulators (256 columns each)
-// with tcgen05.mma.cta_group::2.kind::i8 (M256 N256 K32), operands staged by 3-D TMA (plane = the
-// modulus) with 128-byte swizzle. Roles (320 threads per CTA):
+// Product kernel: persistent CTA pairs over (modulus, tile) work items, modulus-major; a pair runs
+// the whole K loop of one modulus for one 256 x 256 or 256 x 512 tile of C with
+// tcgen05.mma.cta_group::2.kind::i8 (M256 N256 K32; two MMAs per K step for the 512-wide tile), into
+// one of two 256-column TMEM accumulators or one 512-column accumulator; operands staged by 3-D TMA
+// (plane = the modulus) with 128-byte swizzle. Roles (320 threads per CTA):
 //   warp 0      TMA producer (both CTAs)
 //   warp 1      rank 0: MMA issuer for the pair; rank 1: forwards each landed stage to rank 0
 //   warps 2..9  drain: TMEM -> registers, INT32 -> symmetric residue, bytes to the residue planes,
@@ -40,6 +43,7 @@
 #include <cuda.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -92,7 +96,7 @@ inline int64_t ceil_div(int64_t x, int64_t m) { return (x + m - 1) / m; }
 // Constants of a modulus set (host arithmetic, exact)
 // ---------------------------------------------------------------------------------------------
 struct Consts {
-  int n, nl, w, pa, pb;
+  int n, nl, w, ta, tb;  // norm bounds: |V_i|_2 <= 2^ta, |W_j|_2 <= 2^tb
   int32_t m[kMaxMod];
   int32_t h[kMaxMod];             // (m - 1) / 2: the symmetric residues lie in [-h, h]
   // residues of the scaled inputs: x = dp4a(bytes of V + 2^62, coef) + add, x mod m by umulhi
@@ -161,9 +165,10 @@ inline uint32_t inverse_mod(uint32_t a, uint32_t m) {  // a^-1 mod m, gcd(a, m) 
   return static_cast<uint32_t>(t < 0 ? t + m : t);
 }
 
-// Constants for n moduli and inner dimension K (K >= 1): pa + pb is the largest T with
-// K 2^T <= Mprod / 4, split evenly, each at most 62 (the residues are taken from 64-bit integers).
-Consts make_consts(int n, int64_t K) {
+// Constants for n moduli: ta + tb is the largest Tc with 2^Tc <= Mprod (1 - 2^-20) / 2, split
+// evenly, each at most 62 (the residues are taken from 64-bit integers). The margin keeps the
+// quotient estimate of the reconstruction, whose error is far below 2^-21, from rounding the wrong way.
+Consts make_consts(int n) {
   Consts c;
   std::memset(&c, 0, sizeof c);
   c.n = n;
@@ -207,10 +212,11 @@ Consts make_consts(int n, int64_t K) {
   c.f_hi = std::ldexp(1.0, c.w * (c.nl - 1)) / md;
   c.f_lo = std::ldexp(1.0, c.w * (c.nl - 2)) / md;
   Big q = Mp;
-  q.divmod_small(static_cast<uint32_t>(2 * std::max<int64_t>(K, 1)));
-  const int T = q.bit_length() - 2;
-  c.pa = std::min(62, T / 2);
-  c.pb = std::min(62, T - T / 2);
+  q.mul_small((1u << 20) - 1u);
+  q.divmod_small(1u << 21);
+  const int T = q.bit_length() - 1;
+  c.ta = std::min(62, T / 2);
+  c.tb = std::min(62, T - T / 2);
   return c;
 }
 
@@ -219,8 +225,7 @@ Consts make_consts(int n, int64_t K) {
 __host__ __device__ constexpr int limbs_for(int nm) { return nm <= 10 ? 2 : (nm <= 16 ? 3 : 4); }
 
 // The constants of every modulus count in constant memory (filled once per device), read by the
-// kernels with compile-time offsets through the constant cache. pa and pb, which depend on K, are
-// kernel arguments.
+// kernels with compile-time offsets through the constant cache.
 __constant__ Consts c_table[kMaxMod - kMinMod + 1];
 
 int ensure_table(int device) {
@@ -228,7 +233,7 @@ int ensure_table(int device) {
   static cudaError_t err[64];
   std::call_once(once[device], [&] {
     Consts host[kMaxMod - kMinMod + 1];
-    for (int n = kMinMod; n <= kMaxMod; ++n) host[n - kMinMod] = make_consts(n, 1);
+    for (int n = kMinMod; n <= kMaxMod; ++n) host[n - kMinMod] = make_consts(n);
     err[device] = cudaMemcpyToSymbol(c_table, host, sizeof host);
   });
   LT_CUDA_TRY(err[device]);
@@ -236,14 +241,18 @@ int ensure_table(int device) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Workspace: [amaxA: M u64][amaxB: N u64][row exponents: M int][column exponents: N int]
+// Workspace: [chunk exponents of A: M x ncha int][chunk sums of A: M x ncha u64]
+//            [the same for B: N x nchb][row shifts: M int][column shifts: N int]
 //            [A residues n x M x Kp][B residues n x N x Kp]
-//            [C residue planes n x Mp x Np], 256-aligned; Mp, Np = M, N rounded up to the 256 x 256
-//            pair tile (the product writes whole tiles).
+//            [C residue planes n x Mp x Np], 256-aligned; ncha = ceil(K / 512), nchb = ceil(K / 128);
+//            Mp, Np = M, N rounded up to the pair tile (the product writes whole tiles).
 // ---------------------------------------------------------------------------------------------
+constexpr int kChunkA = 512;  // K positions per chunk of a row of A (a warp, 16 per lane)
+constexpr int kChunkB = 128;  // K positions per chunk of a column of B (a block, 16 per thread)
+
 struct Layout {
-  int64_t Kp, Mp, Np;
-  size_t off_amax_a, off_amax_b, off_ea, off_eb, off_ra, off_rb, off_rc, total;
+  int64_t Kp, Mp, Np, ncha, nchb;
+  size_t off_eca, off_sca, off_ecb, off_scb, off_ea, off_eb, off_ra, off_rb, off_rc, total;
 };
 
 Layout layout_for(int64_t M, int64_t N, int64_t K, int n) {
@@ -251,16 +260,186 @@ Layout layout_for(int64_t M, int64_t N, int64_t K, int n) {
   L.Kp = round_up(std::max<int64_t>(K, 1), kBK);
   L.Mp = round_up(std::max<int64_t>(M, 1), 2 * kBM);
   L.Np = round_up(std::max<int64_t>(N, 1), kPadN);
+  L.ncha = ceil_div(std::max<int64_t>(K, 1), kChunkA);
+  L.nchb = ceil_div(std::max<int64_t>(K, 1), kChunkB);
   size_t o = 0;
-  L.off_amax_a = o; o += round_up(8 * M, 256);
-  L.off_amax_b = o; o += round_up(8 * N, 256);
-  L.off_ea = o;     o += round_up(4 * M, 256);
-  L.off_eb = o;     o += round_up(4 * N, 256);
-  L.off_ra = o;     o += round_up(static_cast<int64_t>(n) * M * L.Kp, 256);
-  L.off_rb = o;     o += round_up(static_cast<int64_t>(n) * N * L.Kp, 256);
-  L.off_rc = o;     o += static_cast<size_t>(n) * L.Mp * L.Np;
+  L.off_eca = o; o += round_up(4 * M * L.ncha, 256);
+  L.off_sca = o; o += round_up(8 * M * L.ncha, 256);
+  L.off_ecb = o; o += round_up(4 * N * L.nchb, 256);
+  L.off_scb = o; o += round_up(8 * N * L.nchb, 256);
+  L.off_ea = o;  o += round_up(4 * M, 256);
+  L.off_eb = o;  o += round_up(4 * N, 256);
+  L.off_ra = o;  o += round_up(static_cast<int64_t>(n) * M * L.Kp, 256);
+  L.off_rb = o;  o += round_up(static_cast<int64_t>(n) * N * L.Kp, 256);
+  L.off_rc = o;  o += static_cast<size_t>(n) * L.Mp * L.Np;
   L.total = o;
   return L;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Scaling: bounds on the 2-norms of the rows of A and the columns of B
+// ---------------------------------------------------------------------------------------------
+// Row i of A gets the shift s_i that makes V = trunc(A[i,k] 2^s_i) satisfy |V_i|_2 <= 2^ta (columns
+// of B likewise with 2^tb). The bound is computed in integers, so its value does not depend on the
+// order of the reductions and the CPU oracle (oracle_crt_shift) reproduces it exactly:
+//   entry a != 0: e = its frexp exponent, x = floor(|a| 2^(15 - e)) + 1 (subnormals: e = -1021,
+//     x = 2^14 + 1), so |a| < x 2^(e - 15);
+//   chunk (512 consecutive k of a row of A, 128 of a column of B): E_c = the largest e,
+//     S_c = sum of ceil(x^2 4^(e - E_c)) (each term at most 2^30);
+//   row: sigma = the largest E_c, S = sum of ceil(S_c / 4^(sigma - E_c)) (< 2^54 for K < 2^23),
+//     so that |row|_2^2 < S 2^(2 sigma - 30);
+//   s = t + 15 - sigma - ceil(bitlen(S - 1) / 2): |V|_2^2 < S 2^(2t - 2 ceil(bitlen(S - 1) / 2)) <= 2^2t.
+// A row without nonzero entries takes s = 0, one holding NaN or Inf kSentinel.
+constexpr int kEmpty = INT_MIN;  // chunk or row without a nonzero entry
+
+// (e + 2048) << 16 | x of a finite nonzero entry, 0 for zero, 0xffffffff for NaN or Inf: the largest
+// code of a chunk carries its largest exponent, or flags a non-finite entry.
+__device__ __forceinline__ uint32_t entry_code(double a) {
+  const unsigned long long b = abs_bits(a);
+  if (b == 0ull) return 0u;
+  if (b >= 0x7ff0000000000000ull) return 0xffffffffu;
+  const uint32_t E = static_cast<uint32_t>(b >> 52);
+  if (E == 0u) return ((2048u - 1021u) << 16) | ((1u << 14) + 1u);
+  return ((E + 1026u) << 16) | ((1u << 14) + static_cast<uint32_t>((b >> 38) & 0x3fffu) + 1u);
+}
+
+// ceil(x^2 4^(e - E_c)) of an entry code; ecode = the chunk's largest code >> 16 = E_c + 2048
+__device__ __forceinline__ uint32_t entry_term(uint32_t code, uint32_t ecode) {
+  if (code == 0u) return 0u;
+  const uint32_t x = code & 0xffffu;
+  const uint32_t x2 = x * x;  // x <= 2^15
+  const uint32_t d = 2u * (ecode - (code >> 16));
+  if (d >= 31u) return 1u;  // 0 < x^2 <= 2^30 < 2^d
+  return (x2 + ((1u << d) - 1u)) >> d;  // < 2^31 + 2^30: no overflow
+}
+
+// ceil(v / 2^d), d >= 0, v < 2^62
+__device__ __forceinline__ unsigned long long ceil_shr(unsigned long long v, int d) {
+  if (d == 0) return v;
+  if (d >= 63) return v != 0ull ? 1ull : 0ull;
+  return (v + ((1ull << d) - 1ull)) >> d;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ int chunk_exponent(uint32_t mx) {
+  return mx == 0xffffffffu ? kSentinel : (mx == 0u ? kEmpty : static_cast<int>(mx >> 16) - 2048);
+}
+
+// Chunk statistics of the rows of A (a warp per row and chunk of 512, 16 entries per lane; blocks
+// 0..row_blocks-1) and of the columns of B (a block per 32 columns and chunk of 128, 16 entries per
+// thread, as the column split reads them; the remaining blocks): ec[r * nch + c] = E_c (kEmpty, or
+// kSentinel for a non-finite entry), sc[r * nch + c] = S_c. Either side may be empty (M = 0 or N = 0).
+__global__ void __launch_bounds__(256) crt_stats_kernel(const double* __restrict__ A, int64_t M, int64_t lda,
+                                                        int64_t ncha, const double* __restrict__ B, int64_t N,
+                                                        int64_t ldb, int64_t nchb, int64_t K, int64_t row_blocks,
+                                                        int* __restrict__ ec_a, unsigned long long* __restrict__ sc_a,
+                                                        int* __restrict__ ec_b, unsigned long long* __restrict__ sc_b) {
+  __shared__ uint32_t s_max[8][32];
+  __shared__ unsigned long long s_sum[8][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t code[16];
+  if (static_cast<int64_t>(blockIdx.x) < row_blocks) {
+    const int64_t item = static_cast<int64_t>(blockIdx.x) * 8 + warp;  // row * ncha + chunk
+    if (item >= M * ncha) return;
+    const int64_t row = item / ncha, k0 = (item - row * ncha) * kChunkA + lane * 16;
+    const double* a = A + row * lda + k0;
+    if (k0 + 16 <= K && (reinterpret_cast<uintptr_t>(a) & 15) == 0) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const double2 x = __ldcs(reinterpret_cast<const double2*>(a) + j);
+        code[2 * j] = entry_code(x.x);
+        code[2 * j + 1] = entry_code(x.y);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) code[j] = (k0 + j < K) ? entry_code(__ldcs(a + j)) : 0u;
+    }
+    uint32_t mx = 0u;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) mx = max(mx, code[j]);
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    unsigned long long sum = 0ull;
+    if (mx != 0u && mx != 0xffffffffu) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) sum += entry_term(code[j], mx >> 16);
+      sum = warp_sum_u64(sum);
+    }
+    if (lane == 0) {
+      ec_a[item] = chunk_exponent(mx);
+      sc_a[item] = sum;
+    }
+  } else {
+    const int64_t ncb = (N + 31) / 32, bi = static_cast<int64_t>(blockIdx.x) - row_blocks;
+    const int64_t c = bi / ncb, col = (bi - c * ncb) * 32 + lane;
+    const int64_t k0 = c * kChunkB + warp * 16;
+    const double* b = B + k0 * ldb + col;
+    if (col < N && k0 + 16 <= K) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) code[j] = entry_code(__ldcs(b + j * ldb));
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) code[j] = (col < N && k0 + j < K) ? entry_code(__ldcs(b + j * ldb)) : 0u;
+    }
+    uint32_t mx = 0u;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) mx = max(mx, code[j]);
+    s_max[warp][lane] = mx;
+    __syncthreads();
+    mx = 0u;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) mx = max(mx, s_max[w][lane]);
+    unsigned long long sum = 0ull;
+    if (mx != 0u && mx != 0xffffffffu) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) sum += entry_term(code[j], mx >> 16);
+    }
+    s_sum[warp][lane] = sum;
+    __syncthreads();
+    if (warp == 0 && col < N) {
+      unsigned long long total = 0ull;
+#pragma unroll
+      for (int w = 0; w < 8; ++w) total += s_sum[w][lane];
+      ec_b[col * nchb + c] = chunk_exponent(mx);
+      sc_b[col * nchb + c] = total;
+    }
+  }
+}
+
+// The shifts: a warp per row of A (warps 0..M-1) and per column of B (the next N) combines that
+// row's chunk statistics.
+__global__ void __launch_bounds__(256) crt_shift_kernel(const int* __restrict__ ec_a,
+                                                        const unsigned long long* __restrict__ sc_a, int64_t M,
+                                                        int64_t ncha, const int* __restrict__ ec_b,
+                                                        const unsigned long long* __restrict__ sc_b, int64_t N,
+                                                        int64_t nchb, int ta, int tb, int* __restrict__ sh_a,
+                                                        int* __restrict__ sh_b) {
+  const int64_t wid = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (wid >= M + N) return;
+  const bool is_a = wid < M;
+  const int64_t r = is_a ? wid : wid - M, nch = is_a ? ncha : nchb;
+  const int* ec = is_a ? ec_a + r * ncha : ec_b + r * nchb;
+  const unsigned long long* sc = is_a ? sc_a + r * ncha : sc_b + r * nchb;
+  int sigma = kEmpty;
+  for (int64_t c = lane; c < nch; c += 32) sigma = max(sigma, ec[c]);
+  sigma = __reduce_max_sync(0xffffffffu, sigma);
+  int out = 0;
+  if (sigma == kSentinel) {
+    out = kSentinel;
+  } else if (sigma != kEmpty) {
+    unsigned long long S = 0ull;
+    for (int64_t c = lane; c < nch; c += 32)
+      if (ec[c] != kEmpty) S += ceil_shr(sc[c], 2 * (sigma - ec[c]));
+    S = warp_sum_u64(S);
+    const int b = S > 1ull ? 64 - __clzll(static_cast<long long>(S - 1ull)) : 0;  // bitlen(S - 1)
+    out = (is_a ? ta : tb) + 15 - sigma - (b + 1) / 2;
+  }
+  if (lane == 0) (is_a ? sh_a : sh_b)[r] = out;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -292,14 +471,13 @@ __device__ __forceinline__ uint4 residue_plane(int l, const uint32_t (&ulo)[16],
                     residue_word(l, ulo + 8, uhi + 8, c), residue_word(l, ulo + 12, uhi + 12, c));
 }
 
-// V = trunc(a 2^(p - e)) of 16 finite entries of a row (column) whose largest magnitude is below 2^e,
-// as U = V + 2^62 in two words each: the product by 2^(p - e) is exact whenever it is at least 1 in
-// magnitude (a power-of-two scaling to a normal number) and anything smaller truncates to 0, so one
-// multiplication (two when 2^(p - e) is above the double range) and a truncating conversion give V
-// exactly, below 2^p <= 2^62. A row (column) holding NaN or Inf (e = kSentinel) gets V = 0.
-__device__ __forceinline__ void scaled_words(const double (&v)[16], int e, int p, uint32_t (&ulo)[16],
-                                             uint32_t (&uhi)[16]) {
-  if (e == kSentinel) {
+// V = trunc(a 2^s) of 16 finite entries of a row (column) with shift s, as U = V + 2^62 in two words
+// each: the product by 2^s is exact whenever it is at least 1 in magnitude (a power-of-two scaling to
+// a normal number) and anything smaller truncates to 0, so one multiplication (two when 2^s is above
+// the double range) and a truncating conversion give V exactly; |V| <= |V_row|_2 <= 2^62. A row
+// (column) holding NaN or Inf (s = kSentinel) gets V = 0.
+__device__ __forceinline__ void scaled_words(const double (&v)[16], int s, uint32_t (&ulo)[16], uint32_t (&uhi)[16]) {
+  if (s == kSentinel) {
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       ulo[i] = 0u;
@@ -307,12 +485,12 @@ __device__ __forceinline__ void scaled_words(const double (&v)[16], int e, int p
     }
     return;
   }
-  const int d = p - e, d1 = d < 1023 ? d : 1023;
-  const double s1 = pow2i(d1), s2 = pow2i(d - d1);
+  const int d1 = s < 1023 ? s : 1023;  // s > -1022: the shift of the largest finite rows is above -1000
+  const double s1 = pow2i(d1), s2 = pow2i(s - d1);
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
     double x = __dmul_rn(v[i], s1);
-    if (d > 1023) x = __dmul_rn(x, s2);
+    if (s > 1023) x = __dmul_rn(x, s2);
     const unsigned long long U = static_cast<unsigned long long>(__double2ll_rz(x) + (1ll << 62));
     ulo[i] = static_cast<uint32_t>(U);
     uhi[i] = static_cast<uint32_t>(U >> 32);
@@ -324,16 +502,14 @@ __device__ __forceinline__ void scaled_words(const double (&v)[16], int e, int p
 template <int NM>
 __global__ void __launch_bounds__(256, 3) crt_split_rows_kernel(const double* __restrict__ A, int64_t M, int64_t K,
                                                              int64_t lda, int64_t Kp,
-                                                             const unsigned long long* __restrict__ amax,
-                                                             int8_t* __restrict__ out, int64_t plane, int pa,
-                                                             int* __restrict__ exps) {
+                                                             const int* __restrict__ shifts,
+                                                             int8_t* __restrict__ out, int64_t plane) {
   const Consts& c = c_table[NM - kMinMod];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t row = static_cast<int64_t>(blockIdx.x) * 8 + warp;
   const int64_t k0 = static_cast<int64_t>(blockIdx.y) * 512 + lane * 16;
   if (row >= M || k0 >= Kp) return;
-  const int e = exponent_of_maxbits(amax[row]);
-  if (blockIdx.y == 0 && lane == 0) exps[row] = e;  // the row's exponent, for the reconstruction
+  const int sh = shifts[row];
   const double* a = A + row * lda + k0;
   double v[16];
   if (k0 + 16 <= K && (reinterpret_cast<uintptr_t>(a) & 15) == 0) {
@@ -348,7 +524,7 @@ __global__ void __launch_bounds__(256, 3) crt_split_rows_kernel(const double* __
     for (int j = 0; j < 16; ++j) v[j] = (k0 + j < K) ? __ldcs(a + j) : 0.0;
   }
   uint32_t ulo[16], uhi[16];
-  scaled_words(v, e, pa, ulo, uhi);
+  scaled_words(v, sh, ulo, uhi);
   int8_t* dst = out + row * Kp + k0;
 #pragma unroll
   for (int l = 0; l < NM; ++l) *reinterpret_cast<uint4*>(dst + l * plane) = residue_plane(l, ulo, uhi, c);
@@ -363,9 +539,8 @@ constexpr int kColPlanes = 8;   // planes staged at a time (8 x 4.5 KB)
 template <int NM>
 __global__ void __launch_bounds__(256, 3) crt_split_cols_kernel(const double* __restrict__ B, int64_t K, int64_t N,
                                                              int64_t ldb, int64_t Kp,
-                                                             const unsigned long long* __restrict__ amax,
-                                                             int8_t* __restrict__ out, int64_t plane, int pb,
-                                                             int* __restrict__ exps) {
+                                                             const int* __restrict__ shifts,
+                                                             int8_t* __restrict__ out, int64_t plane) {
   __shared__ __align__(16) uint8_t stage[kColPlanes][32 * kColPitch];
   const Consts& c = c_table[NM - kMinMod];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -373,8 +548,7 @@ __global__ void __launch_bounds__(256, 3) crt_split_cols_kernel(const double* __
   const int64_t kb = static_cast<int64_t>(blockIdx.y) * kBK;
   const int64_t col = col0 + lane;
   const int64_t k0 = kb + warp * 16;
-  const int e = col < N ? exponent_of_maxbits(amax[col]) : 0;
-  if (blockIdx.y == 0 && warp == 0 && col < N) exps[col] = e;  // the column's exponent, for the reconstruction
+  const int sh = col < N ? shifts[col] : 0;
   double v[16];
   const double* b = B + k0 * ldb + col;
   if (col < N && k0 + 16 <= K) {
@@ -385,7 +559,7 @@ __global__ void __launch_bounds__(256, 3) crt_split_cols_kernel(const double* __
     for (int j = 0; j < 16; ++j) v[j] = (col < N && k0 + j < K) ? __ldcs(b + j * ldb) : 0.0;
   }
   uint32_t ulo[16], uhi[16];
-  scaled_words(v, e, pb, ulo, uhi);
+  scaled_words(v, sh, ulo, uhi);
   // thread t then writes 16 bytes of column t / 8 (K bytes 16 (t % 8) ..) of each staged plane
   const int cl = threadIdx.x >> 3, part = threadIdx.x & 7;
   const bool writes = col0 + cl < N;
@@ -497,7 +671,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t rank = cluster_ctarank();
   // Work items modulus-major: every pair works on the same residue plane at a time, tile by tile in
   // raster order, so the operand strips one wave of pairs reads are shared in L2 (tile-major order,
-  // each pair running all moduli of its tile, read 3x the DRAM bytes at 8192^3).
+  // each pair running all moduli of its tile, read twice the DRAM bytes at 8192^3, 16.8 against
+  // 8.2 GB, in the same time), and a problem with fewer tiles than pairs still occupies every pair.
   const int64_t tiles = static_cast<int64_t>(p.tiles_m) * p.tiles_n;
   const int64_t items = tiles * NM;
   const int64_t first = cluster_id_x(), stride = num_clusters_x();
@@ -703,14 +878,14 @@ __device__ __forceinline__ double reconstruct(const uint32_t (&w)[NM], int e, co
   return t;
 }
 
-// One thread per four consecutive columns of a row (blockIdx.x: 1024-column block, blockIdx.y: rows
-// with a grid stride): 4-byte loads from each residue plane and 16-byte loads / stores of C,
-// coalesced across the warp (128 columns of a row).
+// One thread per four consecutive columns of a row (blockIdx.x: a block of 4 * blockDim.x columns,
+// blockIdx.y: rows with a grid stride): 4-byte loads from each residue plane and 16-byte loads /
+// stores of C, coalesced across the warp (128 columns of a row).
 template <int NM>
 __global__ void __launch_bounds__(256) crt_recon_kernel(const uint8_t* __restrict__ res, int64_t plane, int64_t Np,
                                                         double* __restrict__ C, int64_t M, int64_t N, int64_t ldc,
                                                         const int* __restrict__ ea, const int* __restrict__ eb,
-                                                        double alpha, double beta, int pa, int pb) {
+                                                        double alpha, double beta) {
   constexpr int NL = limbs_for(NM);
   const Consts& c = c_table[NM - kMinMod];
   const int64_t j0 = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 4;
@@ -734,28 +909,28 @@ __global__ void __launch_bounds__(256) crt_recon_kernel(const uint8_t* __restric
           if (j0 + e < N) c0[e] = crow[j0 + e];
       }
     }
-    const int sig = ea[i];
-    int tau[4];
+    const int sr = ea[i];
+    int sc[4];
     if (j0 + 4 <= N) {
       const int4 t4 = *reinterpret_cast<const int4*>(eb + j0);
-      tau[0] = t4.x; tau[1] = t4.y; tau[2] = t4.z; tau[3] = t4.w;
+      sc[0] = t4.x; sc[1] = t4.y; sc[2] = t4.z; sc[3] = t4.w;
     } else {
 #pragma unroll
-      for (int e = 0; e < 4; ++e) tau[e] = j0 + e < N ? eb[j0 + e] : 0;
+      for (int e = 0; e < 4; ++e) sc[e] = j0 + e < N ? eb[j0 + e] : 0;
     }
-    // C' 2^(sigma - pa) 2^(tau - pb): with both factors in the double range this is two exact-factor
+    // C' 2^-s_i 2^-s_j: with both factors in the double range this is two exact-factor
     // multiplications, which is what scale_pow2 does there; scale_pow2 takes the rest
-    const int es = sig - pa;
-    const bool row_fast = sig != kSentinel && es >= -1022 && es <= 1023;
+    const int es = -sr;
+    const bool row_fast = sr != kSentinel && es >= -1022 && es <= 1023;
     const double rs = pow2i(row_fast ? es : 0);
     double out[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
-      if (sig == kSentinel || tau[e] == kSentinel) {
+      if (sr == kSentinel || sc[e] == kSentinel) {
         out[e] = __longlong_as_double(0x7ff8000000000000ll);
       } else {
         const double t = reconstruct<NM, NL>(w, e, c);
-        const int et = tau[e] - pb;
+        const int et = -sc[e];
         const double tv = (row_fast && et >= -1022 && et <= 1023) ? __dmul_rn(__dmul_rn(t, rs), pow2i(et))
                                                                    : scale_pow2(scale_pow2(t, es), et);
         out[e] = (beta != 0.0) ? fma(alpha, tv, __dmul_rn(beta, c0[e])) : __dmul_rn(alpha, tv);
@@ -812,22 +987,40 @@ int raster_group() {
   return g;
 }
 
+// Chunk statistics and shifts of rows 0..M-1 of A (row stride K) and of the columns of B (row
+// stride N); either side may be empty. `ec_a` / `sc_a` hold ncha entries per row, `ec_b` / `sc_b`
+// nchb per column.
+int scale(const double* A, int64_t M, const double* B, int64_t N, int64_t K, const Layout& L, int* ec_a,
+          unsigned long long* sc_a, int* ec_b, unsigned long long* sc_b, int* sh_a, int* sh_b, const Consts& c,
+          cudaStream_t stream) {
+  if (M + N == 0) return LT_OK;
+  const int64_t row_blocks = ceil_div(M * L.ncha, 8);
+  const int64_t blocks = row_blocks + ceil_div(N, 32) * L.nchb;
+  crt_stats_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(A, M, K, L.ncha, B, N, N, L.nchb, K, row_blocks,
+                                                                       ec_a, sc_a, ec_b, sc_b);
+  LT_CUDA_TRY(cudaGetLastError());
+  crt_shift_kernel<<<static_cast<unsigned>(ceil_div((M + N) * 32, 256)), 256, 0, stream>>>(
+      ec_a, sc_a, M, L.ncha, ec_b, sc_b, N, L.nchb, c.ta, c.tb, sh_a, sh_b);
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
 // Residue planes of rows 0..M-1 of A (row stride K) into `ra` (plane stride `plane`), and of the
-// columns of B (row stride N) into `rb`, for NM moduli.
+// columns of B (row stride N) into `rb`, for NM moduli, with the shifts `scale` wrote.
 template <int NM>
-int split_rows_n(const double* A, int64_t M, int64_t K, int64_t Kp, const unsigned long long* amax, int8_t* ra,
-                 int64_t plane, int pa, int* exps, cudaStream_t stream) {
+int split_rows_n(const double* A, int64_t M, int64_t K, int64_t Kp, const int* shifts, int8_t* ra, int64_t plane,
+                 cudaStream_t stream) {
   const dim3 grid(static_cast<unsigned>(ceil_div(M, 8)), static_cast<unsigned>(ceil_div(Kp, 512)));
-  crt_split_rows_kernel<NM><<<grid, 256, 0, stream>>>(A, M, K, K, Kp, amax, ra, plane, pa, exps);
+  crt_split_rows_kernel<NM><<<grid, 256, 0, stream>>>(A, M, K, K, Kp, shifts, ra, plane);
   LT_CUDA_TRY(cudaGetLastError());
   return LT_OK;
 }
 
 template <int NM>
-int split_cols_n(const double* B, int64_t K, int64_t N, int64_t Kp, const unsigned long long* amax, int8_t* rb,
-                 int64_t plane, int pb, int* exps, cudaStream_t stream) {
+int split_cols_n(const double* B, int64_t K, int64_t N, int64_t Kp, const int* shifts, int8_t* rb, int64_t plane,
+                 cudaStream_t stream) {
   const dim3 grid(static_cast<unsigned>(ceil_div(N, 32)), static_cast<unsigned>(Kp / kBK));
-  crt_split_cols_kernel<NM><<<grid, 256, 0, stream>>>(B, K, N, N, Kp, amax, rb, plane, pb, exps);
+  crt_split_cols_kernel<NM><<<grid, 256, 0, stream>>>(B, K, N, N, Kp, shifts, rb, plane);
   LT_CUDA_TRY(cudaGetLastError());
   return LT_OK;
 }
@@ -841,18 +1034,37 @@ int split_cols_n(const double* B, int64_t K, int64_t N, int64_t Kp, const unsign
     default: return set_error(LT_ERR_INVALID_ARGUMENT, "modulus count %d outside [%d, %d]", n, kMinMod, kMaxMod); \
   }
 
-int split_rows(int n, const double* A, int64_t M, int64_t K, int64_t Kp, const unsigned long long* amax, int8_t* ra,
-               int64_t plane, int pa, int* exps, cudaStream_t stream) {
-#define LT_CALL(NM) split_rows_n<NM>(A, M, K, Kp, amax, ra, plane, pa, exps, stream)
+int split_rows(int n, const double* A, int64_t M, int64_t K, int64_t Kp, const int* shifts, int8_t* ra, int64_t plane,
+               cudaStream_t stream) {
+#define LT_CALL(NM) split_rows_n<NM>(A, M, K, Kp, shifts, ra, plane, stream)
   LT_CRT_DISPATCH(n, LT_CALL)
 #undef LT_CALL
 }
 
-int split_cols(int n, const double* B, int64_t K, int64_t N, int64_t Kp, const unsigned long long* amax, int8_t* rb,
-               int64_t plane, int pb, int* exps, cudaStream_t stream) {
-#define LT_CALL(NM) split_cols_n<NM>(B, K, N, Kp, amax, rb, plane, pb, exps, stream)
+int split_cols(int n, const double* B, int64_t K, int64_t N, int64_t Kp, const int* shifts, int8_t* rb, int64_t plane,
+               cudaStream_t stream) {
+#define LT_CALL(NM) split_cols_n<NM>(B, K, N, Kp, shifts, rb, plane, stream)
   LT_CRT_DISPATCH(n, LT_CALL)
 #undef LT_CALL
+}
+
+struct Scratch {  // the workspace's arrays
+  int *ec_a, *ec_b, *ea, *eb;
+  unsigned long long *sc_a, *sc_b;
+  int8_t *ra, *rb;
+};
+
+Scratch scratch(uint8_t* ws, const Layout& L) {
+  Scratch s;
+  s.ec_a = reinterpret_cast<int*>(ws + L.off_eca);
+  s.sc_a = reinterpret_cast<unsigned long long*>(ws + L.off_sca);
+  s.ec_b = reinterpret_cast<int*>(ws + L.off_ecb);
+  s.sc_b = reinterpret_cast<unsigned long long*>(ws + L.off_scb);
+  s.ea = reinterpret_cast<int*>(ws + L.off_ea);
+  s.eb = reinterpret_cast<int*>(ws + L.off_eb);
+  s.ra = reinterpret_cast<int8_t*>(ws + L.off_ra);
+  s.rb = reinterpret_cast<int8_t*>(ws + L.off_rb);
+  return s;
 }
 
 int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int n, void* workspace,
@@ -861,20 +1073,13 @@ int split(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int
   if (ctx == nullptr) return last_error();
   const Layout L = layout_for(M, N, K, n);
   if (workspace_bytes < L.total) return set_error(LT_ERR_NO_MEMORY, "CRT workspace too small");
-  uint8_t* ws = static_cast<uint8_t*>(workspace);
-  auto* amax_a = reinterpret_cast<unsigned long long*>(ws + L.off_amax_a);
-  auto* amax_b = reinterpret_cast<unsigned long long*>(ws + L.off_amax_b);
-  LT_CUDA_TRY(cudaMemsetAsync(ws, 0, L.off_ra, stream));
   if (K == 0) return LT_OK;
   LT_TRY(ensure_table(ctx->device));
-  LT_TRY(ozaki::exponents(A, B, M, N, K, amax_a, amax_b, ctx->sm_count, stream));
-  const Consts c = make_consts(n, K);
-  auto* ra = reinterpret_cast<int8_t*>(ws + L.off_ra);
-  auto* rb = reinterpret_cast<int8_t*>(ws + L.off_rb);
-  auto* ea = reinterpret_cast<int*>(ws + L.off_ea);
-  auto* eb = reinterpret_cast<int*>(ws + L.off_eb);
-  LT_TRY(split_rows(n, A, M, K, L.Kp, amax_a, ra, M * L.Kp, c.pa, ea, stream));
-  return split_cols(n, B, K, N, L.Kp, amax_b, rb, N * L.Kp, c.pb, eb, stream);
+  const Consts c = make_consts(n);
+  const Scratch w = scratch(static_cast<uint8_t*>(workspace), L);
+  LT_TRY(scale(A, M, B, N, K, L, w.ec_a, w.sc_a, w.ec_b, w.sc_b, w.ea, w.eb, c, stream));
+  LT_TRY(split_rows(n, A, M, K, L.Kp, w.ea, w.ra, M * L.Kp, stream));
+  return split_cols(n, B, K, N, L.Kp, w.eb, w.rb, N * L.Kp, stream);
 }
 
 // One product stage over rows 0..M-1 of residue planes `ra` (plane stride a_plane) against all N
@@ -890,8 +1095,8 @@ struct ProductArgs {
   int64_t res_plane, Np;
   double* C;
   int64_t M, N, ldc, K;
-  const int* ea;  // row exponents of A (sigma)
-  const int* eb;  // column exponents of B (tau)
+  const int* ea;  // row shifts of A
+  const int* eb;  // column shifts of B
   double alpha, beta;
   int n;
 };
@@ -942,8 +1147,7 @@ int launch_product_n(const CUtensorMap& tmA, const CUtensorMap& tmB, const Probl
     const int64_t bx = ceil_div(quads, tx);
     const int64_t by = std::min<int64_t>(M, std::max<int64_t>(1, 8 * ctx->sm_count * (256 / tx) / bx));
     crt_recon_kernel<NM><<<dim3(static_cast<unsigned>(bx), static_cast<unsigned>(by)), static_cast<unsigned>(tx), 0,
-                           stream>>>(p.res, p.plane, p.Np, C, M, N, ldc, ea,
-                                                                             eb, alpha, beta, c.pa, c.pb);
+                           stream>>>(p.res, p.plane, p.Np, C, M, N, ldc, ea, eb, alpha, beta);
     LT_CUDA_TRY(cudaGetLastError());
   }
   return LT_OK;
@@ -966,7 +1170,7 @@ int run_product(const ProductArgs& a, DeviceContext* ctx, cudaStream_t stream, b
   p.ksteps = static_cast<int>(a.Kp / kBK);
   p.kgroups = static_cast<int>(ceil_div(p.ksteps, kGroupSteps));
   p.group = raster_group();
-  const Consts c = make_consts(a.n, a.K);
+  const Consts c = make_consts(a.n);
 #define LT_CALL(NM)                                                                                              \
   (p.bn == 512 ? launch_product_n<NM, 512>(tmA, tmB, p, c, a.C, a.M, a.N, a.ldc, a.ea, a.eb, a.alpha, a.beta, ctx, \
                                            stream, do_multiply, do_reconstruct)                                   \
@@ -1016,7 +1220,7 @@ int product(double* C, int64_t M, int64_t N, int64_t K, double alpha, double bet
 }
 
 // ---------------------------------------------------------------------------------------------
-// Host-resident operands (lt_dgemm_ozaki_crt_host): B is copied, its exponents and residues taken;
+// Host-resident operands (lt_dgemm_ozaki_crt_host): B is copied, its shifts and residues taken;
 // then row panels of A (and of C0 when beta != 0), whole 256-row pair blocks each, are copied on one
 // stream while earlier panels are split, multiplied and reconstructed on the caller's stream, and
 // finished panels of C go back on a third, so the PCIe copies overlap the kernels. Each panel's rows
@@ -1045,14 +1249,11 @@ int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, 
   LT_TRY(ensure_workspace(ctx, total, &base));
   LT_TRY(ensure_table(ctx->device));
   uint8_t* ws = static_cast<uint8_t*>(base);
-  auto* amax_a = reinterpret_cast<unsigned long long*>(ws + L.off_amax_a);
-  auto* amax_b = reinterpret_cast<unsigned long long*>(ws + L.off_amax_b);
-  auto* ra = reinterpret_cast<int8_t*>(ws + L.off_ra);
-  auto* rb = reinterpret_cast<int8_t*>(ws + L.off_rb);
+  const Scratch w = scratch(ws, L);
   auto* Ad = reinterpret_cast<double*>(ws + off_a);
   auto* Bd = reinterpret_cast<double*>(ws + off_b);
   auto* Cd = reinterpret_cast<double*>(ws + off_c);
-  const Consts c = make_consts(n, K);
+  const Consts c = make_consts(n);
 
   const int64_t panel = std::max<int64_t>(2 * kBM, round_up(ceil_div(M, host_panels()), 2 * kBM));
   const int64_t npanels = ceil_div(M, panel);
@@ -1075,13 +1276,11 @@ int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, 
     cuda(cudaStreamWaitEvent(d2h, e_start, 0), "wait");
     if (K > 0) cuda(cudaMemcpyAsync(Bd, B, 8 * static_cast<size_t>(K) * N, cudaMemcpyHostToDevice, h2d), "copy B");
     cuda(cudaEventRecord(e_b, h2d), "record");
-    cuda(cudaMemsetAsync(ws, 0, L.off_ra, stream), "memset");
     cuda(cudaStreamWaitEvent(stream, e_b, 0), "wait");
   }
-  if (rc == LT_OK && K > 0) rc = ozaki::exponents_cols(Bd, K, N, N, amax_b, ctx->sm_count, stream);
-  auto* ea = reinterpret_cast<int*>(ws + L.off_ea);
-  auto* eb = reinterpret_cast<int*>(ws + L.off_eb);
-  if (rc == LT_OK && K > 0) rc = split_cols(n, Bd, K, N, L.Kp, amax_b, rb, N * L.Kp, c.pb, eb, stream);
+  if (rc == LT_OK && K > 0)
+    rc = scale(nullptr, 0, Bd, N, K, L, nullptr, nullptr, w.ec_b, w.sc_b, nullptr, w.eb, c, stream);
+  if (rc == LT_OK && K > 0) rc = split_cols(n, Bd, K, N, L.Kp, w.eb, w.rb, N * L.Kp, stream);
   for (int64_t i = 0; i < npanels && rc == LT_OK; ++i) {
     const int64_t r0 = i * panel, rows = std::min(panel, M - r0);
     cudaEvent_t e_in = ev[2 * i], e_out = ev[2 * i + 1];
@@ -1099,14 +1298,14 @@ int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, 
       k0_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(Cd + r0 * N, rows, N, N, alpha, beta);
       cuda(cudaGetLastError(), "k0 kernel");
     } else {
-      rc = ozaki::exponents_rows(Ad + r0 * K, rows, K, K, amax_a + r0, ctx->sm_count, stream);
-      if (rc == LT_OK)
-        rc = split_rows(n, Ad + r0 * K, rows, K, L.Kp, amax_a + r0, ra + r0 * L.Kp, M * L.Kp, c.pa, ea + r0, stream);
+      rc = scale(Ad + r0 * K, rows, nullptr, 0, K, L, w.ec_a + r0 * L.ncha, w.sc_a + r0 * L.ncha, nullptr, nullptr,
+                 w.ea + r0, nullptr, c, stream);
+      if (rc == LT_OK) rc = split_rows(n, Ad + r0 * K, rows, K, L.Kp, w.ea + r0, w.ra + r0 * L.Kp, M * L.Kp, stream);
       if (rc != LT_OK) break;
       ProductArgs a;
-      a.ra = ra + r0 * L.Kp;
+      a.ra = w.ra + r0 * L.Kp;
       a.a_plane = M * L.Kp;
-      a.rb = rb;
+      a.rb = w.rb;
       a.b_plane = N * L.Kp;
       a.Kp = L.Kp;
       a.res = ws + L.off_rc + r0 * L.Np;
@@ -1117,8 +1316,8 @@ int host_run(const double* A, const double* B, double* C, int64_t M, int64_t N, 
       a.N = N;
       a.ldc = N;
       a.K = K;
-      a.ea = ea + r0;
-      a.eb = eb;
+      a.ea = w.ea + r0;
+      a.eb = w.eb;
       a.alpha = alpha;
       a.beta = beta;
       a.n = n;
@@ -1187,13 +1386,13 @@ size_t lt_ozaki_crt_workspace_size(int64_t M, int64_t N, int64_t K, int moduli) 
   return lt::crt::workspace_size(M, N, K, moduli);
 }
 
-int lt_ozaki_crt_info(int moduli, int64_t K, int* pa, int* pb, int* moduli_out) {
-  if (moduli < LT_OZAKI_CRT_MIN_MODULI || moduli > LT_OZAKI_CRT_MAX_MODULI || K < 0)
+int lt_ozaki_crt_info(int moduli, int* ta, int* tb, int* moduli_out) {
+  if (moduli < LT_OZAKI_CRT_MIN_MODULI || moduli > LT_OZAKI_CRT_MAX_MODULI)
     return lt::set_error(LT_ERR_INVALID_ARGUMENT, "modulus count %d outside [%d, %d]", moduli,
                          LT_OZAKI_CRT_MIN_MODULI, LT_OZAKI_CRT_MAX_MODULI);
-  const lt::crt::Consts c = lt::crt::make_consts(moduli, K);
-  if (pa != nullptr) *pa = c.pa;
-  if (pb != nullptr) *pb = c.pb;
+  const lt::crt::Consts c = lt::crt::make_consts(moduli);
+  if (ta != nullptr) *ta = c.ta;
+  if (tb != nullptr) *tb = c.tb;
   if (moduli_out != nullptr)
     for (int l = 0; l < moduli; ++l) moduli_out[l] = c.m[l];
   return lt::ok();

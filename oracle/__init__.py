@@ -77,8 +77,12 @@ def lib() -> ctypes.CDLL:
         L.oracle_ozaki_split_rows.argtypes = [_vp, _i64, _i64, _vp, _i32, _vp, _i64]
         L.oracle_ozaki_split_cols.argtypes = [_vp, _i64, _i64, _vp, _i32, _vp, _i64]
         L.oracle_ozaki_dgemm.argtypes = [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _i32, _i32]
-        L.oracle_crt_split_rows.argtypes = [_vp, _i64, _i64, _vp, _i32, _i32, _vp, _vp, _i64]
-        L.oracle_crt_split_cols.argtypes = [_vp, _i64, _i64, _vp, _i32, _i32, _vp, _vp, _i64]
+        L.oracle_crt_shift.restype = _i32
+        L.oracle_crt_shift.argtypes = [_vp, _i64, _i64, _i32, _i64]
+        L.oracle_crt_row_shifts.argtypes = [_vp, _i64, _i64, _i32, _vp]
+        L.oracle_crt_col_shifts.argtypes = [_vp, _i64, _i64, _i32, _vp]
+        L.oracle_crt_split_rows.argtypes = [_vp, _i64, _i64, _vp, _i32, _vp, _vp, _i64]
+        L.oracle_crt_split_cols.argtypes = [_vp, _i64, _i64, _vp, _i32, _vp, _vp, _i64]
         L.oracle_crt_dgemm.argtypes = [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _i32, _i32, _i32, _i32, _i32,
                                        _vp, _vp, _vp, _f64, _f64, _i32]
         L.oracle_ozaki_analytic_slices.restype = _i32
@@ -319,12 +323,19 @@ CRT_MODULI = (256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 1
 CRT_MIN, CRT_MAX = 8, 20
 
 
-def crt_constants(n: int, K: int) -> dict:
-    """Constants of the CRT form with n moduli for inner dimension K, by exact integer arithmetic:
-    Mprod, the limb width w and count nl, the limbs P[l][k] of the CRT basis
-    P_l = (Mprod/m_l) * ((Mprod/m_l)^-1 mod m_l), the limbs of Mprod, f_hi / f_lo = 2^(w k) / Mprod_d
-    (Mprod_d = the limbs summed by Horner in double), and the operand bits pa, pb with
-    K 2^(pa+pb) <= Mprod / 4 (each at most 62)."""
+def crt_norm_bits(Mp: int) -> tuple[int, int]:
+    """(ta, tb): the rows of A are scaled to 2-norm at most 2^ta and the columns of B to at most 2^tb,
+    with ta + tb = Tc the largest integer such that 2^Tc <= Mprod (1 - 2^-20) / 2 (each at most 62):
+    then |sum_k V W| <= |V|_2 |W|_2 < Mprod / 2 by the Cauchy-Schwarz inequality."""
+    Tc = (Mp * (2 ** 20 - 1) // 2 ** 21).bit_length() - 1
+    return min(62, Tc // 2), min(62, Tc - Tc // 2)
+
+
+def crt_constants(n: int) -> dict:
+    """Constants of the CRT form with n moduli, by exact integer arithmetic: Mprod, the limb width w
+    and count nl, the limbs P[l][k] of the CRT basis P_l = (Mprod/m_l) * ((Mprod/m_l)^-1 mod m_l), the
+    limbs of Mprod, f_hi / f_lo = 2^(w k) / Mprod_d (Mprod_d = the limbs summed by Horner in double),
+    and the norm bounds ta, tb (crt_norm_bits)."""
     assert CRT_MIN <= n <= CRT_MAX
     mods = CRT_MODULI[:n]
     Mp = 1
@@ -342,42 +353,52 @@ def crt_constants(n: int, K: int) -> dict:
     md = float(Mk[nl - 1])
     for k in range(nl - 2, -1, -1):
         md = md * 2.0 ** w + float(Mk[k])  # exact scaling, one rounding per step (= fma(md, 2^w, M_k))
-    T = (Mp // (2 * max(K, 1))).bit_length() - 2
-    pa, pb = min(62, T // 2), min(62, T - T // 2)
+    ta, tb = crt_norm_bits(Mp)
     return {"n": n, "mods": np.array(mods, dtype=np.int32), "Mprod": Mp, "w": w, "nl": nl, "P": Pl, "Mk": Mk,
-            "f_hi": 2.0 ** (w * (nl - 1)) / md, "f_lo": 2.0 ** (w * (nl - 2)) / md, "pa": pa, "pb": pb}
+            "f_hi": 2.0 ** (w * (nl - 1)) / md, "f_lo": 2.0 ** (w * (nl - 2)) / md, "ta": ta, "tb": tb}
 
 
 def crt_dgemm(A, B, C0, alpha, beta, n, threads: int | None = None) -> np.ndarray:
     """The CRT form restated (oracle_crt_dgemm) with n moduli."""
     M, K = A.shape
     N = B.shape[1]
-    c = crt_constants(n, K)
+    c = crt_constants(n)
     C = np.ascontiguousarray(C0).copy()
     P = np.ascontiguousarray(c["P"])
     lib().oracle_crt_dgemm(_p(np.ascontiguousarray(A)), _p(np.ascontiguousarray(B)), _p(C), M, N, K, alpha, beta, n,
-                           c["nl"], c["w"], c["pa"], c["pb"], _p(c["mods"]), _p(P), _p(c["Mk"]), c["f_hi"], c["f_lo"],
+                           c["nl"], c["w"], c["ta"], c["tb"], _p(c["mods"]), _p(P), _p(c["Mk"]), c["f_hi"], c["f_lo"],
                            threads or nthreads())
     return C
 
 
-def crt_split(A, B, n):
-    """(sigma, tau, residues of A [n][M][K], residues of B transposed [n][N][K]) of the CRT form."""
+def crt_shifts(A, B, n):
+    """(row shifts of A, column shifts of B) of the CRT form with n moduli (oracle_crt_shift)."""
     M, K = A.shape
     N = B.shape[1]
-    c = crt_constants(n, K)
+    c = crt_constants(n)
+    sa = np.empty(M, dtype=np.int32)
+    sb = np.empty(N, dtype=np.int32)
+    A, B = np.ascontiguousarray(A), np.ascontiguousarray(B)
+    lib().oracle_crt_row_shifts(_p(A), M, K, c["ta"], _p(sa))
+    lib().oracle_crt_col_shifts(_p(B), K, N, c["tb"], _p(sb))
+    return sa, sb
+
+
+def crt_split(A, B, n):
+    """(row shifts, column shifts, residues of A [n][M][K], residues of B transposed [n][N][K]) of the
+    CRT form."""
+    M, K = A.shape
+    N = B.shape[1]
+    c = crt_constants(n)
     Kp = max(K, 1)
-    sigma = np.empty(M, dtype=np.int32)
-    tau = np.empty(N, dtype=np.int32)
+    sa, sb = crt_shifts(A, B, n)
     ra = np.empty((n, M, Kp), dtype=np.int8)
     rb = np.empty((n, N, Kp), dtype=np.int8)
     L = lib()
     A, B = np.ascontiguousarray(A), np.ascontiguousarray(B)
-    L.oracle_ozaki_row_exponents(_p(A), M, K, _p(sigma))
-    L.oracle_ozaki_col_exponents(_p(B), K, N, _p(tau))
-    L.oracle_crt_split_rows(_p(A), M, K, _p(sigma), c["pa"], n, _p(c["mods"]), _p(ra), Kp)
-    L.oracle_crt_split_cols(_p(B), K, N, _p(tau), c["pb"], n, _p(c["mods"]), _p(rb), Kp)
-    return sigma, tau, ra, rb
+    L.oracle_crt_split_rows(_p(A), M, K, _p(sa), n, _p(c["mods"]), _p(ra), Kp)
+    L.oracle_crt_split_cols(_p(B), K, N, _p(sb), n, _p(c["mods"]), _p(rb), Kp)
+    return sa, sb, ra, rb
 
 
 def analytic_slices(tol: float, gap_bits: int) -> int:

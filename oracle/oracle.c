@@ -651,9 +651,18 @@ void oracle_hgemm_exact_rows(const uint16_t* A, const uint16_t* B, const uint16_
 /* Ozaki scheme II restated (integer residues and the Chinese remainder theorem), the arithmetic  */
 /* of the library's CRT form (no reference counterpart; the reference's DGEMM contract is        */
 /* routines/dgemm/dgemm.h:9, its host check routines/dgemm/dgemm.cpp:122-133):                    */
-/*  1. sigma_i, tau_j: frexp exponents of the row / column maxima (as in the slice form).        */
-/*  2. V = trunc(A[i,k] 2^(pa - sigma_i)), W = trunc(B[k,j] 2^(pb - tau_j)): integers below 2^pa  */
-/*     and 2^pb in magnitude, with K 2^(pa+pb) <= Mprod / 4 (Mprod = product of the moduli).       */
+/*  1. Scaling by a bound on each row's (column's) 2-norm. Per entry a != 0: e = its frexp        */
+/*     exponent and x = floor(|a| 2^(15-e)) + 1 (subnormals: e = -1021, x = 2^14 + 1), so         */
+/*     |a| < x 2^(e-15). Per chunk (512 consecutive k of a row of A, 128 of a column of B):       */
+/*     E_c = the largest e, S_c = the sum of ceil(x^2 4^(e-E_c)); per row: sigma = the largest    */
+/*     E_c, S = the sum over chunks of ceil(S_c / 4^(sigma-E_c)) (integer sums: their order is    */
+/*     immaterial), so that |row|_2^2 < S 2^(2 sigma - 30). The shift                            */
+/*     s = t + 15 - sigma - ceil(bitlen(S - 1) / 2) makes V = trunc(a 2^s) satisfy |V|_2 <= 2^t;  */
+/*     a row without nonzero entries takes s = 0, one holding NaN or Inf the sentinel 0x7fffffff. */
+/*  2. t = ta for the rows of A, tb for the columns of B: ta + tb = Tc, the largest integer with  */
+/*     2^Tc <= Mprod (1 - 2^-20) / 2 (Mprod = product of the moduli), split evenly, each at most  */
+/*     62. By the Cauchy-Schwarz inequality |sum_k V W| <= |V|_2 |W|_2 <= 2^Tc < Mprod / 2, with   */
+/*     a margin of 2^-21 Mprod for the rounding of the quotient estimate in step 4.              */
 /*  3. For each modulus m_l: symmetric residues of V and W, their exact integer product over K,  */
 /*     reduced to the symmetric residue c_l of sum_k V W modulo m_l.                              */
 /*  4. C' = the integer in (-Mprod/2, Mprod/2) with C' = c_l mod m_l, through FP64 limb sums:      */
@@ -661,19 +670,100 @@ void oracle_hgemm_exact_rows(const uint16_t* A, const uint16_t* B, const uint16_
 /*     t = Horner of the D_k in base 2^w. The constants (moduli, limbs P_lk of the CRT basis,     */
 /*     limbs M_k of Mprod, F = 2^(w k) / Mprod) come from the caller (oracle/__init__.py derives  */
 /*     them with exact integer arithmetic).                                                        */
-/*  5. C = fma(alpha, t 2^(sigma_i - pa) 2^(tau_j - pb), beta*C0)  (alpha * that when beta == 0); */
-/*     NaN where the row of A or the column of B holds NaN or Inf.                                */
+/*  5. C = fma(alpha, t 2^(-s_i) 2^(-s_j), beta*C0)  (alpha * that when beta == 0); NaN where the */
+/*     row of A or the column of B holds NaN or Inf.                                              */
 /* ------------------------------------------------------------------------------------------ */
 typedef struct {
-  int n, nl, w, pa, pb;
+  int n, nl, w;
   const int32_t* mods;   /* n moduli */
   const double* P;       /* n x nl limbs of the CRT basis P_l = (Mprod/m_l) ((Mprod/m_l)^-1 mod m_l) */
   const double* Mk;      /* nl limbs of Mprod */
   double f_hi, f_lo;     /* 2^(w (nl-1)) / Mprod_d and 2^(w (nl-2)) / Mprod_d */
 } crt_consts_t;
 
-/* trunc(a 2^(p - e)) from the IEEE fields; |result| < 2^p (p <= 62); zero for zero / NaN / Inf */
-static int64_t crt_scaled_int(double a, int32_t e, int p) {
+#define CRT_CHUNK_ROWS 512 /* chunk of a row of A */
+#define CRT_CHUNK_COLS 128 /* chunk of a column of B */
+#define CRT_BAD 0x7fffffff
+#define CRT_EMPTY INT32_MIN
+
+/* exponent e and 15-bit bound x of a finite nonzero a: |a| < x 2^(e-15) */
+static void crt_entry_bound(double a, int* e, uint64_t* x) {
+  uint64_t bits;
+  memcpy(&bits, &a, sizeof bits);
+  const int E = (int)((bits >> 52) & 0x7ff);
+  if (E == 0) {
+    *e = -1021;
+    *x = (1u << 14) + 1;
+  } else {
+    *e = E - 1022;
+    *x = (1u << 14) + ((bits & 0x000fffffffffffffull) >> 38) + 1;
+  }
+}
+
+/* ceil(v / 2^d) for d >= 0 and v < 2^62 */
+static uint64_t crt_ceil_shr(uint64_t v, int d) {
+  if (d == 0) return v;
+  if (d >= 63) return v != 0;
+  return (v + ((1ull << d) - 1)) >> d;
+}
+
+/* The scaling shift of one row (stride 1) or column (stride N) of K entries for the bound 2^t, with
+   chunks of `chunk` consecutive k */
+int32_t oracle_crt_shift(const double* p, int64_t stride, int64_t K, int t, int64_t chunk) {
+  const int64_t nch = (K + chunk - 1) / chunk;
+  int32_t sigma = CRT_EMPTY;
+  uint64_t S = 0;
+  int32_t* Ec = (int32_t*)malloc(sizeof(int32_t) * (size_t)(nch > 0 ? nch : 1));
+  uint64_t* Sc = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(nch > 0 ? nch : 1));
+  for (int64_t c = 0; c < nch; ++c) {
+    const int64_t k1 = (c + 1) * chunk < K ? (c + 1) * chunk : K;
+    int32_t E = CRT_EMPTY;
+    for (int64_t k = c * chunk; k < k1; ++k) {
+      const double a = p[k * stride];
+      if (!isfinite(a)) { free(Ec); free(Sc); return CRT_BAD; }
+      if (a != 0.0) {
+        int e;
+        uint64_t x;
+        crt_entry_bound(a, &e, &x);
+        if (e > E) E = e;
+      }
+    }
+    uint64_t sum = 0;
+    if (E != CRT_EMPTY) {
+      for (int64_t k = c * chunk; k < k1; ++k) {
+        const double a = p[k * stride];
+        if (a == 0.0) continue;
+        int e;
+        uint64_t x;
+        crt_entry_bound(a, &e, &x);
+        sum += crt_ceil_shr(x * x, 2 * (E - e));
+      }
+    }
+    Ec[c] = E;
+    Sc[c] = sum;
+    if (E > sigma) sigma = E;
+  }
+  if (sigma != CRT_EMPTY)
+    for (int64_t c = 0; c < nch; ++c)
+      if (Ec[c] != CRT_EMPTY) S += crt_ceil_shr(Sc[c], 2 * (sigma - Ec[c]));
+  free(Ec);
+  free(Sc);
+  if (sigma == CRT_EMPTY) return 0;
+  int b = 0;
+  while (b < 64 && ((S - 1) >> b) != 0) ++b; /* bitlen(S - 1) */
+  return t + 15 - sigma - (b + 1) / 2;
+}
+
+void oracle_crt_row_shifts(const double* A, int64_t M, int64_t K, int t, int32_t* shift) {
+  for (int64_t i = 0; i < M; ++i) shift[i] = oracle_crt_shift(A + i * K, 1, K, t, CRT_CHUNK_ROWS);
+}
+
+void oracle_crt_col_shifts(const double* B, int64_t K, int64_t N, int t, int32_t* shift) {
+  for (int64_t j = 0; j < N; ++j) shift[j] = oracle_crt_shift(B + j, N, K, t, CRT_CHUNK_COLS);
+}
+
+/* trunc(a 2^s) from the IEEE fields (|result| <= 2^62 under the shifts above); zero for zero */
+static int64_t crt_scaled_int(double a, int32_t s) {
   uint64_t bits;
   memcpy(&bits, &a, sizeof bits);
   const uint64_t mag = bits & 0x7fffffffffffffffull;
@@ -687,7 +777,7 @@ static int64_t crt_scaled_int(double a, int32_t e, int p) {
     m |= 0x0010000000000000ull;
     t = E - 1075;
   }
-  const int sh = t - e + p;
+  const int sh = t + s;
   uint64_t X;
   if (sh >= 0) X = m << sh;
   else X = (-sh >= 64) ? 0 : (m >> (-sh));
@@ -703,30 +793,26 @@ static int32_t crt_residue(int64_t v, int32_t m) {
 }
 
 /* residues of the scaled rows of A: out[l][i][k] (Kp >= K, zero padded) */
-void oracle_crt_split_rows(const double* A, int64_t M, int64_t K, const int32_t* sigma, int p, int n,
+void oracle_crt_split_rows(const double* A, int64_t M, int64_t K, const int32_t* shift, int n,
                            const int32_t* mods, int8_t* out, int64_t Kp) {
   memset(out, 0, (size_t)(n * M * Kp));
   for (int64_t i = 0; i < M; ++i) {
-    int bad = 0;
-    for (int64_t k = 0; k < K; ++k) if (!isfinite(A[i * K + k])) { bad = 1; break; }
-    if (bad) continue;
+    if (shift[i] == CRT_BAD) continue;
     for (int64_t k = 0; k < K; ++k) {
-      const int64_t v = crt_scaled_int(A[i * K + k], sigma[i], p);
+      const int64_t v = crt_scaled_int(A[i * K + k], shift[i]);
       for (int l = 0; l < n; ++l) out[((int64_t)l * M + i) * Kp + k] = (int8_t)crt_residue(v, mods[l]);
     }
   }
 }
 
 /* residues of the scaled columns of B, transposed: out[l][j][k] */
-void oracle_crt_split_cols(const double* B, int64_t K, int64_t N, const int32_t* tau, int p, int n,
+void oracle_crt_split_cols(const double* B, int64_t K, int64_t N, const int32_t* shift, int n,
                            const int32_t* mods, int8_t* out, int64_t Kp) {
   memset(out, 0, (size_t)(n * N * Kp));
   for (int64_t j = 0; j < N; ++j) {
-    int bad = 0;
-    for (int64_t k = 0; k < K; ++k) if (!isfinite(B[k * N + j])) { bad = 1; break; }
-    if (bad) continue;
+    if (shift[j] == CRT_BAD) continue;
     for (int64_t k = 0; k < K; ++k) {
-      const int64_t v = crt_scaled_int(B[k * N + j], tau[j], p);
+      const int64_t v = crt_scaled_int(B[k * N + j], shift[j]);
       for (int l = 0; l < n; ++l) out[((int64_t)l * N + j) * Kp + k] = (int8_t)crt_residue(v, mods[l]);
     }
   }
@@ -750,8 +836,7 @@ double oracle_crt_reconstruct(const int32_t* c, const crt_consts_t* cc) {
 
 typedef struct {
   const int8_t *ra, *rb;
-  const int32_t *sigma, *tau;
-  const double *A, *B;
+  const int32_t *sa, *sb; /* row / column shifts */
   double* C;
   int64_t M, N, K, Kp;
   double alpha, beta;
@@ -765,11 +850,8 @@ static void* crt_worker(void* arg) {
   const int64_t M = j->M, N = j->N, K = j->K, Kp = j->Kp;
   int32_t c[32];
   for (int64_t i = j->tid; i < M; i += j->nthreads) {
-    int row_bad = 0;
-    for (int64_t k = 0; k < K; ++k) if (!isfinite(j->A[i * K + k])) { row_bad = 1; break; }
     for (int64_t col = 0; col < N; ++col) {
-      int bad = row_bad;
-      if (!bad) for (int64_t k = 0; k < K; ++k) if (!isfinite(j->B[k * N + col])) { bad = 1; break; }
+      const int bad = j->sa[i] == CRT_BAD || j->sb[col] == CRT_BAD;
       for (int l = 0; l < cc->n; ++l) {
         const int8_t* a = j->ra + ((int64_t)l * M + i) * Kp;
         const int8_t* b = j->rb + ((int64_t)l * N + col) * Kp;
@@ -777,11 +859,12 @@ static void* crt_worker(void* arg) {
         for (int64_t k = 0; k < K; ++k) acc += (int64_t)a[k] * (int64_t)b[k];
         c[l] = crt_residue(acc, cc->mods[l]);
       }
-      const double t = scale_pow2(scale_pow2(oracle_crt_reconstruct(c, cc), j->sigma[i] - cc->pa), j->tau[col] - cc->pb);
-      double out;
-      if (j->beta != 0.0) out = fma(j->alpha, t, j->beta * j->C[i * N + col]);
-      else out = j->alpha * t;
-      if (bad) out = NAN;
+      double out = NAN;
+      if (!bad) {
+        const double t = scale_pow2(scale_pow2(oracle_crt_reconstruct(c, cc), -j->sa[i]), -j->sb[col]);
+        if (j->beta != 0.0) out = fma(j->alpha, t, j->beta * j->C[i * N + col]);
+        else out = j->alpha * t;
+      }
       j->C[i * N + col] = out;
     }
   }
@@ -789,27 +872,27 @@ static void* crt_worker(void* arg) {
 }
 
 void oracle_crt_dgemm(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
-                      double beta, int n, int nl, int w, int pa, int pb, const int32_t* mods, const double* P,
+                      double beta, int n, int nl, int w, int ta, int tb, const int32_t* mods, const double* P,
                       const double* Mk, double f_hi, double f_lo, int nthreads) {
-  crt_consts_t cc = {n, nl, w, pa, pb, mods, P, Mk, f_hi, f_lo};
+  crt_consts_t cc = {n, nl, w, mods, P, Mk, f_hi, f_lo};
   const int64_t Kp = K > 0 ? K : 1;
-  int32_t* sigma = (int32_t*)malloc(sizeof(int32_t) * (size_t)(M > 0 ? M : 1));
-  int32_t* tau = (int32_t*)malloc(sizeof(int32_t) * (size_t)(N > 0 ? N : 1));
+  int32_t* sa = (int32_t*)malloc(sizeof(int32_t) * (size_t)(M > 0 ? M : 1));
+  int32_t* sb = (int32_t*)malloc(sizeof(int32_t) * (size_t)(N > 0 ? N : 1));
   int8_t* ra = (int8_t*)malloc((size_t)(n * M * Kp + 1));
   int8_t* rb = (int8_t*)malloc((size_t)(n * N * Kp + 1));
-  oracle_ozaki_row_exponents(A, M, K, sigma);
-  oracle_ozaki_col_exponents(B, K, N, tau);
-  oracle_crt_split_rows(A, M, K, sigma, pa, n, mods, ra, Kp);
-  oracle_crt_split_cols(B, K, N, tau, pb, n, mods, rb, Kp);
+  oracle_crt_row_shifts(A, M, K, ta, sa);
+  oracle_crt_col_shifts(B, K, N, tb, sb);
+  oracle_crt_split_rows(A, M, K, sa, n, mods, ra, Kp);
+  oracle_crt_split_cols(B, K, N, sb, n, mods, rb, Kp);
   if (nthreads < 1) nthreads = 1;
   if (nthreads > 256) nthreads = 256;
   pthread_t th[256];
   crt_job_t jobs[256];
   for (int t = 0; t < nthreads; ++t) {
-    crt_job_t jb = {ra, rb, sigma, tau, A, B, C, M, N, K, Kp, alpha, beta, &cc, t, nthreads};
+    crt_job_t jb = {ra, rb, sa, sb, C, M, N, K, Kp, alpha, beta, &cc, t, nthreads};
     jobs[t] = jb;
     pthread_create(&th[t], NULL, crt_worker, &jobs[t]);
   }
   for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
-  free(sigma); free(tau); free(ra); free(rb);
+  free(sa); free(sb); free(ra); free(rb);
 }

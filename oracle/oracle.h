@@ -96,15 +96,22 @@ int oracle_ozaki_analytic_slices(double tol, int gap_bits);
 int oracle_max_gap(const double* X, int64_t rows, int64_t cols, int by_rows);
 
 /* ---- Ozaki scheme II (CRT form) restatement ---- */
-/* residues out[(l*M + i)*Kp + k] of trunc(A[i,k] 2^(p - sigma_i)) modulo mods[l] (symmetric) */
-void oracle_crt_split_rows(const double* A, int64_t M, int64_t K, const int32_t* sigma, int p, int n,
+/* scaling shift of one row (stride 1) or column (stride N) of K entries, chunks of `chunk` consecutive
+   k (512 for the rows of A, 128 for the columns of B): trunc(a 2^s) has 2-norm at most 2^t; 0 for a
+   row without nonzero entries, 0x7fffffff when it holds NaN or Inf */
+int32_t oracle_crt_shift(const double* p, int64_t stride, int64_t K, int t, int64_t chunk);
+void oracle_crt_row_shifts(const double* A, int64_t M, int64_t K, int t, int32_t* shift);
+void oracle_crt_col_shifts(const double* B, int64_t K, int64_t N, int t, int32_t* shift);
+/* residues out[(l*M + i)*Kp + k] of trunc(A[i,k] 2^shift_i) modulo mods[l] (symmetric) */
+void oracle_crt_split_rows(const double* A, int64_t M, int64_t K, const int32_t* shift, int n,
                            const int32_t* mods, int8_t* out, int64_t Kp);
 /* the same for the columns of B, transposed: out[(l*N + j)*Kp + k] */
-void oracle_crt_split_cols(const double* B, int64_t K, int64_t N, const int32_t* tau, int p, int n,
+void oracle_crt_split_cols(const double* B, int64_t K, int64_t N, const int32_t* shift, int n,
                            const int32_t* mods, int8_t* out, int64_t Kp);
-/* Full CRT-form DGEMM with the caller's constants (n moduli, nl limbs of w bits, pa / pb bits). */
+/* Full CRT-form DGEMM with the caller's constants (n moduli, nl limbs of w bits, norm bounds 2^ta
+   for the rows of A and 2^tb for the columns of B). */
 void oracle_crt_dgemm(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
-                      double beta, int n, int nl, int w, int pa, int pb, const int32_t* mods, const double* P,
+                      double beta, int n, int nl, int w, int ta, int tb, const int32_t* mods, const double* P,
                       const double* Mk, double f_hi, double f_lo, int nthreads);
 
 /* ---- learned slice selector restatements ---- */
