@@ -37,7 +37,8 @@ bool streamk_enabled() {
 //  * stream-K: the tiles x k-blocks iterations shared evenly by `cap` CTAs; each CTA pays one fill
 //    and ~3 k-blocks per extra tile its range touches, plus the partial-sum slots (mostly L2
 //    traffic) and the fix-up launch.
-// A schedule replaces no split only when it is at least 3 % faster.
+// A schedule replaces no split only when it is at least 3 % faster. Stream-K is considered only
+// while enabled (LIBTHOM_FP64_STREAMK), so turning it off falls back to the best remaining schedule.
 Schedule choose_schedule(int64_t tiles, int64_t cap, int64_t M, int64_t N, int64_t K, int bm, int bn) {
   Schedule best;
   const int64_t nkb = (K + 15) / 16;
@@ -54,7 +55,7 @@ Schedule choose_schedule(int64_t tiles, int64_t cap, int64_t M, int64_t N, int64
     if (t < std::min(best.t, plain * 0.97)) best = Schedule{S, false, t};
   }
   const int64_t total = tiles * nkb;
-  if (total >= 2) {
+  if (total >= 2 && streamk_enabled()) {
     const int64_t G = std::min(cap, total);
     const int64_t per = (total + G - 1) / G;
     const int64_t touched = 1 + (per + nkb - 1) / nkb;
@@ -99,7 +100,7 @@ int launch(const Params& p0, cudaStream_t stream, DeviceContext* ctx) {
   const int64_t nkb = (p.K + Cfg::BK - 1) / Cfg::BK;
   const Schedule sched = choose_schedule(tiles, cap, p.M, p.N, p.K, Cfg::BM, Cfg::BN);
   p.splits = sched.splits;
-  p.streamk = (sched.streamk && streamk_enabled()) ? 1 : 0;
+  p.streamk = sched.streamk ? 1 : 0;
   p.W = nullptr;
   int64_t grid = tiles * p.splits < cap ? tiles * p.splits : cap;
   if (p.streamk) grid = std::min(cap, tiles * nkb);
