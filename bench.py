@@ -649,7 +649,8 @@ def run_ours(args) -> None:
                      "frac_of_bf16x2": achieved / (2.0 * bf16) if bf16 else None,
                      "traffic": traffic,
                      "algorithmic": f"{n} INT8 residue products x 2MNK = {int8_ops:.4g} ops per launch"},
-        "roofline_split": {"bound": "hbm", "kernels": "amax_both_kernel, crt_split_rows_kernel, crt_split_cols_kernel",
+        "roofline_split": {"bound": "hbm",
+                           "kernels": "crt_stats_kernel, crt_shift_kernel, crt_split_rows_kernel, crt_split_cols_kernel",
                            "achieved": split_bytes / (split_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
                            "frac": split_bytes / (split_ms * 1e-3) / 1e9 / hbm if hbm else None,
                            "algorithmic": f"(16 + {n}) (MK + KN) bytes: A, B read twice, {n} residue bytes written"},
@@ -669,9 +670,9 @@ def run_ours(args) -> None:
                         "the call, row panels overlapping the copies with the kernels"},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
-        # per timed step: amax_both_kernel, crt_split_rows_kernel, crt_split_cols_kernel, crt_pair_kernel,
-        # crt_recon_kernel
-        "gpu_launches": 5 * args.steps,
+        # per timed step: crt_stats_kernel, crt_shift_kernel, crt_split_rows_kernel, crt_split_cols_kernel,
+        # crt_pair_kernel, crt_recon_kernel
+        "gpu_launches": 6 * args.steps,
     }
     line.update(extra)
     print(json.dumps(line), flush=True)
