@@ -103,14 +103,15 @@ struct Consts {
   uint32_t coef_lo[kMaxMod], coef_hi[kMaxMod];  // bytes (2^(8d) mod m), d = 0..3 and 4..7
   uint32_t add[kMaxMod];                        // m - (2^62 mod m)
   uint32_t split_magic[kMaxMod];                // ceil(2^32 / m)
-  // INT32 accumulators -> residues: y = (acc >> 16) c16 + (acc & 0xffff) + bias, q = umulhi(y, magic) >> 7
-  int32_t c16[kMaxMod];           // 2^16 mod m
-  int32_t bias[kMaxMod];          // m ceil(2^23 / m): y + bias in [0, 2^25)
+  // INT32 accumulators -> residues in [0, m): y = dp2a(acc ^ 2^31, 1 | c16 << 8, acc_add) < 2^24,
+  // q = umulhi(y, magic) >> 7
+  uint32_t c16[kMaxMod];          // 2^16 mod m
+  uint32_t acc_add[kMaxMod];      // m - (2^31 mod m)
   uint32_t drain_magic[kMaxMod];  // ceil(2^39 / m)
   // reconstruction
   double P[kMaxMod][4];  // limbs of the CRT basis
   double Mk[4];          // limbs of Mprod
-  double Kc[4];          // -128 sum_l P_lk (residues are stored as c + 128)
+  double Kc[4];          // -128 sum_l P_lk, plus 128 in limb 0 (residues r in [0, m) enter as r - 128)
   double f_hi, f_lo;
 };
 
@@ -190,8 +191,8 @@ Consts make_consts(int n) {
     c.coef_hi[l] = hi;
     c.add[l] = m - pow2_mod(62, m);
     c.split_magic[l] = static_cast<uint32_t>(((uint64_t(1) << 32) + m - 1) / m);
-    c.c16[l] = static_cast<int32_t>(pow2_mod(16, m));
-    c.bias[l] = static_cast<int32_t>(m * (((uint32_t(1) << 23) + m - 1) / m));
+    c.c16[l] = pow2_mod(16, m);
+    c.acc_add[l] = m - pow2_mod(31, m);
     c.drain_magic[l] = static_cast<uint32_t>(((uint64_t(1) << 39) + m - 1) / m);
     Big Ml = Mp;
     Ml.divmod_small(m);
@@ -205,7 +206,7 @@ Consts make_consts(int n) {
     c.Mk[k] = static_cast<double>(Mp.bits(c.w * k, c.w));
     int64_t s = 0;
     for (int l = 0; l < n; ++l) s += static_cast<int64_t>(c.P[l][k]);
-    c.Kc[k] = -128.0 * static_cast<double>(s);
+    c.Kc[k] = -128.0 * static_cast<double>(s) + (k == 0 ? 128.0 : 0.0);
   }
   double md = c.Mk[c.nl - 1];
   for (int k = c.nl - 2; k >= 0; --k) md = std::fma(md, std::ldexp(1.0, c.w), c.Mk[k]);
@@ -602,49 +603,54 @@ __device__ __forceinline__ void tile_coords(const Problem& p, int64_t t, int* m0
   *n0 = static_cast<int>((in_group / gsize) * p.bn);
 }
 
-// Symmetric residue of an INT32 accumulator modulo c.m[l] (an odd modulus), from
-// y = (acc >> 16)(2^16 mod m) + (acc & 0xffff) + m ceil(2^23 / m), congruent to acc and in [0, 2^25):
-// floor(y / m) = (y ceil(2^39 / m)) >> 39 exactly (the error term is below y m / 2^39 < 1 / m).
-__device__ __forceinline__ int sym_residue_odd(int32_t acc, int m, int c16, int bias, uint32_t magic) {
-  const uint32_t y = static_cast<uint32_t>((acc >> 16) * c16 + (acc & 0xffff) + bias);
-  const int q = static_cast<int>(__umulhi(y, magic) >> 7);
-  const int r = static_cast<int>(y) - q * m;
-  return r > (m >> 1) ? r - m : r;
+// Residue in [0, m) of an INT32 accumulator modulo an odd modulus m: U = acc + 2^31 (acc ^ 2^31 as an
+// unsigned word) has 16-bit halves hi, lo, and y = lo + hi (2^16 mod m) + (m - 2^31 mod m), one dp2a,
+// is congruent to acc and below 2^24; floor(y / m) = (y ceil(2^39 / m)) >> 39 exactly (the error term
+// is below y m / 2^39 < 1 / m).
+__device__ __forceinline__ uint32_t residue_odd(uint32_t acc, uint32_t coef, uint32_t add, uint32_t magic,
+                                                uint32_t m) {
+  const uint32_t y = __dp2a_lo(acc ^ 0x80000000u, coef, add);
+  return y - (__umulhi(y, magic) >> 7) * m;
 }
 
-// 32 accumulators of one row -> their residues modulo c.m[l], stored as bytes c + 128, two 16-byte
-// words. For accumulation group g > 0 the residue of the previous groups (already in `dst`) is added.
+// 32 accumulators of one row -> their residues r in [0, m) modulo m = c.m[l], stored as bytes, two
+// 16-byte words. For accumulation group g > 0 the residue of the previous groups (already in `dst`)
+// is added modulo m.
 __device__ __forceinline__ void drain_chunk(const uint32_t (&v)[32], int l, bool add_prev, const Consts& c,
                                             uint4* dst) {
-  uint32_t prev[8] = {};
-  if (add_prev) {
-    const uint4 a = dst[0], b = dst[1];
-    prev[0] = a.x; prev[1] = a.y; prev[2] = a.z; prev[3] = a.w;
-    prev[4] = b.x; prev[5] = b.y; prev[6] = b.z; prev[7] = b.w;
-  }
-  const int m = c.m[l], c16 = c.c16[l], bias = c.bias[l];
-  const uint32_t magic = c.drain_magic[l];
   uint32_t w[8];
+  if (l == 0) {  // m = 256: the low byte
 #pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    uint32_t word = 0;
+    for (int q = 0; q < 8; ++q)
+      w[q] = __byte_perm(__byte_perm(v[4 * q], v[4 * q + 1], 0x0040), __byte_perm(v[4 * q + 2], v[4 * q + 3], 0x0040),
+                         0x5410);
+  } else {
+    const uint32_t m = static_cast<uint32_t>(c.m[l]), coef = 1u | (c.c16[l] << 8), add = c.acc_add[l],
+                   magic = c.drain_magic[l];
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int32_t acc = static_cast<int32_t>(v[4 * q + b]);
-      int r;
-      if (l == 0) {
-        r = static_cast<int8_t>(acc & 0xff);
-        if (add_prev) r = static_cast<int8_t>((r + static_cast<int>((prev[q] >> (8 * b)) & 0xffu) - 128) & 0xff);
-      } else {
-        r = sym_residue_odd(acc, m, c16, bias, magic);
-        if (add_prev) {
-          r += static_cast<int>((prev[q] >> (8 * b)) & 0xffu) - 128;  // |r| <= m - 1
-          r = r > (m >> 1) ? r - m : (r < -(m >> 1) ? r + m : r);
-        }
-      }
-      word |= static_cast<uint32_t>(r + 128) << (8 * b);
+    for (int q = 0; q < 8; ++q) {
+      const uint32_t r0 = residue_odd(v[4 * q], coef, add, magic, m);
+      const uint32_t r1 = residue_odd(v[4 * q + 1], coef, add, magic, m);
+      const uint32_t r2 = residue_odd(v[4 * q + 2], coef, add, magic, m);
+      const uint32_t r3 = residue_odd(v[4 * q + 3], coef, add, magic, m);
+      w[q] = __byte_perm(__byte_perm(r0, r1, 0x0040), __byte_perm(r2, r3, 0x0040), 0x5410);
     }
-    w[q] = word;
+  }
+  if (add_prev) {  // K beyond one INT32 group: add the earlier groups' residues modulo m
+    const uint4 a = dst[0], b = dst[1];
+    const uint32_t prev[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    const uint32_t m = static_cast<uint32_t>(c.m[l]);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      uint32_t word = 0;
+#pragma unroll
+      for (int b4 = 0; b4 < 4; ++b4) {
+        uint32_t r = ((w[q] >> (8 * b4)) & 0xffu) + ((prev[q] >> (8 * b4)) & 0xffu);
+        r = l == 0 ? (r & 0xffu) : (r >= m ? r - m : r);
+        word |= r << (8 * b4);
+      }
+      w[q] = word;
+    }
   }
   dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
   dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
@@ -826,18 +832,26 @@ __global__ void __launch_bounds__(kThreads, 1)
           tc_fence_after();
           const uint32_t lane_base =
               tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + buf * kBN + colhalf * (BN / 2);
+          // Chunks of 32 columns, the TMEM load of the next issued before the current one is reduced;
+          // the accumulator goes back to the MMA warp once the last load has landed.
+          constexpr int kChunks = BN / 64;
+          uint32_t va[32], vb[32];
+          tmem_ld_32x32b_x32(lane_base, va);
+          tmem_ld_wait(va);
 #pragma unroll 1
-          for (int ch = 0; ch < BN / 64; ++ch) {
-            uint32_t v[32];
-            tmem_ld_32x32b_x32(lane_base + static_cast<uint32_t>(ch * 32), v);
-            tmem_ld_wait();
-            if (ch == BN / 64 - 1) {
-              // The whole accumulator is in registers: hand the buffer back before the last stores.
+          for (int ch = 0; ch < kChunks; ch += 2) {
+            tmem_ld_32x32b_x32(lane_base + static_cast<uint32_t>((ch + 1) * 32), vb);
+            drain_chunk(va, l, g > 0, c, reinterpret_cast<uint4*>(dst + ch * 32));
+            tmem_ld_wait(vb);
+            if (ch + 2 < kChunks) {
+              tmem_ld_32x32b_x32(lane_base + static_cast<uint32_t>((ch + 2) * 32), va);
+            } else {
               tc_fence_before();
               __syncwarp();
               if (lane == 0) mbar_arrive_cluster(acc_empty_r0[buf]);
             }
-            drain_chunk(v, l, g > 0, c, reinterpret_cast<uint4*>(dst + ch * 32));
+            drain_chunk(vb, l, g > 0, c, reinterpret_cast<uint4*>(dst + (ch + 1) * 32));
+            if (ch + 2 < kChunks) tmem_ld_wait(va);
           }
         }
       }

@@ -664,9 +664,10 @@ void oracle_hgemm_exact_rows(const uint16_t* A, const uint16_t* B, const uint16_
 /*     62. By the Cauchy-Schwarz inequality |sum_k V W| <= |V|_2 |W|_2 <= 2^Tc < Mprod / 2, with   */
 /*     a margin of 2^-21 Mprod for the rounding of the quotient estimate in step 4.              */
 /*  3. For each modulus m_l: symmetric residues of V and W, their exact integer product over K,  */
-/*     reduced to the symmetric residue c_l of sum_k V W modulo m_l.                              */
-/*  4. C' = the integer in (-Mprod/2, Mprod/2) with C' = c_l mod m_l, through FP64 limb sums:      */
-/*     L_k = sum_l c_l P_lk (exact), Q = rint(L_hi F_hi + L_lo F_lo), D_k = fma(-Q, M_k, L_k),     */
+/*     reduced to its residue r_l in [0, m_l).                                                    */
+/*  4. C' = the integer in (-Mprod/2, Mprod/2) with C' = r_l mod m_l, through FP64 limb sums:      */
+/*     L_k = K_k + sum_l r_l P_lk (exact; K_k = -128 sum_l P_lk, +128 in limb 0, keeps them below */
+/*     2^53), Q = rint(L_hi F_hi + L_lo F_lo), D_k = fma(-Q, M_k, L_k),                           */
 /*     t = Horner of the D_k in base 2^w. The constants (moduli, limbs P_lk of the CRT basis,     */
 /*     limbs M_k of Mprod, F = 2^(w k) / Mprod) come from the caller (oracle/__init__.py derives  */
 /*     them with exact integer arithmetic).                                                        */
@@ -818,12 +819,19 @@ void oracle_crt_split_cols(const double* B, int64_t K, int64_t N, const int32_t*
   }
 }
 
-/* C' (as a double) from the residues c[0..n-1] */
-double oracle_crt_reconstruct(const int32_t* c, const crt_consts_t* cc) {
+/* C' (as a double) from the residues r[0..n-1] in [0, m_l): the limb sums start from
+   K_k = -128 sum_l P_lk (+128 in limb 0), so that L = sum_l (r_l - 128) P_l + 128 = C' (mod Mprod)
+   (sum_l P_l = 1 mod Mprod) and every partial sum stays below 2^53 in magnitude */
+double oracle_crt_reconstruct(const int32_t* r, const crt_consts_t* cc) {
   double L[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (int l = 0; l < cc->n; ++l)
-    for (int k = 0; k < cc->nl; ++k) L[k] = fma((double)c[l], cc->P[l * cc->nl + k], L[k]);
   const int nl = cc->nl;
+  for (int k = 0; k < nl; ++k) {
+    int64_t sp = 0;
+    for (int l = 0; l < cc->n; ++l) sp += (int64_t)cc->P[l * nl + k];
+    L[k] = -128.0 * (double)sp + (k == 0 ? 128.0 : 0.0);
+  }
+  for (int l = 0; l < cc->n; ++l)
+    for (int k = 0; k < nl; ++k) L[k] = fma((double)r[l], cc->P[l * nl + k], L[k]);
   const double s = fma(L[nl - 1], cc->f_hi, L[nl - 2] * cc->f_lo);
   const double Q = rint(s);
   double D[8];
@@ -857,7 +865,7 @@ static void* crt_worker(void* arg) {
         const int8_t* b = j->rb + ((int64_t)l * N + col) * Kp;
         int64_t acc = 0;
         for (int64_t k = 0; k < K; ++k) acc += (int64_t)a[k] * (int64_t)b[k];
-        c[l] = crt_residue(acc, cc->mods[l]);
+        c[l] = (int32_t)(((acc % cc->mods[l]) + cc->mods[l]) % cc->mods[l]); /* residue in [0, m) */
       }
       double out = NAN;
       if (!bad) {

@@ -28,25 +28,34 @@ def _sym(x: int, m: int) -> int:
 
 @pytest.mark.parametrize("n", [8, 10, 11, 13, 15, 16, 17, 20])
 def test_reconstruction_is_exact(oracle_mod, n):
-    """The limb sums stay below 2^53 and Q = rint(L_hi F_hi + L_lo F_lo) is exact for every integer
-    below Mprod (1 - 2^-20) / 2 in magnitude (the bound the scaling guarantees); values at the edges
-    included."""
+    """With residues r_l in [0, m_l) (what the product stores), the limb sums started from
+    K_k = -128 sum_l P_lk (+128 in limb 0) stay below 2^53, and Q = rint(L_hi F_hi + L_lo F_lo) is
+    exact for every integer below Mprod (1 - 2^-20) / 2 in magnitude (the bound the scaling
+    guarantees); values at the edges and every residue at its extremes included."""
     c = oracle_mod.crt_constants(n)
-    Mp, mods, nl = c["Mprod"], [int(m) for m in c["mods"]], c["nl"]
+    Mp, mods, nl, w = c["Mprod"], [int(m) for m in c["mods"]], c["nl"], c["w"]
     edge = Mp * (2 ** 20 - 1) // 2 ** 21
     rng = random.Random(n)
     xs = [0, 1, -1, edge, -edge, edge - 1, -edge + 1] + [rng.randrange(-edge, edge + 1) for _ in range(400)]
     xs += [rng.randrange(-2 ** 40, 2 ** 40) for _ in range(100)]
+    Kc = [-128.0 * float(sum(int(c["P"][l][k]) for l in range(n))) + (128.0 if k == 0 else 0.0) for k in range(nl)]
     for x in xs:
-        res = [_sym(x, m) for m in mods]
-        L = [0.0] * nl
+        res = [x % m for m in mods]
+        L = list(Kc)
         for l in range(n):
             for k in range(nl):
-                L[k] = float(res[l]) * float(c["P"][l][k]) + L[k]
+                L[k] = float(res[l]) * float(c["P"][l][k]) + L[k]  # exact: the products and sums are integers
                 assert abs(L[k]) < 2.0 ** 53
+        Lint = sum(int(L[k]) << (w * k) for k in range(nl))
         Q = round(L[nl - 1] * c["f_hi"] + L[nl - 2] * c["f_lo"])
-        S = sum(r * ((Mp // m) * pow((Mp // m) % m, -1, m)) for r, m in zip(res, mods))
-        assert S - Q * Mp == x
+        assert Lint - Q * Mp == x
+    # limb sums at their extremes: every residue 0 (most negative) or m - 1 (largest)
+    for r in (0, None):
+        L = list(Kc)
+        for l in range(n):
+            for k in range(nl):
+                L[k] += float(mods[l] - 1 if r is None else r) * float(c["P"][l][k])
+                assert abs(L[k]) < 2.0 ** 53
 
 
 def test_norm_bounds_respect_the_modulus_product(oracle_mod):
