@@ -310,6 +310,20 @@ int lt_ozaki_select_slices(const double* A, const double* B, int64_t M, int64_t 
  * learned choice was used and no gap was measured). */
 int lt_ozaki_select_info(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol,
                          int* slices, int* learned, int* gap_bits, void* stream);
+/* Selection on the device (no reference counterpart): a plan holds one problem's pointers and sizes
+ * (the data behind them may change between runs) and a CUDA graph that runs the selector's feature
+ * kernels and network, the exponent-gap pass only when the network is not confident, picks the slice
+ * count on the device with the same rule as lt_ozaki_select_slices, and runs the slice form's split
+ * and product for that count through a switch node. A run is one graph launch with no host
+ * synchronisation (replayable; it can be captured into a caller's graph as a child). The workspace is
+ * sized for LT_OZAKI_MAX_SLICES slices. lt_ozaki_auto_plan_choice reads the last run's choice
+ * (synchronous). */
+typedef struct lt_ozaki_auto_plan lt_ozaki_auto_plan;
+int lt_ozaki_auto_plan_create(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
+                              double alpha, double beta, double tol, lt_ozaki_auto_plan** plan);
+int lt_ozaki_auto_plan_run(lt_ozaki_auto_plan* plan, void* stream);
+int lt_ozaki_auto_plan_choice(lt_ozaki_auto_plan* plan, int* slices, int* learned);
+void lt_ozaki_auto_plan_destroy(lt_ozaki_auto_plan* plan);
 
 /* ---- harness helpers (replace the reference's cuRAND fill, routines/dgemm/dgemm.cpp:100-119) -- */
 /* X[i] = u 2^e, u ~ U[-1,1), e ~ U{-phi..phi}; counter-based, identical to the CPU oracle. */

@@ -133,6 +133,10 @@ SIGNATURES = {
     "lt_ozaki_analytic_slices": (_i32, [_f64, _i32]),
     "lt_ozaki_gap_bits": (_i32, [_vp, _vp, _i64, _i64, _i64, _c.POINTER(_i32), _vp]),
     "lt_ozaki_select_slices": (_i32, [_vp, _vp, _i64, _i64, _i64, _f64, _c.POINTER(_i32), _vp]),
+    "lt_ozaki_auto_plan_create": (_i32, [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _f64, _c.POINTER(_vp)]),
+    "lt_ozaki_auto_plan_run": (_i32, [_vp, _vp]),
+    "lt_ozaki_auto_plan_choice": (_i32, [_vp, _c.POINTER(_i32), _c.POINTER(_i32)]),
+    "lt_ozaki_auto_plan_destroy": (None, [_vp]),
     "lt_ozaki_select_info": (_i32, [_vp, _vp, _i64, _i64, _i64, _f64, _c.POINTER(_i32), _c.POINTER(_i32),
                                     _c.POINTER(_i32), _vp]),
     "lt_fill": (_i32, [_vp, _i64, _u64, _u64, _i32, _vp]),
@@ -218,6 +222,37 @@ def dgemm_fp64(A, B, C, M, N, K, alpha=1.0, beta=0.0, stream=None, config: int =
     else:
         check(lib().lt_dgemm_fp64_config(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, config,
                                          _stream(stream)))
+
+
+class OzakiAutoPlan:
+    """lt_ozaki_auto_plan: slice selection and the slice form in one CUDA graph (device-side choice).
+    Holds the tensors' pointers; run() replays the graph on `stream` without host synchronisation."""
+
+    def __init__(self, A, B, C, M, N, K, alpha, beta, tol):
+        self._h = ctypes.c_void_p()
+        self._keep = (A, B, C)
+        check(lib().lt_ozaki_auto_plan_create(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, tol,
+                                              ctypes.byref(self._h)))
+
+    def run(self, stream=None) -> None:
+        check(lib().lt_ozaki_auto_plan_run(self._h, _stream(stream)))
+
+    def choice(self) -> tuple[int, bool]:
+        """(slice count, learned?) of the last run (synchronous)."""
+        s, learned = ctypes.c_int(), ctypes.c_int()
+        check(lib().lt_ozaki_auto_plan_choice(self._h, ctypes.byref(s), ctypes.byref(learned)))
+        return s.value, bool(learned.value)
+
+    def close(self) -> None:
+        if self._h:
+            lib().lt_ozaki_auto_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def dgemm_ozaki(A, B, C, M, N, K, alpha=1.0, beta=0.0, slices=8, stream=None, workspace=None) -> None:

@@ -35,6 +35,13 @@ int selector_infer(const double* A, const double* B, int64_t M, int64_t N, int64
                    float* feat_dev, float* probs_host, cudaStream_t stream);
 int gap_into(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int* out, void* scratch,
              cudaStream_t stream);
+// A plan's own feature scratch (selector_stats.cu): size, initial state, the two feature kernels
+// without host synchronisation, and the device address of the class probabilities they leave.
+size_t selector_scratch_bytes();
+int selector_scratch_init(void* scratch, cudaStream_t stream);
+int selector_features_async(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol,
+                            const float* params, void* scratch, cudaStream_t stream);
+const float* selector_probs(const void* scratch);
 
 namespace tuner {
 // Tuned FP64 config for this shape class, or -1.

@@ -490,3 +490,238 @@ float dgemm_auto(const double* A, const double* B, double* C, size_t M, size_t N
 }
 
 }  // extern "C"
+
+// ---- slice selection on the device: a CUDA graph with conditional nodes (no reference counterpart)
+// One plan per problem (pointers and sizes, like a grouped plan; the data may change between runs).
+// Its graph runs the sampled-feature kernels and the network, then
+//   decide_learned: the learned count if the network is confident (the same rule as `decide`),
+//                   otherwise it turns on the IF node below;
+//   IF (not confident): the exponent-gap pass over all of A and B;
+//   decide_final: the analytic count from the gaps when the network was not confident; sets the
+//                 SWITCH node's value to slices - 1;
+//   SWITCH: body s - 1 runs the slice form's split and product with s slices.
+// So the choice never leaves the device: one graph launch per call, no host synchronisation, and the
+// result is what lt_ozaki_select_slices followed by lt_dgemm_ozaki computes (same rule, same kernels).
+namespace lt {
+namespace sel {
+
+__device__ bool decide_dev(const float* probs, int* slices) {
+  int top = 0;
+  for (int c = 1; c < C; ++c)
+    if (probs[c] > probs[top]) top = c;
+  if (!(probs[top] >= 0.5f) || top == C - 1) return false;
+  float cdf = 0.f;
+  for (int c = 0; c < C - 1; ++c) {
+    cdf += probs[c];
+    if (cdf >= 0.9f) {
+      *slices = 3 + c;
+      return true;
+    }
+  }
+  return false;
+}
+
+__device__ int analytic_dev(double tol, int gap_bits) {
+  for (int s = 1; s <= LT_OZAKI_MAX_SLICES; ++s)
+    if ((s + 3) * ldexp(1.0, gap_bits + 4 - 8 * s) + 4.0 * ldexp(1.0, -53) <= tol) return s;
+  return LT_OZAKI_MAX_SLICES;
+}
+
+// decision = {slices, learned}; the gap pair is zeroed for the fallback pass.
+__global__ void auto_decide_learned_kernel(const float* probs, int use_net, int* decision, int* gap,
+                                           cudaGraphConditionalHandle fallback) {
+  int s = 0;
+  const bool learned = use_net != 0 && decide_dev(probs, &s);
+  decision[0] = s;
+  decision[1] = learned ? 1 : 0;
+  gap[0] = 0;
+  gap[1] = 0;
+  cudaGraphSetConditional(fallback, learned ? 0u : 1u);
+}
+
+__global__ void auto_decide_final_kernel(double tol, int* decision, const int* gap, cudaGraphConditionalHandle which) {
+  if (decision[1] == 0) decision[0] = analytic_dev(tol, gap[0] + gap[1]);
+  cudaGraphSetConditional(which, static_cast<unsigned>(decision[0] - 1));
+}
+
+}  // namespace sel
+}  // namespace lt
+
+struct lt_ozaki_auto_plan {
+  int device = -1;
+  const double* A = nullptr;
+  const double* B = nullptr;
+  double* C = nullptr;
+  int64_t M = 0, N = 0, K = 0;
+  uint8_t* mem = nullptr;  // feature scratch | gap scratch | gap pair, decision | slice workspace
+  int* decision = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+// Adds a conditional node after the work captured so far on `s` and makes it the capture's only
+// dependency; its body graphs are returned through `bodies`.
+int add_conditional(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                    unsigned size, cudaGraph_t** bodies) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  LT_CUDA_TRY(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &ndeps));
+  if (st != cudaStreamCaptureStatusActive) return lt::set_error(LT_ERR_CUDA, "auto plan: capture not active");
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = type;
+  p.conditional.size = size;
+  cudaGraphNode_t node;
+  LT_CUDA_TRY(cudaGraphAddNode(&node, g, deps, ndeps, &p));
+  LT_CUDA_TRY(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  *bodies = p.conditional.phGraph_out;
+  return LT_OK;
+}
+
+// Captures fn(stream) into the (empty) body graph `body` on stream `s`.
+template <class F>
+int capture_body(cudaStream_t s, cudaGraph_t body, F fn) {
+  LT_CUDA_TRY(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  const int rc = fn(s);
+  cudaGraph_t out = body;
+  const cudaError_t e = cudaStreamEndCapture(s, &out);
+  if (rc != LT_OK) return rc;
+  LT_CUDA_TRY(e);
+  return LT_OK;
+}
+
+int build_auto_plan(lt_ozaki_auto_plan* p, double alpha, double beta, double tol, cudaStream_t s, cudaStream_t sb) {
+  const float* shared_params = nullptr;
+  LT_TRY(lt::sel::device_params(&shared_params));
+  const size_t par_bytes = (sizeof(float) * lt::sel::P + 255) / 256 * 256;
+  const size_t sc_bytes = (lt::selector_scratch_bytes() + 255) / 256 * 256;
+  const size_t gap_bytes = (8 * static_cast<size_t>(p->M + p->N) + 255) / 256 * 256;
+  const size_t ws_bytes = lt_ozaki_workspace_size(p->M, p->N, p->K, LT_OZAKI_MAX_SLICES);
+  LT_CUDA_TRY(cudaMalloc(&p->mem, par_bytes + sc_bytes + gap_bytes + 256 + ws_bytes));
+  // the plan keeps the weights installed when it was created
+  float* params = shared_params != nullptr ? reinterpret_cast<float*>(p->mem) : nullptr;
+  void* sc = p->mem + par_bytes;
+  void* gap_scratch = p->mem + par_bytes + sc_bytes;
+  int* gap = reinterpret_cast<int*>(p->mem + par_bytes + sc_bytes + gap_bytes);
+  p->decision = gap + 2;
+  void* ws = p->mem + par_bytes + sc_bytes + gap_bytes + 256;
+  if (params != nullptr)
+    LT_CUDA_TRY(cudaMemcpyAsync(params, shared_params, sizeof(float) * lt::sel::P, cudaMemcpyDeviceToDevice, s));
+  LT_TRY(lt::selector_scratch_init(sc, s));
+  LT_CUDA_TRY(cudaMemsetAsync(gap, 0, 256, s));
+  LT_CUDA_TRY(cudaStreamSynchronize(s));
+
+  LT_CUDA_TRY(cudaGraphCreate(&p->graph, 0));
+  cudaGraphConditionalHandle h_fallback, h_slices;
+  LT_CUDA_TRY(cudaGraphConditionalHandleCreate(&h_fallback, p->graph, 1, cudaGraphCondAssignDefault));
+  // default: no body (a value past the switch's bodies), set by decide_final on every run
+  LT_CUDA_TRY(cudaGraphConditionalHandleCreate(&h_slices, p->graph, LT_OZAKI_MAX_SLICES, cudaGraphCondAssignDefault));
+
+  const double *A = p->A, *B = p->B;
+  double* C = p->C;
+  const int64_t M = p->M, N = p->N, K = p->K;
+  LT_CUDA_TRY(cudaStreamBeginCaptureToGraph(s, p->graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  int rc = LT_OK;
+  cudaGraph_t* fb_body = nullptr;
+  cudaGraph_t* sw_bodies = nullptr;
+  if (params != nullptr) rc = lt::selector_features_async(A, B, M, N, K, tol, params, sc, s);
+  if (rc == LT_OK) {
+    lt::sel::auto_decide_learned_kernel<<<1, 1, 0, s>>>(lt::selector_probs(sc), params != nullptr ? 1 : 0,
+                                                       p->decision, gap, h_fallback);
+    if (cudaGetLastError() != cudaSuccess) rc = lt::set_error(LT_ERR_CUDA, "auto plan: decide launch");
+  }
+  if (rc == LT_OK) rc = add_conditional(s, h_fallback, cudaGraphCondTypeIf, 1, &fb_body);
+  if (rc == LT_OK) {
+    lt::sel::auto_decide_final_kernel<<<1, 1, 0, s>>>(tol, p->decision, gap, h_slices);
+    if (cudaGetLastError() != cudaSuccess) rc = lt::set_error(LT_ERR_CUDA, "auto plan: decide launch");
+  }
+  if (rc == LT_OK) rc = add_conditional(s, h_slices, cudaGraphCondTypeSwitch, LT_OZAKI_MAX_SLICES, &sw_bodies);
+  cudaGraph_t captured = p->graph;
+  const cudaError_t e = cudaStreamEndCapture(s, &captured);
+  if (rc != LT_OK) return rc;
+  LT_CUDA_TRY(e);
+
+  LT_TRY(capture_body(sb, fb_body[0],
+                      [&](cudaStream_t st) { return lt::gap_into(A, B, M, N, K, gap, gap_scratch, st); }));
+  for (int b = 0; b < LT_OZAKI_MAX_SLICES; ++b) {
+    const int slices = b + 1;
+    LT_TRY(capture_body(sb, sw_bodies[b], [&](cudaStream_t st) {
+      int r = lt_ozaki_split(A, B, M, N, K, slices, ws, ws_bytes, st);
+      if (r == LT_OK) r = lt_ozaki_product(C, M, N, K, alpha, beta, slices, ws, ws_bytes, st);
+      return r;
+    }));
+  }
+  LT_CUDA_TRY(cudaGraphInstantiate(&p->exec, p->graph, 0));
+  return LT_OK;
+}
+
+void destroy_auto_plan(lt_ozaki_auto_plan* p) {
+  if (p == nullptr) return;
+  if (p->exec != nullptr) cudaGraphExecDestroy(p->exec);
+  if (p->graph != nullptr) cudaGraphDestroy(p->graph);
+  if (p->mem != nullptr) cudaFree(p->mem);
+  delete p;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lt_ozaki_auto_plan_create(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
+                              double alpha, double beta, double tol, lt_ozaki_auto_plan** plan) {
+  if (plan == nullptr) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_ozaki_auto_plan_create: null plan");
+  *plan = nullptr;
+  if (M <= 0 || N <= 0 || K <= 0 || A == nullptr || B == nullptr || C == nullptr || !(tol > 0.0))
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_ozaki_auto_plan_create: bad arguments");
+  if (((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(C)) & 7) != 0)
+    return lt::set_error(LT_ERR_UNALIGNED, "matrix pointers must be 8-byte aligned");
+  lt::DeviceContext* ctx = lt::context();
+  if (ctx == nullptr) return lt::last_error();
+  auto* p = new lt_ozaki_auto_plan;
+  p->device = ctx->device;
+  p->A = A;
+  p->B = B;
+  p->C = C;
+  p->M = M;
+  p->N = N;
+  p->K = K;
+  cudaStream_t s = nullptr, sb = nullptr;
+  int rc = LT_OK;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&sb, cudaStreamNonBlocking) != cudaSuccess)
+    rc = lt::set_error(LT_ERR_CUDA, "auto plan: stream creation");
+  if (rc == LT_OK) rc = build_auto_plan(p, alpha, beta, tol, s, sb);
+  if (s != nullptr) cudaStreamDestroy(s);
+  if (sb != nullptr) cudaStreamDestroy(sb);
+  if (rc != LT_OK) {
+    destroy_auto_plan(p);
+    return rc;
+  }
+  *plan = p;
+  return lt::ok();
+}
+
+int lt_ozaki_auto_plan_run(lt_ozaki_auto_plan* plan, void* stream) {
+  if (plan == nullptr || plan->exec == nullptr)
+    return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_ozaki_auto_plan_run: no plan");
+  LT_CUDA_TRY(cudaGraphLaunch(plan->exec, lt::as_stream(stream)));
+  return lt::ok();
+}
+
+int lt_ozaki_auto_plan_choice(lt_ozaki_auto_plan* plan, int* slices, int* learned) {
+  if (plan == nullptr) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_ozaki_auto_plan_choice: no plan");
+  int h[2] = {0, 0};
+  LT_CUDA_TRY(cudaMemcpy(h, plan->decision, sizeof h, cudaMemcpyDeviceToHost));
+  if (slices != nullptr) *slices = h[0];
+  if (learned != nullptr) *learned = h[1];
+  return lt::ok();
+}
+
+void lt_ozaki_auto_plan_destroy(lt_ozaki_auto_plan* plan) { destroy_auto_plan(plan); }
+
+}  // extern "C"

@@ -253,6 +253,42 @@ sel::SelScratch* g_sel_scratch[64] = {};
 float* g_sel_host[64] = {};
 }  // namespace
 
+// A feature scratch of one's own (a plan's), in its initial state; the feature kernels leave it so.
+size_t selector_scratch_bytes() { return sizeof(sel::SelScratch); }
+
+int selector_scratch_init(void* scratch, cudaStream_t stream) {
+  auto* sc = static_cast<sel::SelScratch*>(scratch);
+  LT_CUDA_TRY(cudaMemsetAsync(sc, 0, sizeof(sel::SelScratch), stream));
+  LT_CUDA_TRY(cudaMemsetAsync(sc->rmax, 0x80, sizeof(sc->rmax) + sizeof(sc->cmax), stream));  // kNone
+  return LT_OK;
+}
+
+// The two feature kernels (sampled rows and column groups, then the network's forward pass) on
+// `stream` with the caller's scratch; no host synchronisation. The class probabilities are left at
+// selector_probs(scratch).
+int selector_features_async(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol,
+                            const float* params, void* scratch, cudaStream_t stream) {
+  DeviceContext* ctx = context();
+  if (ctx == nullptr) return last_error();
+  auto* sc = static_cast<sel::SelScratch*>(scratch);
+  sel::FeatGrid g;
+  g.rows = static_cast<int>(M < sel::kSampleRows ? M : sel::kSampleRows);
+  g.groups = static_cast<int>((N + 31) / 32 < sel::kColGroups ? (N + 31) / 32 : sel::kColGroups);
+  const int64_t target = 4LL * ctx->sm_count;
+  g.kr = sel::k_segment(K, g.rows, target, 256);
+  g.kc = sel::k_segment(K, g.groups, target, 64);
+  g.rseg = static_cast<int>((K + g.kr - 1) / g.kr);
+  g.cseg = static_cast<int>((K + g.kc - 1) / g.kc);
+  const unsigned blocks = static_cast<unsigned>(g.rows * g.rseg + g.groups * g.cseg);
+  sel::feat_max_fused_kernel<<<blocks, 256, 0, stream>>>(A, B, M, N, K, g, sc);
+  LT_CUDA_TRY(cudaGetLastError());
+  sel::feat_hist_fused_kernel<<<blocks, 256, 0, stream>>>(A, B, M, N, K, g, tol, params, sc);
+  LT_CUDA_TRY(cudaGetLastError());
+  return LT_OK;
+}
+
+const float* selector_probs(const void* scratch) { return static_cast<const sel::SelScratch*>(scratch)->out + 48; }
+
 int selector_infer(const double* A, const double* B, int64_t M, int64_t N, int64_t K, double tol, const float* params,
                    float* feat_dev, float* probs_host, cudaStream_t stream) {
   DeviceContext* ctx = context();
@@ -276,19 +312,7 @@ int selector_infer(const double* A, const double* B, int64_t M, int64_t N, int64
     g_sel_host[dev] = h;
   }
   sel::SelScratch* sc = g_sel_scratch[dev];
-  sel::FeatGrid g;
-  g.rows = static_cast<int>(M < sel::kSampleRows ? M : sel::kSampleRows);
-  g.groups = static_cast<int>((N + 31) / 32 < sel::kColGroups ? (N + 31) / 32 : sel::kColGroups);
-  const int64_t target = 4LL * ctx->sm_count;
-  g.kr = sel::k_segment(K, g.rows, target, 256);
-  g.kc = sel::k_segment(K, g.groups, target, 64);
-  g.rseg = static_cast<int>((K + g.kr - 1) / g.kr);
-  g.cseg = static_cast<int>((K + g.kc - 1) / g.kc);
-  const unsigned blocks = static_cast<unsigned>(g.rows * g.rseg + g.groups * g.cseg);
-  sel::feat_max_fused_kernel<<<blocks, 256, 0, stream>>>(A, B, M, N, K, g, sc);
-  LT_CUDA_TRY(cudaGetLastError());
-  sel::feat_hist_fused_kernel<<<blocks, 256, 0, stream>>>(A, B, M, N, K, g, tol, params, sc);
-  LT_CUDA_TRY(cudaGetLastError());
+  LT_TRY(selector_features_async(A, B, M, N, K, tol, params, sc, stream));
   if (feat_dev != nullptr)
     LT_CUDA_TRY(cudaMemcpyAsync(feat_dev, sc->out, sel::F * sizeof(float), cudaMemcpyDeviceToDevice, stream));
   float* h = g_sel_host[dev];

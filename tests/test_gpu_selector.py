@@ -187,3 +187,57 @@ def test_ozaki_auto_meets_tolerance(cuda, oracle_mod):
         assert oracle_mod.componentwise_error(dC.cpu().numpy(), Cref, den)[0] <= 1e-12
     finally:
         L.lt_set_ozaki_tolerance(1e-15)
+
+
+def _install_weights(lt, on):
+    L = lt.lib()
+    if on:
+        w = np.fromfile(WEIGHTS, dtype=np.float32)
+        lt.check(L.lt_selector_set_params(w.ctypes.data))
+    else:
+        lt.check(L.lt_selector_set_params(None))
+
+
+@pytest.mark.parametrize("weights", [True, False])
+def test_auto_plan_chooses_on_the_device_what_the_host_path_chooses(cuda, oracle_mod, weights):
+    """lt_ozaki_auto_plan: its graph picks the slice count on the device with the same rule and kernels
+    as lt_ozaki_select_info (learned when the network is confident, else the analytic count from the
+    exponent gaps; without weights always the analytic count), and its result is lt_dgemm_ozaki's with
+    that count, bit for bit. A replay after the data behind the pointers changed chooses again."""
+    import libthom_b200 as lt
+
+    if weights and not WEIGHTS.exists():
+        pytest.fail("libthom_b200/selector_weights.bin missing")
+    torch = cuda
+    _install_weights(lt, weights)
+    try:
+        cases = [(300, 200, 150, 0, 0, 1e-12), (256, 320, 700, 8, 0, 1e-14), (90, 17, 500, 30, 40, 1e-15),
+                 (513, 260, 1000, 2, 20, 1e-12)]
+        for M, N, K, phi, smax, tol in cases:
+            A, B, C0 = oracle_mod.make_problem(M, N, K, phi=phi, seed=M + K, smax=smax)
+            dA, dB, dC = to_dev(torch, A), to_dev(torch, B), to_dev(torch, C0)
+            plan = lt.OzakiAutoPlan(dA, dB, dC, M, N, K, 1.5, 0.5, tol)
+            try:
+                for rep in range(2):
+                    if rep == 1:  # new data behind the same pointers
+                        A, B, C0 = oracle_mod.make_problem(M, N, K, phi=(phi + 17) % 40, seed=M + K + 1, smax=smax)
+                        dA.copy_(torch.from_numpy(A))
+                        dB.copy_(torch.from_numpy(B))
+                    dC.copy_(torch.from_numpy(C0))
+                    plan.run()
+                    torch.cuda.synchronize()
+                    lt.device_status()
+                    s, learned = plan.choice()
+                    hs, hlearned, _ = select(torch, A, B, tol)
+                    assert (s, learned) == (hs, hlearned), (M, N, K, rep)
+                    if not weights:
+                        assert not learned
+                    ref = to_dev(torch, C0)
+                    lt.dgemm_ozaki(dA, dB, ref, M, N, K, 1.5, 0.5, slices=s)
+                    torch.cuda.synchronize()
+                    assert np.array_equal(dC.cpu().numpy(), ref.cpu().numpy()), (M, N, K, rep, s)
+            finally:
+                plan.close()
+    finally:
+        _install_weights(lt, WEIGHTS.exists())
+
