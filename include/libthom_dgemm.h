@@ -314,13 +314,18 @@ int lt_ozaki_select_info(const double* A, const double* B, int64_t M, int64_t N,
  * (the data behind them may change between runs) and a CUDA graph that runs the selector's feature
  * kernels and network, the exponent-gap pass only when the network is not confident, picks the slice
  * count on the device with the same rule as lt_ozaki_select_slices, and runs the slice form's split
- * and product for that count through a switch node. A run is one graph launch with no host
- * synchronisation (replayable; it can be captured into a caller's graph as a child). The workspace is
- * sized for LT_OZAKI_MAX_SLICES slices. lt_ozaki_auto_plan_choice reads the last run's choice
- * (synchronous). */
+ * and product for that count through a switch node. forms = LT_AUTO_PLAN_OZAKI: always the slice
+ * form; LT_AUTO_PLAN_ANY_FORM: native FP64 instead wherever lt_dgemm_auto's cost model predicts it
+ * faster than the chosen count (for shapes where it wins even against 3 slices the plan is the FP64
+ * kernel alone, with no selection). A run is one graph launch with no host synchronisation
+ * (replayable; it can be captured into a caller's graph as a child). The workspace is sized for
+ * LT_OZAKI_MAX_SLICES slices. lt_ozaki_auto_plan_choice reads the last run's choice (slices = 0:
+ * native FP64 ran; synchronous). */
+#define LT_AUTO_PLAN_OZAKI 0
+#define LT_AUTO_PLAN_ANY_FORM 1
 typedef struct lt_ozaki_auto_plan lt_ozaki_auto_plan;
 int lt_ozaki_auto_plan_create(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
-                              double alpha, double beta, double tol, lt_ozaki_auto_plan** plan);
+                              double alpha, double beta, double tol, int forms, lt_ozaki_auto_plan** plan);
 int lt_ozaki_auto_plan_run(lt_ozaki_auto_plan* plan, void* stream);
 int lt_ozaki_auto_plan_choice(lt_ozaki_auto_plan* plan, int* slices, int* learned);
 void lt_ozaki_auto_plan_destroy(lt_ozaki_auto_plan* plan);

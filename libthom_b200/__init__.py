@@ -133,7 +133,7 @@ SIGNATURES = {
     "lt_ozaki_analytic_slices": (_i32, [_f64, _i32]),
     "lt_ozaki_gap_bits": (_i32, [_vp, _vp, _i64, _i64, _i64, _c.POINTER(_i32), _vp]),
     "lt_ozaki_select_slices": (_i32, [_vp, _vp, _i64, _i64, _i64, _f64, _c.POINTER(_i32), _vp]),
-    "lt_ozaki_auto_plan_create": (_i32, [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _f64, _c.POINTER(_vp)]),
+    "lt_ozaki_auto_plan_create": (_i32, [_vp, _vp, _vp, _i64, _i64, _i64, _f64, _f64, _f64, _i32, _c.POINTER(_vp)]),
     "lt_ozaki_auto_plan_run": (_i32, [_vp, _vp]),
     "lt_ozaki_auto_plan_choice": (_i32, [_vp, _c.POINTER(_i32), _c.POINTER(_i32)]),
     "lt_ozaki_auto_plan_destroy": (None, [_vp]),
@@ -224,21 +224,25 @@ def dgemm_fp64(A, B, C, M, N, K, alpha=1.0, beta=0.0, stream=None, config: int =
                                          _stream(stream)))
 
 
+LT_AUTO_PLAN_OZAKI, LT_AUTO_PLAN_ANY_FORM = 0, 1
+
+
 class OzakiAutoPlan:
-    """lt_ozaki_auto_plan: slice selection and the slice form in one CUDA graph (device-side choice).
+    """lt_ozaki_auto_plan: slice selection and the slice form (or, with forms=LT_AUTO_PLAN_ANY_FORM,
+    native FP64 where the cost model prefers it) in one CUDA graph with the choice made on the device.
     Holds the tensors' pointers; run() replays the graph on `stream` without host synchronisation."""
 
-    def __init__(self, A, B, C, M, N, K, alpha, beta, tol):
+    def __init__(self, A, B, C, M, N, K, alpha, beta, tol, forms=LT_AUTO_PLAN_OZAKI):
         self._h = ctypes.c_void_p()
         self._keep = (A, B, C)
-        check(lib().lt_ozaki_auto_plan_create(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, tol,
+        check(lib().lt_ozaki_auto_plan_create(_ptr(A), _ptr(B), _ptr(C), M, N, K, alpha, beta, tol, forms,
                                               ctypes.byref(self._h)))
 
     def run(self, stream=None) -> None:
         check(lib().lt_ozaki_auto_plan_run(self._h, _stream(stream)))
 
     def choice(self) -> tuple[int, bool]:
-        """(slice count, learned?) of the last run (synchronous)."""
+        """(slice count, learned?) of the last run; slice count 0: native FP64 ran (synchronous)."""
         s, learned = ctypes.c_int(), ctypes.c_int()
         check(lib().lt_ozaki_auto_plan_choice(self._h, ctypes.byref(s), ctypes.byref(learned)))
         return s.value, bool(learned.value)

@@ -68,7 +68,7 @@ float timed(const char* name, F&& fn) {
 }  // namespace
 
 int dgemm_fp64_dispatch(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
-                        double beta, int config, cudaStream_t stream) {
+                        double beta, int config, cudaStream_t stream, const fp64::ScratchUse* scratch) {
   LT_TRY(check_gemm_args(A, B, C, M, N, K));
   if (M == 0 || N == 0) return ok();
   DeviceContext* ctx = context();
@@ -78,7 +78,7 @@ int dgemm_fp64_dispatch(const double* A, const double* B, double* C, int64_t M, 
   if (config < 0) config = fp64::heuristic_config(A, B, M, N, K, ctx->sm_count);
   if (fp64::config_is_tma(config) && !tma)
     return set_error(LT_ERR_UNALIGNED, "config %s needs 16-byte aligned A/B and even N, K", fp64::config_name(config));
-  LT_TRY(fp64::run_config(config, A, B, C, M, N, K, alpha, beta, stream));
+  LT_TRY(fp64::run_config(config, A, B, C, M, N, K, alpha, beta, stream, scratch));
   return ok();
 }
 
@@ -88,13 +88,13 @@ extern "C" {
 
 int lt_dgemm_fp64(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
                   double beta, void* stream) {
-  return lt::dgemm_fp64_dispatch(A, B, C, M, N, K, alpha, beta, -1, lt::as_stream(stream));
+  return lt::dgemm_fp64_dispatch(A, B, C, M, N, K, alpha, beta, -1, lt::as_stream(stream), nullptr);
 }
 
 int lt_dgemm_fp64_config(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
                          double beta, int config, void* stream) {
   if (config >= lt::fp64::num_configs()) return lt::set_error(LT_ERR_NOT_FOUND, "no FP64 config %d", config);
-  return lt::dgemm_fp64_dispatch(A, B, C, M, N, K, alpha, beta, config, lt::as_stream(stream));
+  return lt::dgemm_fp64_dispatch(A, B, C, M, N, K, alpha, beta, config, lt::as_stream(stream), nullptr);
 }
 
 int lt_fp64_num_configs(void) { return lt::fp64::num_configs(); }

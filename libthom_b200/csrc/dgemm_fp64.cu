@@ -104,11 +104,19 @@ int launch(const Params& p0, cudaStream_t stream, DeviceContext* ctx) {
   p.W = nullptr;
   int64_t grid = tiles * p.splits < cap ? tiles * p.splits : cap;
   if (p.streamk) grid = std::min(cap, tiles * nkb);
-  if (p.splits > 1 || p.streamk) {
-    const size_t bytes = p.streamk ? static_cast<size_t>(2 * grid) * Cfg::BM * Cfg::BN * sizeof(double)
-                                   : static_cast<size_t>(p.splits) * p.M * p.N * sizeof(double);
-    void* w = nullptr;
-    LT_TRY(ensure_splitk_workspace(ctx, bytes, &w));
+  size_t bytes = 0;
+  if (p.splits > 1 || p.streamk)
+    bytes = p.streamk ? static_cast<size_t>(2 * grid) * Cfg::BM * Cfg::BN * sizeof(double)
+                      : static_cast<size_t>(p.splits) * p.M * p.N * sizeof(double);
+  if (p0.scratch_query != nullptr) {
+    *p0.scratch_query = bytes;
+    return LT_OK;
+  }
+  if (bytes > 0) {
+    void* w = p0.scratch;
+    if (w != nullptr && p0.scratch_bytes < bytes)
+      return set_error(LT_ERR_NO_MEMORY, "FP64 scratch of %zu bytes given, %zu needed", p0.scratch_bytes, bytes);
+    if (w == nullptr) LT_TRY(ensure_splitk_workspace(ctx, bytes, &w));
     p.W = static_cast<double*>(w);
   }
   dgemm_fp64_kernel<Cfg><<<static_cast<unsigned>(grid), Cfg::THREADS, Cfg::SMEM_BYTES, stream>>>(tmA, tmB, p);
@@ -441,12 +449,12 @@ void grouped_destroy(GroupedFp64* G) {
 int64_t grouped_tiles(const GroupedFp64* G) { return G->ntiles; }
 
 int run_config(int cfg, const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
-               double beta, cudaStream_t stream) {
-  return run_config_ld(cfg, A, K, B, N, C, N, M, N, K, alpha, beta, stream);
+               double beta, cudaStream_t stream, const ScratchUse* scratch) {
+  return run_config_ld(cfg, A, K, B, N, C, N, M, N, K, alpha, beta, stream, scratch);
 }
 
 int run_config_ld(int cfg, const double* A, int64_t lda, const double* B, int64_t ldb, double* C, int64_t ldc, int64_t M,
-                  int64_t N, int64_t K, double alpha, double beta, cudaStream_t stream) {
+                  int64_t N, int64_t K, double alpha, double beta, cudaStream_t stream, const ScratchUse* scratch) {
   if (cfg < 0 || cfg >= kNumConfigs) return set_error(LT_ERR_INVALID_ARGUMENT, "FP64 config %d out of range", cfg);
   DeviceContext* ctx = context();
   if (ctx == nullptr) return last_error();
@@ -463,6 +471,11 @@ int run_config_ld(int cfg, const double* A, int64_t lda, const double* B, int64_
   p.lda = lda;
   p.ldb = ldb;
   p.ldc = ldc;
+  if (scratch != nullptr) {
+    p.scratch = scratch->ptr;
+    p.scratch_bytes = scratch->bytes;
+    p.scratch_query = scratch->query;
+  }
   return kConfigs[cfg].fn(p, stream, ctx);
 }
 

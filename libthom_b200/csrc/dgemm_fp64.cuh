@@ -57,6 +57,12 @@ struct Params {
   // of a tile shared by several CTAs go to per-CTA slots (W + (2b + j)*BM*BN for CTA b, j = 0 for
   // its first tile, 1 for its last) and streamk_fixup sums them in K order.
   int streamk;
+  // Host side only (not read by the kernels): scratch for the partial sums of the K split and stream-K
+  // schedules supplied by the caller instead of the per-device cache, or, with `scratch_query` set,
+  // the bytes this launch would need, reported there without launching anything.
+  void* scratch;
+  size_t scratch_bytes;
+  size_t* scratch_query;
 };
 
 template <int BM_, int BN_, int STAGES_, bool TMA_>

@@ -20,11 +20,21 @@ const char* config_name(int i);
 bool config_is_tma(int i);
 int heuristic_config(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int sm_count);
 int heuristic_config_for(int64_t M, int64_t N, int64_t K, int sm_count, bool tma);
+// Scratch of a caller for the partial sums of the K split and stream-K schedules, instead of the
+// growable per-device cache (whose reallocation would leave a captured graph pointing at freed memory):
+// with `query` set nothing is launched and the bytes needed are reported there; otherwise `ptr` (at
+// least `bytes`, null when the schedule needs none) is used.
+struct ScratchUse {
+  void* ptr;
+  size_t bytes;
+  size_t* query;
+};
 int run_config(int cfg, const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
-               double beta, cudaStream_t stream);
+               double beta, cudaStream_t stream, const ScratchUse* scratch = nullptr);
 // Same with row strides (lda >= K, ldb >= N, ldc >= N).
 int run_config_ld(int cfg, const double* A, int64_t lda, const double* B, int64_t ldb, double* C, int64_t ldc, int64_t M,
-                  int64_t N, int64_t K, double alpha, double beta, cudaStream_t stream);
+                  int64_t N, int64_t K, double alpha, double beta, cudaStream_t stream,
+                  const ScratchUse* scratch = nullptr);
 }  // namespace fp64
 
 // Selector statistics (selector_stats.cu). selector_infer: the features of one problem (copied to
@@ -35,6 +45,10 @@ int selector_infer(const double* A, const double* B, int64_t M, int64_t N, int64
                    float* feat_dev, float* probs_host, cudaStream_t stream);
 int gap_into(const double* A, const double* B, int64_t M, int64_t N, int64_t K, int* out, void* scratch,
              cudaStream_t stream);
+// Native FP64 DGEMM with the tuned or heuristic tile configuration (capi.cu); scratch as for
+// fp64::run_config (null: the per-device cache).
+int dgemm_fp64_dispatch(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K, double alpha,
+                        double beta, int config, cudaStream_t stream, const fp64::ScratchUse* scratch);
 // A plan's own feature scratch (selector_stats.cu): size, initial state, the two feature kernels
 // without host synchronisation, and the device address of the class probabilities they leave.
 size_t selector_scratch_bytes();

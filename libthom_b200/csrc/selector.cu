@@ -218,9 +218,14 @@ int device_params(const float** out) {
 }
 
 // Learned choice from the network's class probabilities (slice counts 3..10, the last class
-// standing for "10 or more"): the smallest count whose cumulative probability reaches 0.9, if the
-// network is confident (top class >= 0.5) and neither the top class nor that count is the last
-// class. Returns false when the analytic fallback must decide.
+// standing for "10 or more"): the smallest count whose cumulative probability reaches kQuantile, if
+// the network is confident (top class >= 0.5) and neither the top class nor that count is the last
+// class. Returns false when the analytic fallback must decide. kQuantile = 0.999: on 800 held-out
+// problems (2 400 problem-tolerance pairs, selector_train's distribution) it misses the tolerance on
+// none of the reachable ones, as the analytic count does, and picks 8.2 / 9.7 / 11.9 slices on average
+// at 1e-12 / 1e-14 / 1e-15 against the analytic 12.0; the 0.9 quantile saved 0.2 more slices but
+// missed on 11 and 6 reachable problems at 1e-12 and 1e-14.
+constexpr float kQuantile = 0.999f;
 bool decide(const float* probs, int* slices) {
   int top = 0;
   for (int c = 1; c < C; ++c)
@@ -229,7 +234,7 @@ bool decide(const float* probs, int* slices) {
   float cdf = 0.f;
   for (int c = 0; c < C - 1; ++c) {
     cdf += probs[c];
-    if (cdf >= 0.9f) {
+    if (cdf >= kQuantile) {
       *slices = 3 + c;
       return true;
     }
@@ -498,10 +503,15 @@ float dgemm_auto(const double* A, const double* B, double* C, size_t M, size_t N
 //                   otherwise it turns on the IF node below;
 //   IF (not confident): the exponent-gap pass over all of A and B;
 //   decide_final: the analytic count from the gaps when the network was not confident; sets the
-//                 SWITCH node's value to slices - 1;
-//   SWITCH: body s - 1 runs the slice form's split and product with s slices.
-// So the choice never leaves the device: one graph launch per call, no host synchronisation, and the
-// result is what lt_ozaki_select_slices followed by lt_dgemm_ozaki computes (same rule, same kernels).
+//                 SWITCH node's value to the body for that count;
+//   SWITCH: body s (1..LT_OZAKI_MAX_SLICES) runs the slice form's split and product with s slices,
+//           body 0 the native FP64 kernel.
+// So the choice never leaves the device: one graph launch per call, no host synchronisation. With
+// forms = LT_AUTO_PLAN_OZAKI the result is what lt_ozaki_select_slices followed by lt_dgemm_ozaki
+// computes (same rule, same kernels); with LT_AUTO_PLAN_ANY_FORM the count is mapped to body 0 where
+// the cost model of lt_dgemm_auto (estimate_ms) predicts native FP64 faster than that many slices, and
+// a shape where FP64 wins even against 3 slices gets a plan of the FP64 kernel alone (no selection),
+// as lt_dgemm_auto skips the selector there.
 namespace lt {
 namespace sel {
 
@@ -513,7 +523,7 @@ __device__ bool decide_dev(const float* probs, int* slices) {
   float cdf = 0.f;
   for (int c = 0; c < C - 1; ++c) {
     cdf += probs[c];
-    if (cdf >= 0.9f) {
+    if (cdf >= kQuantile) {
       *slices = 3 + c;
       return true;
     }
@@ -539,9 +549,13 @@ __global__ void auto_decide_learned_kernel(const float* probs, int use_net, int*
   cudaGraphSetConditional(fallback, learned ? 0u : 1u);
 }
 
-__global__ void auto_decide_final_kernel(double tol, int* decision, const int* gap, cudaGraphConditionalHandle which) {
+// body_of[s]: the switch body that runs s slices (s itself), or 0, native FP64, where the cost model
+// predicts it faster; decision[2] = the body taken.
+__global__ void auto_decide_final_kernel(double tol, int* decision, const int* gap, const int* body_of,
+                                         cudaGraphConditionalHandle which) {
   if (decision[1] == 0) decision[0] = analytic_dev(tol, gap[0] + gap[1]);
-  cudaGraphSetConditional(which, static_cast<unsigned>(decision[0] - 1));
+  decision[2] = body_of[decision[0]];
+  cudaGraphSetConditional(which, static_cast<unsigned>(decision[2]));
 }
 
 }  // namespace sel
@@ -553,7 +567,8 @@ struct lt_ozaki_auto_plan {
   const double* B = nullptr;
   double* C = nullptr;
   int64_t M = 0, N = 0, K = 0;
-  uint8_t* mem = nullptr;  // feature scratch | gap scratch | gap pair, decision | slice workspace
+  uint8_t* mem = nullptr;  // weights | feature scratch | gap scratch | gap pair, decision | slice workspace
+  void* fp64_scratch = nullptr;  // partial sums of the FP64 body's K split / stream-K schedule, if any
   int* decision = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -595,7 +610,8 @@ int capture_body(cudaStream_t s, cudaGraph_t body, F fn) {
   return LT_OK;
 }
 
-int build_auto_plan(lt_ozaki_auto_plan* p, double alpha, double beta, double tol, cudaStream_t s, cudaStream_t sb) {
+int build_auto_plan(lt_ozaki_auto_plan* p, double alpha, double beta, double tol, int forms, cudaStream_t s,
+                    cudaStream_t sb) {
   const float* shared_params = nullptr;
   LT_TRY(lt::sel::device_params(&shared_params));
   const size_t par_bytes = (sizeof(float) * lt::sel::P + 255) / 256 * 256;
@@ -608,13 +624,45 @@ int build_auto_plan(lt_ozaki_auto_plan* p, double alpha, double beta, double tol
   void* sc = p->mem + par_bytes;
   void* gap_scratch = p->mem + par_bytes + sc_bytes;
   int* gap = reinterpret_cast<int*>(p->mem + par_bytes + sc_bytes + gap_bytes);
-  p->decision = gap + 2;
+  p->decision = gap + 2;                  // {slices, learned, body}
+  int* body_of = gap + 8;                 // LT_OZAKI_MAX_SLICES + 1 ints
   void* ws = p->mem + par_bytes + sc_bytes + gap_bytes + 256;
+  const int64_t M0 = p->M, N0 = p->N, K0 = p->K;
+  const double t64 = lt::sel::estimate_ms(LT_FORM_FP64, M0, N0, K0, 0);
+  int host_body[LT_OZAKI_MAX_SLICES + 1] = {0};
+  for (int sl = 1; sl <= LT_OZAKI_MAX_SLICES; ++sl)
+    host_body[sl] = (forms == LT_AUTO_PLAN_ANY_FORM && !(lt::sel::estimate_ms(LT_FORM_OZAKI, M0, N0, K0, sl) < t64)) ? 0 : sl;
+  // native FP64 alone when it wins even against the fewest slices (as lt_dgemm_auto)
+  const bool fp64_only = forms == LT_AUTO_PLAN_ANY_FORM &&
+                         !(lt::sel::estimate_ms(LT_FORM_OZAKI, M0, N0, K0, 3) + lt::sel::kSelectMs < t64);
   if (params != nullptr)
     LT_CUDA_TRY(cudaMemcpyAsync(params, shared_params, sizeof(float) * lt::sel::P, cudaMemcpyDeviceToDevice, s));
   LT_TRY(lt::selector_scratch_init(sc, s));
   LT_CUDA_TRY(cudaMemsetAsync(gap, 0, 256, s));
+  LT_CUDA_TRY(cudaMemcpyAsync(body_of, host_body, sizeof host_body, cudaMemcpyHostToDevice, s));
   LT_CUDA_TRY(cudaStreamSynchronize(s));
+  const double *A = p->A, *B = p->B;
+  double* C = p->C;
+  const int64_t M = p->M, N = p->N, K = p->K;
+  // The FP64 body keeps lt_dgemm_fp64's schedule with scratch of the plan's own (the per-device cache
+  // may be reallocated after the capture).
+  lt::fp64::ScratchUse fp64_scratch{nullptr, 0, nullptr};
+  if (forms == LT_AUTO_PLAN_ANY_FORM) {
+    size_t need = 0;
+    lt::fp64::ScratchUse q{nullptr, 0, &need};
+    LT_TRY(lt::dgemm_fp64_dispatch(A, B, C, M, N, K, alpha, beta, -1, s, &q));
+    if (need > 0) LT_CUDA_TRY(cudaMalloc(&p->fp64_scratch, need));
+    fp64_scratch = lt::fp64::ScratchUse{p->fp64_scratch, need, nullptr};
+  }
+  auto run_fp64 = [&](cudaStream_t st) {
+    return lt::dgemm_fp64_dispatch(A, B, C, M, N, K, alpha, beta, -1, st, &fp64_scratch);
+  };
+  if (fp64_only) {  // decision stays {0, 0, 0}: native FP64
+    LT_CUDA_TRY(cudaGraphCreate(&p->graph, 0));
+    LT_TRY(capture_body(s, p->graph, run_fp64));
+    LT_CUDA_TRY(cudaGraphInstantiate(&p->exec, p->graph, 0));
+    return LT_OK;
+  }
 
   LT_CUDA_TRY(cudaGraphCreate(&p->graph, 0));
   cudaGraphConditionalHandle h_fallback, h_slices;
@@ -622,9 +670,6 @@ int build_auto_plan(lt_ozaki_auto_plan* p, double alpha, double beta, double tol
   // default: no body (a value past the switch's bodies), set by decide_final on every run
   LT_CUDA_TRY(cudaGraphConditionalHandleCreate(&h_slices, p->graph, LT_OZAKI_MAX_SLICES, cudaGraphCondAssignDefault));
 
-  const double *A = p->A, *B = p->B;
-  double* C = p->C;
-  const int64_t M = p->M, N = p->N, K = p->K;
   LT_CUDA_TRY(cudaStreamBeginCaptureToGraph(s, p->graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
   int rc = LT_OK;
   cudaGraph_t* fb_body = nullptr;
@@ -637,10 +682,10 @@ int build_auto_plan(lt_ozaki_auto_plan* p, double alpha, double beta, double tol
   }
   if (rc == LT_OK) rc = add_conditional(s, h_fallback, cudaGraphCondTypeIf, 1, &fb_body);
   if (rc == LT_OK) {
-    lt::sel::auto_decide_final_kernel<<<1, 1, 0, s>>>(tol, p->decision, gap, h_slices);
+    lt::sel::auto_decide_final_kernel<<<1, 1, 0, s>>>(tol, p->decision, gap, body_of, h_slices);
     if (cudaGetLastError() != cudaSuccess) rc = lt::set_error(LT_ERR_CUDA, "auto plan: decide launch");
   }
-  if (rc == LT_OK) rc = add_conditional(s, h_slices, cudaGraphCondTypeSwitch, LT_OZAKI_MAX_SLICES, &sw_bodies);
+  if (rc == LT_OK) rc = add_conditional(s, h_slices, cudaGraphCondTypeSwitch, LT_OZAKI_MAX_SLICES + 1, &sw_bodies);
   cudaGraph_t captured = p->graph;
   const cudaError_t e = cudaStreamEndCapture(s, &captured);
   if (rc != LT_OK) return rc;
@@ -648,11 +693,15 @@ int build_auto_plan(lt_ozaki_auto_plan* p, double alpha, double beta, double tol
 
   LT_TRY(capture_body(sb, fb_body[0],
                       [&](cudaStream_t st) { return lt::gap_into(A, B, M, N, K, gap, gap_scratch, st); }));
-  for (int b = 0; b < LT_OZAKI_MAX_SLICES; ++b) {
-    const int slices = b + 1;
-    LT_TRY(capture_body(sb, sw_bodies[b], [&](cudaStream_t st) {
-      int r = lt_ozaki_split(A, B, M, N, K, slices, ws, ws_bytes, st);
-      if (r == LT_OK) r = lt_ozaki_product(C, M, N, K, alpha, beta, slices, ws, ws_bytes, st);
+  bool any_fp64 = false;
+  for (int sl = 1; sl <= LT_OZAKI_MAX_SLICES; ++sl) any_fp64 = any_fp64 || host_body[sl] == 0;
+  if (any_fp64)
+    LT_TRY(capture_body(sb, sw_bodies[0], run_fp64));
+  for (int sl = 1; sl <= LT_OZAKI_MAX_SLICES; ++sl) {
+    if (host_body[sl] != sl) continue;  // that count runs native FP64
+    LT_TRY(capture_body(sb, sw_bodies[sl], [&](cudaStream_t st) {
+      int r = lt_ozaki_split(A, B, M, N, K, sl, ws, ws_bytes, st);
+      if (r == LT_OK) r = lt_ozaki_product(C, M, N, K, alpha, beta, sl, ws, ws_bytes, st);
       return r;
     }));
   }
@@ -665,6 +714,7 @@ void destroy_auto_plan(lt_ozaki_auto_plan* p) {
   if (p->exec != nullptr) cudaGraphExecDestroy(p->exec);
   if (p->graph != nullptr) cudaGraphDestroy(p->graph);
   if (p->mem != nullptr) cudaFree(p->mem);
+  if (p->fp64_scratch != nullptr) cudaFree(p->fp64_scratch);
   delete p;
 }
 
@@ -673,10 +723,11 @@ void destroy_auto_plan(lt_ozaki_auto_plan* p) {
 extern "C" {
 
 int lt_ozaki_auto_plan_create(const double* A, const double* B, double* C, int64_t M, int64_t N, int64_t K,
-                              double alpha, double beta, double tol, lt_ozaki_auto_plan** plan) {
+                              double alpha, double beta, double tol, int forms, lt_ozaki_auto_plan** plan) {
   if (plan == nullptr) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_ozaki_auto_plan_create: null plan");
   *plan = nullptr;
-  if (M <= 0 || N <= 0 || K <= 0 || A == nullptr || B == nullptr || C == nullptr || !(tol > 0.0))
+  if (M <= 0 || N <= 0 || K <= 0 || A == nullptr || B == nullptr || C == nullptr || !(tol > 0.0) ||
+      (forms != LT_AUTO_PLAN_OZAKI && forms != LT_AUTO_PLAN_ANY_FORM))
     return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_ozaki_auto_plan_create: bad arguments");
   if (((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(C)) & 7) != 0)
     return lt::set_error(LT_ERR_UNALIGNED, "matrix pointers must be 8-byte aligned");
@@ -695,7 +746,7 @@ int lt_ozaki_auto_plan_create(const double* A, const double* B, double* C, int64
   if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&sb, cudaStreamNonBlocking) != cudaSuccess)
     rc = lt::set_error(LT_ERR_CUDA, "auto plan: stream creation");
-  if (rc == LT_OK) rc = build_auto_plan(p, alpha, beta, tol, s, sb);
+  if (rc == LT_OK) rc = build_auto_plan(p, alpha, beta, tol, forms, s, sb);
   if (s != nullptr) cudaStreamDestroy(s);
   if (sb != nullptr) cudaStreamDestroy(sb);
   if (rc != LT_OK) {
@@ -715,9 +766,9 @@ int lt_ozaki_auto_plan_run(lt_ozaki_auto_plan* plan, void* stream) {
 
 int lt_ozaki_auto_plan_choice(lt_ozaki_auto_plan* plan, int* slices, int* learned) {
   if (plan == nullptr) return lt::set_error(LT_ERR_INVALID_ARGUMENT, "lt_ozaki_auto_plan_choice: no plan");
-  int h[2] = {0, 0};
+  int h[3] = {0, 0, 0};
   LT_CUDA_TRY(cudaMemcpy(h, plan->decision, sizeof h, cudaMemcpyDeviceToHost));
-  if (slices != nullptr) *slices = h[0];
+  if (slices != nullptr) *slices = h[2] == 0 ? 0 : h[0];  // 0: native FP64 ran
   if (learned != nullptr) *learned = h[1];
   return lt::ok();
 }

@@ -183,14 +183,17 @@ def learned_only(probs):
     return 3 + int(np.argmax(np.cumsum(probs) >= 0.9))
 
 
+QUANTILE = 0.999  # the library's kQuantile (selector.cu)
+
+
 def decide(probs, s_analytic):
     """The library's rule (selector.cu, decide): the learned count if the top class has >= 0.5 and
-    neither it nor the 0.9-quantile is the last class; the analytic count otherwise.
+    neither it nor the 0.999-quantile is the last class; the analytic count otherwise.
     Returns (slices, learned?)."""
     top = int(np.argmax(probs))
     if probs[top] < 0.5 or top == len(probs) - 1:
         return s_analytic, False
-    c = int(np.argmax(np.cumsum(probs) >= 0.9))
+    c = int(np.argmax(np.cumsum(np.asarray(probs, dtype=np.float32), dtype=np.float32) >= np.float32(QUANTILE)))
     if c == len(probs) - 1:
         return s_analytic, False
     return 3 + c, True
@@ -242,11 +245,15 @@ def evaluate(torch, gen, params, rows):
 
 def throughput(torch, gen, chosen, limit=150):
     """End-to-end time over held-out problems, selection included: the library's selector
-    (lt_ozaki_select_slices, then Ozaki), the analytic count (gap pass, then Ozaki), fixed s = 8 and
-    s = 10, and native FP64."""
+    (lt_ozaki_select_slices, then Ozaki), the same selection inside a plan's CUDA graph (plan built
+    beforehand, as plans are for repeated calls; one graph launch per call), the plan that may also
+    pick native FP64 (auto_plan) and its host-side counterpart lt_dgemm_auto, the analytic count (gap
+    pass, then Ozaki), fixed s = 8, 10 and 12 (12: the count that meets 1e-12 on every reachable
+    problem of this distribution), and native FP64."""
     L = lt.lib()
     A, B, C = gen.A.data_ptr(), gen.B.data_ptr(), gen.C.data_ptr()
-    tot = dict(selector=0.0, analytic=0.0, fixed8=0.0, fixed10=0.0, fp64=0.0)
+    tot = dict(selector=0.0, selector_plan=0.0, auto_plan=0.0, auto=0.0, analytic=0.0, fixed8=0.0, fixed10=0.0,
+               fixed12=0.0, fp64=0.0)
     flops = 0.0
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -266,11 +273,17 @@ def throughput(torch, gen, chosen, limit=150):
         M, N, K = r["M"], r["N"], r["K"]
         gen.problem(M, N, K, r["phi"], r["smax"], r["seed"])
         flops += 2.0 * M * N * K
+        plan = lt.OzakiAutoPlan(gen.A, gen.B, gen.C, M, N, K, 1.0, 0.0, tol)
+        aplan = lt.OzakiAutoPlan(gen.A, gen.B, gen.C, M, N, K, 1.0, 0.0, tol, forms=lt.LT_AUTO_PLAN_ANY_FORM)
         runs = {
             "selector": lambda: via_selector(M, N, K, tol),
+            "selector_plan": lambda: plan.run(),
+            "auto_plan": lambda: aplan.run(),
+            "auto": lambda: lt.check(L.lt_dgemm_auto(A, B, C, M, N, K, 1.0, 0.0, None, None, None)),
             "analytic": lambda: via_analytic(M, N, K, tol),
             "fixed8": lambda: lt.check(L.lt_dgemm_ozaki(A, B, C, M, N, K, 1.0, 0.0, 8, None)),
             "fixed10": lambda: lt.check(L.lt_dgemm_ozaki(A, B, C, M, N, K, 1.0, 0.0, 10, None)),
+            "fixed12": lambda: lt.check(L.lt_dgemm_ozaki(A, B, C, M, N, K, 1.0, 0.0, 12, None)),
             "fp64": lambda: lt.check(L.lt_dgemm_fp64(A, B, C, M, N, K, 1.0, 0.0, None)),
         }
         for name, fn in runs.items():
@@ -281,6 +294,8 @@ def throughput(torch, gen, chosen, limit=150):
             e1.record()
             e1.synchronize()
             tot[name] += e0.elapsed_time(e1)
+        plan.close()
+        aplan.close()
     return {k: flops / (v * 1e-3) / 1e12 for k, v in tot.items()}, tot
 
 

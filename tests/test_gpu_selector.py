@@ -125,9 +125,9 @@ def test_analytic_fallback_without_weights(cuda, oracle_mod):
 
 def test_trained_selector_gains_over_analytic(cuda, oracle_mod):
     """Held-out problems (seeds never used in training): with the trained weights the selector
-    picks fewer slices than the analytic count on average and still meets the tolerance (checked
-    against the compensated oracle, not the FP64 result the labels came from) on all but a small
-    fraction of the problems where the tolerance is reachable at all. A problem is unreachable when
+    picks fewer slices than the analytic count on average and misses the tolerance (checked against
+    the compensated oracle, not the FP64 result the labels came from) on no more of the problems where
+    it is reachable than the analytic count does. A problem is unreachable when
     even the largest slice count misses the tolerance (wide exponent spread in both operands): no
     choice of s can meet it, so it does not count as a miss of the selector."""
     import libthom_b200 as lt
@@ -139,7 +139,7 @@ def test_trained_selector_gains_over_analytic(cuda, oracle_mod):
     lt.check(L.lt_selector_set_params(w.ctypes.data))
     torch = cuda
     rng = np.random.default_rng(424242)
-    saved, misses, n = [], 0, 0
+    saved, misses, misses_analytic, n = [], 0, 0, 0
 
     def error_at(dA, dB, M, N, K, s, Cref, den):
         dC = torch.zeros(M, N, dtype=torch.float64, device="cuda")
@@ -165,10 +165,11 @@ def test_trained_selector_gains_over_analytic(cuda, oracle_mod):
         if error_at(dA, dB, M, N, K, lt.LT_OZAKI_MAX_SLICES, Cref, den) > tol:
             continue  # unreachable
         misses += error_at(dA, dB, M, N, K, s, Cref, den) > tol
+        misses_analytic += error_at(dA, dB, M, N, K, sa, Cref, den) > tol
         n += 1
     assert np.mean(saved) >= 1.0, saved
     assert n >= 8, n
-    assert misses <= 0.15 * n, (misses, n)
+    assert misses <= misses_analytic, (misses, misses_analytic, n)
 
 
 def test_ozaki_auto_meets_tolerance(cuda, oracle_mod):
@@ -241,3 +242,128 @@ def test_auto_plan_chooses_on_the_device_what_the_host_path_chooses(cuda, oracle
     finally:
         _install_weights(lt, WEIGHTS.exists())
 
+
+
+def test_any_form_plan_picks_native_fp64_where_the_cost_model_does(cuda, oracle_mod):
+    """With LT_AUTO_PLAN_ANY_FORM a shape on which native FP64 beats even 3 slices (512^3) becomes a
+    plan of the FP64 kernel alone (choice: 0 slices), one where the slice form wins (2048^3) keeps the
+    selection; both results are within the FP64 bound against the compensated reference."""
+    import libthom_b200 as lt
+    from conftest import fp64_bound
+
+    torch = cuda
+    _install_weights(lt, WEIGHTS.exists())
+    for n, want_fp64 in ((512, True), (2048, False)):
+        A = torch.empty(n, n, dtype=torch.float64, device="cuda")
+        B = torch.empty_like(A)
+        C = torch.zeros_like(A)
+        lt.fill(A, n * n, 11, 1, 0)
+        lt.fill(B, n * n, 11, 2, 0)
+        rows = torch.linspace(0, n - 1, 4, device="cuda").round().to(torch.int64)
+        Cref = torch.empty(4, n, dtype=torch.float64, device="cuda")
+        den = torch.empty_like(Cref)
+        lt.dot2_rows(A, B, C, n, n, n, 1.0, 0.0, rows, Cref, den)
+        plan = lt.OzakiAutoPlan(A, B, C, n, n, n, 1.0, 0.0, 1e-12, forms=lt.LT_AUTO_PLAN_ANY_FORM)
+        try:
+            plan.run()
+            torch.cuda.synchronize()
+            lt.device_status()
+            s, _ = plan.choice()
+            assert (s == 0) == want_fp64, (n, s)
+            e = lt.componentwise_error(C[rows].contiguous(), Cref, den, Cref.numel())[0]
+            assert e <= (fp64_bound(n) if s == 0 else 1e-12), (n, s, e)
+        finally:
+            plan.close()
+
+
+def test_auto_plan_beats_the_fixed_slice_count_for_the_tolerance(cuda, oracle_mod):
+    """Held-out problems from the selector's own distribution (selector_train.draw_shape: square,
+    tall-skinny and long-K shapes up to 2048, exponent spread phi over 0..64, row/column scaling) at
+    tolerance 1e-12: 8 drawn as they come and 4 from the distribution's tail (scaled rows and
+    columns with phi >= 56), since 1 in 13 of its problems needs 10 or more slices at 1e-12 and a
+    fixed count must cover them (12 on 800 held-out problems). The fixed slice count a user without
+    the selector would need is the smallest meeting the tolerance on every problem of the set where
+    any count does. The plans (LT_AUTO_PLAN_ANY_FORM: the choice inside their graphs, no host round
+    trip, native FP64 where the cost model prefers it to the chosen count) run the whole set in less
+    time than that fixed count, and meet the tolerance wherever it is reachable (errors on 4 sampled
+    rows against the compensated reference on the device)."""
+    import libthom_b200 as lt
+    from libthom_b200 import selector_train as st
+
+    if not WEIGHTS.exists():
+        pytest.fail("libthom_b200/selector_weights.bin missing")
+    torch = cuda
+    _install_weights(lt, True)
+    tol = 1e-12
+    rng = np.random.default_rng(55555)
+    probs = []
+    for i in range(12):
+        fam, M, N, K, phi, smax, seed = st.draw_shape(rng)
+        while i >= 8 and fam == 0:  # the tail: a scaled family
+            fam, M, N, K, phi, smax, seed = st.draw_shape(rng)
+        if i >= 8:
+            phi, smax = int(rng.integers(56, 65)), int(rng.integers(48, 65))
+        A = torch.empty(M, K, dtype=torch.float64, device="cuda")
+        B = torch.empty(K, N, dtype=torch.float64, device="cuda")
+        lt.fill(A, M * K, seed, 1, phi)
+        lt.fill(B, K * N, seed, 2, phi)
+        if smax:
+            lt.scale_rows(A, M, K, seed, 4, smax)
+            lt.scale_cols(B, K, N, seed, 5, smax)
+        C = torch.zeros(M, N, dtype=torch.float64, device="cuda")
+        rows = torch.linspace(0, M - 1, min(M, 4), device="cuda").round().to(torch.int64)
+        Cref = torch.empty(rows.numel(), N, dtype=torch.float64, device="cuda")
+        den = torch.empty_like(Cref)
+        lt.dot2_rows(A, B, C, M, N, K, 1.0, 0.0, rows, Cref, den)
+        probs.append((A, B, C, M, N, K, rows, Cref, den))
+
+    def err(p):
+        A, B, C, M, N, K, rows, Cref, den = p
+        torch.cuda.synchronize()
+        return lt.componentwise_error(C[rows].contiguous(), Cref, den, Cref.numel())[0]
+
+    def run_fixed(p, s):
+        lt.dgemm_ozaki(p[0], p[1], p[2], p[3], p[4], p[5], 1.0, 0.0, slices=s)
+
+    reachable = []
+    for p in probs:
+        run_fixed(p, lt.LT_OZAKI_MAX_SLICES)
+        reachable.append(err(p) <= tol)
+    fixed = None
+    for s in range(3, lt.LT_OZAKI_MAX_SLICES + 1):
+        ok = True
+        for p, r in zip(probs, reachable):
+            if r:
+                run_fixed(p, s)
+                ok = ok and err(p) <= tol
+        if ok:
+            fixed = s
+            break
+    assert fixed is not None and sum(reachable) >= 8, reachable
+    plans = [lt.OzakiAutoPlan(p[0], p[1], p[2], p[3], p[4], p[5], 1.0, 0.0, tol, forms=lt.LT_AUTO_PLAN_ANY_FORM)
+             for p in probs]
+    try:
+        for pl, p, r in zip(plans, probs, reachable):
+            pl.run()
+            if r:
+                assert err(p) <= tol, pl.choice()
+
+        def timed(fn, reps=5):
+            for _ in range(2):
+                fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps
+
+        t_fixed = timed(lambda: [run_fixed(p, fixed) for p in probs])
+        t_plan = timed(lambda: [pl.run() for pl in plans])
+        lt.device_status()
+        chosen = [pl.choice()[0] for pl in plans]
+        assert t_plan < t_fixed, (t_plan, t_fixed, fixed, chosen)
+    finally:
+        for pl in plans:
+            pl.close()
