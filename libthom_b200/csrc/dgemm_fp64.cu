@@ -67,7 +67,10 @@ Schedule choose_schedule(int64_t tiles, int64_t cap, int64_t M, int64_t N, int64
 }
 
 template <class Cfg>
-int launch(const Params& p0, cudaStream_t stream, DeviceContext* ctx) {
+// `scratch` (host side only, kept out of the kernels' Params, whose size costs registers there): the
+// caller's scratch for the K split / stream-K partial sums, or a query of the bytes needed; null: the
+// per-device cache.
+int launch(const Params& p0, cudaStream_t stream, DeviceContext* ctx, const ScratchUse* scratch) {
   Params p = p0;
   p.status = ctx->status;
   CUtensorMap tmA, tmB;
@@ -108,14 +111,14 @@ int launch(const Params& p0, cudaStream_t stream, DeviceContext* ctx) {
   if (p.splits > 1 || p.streamk)
     bytes = p.streamk ? static_cast<size_t>(2 * grid) * Cfg::BM * Cfg::BN * sizeof(double)
                       : static_cast<size_t>(p.splits) * p.M * p.N * sizeof(double);
-  if (p0.scratch_query != nullptr) {
-    *p0.scratch_query = bytes;
+  if (scratch != nullptr && scratch->query != nullptr) {
+    *scratch->query = bytes;
     return LT_OK;
   }
   if (bytes > 0) {
-    void* w = p0.scratch;
-    if (w != nullptr && p0.scratch_bytes < bytes)
-      return set_error(LT_ERR_NO_MEMORY, "FP64 scratch of %zu bytes given, %zu needed", p0.scratch_bytes, bytes);
+    void* w = scratch != nullptr ? scratch->ptr : nullptr;
+    if (w != nullptr && scratch->bytes < bytes)
+      return set_error(LT_ERR_NO_MEMORY, "FP64 scratch of %zu bytes given, %zu needed", scratch->bytes, bytes);
     if (w == nullptr) LT_TRY(ensure_splitk_workspace(ctx, bytes, &w));
     p.W = static_cast<double*>(w);
   }
@@ -137,7 +140,7 @@ int launch(const Params& p0, cudaStream_t stream, DeviceContext* ctx) {
   return LT_OK;
 }
 
-using LaunchFn = int (*)(const Params&, cudaStream_t, DeviceContext*);
+using LaunchFn = int (*)(const Params&, cudaStream_t, DeviceContext*, const ScratchUse*);
 
 struct Entry {
   const char* name;
@@ -471,12 +474,7 @@ int run_config_ld(int cfg, const double* A, int64_t lda, const double* B, int64_
   p.lda = lda;
   p.ldb = ldb;
   p.ldc = ldc;
-  if (scratch != nullptr) {
-    p.scratch = scratch->ptr;
-    p.scratch_bytes = scratch->bytes;
-    p.scratch_query = scratch->query;
-  }
-  return kConfigs[cfg].fn(p, stream, ctx);
+  return kConfigs[cfg].fn(p, stream, ctx, scratch);
 }
 
 }  // namespace fp64

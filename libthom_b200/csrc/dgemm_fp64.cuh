@@ -23,15 +23,14 @@
 // This is exactly what TMA's SWIZZLE_128B writes for boxes {16, BM} and {16, 16}.
 //
 // K-permutation: within a 16-wide k-block, thread t of a quad feeds the MMA's logical k = t+4i
-// (i = 0..3) with the physical k of the 16-byte chunks c1 = 2t + (t >> 1) and c2 = c1 ^ 1
-// (i = 0, 1: k = 2 c1, 2 c1 + 1; i = 2, 3: k = 2 c2, 2 c2 + 1), for A and B alike. The sum over k is
-// unchanged, every A fragment is two 16-byte chunks of a row (128-bit loads), and both fragment loads
-// are free of bank conflicts under the 128-byte swizzle: a 128-bit load is served in quarter-warps
-// (two rows g, g+1 of four lanes), whose chunks {c1} ^ g and {c1} ^ (g+1) are disjoint because the c1
-// of the four threads lie in different chunk pairs {2a, 2a+1}; a 64-bit B load is served in
-// half-warps (four columns of four lanes), whose k rows (k & 7) >> 1 are distinct across the four
-// threads because c1 & 3 (c2 & 3) are. The first permutation, physical k = 4t + i, put k rows i and
-// i + 8 (same swizzle phase) into one half-warp: each B load took 4 wavefronts instead of 2.
+// with physical k = 4t+i (i = 0..3), for A and B alike. The sum over k is unchanged and every A
+// fragment becomes two contiguous 32-byte row segments (128-bit loads). The B fragment loads (64-bit,
+// served in half-warps) then meet k rows i and i + 8 of one swizzle phase in the same half-warp and
+// take 4 wavefronts instead of 2. A permutation without those conflicts exists (thread t reading the
+// chunks c1 = 2t + (t >> 1) and c1 ^ 1): it removed the replays (404 M -> 270 M wavefronts at 4096^3)
+// but ran 3 % slower at 8192^3 (33.1 against 34.0 TF/s, same box): the replays only cost issue slots
+// in a kernel the DMMA pipe bounds, and its per-thread chunk offsets cost address arithmetic under
+// the 168-register cap. Not kept.
 #pragma once
 #include <cuda.h>
 
@@ -57,12 +56,6 @@ struct Params {
   // of a tile shared by several CTAs go to per-CTA slots (W + (2b + j)*BM*BN for CTA b, j = 0 for
   // its first tile, 1 for its last) and streamk_fixup sums them in K order.
   int streamk;
-  // Host side only (not read by the kernels): scratch for the partial sums of the K split and stream-K
-  // schedules supplied by the caller instead of the per-device cache, or, with `scratch_query` set,
-  // the bytes this launch would need, reported there without launching anything.
-  void* scratch;
-  size_t scratch_bytes;
-  size_t* scratch_query;
 };
 
 template <int BM_, int BN_, int STAGES_, bool TMA_>
@@ -335,7 +328,6 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
     // ------------------------------- consumer warps -------------------------------
     const int wm = warp / Cfg::WARPS_N, wn = warp % Cfg::WARPS_N;
     const int g = lane >> 2, tq = lane & 3;
-    const int c1 = 2 * tq + (tq >> 1), c2 = c1 ^ 1;  // this thread's 16-byte K chunks (K-permutation)
     const uint32_t smem_base = smem_u32(smem);
     int stage = 0;
     uint32_t phase = 0;
@@ -369,12 +361,12 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
           const int r0 = wm * Cfg::WM + i * 16 + g;
-          // chunks c1, c2 of rows r0 and r0+8 (the K-permutation above)
+          // physical k 4tq..4tq+3 = chunks 2tq, 2tq+1 of rows r0 and r0+8
           double x0, x1, x2, x3, y0, y1, y2, y3;
-          lds128(x0, x1, sa + a_off(r0, c1));
-          lds128(x2, x3, sa + a_off(r0, c2));
-          lds128(y0, y1, sa + a_off(r0 + 8, c1));
-          lds128(y2, y3, sa + a_off(r0 + 8, c2));
+          lds128(x0, x1, sa + a_off(r0, 2 * tq));
+          lds128(x2, x3, sa + a_off(r0, 2 * tq + 1));
+          lds128(y0, y1, sa + a_off(r0 + 8, 2 * tq));
+          lds128(y2, y3, sa + a_off(r0 + 8, 2 * tq + 1));
           af[i][0] = x0; af[i][1] = y0; af[i][2] = x1; af[i][3] = y1;
           af[i][4] = x2; af[i][5] = y2; af[i][6] = x3; af[i][7] = y3;
         }
@@ -382,7 +374,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
         for (int j = 0; j < 4; ++j) {
           const int n = wn * Cfg::WN + j * 8 + g;
 #pragma unroll
-          for (int i = 0; i < 4; ++i) bf[j][i] = lds64(sb + b_off(2 * (i < 2 ? c1 : c2) + (i & 1), n));
+          for (int i = 0; i < 4; ++i) bf[j][i] = lds64(sb + b_off(4 * tq + i, n));
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[stage]);

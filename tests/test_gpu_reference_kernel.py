@@ -60,9 +60,13 @@ def test_native_and_ozaki_beat_reference_final_at_8192(cuda, ref_final):
         return e0.elapsed_time(e1) / reps
 
     flop = 2.0 * n ** 3
-    t_ref = timed(lambda: ref_final.ref_dgemm_final(A.data_ptr(), B.data_ptr(), C.data_ptr(), n, n, n, 1.5, 0.5))
-    t_fp64 = timed(lambda: lt.dgemm_fp64(A, B, C, n, n, n, 1.5, 0.5))
-    t_oz = timed(lambda: lt.dgemm_ozaki(A, B, C, n, n, n, 1.5, 0.5, slices=8))
+    # alternated and the best of each taken, so that a clock dip during one sample decides nothing
+    t_ref = t_fp64 = t_oz = float("inf")
+    for _ in range(2):
+        t_ref = min(t_ref, timed(lambda: ref_final.ref_dgemm_final(A.data_ptr(), B.data_ptr(), C.data_ptr(), n, n, n,
+                                                                   1.5, 0.5)))
+        t_fp64 = min(t_fp64, timed(lambda: lt.dgemm_fp64(A, B, C, n, n, n, 1.5, 0.5)))
+        t_oz = min(t_oz, timed(lambda: lt.dgemm_ozaki(A, B, C, n, n, n, 1.5, 0.5, slices=8)))
     lt.device_status()
     tf = {k: flop / (v * 1e-3) / 1e12 for k, v in (("reference dgemm_final", t_ref), ("tc100", t_fp64),
                                                    ("ozaki8", t_oz))}
