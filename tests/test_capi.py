@@ -159,3 +159,31 @@ def test_auto_form_cost_model_without_gpu():
     assert lt.estimate_ms(F, 0, 5, 5) == 0.0
     assert lt.estimate_ms(7, 8, 8, 8) == -1.0 and lt.estimate_ms(O, 8, 8, 8, 0) == -1.0
     assert lt.estimate_ms(O, 8, 8, 8, 13) == -1.0
+
+
+def test_auto_plan_rejects_bad_arguments():
+    """lt_ozaki_auto_plan_create checks its arguments before any device work; run/choice reject a
+    missing plan and destroy accepts NULL."""
+    import ctypes
+
+    import libthom_b200 as lt
+
+    L = lt.lib()
+    h = ctypes.c_void_p()
+    p = 0x1000
+    bad = [
+        (p, p, p, 0, 4, 4, 1e-12, lt.LT_AUTO_PLAN_OZAKI),       # empty
+        (p, p, p, 4, 4, -1, 1e-12, lt.LT_AUTO_PLAN_OZAKI),      # negative K
+        (None, p, p, 4, 4, 4, 1e-12, lt.LT_AUTO_PLAN_OZAKI),    # null A
+        (p, p, p, 4, 4, 4, 0.0, lt.LT_AUTO_PLAN_OZAKI),         # no tolerance
+        (p, p, p, 4, 4, 4, 1e-12, 7),                           # unknown forms
+    ]
+    for A, B, C, M, N, K, tol, forms in bad:
+        assert L.lt_ozaki_auto_plan_create(A, B, C, M, N, K, 1.0, 0.0, tol, forms, ctypes.byref(h)) == \
+            lt.LT_ERR_INVALID_ARGUMENT, (M, N, K, tol, forms)
+        assert not h.value
+    assert L.lt_ozaki_auto_plan_create(p + 4, p, p, 4, 4, 4, 1.0, 0.0, 1e-12, 0, ctypes.byref(h)) == lt.LT_ERR_UNALIGNED
+    assert L.lt_ozaki_auto_plan_create(p, p, p, 4, 4, 4, 1.0, 0.0, 1e-12, 0, None) == lt.LT_ERR_INVALID_ARGUMENT
+    assert L.lt_ozaki_auto_plan_run(None, None) == lt.LT_ERR_INVALID_ARGUMENT
+    assert L.lt_ozaki_auto_plan_choice(None, None, None) == lt.LT_ERR_INVALID_ARGUMENT
+    L.lt_ozaki_auto_plan_destroy(None)
