@@ -82,3 +82,24 @@ def test_cli_tune_command_saves_a_table(cuda, tmp_path):
     assert re.search(r"\[best\] 384x256x640: \S+ ", r.stdout), r.stdout
     # one line per shape class, each dimension rounded up to a power of two: 512 256 1024
     assert any(line.startswith("512 256 1024 ") for line in path.read_text().splitlines()), path.read_text()
+
+
+def test_cli_bench_writes_the_reference_csv(cuda, tmp_path):
+    """`libthom bench dgemm <impl>` (the reference's bench_handler, routines/routines.h:132-169, with
+    exportCSV, routines/dgemm/dgemm.cpp:209-219): one `M,N,K,gflops` row per bench size in
+    bench_dgemm_<impl>.csv in the working directory, equal to the medians printed as
+    `[size: n] ==> g`, and each GFLOP/s plausible for the form (2MNK / (ms 1e6), dgemm.cpp:161-165)."""
+    assert CLI.exists()
+    r = subprocess.run([str(CLI), "bench", "dgemm", "ozaki_crt14"], capture_output=True, text=True, timeout=600,
+                       cwd=tmp_path)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    printed = {int(n): float(g) for n, g in re.findall(r"\[size: (\d+)\] ==> (\S+)", r.stdout)}
+    lines = (tmp_path / "bench_dgemm_ozaki_crt14.csv").read_text().strip().splitlines()
+    assert lines[0] == "M,N,K,gflops"
+    rows = [line.split(",") for line in lines[1:]]
+    assert len(rows) == len(printed) >= 3
+    for M, N, K, g in rows:
+        assert M == N == K and int(M) in printed
+        assert abs(float(g) - printed[int(M)]) <= 1e-3 * printed[int(M)] + 1e-3
+        assert 100.0 < float(g) < 400000.0, (M, g)  # 0.1 .. 400 TFLOP/s
+    assert printed[max(printed)] > 50000.0, printed  # the largest size runs the CRT form above 50 TFLOP/s
