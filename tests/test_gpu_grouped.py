@@ -222,3 +222,43 @@ def test_grouped_rejects_bad_problems(cuda):
     plan = ctypes.c_void_p()
     assert L.lt_grouped_plan_create(table, 1, lt.LT_FORM_FP64, 0, ctypes.byref(plan)) == lt.LT_ERR_INVALID_ARGUMENT
     assert L.lt_grouped_plan_create(table, 0, lt.LT_FORM_FP64, 0, ctypes.byref(plan)) == lt.LT_ERR_INVALID_ARGUMENT
+
+
+def test_grouped_fp64_at_the_configuration_size(cuda):
+    """The batched configuration itself: 512 problems with M, N, K log-uniform in [32, 1024] and
+    entries U[-1, 1) (generated on the device), alpha = 1, beta = 0, in one plan run directly and as a
+    CUDA graph. Every problem's componentwise error against cuBLAS FP64 (torch.matmul on the same
+    device buffers) is within the FP64 bound of its K and the largest within 64 u, and the graph replay
+    is bit-identical to the direct run."""
+    import libthom_b200 as lt
+
+    torch = cuda
+    rng = np.random.default_rng(20260)
+    dims = np.rint(np.exp(rng.uniform(np.log(32), np.log(1024), size=(512, 3)))).astype(int)
+    bufs = []
+    table = (lt.GemmProblem * len(dims))()
+    for i, (M, N, K) in enumerate(dims):
+        M, N, K = int(M), int(N), int(K)
+        A = torch.empty(M, K, dtype=torch.float64, device="cuda")
+        B = torch.empty(K, N, dtype=torch.float64, device="cuda")
+        C = torch.zeros(M, N, dtype=torch.float64, device="cuda")
+        lt.fill(A, M * K, 777 + i, 1, 0)
+        lt.fill(B, K * N, 777 + i, 2, 0)
+        bufs.append((A, B, C))
+        table[i] = lt.GemmProblem(M, N, K, A.data_ptr(), B.data_ptr(), C.data_ptr(), 1.0, 0.0)
+    plan_run(torch, table, len(dims), lt.LT_FORM_FP64, 0)
+    direct = [C.clone() for _, _, C in bufs]
+    for _, _, C in bufs:
+        C.zero_()
+    plan_run(torch, table, len(dims), lt.LT_FORM_FP64, 0, graph=True)
+    worst = 0.0
+    for (A, B, C), D, (M, N, K) in zip(bufs, direct, dims):
+        assert torch.equal(C, D)
+        ref = torch.matmul(A, B)
+        den = torch.matmul(A.abs(), B.abs())
+        err = float(((C - ref).abs() / den.clamp_min(1e-300)).max())
+        worst = max(worst, err)
+        assert err <= fp64_bound(int(K)), (M, N, K, err)
+    # statistical bar, far below the worst case (K + 4) u: both sides round their partial sums, and on
+    # this set the largest difference is about 1e-15 (64 u = 7.1e-15)
+    assert worst <= 64 * 2.0 ** -53, worst
