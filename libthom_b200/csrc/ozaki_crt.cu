@@ -14,14 +14,15 @@
 //      plane l of A holds V mod m_l, row-major [M][Kp]; plane l of B holds W mod m_l transposed,
 //      [N][Kp] (K-major, as the tensor core reads both operands).
 //   3. products (tensor cores): for each modulus, one INT8 x INT8 -> INT32 GEMM of the residue
-//      planes (exact), reduced to the symmetric residue c_l of (sum_k V W) mod m_l and stored as the
-//      byte c_l + 128 in residue plane l of C.
+//      planes (exact), reduced to the residue r_l in [0, m_l) of (sum_k V W) and stored as a byte in
+//      residue plane l of C.
 //   4. reconstruction (FP64 ALU, its own kernel): C' = sum_k V W is the integer in (-Mprod/2,
-//      Mprod/2) with C' = c_l (mod m_l). With the CRT basis P_l = (Mprod/m_l) y_l,
-//      y_l = (Mprod/m_l)^-1 mod m_l, split into nl limbs of w bits: L_k = sum_l c_l P_lk (exact in
-//      FP64), Q = rint(L_hi F_hi + L_lo F_lo) (F_k = 2^(w k) / Mprod), D_k = fma(-Q, M_k, L_k) and
-//      C' = Horner of the D_k in base 2^w; then C = fma(alpha, C' 2^-s_i 2^-s_j, beta C0). The CPU oracle (oracle/oracle.c, oracle_crt_dgemm) performs the same arithmetic,
-//      so results are bit-identical.
+//      Mprod/2) with C' = r_l (mod m_l). With the CRT basis P_l = (Mprod/m_l) y_l,
+//      y_l = (Mprod/m_l)^-1 mod m_l, split into nl limbs of w bits: L_k = sum_l (r_l - 128) P_lk plus
+//      128 in limb 0 (exact in FP64; sum_l P_l = 1 mod Mprod, so L = C' mod Mprod), Q = rint(L_hi
+//      F_hi + L_lo F_lo) (F_k = 2^(w k) / Mprod), D_k = fma(-Q, M_k, L_k) and C' = Horner of the D_k
+//      in base 2^w; then C = fma(alpha, C' 2^-s_i 2^-s_j, beta C0). The CPU oracle (oracle/oracle.c,
+//      oracle_crt_dgemm) performs the same arithmetic, so results are bit-identical.
 //
 // Against the slice form (ozaki.cu) the product count is n, not s(s+1)/2: at FP64 accuracy on the
 // 8192^3 workload 14 INT8 products instead of 28. Scaling by the 2-norm rather than by K times the
