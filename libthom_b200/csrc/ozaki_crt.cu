@@ -36,7 +36,7 @@
 // (plane = the modulus) with 128-byte swizzle. Roles (320 threads per CTA):
 //   warp 0      TMA producer (both CTAs)
 //   warp 1      rank 0: MMA issuer for the pair; rank 1: forwards each landed stage to rank 0
-//   warps 2..9  drain: TMEM -> registers, INT32 -> symmetric residue, bytes to the residue planes,
+//   warps 2..9  drain: TMEM -> registers, INT32 -> residue in [0, m), bytes to the residue planes,
 //               then the accumulator goes back to the MMA warp
 // The reconstruction runs afterwards as a separate kernel at full occupancy: done inside the product
 // kernel by a few warps it was latency-bound (one warp per sub-partition, long FP64 chains, global
