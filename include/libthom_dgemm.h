@@ -319,8 +319,9 @@ int lt_ozaki_select_info(const double* A, const double* B, int64_t M, int64_t N,
  * faster than the chosen count (for shapes where it wins even against 3 slices the plan is the FP64
  * kernel alone, with no selection). A run is one graph launch with no host synchronisation
  * (replayable; it can be captured into a caller's graph as a child). The workspace is sized for
- * LT_OZAKI_MAX_SLICES slices. lt_ozaki_auto_plan_choice reads the last run's choice (slices = 0:
- * native FP64 ran; synchronous). */
+ * LT_OZAKI_MAX_SLICES slices. A plan's runs use its own buffers, so runs of one plan must be ordered
+ * (one stream, or events); different plans may run concurrently. lt_ozaki_auto_plan_choice reads the
+ * last run's choice (slices = 0: native FP64 ran; synchronous). */
 #define LT_AUTO_PLAN_OZAKI 0
 #define LT_AUTO_PLAN_ANY_FORM 1
 typedef struct lt_ozaki_auto_plan lt_ozaki_auto_plan;
