@@ -31,6 +31,12 @@
 // but ran 3 % slower at 8192^3 (33.1 against 34.0 TF/s, same box): the replays only cost issue slots
 // in a kernel the DMMA pipe bounds, and its per-thread chunk offsets cost address arithmetic under
 // the 168-register cap. Not kept.
+//
+// Register cap: 8 consumer warps + the producer warp put 3 warps on one SM sub-partition, hence
+// ptxas's 168 registers a thread and a few spills. Issuing the TMA loads from lane 0 of a consumer
+// warp instead (8 warps, 220 registers, no spills; 240 with a second fragment set loaded while the
+// current block's MMAs run) was bit-identical and slower at 8192^3: 32.2 and 29.7 against 34.7
+// TF/s. The producer warp stays.
 #pragma once
 #include <cuda.h>
 
