@@ -163,6 +163,7 @@ const Entry kConfigs[] = {
     {"cpa_64x64_s6", launch<Config<64, 64, 6, false>>, 64, 64, false},
     {"cpa_64x32_s6", launch<Config<64, 32, 6, false>>, 64, 32, false},
     {"cpa_32x32_s6", launch<Config<32, 32, 6, false>>, 32, 32, false},
+    {"tma_64x64_s6_x2", launch<Config<64, 64, 6, true, 2>>, 64, 64, true},
 };
 constexpr int kNumConfigs = static_cast<int>(sizeof(kConfigs) / sizeof(kConfigs[0]));
 
@@ -223,7 +224,9 @@ struct PackJob {
 
 namespace {
 
-// One warp per row (found by binary search over row0), consecutive lanes on consecutive doubles.
+// One warp per row (found by binary search over row0), consecutive lanes on consecutive doubles,
+// four loads in flight per lane before their stores (one load per lane at a time held the copy at
+// about half the HBM rate: rows are a few hundred doubles).
 __global__ void pack_rows_kernel(const PackJob* __restrict__ jobs, int njobs, int64_t total_rows) {
   const int64_t wpb = blockDim.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -238,13 +241,23 @@ __global__ void pack_rows_kernel(const PackJob* __restrict__ jobs, int njobs, in
     const int64_t row = r - j.row0;
     const double* __restrict__ src = j.src + row * j.cols;
     double* __restrict__ dst = j.dst + row * j.dpitch;
-    for (int64_t c = lane; c < j.cols; c += 32) dst[c] = src[c];
+    for (int64_t c0 = lane; c0 < j.cols; c0 += 128) {
+      double v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (c0 + 32 * u < j.cols) v[u] = src[c0 + 32 * u];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (c0 + 32 * u < j.cols) dst[c0 + 32 * u] = v[u];
+    }
   }
 }
 
+// setup_only: sets the kernel's attributes and, when `ctas` is given, stores the number of CTAs a
+// launch runs at most (SMs x CTAs per SM) there; no launch.
 template <class Cfg>
 int launch_grouped(const GroupProblem* problems, const GroupTile* tiles, int64_t ntiles, cudaStream_t stream,
-                   DeviceContext* ctx, bool setup_only) {
+                   DeviceContext* ctx, bool setup_only, int64_t* ctas = nullptr) {
   static std::once_flag once[64];
   static int occupancy[64];
   static cudaError_t attr_err[64];
@@ -259,6 +272,7 @@ int launch_grouped(const GroupProblem* problems, const GroupTile* tiles, int64_t
   });
   LT_CUDA_TRY(attr_err[ctx->device]);
   int64_t grid = static_cast<int64_t>(ctx->sm_count) * occupancy[ctx->device];
+  if (ctas != nullptr) *ctas = grid;
   if (grid > ntiles) grid = ntiles;
   if (grid < 1 || setup_only) return LT_OK;
   GroupedSource src{problems, tiles, ntiles};
@@ -268,7 +282,8 @@ int launch_grouped(const GroupProblem* problems, const GroupTile* tiles, int64_t
   return LT_OK;
 }
 
-using GroupedFn = int (*)(const GroupProblem*, const GroupTile*, int64_t, cudaStream_t, DeviceContext*, bool);
+using GroupedFn = int (*)(const GroupProblem*, const GroupTile*, int64_t, cudaStream_t, DeviceContext*, bool,
+                          int64_t*);
 struct GroupedEntry {
   const char* name;
   GroupedFn fn;
@@ -293,6 +308,10 @@ const GroupedEntry kGrouped[] = {
     {"grouped_tma_64x64_s4", launch_grouped<Config<64, 64, 4, true>>, 64, 64, true},
     {"grouped_tma_32x64_s4", launch_grouped<Config<32, 64, 4, true>>, 32, 64, true},
     {"grouped_tma_32x32_s4", launch_grouped<Config<32, 32, 4, true>>, 32, 32, true},
+    {"grouped_tma_64x64_s6_x2", launch_grouped<Config<64, 64, 6, true, 2>>, 64, 64, true},
+    {"grouped_tma_64x64_s4_x2", launch_grouped<Config<64, 64, 4, true, 2>>, 64, 64, true},
+    {"grouped_tma_64x32_s6_x2", launch_grouped<Config<64, 32, 6, true, 2>>, 64, 32, true},
+    {"grouped_cpa_64x64_s3_x2", launch_grouped<Config<64, 64, 3, false, 2>>, 64, 64, false},
 };
 constexpr int kNumGrouped = static_cast<int>(sizeof(kGrouped) / sizeof(kGrouped[0]));
 
@@ -331,6 +350,25 @@ int grouped_create(const lt_gemm_problem* problems, int count, int cfg, GroupedF
     const int64_t tm = (problems[i].M + bm - 1) / bm, tn = (problems[i].N + bn - 1) / bn;
     for (int64_t a = 0; a < tm; ++a)
       for (int64_t b = 0; b < tn; ++b) tiles.push_back(GroupTile{i, static_cast<int>(a * bm), static_cast<int>(b * bn), 0});
+  }
+  // CTA c of a G-CTA launch takes tiles c, c + G, c + 2G, ... Dealt in plain order, CTA 0 would get
+  // the longest tile of every round and finish up to one long tile after CTA G - 1, so every other
+  // full round is dealt in reverse (the tiles' K falls along the list); the partial last round
+  // stays in order. Only the balance depends on G: every tile is still taken exactly once.
+  {
+    DeviceContext* ctx = context();
+    int64_t G = 0;
+    if (ctx == nullptr) return last_error();
+    LT_TRY(kGrouped[cfg].fn(nullptr, nullptr, static_cast<int64_t>(tiles.size()), nullptr, ctx, true, &G));
+    const int64_t n = static_cast<int64_t>(tiles.size());
+    if (G > 1 && n > G) {
+      std::vector<GroupTile> dealt(tiles);
+      for (int64_t i = 0; i < (n / G) * G; ++i) {
+        const int64_t r = i / G, j = i % G;
+        dealt[r * G + ((r & 1) ? G - 1 - j : j)] = tiles[i];
+      }
+      tiles.swap(dealt);
+    }
   }
   auto* G = new GroupedFp64();
   G->cfg = cfg;
@@ -432,14 +470,14 @@ int grouped_run(const GroupedFp64* G, cudaStream_t stream) {
     pack_rows_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(G->d_pack, G->npack, G->pack_rows);
     LT_CUDA_TRY(cudaGetLastError());
   }
-  return kGrouped[G->cfg].fn(G->d_problems, G->d_tiles, G->ntiles, stream, ctx, false);
+  return kGrouped[G->cfg].fn(G->d_problems, G->d_tiles, G->ntiles, stream, ctx, false, nullptr);
 }
 
 // Kernel attribute set-up only (before a stream capture, which must not contain it).
 int grouped_prepare(const GroupedFp64* G) {
   DeviceContext* ctx = context();
   if (ctx == nullptr) return last_error();
-  return kGrouped[G->cfg].fn(G->d_problems, G->d_tiles, G->ntiles, nullptr, ctx, true);
+  return kGrouped[G->cfg].fn(G->d_problems, G->d_tiles, G->ntiles, nullptr, ctx, true, nullptr);
 }
 
 void grouped_destroy(GroupedFp64* G) {

@@ -64,9 +64,10 @@ struct Params {
   int streamk;
 };
 
-template <int BM_, int BN_, int STAGES_, bool TMA_>
+template <int BM_, int BN_, int STAGES_, bool TMA_, int MINB_ = 1>
 struct Config {
   static constexpr int BM = BM_, BN = BN_, STAGES = STAGES_;
+  static constexpr int MIN_BLOCKS = MINB_;  // CTAs per SM the register budget is sized for
   static constexpr bool kTMA = TMA_;
   static constexpr int BK = 16;  // doubles of K per stage: one 128-byte swizzle row
   static constexpr int WM = 32, WN = 32;
@@ -290,6 +291,16 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
 #pragma unroll
             for (int j = 0; j < Cfg::BN / 16; ++j)
               tma_load_2d(sb + j * 2048, J.tmB, &full[stage], static_cast<int>(n0) + 16 * j, k0);
+            // Grouped launches keep each problem's tensor maps in device memory and consecutive
+            // tiles of a CTA mostly belong to different problems: once this tile's first loads are
+            // out, the next tile's maps are brought into the descriptor cache.
+            if (tmA == nullptr && kb == J.kb0 && t + t_step < t_end) {
+              const Job Jn = src.get(t + t_step);
+              if (Jn.tmA != nullptr) {
+                tma_prefetch_desc(Jn.tmA);
+                tma_prefetch_desc(Jn.tmB);
+              }
+            }
           }
         } else {
           // A: BM rows x 16 doubles as 16-byte pairs (one shared-memory chunk each): one 16-byte
@@ -470,7 +481,7 @@ __device__ __forceinline__ void gemm_body(const CUtensorMap* tmA, const CUtensor
 }
 
 template <class Cfg>
-__global__ void __launch_bounds__(Cfg::THREADS, 1)
+__global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
     dgemm_fp64_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p) {
   SingleSource<Cfg> src{p, (p.M + Cfg::BM - 1) / Cfg::BM, (p.N + Cfg::BN - 1) / Cfg::BN, &tmA, &tmB};
   gemm_body<Cfg>(&tmA, &tmB, src, p.status);
@@ -528,7 +539,7 @@ __global__ void __launch_bounds__(kFixupThreads)
 }
 
 template <class Cfg>
-__global__ void __launch_bounds__(Cfg::THREADS, 1)
+__global__ void __launch_bounds__(Cfg::THREADS, Cfg::MIN_BLOCKS)
     dgemm_fp64_grouped_kernel(GroupedSource src, DeviceStatus* status) {
   gemm_body<Cfg>(nullptr, nullptr, src, status);
 }

@@ -186,11 +186,12 @@ int lt_grouped_plan_create(const lt_gemm_problem* problems, int count, int form,
     p->flops += 2.0 * static_cast<double>(q.M) * static_cast<double>(q.N) * static_cast<double>(q.K);
   int rc;
   if (form == LT_FORM_FP64) {
-    // Without a tuning run: problems with min(M, N) >= 96 on 128x64 TMA tiles, the rest on 32x32
-    // cp.async tiles with a shallow ring (many CTAs per SM), concurrently: the tuner's choice on
-    // 512 problems with dimensions log-uniform in [32, 1024].
-    rc = lt::build_fp64(p, lt::grouped_config_index("grouped_tma_128x64_s6"),
-                        lt::grouped_config_index("grouped_cpa_32x32_s3"), 96);
+    // Without a tuning run: problems with min(M, N) >= 96 on 64x64 TMA tiles, the rest on 64x64
+    // cp.async tiles (no operand packing), both at two CTAs per SM so that one CTA's epilogue and
+    // pipeline fill overlap the other's MMAs; the fastest pair measured on 512 problems with
+    // dimensions log-uniform in [32, 1024] (22.2 TFLOP/s; 128x64 + 32x32 tiles: 20.0).
+    rc = lt::build_fp64(p, lt::grouped_config_index("grouped_tma_64x64_s4_x2"),
+                        lt::grouped_config_index("grouped_cpa_64x64_s3_x2"), 96);
   } else {
     rc = lt::ozaki::grouped_create(problems, count, slices, &p->oz);
   }
@@ -348,13 +349,14 @@ int lt_grouped_plan_tune(lt_grouped_plan* plan, int iters, float* best_ms) {
   std::vector<Cand> cands;
   const int ncfg = lt::fp64::grouped_num_configs();
   for (int c = 0; c < ncfg; ++c) cands.push_back({c, -1, 0});
-  for (int64_t split : {96, 192, 384}) {
+  for (int64_t split : {64, 96, 192, 384}) {
     for (int c = 0; c < ncfg; ++c) {
       const char* nb = lt::fp64::grouped_config_name(c);
       if (strstr(nb, "32x32") != nullptr) continue;  // big class: 64-wide tiles or more
       for (int cs = 0; cs < ncfg; ++cs) {
         const char* ns = lt::fp64::grouped_config_name(cs);
-        if (strstr(ns, "32") == nullptr) continue;  // small class: a 32-wide dimension
+        // small class: a 32-wide dimension, or 64x64 tiles at two CTAs per SM
+        if (strstr(ns, "32") == nullptr && strstr(ns, "_x2") == nullptr) continue;
         cands.push_back({c, cs, split});
       }
     }
