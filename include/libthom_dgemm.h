@@ -243,8 +243,10 @@ int lt_grouped_plan_run_graph(lt_grouped_plan* plan, void* stream);
 int lt_grouped_plan_info(const lt_grouped_plan* plan, int64_t* tiles, double* flops);
 /* Autotunes the plan's FP64 tile configuration on its own problems (validated against cuBLAS FP64,
  * median of `iters` timed runs, scratch outputs): every single tile shape, and two size classes
- * (problems with min(M, N) at or above a threshold on a large tile, the rest on a small one, as
- * two persistent launches); no-op for the Ozaki form. Synchronous. */
+ * (problems with min(M, N) at or above a threshold of 64, 96, 192 or 384 on one configuration, the
+ * rest on a smaller tile or one that runs more CTAs per SM, as two persistent launches); no-op for
+ * the Ozaki form. Synchronous. Untuned plans use 64x64 tiles at two CTAs per SM for both classes
+ * (TMA at min(M, N) >= 96, cp.async below). */
 int lt_grouped_plan_tune(lt_grouped_plan* plan, int iters, float* best_ms);
 /* Name of the kernel configuration the plan runs. */
 int lt_grouped_plan_config(const lt_grouped_plan* plan, char* name, int name_len);
