@@ -130,6 +130,32 @@ def test_stream_k_every_config(cuda, oracle_mod, M, N, K, offset, beta):
         check(C, Cref, den, K, e_cublas, name)
 
 
+def test_long_k_stream_k_at_4096_cubed(cuda, oracle_mod):
+    """4096^3 with the default configuration: 256 k-blocks per 128x64 tile, where the schedule model
+    takes stream-K for its modelled 2 % gain over the 13.84-wave whole-tile grid. Every CTA's range
+    then starts and ends inside tiles, so about 2 x 148 tile pieces go through the fix-up. Checked on
+    sampled rows against the compensated oracle, and against cuBLAS on the same inputs."""
+    import libthom_b200 as lt
+
+    torch = cuda
+    n = 4096
+    A, B, C0 = oracle_mod.make_problem(n, n, n, phi=2, seed=4096)
+    rows = np.array([0, 1, 127, 128, 1337, 2048, 4000, n - 1])
+    Cref, den = oracle_mod.dot2_rows(A, B, C0, 1.5, 0.5, rows=rows)
+    dA, dB = to_dev(torch, A), to_dev(torch, B)
+    dC, dR = to_dev(torch, C0), to_dev(torch, C0)
+    lt.dgemm_fp64(dA, dB, dC, n, n, n, 1.5, 0.5)
+    lt.dgemm_cublas(dA, dB, dR, n, n, n, 1.5, 0.5)
+    torch.cuda.synchronize()
+    lt.device_status()
+    C, R = dC.cpu().numpy(), dR.cpu().numpy()
+    e_cublas = oracle_mod.componentwise_error(R[rows], Cref, den)[0]
+    check(C[rows], Cref, den, n, e_cublas, "4096^3")
+    # every element, not only the sampled rows: within the two kernels' summed error bars of cuBLAS
+    scale = 1.5 * (np.abs(A) @ np.abs(B)) + 0.5 * np.abs(C0)
+    assert np.all(np.abs(C - R) <= 2 * fp64_bound(n) * scale)
+
+
 def test_unaligned_pointers_take_general_path(cuda, oracle_mod):
     M, N, K = 96, 64, 80
     A, B, C0 = oracle_mod.make_problem(M, N, K, seed=4)
